@@ -1,0 +1,649 @@
+/*
+ * CPU restatement of NUC3d's RHS evaluation and TVD-RK3 step.
+ *
+ * TEST INFRASTRUCTURE ONLY (see nuc3d_oracle.h).  Every function cites the
+ * reference file:line whose arithmetic it restates.  Operation order follows
+ * the reference expression by expression so that, compiled with strict IEEE
+ * FP64 (no -ffast-math, no FMA contraction on x86-64), the results are
+ * bitwise identical to the reference's own code.  Two details matter for
+ * that:
+ *   - the reference writes squares two ways.  std::pow(x, 2) with a literal
+ *     exponent is folded to x*x by the compiler; std::pow(x, p) with the
+ *     scheme's int member p is a libm pow() call, which differs from x*x by
+ *     one ulp for about 0.1% of inputs.  SQ() and PW() below keep them apart.
+ *   - Sutherland's T^1.5 is libm pow(T, 1.5) (physicsModel.cpp:220).
+ */
+#include "nuc3d_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* The reference's schemes hold p = 2 as a runtime member (weno5js.cpp:9,
+ * weno5z.cpp:8, crweno5.cpp:15).  Keeping it in a global stops the compiler
+ * from folding pow(x, p) into x*x, as it cannot in the reference. */
+int or_weno_p = 2;
+
+#define SQ(x) ((x) * (x))
+#define PW(x) pow((x), (double)or_weno_p)
+
+/* schemes.hpp:14-36 */
+static const double A[3][3] = {{1.0 / 3.0, -7.0 / 6.0, 11.0 / 6.0},
+                               {-1.0 / 6.0, 5.0 / 6.0, 1.0 / 3.0},
+                               {1.0 / 3.0, 5.0 / 6.0, -1.0 / 6.0}};
+static const double C_W5[3] = {0.1, 0.6, 0.3};
+static const double C_CR5[3] = {0.2, 0.5, 0.3};
+static const double G0 = 13.0 / 12.0;
+static const double G1 = 1.0 / 4.0;
+static const double CD6[3] = {3.0 / 4.0, -3.0 / 20.0, 1.0 / 60.0};
+
+/* ---------------------------------------------------------------- WENO5 --- */
+
+/* WENO5-JS on an upwind-oriented stencil f[0..4] (f[0] farthest upwind).
+ * weno5js.cpp:75-108 (inner +), :156-189 (inner -), :275-308 (halo forms);
+ * all four are this expression on differently gathered stencils.  eps=1e-6. */
+static double weno5js_face(const double f[5]) {
+    const double ss = 1.0e-6;
+    double is0 = G0 * SQ(f[0] - 2.0 * f[1] + f[2]) + G1 * SQ(f[0] - 4.0 * f[1] + 3.0 * f[2]);
+    double is1 = G0 * SQ(f[1] - 2.0 * f[2] + f[3]) + G1 * SQ(f[1] - f[3]);
+    double is2 = G0 * SQ(f[2] - 2.0 * f[3] + f[4]) + G1 * SQ(3.0 * f[2] - 4.0 * f[3] + f[4]);
+    double q30 = A[0][0] * f[0] + A[0][1] * f[1] + A[0][2] * f[2];
+    double q31 = A[1][0] * f[1] + A[1][1] * f[2] + A[1][2] * f[3];
+    double q32 = A[2][0] * f[2] + A[2][1] * f[3] + A[2][2] * f[4];
+    double alpha0 = C_W5[0] / PW(ss + is0);
+    double alpha1 = C_W5[1] / PW(ss + is1);
+    double alpha2 = C_W5[2] / PW(ss + is2);
+    double alphaSum = alpha0 + alpha1 + alpha2;
+    double omega0 = alpha0 / alphaSum;
+    double omega1 = alpha1 / alphaSum;
+    double omega2 = alpha2 / alphaSum;
+    return omega0 * q30 + omega1 * q31 + omega2 * q32;
+}
+
+/* WENO5-Z, weno5z.cpp:74-109 and the halo forms :275-310.  eps=1e-40.
+ * beta2_quirk reproduces weno5z.cpp:80 (inner '+' only): the first term of
+ * beta2 reads f[i]-2f[i+1]+f[i+1] instead of f[i]-2f[i+1]+f[i+2]. */
+static double weno5z_face(const double f[5], int beta2_quirk) {
+    const double ss = 1.0e-40;
+    double is0 = G0 * PW(f[0] - 2.0 * f[1] + f[2]) + G1 * PW(f[0] - 4.0 * f[1] + 3.0 * f[2]);
+    double is1 = G0 * PW(f[1] - 2.0 * f[2] + f[3]) + G1 * PW(f[1] - f[3]);
+    double is2 = beta2_quirk
+                     ? G0 * PW(f[2] - 2.0 * f[3] + f[3]) + G1 * PW(3.0 * f[2] - 4.0 * f[3] + f[4])
+                     : G0 * PW(f[2] - 2.0 * f[3] + f[4]) + G1 * PW(3.0 * f[2] - 4.0 * f[3] + f[4]);
+    double q30 = A[0][0] * f[0] + A[0][1] * f[1] + A[0][2] * f[2];
+    double q31 = A[1][0] * f[1] + A[1][1] * f[2] + A[1][2] * f[3];
+    double q32 = A[2][0] * f[2] + A[2][1] * f[3] + A[2][2] * f[4];
+    double tau = fabs(is2 - is0);
+    double alpha0 = C_W5[0] * (1.0 + PW(tau / (is0 + ss)));
+    double alpha1 = C_W5[1] * (1.0 + PW(tau / (is1 + ss)));
+    double alpha2 = C_W5[2] * (1.0 + PW(tau / (is2 + ss)));
+    double alphaSum = alpha0 + alpha1 + alpha2;
+    double omega0 = alpha0 / alphaSum;
+    double omega1 = alpha1 / alphaSum;
+    double omega2 = alpha2 / alphaSum;
+    return omega0 * q30 + omega1 * q31 + omega2 * q32;
+}
+
+/* One compact-WENO row (crweno5.cpp:131-162 for '+', :311-341 for '-').
+ * f[0..4] is the upwind-oriented 5-cell stencil of the row's cell i
+ * ('+': cells i-2..i+2; '-': cells i+3..i-1), so f[1], f[2], f[3] are the
+ * row's three right-hand-side cells in upwind order.  Returns the coefficient
+ * of the upwind-side neighbour face (lo), the diagonal (b), the downwind-side
+ * neighbour (hi) and the right-hand side d. */
+static void crweno5_row(const double f[5], double *lo, double *b, double *hi, double *d) {
+    const double ss = 1.0e-6;
+    double is0 = G0 * SQ(f[0] - 2.0 * f[1] + f[2]) + G1 * SQ(f[0] - 4.0 * f[1] + 3.0 * f[2]);
+    double is1 = G0 * SQ(f[1] - 2.0 * f[2] + f[3]) + G1 * SQ(f[1] - f[3]);
+    double is2 = G0 * SQ(f[2] - 2.0 * f[3] + f[4]) + G1 * SQ(3.0 * f[2] - 4.0 * f[3] + f[4]);
+    double alpha0 = C_CR5[0] / PW(ss + is0);
+    double alpha1 = C_CR5[1] / PW(ss + is1);
+    double alpha2 = C_CR5[2] / PW(ss + is2);
+    double alphaSum = alpha0 + alpha1 + alpha2;
+    double omega0 = alpha0 / alphaSum;
+    double omega1 = alpha1 / alphaSum;
+    double omega2 = alpha2 / alphaSum;
+    *lo = 2.0 / 3.0 * omega0 + 1.0 / 3.0 * omega1;
+    *b = 1.0 / 3.0 * omega0 + 2.0 / 3.0 * (omega1 + omega2);
+    *hi = 1.0 / 3.0 * omega2;
+    *d = 1.0 / 6.0 * omega0 * f[1] + (5.0 * (omega0 + omega1) + omega2) * f[2] / 6.0 +
+         (omega1 + 5.0 * omega2) * f[3] / 6.0;
+}
+
+/* Gather the upwind-oriented stencil of face m from a line whose cell c lives
+ * at line[c] (line must cover cells -3..n+2).  '+': cells m-3..m+1 (face m is
+ * the left face of cell m, weno5js.cpp:108 writes face i+1 from cells
+ * i-2..i+2); '-': cells m+2..m-2. */
+static void face_stencil(const double *line, int m, int upwind, double f[5]) {
+    for (int k = 0; k < 5; ++k) f[k] = upwind > 0 ? line[m - 3 + k] : line[m + 2 - k];
+}
+
+/* Thomas sweep exactly as crweno5.cpp:208-219: rows 0..M-1 with a (sub),
+ * b (diag), c (super); row 0 must be an identity row.  Solution to x. */
+static void thomas_ref(int M, double *a, double *b, double *c, double *d, double *x) {
+    for (int i = 1; i < M; i++) {
+        c[i] = c[i] / (b[i] - c[i - 1] * a[i]);
+        d[i] = (d[i] - d[i - 1] * a[i]) / (b[i] - c[i - 1] * a[i]);
+    }
+    x[M - 1] = d[M - 1];
+    for (int i = M - 2; i >= 0; i--) x[i] = d[i] - c[i] * x[i + 1];
+}
+
+/* Reconstruct all n+1 faces of one line.  line[] covers cells -3..n+2 (index
+ * with line[c], c may be negative).  out[m], m=0..n.  This is what
+ * interpolationInner + interpolationBoundaryL + interpolationBoundaryR
+ * produce for one line (fieldOperator.cpp:387-465):
+ *   faces 0..2   boundary-L form (halo), faces n-2..n boundary-R form,
+ *   faces 3..n-3 inner form (for CRWENO5: the tridiagonal solve whose first
+ *                and last rows are identity rows holding WENO5-JS values). */
+static void reconstruct_line_ref(int scheme, int upwind, unsigned quirks, int n,
+                                 const double *line, double *out, double *work) {
+    double f[5];
+    if (scheme == OR_CRWENO5) {
+        for (int m = 0; m <= 2 && m <= n; ++m) {
+            face_stencil(line, m, upwind, f);
+            out[m] = weno5js_face(f);
+        }
+        for (int m = n - 2; m <= n; ++m) {
+            if (m < 0) continue;
+            face_stencil(line, m, upwind, f);
+            out[m] = weno5js_face(f);
+        }
+        /* rows for cells i = 2..n-4, i.e. faces 3..n-3 (crweno5.cpp:76-219) */
+        int ibeg = 2, iend = n - 3, M = iend - ibeg;
+        if (M < 2) return;
+        double *a = work, *b = work + M, *c = work + 2 * M, *d = work + 3 * M, *x = work + 4 * M;
+        for (int r = 0; r < M; ++r) {
+            int i = ibeg + r;
+            if (r == 0 || r == M - 1) {
+                face_stencil(line, i + 1, upwind, f);
+                a[r] = 0.0;
+                b[r] = 1.0;
+                c[r] = 0.0;
+                d[r] = weno5js_face(f);
+            } else {
+                double lo, bb, hi, dd;
+                if (upwind > 0) {
+                    for (int k = 0; k < 5; ++k) f[k] = line[i - 2 + k];
+                    crweno5_row(f, &lo, &bb, &hi, &dd);
+                    a[r] = lo;  /* couples face i   (crweno5.cpp:156) */
+                    c[r] = hi;  /* couples face i+2 (crweno5.cpp:158) */
+                } else {
+                    for (int k = 0; k < 5; ++k) f[k] = line[i + 3 - k];
+                    crweno5_row(f, &lo, &bb, &hi, &dd);
+                    c[r] = lo;  /* crweno5.cpp:335: upwind side is face i+2 */
+                    a[r] = hi;  /* crweno5.cpp:337 */
+                }
+                b[r] = bb;
+                d[r] = dd;
+            }
+        }
+        thomas_ref(M, a, b, c, d, x);
+        for (int r = 0; r < M; ++r) out[ibeg + 1 + r] = x[r];
+        return;
+    }
+    for (int m = 0; m <= n; ++m) {
+        face_stencil(line, m, upwind, f);
+        int inner = (m >= 3 && m <= n - 3);
+        if (scheme == OR_WENO5JS)
+            out[m] = weno5js_face(f);
+        else
+            out[m] = weno5z_face(f, upwind > 0 && inner && (quirks & OR_Q_WENOZ_BETA2));
+    }
+}
+
+/* Solve the periodic (cyclic) tridiagonal system a x[i-1] + b x[i] + c x[i+1]
+ * = d, i = 0..n-1 with wrap-around, by Sherman-Morrison on two Thomas solves.
+ * Used by the periodic CRWENO5 form (quirk bit OR_Q_CRWENO_BOUNDED cleared),
+ * which the reference does not have. */
+static void cyclic_solve(int n, const double *a, const double *b, const double *c,
+                         const double *d, double *x, double *w) {
+    double *bb = w, *u = w + n, *cp = w + 2 * n, *dp = w + 3 * n, *z = w + 4 * n;
+    double gamma = -b[0];
+    for (int i = 0; i < n; ++i) bb[i] = b[i];
+    bb[0] = b[0] - gamma;
+    bb[n - 1] = b[n - 1] - a[0] * c[n - 1] / gamma;
+    /* Thomas on (a, bb, c) for rhs d -> x and rhs u -> z */
+    for (int pass = 0; pass < 2; ++pass) {
+        const double *rhs = d;
+        double *sol = x;
+        if (pass == 1) {
+            for (int i = 0; i < n; ++i) u[i] = 0.0;
+            u[0] = gamma;
+            u[n - 1] = c[n - 1];
+            rhs = u;
+            sol = z;
+        }
+        cp[0] = c[0] / bb[0];
+        dp[0] = rhs[0] / bb[0];
+        for (int i = 1; i < n; ++i) {
+            double den = bb[i] - a[i] * cp[i - 1];
+            cp[i] = c[i] / den;
+            dp[i] = (rhs[i] - a[i] * dp[i - 1]) / den;
+        }
+        sol[n - 1] = dp[n - 1];
+        for (int i = n - 2; i >= 0; --i) sol[i] = dp[i] - cp[i] * sol[i + 1];
+    }
+    double fact = (x[0] + a[0] * x[n - 1] / gamma) / (1.0 + z[0] + a[0] * z[n - 1] / gamma);
+    for (int i = 0; i < n; ++i) x[i] -= fact * z[i];
+}
+
+static void reconstruct_line_periodic_crweno(int upwind, int n, const double *line, double *out,
+                                             double *work) {
+    double *a = work, *b = work + n, *c = work + 2 * n, *d = work + 3 * n, *x = work + 4 * n;
+    double *w = work + 5 * n;
+    double f[5];
+    for (int m = 0; m < n; ++m) {
+        int i = m - 1; /* row of face m belongs to cell i = m-1 */
+        double lo, bb, hi, dd;
+        if (upwind > 0) {
+            for (int k = 0; k < 5; ++k) f[k] = line[i - 2 + k];
+            crweno5_row(f, &lo, &bb, &hi, &dd);
+            a[m] = lo;
+            c[m] = hi;
+        } else {
+            for (int k = 0; k < 5; ++k) f[k] = line[i + 3 - k];
+            crweno5_row(f, &lo, &bb, &hi, &dd);
+            c[m] = lo;
+            a[m] = hi;
+        }
+        b[m] = bb;
+        d[m] = dd;
+    }
+    cyclic_solve(n, a, b, c, d, x, w);
+    for (int m = 0; m < n; ++m) out[m] = x[m];
+    out[n] = x[0];
+}
+
+int or_reconstruct_field(int scheme, int upwind, unsigned quirks, int nx, int ny, int nz,
+                         const double *in, const double *halo_l, const double *halo_r,
+                         double *out) {
+    if (nx < 5 || (upwind != 1 && upwind != -1)) return -1;
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(nx + 6));
+    double *work = (double *)malloc(sizeof(double) * (size_t)(10 * (nx + 1)));
+    double *line = buf + 3;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j) {
+            for (int c = 0; c < 3; ++c) {
+                line[c - 3] = halo_l[c + 3 * (j + ny * k)];
+                line[nx + c] = halo_r[c + 3 * (j + ny * k)];
+            }
+            for (int i = 0; i < nx; ++i) line[i] = in[i + nx * (j + ny * k)];
+            reconstruct_line_ref(scheme, upwind, quirks, nx, line,
+                                 out + (size_t)(nx + 1) * (j + ny * k), work);
+        }
+    free(buf);
+    free(work);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ CD6 --- */
+
+/* centraldifference6th.cpp:44-46 (inner) and :111-113 / :179-181 (halo). */
+static double cd6_at(const double *line, int i, double dx) {
+    return (CD6[2] * (line[i + 3] - line[i - 3]) + CD6[1] * (line[i + 2] - line[i - 2]) +
+            CD6[0] * (line[i + 1] - line[i - 1])) /
+           dx;
+}
+
+int or_cd6_field(int nx, int ny, int nz, double dx, const double *in, const double *halo_l,
+                 const double *halo_r, double *out) {
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(nx + 6));
+    double *line = buf + 3;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j) {
+            for (int c = 0; c < 3; ++c) {
+                line[c - 3] = halo_l[c + 3 * (j + ny * k)];
+                line[nx + c] = halo_r[c + 3 * (j + ny * k)];
+            }
+            for (int i = 0; i < nx; ++i) line[i] = in[i + nx * (j + ny * k)];
+            for (int i = 0; i < nx; ++i) out[i + nx * (j + ny * k)] = cd6_at(line, i, dx);
+        }
+    free(buf);
+    return 0;
+}
+
+/* ------------------------------------------------------------ physics ---- */
+
+void or_con2prim(const or_box *b, const double *const q[5], double *const prim[8]) {
+    /* physicsModel.cpp:317-356 */
+    const double gamma = b->gamma, Mach = b->mach;
+    const long N = (long)b->nx * b->ny * b->nz;
+    for (long n = 0; n < N; ++n) {
+        double rho = q[0][n];
+        double u = q[1][n] / rho;
+        double v = q[2][n] / rho;
+        double w = q[3][n] / rho;
+        double E = q[4][n];
+        double p = (E - 0.5 * rho * (u * u + v * v + w * w)) * (gamma - 1.0);
+        if (b->quirks & OR_Q_FABS_PRESSURE) p = fabs(p);
+        double e = p / rho / (gamma - 1.0);
+        double alpha = sqrt(gamma * p / rho);
+        double T = gamma * Mach * Mach * p / rho;
+        prim[0][n] = rho;
+        prim[1][n] = u;
+        prim[2][n] = v;
+        prim[3][n] = w;
+        prim[4][n] = p;
+        prim[5][n] = T;
+        prim[6][n] = e;
+        prim[7][n] = alpha;
+    }
+}
+
+void or_lf_split(const or_box *b, const double *const q[5], const double *const prim[8],
+                 double *const fl[3][5], double *const fr[3][5], double eig[3]) {
+    /* physicsModel.cpp:520-679.  The three loops run in the reference's order
+     * (xi, eta, zeta) so the running fmax values match. */
+    const long N = (long)b->nx * b->ny * b->nz;
+    double me[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < 3; ++d) {
+        int slot = d;
+        if (d == 2 && (b->quirks & OR_Q_ZETA_EIGEN)) slot = 1; /* :653-654 */
+        for (long n = 0; n < N; ++n) {
+            double un = prim[1 + d][n];
+            double p0 = prim[4][n];
+            double alpha0 = prim[7][n];
+            double Q[5] = {q[0][n], q[1][n], q[2][n], q[3][n], q[4][n]};
+            double lam = fabs(un) + alpha0;
+            me[slot] = fmax(lam, me[slot]);
+            double flux[5];
+            flux[0] = un * Q[0];
+            flux[1] = un * Q[1];
+            flux[2] = un * Q[2];
+            flux[3] = un * Q[3];
+            flux[1 + d] = un * Q[1 + d] + p0;
+            flux[4] = un * (Q[4] + p0);
+            for (int e = 0; e < 5; ++e) {
+                fl[d][e][n] = 0.5 * (flux[e] + lam * Q[e]);
+                fr[d][e][n] = 0.5 * (flux[e] - lam * Q[e]);
+            }
+        }
+    }
+    eig[0] = me[0];
+    eig[1] = me[1];
+    eig[2] = me[2];
+}
+
+/* physicsModel.cpp:193-266 (+ an extra power-law model). */
+static void viscosity(const or_box *b, double T, double *miu, double *coeff) {
+    double m;
+    if (b->visc_model == OR_SUTHERLAND) {
+        double non_dim_T_ref = b->t_ref / b->t_inf;
+        m = (1.0 + non_dim_T_ref) / (T + non_dim_T_ref) * pow(T, 1.5) / b->reynolds;
+    } else if (b->visc_model == OR_CONSTANT) {
+        m = 1.0 / b->reynolds;
+    } else {
+        m = pow(T, b->powerlaw_exp) / b->reynolds;
+    }
+    *miu = m;
+    *coeff = m / ((b->gamma - 1.0) * b->mach * b->mach * b->prandtl);
+}
+
+/* --------------------------------------------------------------- RHS ---- */
+
+typedef struct {
+    long base;
+    long stride;
+} line_t;
+
+static long dir_stride(const or_box *b, int d) {
+    return d == 0 ? 1 : (d == 1 ? (long)b->nx : (long)b->nx * b->ny);
+}
+static int dir_len(const or_box *b, int d) { return d == 0 ? b->nx : (d == 1 ? b->ny : b->nz); }
+
+/* enumerate line bases for direction d */
+static long line_base(const or_box *b, int d, int a, int c) {
+    /* a, c: the two transverse indices in increasing memory order */
+    if (d == 0) return (long)b->nx * (a + (long)b->ny * c);  /* a=j, c=k */
+    if (d == 1) return a + (long)b->nx * b->ny * c;          /* a=i, c=k */
+    return a + (long)b->nx * c;                              /* a=i, c=j */
+}
+static void line_counts(const or_box *b, int d, int *na, int *nc) {
+    if (d == 0) { *na = b->ny; *nc = b->nz; }
+    else if (d == 1) { *na = b->nx; *nc = b->nz; }
+    else { *na = b->nx; *nc = b->ny; }
+}
+
+static void gather_periodic(const double *src, long base, long stride, int n, double *line) {
+    for (int c = -3; c < n + 3; ++c) {
+        int cc = ((c % n) + n) % n;
+        line[c] = src[base + (long)cc * stride];
+    }
+}
+
+/* Inviscid derivative of one direction (euler3d.cpp:307-387 solveInv,
+ * :23-56 combineFluxLR, :143-253 setDerivatives*Inv): for every equation,
+ * F^ = F^+(face) + F^-(face), dF/dx(cell i) = (F^[i+1] - F^[i]) / delta. */
+static void inviscid_direction(const or_box *b, int d, double *const fl[5], double *const fr[5],
+                               double *const df[5]) {
+    int n = dir_len(b, d);
+    long s = dir_stride(b, d);
+    double delta = d == 0 ? b->dx : (d == 1 ? b->dy : b->dz);
+    int na, nc;
+    line_counts(b, d, &na, &nc);
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(n + 6));
+    double *line = buf + 3;
+    double *rp = (double *)malloc(sizeof(double) * (size_t)(n + 1));
+    double *rn = (double *)malloc(sizeof(double) * (size_t)(n + 1));
+    double *work = (double *)malloc(sizeof(double) * (size_t)(10 * (n + 1)));
+    int periodic_cr = b->scheme[d] == OR_CRWENO5 && !(b->quirks & OR_Q_CRWENO_BOUNDED);
+    for (int e = 0; e < 5; ++e)
+        for (int c = 0; c < nc; ++c)
+            for (int a = 0; a < na; ++a) {
+                long base = line_base(b, d, a, c);
+                gather_periodic(fl[e], base, s, n, line);
+                if (periodic_cr)
+                    reconstruct_line_periodic_crweno(1, n, line, rp, work);
+                else
+                    reconstruct_line_ref(b->scheme[d], 1, b->quirks, n, line, rp, work);
+                gather_periodic(fr[e], base, s, n, line);
+                if (periodic_cr)
+                    reconstruct_line_periodic_crweno(-1, n, line, rn, work);
+                else
+                    reconstruct_line_ref(b->scheme[d], -1, b->quirks, n, line, rn, work);
+                for (int m = 0; m <= n; ++m) rp[m] = rp[m] + rn[m];
+                for (int i = 1; i <= n; ++i) {
+                    double df_loc = rp[i] - rp[i - 1];
+                    df[e][base + (long)(i - 1) * s] = df_loc / delta;
+                }
+            }
+    free(buf);
+    free(rp);
+    free(rn);
+    free(work);
+}
+
+/* CD6 along direction d of a periodic field (the halo exchange with one
+ * rank is the periodic wrap). */
+static void cd6_direction(const or_box *b, int d, const double *src, double *dst) {
+    int n = dir_len(b, d);
+    long s = dir_stride(b, d);
+    double delta = d == 0 ? b->dx : (d == 1 ? b->dy : b->dz);
+    int na, nc;
+    line_counts(b, d, &na, &nc);
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(n + 6));
+    double *line = buf + 3;
+    for (int c = 0; c < nc; ++c)
+        for (int a = 0; a < na; ++a) {
+            long base = line_base(b, d, a, c);
+            gather_periodic(src, base, s, n, line);
+            for (int i = 0; i < n; ++i) dst[base + (long)i * s] = cd6_at(line, i, delta);
+        }
+    free(buf);
+}
+
+static double *alloc_fields(int count, long N, double **ptrs) {
+    double *blk = (double *)calloc((size_t)count * (size_t)N, sizeof(double));
+    for (int i = 0; i < count; ++i) ptrs[i] = blk + (size_t)i * N;
+    return blk;
+}
+
+double or_rhs(const or_box *b, const double *const q[5], double *const rhs[5]) {
+    const long N = (long)b->nx * b->ny * b->nz;
+    double *prim[8], *flp[15], *frp[15], *dinv[15];
+    double *blk_prim = alloc_fields(8, N, prim);
+    double *blk_fl = alloc_fields(15, N, flp);
+    double *blk_fr = alloc_fields(15, N, frp);
+    double *blk_d = alloc_fields(15, N, dinv);
+    double *fl[3][5], *fr[3][5];
+    for (int d = 0; d < 3; ++d)
+        for (int e = 0; e < 5; ++e) {
+            fl[d][e] = flp[d * 5 + e];
+            fr[d][e] = frp[d * 5 + e];
+        }
+    double eig[3];
+    or_con2prim(b, q, prim);                 /* NaiverStokes3d.cpp:46 */
+    or_lf_split(b, q, (const double *const *)prim, fl, fr, eig); /* :48 */
+    for (int d = 0; d < 3; ++d) inviscid_direction(b, d, fl[d], fr[d], dinv + 5 * d); /* :52 */
+
+    double *dvis[15] = {0};
+    double *blk_v = NULL;
+    if (b->navier_stokes) {
+        /* solveGrads (NaiverStokes3d.cpp:87-175): CD6 of u, v, w, T along x, y, z */
+        double *g[12];
+        double *blk_g = alloc_fields(12, N, g);
+        const double *src[4] = {prim[1], prim[2], prim[3], prim[5]};
+        for (int vix = 0; vix < 4; ++vix)
+            for (int d = 0; d < 3; ++d) cd6_direction(b, d, src[vix], g[vix * 3 + d]);
+        /* solveViscousFlux (NaiverStokes3d.cpp:177-303) */
+        double *fv[15];
+        double *blk_fv = alloc_fields(15, N, fv);
+        const double c23 = 2.0 / 3.0;
+        int offdiag = (b->quirks & OR_Q_OFFDIAG_DIV) != 0;
+        for (long n = 0; n < N; ++n) {
+            double ux = g[0][n], uy = g[1][n], uz = g[2][n];
+            double vx = g[3][n], vy = g[4][n], vz = g[5][n];
+            double wx = g[6][n], wy = g[7][n], wz = g[8][n];
+            double tx = g[9][n], ty = g[10][n], tz = g[11][n];
+            double grad = ux + vy + wz;
+            double miu0, coeff0;
+            viscosity(b, prim[5][n], &miu0, &coeff0);
+            double tau_xx = miu0 * (2.0 * ux - c23 * grad);
+            double tau_xy = offdiag ? miu0 * (uy + vx - c23 * grad) : miu0 * (uy + vx);
+            double tau_xz = offdiag ? miu0 * (uz + wx - c23 * grad) : miu0 * (uz + wx);
+            double tau_yy = miu0 * (2.0 * vy - c23 * grad);
+            double tau_yz = offdiag ? miu0 * (vz + wy - c23 * grad) : miu0 * (vz + wy);
+            double tau_zz = miu0 * (2.0 * wz - c23 * grad);
+            double tau_tx = coeff0 * tx, tau_ty = coeff0 * ty, tau_tz = coeff0 * tz;
+            double u = prim[1][n], v = prim[2][n], w = prim[3][n];
+            fv[0][n] = 0.0;
+            fv[1][n] = tau_xx;
+            fv[2][n] = tau_xy;
+            fv[3][n] = tau_xz;
+            fv[4][n] = u * tau_xx + v * tau_xy + w * tau_xz + tau_tx;
+            fv[5][n] = 0.0;
+            fv[6][n] = tau_xy;
+            fv[7][n] = tau_yy;
+            fv[8][n] = tau_yz;
+            fv[9][n] = u * tau_xy + v * tau_yy + w * tau_yz + tau_ty;
+            fv[10][n] = 0.0;
+            fv[11][n] = tau_xz;
+            fv[12][n] = tau_yz;
+            fv[13][n] = tau_zz;
+            fv[14][n] = u * tau_xz + v * tau_yz + w * tau_zz + tau_tz;
+        }
+        /* setDerivativesVis (NaiverStokes3d.cpp:305-369) */
+        blk_v = alloc_fields(15, N, dvis);
+        for (int d = 0; d < 3; ++d)
+            for (int e = 0; e < 5; ++e) cd6_direction(b, d, fv[d * 5 + e], dvis[d * 5 + e]);
+        free(blk_g);
+        free(blk_fv);
+    }
+    /* solveRHS: NaiverStokes3d.cpp:385-499 / euler3d.cpp:389-457 */
+    for (int e = 0; e < 5; ++e)
+        for (long n = 0; n < N; ++n) {
+            double r = dinv[e][n];
+            r += dinv[5 + e][n];
+            r += dinv[10 + e][n];
+            if (b->navier_stokes) {
+                r -= dvis[e][n];
+                r -= dvis[5 + e][n];
+                r -= dvis[10 + e][n];
+            }
+            rhs[e][n] = r;
+        }
+    free(blk_prim);
+    free(blk_fl);
+    free(blk_fr);
+    free(blk_d);
+    free(blk_v);
+    /* getDt (euler3d.cpp:459-466) */
+    double dt_xi = b->dx / eig[0];
+    double dt_eta = b->dy / eig[1];
+    double dt_zeta = b->dz / eig[2];
+    return 1.0 / (1.0 / dt_xi + 1.0 / dt_eta + 1.0 / dt_zeta);
+}
+
+/* ------------------------------------------------------------- RK3 ------- */
+
+void or_rk3_stage(int stage, long n, double dt, const double *const rhs[5],
+                  const double *const un[5], double *const ui[5]) {
+    /* TVD-RK3.h:9-12 coefficients; TVD-RK3.cpp:76-196 */
+    static const double c[3][2] = {{1.0, 1.0}, {3.0 / 4.0, 1.0 / 4.0}, {1.0 / 3.0, 2.0 / 3.0}};
+    for (int e = 0; e < 5; ++e)
+        for (long i = 0; i < n; ++i) {
+            double r = -rhs[e][i];
+            if (stage == 0) {
+                double u = ui[e][i];
+                ui[e][i] = c[0][0] * u + c[0][1] * r * dt;
+            } else {
+                double u = un[e][i];
+                double uk = ui[e][i];
+                ui[e][i] = c[stage][0] * u + c[stage][1] * (r * dt + uk);
+            }
+        }
+}
+
+void or_run_steps(const or_box *b, double cfl, int nsteps, double *const q[5], double *dt,
+                  double *res) {
+    const long N = (long)b->nx * b->ny * b->nz;
+    double *un[5], *rhs[5];
+    double *blk_un = alloc_fields(5, N, un);
+    double *blk_r = alloc_fields(5, N, rhs);
+    for (int s = 0; s < nsteps; ++s) {
+        double dt_global = 0.0;
+        for (int stage = 0; stage < 3; ++stage) {
+            double dt_local = or_rhs(b, (const double *const *)q, rhs);
+            if (stage == 0) { /* PDEData3d.cpp:161-165 */
+                for (int e = 0; e < 5; ++e) memcpy(un[e], q[e], sizeof(double) * (size_t)N);
+                dt_global = dt_local * cfl;
+            }
+            or_rk3_stage(stage, N, dt_global, (const double *const *)rhs,
+                         (const double *const *)un, q);
+        }
+        /* setRES (PDEData3d.cpp:178-213) */
+        double res_this = 0.0;
+        for (int e = 0; e < 5; ++e)
+            for (long i = 0; i < N; ++i) res_this += SQ(q[e][i] - un[e][i]);
+        dt[s] = dt_global;
+        res[s] = sqrt(res_this / (double)((size_t)N * 5u)) / dt_global;
+    }
+    free(blk_un);
+    free(blk_r);
+}
+
+/* ------------------------------------------------------------- ICs ------- */
+
+void or_init_tgv(const or_box *b, double x0, double y0, double z0, double *const q[5]) {
+    /* mesh centres block.cpp:120-122 with one rank (coord 0); TGV :369-394 */
+    const double gamma = b->gamma, mach = b->mach;
+    for (int k = 0; k < b->nz; k++)
+        for (int j = 0; j < b->ny; j++)
+            for (int i = 0; i < b->nx; i++) {
+                long idx = i + (long)b->nx * (j + (long)b->ny * k);
+                double xc = 0.0 + b->dx * (0.5 + i) - x0;
+                double yc = 0.0 + b->dy * (0.5 + j) - y0;
+                double zc = 0.0 + b->dz * (0.5 + k) - z0;
+                double rho0 = 1.0;
+                double u0 = sin(xc) * cos(yc) * cos(zc);
+                double v0 = -cos(xc) * sin(yc) * cos(zc);
+                double w0 = 0.0;
+                double p0 = 1.0 / (gamma * mach * mach) +
+                            ((cos(2.0 * zc) + 2.0) * (cos(2.0 * xc) + cos(2.0 * yc)) - 2.0) / 16.0;
+                q[0][idx] = rho0;
+                q[1][idx] = rho0 * u0;
+                q[2][idx] = rho0 * v0;
+                q[3][idx] = rho0 * w0;
+                q[4][idx] = p0 / (gamma - 1.0) + 0.5 * rho0 * (u0 * u0 + v0 * v0 + w0 * w0);
+            }
+}

@@ -1,0 +1,266 @@
+"""ctypes access to the two CPU checkers.  TEST INFRASTRUCTURE ONLY.
+
+* ``Oracle`` wraps oracle/_build/libnuc3d_oracle.so, the C restatement of the
+  reference's RHS + TVD-RK3 path (oracle/nuc3d_oracle.c).
+* ``Reference`` wraps oracle/_ref/libnuc3d_ref.so, the reference's own
+  translation units compiled where they lie (``make -C oracle ref``).  It only
+  exists where the reference sources were present at build time.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, and only as the checker.  Arrays are FP64, x-fastest, shaped
+(nz, ny, nx) in numpy (C order), i.e. idx = i + nx*(j + ny*k).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "libnuc3d_oracle.so"
+REF_SO = HERE / "_ref" / "libnuc3d_ref.so"
+
+WENO5JS, WENO5Z, CRWENO5 = 0, 1, 2
+SCHEME_NAMES = {WENO5JS: "weno5js", WENO5Z: "weno5z", CRWENO5: "crweno5"}
+SUTHERLAND, CONSTANT, POWERLAW = 0, 1, 2
+VISC_NAMES = {SUTHERLAND: "Sutherland", CONSTANT: "Constant"}
+
+Q_ZETA_EIGEN = 1 << 0
+Q_WENOZ_BETA2 = 1 << 1
+Q_OFFDIAG_DIV = 1 << 2
+Q_FABS_PRESSURE = 1 << 3
+Q_CRWENO_BOUNDED = 1 << 4
+QUIRKS_REFERENCE = 0x1F
+
+_DP = C.POINTER(C.c_double)
+
+
+class _Box(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+        ("scheme", C.c_int * 3),
+        ("navier_stokes", C.c_int),
+        ("visc_model", C.c_int),
+        ("gamma", C.c_double), ("mach", C.c_double), ("reynolds", C.c_double),
+        ("prandtl", C.c_double), ("t_ref", C.c_double), ("t_inf", C.c_double),
+        ("powerlaw_exp", C.c_double),
+        ("quirks", C.c_uint),
+    ]
+
+
+@dataclass
+class Box:
+    """Box and model parameters; defaults are the Taylor-Green case of the
+    reference decks (Re 1600, M 0.1, Pr 0.71, Sutherland, WENO5-JS + CD6)."""
+
+    nx: int
+    ny: int
+    nz: int
+    lx: float = 2.0 * np.pi
+    ly: float = 2.0 * np.pi
+    lz: float = 2.0 * np.pi
+    scheme: tuple = (WENO5JS, WENO5JS, WENO5JS)
+    navier_stokes: bool = True
+    visc_model: int = SUTHERLAND
+    gamma: float = 1.4
+    mach: float = 0.1
+    reynolds: float = 1600.0
+    prandtl: float = 0.71
+    t_ref: float = 110.4
+    t_inf: float = 288.0
+    powerlaw_exp: float = 0.76
+    quirks: int = QUIRKS_REFERENCE
+
+    @property
+    def dx(self):
+        return self.lx / self.nx  # block.cpp:62-64
+
+    @property
+    def dy(self):
+        return self.ly / self.ny
+
+    @property
+    def dz(self):
+        return self.lz / self.nz
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny, self.nx)
+
+    def c_struct(self) -> _Box:
+        b = _Box()
+        b.nx, b.ny, b.nz = self.nx, self.ny, self.nz
+        b.dx, b.dy, b.dz = self.dx, self.dy, self.dz
+        for d in range(3):
+            b.scheme[d] = int(self.scheme[d])
+        b.navier_stokes = int(self.navier_stokes)
+        b.visc_model = int(self.visc_model)
+        b.gamma, b.mach, b.reynolds = self.gamma, self.mach, self.reynolds
+        b.prandtl, b.t_ref, b.t_inf = self.prandtl, self.t_ref, self.t_inf
+        b.powerlaw_exp = self.powerlaw_exp
+        b.quirks = int(self.quirks)
+        return b
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_DP)
+
+
+def _ptrs(arrs):
+    arr_t = _DP * len(arrs)
+    return arr_t(*[_ptr(a) for a in arrs])
+
+
+def build_oracle():
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+class Oracle:
+    def __init__(self, so: Path = ORACLE_SO):
+        if not Path(so).exists():
+            build_oracle()
+        self.lib = C.CDLL(str(so))
+        L = self.lib
+        L.or_rhs.restype = C.c_double
+        L.or_reconstruct_field.restype = C.c_int
+        L.or_cd6_field.restype = C.c_int
+
+    def reconstruct_field(self, scheme, upwind, quirks, fin, hl, hr):
+        nz, ny, nx = fin.shape
+        out = np.zeros((nz, ny, nx + 1))
+        rc = self.lib.or_reconstruct_field(scheme, upwind, C.c_uint(quirks), nx, ny, nz,
+                                           _ptr(fin), _ptr(hl), _ptr(hr), _ptr(out))
+        assert rc == 0
+        return out
+
+    def cd6_field(self, fin, dx, hl, hr):
+        nz, ny, nx = fin.shape
+        out = np.zeros_like(fin)
+        rc = self.lib.or_cd6_field(nx, ny, nz, C.c_double(dx), _ptr(fin), _ptr(hl), _ptr(hr),
+                                   _ptr(out))
+        assert rc == 0
+        return out
+
+    def con2prim(self, box: Box, q):
+        prim = [np.zeros(box.shape) for _ in range(8)]
+        b = box.c_struct()
+        self.lib.or_con2prim(C.byref(b), _ptrs(q), _ptrs(prim))
+        return prim
+
+    def rk3_stage(self, stage, dt, rhs, un, ui):
+        n = rhs[0].size
+        self.lib.or_rk3_stage(stage, C.c_long(n), C.c_double(dt), _ptrs(rhs), _ptrs(un),
+                              _ptrs(ui))
+
+    def rhs(self, box: Box, q):
+        out = [np.zeros(box.shape) for _ in range(5)]
+        b = box.c_struct()
+        dt_local = self.lib.or_rhs(C.byref(b), _ptrs(q), _ptrs(out))
+        return out, dt_local
+
+    def run_steps(self, box: Box, cfl, nsteps, q):
+        q = [np.ascontiguousarray(a, dtype=np.float64).copy() for a in q]
+        dt = np.zeros(nsteps)
+        res = np.zeros(nsteps)
+        b = box.c_struct()
+        self.lib.or_run_steps(C.byref(b), C.c_double(cfl), nsteps, _ptrs(q), _ptr(dt), _ptr(res))
+        return q, dt, res
+
+    def tgv(self, box: Box, origin=(0.0, 0.0, 0.0)):
+        q = [np.zeros(box.shape) for _ in range(5)]
+        b = box.c_struct()
+        self.lib.or_init_tgv(C.byref(b), C.c_double(origin[0]), C.c_double(origin[1]),
+                             C.c_double(origin[2]), _ptrs(q))
+        return q
+
+
+def write_decks(dirpath: Path, box: Box, cfl: float = 0.5):
+    """Write the reference's inp/ decks for ``box`` (formats: fieldOperator.cpp:
+    100-125, physicsModel.cpp:66-112; the first six PhysModel lines are
+    positional, Forcing included)."""
+    inp = Path(dirpath) / "inp"
+    inp.mkdir(parents=True, exist_ok=True)
+    names = [SCHEME_NAMES[s] for s in box.scheme]
+    (inp / "Method.in").write_text(
+        "scheme_time RK3\n"
+        f"scheme_x_ivs {names[0]}\nscheme_y_ivs {names[1]}\nscheme_z_ivs {names[2]}\n"
+        "scheme_x_vis cd6\nscheme_y_vis cd6\nscheme_z_vis cd6\n")
+    model = "NavierStokes3d" if box.navier_stokes else "Euler3d"
+    (inp / "PhysModel.in").write_text(
+        "Neqs 5\nEosName IdealGas\nRiemannSolver LF\n"
+        f"PDEModel {model}\nViscousModel {VISC_NAMES[box.visc_model]}\nForcing None\n"
+        f"Reynolds {box.reynolds!r}\nMach {box.mach!r}\nPt {box.prandtl!r}\n"
+        f"Gamma {box.gamma!r}\nT_ref {box.t_ref!r}\nT_inf {box.t_inf!r}\n")
+
+
+class Reference:
+    """The reference's own code, driven through oracle/ref/ref_harness.cpp."""
+
+    def __init__(self, so: Path = REF_SO):
+        if not Path(so).exists():
+            raise FileNotFoundError(f"{so} not built (make -C oracle ref needs the reference)")
+        self.lib = C.CDLL(str(so))
+
+    @staticmethod
+    def available() -> bool:
+        return REF_SO.exists()
+
+    def reconstruct_field(self, scheme, upwind, fin, hl, hr):
+        nz, ny, nx = fin.shape
+        out = np.zeros((nz, ny, nx + 1))
+        rc = self.lib.ref_reconstruct(scheme, upwind, nx, ny, nz, _ptr(fin), _ptr(hl), _ptr(hr),
+                                      _ptr(out))
+        assert rc == 0
+        return out
+
+    def cd6_field(self, fin, dx, hl, hr):
+        nz, ny, nx = fin.shape
+        out = np.zeros_like(fin)
+        self.lib.ref_cd6(nx, ny, nz, C.c_double(dx), _ptr(fin), _ptr(hl), _ptr(hr), _ptr(out))
+        return out
+
+    def rk3_stage(self, stage, dt, rhs, un, ui):
+        n = rhs[0].size
+        self.lib.ref_rk3_stage(stage, n, C.c_double(dt), _ptrs(rhs), _ptrs(un), _ptrs(ui))
+
+    def split(self, box: Box, q):
+        with tempfile.TemporaryDirectory() as td:
+            write_decks(Path(td), box)
+            prim = [np.zeros(box.shape) for _ in range(8)]
+            # rotated layouts: eta (nx, nz, ny) as (slow..fast), zeta (ny, nx, nz)
+            shp = [box.shape, (box.nx, box.nz, box.ny), (box.ny, box.nx, box.nz)]
+            fl = [np.zeros(shp[d // 5]) for d in range(15)]
+            fr = [np.zeros(shp[d // 5]) for d in range(15)]
+            eig = np.zeros(3)
+            self.lib.ref_split(str(td).encode(), box.nx, box.ny, box.nz, _ptrs(q), _ptrs(prim),
+                               _ptrs(fl), _ptrs(fr), _ptr(eig))
+        return prim, fl, fr, eig
+
+    def rhs(self, box: Box, q):
+        with tempfile.TemporaryDirectory() as td:
+            write_decks(Path(td), box)
+            out = [np.zeros(box.shape) for _ in range(5)]
+            dtl = C.c_double(0.0)
+            self.lib.ref_rhs(str(td).encode(), box.nx, box.ny, box.nz, C.c_double(box.dx),
+                             C.c_double(box.dy), C.c_double(box.dz), _ptrs(q), _ptrs(out),
+                             C.byref(dtl))
+        return out, dtl.value
+
+    def run_steps(self, box: Box, cfl, nsteps, q):
+        q = [np.ascontiguousarray(a, dtype=np.float64).copy() for a in q]
+        dt = np.zeros(nsteps)
+        res = np.zeros(nsteps)
+        with tempfile.TemporaryDirectory() as td:
+            write_decks(Path(td), box, cfl)
+            self.lib.ref_run_steps(str(td).encode(), box.nx, box.ny, box.nz, C.c_double(box.dx),
+                                   C.c_double(box.dy), C.c_double(box.dz), C.c_double(cfl),
+                                   nsteps, _ptrs(q), _ptr(dt), _ptr(res))
+        return q, dt, res
