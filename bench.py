@@ -1,0 +1,433 @@
+#!/usr/bin/env python
+"""Benchmark: NUC3d RHS + TVD-RK3 time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one box per GPU): decaying isotropic turbulence on a periodic 256^3
+box, seeded solenoidal velocity with E(k) ~ k^4 exp(-2 (k/4)^2), M = 1,
+turbulent Mach 0.3, Reynolds number set for Re_lambda = 100; Navier-Stokes,
+Lax-Friedrichs split, WENO5-Z reconstruction, CD6 viscous terms, TVD-RK3 at
+CFL 0.5.  One "step" is one TVD-RK3 step (3 RHS evaluations) of every box.
+The metric is cell-updates/s (cells x steps / s) over the whole job.
+
+* ``value``: FP64 path, state resident in HBM, device-timed with CUDA events
+  (max over ranks).  The state (671 MB per box) is larger than the 126 MB L2,
+  so no flush is needed between steps.
+* ``e2e``: the same metric through the C ABI with host buffers: each step
+  uploads the state from pinned host memory (nuc3d_set_state_host), advances
+  one step with the dt/residual read back (nuc3d_step), and downloads the
+  state (nuc3d_get_state_host).
+* ``mixed``: the FP32-bulk / FP64-state form on the same workload, with its
+  per-field relative L2 distance to the FP64 path after 100 steps.
+* ``roofline``: the dominant kernel (inviscid WENO sweep), algorithmic FP64
+  flops per launch over its event-timed average launch duration, against the
+  FP64 FMA rate measured in the same run (nuc3d_probe_peak).
+* ``cpu_baseline``: the reference's own code (oracle/_ref) on host cores.
+
+With --gpus N > 1 (torchrun), every rank advances its own box (independent
+replicas, no data-path collective); timing is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "nuc3d-cartisian_b200" / "python"))
+
+METRIC = "cell-updates/s at 256^3 (decaying HIT, WENO5-Z, N-S, TVD-RK3)"
+UNIT = "cell-updates/s"
+NX = 256
+SEED = 0
+K_PEAK = 4.0
+MACH_T = 0.3
+RE_LAMBDA = 100.0
+CFL = 0.5
+# Algorithmic FP64 flops (add/mul/div/sqrt = 1, FMA = 2) per cell, counted
+# from the kernels' formulas: one directional sweep = 5 equations x
+# (2 WENO5-Z faces of 76 flops + F^+ + F^- add + difference 2) + LF split 33.
+FLOPS_INV_Z = 5 * (2 * 76 + 1 + 2) + 33
+FLOPS_INV_JS = 5 * (2 * 68 + 1 + 2) + 33
+FLOPS_PER_CELL_STAGE = 3 * FLOPS_INV_Z + 20 + 156 + 111  # + prim, viscous flux, update
+STATE_BYTES_PER_CELL_UPDATE = 320  # compulsory FP64 state traffic of 3 RK stages
+# DRAM bytes per launch of the inviscid sweep at 256^3, from the ncu capture
+# summarised in profiles/k_inviscid_weno5z_256.md (None until captured).
+INV_TRAFFIC_BYTES = None
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def config_dict(n_gpus, reynolds):
+    return {
+        "workload": f"decaying isotropic turbulence {NX}^3 periodic box, seeded solenoidal "
+                    f"E(k)~k^4 exp(-2(k/{K_PEAK:g})^2), M=1, Mt={MACH_T}, Re_lambda={RE_LAMBDA:g}; "
+                    "Navier-Stokes, LF split, WENO5-Z, CD6 viscous, TVD-RK3 CFL 0.5",
+        "cells_per_box": NX ** 3,
+        "boxes_per_gpu": 1,
+        "reynolds": reynolds,
+        "parallelism": f"replicas x{n_gpus} (one box per GPU, no collective)",
+        "l2_flush": "not needed: 671 MB FP64 state per box > 126 MB L2",
+    }
+
+
+# ------------------------------------------------------------- CPU side ----
+def _cpu_worker(args):
+    """One reference (or oracle) box of the bounded sample, timed."""
+    kind, n, steps, warm, reynolds = args
+    # the reference prints its MPI topology on stdout; keep the bench's
+    # stdout to the one JSON line
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    sys.path.insert(0, str(ROOT / "nuc3d-cartisian_b200" / "python"))
+    import numpy as np
+    import oracle_ctypes as oc
+    from nuc3d_b200.initial import hit_field
+    import nuc3d_b200 as nb
+    desc = nb.BoxDesc(n, n, n, mach=1.0)
+    q = hit_field(desc, seed=SEED, k_peak=K_PEAK, mach_t=MACH_T)
+    box = oc.Box(n, n, n, scheme=(oc.WENO5Z,) * 3, mach=1.0, reynolds=reynolds)
+    eng = oc.Reference() if kind == "reference" else oc.Oracle()
+    if warm:
+        q, _, _ = eng.run_steps(box, CFL, warm, q)
+    t0 = time.perf_counter()
+    eng.run_steps(box, CFL, steps, q)
+    return time.perf_counter() - t0
+
+
+def cpu_sample(n, steps, warm, reynolds, workers):
+    """Run `workers` independent boxes concurrently (spawned processes, one
+    per core: the reference is one MPI rank per core and this machine has no
+    MPI).  Returns (cell-updates/s, wall seconds, kind)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_ctypes as oc
+    kind = "reference" if oc.Reference.available() else "port"
+    if kind == "port":
+        oc.build_oracle()
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(workers) as pool:
+        times = pool.map(_cpu_worker, [(kind, n, steps, warm, reynolds)] * workers)
+    wall = time.perf_counter() - t0
+    slowest = max(times)
+    return workers * n ** 3 * steps / slowest, slowest, kind
+
+
+# ------------------------------------------------------------ clocks -------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, power, reasons = [], None, [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+                power.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "power_w_median": statistics.median(power) if power else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------ GPU arm ------
+def run_b200(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import nuc3d_b200 as nb
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+
+    desc = nb.BoxDesc(NX, NX, NX, mach=1.0, scheme=(nb.WENO5Z,) * 3)
+    q, reynolds = nb.hit_field(desc, seed=SEED + rank, k_peak=K_PEAK, mach_t=MACH_T,
+                               re_lambda=RE_LAMBDA)
+    desc = nb.BoxDesc(NX, NX, NX, mach=1.0, scheme=(nb.WENO5Z,) * 3, reynolds=reynolds)
+    cells = desc.cells
+    pinned = [torch.from_numpy(a).pin_memory() for a in q]
+    host_q = [p.numpy() for p in pinned]
+
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(solver, k):
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solver.step(k, CFL, stats=False)
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1)
+
+    peak64 = nb.probe_peak(nb.FP64)
+    peak32 = nb.probe_peak(nb.MIXED)
+
+    # ---- FP64, resident state: the headline value
+    s64 = nb.Solver(desc, stream=stream)
+    s64.set_state(host_q)
+    s64.step(args.warmup, CFL, stats=False)
+    s64.sync()
+    clocks = ClockSampler(local_rank)
+    launches0 = s64.launch_count()
+    ms = timed_steps(s64, args.steps)
+    launches = s64.launch_count() - launches0
+    clock_info = clocks.stop()
+    s64.sync()
+    ms_max = max_over_ranks(ms)
+    ms_per_step = ms_max / args.steps
+    value = world * cells / (ms_per_step * 1e-3)
+
+    # ---- per-kernel event timing (separate short pass, same workload)
+    s64.profile(True)
+    s64.step(2, CFL, stats=False)
+    prof = s64.profile_read(reset=True)
+    s64.profile(False)
+    inv_ms = sum(prof[k][0] for k in ("inv_x", "inv_y", "inv_z"))
+    inv_n = sum(prof[k][1] for k in ("inv_x", "inv_y", "inv_z"))
+    total_ms = sum(v[0] for v in prof.values())
+    inv_avg_ms = inv_ms / max(inv_n, 1)
+    achieved = FLOPS_INV_Z * cells / (inv_avg_ms * 1e-3) / 1e12
+    roofline = {
+        "bound": "fp64",
+        "kernel": "k_inviscid<WENO5-Z, FP64> (directional sweep, x/y/z)",
+        "achieved": achieved,
+        "peak": peak64,
+        "unit": "TFLOP/s",
+        "frac": achieved / peak64,
+        "peak_source": "FP64 FMA rate measured in this run (nuc3d_probe_peak)",
+        "traffic": INV_TRAFFIC_BYTES,
+        "flops_per_launch": FLOPS_INV_Z * cells,
+        "avg_launch_ms": inv_avg_ms,
+        "share_of_step": inv_ms / total_ms if total_ms else None,
+        "kernel_ms_per_step": {k: v[0] / 2 for k, v in prof.items()},
+        "step_fp64_tflops": FLOPS_PER_CELL_STAGE * 3 * cells / (ms_per_step * 1e-3) / 1e12,
+        "hbm_state_frac": STATE_BYTES_PER_CELL_UPDATE * cells / (ms_per_step * 1e-3) / 1e9
+                          / 6550.7,
+    }
+
+    # ---- e2e through the C ABI with host buffers
+    e2e_steps = max(1, min(args.steps, 5))
+    s64.set_state(host_q)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s64.set_state(host_q)              # H2D of the step's input state (pinned)
+        s64.step(1, CFL, stats=True)       # dt and residual read back
+        s64.get_state(host_q)              # D2H of the step's result state
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * cells * e2e_steps / e2e_s
+    # resident variant: state stays on the device, dt/residual read each step
+    s64.set_state(host_q)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s64.step(1, CFL, stats=True)
+    barrier()
+    res_s = max_over_ranks(time.perf_counter() - t0)
+    s64.close()
+
+    # ---- mixed precision form
+    mixed = None
+    if not args.skip_mixed:
+        dm = nb.BoxDesc(**{**desc.__dict__, "precision": nb.MIXED})
+        sm = nb.Solver(dm, stream=stream)
+        sm.set_state(q)
+        sm.step(args.warmup, CFL, stats=False)
+        sm.sync()
+        ms_m = max_over_ranks(timed_steps(sm, args.steps))
+        sm.close()
+        # accuracy: 100 steps from the same state, both precisions
+        nacc = args.accuracy_steps
+        a64 = nb.Solver(desc, stream=stream)
+        a64.set_state(q)
+        a64.step(nacc, CFL, stats=False)
+        r64 = a64.get_state()
+        a64.close()
+        a32 = nb.Solver(dm, stream=stream)
+        a32.set_state(q)
+        a32.step(nacc, CFL, stats=False)
+        r32 = a32.get_state()
+        a32.close()
+        errs = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(r32, r64)]
+        ke = [0.5 * float(np.sum((r[1] ** 2 + r[2] ** 2 + r[3] ** 2) / r[0])) for r in (r32, r64)]
+        mixed = {
+            "value": world * cells / (ms_m / args.steps * 1e-3),
+            "ms_per_step": ms_m / args.steps,
+            "speedup_vs_fp64": ms_per_step / (ms_m / args.steps),
+            "dtype": "fp32 bulk / fp64 state",
+            "rel_l2_vs_fp64": max(errs),
+            "rel_l2_per_field": errs,
+            "tke_rel_diff": abs(ke[0] - ke[1]) / ke[1],
+            "accuracy_steps": nacc,
+            "peak_fp32_tflops": peak32,
+        }
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return None
+    cpu = None
+    if args.cpu_result is not None:
+        cpu = args.cpu_result
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded HIT field; no dataset)",
+        "config": config_dict(world, reynolds),
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": 5 * 8 * cells, "d2h_bytes_per_step": 5 * 8 * cells + 16,
+                "steps": e2e_steps,
+                "resident": {"value": world * cells * e2e_steps / res_s, "unit": UNIT,
+                             "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 16}},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "clocks": clock_info,
+        "mixed": mixed,
+        "cpu_baseline": cpu,
+    }
+    if dist is not None:
+        dist.destroy_process_group()
+    return line
+
+
+# ------------------------------------------------------- reference arm -----
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    import nuc3d_b200 as nb
+    n = args.cpu_n
+    desc = nb.BoxDesc(n, n, n, mach=1.0)
+    _, reynolds = nb.hit_field(desc, seed=SEED, k_peak=K_PEAK, mach_t=MACH_T, re_lambda=RE_LAMBDA)
+    workers = args.cpu_workers or min(os.cpu_count() or 1, 64)
+    value, wall, kind = cpu_sample(n, args.steps, args.warmup, reynolds, workers)
+    sample = (f"{workers} concurrent {n}^3 boxes (one per core, the reference's single-rank "
+              f"code), {args.warmup}+{args.steps} steps each, same physics and scheme")
+    cfg = config_dict(world, reynolds)
+    cfg["reference_sample"] = sample
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded HIT field)",
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--skip-mixed", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=100)
+    ap.add_argument("--cpu-n", type=int, default=48, help="box edge of the CPU sample")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-workers", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", args.gpus)
+    local_rank = env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+
+    args.cpu_result = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # before any CUDA call: the CPU pool is spawned from a clean process
+        import nuc3d_b200 as nb
+        d = nb.BoxDesc(args.cpu_n, args.cpu_n, args.cpu_n, mach=1.0)
+        _, re_cpu = nb.hit_field(d, seed=SEED, k_peak=K_PEAK, mach_t=MACH_T, re_lambda=RE_LAMBDA)
+        workers = args.cpu_workers or min(os.cpu_count() or 1, 64)
+        v, wall, kind = cpu_sample(args.cpu_n, args.cpu_steps, 0, re_cpu, workers)
+        args.cpu_result = {
+            "value": v, "unit": UNIT, "cores": workers, "kind": kind,
+            "sample": f"{workers} concurrent {args.cpu_n}^3 HIT boxes (one per core), "
+                      f"{args.cpu_steps} TVD-RK3 steps each, WENO5-Z N-S, {wall:.1f} s",
+        }
+    line = run_b200(args, rank, world, local_rank)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,182 @@
+/*
+ * nuc3d_b200 — C ABI of the B200-native NUC3d RHS + TVD-RK3 path.
+ *
+ * Plain C types only (pointers, sizes, doubles); no CUDA or torch types.  A
+ * stream is passed as `void *` holding a cudaStream_t (NULL = legacy default
+ * stream).  Every entry point returns an int status (NUC3D_OK = 0, negative on
+ * error) and never aborts the process: the reference's error behaviour
+ * (print + exit(-1) / MPI_Abort, e.g. weno5js.cpp:32-34) becomes a status code
+ * plus nuc3d_last_error() text.
+ *
+ * Fields are FP64, x-fastest, idx = i + nx*(j + ny*k): the layout of the
+ * reference's Field (field.h:9-79, block.cpp:119).  Device pointers are
+ * marked d_*, host pointers h_*.
+ */
+#ifndef NUC3D_B200_H
+#define NUC3D_B200_H
+
+#if defined(__GNUC__)
+#define NUC3D_API __attribute__((visibility("default")))
+#else
+#define NUC3D_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NUC3D_OK 0
+#define NUC3D_ERR_INVALID (-1)     /* bad argument or size */
+#define NUC3D_ERR_CUDA (-2)        /* a CUDA call failed */
+#define NUC3D_ERR_NOMEM (-3)       /* device allocation failed */
+#define NUC3D_ERR_UNSUPPORTED (-4) /* scheme / model not available */
+#define NUC3D_ERR_NONFINITE (-5)   /* the state went NaN/Inf (finite check) */
+
+/* Reconstruction schemes: the Method.in strings weno5js, weno5z, crweno5
+ * (fieldOperator.cpp:152-166). */
+#define NUC3D_WENO5JS 0
+#define NUC3D_WENO5Z 1
+#define NUC3D_CRWENO5 2
+
+/* PDEModel (block.cpp:146-157) */
+#define NUC3D_EULER3D 0
+#define NUC3D_NAVIERSTOKES3D 1
+
+/* ViscousModel (physicsModel.cpp:44-49); POWERLAW mu = T^w / Re is an extra
+ * model the reference does not have. */
+#define NUC3D_VISC_SUTHERLAND 0
+#define NUC3D_VISC_CONSTANT 1
+#define NUC3D_VISC_POWERLAW 2
+
+/* Arithmetic of the bulk (reconstruction, flux differences, viscous
+ * stencils).  The conserved state, pressure/temperature recovery, the RK
+ * accumulation and all global reductions are FP64 in both. */
+#define NUC3D_FP64 0
+#define NUC3D_MIXED 1
+
+/* Reference behaviours that look like defects.  Each is reproduced while its
+ * bit is set; NUC3D_QUIRKS_REFERENCE (all set) is the drop-in default. */
+#define NUC3D_QUIRK_ZETA_EIGEN 0x1u     /* physicsModel.cpp:653-654, euler3d.cpp:459-466 */
+#define NUC3D_QUIRK_WENOZ_BETA2 0x2u    /* weno5z.cpp:80 */
+#define NUC3D_QUIRK_OFFDIAG_DIV 0x4u    /* NaiverStokes3d.cpp:267-270 */
+#define NUC3D_QUIRK_FABS_PRESSURE 0x8u  /* physicsModel.cpp:340 */
+#define NUC3D_QUIRK_CRWENO_BOUNDED 0x10u /* crweno5.cpp:45-402 (cleared: periodic lines) */
+#define NUC3D_QUIRKS_REFERENCE 0x1fu
+
+typedef struct nuc3d_box_desc {
+    int nx, ny, nz;          /* cells; block.in line 2 (single rank) */
+    double lx, ly, lz;       /* box lengths; dx = lx/nx (block.cpp:62-64) */
+    int scheme[3];           /* scheme_{x,y,z}_ivs */
+    int pde_model;           /* PDEModel */
+    int visc_model;          /* ViscousModel */
+    double gamma, mach, reynolds, prandtl, t_ref, t_inf; /* PhysModel.in keys */
+    double powerlaw_exp;     /* exponent of NUC3D_VISC_POWERLAW */
+    int precision;           /* NUC3D_FP64 or NUC3D_MIXED */
+    unsigned quirks;         /* NUC3D_QUIRK_* mask */
+} nuc3d_box_desc;
+
+typedef struct nuc3d_ctx nuc3d_ctx;
+
+/* Text of the last error on the calling thread ("" if none). */
+NUC3D_API const char *nuc3d_last_error(void);
+/* Version string of the library. */
+NUC3D_API const char *nuc3d_version(void);
+
+/* Fill *d with the reference decks' defaults (TGV-like: 64^3 2*pi box,
+ * WENO5-JS, Navier-Stokes, Sutherland, Re 1000, M 0.5, Pr 0.72, gamma 1.4,
+ * T_ref 110.4, T_inf 288, FP64, reference quirks) — physicsModel.cpp:23-64,
+ * fieldOperator.cpp:22-32. */
+NUC3D_API void nuc3d_box_desc_default(nuc3d_box_desc *d);
+
+/* ---- whole-step solver (replaces block::solve's stage loop) --------------
+ * One periodic box resident on the current device.  Replaces
+ * NaiverStokesData3d::solve / EulerData3D::solve (NaiverStokes3d.cpp:37-73,
+ * euler3d.cpp:260-277) + PDEData3d::solve (PDEData3d.cpp:155-176) +
+ * tvdrk3rd (TVD-RK3.cpp:16-157) for the single-rank periodic case, with the
+ * halo exchange (MPICommunicator.cpp:81-132) replaced by an in-kernel wrap. */
+NUC3D_API int nuc3d_ctx_create(const nuc3d_box_desc *desc, void *stream, nuc3d_ctx **out);
+NUC3D_API int nuc3d_ctx_destroy(nuc3d_ctx *ctx);
+/* Bytes of device memory a context of this description holds. */
+NUC3D_API long long nuc3d_ctx_bytes(const nuc3d_box_desc *desc);
+
+/* State in/out (the 5 conserved fields rho, rho u, rho v, rho w, rho E).
+ * Host variants copy through the context's stream and synchronise;
+ * device variants are stream-ordered.  block.cpp:609-671 holds the same
+ * five fields in its restart files. */
+NUC3D_API int nuc3d_set_state_host(nuc3d_ctx *ctx, const double *const h_q[5]);
+NUC3D_API int nuc3d_get_state_host(nuc3d_ctx *ctx, double *const h_q[5]);
+NUC3D_API int nuc3d_set_state_device(nuc3d_ctx *ctx, const double *const d_q[5]);
+NUC3D_API int nuc3d_get_state_device(nuc3d_ctx *ctx, double *const d_q[5]);
+
+/* Advance nsteps TVD-RK3 steps with dt = cfl * dt_local computed from the
+ * state at each step's stage 0 (PDEData3d.cpp:161-165).  h_dt / h_res (host,
+ * nsteps entries each, may be NULL) receive each step's dt and residual
+ * (PDEData3d.cpp:178-213).  Synchronises only when h_dt or h_res is given. */
+NUC3D_API int nuc3d_step(nuc3d_ctx *ctx, int nsteps, double cfl, double *h_dt, double *h_res);
+
+/* Wait for the context's stream and report NUC3D_ERR_NONFINITE if any stage
+ * produced a NaN/Inf state since the context was created (the reference has
+ * no such check; physicsModel.cpp:340 masks negative pressure with fabs). */
+NUC3D_API int nuc3d_sync(nuc3d_ctx *ctx);
+
+/* One RHS evaluation of the current state (the NaiverStokesData3d::solve
+ * part): d_rhs receives the 5 RHS fields (device), *h_dt_local the value the
+ * reference passes to PDEData3d::setDt. */
+NUC3D_API int nuc3d_rhs(nuc3d_ctx *ctx, double *const d_rhs[5], double *h_dt_local);
+
+/* Kernel timing.  While enabled, every kernel nuc3d_step launches is
+ * bracketed by CUDA events on the context's stream and the step waits for
+ * them; nuc3d_profile_read adds up milliseconds and launch counts per kernel
+ * class (NUC3D_PROF_* indices) since the last reset. */
+#define NUC3D_PROF_PRIM 0      /* con2prim + max eigenvalue */
+#define NUC3D_PROF_DT 1        /* dt from the eigenvalues */
+#define NUC3D_PROF_VISC 2      /* CD6 gradients + viscous fluxes */
+#define NUC3D_PROF_INV_X 3     /* inviscid sweep along x (WENO5 or CRWENO5) */
+#define NUC3D_PROF_INV_Y 4
+#define NUC3D_PROF_INV_Z 5
+#define NUC3D_PROF_UPDATE 6    /* viscous divergence + RK stage */
+#define NUC3D_PROF_RESIDUAL 7
+#define NUC3D_PROF_CLASSES 8
+NUC3D_API int nuc3d_profile_enable(nuc3d_ctx *ctx, int on);
+NUC3D_API int nuc3d_profile_read(nuc3d_ctx *ctx, double *ms, long long *launches, int reset);
+/* Kernels this context has launched since creation (all classes). */
+NUC3D_API long long nuc3d_launch_count(const nuc3d_ctx *ctx);
+
+/* Measured FMA-pipe throughput of the current device in TFLOP/s (FP64 for
+ * NUC3D_FP64, FP32 for NUC3D_MIXED): the roofline denominator of these
+ * stencil kernels.  Runs a ~10 ms probe kernel on the legacy stream. */
+NUC3D_API int nuc3d_probe_peak(int precision, double *tflops);
+
+/* Simulated time advanced by this context so far (block.cpp:208-209). */
+NUC3D_API double nuc3d_ctx_time(const nuc3d_ctx *ctx);
+
+/* ---- per-operator entry points (the reference's scheme plug-in API) -------
+ * These mirror the `interoplation`, `differential` and `integration`
+ * interfaces (fieldOperator.h:13-81) on device buffers, so a reference-side
+ * subclass can forward to them; halos are explicit, as in the reference.
+ *
+ * nuc3d_reconstruct = interpolationInner + interpolationBoundaryL +
+ *   interpolationBoundaryR of weno5js (weno5js.cpp:19-628), weno5z
+ *   (weno5z.cpp:18-637) or crweno5 (crweno5.cpp:25-837) with tilesize 3.
+ *   Along the fastest axis of an (nx,ny,nz) field; halo_l/halo_r are (3,ny,nz)
+ *   (the received MPI buffers, bufferData.cpp:16-47); out is (nx+1,ny,nz),
+ *   face m between cells m-1 and m.  upwind = +1 or -1.  crweno5 needs
+ *   nx <= 4096.  quirks: NUC3D_QUIRK_WENOZ_BETA2 is honoured. */
+NUC3D_API int nuc3d_reconstruct(int scheme, int upwind, unsigned quirks, int nx, int ny, int nz,
+                      const double *d_in, const double *d_halo_l, const double *d_halo_r,
+                      double *d_out, void *stream);
+
+/* centraldifference6th::differentialInner + BoundaryL + BoundaryR
+ * (centraldifference6th.cpp:16-186); out is (nx,ny,nz). */
+NUC3D_API int nuc3d_cd6(int nx, int ny, int nz, double dx, const double *d_in, const double *d_halo_l,
+              const double *d_halo_r, double *d_out, void *stream);
+
+/* tvdrk3rd::integrationAll (TVD-RK3.cpp:16-157): d_ui updated in place from
+ * d_rhs (the RHS R, dQ/dt = -R), d_un (u_n), stage 0..2. */
+NUC3D_API int nuc3d_tvdrk3_stage(int stage, long long n, double dt, const double *const d_rhs[5],
+                       const double *const d_un[5], double *const d_ui[5], void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NUC3D_B200_H */

@@ -1,0 +1,189 @@
+// Device-side building blocks of the NUC3d RHS: WENO5 reconstructions, CD6,
+// viscosity models and the box description passed to every kernel.
+//
+// Template parameter B is the "bulk" arithmetic type (double for the FP64
+// path, float for the mixed path).  The conserved state is always double.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nuc3d {
+
+enum : unsigned {
+    QK_ZETA_EIGEN = 0x1u,
+    QK_WENOZ_BETA2 = 0x2u,
+    QK_OFFDIAG_DIV = 0x4u,
+    QK_FABS_PRESSURE = 0x8u,
+    QK_CRWENO_BOUNDED = 0x10u,
+};
+
+enum : int { SCHEME_JS = 0, SCHEME_Z = 1, SCHEME_CR = 2 };
+enum : int { VISC_SUTHERLAND = 0, VISC_CONSTANT = 1, VISC_POWERLAW = 2 };
+
+// Everything a kernel needs to know about one periodic box.
+struct BoxParams {
+    int n[3];            // nx, ny, nz
+    long long N;         // nx*ny*nz
+    long long stride[3]; // 1, nx, nx*ny
+    double d[3];         // dx, dy, dz
+    double inv_d[3];     // 1/dx, 1/dy, 1/dz
+    double gamma, mach, reynolds, prandtl, tref_nd, powerlaw_exp;
+    double cfl;
+    int visc_model, navier_stokes;
+    unsigned quirks;
+    int scheme[3];
+};
+
+// Field pointers of one box.  q: conserved state (double); w: primitives in
+// the bulk type (u, v, w, p, c, T); r: inviscid RHS accumulator (bulk);
+// vf: viscous flux components (bulk) tau_xx, tau_xy, tau_xz, tau_yy, tau_yz,
+// tau_zz, E_x, E_y, E_z.
+template <typename B>
+struct Fields {
+    const double *q[5];
+    B *w[6];
+    B *r[5];
+    B *vf[9];
+};
+
+// schemes.hpp:14-36 constants
+struct K {
+    static constexpr double A00 = 1.0 / 3.0, A01 = -7.0 / 6.0, A02 = 11.0 / 6.0;
+    static constexpr double A10 = -1.0 / 6.0, A11 = 5.0 / 6.0, A12 = 1.0 / 3.0;
+    static constexpr double A20 = 1.0 / 3.0, A21 = 5.0 / 6.0, A22 = -1.0 / 6.0;
+    static constexpr double C0 = 0.1, C1 = 0.6, C2 = 0.3;      // WENO5 linear weights
+    static constexpr double CR0 = 0.2, CR1 = 0.5, CR2 = 0.3;   // CRWENO5 linear weights
+    static constexpr double G0 = 13.0 / 12.0, G1 = 1.0 / 4.0;
+    static constexpr double CD1 = 3.0 / 4.0, CD2 = -3.0 / 20.0, CD3 = 1.0 / 60.0;
+};
+
+__device__ __forceinline__ int wrap(int c, int n) {
+    // periodic index for c in [-n, 2n)
+    return c < 0 ? c + n : (c >= n ? c - n : c);
+}
+
+// Smoothness indicators of the three 3-cell sub-stencils (schemes.hpp
+// gamma0/gamma1 form, weno5js.cpp:75-82).  f0 is the farthest-upwind cell.
+template <typename B>
+__device__ __forceinline__ void weno5_beta(B f0, B f1, B f2, B f3, B f4, B &is0, B &is1, B &is2,
+                                           bool beta2_quirk) {
+    const B g0 = B(K::G0), g1 = B(K::G1);
+    B d0 = f0 - B(2) * f1 + f2, e0 = f0 - B(4) * f1 + B(3) * f2;
+    B d1 = f1 - B(2) * f2 + f3, e1 = f1 - f3;
+    // weno5z.cpp:80 reads f[i]-2f[i+1]+f[i+1] on inner '+' faces
+    B d2 = beta2_quirk ? (f2 - B(2) * f3 + f3) : (f2 - B(2) * f3 + f4);
+    B e2 = B(3) * f2 - B(4) * f3 + f4;
+    is0 = g0 * d0 * d0 + g1 * e0 * e0;
+    is1 = g0 * d1 * d1 + g1 * e1 * e1;
+    is2 = g0 * d2 * d2 + g1 * e2 * e2;
+}
+
+template <typename B>
+__device__ __forceinline__ void weno5_candidates(B f0, B f1, B f2, B f3, B f4, B &q0, B &q1,
+                                                 B &q2) {
+    q0 = B(K::A00) * f0 + B(K::A01) * f1 + B(K::A02) * f2;
+    q1 = B(K::A10) * f1 + B(K::A11) * f2 + B(K::A12) * f3;
+    q2 = B(K::A20) * f2 + B(K::A21) * f3 + B(K::A22) * f4;
+}
+
+// WENO5-JS face value (weno5js.cpp:75-108), eps = 1e-6, p = 2.
+// FP64: alpha_k = c_k/s_k^2 normalised by their sum, written with a single
+// division by multiplying through with s0^2 s1^2 s2^2 (an exact
+// rearrangement).  FP32: reciprocal form.
+__device__ __forceinline__ double weno5js_face(double f0, double f1, double f2, double f3,
+                                               double f4) {
+    double is0, is1, is2, q0, q1, q2;
+    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
+    weno5_candidates(f0, f1, f2, f3, f4, q0, q1, q2);
+    const double ss = 1.0e-6;
+    double s0 = ss + is0, s1 = ss + is1, s2 = ss + is2;
+    s0 *= s0;
+    s1 *= s1;
+    s2 *= s2;
+    double w0 = K::C0 * (s1 * s2), w1 = K::C1 * (s0 * s2), w2 = K::C2 * (s0 * s1);
+    return (w0 * q0 + w1 * q1 + w2 * q2) / (w0 + w1 + w2);
+}
+__device__ __forceinline__ float weno5js_face(float f0, float f1, float f2, float f3, float f4) {
+    float is0, is1, is2, q0, q1, q2;
+    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
+    weno5_candidates(f0, f1, f2, f3, f4, q0, q1, q2);
+    const float ss = 1.0e-6f;
+    float r0 = __frcp_rn(ss + is0), r1 = __frcp_rn(ss + is1), r2 = __frcp_rn(ss + is2);
+    float a0 = float(K::C0) * r0 * r0, a1 = float(K::C1) * r1 * r1, a2 = float(K::C2) * r2 * r2;
+    return (a0 * q0 + a1 * q1 + a2 * q2) * __frcp_rn(a0 + a1 + a2);
+}
+
+// WENO5-Z face value (weno5z.cpp:74-109), eps = 1e-40, p = 2:
+// alpha_k = c_k (1 + (tau/(beta_k+eps))^2), tau = |beta2 - beta0|.
+__device__ __forceinline__ double weno5z_face(double f0, double f1, double f2, double f3,
+                                              double f4, bool beta2_quirk) {
+    double is0, is1, is2, q0, q1, q2;
+    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, beta2_quirk);
+    weno5_candidates(f0, f1, f2, f3, f4, q0, q1, q2);
+    const double ss = 1.0e-40;
+    double tau = fabs(is2 - is0);
+    double t2 = tau * tau;
+    double s0 = is0 + ss, s1 = is1 + ss, s2 = is2 + ss;
+    s0 *= s0;
+    s1 *= s1;
+    s2 *= s2;
+    // alpha_k * s0^2 s1^2 s2^2 = c_k (s_k^2 + tau^2) prod_{j!=k} s_j^2
+    double w0 = K::C0 * (s0 + t2) * (s1 * s2);
+    double w1 = K::C1 * (s1 + t2) * (s0 * s2);
+    double w2 = K::C2 * (s2 + t2) * (s0 * s1);
+    return (w0 * q0 + w1 * q1 + w2 * q2) / (w0 + w1 + w2);
+}
+__device__ __forceinline__ float weno5z_face(float f0, float f1, float f2, float f3, float f4,
+                                             bool beta2_quirk) {
+    float is0, is1, is2, q0, q1, q2;
+    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, beta2_quirk);
+    weno5_candidates(f0, f1, f2, f3, f4, q0, q1, q2);
+    // 1e-40 is below FP32's normal range; 1e-30 keeps the ratio finite and
+    // only differs where a sub-stencil is exactly constant.
+    const float ss = 1.0e-30f, cap = 1.0e18f;
+    float tau = fabsf(is2 - is0);
+    float t0 = fminf(tau * __frcp_rn(is0 + ss), cap);
+    float t1 = fminf(tau * __frcp_rn(is1 + ss), cap);
+    float t2 = fminf(tau * __frcp_rn(is2 + ss), cap);
+    float a0 = float(K::C0) * (1.0f + t0 * t0);
+    float a1 = float(K::C1) * (1.0f + t1 * t1);
+    float a2 = float(K::C2) * (1.0f + t2 * t2);
+    return (a0 * q0 + a1 * q1 + a2 * q2) * __frcp_rn(a0 + a1 + a2);
+}
+
+template <int SCHEME, typename B>
+__device__ __forceinline__ B weno5_face(B f0, B f1, B f2, B f3, B f4, bool beta2_quirk) {
+    if (SCHEME == SCHEME_Z) return weno5z_face(f0, f1, f2, f3, f4, beta2_quirk);
+    return weno5js_face(f0, f1, f2, f3, f4);
+}
+
+// CD6 first derivative (centraldifference6th.cpp:44-46), times 1/dx.
+template <typename B>
+__device__ __forceinline__ B cd6(B m3, B m2, B m1, B p1, B p2, B p3, B inv_dx) {
+    return (B(K::CD3) * (p3 - m3) + B(K::CD2) * (p2 - m2) + B(K::CD1) * (p1 - m1)) * inv_dx;
+}
+
+// Viscosity and heat-conduction coefficient (physicsModel.cpp:193-266).
+template <typename B>
+__device__ __forceinline__ void viscosity(const BoxParams &bp, B T, B &miu, B &coeff) {
+    B m;
+    if (bp.visc_model == VISC_SUTHERLAND) {
+        B tr = B(bp.tref_nd);
+        m = (B(1) + tr) / (T + tr) * (T * sqrt(T)) / B(bp.reynolds);
+    } else if (bp.visc_model == VISC_CONSTANT) {
+        m = B(1) / B(bp.reynolds);
+    } else {
+        m = pow(T, B(bp.powerlaw_exp)) / B(bp.reynolds);
+    }
+    miu = m;
+    coeff = m / B((bp.gamma - 1.0) * bp.mach * bp.mach * bp.prandtl);
+}
+
+// atomic max of a non-negative double (its bit pattern orders as an integer)
+__device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
+    atomicMax(reinterpret_cast<unsigned long long *>(addr),
+              static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+}  // namespace nuc3d

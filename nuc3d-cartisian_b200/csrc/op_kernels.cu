@@ -1,0 +1,171 @@
+// Per-operator kernels behind nuc3d_reconstruct / nuc3d_cd6 /
+// nuc3d_tvdrk3_stage: the reference's scheme plug-in interface
+// (fieldOperator.h:13-81) on device buffers, with explicit halos.
+//
+// Convention (as the reference): the operator runs along the fastest axis of
+// an (nx,ny,nz) field; halo_l / halo_r are (3,ny,nz) arrays holding the three
+// cells beyond each end of every line; reconstruction output is (nx+1,ny,nz).
+#include "nuc3d_device.cuh"
+#include "op_kernels.h"
+
+namespace nuc3d {
+
+namespace {
+
+// value of cell c (-3 <= c < nx+3) of line (j,k)
+__device__ __forceinline__ double line_at(const double *in, const double *hl, const double *hr,
+                                          int nx, long long line, int c) {
+    if (c < 0) return hl[3 * line + (c + 3)];
+    if (c >= nx) return hr[3 * line + (c - nx)];
+    return in[(long long)nx * line + c];
+}
+
+}  // namespace
+
+// One thread per face.  weno5js.cpp:39-628 / weno5z.cpp:38-637: every face m
+// reads cells m-3..m+1 ('+') or m+2..m-2 ('-'); faces 3..nx-3 are the
+// "inner" faces where weno5z.cpp:80 applies.
+template <int SCHEME>
+__global__ void k_op_weno(int upwind, unsigned quirks, int nx, long long lines, const double *in,
+                          const double *hl, const double *hr, double *out) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long total = (long long)(nx + 1) * lines;
+    if (t >= total) return;
+    long long line = t / (nx + 1);
+    int m = (int)(t - line * (nx + 1));
+    double f[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+        f[k] = upwind > 0 ? line_at(in, hl, hr, nx, line, m - 3 + k)
+                          : line_at(in, hl, hr, nx, line, m + 2 - k);
+    bool quirk = SCHEME == SCHEME_Z && upwind > 0 && (quirks & QK_WENOZ_BETA2) && m >= 3 &&
+                 m <= nx - 3;
+    out[t] = SCHEME == SCHEME_Z ? weno5z_face(f[0], f[1], f[2], f[3], f[4], quirk)
+                                : weno5js_face(f[0], f[1], f[2], f[3], f[4]);
+}
+
+// One thread per line: crweno5.cpp:45-402 + halo faces :425-837.  scratch
+// holds 2*(nx) values per line (c' and d' of the Thomas sweep).
+__global__ void k_op_crweno(int upwind, int nx, long long lines, const double *in,
+                            const double *hl, const double *hr, double *out, double *scratch) {
+    long long line = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (line >= lines) return;
+    auto F = [&](int c) { return line_at(in, hl, hr, nx, line, c); };
+    auto js = [&](int m) {
+        if (upwind > 0) return weno5js_face(F(m - 3), F(m - 2), F(m - 1), F(m), F(m + 1));
+        return weno5js_face(F(m + 2), F(m + 1), F(m), F(m - 1), F(m - 2));
+    };
+    double *o = out + (long long)(nx + 1) * line;
+    for (int m = 0; m <= 2; ++m) o[m] = js(m);
+    for (int m = nx - 2; m <= nx; ++m) o[m] = js(m);
+    const int M = nx - 5;
+    double *cs = scratch + 2 * (long long)nx * line;
+    double *ds = cs + nx;
+    double cp = 0.0, dp = js(3);
+    cs[0] = cp;
+    ds[0] = dp;
+    for (int r = 1; r < M; ++r) {
+        double a, b, c, d;
+        if (r == M - 1) {
+            a = 0.0; b = 1.0; c = 0.0; d = js(r + 3);
+        } else {
+            int i = r + 2;
+            double f0, f1, f2, f3, f4;
+            if (upwind > 0) {
+                f0 = F(i - 2); f1 = F(i - 1); f2 = F(i); f3 = F(i + 1); f4 = F(i + 2);
+            } else {
+                f0 = F(i + 3); f1 = F(i + 2); f2 = F(i + 1); f3 = F(i); f4 = F(i - 1);
+            }
+            double is0, is1, is2;
+            weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
+            double a0 = K::CR0 / ((1e-6 + is0) * (1e-6 + is0));
+            double a1 = K::CR1 / ((1e-6 + is1) * (1e-6 + is1));
+            double a2 = K::CR2 / ((1e-6 + is2) * (1e-6 + is2));
+            double sum = a0 + a1 + a2;
+            double w0 = a0 / sum, w1 = a1 / sum, w2 = a2 / sum;
+            double lo = 2.0 / 3.0 * w0 + 1.0 / 3.0 * w1;
+            double hi = 1.0 / 3.0 * w2;
+            b = 1.0 / 3.0 * w0 + 2.0 / 3.0 * (w1 + w2);
+            d = 1.0 / 6.0 * w0 * f1 + (5.0 * (w0 + w1) + w2) * f2 / 6.0 + (w1 + 5.0 * w2) * f3 / 6.0;
+            if (upwind > 0) { a = lo; c = hi; } else { c = lo; a = hi; }
+        }
+        double den = b - cp * a;
+        cp = c / den;
+        dp = (d - dp * a) / den;
+        cs[r] = cp;
+        ds[r] = dp;
+    }
+    double x = ds[M - 1];
+    o[nx - 3] = x;
+    for (int r = M - 2; r >= 0; --r) {
+        x = ds[r] - cs[r] * x;
+        o[r + 3] = x;
+    }
+}
+
+// centraldifference6th.cpp:16-186: one thread per cell.
+__global__ void k_op_cd6(int nx, long long lines, double inv_dx, const double *in,
+                         const double *hl, const double *hr, double *out) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)nx * lines) return;
+    long long line = t / nx;
+    int i = (int)(t - line * nx);
+    auto F = [&](int c) { return line_at(in, hl, hr, nx, line, c); };
+    out[t] = cd6<double>(F(i - 3), F(i - 2), F(i - 1), F(i + 1), F(i + 2), F(i + 3), inv_dx);
+}
+
+// TVD-RK3.cpp:76-196
+__global__ void k_op_rk3(int stage, long long n, double dt, RK5 rk) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= 5 * n) return;
+    int e = (int)(t / n);
+    long long i = t - e * n;
+    double rhs = -rk.rhs[e][i];
+    double u;
+    if (stage == 0) {
+        u = 1.0 * rk.ui[e][i] + 1.0 * rhs * dt;
+    } else if (stage == 1) {
+        u = 0.75 * rk.un[e][i] + 0.25 * (rhs * dt + rk.ui[e][i]);
+    } else {
+        u = (1.0 / 3.0) * rk.un[e][i] + (2.0 / 3.0) * (rhs * dt + rk.ui[e][i]);
+    }
+    rk.ui[e][i] = u;
+}
+
+cudaError_t op_reconstruct(int scheme, int upwind, unsigned quirks, int nx, long long lines,
+                           const double *in, const double *hl, const double *hr, double *out,
+                           cudaStream_t st) {
+    if (scheme == SCHEME_CR) {
+        double *scratch = nullptr;
+        size_t bytes = sizeof(double) * 2 * (size_t)nx * (size_t)lines;
+        cudaError_t e = cudaMallocAsync(&scratch, bytes, st);
+        if (e != cudaSuccess) return e;
+        unsigned grid = (unsigned)((lines + 127) / 128);
+        k_op_crweno<<<grid, 128, 0, st>>>(upwind, nx, lines, in, hl, hr, out, scratch);
+        e = cudaGetLastError();
+        cudaError_t f = cudaFreeAsync(scratch, st);
+        return e != cudaSuccess ? e : f;
+    }
+    long long total = (long long)(nx + 1) * lines;
+    unsigned grid = (unsigned)((total + 255) / 256);
+    if (scheme == SCHEME_Z)
+        k_op_weno<SCHEME_Z><<<grid, 256, 0, st>>>(upwind, quirks, nx, lines, in, hl, hr, out);
+    else
+        k_op_weno<SCHEME_JS><<<grid, 256, 0, st>>>(upwind, quirks, nx, lines, in, hl, hr, out);
+    return cudaGetLastError();
+}
+
+cudaError_t op_cd6(int nx, long long lines, double dx, const double *in, const double *hl,
+                   const double *hr, double *out, cudaStream_t st) {
+    long long total = (long long)nx * lines;
+    k_op_cd6<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(nx, lines, 1.0 / dx, in, hl, hr, out);
+    return cudaGetLastError();
+}
+
+cudaError_t op_rk3(int stage, long long n, double dt, RK5 rk, cudaStream_t st) {
+    long long total = 5 * n;
+    k_op_rk3<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(stage, n, dt, rk);
+    return cudaGetLastError();
+}
+
+}  // namespace nuc3d

@@ -1,0 +1,290 @@
+"""Python binding of the nuc3d_b200 C ABI (include/nuc3d_b200.h).
+
+The CUDA path lives in lib/libnuc3d_b200.so (built by build.py).  This module
+only marshals arguments: device memory is owned by the caller (torch tensors)
+or by a solver context.  There is no CPU fallback — if the library is missing
+every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass, field, replace
+from pathlib import Path
+
+PKG_ROOT = Path(__file__).resolve().parents[2]
+LIB_PATH = PKG_ROOT / "lib" / "libnuc3d_b200.so"
+
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2, -3, -4, -5
+WENO5JS, WENO5Z, CRWENO5 = 0, 1, 2
+SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5}
+EULER3D, NAVIERSTOKES3D = 0, 1
+SUTHERLAND, CONSTANT, POWERLAW = 0, 1, 2
+FP64, MIXED = 0, 1
+QUIRK_ZETA_EIGEN = 0x1
+QUIRK_WENOZ_BETA2 = 0x2
+QUIRK_OFFDIAG_DIV = 0x4
+QUIRK_FABS_PRESSURE = 0x8
+QUIRK_CRWENO_BOUNDED = 0x10
+QUIRKS_REFERENCE = 0x1F
+PROF_NAMES = ("prim", "dt", "visc", "inv_x", "inv_y", "inv_z", "update", "residual")
+PROF_CLASSES = len(PROF_NAMES)
+
+
+class Nuc3dError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"nuc3d error {code}: {msg}")
+        self.code = code
+
+
+class _Desc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+        ("scheme", C.c_int * 3),
+        ("pde_model", C.c_int),
+        ("visc_model", C.c_int),
+        ("gamma", C.c_double), ("mach", C.c_double), ("reynolds", C.c_double),
+        ("prandtl", C.c_double), ("t_ref", C.c_double), ("t_inf", C.c_double),
+        ("powerlaw_exp", C.c_double),
+        ("precision", C.c_int),
+        ("quirks", C.c_uint),
+    ]
+
+
+_P5 = C.c_void_p * 5
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with python nuc3d-cartisian_b200/build.py")
+        L = C.CDLL(str(LIB_PATH))
+        L.nuc3d_last_error.restype = C.c_char_p
+        L.nuc3d_version.restype = C.c_char_p
+        L.nuc3d_ctx_bytes.restype = C.c_longlong
+        L.nuc3d_ctx_bytes.argtypes = [C.POINTER(_Desc)]
+        L.nuc3d_ctx_create.argtypes = [C.POINTER(_Desc), C.c_void_p, C.POINTER(C.c_void_p)]
+        L.nuc3d_ctx_destroy.argtypes = [C.c_void_p]
+        L.nuc3d_set_state_host.argtypes = [C.c_void_p, _P5]
+        L.nuc3d_get_state_host.argtypes = [C.c_void_p, _P5]
+        L.nuc3d_set_state_device.argtypes = [C.c_void_p, _P5]
+        L.nuc3d_get_state_device.argtypes = [C.c_void_p, _P5]
+        L.nuc3d_step.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        L.nuc3d_sync.argtypes = [C.c_void_p]
+        L.nuc3d_rhs.argtypes = [C.c_void_p, _P5, C.POINTER(C.c_double)]
+        L.nuc3d_ctx_time.restype = C.c_double
+        L.nuc3d_ctx_time.argtypes = [C.c_void_p]
+        L.nuc3d_profile_enable.argtypes = [C.c_void_p, C.c_int]
+        L.nuc3d_profile_read.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.nuc3d_launch_count.restype = C.c_longlong
+        L.nuc3d_launch_count.argtypes = [C.c_void_p]
+        L.nuc3d_probe_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+        L.nuc3d_reconstruct.argtypes = [C.c_int, C.c_int, C.c_uint, C.c_int, C.c_int, C.c_int,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]
+        L.nuc3d_cd6.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nuc3d_tvdrk3_stage.argtypes = [C.c_int, C.c_longlong, C.c_double, _P5, _P5, _P5,
+                                         C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def check(rc: int):
+    if rc != OK:
+        raise Nuc3dError(rc, lib().nuc3d_last_error().decode())
+
+
+@dataclass
+class BoxDesc:
+    """Mirror of nuc3d_box_desc.  Defaults follow the reference decks
+    (physicsModel.cpp:23-64, fieldOperator.cpp:22-32) with a 2*pi box."""
+
+    nx: int = 64
+    ny: int = 64
+    nz: int = 64
+    lx: float = 2.0 * math.pi
+    ly: float = 2.0 * math.pi
+    lz: float = 2.0 * math.pi
+    scheme: tuple = (WENO5JS, WENO5JS, WENO5JS)
+    pde_model: int = NAVIERSTOKES3D
+    visc_model: int = SUTHERLAND
+    gamma: float = 1.4
+    mach: float = 0.5
+    reynolds: float = 1000.0
+    prandtl: float = 0.72
+    t_ref: float = 110.4
+    t_inf: float = 288.0
+    powerlaw_exp: float = 0.76
+    precision: int = FP64
+    quirks: int = QUIRKS_REFERENCE
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny, self.nx)
+
+    def c_struct(self) -> _Desc:
+        d = _Desc()
+        d.nx, d.ny, d.nz = self.nx, self.ny, self.nz
+        d.lx, d.ly, d.lz = self.lx, self.ly, self.lz
+        for i in range(3):
+            d.scheme[i] = int(self.scheme[i])
+        d.pde_model, d.visc_model = int(self.pde_model), int(self.visc_model)
+        d.gamma, d.mach, d.reynolds = self.gamma, self.mach, self.reynolds
+        d.prandtl, d.t_ref, d.t_inf = self.prandtl, self.t_ref, self.t_inf
+        d.powerlaw_exp = self.powerlaw_exp
+        d.precision = int(self.precision)
+        d.quirks = int(self.quirks)
+        return d
+
+    def device_bytes(self) -> int:
+        d = self.c_struct()
+        return int(lib().nuc3d_ctx_bytes(C.byref(d)))
+
+
+def _ptrs5(arrs) -> "_P5":
+    out = _P5()
+    for i, a in enumerate(arrs):
+        if hasattr(a, "data_ptr"):  # torch tensor
+            assert a.is_contiguous() and str(a.dtype) == "torch.float64"
+            out[i] = a.data_ptr()
+        else:  # numpy array (host)
+            assert a.dtype.name == "float64" and a.flags.c_contiguous
+            out[i] = a.ctypes.data
+    return out
+
+
+def _stream_handle(stream) -> int:
+    if stream is None:
+        return 0
+    if hasattr(stream, "cuda_stream"):
+        return int(stream.cuda_stream)
+    return int(stream)
+
+
+class Solver:
+    """One periodic box resident on the current CUDA device (nuc3d_ctx)."""
+
+    def __init__(self, desc: BoxDesc, stream=None):
+        self.desc = desc
+        self._cdesc = desc.c_struct()
+        h = C.c_void_p()
+        check(lib().nuc3d_ctx_create(C.byref(self._cdesc), _stream_handle(stream), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().nuc3d_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def set_state(self, q):
+        """q: 5 host numpy float64 arrays or 5 CUDA float64 tensors."""
+        if hasattr(q[0], "is_cuda") and q[0].is_cuda:
+            check(lib().nuc3d_set_state_device(self._h, _ptrs5(q)))
+        else:
+            check(lib().nuc3d_set_state_host(self._h, _ptrs5(q)))
+
+    def get_state(self, out=None):
+        import numpy as np
+        if out is None:
+            out = [np.zeros(self.desc.shape) for _ in range(5)]
+        if hasattr(out[0], "is_cuda") and out[0].is_cuda:
+            check(lib().nuc3d_get_state_device(self._h, _ptrs5(out)))
+        else:
+            check(lib().nuc3d_get_state_host(self._h, _ptrs5(out)))
+        return out
+
+    def step(self, nsteps: int, cfl: float, stats: bool = True):
+        import numpy as np
+        if stats:
+            dt = np.zeros(max(nsteps, 1))
+            res = np.zeros(max(nsteps, 1))
+            check(lib().nuc3d_step(self._h, nsteps, cfl, dt.ctypes.data, res.ctypes.data))
+            return dt[:nsteps], res[:nsteps]
+        check(lib().nuc3d_step(self._h, nsteps, cfl, None, None))
+        return None
+
+    def sync(self):
+        check(lib().nuc3d_sync(self._h))
+
+    def rhs(self, out):
+        """out: 5 CUDA float64 tensors.  Returns dt_local."""
+        dtl = C.c_double(0.0)
+        check(lib().nuc3d_rhs(self._h, _ptrs5(out), C.byref(dtl)))
+        return dtl.value
+
+    def time(self) -> float:
+        return lib().nuc3d_ctx_time(self._h)
+
+    def profile(self, on: bool):
+        check(lib().nuc3d_profile_enable(self._h, int(on)))
+
+    def profile_read(self, reset: bool = True):
+        """{class: (milliseconds, launches)} accumulated while profiling."""
+        import numpy as np
+        ms = np.zeros(PROF_CLASSES)
+        n = np.zeros(PROF_CLASSES, dtype=np.int64)
+        check(lib().nuc3d_profile_read(self._h, ms.ctypes.data, n.ctypes.data, int(reset)))
+        return {name: (float(ms[i]), int(n[i])) for i, name in enumerate(PROF_NAMES)}
+
+    def launch_count(self) -> int:
+        return int(lib().nuc3d_launch_count(self._h))
+
+
+def probe_peak(precision=FP64) -> float:
+    """Measured FMA-pipe TFLOP/s of the current device (nuc3d_probe_peak)."""
+    t = C.c_double(0.0)
+    check(lib().nuc3d_probe_peak(int(precision), C.byref(t)))
+    return t.value
+
+
+def reconstruct(scheme, upwind, quirks, d_in, d_hl, d_hr, d_out, stream=None):
+    """nuc3d_reconstruct on torch CUDA tensors shaped (nz,ny,nx), (nz,ny,3)x2,
+    (nz,ny,nx+1)."""
+    nz, ny, nx = d_in.shape
+    check(lib().nuc3d_reconstruct(scheme, upwind, quirks, nx, ny, nz, d_in.data_ptr(),
+                                  d_hl.data_ptr(), d_hr.data_ptr(), d_out.data_ptr(),
+                                  _stream_handle(stream)))
+
+
+def cd6(dx, d_in, d_hl, d_hr, d_out, stream=None):
+    nz, ny, nx = d_in.shape
+    check(lib().nuc3d_cd6(nx, ny, nz, dx, d_in.data_ptr(), d_hl.data_ptr(), d_hr.data_ptr(),
+                          d_out.data_ptr(), _stream_handle(stream)))
+
+
+def tvdrk3_stage(stage, dt, d_rhs, d_un, d_ui, stream=None):
+    n = d_rhs[0].numel()
+    check(lib().nuc3d_tvdrk3_stage(stage, n, dt, _ptrs5(d_rhs), _ptrs5(d_un), _ptrs5(d_ui),
+                                   _stream_handle(stream)))
+
+
+from .decks import read_decks, write_decks  # noqa: E402
+from .initial import taylor_green, hit_field  # noqa: E402

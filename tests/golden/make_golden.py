@@ -1,0 +1,98 @@
+"""Generate the golden fixtures in this directory from the REFERENCE'S OWN
+CODE (oracle/_ref/libnuc3d_ref.so, built by ``make -C oracle ref`` from the
+reference sources).  Run from the repository root:
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+The fixtures pin both the C restatement (oracle/) and, through it, the CUDA
+path.  Inputs are seeded; every array is FP64 in numpy (nz, ny, nx) order.
+"""
+
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT / "oracle"))
+
+from oracle_ctypes import (CRWENO5, WENO5JS, WENO5Z, Box, Oracle, Reference)  # noqa: E402
+
+SCHEME_TAG = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr"}
+
+
+def perturbed_tgv(box: Box, seed: int):
+    """Taylor-Green state with seeded multiplicative noise (breaks the TGV
+    symmetries so that axis or sign slips cannot cancel)."""
+    q = Oracle().tgv(box)
+    rng = np.random.default_rng(seed)
+    return [np.ascontiguousarray(a * (1.0 + 0.02 * rng.standard_normal(a.shape))) for a in q]
+
+
+def main():
+    R = Reference()
+    rng = np.random.default_rng(2024)
+    out = {}
+    # --- per-operator: reconstruction, CD6, RK stages -------------------
+    shape = (5, 4, 14)
+    for s in (WENO5JS, WENO5Z, CRWENO5):
+        for up in (1, -1):
+            f = rng.standard_normal(shape)
+            hl = rng.standard_normal(shape[:2] + (3,))
+            hr = rng.standard_normal(shape[:2] + (3,))
+            tag = f"{SCHEME_TAG[s]}_{'p' if up > 0 else 'm'}"
+            out[f"rec_{tag}_in"], out[f"rec_{tag}_hl"], out[f"rec_{tag}_hr"] = f, hl, hr
+            out[f"rec_{tag}_out"] = R.reconstruct_field(s, up, f, hl, hr)
+    f = rng.standard_normal(shape)
+    hl = rng.standard_normal(shape[:2] + (3,))
+    hr = rng.standard_normal(shape[:2] + (3,))
+    out["cd6_in"], out["cd6_hl"], out["cd6_hr"] = f, hl, hr
+    out["cd6_dx"] = np.array(0.37)
+    out["cd6_out"] = R.cd6_field(f, 0.37, hl, hr)
+    for st in range(3):
+        rhs = [rng.standard_normal(40) for _ in range(5)]
+        un = [rng.standard_normal(40) for _ in range(5)]
+        ui = [rng.standard_normal(40) for _ in range(5)]
+        out[f"rk{st}_rhs"], out[f"rk{st}_un"], out[f"rk{st}_ui"] = (np.stack(rhs), np.stack(un),
+                                                                    np.stack(ui))
+        R.rk3_stage(st, 0.013, rhs, un, ui)
+        out[f"rk{st}_out"] = np.stack(ui)
+    out["rk_dt"] = np.array(0.013)
+    np.savez_compressed(HERE / "operators.npz", **out)
+
+    # --- con2prim + LF split ----------------------------------------------
+    box = Box(12, 10, 8, mach=0.3, reynolds=800.0)
+    q = perturbed_tgv(box, 7)
+    prim, fl, fr, eig = R.split(box, q)
+    dirs = ("xi", "eta", "zeta")  # the reference's rotated layouts (euler3d.cpp:71-76)
+    np.savez_compressed(HERE / "split.npz", q=np.stack(q), prim=np.stack(prim), eig=eig,
+                        **{f"fl_{d}": np.stack(fl[5 * i:5 * i + 5]) for i, d in enumerate(dirs)},
+                        **{f"fr_{d}": np.stack(fr[5 * i:5 * i + 5]) for i, d in enumerate(dirs)})
+
+    # --- one RHS and three steps, per scheme, N-S and Euler ----------------
+    for s in (WENO5JS, WENO5Z, CRWENO5):
+        for ns in (True, False):
+            box = Box(16, 12, 10, scheme=(s, s, s), navier_stokes=ns, mach=0.1, reynolds=1600.0,
+                      prandtl=0.71)
+            q = perturbed_tgv(box, 11 + s)
+            rhs, dtl = R.rhs(box, q)
+            tag = f"{SCHEME_TAG[s]}_{'ns' if ns else 'eu'}"
+            qn, dt, res = R.run_steps(box, 0.5, 3, q)
+            np.savez_compressed(HERE / f"step_{tag}.npz", q0=np.stack(q), rhs=np.stack(rhs),
+                                dt_local=np.array(dtl), q3=np.stack(qn), dt=dt, res=res,
+                                shape=np.array(box.shape), mach=box.mach, reynolds=box.reynolds,
+                                prandtl=box.prandtl)
+
+    # --- Taylor-Green 24^3, WENO5-JS + CD6, 10 steps (config-1 physics) ----
+    box = Box(24, 24, 24, mach=0.1, reynolds=1600.0, prandtl=0.71)
+    q0 = Oracle().tgv(box)
+    qn, dt, res = R.run_steps(box, 0.5, 10, q0)
+    np.savez_compressed(HERE / "tgv24_js_10.npz", q10=np.stack(qn), dt=dt, res=res)
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

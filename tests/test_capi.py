@@ -1,0 +1,70 @@
+"""The C-ABI library loads without a GPU and exports every entry point that
+include/nuc3d_b200.h declares; argument validation answers with status codes
+before any device work (the reference prints and exits instead,
+weno5js.cpp:32-34)."""
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+import nuc3d_b200 as nb
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "nuc3d_b200.h"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"NUC3D_API[^;(]*?\b(nuc3d_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    syms = declared_symbols()
+    assert len(syms) >= 15
+    L = nb.lib()
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_version_and_default_desc():
+    assert b"sm_100a" in nb.lib().nuc3d_version()
+    d = nb._Desc()
+    nb.lib().nuc3d_box_desc_default(C.byref(d))
+    # physicsModel.cpp:25-35 defaults, fieldOperator.cpp:22-32 (weno5js, cd6, RK3)
+    assert (d.nx, d.ny, d.nz) == (64, 64, 64)
+    assert d.reynolds == 1000.0 and d.mach == 0.5 and d.prandtl == 0.72 and d.gamma == 1.4
+    assert d.t_ref == 110.4 and d.t_inf == 288.0
+    assert list(d.scheme) == [0, 0, 0] and d.quirks == nb.QUIRKS_REFERENCE
+
+
+def test_ctx_bytes_accounting():
+    d = nb.BoxDesc(32, 32, 32)
+    fp64 = d.device_bytes()
+    mixed = nb.BoxDesc(32, 32, 32, precision=nb.MIXED).device_bytes()
+    assert fp64 >= 21 * 32 ** 3 * 8 + 14 * 32 ** 3 * 8
+    assert mixed < fp64
+    assert nb.BoxDesc(4, 32, 32).device_bytes() == -1  # too small a box
+
+
+@pytest.mark.parametrize("args,code", [
+    ((7, 1, 0, 16, 2, 2), nb.ERR_UNSUPPORTED),   # no such scheme
+    ((0, 2, 0, 16, 2, 2), nb.ERR_INVALID),       # no such direction
+    ((0, 1, 0, 5, 2, 2), nb.ERR_INVALID),        # line too short
+    ((2, 1, 0, 5000, 2, 2), nb.ERR_INVALID),     # crweno5 line too long
+])
+def test_reconstruct_validation_without_device(args, code):
+    rc = nb.lib().nuc3d_reconstruct(*args, None, None, None, None, None)
+    assert rc == code
+    assert nb.lib().nuc3d_last_error()
+
+
+def test_ctx_create_rejects_bad_descriptions_without_device():
+    L = nb.lib()
+    h = C.c_void_p()
+    for bad in (nb.BoxDesc(4, 16, 16), nb.BoxDesc(16, 16, 16, scheme=(0, 5, 0)),
+                nb.BoxDesc(16, 16, 16, mach=-1.0), nb.BoxDesc(16, 16, 16, precision=3)):
+        d = bad.c_struct()
+        assert L.nuc3d_ctx_create(C.byref(d), None, C.byref(h)) in (nb.ERR_INVALID,
+                                                                    nb.ERR_UNSUPPORTED)
+        assert not h.value

@@ -1,0 +1,29 @@
+"""Deck parsing mirrors the reference's readers (fieldOperator.cpp:100-125,
+physicsModel.cpp:66-156, block.cpp:49-61)."""
+
+import pytest
+
+import nuc3d_b200 as nb
+
+
+def test_decks_round_trip(tmp_path):
+    d = nb.BoxDesc(48, 32, 24, lx=6.0, ly=5.0, lz=4.0, scheme=(nb.WENO5Z, nb.CRWENO5, nb.WENO5JS),
+                   mach=0.3, reynolds=1234.5, prandtl=0.7, pde_model=nb.EULER3D)
+    nb.write_decks(tmp_path, d, {"cfl": 0.4, "endStep": 10})
+    r, io, phys = nb.read_decks(tmp_path)
+    for k in ("nx", "ny", "nz", "lx", "ly", "lz", "scheme", "mach", "reynolds", "prandtl",
+              "pde_model", "gamma", "t_ref", "t_inf"):
+        assert getattr(r, k) == getattr(d, k), k
+    assert io["cfl"] == 0.4 and io["endStep"] == 10
+
+
+def test_decks_reject_paths_off_the_gpu_route(tmp_path):
+    nb.write_decks(tmp_path, nb.BoxDesc(16, 16, 16))
+    p = tmp_path / "inp" / "PhysModel.in"
+    p.write_text(p.read_text().replace("RiemannSolver LF", "RiemannSolver AUSM"))
+    with pytest.raises(ValueError):
+        nb.read_decks(tmp_path)
+    nb.write_decks(tmp_path, nb.BoxDesc(16, 16, 16))
+    p.write_text(p.read_text() + "Bogus 1.0\n")
+    with pytest.raises(ValueError, match="does not exist"):
+        nb.read_decks(tmp_path)

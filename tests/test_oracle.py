@@ -1,0 +1,117 @@
+"""The CPU oracle (oracle/nuc3d_oracle.c) pinned against the reference.
+
+Golden fixtures were produced by the reference's own translation units
+(tests/golden/make_golden.py); the oracle must reproduce them bitwise.  When
+the reference checker library is present (this container), the oracle is
+also compared live on fresh seeded inputs.
+"""
+
+import numpy as np
+import pytest
+
+from helpers import box_from_golden, golden
+from oracle_ctypes import (CRWENO5, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_WENOZ_BETA2, WENO5JS,
+                           WENO5Z, Box, Oracle, Reference)
+
+TAGS = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr"}
+
+
+@pytest.fixture(scope="module")
+def O():
+    return Oracle()
+
+
+@pytest.mark.parametrize("scheme", [WENO5JS, WENO5Z, CRWENO5])
+@pytest.mark.parametrize("up", [1, -1])
+def test_reconstruct_matches_reference_golden(O, scheme, up):
+    z = golden("operators.npz")
+    tag = f"{TAGS[scheme]}_{'p' if up > 0 else 'm'}"
+    out = O.reconstruct_field(scheme, up, QUIRKS_REFERENCE, z[f"rec_{tag}_in"],
+                              z[f"rec_{tag}_hl"], z[f"rec_{tag}_hr"])
+    assert np.array_equal(out, z[f"rec_{tag}_out"])
+
+
+def test_cd6_and_rk3_match_reference_golden(O):
+    z = golden("operators.npz")
+    out = O.cd6_field(z["cd6_in"], float(z["cd6_dx"]), z["cd6_hl"], z["cd6_hr"])
+    assert np.array_equal(out, z["cd6_out"])
+    for st in range(3):
+        ui = [np.ascontiguousarray(a) for a in z[f"rk{st}_ui"]]
+        O.rk3_stage(st, float(z["rk_dt"]), list(z[f"rk{st}_rhs"]), list(z[f"rk{st}_un"]), ui)
+        assert np.array_equal(np.stack(ui), z[f"rk{st}_out"])
+
+
+def test_split_matches_reference_golden(O):
+    z = golden("split.npz")
+    box = Box(12, 10, 8, mach=0.3, reynolds=800.0)
+    q = [np.ascontiguousarray(a) for a in z["q"]]
+    prim = O.con2prim(box, q)
+    assert np.array_equal(np.stack(prim), z["prim"])
+
+
+@pytest.mark.parametrize("scheme", [WENO5JS, WENO5Z, CRWENO5])
+@pytest.mark.parametrize("ns", [True, False])
+def test_rhs_and_steps_match_reference_golden(O, scheme, ns):
+    z = golden(f"step_{TAGS[scheme]}_{'ns' if ns else 'eu'}.npz")
+    box = box_from_golden(z, scheme, ns)
+    q0 = [np.ascontiguousarray(a) for a in z["q0"]]
+    rhs, dtl = O.rhs(box, q0)
+    assert np.array_equal(np.stack(rhs), z["rhs"])
+    assert dtl == float(z["dt_local"])
+    q3, dt, res = O.run_steps(box, 0.5, 3, q0)
+    assert np.array_equal(np.stack(q3), z["q3"])
+    assert np.array_equal(dt, z["dt"]) and np.array_equal(res, z["res"])
+
+
+def test_tgv24_ten_steps_match_reference_golden(O):
+    z = golden("tgv24_js_10.npz")
+    box = Box(24, 24, 24, mach=0.1, reynolds=1600.0, prandtl=0.71)
+    q, dt, res = O.run_steps(box, 0.5, 10, O.tgv(box))
+    assert np.array_equal(np.stack(q), z["q10"])
+    assert np.array_equal(dt, z["dt"]) and np.array_equal(res, z["res"])
+
+
+@pytest.mark.skipif(not Reference.available(), reason="reference checker not built here")
+@pytest.mark.parametrize("scheme", [WENO5JS, WENO5Z, CRWENO5])
+def test_oracle_matches_reference_live(O, scheme):
+    R = Reference()
+    rng = np.random.default_rng(99 + scheme)
+    box = Box(14, 9, 11, scheme=(scheme,) * 3, mach=0.2, reynolds=500.0)
+    q = [a * (1 + 0.05 * rng.standard_normal(a.shape)) for a in O.tgv(box, (0.3, -0.2, 0.1))]
+    a, dta = O.rhs(box, q)
+    b, dtb = R.rhs(box, q)
+    assert np.array_equal(np.stack(a), np.stack(b)) and dta == dtb
+    qa, _, ra = O.run_steps(box, 0.4, 2, q)
+    qb, _, rb = R.run_steps(box, 0.4, 2, q)
+    assert np.array_equal(np.stack(qa), np.stack(qb)) and np.array_equal(ra, rb)
+
+
+def test_oracle_translation_invariance_without_position_quirks(O):
+    """With the two position-dependent reference behaviours switched off
+    (WENO5-Z inner beta2, bounded CRWENO lines), the periodic RHS commutes
+    with a shift of the box."""
+    quirks = QUIRKS_REFERENCE & ~Q_WENOZ_BETA2 & ~Q_CRWENO_BOUNDED
+    rng = np.random.default_rng(3)
+    for scheme in (WENO5JS, WENO5Z, CRWENO5):
+        box = Box(12, 10, 9, scheme=(scheme,) * 3, quirks=quirks, mach=0.3)
+        q = [a * (1 + 0.03 * rng.standard_normal(a.shape)) for a in O.tgv(box)]
+        r0, _ = O.rhs(box, q)
+        qs = [np.ascontiguousarray(np.roll(a, (2, -1, 3), axis=(0, 1, 2))) for a in q]
+        r1, _ = O.rhs(box, qs)
+        for a, b in zip(r0, r1):
+            np.testing.assert_allclose(np.roll(a, (2, -1, 3), axis=(0, 1, 2)), b, rtol=0,
+                                       atol=1e-10 * np.abs(a).max())
+
+
+def test_oracle_weno_z_quirk_changes_only_inner_plus_faces(O):
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal((2, 3, 16))
+    hl = rng.standard_normal((2, 3, 3))
+    hr = rng.standard_normal((2, 3, 3))
+    a = O.reconstruct_field(WENO5Z, 1, QUIRKS_REFERENCE, f, hl, hr)
+    b = O.reconstruct_field(WENO5Z, 1, QUIRKS_REFERENCE & ~Q_WENOZ_BETA2, f, hl, hr)
+    diff = np.abs(a - b).max(axis=(0, 1))
+    assert np.all(diff[:3] == 0) and np.all(diff[-3:] == 0) and np.all(diff[3:-3] > 0)
+    am = O.reconstruct_field(WENO5Z, -1, QUIRKS_REFERENCE, f, hl, hr)
+    bm = O.reconstruct_field(WENO5Z, -1, QUIRKS_REFERENCE & ~Q_WENOZ_BETA2, f, hl, hr)
+    assert np.array_equal(am, bm)
