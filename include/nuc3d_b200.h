@@ -166,6 +166,22 @@ NUC3D_API int nuc3d_reconstruct(int scheme, int upwind, unsigned quirks, int nx,
                       const double *d_in, const double *d_halo_l, const double *d_halo_r,
                       double *d_out, void *stream);
 
+/* CRWENO5 reconstruction that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that cannot let a library allocate device
+ * memory (a host code that owns all device memory through its own pool, or
+ * a plug-in called where allocation is forbidden).  Same arguments and
+ * results as nuc3d_reconstruct(NUC3D_CRWENO5, ...), but the Thomas-sweep
+ * scratch is a fixed 4 MiB array in the library's device image (held by
+ * every GPU that loads the library until exit), so 2*nx*ny*nz must not
+ * exceed 524288; larger calls return NUC3D_ERR_INVALID.  The first call on
+ * each device looks up the array's device address (cudaGetSymbolAddress)
+ * and should come before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised. */
+NUC3D_API int nuc3d_reconstruct_crweno5_noalloc(int upwind, int nx, int ny, int nz,
+                                                const double *d_in, const double *d_halo_l,
+                                                const double *d_halo_r, double *d_out,
+                                                void *stream);
+
 /* centraldifference6th::differentialInner + BoundaryL + BoundaryR
  * (centraldifference6th.cpp:16-186); out is (nx,ny,nz). */
 NUC3D_API int nuc3d_cd6(int nx, int ny, int nz, double dx, const double *d_in, const double *d_halo_l,

@@ -59,6 +59,8 @@ int validate(const nuc3d_box_desc *d) {
 
 }  // namespace
 
+int nuc3d::set_last_error(int code, const char *msg) { return fail(code, msg); }
+
 struct nuc3d_ctx {
     nuc3d_box_desc desc;
     BoxParams bp;

@@ -155,6 +155,14 @@ cudaError_t op_reconstruct(int scheme, int upwind, unsigned quirks, int nx, long
     return cudaGetLastError();
 }
 
+cudaError_t op_crweno_into(int upwind, int nx, long long lines, const double *in,
+                           const double *hl, const double *hr, double *out, double *scratch,
+                           cudaStream_t st) {
+    unsigned grid = (unsigned)((lines + 127) / 128);
+    k_op_crweno<<<grid, 128, 0, st>>>(upwind, nx, lines, in, hl, hr, out, scratch);
+    return cudaGetLastError();
+}
+
 cudaError_t op_cd6(int nx, long long lines, double dx, const double *in, const double *hl,
                    const double *hr, double *out, cudaStream_t st) {
     long long total = (long long)nx * lines;
