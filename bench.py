@@ -81,7 +81,8 @@ def config_dict(n_gpus, reynolds):
         "boxes_per_gpu": 1,
         "reynolds": reynolds,
         "parallelism": f"replicas x{n_gpus} (one box per GPU, no collective)",
-        "l2_flush": "not needed: 671 MB FP64 state per box > 126 MB L2",
+        "l2_flush": (f"not needed: {40 * NX ** 3 / 1e6:.0f} MB FP64 state per box > 126 MB L2"
+                     if 40 * NX ** 3 > 126e6 else "state smaller than L2 (profiling size only)"),
     }
 
 
@@ -387,8 +388,10 @@ def run_reference(args, rank, world):
 
 
 def main():
+    global NX, METRIC
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--n", type=int, default=NX, help="box edge (default 256; smaller only for profiling)")
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
@@ -401,6 +404,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    NX = args.n
+    METRIC = METRIC.replace("256^3", f"{NX}^3")
     rank = env_int("RANK", 0)
     world = env_int("WORLD_SIZE", args.gpus)
     local_rank = env_int("LOCAL_RANK", 0)
