@@ -89,13 +89,16 @@ template <typename B>
 struct InvTile<0, B> {  // sweep along x: tile = TL rows (j) x TC cells (x)
     static constexpr int TL = 8, TC = 32;
 };
+// sweep along y / z: tile = TL columns (i) x TC cells along the sweep.  TL
+// columns of B make one full 128-byte row per load; FP64 uses 16 columns so
+// that four to five blocks fit per SM.
 template <typename B>
-struct InvTile<1, B> {  // sweep along y: tile = TL columns (i) x TC cells (y)
-    static constexpr int TL = 32, TC = 16;
+struct InvTile<1, B> {
+    static constexpr int TL = 128 / sizeof(B), TC = 16;
 };
 template <typename B>
 struct InvTile<2, B> {
-    static constexpr int TL = 32, TC = 16;
+    static constexpr int TL = 128 / sizeof(B), TC = 16;
 };
 
 template <int DIR, typename B>
@@ -263,168 +266,6 @@ __global__ void __launch_bounds__(InvGeom<DIR, B>::NT)
     }
 }
 
-// ------------------------------------------------------------ k_visc_flux --
-// solveGrads + solveViscousFlux (NaiverStokes3d.cpp:87-303): CD6 gradients of
-// u, v, w, T (differences in FP64), stresses and heat flux in the bulk type.
-template <typename B>
-__global__ void __launch_bounds__(256) k_visc_flux(BoxParams bp, PrimView w, BView9<B> vf) {
-    const int nx = bp.n[0], ny = bp.n[1], nz = bp.n[2];
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < bp.N;
-         n += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(n % nx);
-        long long rest = n / nx;
-        int j = (int)(rest % ny);
-        int k = (int)(rest / ny);
-        long long base_x = n - i, base_y = i + (long long)nx * ny * k, base_z = i + (long long)nx * j;
-        B g[4][3];
-        const int src[4] = {0, 1, 2, 5};  // u, v, w, T
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const double *f = w.w[src[s]];
-            // along x
-            {
-                double d1 = f[base_x + wrap(i + 1, nx)] - f[base_x + wrap(i - 1, nx)];
-                double d2 = f[base_x + wrap(i + 2, nx)] - f[base_x + wrap(i - 2, nx)];
-                double d3 = f[base_x + wrap(i + 3, nx)] - f[base_x + wrap(i - 3, nx)];
-                g[s][0] = B((K::CD3 * d3 + K::CD2 * d2 + K::CD1 * d1) * bp.inv_d[0]);
-            }
-            {
-                long long sy = nx;
-                double d1 = f[base_y + sy * wrap(j + 1, ny)] - f[base_y + sy * wrap(j - 1, ny)];
-                double d2 = f[base_y + sy * wrap(j + 2, ny)] - f[base_y + sy * wrap(j - 2, ny)];
-                double d3 = f[base_y + sy * wrap(j + 3, ny)] - f[base_y + sy * wrap(j - 3, ny)];
-                g[s][1] = B((K::CD3 * d3 + K::CD2 * d2 + K::CD1 * d1) * bp.inv_d[1]);
-            }
-            {
-                long long sz = (long long)nx * ny;
-                double d1 = f[base_z + sz * wrap(k + 1, nz)] - f[base_z + sz * wrap(k - 1, nz)];
-                double d2 = f[base_z + sz * wrap(k + 2, nz)] - f[base_z + sz * wrap(k - 2, nz)];
-                double d3 = f[base_z + sz * wrap(k + 3, nz)] - f[base_z + sz * wrap(k - 3, nz)];
-                g[s][2] = B((K::CD3 * d3 + K::CD2 * d2 + K::CD1 * d1) * bp.inv_d[2]);
-            }
-        }
-        B ux = g[0][0], uy = g[0][1], uz = g[0][2];
-        B vx = g[1][0], vy = g[1][1], vz = g[1][2];
-        B wx = g[2][0], wy = g[2][1], wz = g[2][2];
-        B tx = g[3][0], ty = g[3][1], tz = g[3][2];
-        B grad = ux + vy + wz;
-        B miu0, coeff0;
-        viscosity<B>(bp, B(w.w[5][n]), miu0, coeff0);
-        const B c23 = B(2.0 / 3.0);
-        const bool od = (bp.quirks & QK_OFFDIAG_DIV) != 0;
-        B dv = od ? c23 * grad : B(0);
-        B t_xx = miu0 * (B(2) * ux - c23 * grad);
-        B t_xy = miu0 * (uy + vx - dv);
-        B t_xz = miu0 * (uz + wx - dv);
-        B t_yy = miu0 * (B(2) * vy - c23 * grad);
-        B t_yz = miu0 * (vz + wy - dv);
-        B t_zz = miu0 * (B(2) * wz - c23 * grad);
-        B u = B(w.w[0][n]), v = B(w.w[1][n]), ww = B(w.w[2][n]);
-        vf.f[0][n] = t_xx;
-        vf.f[1][n] = t_xy;
-        vf.f[2][n] = t_xz;
-        vf.f[3][n] = t_yy;
-        vf.f[4][n] = t_yz;
-        vf.f[5][n] = t_zz;
-        vf.f[6][n] = u * t_xx + v * t_xy + ww * t_xz + coeff0 * tx;
-        vf.f[7][n] = u * t_xy + v * t_yy + ww * t_yz + coeff0 * ty;
-        vf.f[8][n] = u * t_xz + v * t_yz + ww * t_zz + coeff0 * tz;
-    }
-}
-
-// --------------------------------------------------------------- k_update --
-// setDerivativesVis (NaiverStokes3d.cpp:305-369): CD6 of the viscous fluxes,
-// RHS = inviscid - viscous (:385-499), then the TVD-RK3 stage
-// (TVD-RK3.cpp:76-196, dQ/dt = -RHS) in FP64, plus the residual sum of
-// PDEData3d::setRES (PDEData3d.cpp:178-213) on the last stage and a finite
-// check of the new state.
-template <typename B>
-__global__ void __launch_bounds__(256)
-    k_update(BoxParams bp, BView<B> r, BView9<B> vf, StateView un, StateView uin,
-             StateViewMut uout, int stage, const StepScalars *sc, double *res_acc,
-             unsigned *flags) {
-    const int nx = bp.n[0], ny = bp.n[1], nz = bp.n[2];
-    const double dt = sc->dt;
-    double res = 0.0;
-    bool bad = false;
-    const bool vis = bp.navier_stokes != 0;
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < bp.N;
-         n += (long long)gridDim.x * blockDim.x) {
-        B R[5];
-#pragma unroll
-        for (int e = 0; e < 5; ++e) R[e] = r.f[e][n];
-        if (vis) {
-            int i = (int)(n % nx);
-            long long rest = n / nx;
-            int j = (int)(rest % ny);
-            int k = (int)(rest / ny);
-            long long bx = n - i, by = i + (long long)nx * ny * k, bz = i + (long long)nx * j;
-            long long sy = nx, sz = (long long)nx * ny;
-            const B ix = B(bp.inv_d[0]), iy = B(bp.inv_d[1]), iz = B(bp.inv_d[2]);
-            // x: tau_xx, tau_xy, tau_xz, E_x ; y: tau_xy, tau_yy, tau_yz, E_y ;
-            // z: tau_xz, tau_yz, tau_zz, E_z
-            const int cx[4] = {0, 1, 2, 6}, cy[4] = {1, 3, 4, 7}, cz[4] = {2, 4, 5, 8};
-            B dfx[4], dfy[4], dfz[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const B *f = vf.f[cx[e]];
-                dfx[e] = cd6<B>(f[bx + wrap(i - 3, nx)], f[bx + wrap(i - 2, nx)],
-                                f[bx + wrap(i - 1, nx)], f[bx + wrap(i + 1, nx)],
-                                f[bx + wrap(i + 2, nx)], f[bx + wrap(i + 3, nx)], ix);
-                f = vf.f[cy[e]];
-                dfy[e] = cd6<B>(f[by + sy * wrap(j - 3, ny)], f[by + sy * wrap(j - 2, ny)],
-                                f[by + sy * wrap(j - 1, ny)], f[by + sy * wrap(j + 1, ny)],
-                                f[by + sy * wrap(j + 2, ny)], f[by + sy * wrap(j + 3, ny)], iy);
-                f = vf.f[cz[e]];
-                dfz[e] = cd6<B>(f[bz + sz * wrap(k - 3, nz)], f[bz + sz * wrap(k - 2, nz)],
-                                f[bz + sz * wrap(k - 1, nz)], f[bz + sz * wrap(k + 1, nz)],
-                                f[bz + sz * wrap(k + 2, nz)], f[bz + sz * wrap(k + 3, nz)], iz);
-            }
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                B t = R[1 + e];
-                t -= dfx[e];
-                t -= dfy[e];
-                t -= dfz[e];
-                R[1 + e] = t;
-            }
-        }
-        if (stage < 0) {  // RHS only (nuc3d_rhs)
-#pragma unroll
-            for (int e = 0; e < 5; ++e) uout.q[e][n] = double(R[e]);
-            continue;
-        }
-#pragma unroll
-        for (int e = 0; e < 5; ++e) {
-            double rhs = -double(R[e]);
-            double u_n = un.q[e][n];
-            double out;
-            if (stage == 0) {
-                out = 1.0 * uin.q[e][n] + 1.0 * rhs * dt;
-            } else if (stage == 1) {
-                out = 0.75 * u_n + 0.25 * (rhs * dt + uin.q[e][n]);
-            } else {
-                out = (1.0 / 3.0) * u_n + (2.0 / 3.0) * (rhs * dt + uin.q[e][n]);
-                double dd = out - u_n;
-                res += dd * dd;
-            }
-            bad |= !isfinite(out);
-            uout.q[e][n] = out;
-        }
-    }
-    if (bad) atomicOr(flags, 1u);
-    if (stage != 2) return;
-    for (int o = 16; o > 0; o >>= 1) res += __shfl_xor_sync(0xffffffffu, res, o);
-    __shared__ double red[8];
-    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) red[warp] = res;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) res += red[i];
-        atomicAdd(res_acc, res);
-    }
-}
-
 // k_residual_final: residual = sqrt(sum / (5 N)) / dt (PDEData3d.cpp:212)
 __global__ void k_residual(BoxParams bp, StepScalars *sc, double *res_acc, int step) {
     double r = sqrt(*res_acc / (double)(bp.N * 5)) / sc->dt;
@@ -500,22 +341,6 @@ cudaError_t launch_dt(const BoxParams &bp, const double *eig, StepScalars *sc, i
     return cudaGetLastError();
 }
 
-template <typename B>
-cudaError_t launch_visc_flux(const BoxParams &bp, PrimView w, BView9<B> vf, int sms,
-                             cudaStream_t st) {
-    k_visc_flux<B><<<grid_for(bp.N, sms), 256, 0, st>>>(bp, w, vf);
-    return cudaGetLastError();
-}
-
-template <typename B>
-cudaError_t launch_update(const BoxParams &bp, BView<B> r, BView9<B> vf, StateView un,
-                          StateView uin, StateViewMut uout, int stage, const StepScalars *sc,
-                          double *res_acc, unsigned *flags, int sms, cudaStream_t st) {
-    k_update<B><<<grid_for(bp.N, sms), 256, 0, st>>>(bp, r, vf, un, uin, uout, stage, sc,
-                                                     res_acc, flags);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_residual(const BoxParams &bp, StepScalars *sc, double *res_acc, int step,
                             cudaStream_t st) {
     k_residual<<<1, 1, 0, st>>>(bp, sc, res_acc, step);
@@ -526,17 +351,4 @@ template cudaError_t launch_inviscid<double>(const BoxParams &, int, StateView, 
                                              BView<double>, int, cudaStream_t);
 template cudaError_t launch_inviscid<float>(const BoxParams &, int, StateView, PrimView,
                                             BView<float>, int, cudaStream_t);
-template cudaError_t launch_visc_flux<double>(const BoxParams &, PrimView, BView9<double>, int,
-                                              cudaStream_t);
-template cudaError_t launch_visc_flux<float>(const BoxParams &, PrimView, BView9<float>, int,
-                                             cudaStream_t);
-template cudaError_t launch_update<double>(const BoxParams &, BView<double>, BView9<double>,
-                                           StateView, StateView, StateViewMut, int,
-                                           const StepScalars *, double *, unsigned *, int,
-                                           cudaStream_t);
-template cudaError_t launch_update<float>(const BoxParams &, BView<float>, BView9<float>,
-                                          StateView, StateView, StateViewMut, int,
-                                          const StepScalars *, double *, unsigned *, int,
-                                          cudaStream_t);
-
 }  // namespace nuc3d

@@ -1,0 +1,308 @@
+// 2.5-D blocked stencil kernels of the viscous part and the RK update.
+//
+// A block owns a 32 x 8 column tile of the box and marches a chunk of KZ
+// planes along z.  For each plane it stages the tile plus the x/y halo in
+// shared memory (the x- and y-direction CD6 stencils read it there) while
+// every thread keeps a 7-deep register queue of its own column for the
+// z-direction stencil, so each value is fetched from L2/HBM about once per
+// plane instead of once per stencil tap.
+#include "nuc3d_device.cuh"
+#include "rhs_kernels.h"
+
+namespace nuc3d {
+
+namespace {
+
+constexpr int TX = 32, TY = 8, KZ = 32;
+
+// Asynchronous global->shared copy of one element (cp.async, L1-allocating),
+// so a plane's halo tile streams in while the previous plane is computed.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem) {
+    unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem),
+                 "n"(sizeof(T)));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+__device__ __forceinline__ int pmod(int c, int n) {
+    int r = c % n;
+    return r < 0 ? r + n : r;
+}
+
+__device__ __forceinline__ double cd6d(double m3, double m2, double m1, double p1, double p2,
+                                       double p3, double inv) {
+    return (K::CD3 * (p3 - m3) + K::CD2 * (p2 - m2) + K::CD1 * (p1 - m1)) * inv;
+}
+
+}  // namespace
+
+// solveGrads + solveViscousFlux (NaiverStokes3d.cpp:87-303): CD6 gradients
+// of u, v, w, T (FP64 differences), stresses and heat flux in the bulk type,
+// written as tau_xx, tau_xy, tau_xz, tau_yy, tau_yz, tau_zz, E_x, E_y, E_z.
+template <typename B>
+__global__ void __launch_bounds__(TX *TY) k_visc_flux25(BoxParams bp, PrimView w, BView9<B> vf) {
+    __shared__ double sP[2][4][TY + 6][TX + 6];
+    const int nx = bp.n[0], ny = bp.n[1], nz = bp.n[2];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool active = i < nx && j < ny;
+    const long long sz = bp.stride[2];
+    const long long col = active ? (long long)i + (long long)nx * j : 0;
+    const int src[4] = {0, 1, 2, 5};  // u, v, w, T
+    auto issue = [&](int k, int buf) {
+        const long long plane = sz * k;
+        for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
+            int yy = t / (TX + 6), xx = t - yy * (TX + 6);
+            long long g = plane + pmod(i0 - 3 + xx, nx) + (long long)nx * pmod(j0 - 3 + yy, ny);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) cp_async_elem(&sP[buf][f][yy][xx], w.w[src[f]] + g);
+        }
+    };
+    const int kend = min(k0 + KZ, nz);
+    issue(k0, 0);
+    cp_async_commit();
+    double qz[4][7];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        long long g = col + sz * pmod(k0 - 3 + s, nz);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) qz[f][s] = active ? w.w[src[f]][g] : 0.0;
+    }
+    const double ix = bp.inv_d[0], iy = bp.inv_d[1], iz = bp.inv_d[2];
+    const B c23 = B(2.0 / 3.0);
+    const bool od = (bp.quirks & QK_OFFDIAG_DIV) != 0;
+    for (int k = k0; k < kend; ++k) {
+        const int buf = (k - k0) & 1;
+        if (k + 1 < kend) issue(k + 1, buf ^ 1);
+        cp_async_commit();
+        {
+            long long g = col + sz * pmod(k + 3, nz);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) qz[f][6] = active ? w.w[src[f]][g] : 0.0;
+        }
+        cp_async_wait1();
+        __syncthreads();
+        if (active) {
+            B gr[4][3];
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                const int r = ty + 3, c = tx + 3;
+                const double(*P)[TX + 6] = sP[buf][f];
+                gr[f][0] = B(cd6d(P[r][c - 3], P[r][c - 2], P[r][c - 1], P[r][c + 1], P[r][c + 2],
+                                  P[r][c + 3], ix));
+                gr[f][1] = B(cd6d(P[r - 3][c], P[r - 2][c], P[r - 1][c], P[r + 1][c], P[r + 2][c],
+                                  P[r + 3][c], iy));
+                gr[f][2] = B(cd6d(qz[f][0], qz[f][1], qz[f][2], qz[f][4], qz[f][5], qz[f][6], iz));
+            }
+            B ux = gr[0][0], uy = gr[0][1], uz = gr[0][2];
+            B vx = gr[1][0], vy = gr[1][1], vz = gr[1][2];
+            B wx = gr[2][0], wy = gr[2][1], wz = gr[2][2];
+            B tx_ = gr[3][0], ty_ = gr[3][1], tz_ = gr[3][2];
+            B grad = ux + vy + wz;
+            B miu0, coeff0;
+            viscosity<B>(bp, B(qz[3][3]), miu0, coeff0);
+            B dv = od ? c23 * grad : B(0);
+            B t_xx = miu0 * (B(2) * ux - c23 * grad);
+            B t_xy = miu0 * (uy + vx - dv);
+            B t_xz = miu0 * (uz + wx - dv);
+            B t_yy = miu0 * (B(2) * vy - c23 * grad);
+            B t_yz = miu0 * (vz + wy - dv);
+            B t_zz = miu0 * (B(2) * wz - c23 * grad);
+            B u = B(qz[0][3]), v = B(qz[1][3]), ww = B(qz[2][3]);
+            long long g = col + sz * k;
+            vf.f[0][g] = t_xx;
+            vf.f[1][g] = t_xy;
+            vf.f[2][g] = t_xz;
+            vf.f[3][g] = t_yy;
+            vf.f[4][g] = t_yz;
+            vf.f[5][g] = t_zz;
+            vf.f[6][g] = u * t_xx + v * t_xy + ww * t_xz + coeff0 * tx_;
+            vf.f[7][g] = u * t_xy + v * t_yy + ww * t_yz + coeff0 * ty_;
+            vf.f[8][g] = u * t_xz + v * t_yz + ww * t_zz + coeff0 * tz_;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < 6; ++s)
+#pragma unroll
+            for (int f = 0; f < 4; ++f) qz[f][s] = qz[f][s + 1];
+    }
+}
+
+// setDerivativesVis (NaiverStokes3d.cpp:305-369): CD6 of the viscous fluxes,
+// RHS = inviscid - viscous in the reference's order (:385-499), then the
+// TVD-RK3 stage (TVD-RK3.cpp:76-196, dQ/dt = -RHS) in FP64; on the last stage
+// also the residual sum of PDEData3d::setRES (PDEData3d.cpp:178-213).  Every
+// new state value passes a finite check.  stage = -1 writes the total RHS.
+template <typename B, bool VIS>
+__global__ void __launch_bounds__(TX *TY)
+    k_update25(BoxParams bp, BView<B> r, BView9<B> vf, StateView un, StateView uin,
+               StateViewMut uout, int stage, const StepScalars *sc, double *res_acc,
+               unsigned *flags) {
+    // x stencils: tau_xx, tau_xy, tau_xz, E_x; y: tau_xy, tau_yy, tau_yz, E_y;
+    // z: tau_xz, tau_yz, tau_zz, E_z
+    __shared__ B sX[2][VIS ? 4 : 1][TY][TX + 6];
+    __shared__ B sY[2][VIS ? 4 : 1][TY + 6][TX];
+    __shared__ double red[TX * TY / 32];
+    const int cx[4] = {0, 1, 2, 6}, cy[4] = {1, 3, 4, 7}, cz[4] = {2, 4, 5, 8};
+    const int nx = bp.n[0], ny = bp.n[1], nz = bp.n[2];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool active = i < nx && j < ny;
+    const long long sz = bp.stride[2];
+    const long long col = active ? (long long)i + (long long)nx * j : 0;
+    const double dt = sc->dt;
+    const B ixb = B(bp.inv_d[0]), iyb = B(bp.inv_d[1]), izb = B(bp.inv_d[2]);
+    const int kend = min(k0 + KZ, nz);
+    auto issue = [&](int k, int buf) {
+        const long long plane = sz * k;
+        for (int t = tid; t < TY * (TX + 6); t += TX * TY) {
+            int yy = t / (TX + 6), xx = t - yy * (TX + 6);
+            long long g = plane + pmod(i0 - 3 + xx, nx) + (long long)nx * pmod(j0 + yy, ny);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) cp_async_elem(&sX[buf][f][yy][xx], vf.f[cx[f]] + g);
+        }
+        for (int t = tid; t < (TY + 6) * TX; t += TX * TY) {
+            int yy = t / TX, xx = t - yy * TX;
+            long long g = plane + pmod(i0 + xx, nx) + (long long)nx * pmod(j0 - 3 + yy, ny);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) cp_async_elem(&sY[buf][f][yy][xx], vf.f[cy[f]] + g);
+        }
+    };
+    B qz[4][7];
+    if (VIS) {
+        issue(k0, 0);
+        cp_async_commit();
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            long long g = col + sz * pmod(k0 - 3 + s, nz);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) qz[f][s] = active ? vf.f[cz[f]][g] : B(0);
+        }
+    }
+    double res = 0.0;
+    bool bad = false;
+    for (int k = k0; k < kend; ++k) {
+        const int buf = (k - k0) & 1;
+        const long long g = col + sz * k;
+        if (VIS) {
+            if (k + 1 < kend) issue(k + 1, buf ^ 1);
+            cp_async_commit();
+            long long g6 = col + sz * pmod(k + 3, nz);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) qz[f][6] = active ? vf.f[cz[f]][g6] : B(0);
+        }
+        // pointwise operands, loaded before the wait so their latency overlaps
+        B R[5];
+        double ui[5], u_n[5];
+        if (active) {
+#pragma unroll
+            for (int e = 0; e < 5; ++e) {
+                R[e] = r.f[e][g];
+                if (stage >= 0) ui[e] = uin.q[e][g];
+                if (stage >= 1) u_n[e] = un.q[e][g];
+            }
+        }
+        if (VIS) {
+            cp_async_wait1();
+            __syncthreads();
+        }
+        if (active) {
+            if (VIS) {
+#pragma unroll
+                for (int f = 0; f < 4; ++f) {
+                    const int c = tx + 3, rr = ty + 3;
+                    const B *X = sX[buf][f][ty];
+                    B dfx = cd6<B>(X[c - 3], X[c - 2], X[c - 1], X[c + 1], X[c + 2], X[c + 3], ixb);
+                    B dfy = cd6<B>(sY[buf][f][rr - 3][tx], sY[buf][f][rr - 2][tx],
+                                   sY[buf][f][rr - 1][tx], sY[buf][f][rr + 1][tx],
+                                   sY[buf][f][rr + 2][tx], sY[buf][f][rr + 3][tx], iyb);
+                    B dfz = cd6<B>(qz[f][0], qz[f][1], qz[f][2], qz[f][4], qz[f][5], qz[f][6], izb);
+                    B t = R[1 + f];
+                    t -= dfx;
+                    t -= dfy;
+                    t -= dfz;
+                    R[1 + f] = t;
+                }
+            }
+            if (stage < 0) {
+#pragma unroll
+                for (int e = 0; e < 5; ++e) uout.q[e][g] = double(R[e]);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 5; ++e) {
+                    double rhs = -double(R[e]);
+                    double out;
+                    if (stage == 0) {
+                        out = 1.0 * ui[e] + 1.0 * rhs * dt;
+                    } else if (stage == 1) {
+                        out = 0.75 * u_n[e] + 0.25 * (rhs * dt + ui[e]);
+                    } else {
+                        out = (1.0 / 3.0) * u_n[e] + (2.0 / 3.0) * (rhs * dt + ui[e]);
+                        double dd = out - u_n[e];
+                        res += dd * dd;
+                    }
+                    bad |= !isfinite(out);
+                    uout.q[e][g] = out;
+                }
+            }
+        }
+        if (VIS) {
+            __syncthreads();
+#pragma unroll
+            for (int s = 0; s < 6; ++s)
+#pragma unroll
+                for (int f = 0; f < 4; ++f) qz[f][s] = qz[f][s + 1];
+        }
+    }
+    if (bad) atomicOr(flags, 1u);
+    if (stage != 2) return;
+    for (int o = 16; o > 0; o >>= 1) res += __shfl_xor_sync(0xffffffffu, res, o);
+    if ((tid & 31) == 0) red[tid >> 5] = res;
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < TX * TY / 32; ++w) res += red[w];
+        atomicAdd(res_acc, res);
+    }
+}
+
+static dim3 grid25(const BoxParams &bp) {
+    return dim3((bp.n[0] + TX - 1) / TX, (bp.n[1] + TY - 1) / TY, (bp.n[2] + KZ - 1) / KZ);
+}
+
+template <typename B>
+cudaError_t launch_visc_flux(const BoxParams &bp, PrimView w, BView9<B> vf, int, cudaStream_t st) {
+    k_visc_flux25<B><<<grid25(bp), dim3(TX, TY), 0, st>>>(bp, w, vf);
+    return cudaGetLastError();
+}
+
+template <typename B>
+cudaError_t launch_update(const BoxParams &bp, BView<B> r, BView9<B> vf, StateView un,
+                          StateView uin, StateViewMut uout, int stage, const StepScalars *sc,
+                          double *res_acc, unsigned *flags, int, cudaStream_t st) {
+    if (bp.navier_stokes)
+        k_update25<B, true><<<grid25(bp), dim3(TX, TY), 0, st>>>(bp, r, vf, un, uin, uout, stage,
+                                                                 sc, res_acc, flags);
+    else
+        k_update25<B, false><<<grid25(bp), dim3(TX, TY), 0, st>>>(bp, r, vf, un, uin, uout, stage,
+                                                                  sc, res_acc, flags);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_visc_flux<double>(const BoxParams &, PrimView, BView9<double>, int,
+                                              cudaStream_t);
+template cudaError_t launch_visc_flux<float>(const BoxParams &, PrimView, BView9<float>, int,
+                                             cudaStream_t);
+template cudaError_t launch_update<double>(const BoxParams &, BView<double>, BView9<double>,
+                                           StateView, StateView, StateViewMut, int,
+                                           const StepScalars *, double *, unsigned *, int,
+                                           cudaStream_t);
+template cudaError_t launch_update<float>(const BoxParams &, BView<float>, BView9<float>,
+                                          StateView, StateView, StateViewMut, int,
+                                          const StepScalars *, double *, unsigned *, int,
+                                          cudaStream_t);
+
+}  // namespace nuc3d
