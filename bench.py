@@ -238,6 +238,7 @@ def run_b200(args, rank, world, local_rank):
     ms_per_step = ms_max / args.steps
     value = world * cells / (ms_per_step * 1e-3)
 
+    tuning64 = s64.tuning()
     # ---- per-kernel event timing (separate short pass, same workload)
     s64.profile(True)
     s64.step(2, CFL, stats=False)
@@ -261,6 +262,7 @@ def run_b200(args, rank, world, local_rank):
         "avg_launch_ms": inv_avg_ms,
         "share_of_step": inv_ms / total_ms if total_ms else None,
         "kernel_ms_per_step": {k: v[0] / 2 for k, v in prof.items()},
+        "autotuned_run_length": tuning64,
         "step_fp64_tflops": FLOPS_PER_CELL_STAGE * 3 * cells / (ms_per_step * 1e-3) / 1e12,
         "hbm_state_frac": STATE_BYTES_PER_CELL_UPDATE * cells / (ms_per_step * 1e-3) / 1e9
                           / 6550.7,
@@ -297,6 +299,11 @@ def run_b200(args, rank, world, local_rank):
         sm.step(args.warmup, CFL, stats=False)
         sm.sync()
         ms_m = max_over_ranks(timed_steps(sm, args.steps))
+        tuning32 = sm.tuning()
+        sm.profile(True)
+        sm.step(2, CFL, stats=False)
+        prof_m = sm.profile_read(reset=True)
+        sm.profile(False)
         sm.close()
         # accuracy: 100 steps from the same state, both precisions
         nacc = args.accuracy_steps
@@ -322,7 +329,12 @@ def run_b200(args, rank, world, local_rank):
             "tke_rel_diff": abs(ke[0] - ke[1]) / ke[1],
             "accuracy_steps": nacc,
             "peak_fp32_tflops": peak32,
+            "kernel_ms_per_step": {k: v[0] / 2 for k, v in prof_m.items()},
+            "autotuned_run_length": tuning32,
         }
+
+    ensemble = None if args.skip_ensemble else run_ensemble(args, stream, barrier, max_over_ranks,
+                                                            world, rank)
 
     if rank != 0:
         if dist is not None:
@@ -354,11 +366,67 @@ def run_b200(args, rank, world, local_rank):
         "roofline": roofline,
         "clocks": clock_info,
         "mixed": mixed,
+        "ensemble": ensemble,
         "cpu_baseline": cpu,
     }
     if dist is not None:
         dist.destroy_process_group()
     return line
+
+
+# ------------------------------------------------------------ ensemble -----
+def ensemble_boxes(nboxes, seed0):
+    """The batched-ensemble workload: box edges drawn from {32,48,64,96,128},
+    turbulent Mach U[0.1,0.5], Re_lambda U[40,120], WENO5-JS or WENO5-Z per
+    box, seeded ICs (box b uses seed seed0 + b)."""
+    import numpy as np
+    import nuc3d_b200 as nb
+    rng = np.random.default_rng(2024 + seed0)
+    out = []
+    for b in range(nboxes):
+        n = int(rng.choice([32, 48, 64, 96, 128]))
+        mt = float(rng.uniform(0.1, 0.5))
+        rl = float(rng.uniform(40.0, 120.0))
+        scheme = nb.WENO5JS if rng.uniform() < 0.5 else nb.WENO5Z
+        d = nb.BoxDesc(n, n, n, mach=1.0, scheme=(scheme,) * 3)
+        q, re = nb.hit_field(d, seed=seed0 + b, k_peak=K_PEAK, mach_t=mt, re_lambda=rl)
+        d.reynolds = re
+        out.append((d, q))
+    return out
+
+
+def run_ensemble(args, stream, barrier, max_over_ranks, world, rank):
+    import torch
+    import nuc3d_b200 as nb
+    boxes = ensemble_boxes(args.ensemble_boxes, 64 * rank)
+    cells = sum(d.cells for d, _ in boxes)
+    res = {"boxes_per_gpu": len(boxes), "cells_per_gpu": cells,
+           "edges": sorted({d.nx for d, _ in boxes}),
+           "workload": "batched ensemble: 64 periodic HIT boxes, edges {32,48,64,96,128}, "
+                       "Mt U[0.1,0.5], Re_lambda U[40,120], WENO5-JS/Z per box, one launch per "
+                       "kernel class for all boxes, step replayed as a CUDA graph"}
+    for name, prec in (("mixed", nb.MIXED), ("fp64", nb.FP64)):
+        with nb.Batch(prec, stream=stream) as B:
+            ids = [B.add(d) for d, _ in boxes]
+            for i, (_, q) in zip(ids, boxes):
+                B.set_state(i, q)
+            B.step(args.warmup)
+            B.sync()
+            barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            l0 = B.launch_count()
+            e0.record(stream)
+            B.step(args.steps)
+            e1.record(stream)
+            barrier()
+            ms = max_over_ranks(e0.elapsed_time(e1))
+            B.sync()
+            res[name] = {"value": world * cells * args.steps / (ms * 1e-3), "unit": UNIT,
+                         "ms_per_step": ms / args.steps,
+                         "launches_per_step": (B.launch_count() - l0) / args.steps}
+    res["mixed_speedup_vs_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    return res
 
 
 # ------------------------------------------------------- reference arm -----
@@ -392,10 +460,12 @@ def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--n", type=int, default=NX, help="box edge (default 256; smaller only for profiling)")
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--skip-mixed", action="store_true")
+    ap.add_argument("--skip-ensemble", action="store_true")
+    ap.add_argument("--ensemble-boxes", type=int, default=64)
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--cpu-n", type=int, default=48, help="box edge of the CPU sample")
     ap.add_argument("--cpu-steps", type=int, default=2)

@@ -142,10 +142,57 @@ NUC3D_API int nuc3d_profile_read(nuc3d_ctx *ctx, double *ms, long long *launches
 /* Kernels this context has launched since creation (all classes). */
 NUC3D_API long long nuc3d_launch_count(const nuc3d_ctx *ctx);
 
+/* ---- batches: many periodic boxes advanced together ----------------------
+ * A batch holds boxes of any sizes, parameters and schemes (one precision
+ * per batch) resident on the current device.  nuc3d_batch_step advances every
+ * active box by nsteps TVD-RK3 steps, each box with its own dt (its own CFL
+ * and eigenvalues), with one kernel launch per kernel class for all boxes; the
+ * step is captured once as a CUDA graph and replayed.  Boxes may be added,
+ * removed or (de)activated between steps (the next step rebuilds the work
+ * lists and re-captures).  A box advanced in a batch gives the same result as
+ * the same box advanced alone: no arithmetic crosses boxes.  This is the
+ * batched form of the single-box solver; the reference runs one box per
+ * process (singleBlock.cpp:50-71). */
+typedef struct nuc3d_batch nuc3d_batch;
+NUC3D_API int nuc3d_batch_create(int precision, void *stream, nuc3d_batch **out);
+NUC3D_API int nuc3d_batch_destroy(nuc3d_batch *b);
+/* Allocates the box's device memory (stream-ordered) and returns its id.
+ * desc->precision must equal the batch's. */
+NUC3D_API int nuc3d_batch_add(nuc3d_batch *b, const nuc3d_box_desc *desc, int *box_id);
+NUC3D_API int nuc3d_batch_remove(nuc3d_batch *b, int box_id);
+NUC3D_API int nuc3d_batch_set_active(nuc3d_batch *b, int box_id, int active);
+NUC3D_API int nuc3d_batch_set_cfl(nuc3d_batch *b, int box_id, double cfl);
+NUC3D_API int nuc3d_batch_set_state_host(nuc3d_batch *b, int box_id, const double *const h_q[5]);
+NUC3D_API int nuc3d_batch_get_state_host(nuc3d_batch *b, int box_id, double *const h_q[5]);
+NUC3D_API int nuc3d_batch_set_state_device(nuc3d_batch *b, int box_id,
+                                           const double *const d_q[5]);
+NUC3D_API int nuc3d_batch_get_state_device(nuc3d_batch *b, int box_id, double *const d_q[5]);
+NUC3D_API int nuc3d_batch_step(nuc3d_batch *b, int nsteps);
+/* dt and residual of the box's last n steps (n <= 1024; host arrays). */
+NUC3D_API int nuc3d_batch_history(nuc3d_batch *b, int box_id, int n, double *h_dt,
+                                  double *h_res);
+NUC3D_API int nuc3d_batch_sync(nuc3d_batch *b);
+NUC3D_API long long nuc3d_batch_box_steps(const nuc3d_batch *b, int box_id);
+NUC3D_API double nuc3d_batch_time(nuc3d_batch *b, int box_id);
+NUC3D_API int nuc3d_batch_profile_enable(nuc3d_batch *b, int on);
+NUC3D_API int nuc3d_batch_profile_read(nuc3d_batch *b, double *ms, long long *launches,
+                                       int reset);
+NUC3D_API long long nuc3d_batch_launch_count(const nuc3d_batch *b);
+
 /* Measured FMA-pipe throughput of the current device in TFLOP/s (FP64 for
  * NUC3D_FP64, FP32 for NUC3D_MIXED): the roofline denominator of these
  * stencil kernels.  Runs a ~10 ms probe kernel on the legacy stream. */
 NUC3D_API int nuc3d_probe_peak(int precision, double *tflops);
+
+/* Autotuner result.  The directional WENO sweep has variants that give each
+ * thread a run of 1, 2 or 4 consecutive faces; the first step after the set of
+ * (scheme, direction) pairs changes times every variant on the live boxes and
+ * keeps the fastest.  run_len[s*3+d] (s: 0 WENO5-JS, 1 WENO5-Z; d: x, y, z)
+ * receives the chosen run length (0 = not tuned), ms[(s*3+d)*3+v] the measured
+ * milliseconds per launch of variant v (run length 1, 2, 4).  Either pointer
+ * may be NULL. */
+NUC3D_API int nuc3d_tuning(const nuc3d_ctx *ctx, int *run_len, double *ms);
+NUC3D_API int nuc3d_batch_tuning(const nuc3d_batch *b, int *run_len, double *ms);
 
 /* Simulated time advanced by this context so far (block.cpp:208-209). */
 NUC3D_API double nuc3d_ctx_time(const nuc3d_ctx *ctx);

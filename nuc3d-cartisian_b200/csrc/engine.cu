@@ -1,0 +1,635 @@
+// Engine: host side of the batched solver (see engine.h).
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+#include "op_kernels.h"
+
+namespace nuc3d {
+
+namespace {
+
+long long pad32(long long n) { return (n + 31) / 32 * 32; }
+size_t bulk_size(int precision) { return precision == NUC3D_MIXED ? sizeof(float) : sizeof(double); }
+constexpr size_t kSmallBytes = 256 + sizeof(StepScalars);
+
+bool has_crweno(const nuc3d_box_desc &d) {
+    return d.scheme[0] == NUC3D_CRWENO5 || d.scheme[1] == NUC3D_CRWENO5 ||
+           d.scheme[2] == NUC3D_CRWENO5;
+}
+
+BoxParams make_params(const nuc3d_box_desc &d) {
+    BoxParams bp{};
+    bp.n[0] = d.nx;
+    bp.n[1] = d.ny;
+    bp.n[2] = d.nz;
+    bp.N = (long long)d.nx * d.ny * d.nz;
+    bp.stride[0] = 1;
+    bp.stride[1] = d.nx;
+    bp.stride[2] = (long long)d.nx * d.ny;
+    bp.d[0] = d.lx / d.nx;  // block.cpp:62-64
+    bp.d[1] = d.ly / d.ny;
+    bp.d[2] = d.lz / d.nz;
+    for (int i = 0; i < 3; ++i) bp.inv_d[i] = 1.0 / bp.d[i];
+    bp.gamma = d.gamma;
+    bp.mach = d.mach;
+    bp.reynolds = d.reynolds;
+    bp.prandtl = d.prandtl;
+    bp.tref_nd = d.t_ref / d.t_inf;
+    bp.powerlaw_exp = d.powerlaw_exp;
+    bp.cfl = 0.5;
+    bp.visc_model = d.visc_model;
+    bp.navier_stokes = d.pde_model == NUC3D_NAVIERSTOKES3D;
+    bp.quirks = d.quirks;
+    for (int i = 0; i < 3; ++i) bp.scheme[i] = d.scheme[i];
+    return bp;
+}
+
+int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+}  // namespace
+
+#define ECK(call)                                                         \
+    do {                                                                  \
+        cudaError_t e_ = (call);                                          \
+        if (e_ != cudaSuccess) {                                          \
+            set_last_error(NUC3D_ERR_CUDA, (std::string(#call) + ": " +   \
+                                            cudaGetErrorString(e_)).c_str()); \
+            return NUC3D_ERR_CUDA;                                        \
+        }                                                                 \
+    } while (0)
+
+int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
+    auto bad = [&](int code, const char *m) {
+        if (why) *why = m;
+        return code;
+    };
+    const int n[3] = {d.nx, d.ny, d.nz};
+    for (int i = 0; i < 3; ++i) {
+        if (n[i] < 8) return bad(NUC3D_ERR_INVALID, "every box extent must be >= 8 cells");
+        if (d.scheme[i] < NUC3D_WENO5JS || d.scheme[i] > NUC3D_CRWENO5)
+            return bad(NUC3D_ERR_UNSUPPORTED, "unknown reconstruction scheme");
+    }
+    if ((long long)d.nx * d.ny * d.nz > (1LL << 31)) return bad(NUC3D_ERR_INVALID, "box larger than 2^31 cells");
+    if (!(d.lx > 0 && d.ly > 0 && d.lz > 0)) return bad(NUC3D_ERR_INVALID, "box lengths must be > 0");
+    if (d.pde_model != NUC3D_EULER3D && d.pde_model != NUC3D_NAVIERSTOKES3D)
+        return bad(NUC3D_ERR_UNSUPPORTED, "unknown PDE model");
+    if (d.visc_model < NUC3D_VISC_SUTHERLAND || d.visc_model > NUC3D_VISC_POWERLAW)
+        return bad(NUC3D_ERR_UNSUPPORTED, "unknown viscosity model");
+    if (d.precision != NUC3D_FP64 && d.precision != NUC3D_MIXED)
+        return bad(NUC3D_ERR_UNSUPPORTED, "unknown precision");
+    if (!(d.gamma > 1.0) || !(d.mach > 0.0) || !(d.reynolds > 0.0) || !(d.prandtl > 0.0))
+        return bad(NUC3D_ERR_INVALID, "gamma must be > 1 and Mach, Re, Pr > 0");
+    return NUC3D_OK;
+}
+
+long long Engine::box_bytes(const nuc3d_box_desc &d) {
+    if (validate(d, nullptr) != NUC3D_OK) return -1;
+    BoxParams bp = make_params(d);
+    long long np = pad32(bp.N);
+    long long bs = (long long)bulk_size(d.precision);
+    long long b = 21 * np * 8 + 14 * np * bs + (long long)kSmallBytes;
+    if (has_crweno(d)) b += (long long)crweno_scratch_elems(bp) * bs;
+    return b;
+}
+
+Engine::Engine(int precision, cudaStream_t stream) : precision_(precision), stream_(stream) {}
+
+Engine::~Engine() {
+    cudaStreamSynchronize(stream_);
+    invalidate_graph();
+    for (auto &b : boxes_) {
+        if (b.mem) cudaFreeAsync(b.mem, stream_);
+        if (b.scratch) cudaFreeAsync(b.scratch, stream_);
+    }
+    if (d_boxes_) cudaFreeAsync(d_boxes_, stream_);
+    if (d_items_) cudaFreeAsync(d_items_, stream_);
+    if (d_rhs_ptrs_) cudaFreeAsync(d_rhs_ptrs_, stream_);
+    cudaStreamSynchronize(stream_);
+    for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
+    if (cap_stream_) cudaStreamDestroy(cap_stream_);
+}
+
+void Engine::invalidate_graph() {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    exec_ = nullptr;
+    graph_ = nullptr;
+}
+
+int Engine::add_box(const nuc3d_box_desc &d, int *id) {
+    std::string why;
+    int rc = validate(d, &why);
+    if (rc) return set_last_error(rc, why.c_str());
+    if (d.precision != precision_)
+        return set_last_error(NUC3D_ERR_INVALID, "box precision differs from the batch's");
+    EngineBox b;
+    b.desc = d;
+    b.dev.p = make_params(d);
+    const long long np = pad32(b.dev.p.N);
+    const size_t bs = bulk_size(precision_);
+    const size_t bytes = sizeof(double) * 21 * (size_t)np + bs * 14 * (size_t)np + kSmallBytes;
+    cudaError_t e = cudaMallocAsync(&b.mem, bytes, stream_);
+    if (e == cudaSuccess && has_crweno(d))
+        e = cudaMallocAsync(&b.scratch, bs * crweno_scratch_elems(b.dev.p), stream_);
+    if (e != cudaSuccess) {
+        if (b.mem) cudaFreeAsync(b.mem, stream_);
+        cudaGetLastError();
+        return set_last_error(NUC3D_ERR_NOMEM,
+                              (std::string("device allocation failed: ") + cudaGetErrorString(e)).c_str());
+    }
+    double *dp = static_cast<double *>(b.mem);
+    b.dev.base = dp;
+    b.dev.np = np;
+    char *bk = reinterpret_cast<char *>(dp + 21 * (size_t)np);
+    char *sm = bk + bs * 14 * (size_t)np;
+    b.dev.eig = reinterpret_cast<double *>(sm);
+    b.dev.res_acc = reinterpret_cast<double *>(sm + 64);
+    b.dev.flags = reinterpret_cast<unsigned *>(sm + 128);
+    b.dev.sc = reinterpret_cast<StepScalars *>(sm + 256);
+    b.dev.active = 1;
+    b.live = true;
+    ECK(cudaMemsetAsync(b.mem, 0, bytes, stream_));
+    // sc->cfl = 0.5 (the stream-ordered memset above runs first)
+    static const double half = 0.5;
+    ECK(cudaMemcpyAsync(&b.dev.sc->cfl, &half, sizeof half, cudaMemcpyHostToDevice, stream_));
+    int slot = -1;
+    for (size_t i = 0; i < boxes_.size(); ++i)
+        if (!boxes_[i].live) {
+            slot = (int)i;
+            break;
+        }
+    if (slot < 0) {
+        slot = (int)boxes_.size();
+        boxes_.push_back(b);
+    } else {
+        boxes_[slot] = b;
+    }
+    *id = slot;
+    dirty_ = true;
+    return NUC3D_OK;
+}
+
+int Engine::remove_box(int id) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
+        return set_last_error(NUC3D_ERR_INVALID, "no such box");
+    EngineBox &b = boxes_[id];
+    ECK(cudaFreeAsync(b.mem, stream_));
+    if (b.scratch) ECK(cudaFreeAsync(b.scratch, stream_));
+    b = EngineBox();
+    dirty_ = true;
+    return NUC3D_OK;
+}
+
+int Engine::set_active(int id, bool on) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
+        return set_last_error(NUC3D_ERR_INVALID, "no such box");
+    if ((boxes_[id].dev.active != 0) != on) {
+        boxes_[id].dev.active = on ? 1 : 0;
+        dirty_ = true;
+    }
+    return NUC3D_OK;
+}
+
+int Engine::set_cfl(int id, double cfl) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
+        return set_last_error(NUC3D_ERR_INVALID, "no such box");
+    if (!(cfl > 0.0)) return set_last_error(NUC3D_ERR_INVALID, "cfl must be > 0");
+    EngineBox &b = boxes_[id];
+    if (b.cfl != cfl) {
+        b.cfl = cfl;
+        ECK(cudaMemcpyAsync(&b.dev.sc->cfl, &b.cfl, sizeof(double), cudaMemcpyHostToDevice, stream_));
+        ECK(cudaStreamSynchronize(stream_));  // b.cfl is the pageable source
+    }
+    return NUC3D_OK;
+}
+
+int Engine::set_state(int id, const double *const q[5], cudaMemcpyKind kind, bool sync) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
+        return set_last_error(NUC3D_ERR_INVALID, "no such box");
+    if (!q) return set_last_error(NUC3D_ERR_INVALID, "null argument");
+    EngineBox &b = boxes_[id];
+    size_t bytes = sizeof(double) * (size_t)b.dev.p.N;
+    for (int e = 0; e < 5; ++e) {
+        if (!q[e]) return set_last_error(NUC3D_ERR_INVALID, "null field pointer");
+        ECK(cudaMemcpyAsync(fieldU(b.dev, 0, e), q[e], bytes, kind, stream_));
+    }
+    if (sync) ECK(cudaStreamSynchronize(stream_));
+    return NUC3D_OK;
+}
+
+int Engine::get_state(int id, double *const q[5], cudaMemcpyKind kind, bool sync) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
+        return set_last_error(NUC3D_ERR_INVALID, "no such box");
+    if (!q) return set_last_error(NUC3D_ERR_INVALID, "null argument");
+    EngineBox &b = boxes_[id];
+    size_t bytes = sizeof(double) * (size_t)b.dev.p.N;
+    for (int e = 0; e < 5; ++e) {
+        if (!q[e]) return set_last_error(NUC3D_ERR_INVALID, "null field pointer");
+        ECK(cudaMemcpyAsync(q[e], fieldU(b.dev, 0, e), bytes, kind, stream_));
+    }
+    if (sync) ECK(cudaStreamSynchronize(stream_));
+    return NUC3D_OK;
+}
+
+int Engine::rebuild() {
+    invalidate_graph();
+    ECK(cudaStreamSynchronize(stream_));
+    const bool mixed = precision_ == NUC3D_MIXED;
+    std::vector<BoxDev> table(boxes_.size());
+    std::vector<WorkItem> prim, st25, inv[2][3];
+    crweno_boxes_.clear();
+    any_visc_ = false;
+    nactive_ = 0;
+    for (size_t i = 0; i < boxes_.size(); ++i) {
+        const EngineBox &b = boxes_[i];
+        table[i] = b.dev;
+        if (!b.live) table[i].active = 0;
+        if (!b.live || !b.dev.active) continue;
+        ++nactive_;
+        const BoxParams &p = b.dev.p;
+        const int id = (int)i;
+        any_visc_ = any_visc_ || p.navier_stokes;
+        for (long long c = 0; c * kPrimChunk < p.N; ++c)
+            prim.push_back({id, (int)c, (int)std::min<long long>(kPrimChunk, p.N - c * kPrimChunk), 0});
+        for (int z = 0; z < ceil_div(p.n[2], kT25Z); ++z)
+            for (int y = 0; y < ceil_div(p.n[1], kT25Y); ++y)
+                for (int x = 0; x < ceil_div(p.n[0], kT25X); ++x) st25.push_back({id, x, y, z});
+        bool cr = false;
+        for (int d = 0; d < 3; ++d) {
+            int s = p.scheme[d];
+            if (s == SCHEME_CR) {
+                cr = true;
+                continue;
+            }
+            InvTileDims t = inviscid_tile(d, mixed);
+            auto &L = inv[s][d];
+            if (d == 0) {
+                for (int k = 0; k < p.n[2]; ++k)
+                    for (int b2 = 0; b2 < ceil_div(p.n[1], t.TL); ++b2)
+                        for (int a = 0; a < ceil_div(p.n[0], t.TC); ++a) L.push_back({id, a, b2, k});
+            } else if (d == 1) {
+                for (int k = 0; k < p.n[2]; ++k)
+                    for (int b2 = 0; b2 < ceil_div(p.n[1], t.TC); ++b2)
+                        for (int a = 0; a < ceil_div(p.n[0], t.TL); ++a) L.push_back({id, a, b2, k});
+            } else {
+                for (int c = 0; c < ceil_div(p.n[2], t.TC); ++c)
+                    for (int j = 0; j < p.n[1]; ++j)
+                        for (int a = 0; a < ceil_div(p.n[0], t.TL); ++a) L.push_back({id, a, j, c});
+            }
+        }
+        if (cr) crweno_boxes_.push_back(id);
+    }
+    std::vector<WorkItem> all;
+    auto append = [&](const std::vector<WorkItem> &v, Range &r) {
+        r.off = all.size();
+        r.n = (int)v.size();
+        all.insert(all.end(), v.begin(), v.end());
+    };
+    append(prim, r_prim_);
+    append(st25, r_25d_);
+    for (int s = 0; s < 2; ++s)
+        for (int d = 0; d < 3; ++d) append(inv[s][d], r_inv_[s][d]);
+    if ((int)boxes_.size() > d_boxes_cap_) {
+        if (d_boxes_) ECK(cudaFreeAsync(d_boxes_, stream_));
+        if (d_rhs_ptrs_) ECK(cudaFreeAsync(d_rhs_ptrs_, stream_));
+        d_boxes_cap_ = std::max<int>(8, (int)boxes_.size() * 2);
+        ECK(cudaMallocAsync(&d_boxes_, sizeof(BoxDev) * d_boxes_cap_, stream_));
+        ECK(cudaMallocAsync(&d_rhs_ptrs_, sizeof(double *) * 5 * d_boxes_cap_, stream_));
+    }
+    if (all.size() > d_items_cap_) {
+        if (d_items_) ECK(cudaFreeAsync(d_items_, stream_));
+        d_items_cap_ = std::max<size_t>(1024, all.size() * 5 / 4);
+        ECK(cudaMallocAsync(&d_items_, sizeof(WorkItem) * d_items_cap_, stream_));
+    }
+    if (!table.empty())
+        ECK(cudaMemcpyAsync(d_boxes_, table.data(), sizeof(BoxDev) * table.size(),
+                            cudaMemcpyHostToDevice, stream_));
+    if (!all.empty())
+        ECK(cudaMemcpyAsync(d_items_, all.data(), sizeof(WorkItem) * all.size(),
+                            cudaMemcpyHostToDevice, stream_));
+    ECK(cudaStreamSynchronize(stream_));  // host vectors go out of scope
+    ECK(prepare_inviscid_kernels(mixed));
+    int per_stage = (r_prim_.n > 0) + (any_visc_ && r_25d_.n > 0) + (r_25d_.n > 0);
+    for (int s = 0; s < 2; ++s)
+        for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d].n > 0;
+    launches_per_step_ = 3 * per_stage + 3;  // + clear_eig, dt, residual (crweno counted live)
+    dirty_ = false;
+    return NUC3D_OK;
+}
+
+// Kernel-class timing while profiling (eager launches only).
+struct ProfScope {
+    Engine *e;
+    int cls;
+    cudaEvent_t a = nullptr;
+    cudaEvent_t get() {
+        if (e->ev_next_ == e->ev_pool_.size()) {
+            cudaEvent_t ev;
+            if (cudaEventCreate(&ev) != cudaSuccess) return nullptr;
+            e->ev_pool_.push_back(ev);
+        }
+        return e->ev_pool_[e->ev_next_++];
+    }
+    ProfScope(Engine *e_, int cls_) : e(e_), cls(cls_) {
+        if (e->prof_on && (a = get())) cudaEventRecord(a, e->stream_);
+    }
+    ~ProfScope() {
+        if (!a) return;
+        cudaEvent_t b = get();
+        if (!b) return;
+        cudaEventRecord(b, e->stream_);
+        e->pending_.push_back({cls, a, b});
+    }
+};
+
+int Engine::profile_flush() {
+    if (pending_.empty()) return NUC3D_OK;
+    ECK(cudaStreamSynchronize(stream_));
+    for (auto &m : pending_) {
+        float ms = 0.f;
+        ECK(cudaEventElapsedTime(&ms, m.a, m.b));
+        prof_ms[m.cls] += ms;
+        prof_n[m.cls] += 1;
+    }
+    pending_.clear();
+    ev_next_ = 0;
+    return NUC3D_OK;
+}
+
+template <typename B>
+int Engine::enqueue_step_t(cudaStream_t st) {
+    const int nb = (int)boxes_.size();
+    const WorkItem *it = d_items_;
+    {
+        ProfScope ps(this, NUC3D_PROF_DT);
+        ECK(launch_clear_eig(d_boxes_, nb, st));
+    }
+    for (int stage = 0; stage < 3; ++stage) {
+        const int in = stage, out = (stage + 1) % 3;
+        {
+            ProfScope ps(this, NUC3D_PROF_PRIM);
+            ECK(launch_prim(d_boxes_, it + r_prim_.off, r_prim_.n, in, stage == 0, st));
+        }
+        if (stage == 0) {
+            ProfScope ps(this, NUC3D_PROF_DT);
+            ECK(launch_dt(d_boxes_, nb, st));
+        }
+        if (any_visc_) {
+            ProfScope ps(this, NUC3D_PROF_VISC);
+            ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_.off, r_25d_.n, st)));
+        }
+        for (int d = 0; d < 3; ++d) {
+            ProfScope ps(this, NUC3D_PROF_INV_X + d);
+            for (int s = 0; s < 2; ++s)
+                ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
+                                        r_inv_[s][d].n, in, d > 0, st)));
+            for (int id : crweno_boxes_) {
+                const EngineBox &b = boxes_[id];
+                if (b.dev.p.scheme[d] != SCHEME_CR) continue;
+                StateView q;
+                PrimView w;
+                BView<B> r;
+                for (int e = 0; e < 5; ++e) q.q[e] = fieldU(b.dev, in, e);
+                for (int i = 0; i < 6; ++i) w.w[i] = fieldW(b.dev, i);
+                for (int e = 0; e < 5; ++e) r.f[e] = fieldR<B>(b.dev, e);
+                int nl = 0;
+                ECK((launch_crweno<B>(b.dev.p, d, q, w, r, d > 0, static_cast<B *>(b.scratch),
+                                      st, &nl)));
+                launches += nl;
+            }
+        }
+        {
+            ProfScope ps(this, NUC3D_PROF_UPDATE);
+            StageArgs sa{stage, in, out, nullptr};
+            ECK((launch_update<B>(d_boxes_, it + r_25d_.off, r_25d_.n, sa, any_visc_, st)));
+        }
+    }
+    {
+        ProfScope ps(this, NUC3D_PROF_RESIDUAL);
+        ECK(launch_residual(d_boxes_, nb, st));
+    }
+    return NUC3D_OK;
+}
+
+int Engine::enqueue_step(cudaStream_t s) {
+    return precision_ == NUC3D_MIXED ? enqueue_step_t<float>(s) : enqueue_step_t<double>(s);
+}
+
+// Picks the run length of the directional sweep per scheme and direction by
+// timing every variant on this batch's own work lists (the first step after a
+// rebuild that brings a new (scheme, direction) pair).  The sweeps only write
+// the RHS accumulator, which every stage recomputes, so timing them on the
+// live state changes nothing.
+int Engine::autotune() {
+    bool need = false;
+    for (int s = 0; s < 2; ++s)
+        for (int d = 0; d < 3; ++d) need = need || (r_inv_[s][d].n > 0 && inv_variant[s][d] < 0);
+    if (!need) return NUC3D_OK;
+    // NUC3D_SWEEP_RUN=1|2|4 pins the run length (reproducibility studies)
+    if (const char *pin = std::getenv("NUC3D_SWEEP_RUN")) {
+        int v = std::atoi(pin) == 1 ? 0 : (std::atoi(pin) == 2 ? 1 : 2);
+        for (int s = 0; s < 2; ++s)
+            for (int d = 0; d < 3; ++d)
+                if (r_inv_[s][d].n > 0 && inv_variant[s][d] < 0) inv_variant[s][d] = v;
+        invalidate_graph();
+        return NUC3D_OK;
+    }
+    ECK(launch_prim(d_boxes_, d_items_ + r_prim_.off, r_prim_.n, 0, 0, stream_));
+    cudaEvent_t e0, e1;
+    ECK(cudaEventCreate(&e0));
+    ECK(cudaEventCreate(&e1));
+    const bool mixed = precision_ == NUC3D_MIXED;
+    int rc = NUC3D_OK;
+    for (int s = 0; s < 2 && rc == NUC3D_OK; ++s)
+        for (int d = 0; d < 3 && rc == NUC3D_OK; ++d) {
+            const Range &rg = r_inv_[s][d];
+            if (rg.n <= 0 || inv_variant[s][d] >= 0) continue;
+            int best = 0;
+            for (int v = 0; v < kInvVariants; ++v) {
+                auto go = [&]() {
+                    return mixed ? launch_inviscid<float>(s, d, v, d_boxes_, d_items_ + rg.off, rg.n,
+                                                          0, d > 0, stream_)
+                                 : launch_inviscid<double>(s, d, v, d_boxes_, d_items_ + rg.off,
+                                                           rg.n, 0, d > 0, stream_);
+                };
+                cudaError_t err = go();  // warm-up
+                err = err == cudaSuccess ? cudaEventRecord(e0, stream_) : err;
+                for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) err = go();
+                err = err == cudaSuccess ? cudaEventRecord(e1, stream_) : err;
+                err = err == cudaSuccess ? cudaEventSynchronize(e1) : err;
+                float ms = 0.f;
+                err = err == cudaSuccess ? cudaEventElapsedTime(&ms, e0, e1) : err;
+                if (err != cudaSuccess) {
+                    set_last_error(NUC3D_ERR_CUDA, cudaGetErrorString(err));
+                    rc = NUC3D_ERR_CUDA;
+                    break;
+                }
+                inv_tune_ms[s][d][v] = ms / 3.0;
+                if (inv_tune_ms[s][d][v] < inv_tune_ms[s][d][best]) best = v;
+            }
+            inv_variant[s][d] = best;
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    invalidate_graph();
+    return rc;
+}
+
+int Engine::step(int nsteps) {
+    if (nsteps < 0) return set_last_error(NUC3D_ERR_INVALID, "nsteps must be >= 0");
+    if (dirty_) {
+        int rc = rebuild();
+        if (rc) return rc;
+    }
+    if (nactive_ == 0 || nsteps == 0) return NUC3D_OK;
+    {
+        int rc = autotune();
+        if (rc) return rc;
+    }
+    if (prof_on) {
+        for (int s = 0; s < nsteps; ++s) {
+            int rc = enqueue_step(stream_);
+            if (rc) return rc;
+            launches += launches_per_step_;
+            rc = profile_flush();
+            if (rc) return rc;
+        }
+    } else {
+        if (!exec_) {
+            long long before = launches;
+            if (!cap_stream_) ECK(cudaStreamCreateWithFlags(&cap_stream_, cudaStreamNonBlocking));
+            ECK(cudaStreamBeginCapture(cap_stream_, cudaStreamCaptureModeThreadLocal));
+            int rc = enqueue_step(cap_stream_);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(cap_stream_, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            ECK(e);
+            graph_ = g;
+            ECK(cudaGraphInstantiate(&exec_, graph_, 0));
+            // crweno launches are counted while enqueuing; count them per replay
+            launches_per_step_ += (int)(launches - before);
+            launches = before;
+        }
+        for (int s = 0; s < nsteps; ++s) ECK(cudaGraphLaunch(exec_, stream_));
+        launches += (long long)nsteps * launches_per_step_;
+    }
+    for (auto &b : boxes_)
+        if (b.live && b.dev.active) b.steps += nsteps;
+    return NUC3D_OK;
+}
+
+int Engine::history(int id, int n, double *h_dt, double *h_res) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
+        return set_last_error(NUC3D_ERR_INVALID, "no such box");
+    if (n < 0 || n > kHistory) return set_last_error(NUC3D_ERR_INVALID, "history holds 1024 steps");
+    const EngineBox &b = boxes_[id];
+    if (n > b.steps) n = (int)b.steps;
+    long long first = b.steps - n;
+    int done = 0;
+    while (done < n) {
+        int ring = (int)((first + done) % kHistory);
+        int cnt = std::min(n - done, kHistory - ring);
+        if (h_dt)
+            ECK(cudaMemcpyAsync(h_dt + done, b.dev.sc->dt_hist + ring, sizeof(double) * cnt,
+                                cudaMemcpyDeviceToHost, stream_));
+        if (h_res)
+            ECK(cudaMemcpyAsync(h_res + done, b.dev.sc->res_hist + ring, sizeof(double) * cnt,
+                                cudaMemcpyDeviceToHost, stream_));
+        done += cnt;
+    }
+    ECK(cudaStreamSynchronize(stream_));
+    return NUC3D_OK;
+}
+
+template <typename B>
+int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
+    const int nb = (int)boxes_.size();
+    const WorkItem *it = d_items_;
+    double *ptrs[5];
+    for (int e = 0; e < 5; ++e) ptrs[e] = d_rhs[e];
+    ECK(cudaMemcpyAsync(d_rhs_ptrs_ + 5 * id, ptrs, sizeof ptrs, cudaMemcpyHostToDevice, stream_));
+    ECK(launch_clear_eig(d_boxes_, nb, stream_));
+    ECK(launch_prim(d_boxes_, it + r_prim_.off, r_prim_.n, 0, 1, stream_));
+    ECK(launch_dt(d_boxes_, nb, stream_));
+    if (any_visc_) ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_.off, r_25d_.n, stream_)));
+    for (int d = 0; d < 3; ++d) {
+        for (int s = 0; s < 2; ++s)
+            ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
+                                    r_inv_[s][d].n, 0, d > 0, stream_)));
+        for (int cid : crweno_boxes_) {
+            const EngineBox &b = boxes_[cid];
+            if (b.dev.p.scheme[d] != SCHEME_CR) continue;
+            StateView q;
+            PrimView w;
+            BView<B> r;
+            for (int e = 0; e < 5; ++e) q.q[e] = fieldU(b.dev, 0, e);
+            for (int i = 0; i < 6; ++i) w.w[i] = fieldW(b.dev, i);
+            for (int e = 0; e < 5; ++e) r.f[e] = fieldR<B>(b.dev, e);
+            int nl = 0;
+            ECK((launch_crweno<B>(b.dev.p, d, q, w, r, d > 0, static_cast<B *>(b.scratch), stream_,
+                                  &nl)));
+        }
+    }
+    StageArgs sa{-1, 0, 0, d_rhs_ptrs_};
+    ECK((launch_update<B>(d_boxes_, it + r_25d_.off, r_25d_.n, sa, any_visc_, stream_)));
+    ECK(cudaStreamSynchronize(stream_));  // ptrs is a host stack array
+    return NUC3D_OK;
+}
+
+int Engine::rhs(int id, double *const d_rhs[5], double *h_dt_local) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
+        return set_last_error(NUC3D_ERR_INVALID, "no such box");
+    if (!d_rhs) return set_last_error(NUC3D_ERR_INVALID, "null argument");
+    if (dirty_) {
+        int rc = rebuild();
+        if (rc) return rc;
+    }
+    if (nactive_ != 1 || !boxes_[id].dev.active)
+        return set_last_error(NUC3D_ERR_UNSUPPORTED, "rhs needs exactly this one box active");
+    {
+        int rc = autotune();
+        if (rc) return rc;
+    }
+    int rc = precision_ == NUC3D_MIXED ? enqueue_rhs_t<float>(id, d_rhs) : enqueue_rhs_t<double>(id, d_rhs);
+    if (rc) return rc;
+    if (h_dt_local) {
+        ECK(cudaMemcpyAsync(h_dt_local, &boxes_[id].dev.sc->dt_local, sizeof(double),
+                            cudaMemcpyDeviceToHost, stream_));
+        ECK(cudaStreamSynchronize(stream_));
+    }
+    return NUC3D_OK;
+}
+
+int Engine::sync_and_check(int id) {
+    ECK(cudaStreamSynchronize(stream_));
+    for (size_t i = 0; i < boxes_.size(); ++i) {
+        if (!boxes_[i].live || (id >= 0 && (int)i != id)) continue;
+        unsigned f = 0;
+        ECK(cudaMemcpy(&f, boxes_[i].dev.flags, sizeof f, cudaMemcpyDeviceToHost));
+        if (f & 1u) return set_last_error(NUC3D_ERR_NONFINITE, "state became non-finite (NaN/Inf)");
+    }
+    return NUC3D_OK;
+}
+
+double Engine::time(int id) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live) return NAN;
+    double t = 0.0;
+    if (cudaStreamSynchronize(stream_) != cudaSuccess) return NAN;
+    if (cudaMemcpy(&t, &boxes_[id].dev.sc->time, sizeof t, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return NAN;
+    return t;
+}
+
+long long Engine::box_steps(int id) const {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live) return -1;
+    return boxes_[id].steps;
+}
+
+}  // namespace nuc3d

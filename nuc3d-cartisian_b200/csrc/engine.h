@@ -1,0 +1,110 @@
+// Engine: the host side of the batched solver.  Owns the boxes' device
+// memory, the device box table, the per-kernel work-item lists and a CUDA
+// graph of one TVD-RK3 step of every active box.  Internal; nuc3d_ctx and
+// nuc3d_batch in the C ABI are thin handles over it.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "nuc3d_b200.h"
+#include "rhs_kernels.h"
+
+namespace nuc3d {
+
+struct EngineBox {
+    nuc3d_box_desc desc{};
+    BoxDev dev{};          // host copy of the box's table entry
+    void *mem = nullptr;   // one stream-ordered allocation holding all fields
+    void *scratch = nullptr;
+    double cfl = 0.5;
+    long long steps = 0;   // host mirror of the device step counter
+    bool live = false;     // slot in use
+};
+
+class Engine {
+public:
+    Engine(int precision, cudaStream_t stream);
+    ~Engine();
+
+    // Adds a box (allocates its device memory, stream-ordered); returns slot id.
+    int add_box(const nuc3d_box_desc &d, int *id);
+    int remove_box(int id);
+    int set_active(int id, bool on);
+    int set_cfl(int id, double cfl);
+    int set_state(int id, const double *const q[5], cudaMemcpyKind kind, bool sync);
+    int get_state(int id, double *const q[5], cudaMemcpyKind kind, bool sync);
+    // nsteps TVD-RK3 steps of every active box (graph replay unless profiling)
+    int step(int nsteps);
+    // dt / residual history of the last `n` steps of box id into host arrays
+    int history(int id, int n, double *h_dt, double *h_res);
+    int rhs(int id, double *const d_rhs[5], double *h_dt_local);
+    int sync_and_check(int id_or_all);
+    double time(int id);
+    long long box_steps(int id) const;
+    int nboxes() const { return (int)boxes_.size(); }
+    int precision() const { return precision_; }
+    cudaStream_t stream() const { return stream_; }
+
+    // accounting
+    long long launches = 0;
+    bool prof_on = false;
+    double prof_ms[NUC3D_PROF_CLASSES] = {};
+    long long prof_n[NUC3D_PROF_CLASSES] = {};
+    int profile_flush();
+    // autotuned run length per [scheme JS/Z][dir] (-1: not tuned yet) and the
+    // measured milliseconds per launch of each variant
+    int inv_variant[2][3] = {{-1, -1, -1}, {-1, -1, -1}};
+    double inv_tune_ms[2][3][kInvVariants] = {};
+
+    static long long box_bytes(const nuc3d_box_desc &d);
+    static int validate(const nuc3d_box_desc &d, std::string *why);
+
+private:
+    int rebuild();
+    // launches of one step into stream s (eager on stream_, or on the private
+    // capture stream while recording the graph)
+    int enqueue_step(cudaStream_t s);
+    template <typename B>
+    int enqueue_step_t(cudaStream_t s);
+    template <typename B>
+    int enqueue_rhs_t(int id, double *const d_rhs[5]);
+    void invalidate_graph();
+    int autotune();
+
+    int precision_;
+    cudaStream_t stream_;
+    std::vector<EngineBox> boxes_;
+    bool dirty_ = true;
+    bool any_visc_ = false;
+    int nactive_ = 0;
+    BoxDev *d_boxes_ = nullptr;
+    int d_boxes_cap_ = 0;
+    WorkItem *d_items_ = nullptr;
+    size_t d_items_cap_ = 0;
+    // offsets/counts into d_items_
+    struct Range {
+        size_t off = 0;
+        int n = 0;
+    };
+    Range r_prim_, r_25d_, r_inv_[2][3];  // [scheme JS/Z][dir]
+    std::vector<int> crweno_boxes_;
+    int launches_per_step_ = 0;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+    cudaStream_t cap_stream_ = nullptr;  // graphs cannot be captured on the legacy stream
+    double **d_rhs_ptrs_ = nullptr;  // 5 per box, for stage -1
+    // profiling events
+    std::vector<cudaEvent_t> ev_pool_;
+    struct Mark {
+        int cls;
+        cudaEvent_t a, b;
+    };
+    std::vector<Mark> pending_;
+    size_t ev_next_ = 0;
+    friend struct ProfScope;
+};
+
+}  // namespace nuc3d

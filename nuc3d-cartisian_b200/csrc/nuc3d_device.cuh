@@ -87,69 +87,111 @@ __device__ __forceinline__ void weno5_candidates(B f0, B f1, B f2, B f3, B f4, B
     q2 = B(K::A20) * f2 + B(K::A21) * f3 + B(K::A22) * f4;
 }
 
-// WENO5-JS face value (weno5js.cpp:75-108), eps = 1e-6, p = 2.
-// FP64: alpha_k = c_k/s_k^2 normalised by their sum, written with a single
-// division by multiplying through with s0^2 s1^2 s2^2 (an exact
-// rearrangement).  FP32: reciprocal form.
-__device__ __forceinline__ double weno5js_face(double f0, double f1, double f2, double f3,
-                                               double f4) {
-    double is0, is1, is2, q0, q1, q2;
-    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
-    weno5_candidates(f0, f1, f2, f3, f4, q0, q1, q2);
-    const double ss = 1.0e-6;
-    double s0 = ss + is0, s1 = ss + is1, s2 = ss + is2;
-    s0 *= s0;
-    s1 *= s1;
-    s2 *= s2;
-    double w0 = K::C0 * (s1 * s2), w1 = K::C1 * (s0 * s2), w2 = K::C2 * (s0 * s1);
-    return (w0 * q0 + w1 * q1 + w2 * q2) / (w0 + w1 + w2);
-}
-__device__ __forceinline__ float weno5js_face(float f0, float f1, float f2, float f3, float f4) {
-    float is0, is1, is2, q0, q1, q2;
-    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
-    weno5_candidates(f0, f1, f2, f3, f4, q0, q1, q2);
-    const float ss = 1.0e-6f;
-    float r0 = __frcp_rn(ss + is0), r1 = __frcp_rn(ss + is1), r2 = __frcp_rn(ss + is2);
-    float a0 = float(K::C0) * r0 * r0, a1 = float(K::C1) * r1 * r1, a2 = float(K::C2) * r2 * r2;
-    return (a0 * q0 + a1 * q1 + a2 * q2) * __frcp_rn(a0 + a1 + a2);
+// Explicitly rounded arithmetic.  The sweep kernels come in variants that
+// unroll different numbers of faces per thread; with free FMA contraction the
+// compiler shares products across unrolled faces differently per variant and
+// the results would differ in the last bits.  Spelling every operation with a
+// rounding intrinsic fixes the operation sequence, so all variants (and hence
+// a box alone or in any batch) give bitwise identical results.
+__device__ __forceinline__ double fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double mul_(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub_(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_(float a, float b) { return __fsub_rn(a, b); }
+
+// second difference f0 - 2 f1 + f2
+template <typename B>
+__device__ __forceinline__ B d2_(B f0, B f1, B f2) {
+    return add_(fma_(B(-2), f1, f0), f2);
 }
 
-// WENO5-Z face value (weno5z.cpp:74-109), eps = 1e-40, p = 2:
-// alpha_k = c_k (1 + (tau/(beta_k+eps))^2), tau = |beta2 - beta0|.
-__device__ __forceinline__ double weno5z_face(double f0, double f1, double f2, double f3,
-                                              double f4, bool beta2_quirk) {
-    double is0, is1, is2, q0, q1, q2;
-    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, beta2_quirk);
-    weno5_candidates(f0, f1, f2, f3, f4, q0, q1, q2);
-    const double ss = 1.0e-40;
-    double tau = fabs(is2 - is0);
-    double t2 = tau * tau;
-    double s0 = is0 + ss, s1 = is1 + ss, s2 = is2 + ss;
-    s0 *= s0;
-    s1 *= s1;
-    s2 *= s2;
-    // alpha_k * s0^2 s1^2 s2^2 = c_k (s_k^2 + tau^2) prod_{j!=k} s_j^2
-    double w0 = K::C0 * (s0 + t2) * (s1 * s2);
-    double w1 = K::C1 * (s1 + t2) * (s0 * s2);
-    double w2 = K::C2 * (s2 + t2) * (s0 * s1);
-    return (w0 * q0 + w1 * q1 + w2 * q2) / (w0 + w1 + w2);
+// Fast FP32 reciprocal (one MUFU op, ~1 ulp): the weights only need FP32
+// accuracy in the mixed path.
+__device__ __forceinline__ float frcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 }
-__device__ __forceinline__ float weno5z_face(float f0, float f1, float f2, float f3, float f4,
-                                             bool beta2_quirk) {
-    float is0, is1, is2, q0, q1, q2;
-    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, beta2_quirk);
-    weno5_candidates(f0, f1, f2, f3, f4, q0, q1, q2);
+
+// WENO5-JS nonlinear combination (weno5js.cpp:97-108), eps = 1e-6, p = 2:
+// alpha_k = c_k/(eps+beta_k)^2 normalised by their sum.  FP64 writes it with a
+// single division by multiplying through with s0^2 s1^2 s2^2 (an exact
+// rearrangement); FP32 uses fast reciprocals.
+__device__ __forceinline__ double weno_js_combine(double is0, double is1, double is2, double q0,
+                                                  double q1, double q2) {
+    const double ss = 1.0e-6;
+    double s0 = add_(ss, is0), s1 = add_(ss, is1), s2 = add_(ss, is2);
+    s0 = mul_(s0, s0);
+    s1 = mul_(s1, s1);
+    s2 = mul_(s2, s2);
+    double w0 = mul_(K::C0, mul_(s1, s2)), w1 = mul_(K::C1, mul_(s0, s2));
+    double w2 = mul_(K::C2, mul_(s0, s1));
+    return __ddiv_rn(fma_(w2, q2, fma_(w1, q1, mul_(w0, q0))), add_(add_(w0, w1), w2));
+}
+__device__ __forceinline__ float weno_js_combine(float is0, float is1, float is2, float q0,
+                                                 float q1, float q2) {
+    const float ss = 1.0e-6f;
+    float r0 = frcp_fast(add_(ss, is0)), r1 = frcp_fast(add_(ss, is1)), r2 = frcp_fast(add_(ss, is2));
+    float a0 = mul_(mul_(float(K::C0), r0), r0), a1 = mul_(mul_(float(K::C1), r1), r1);
+    float a2 = mul_(mul_(float(K::C2), r2), r2);
+    return mul_(fma_(a2, q2, fma_(a1, q1, mul_(a0, q0))), frcp_fast(add_(add_(a0, a1), a2)));
+}
+
+// WENO5-Z combination (weno5z.cpp:96-109), eps = 1e-40, p = 2:
+// alpha_k = c_k (1 + (tau/(beta_k+eps))^2), tau = |beta2 - beta0|.
+__device__ __forceinline__ double weno_z_combine(double is0, double is1, double is2, double q0,
+                                                 double q1, double q2) {
+    const double ss = 1.0e-40;
+    double tau = fabs(sub_(is2, is0));
+    double t2 = mul_(tau, tau);
+    double s0 = add_(is0, ss), s1 = add_(is1, ss), s2 = add_(is2, ss);
+    s0 = mul_(s0, s0);
+    s1 = mul_(s1, s1);
+    s2 = mul_(s2, s2);
+    // alpha_k * s0^2 s1^2 s2^2 = c_k (s_k^2 + tau^2) prod_{j!=k} s_j^2
+    double w0 = mul_(mul_(K::C0, add_(s0, t2)), mul_(s1, s2));
+    double w1 = mul_(mul_(K::C1, add_(s1, t2)), mul_(s0, s2));
+    double w2 = mul_(mul_(K::C2, add_(s2, t2)), mul_(s0, s1));
+    return __ddiv_rn(fma_(w2, q2, fma_(w1, q1, mul_(w0, q0))), add_(add_(w0, w1), w2));
+}
+__device__ __forceinline__ float weno_z_combine(float is0, float is1, float is2, float q0, float q1,
+                                                float q2) {
     // 1e-40 is below FP32's normal range; 1e-30 keeps the ratio finite and
     // only differs where a sub-stencil is exactly constant.
     const float ss = 1.0e-30f, cap = 1.0e18f;
-    float tau = fabsf(is2 - is0);
-    float t0 = fminf(tau * __frcp_rn(is0 + ss), cap);
-    float t1 = fminf(tau * __frcp_rn(is1 + ss), cap);
-    float t2 = fminf(tau * __frcp_rn(is2 + ss), cap);
-    float a0 = float(K::C0) * (1.0f + t0 * t0);
-    float a1 = float(K::C1) * (1.0f + t1 * t1);
-    float a2 = float(K::C2) * (1.0f + t2 * t2);
-    return (a0 * q0 + a1 * q1 + a2 * q2) * __frcp_rn(a0 + a1 + a2);
+    float tau = fabsf(sub_(is2, is0));
+    float t0 = fminf(mul_(tau, frcp_fast(add_(is0, ss))), cap);
+    float t1 = fminf(mul_(tau, frcp_fast(add_(is1, ss))), cap);
+    float t2 = fminf(mul_(tau, frcp_fast(add_(is2, ss))), cap);
+    float a0 = mul_(float(K::C0), fma_(t0, t0, 1.0f));
+    float a1 = mul_(float(K::C1), fma_(t1, t1, 1.0f));
+    float a2 = mul_(float(K::C2), fma_(t2, t2, 1.0f));
+    return mul_(fma_(a2, q2, fma_(a1, q1, mul_(a0, q0))), frcp_fast(add_(add_(a0, a1), a2)));
+}
+
+template <int SCHEME, typename B>
+__device__ __forceinline__ B weno_combine(B is0, B is1, B is2, B q0, B q1, B q2) {
+    if (SCHEME == SCHEME_Z) return weno_z_combine(is0, is1, is2, q0, q1, q2);
+    return weno_js_combine(is0, is1, is2, q0, q1, q2);
+}
+
+// Face values from an upwind-oriented 5-cell stencil (f0 farthest upwind).
+template <typename B>
+__device__ __forceinline__ B weno5js_face(B f0, B f1, B f2, B f3, B f4) {
+    B is0, is1, is2, q0, q1, q2;
+    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
+    weno5_candidates(f0, f1, f2, f3, f4, q0, q1, q2);
+    return weno_js_combine(is0, is1, is2, q0, q1, q2);
+}
+template <typename B>
+__device__ __forceinline__ B weno5z_face(B f0, B f1, B f2, B f3, B f4, bool beta2_quirk) {
+    B is0, is1, is2, q0, q1, q2;
+    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, beta2_quirk);
+    weno5_candidates(f0, f1, f2, f3, f4, q0, q1, q2);
+    return weno_z_combine(is0, is1, is2, q0, q1, q2);
 }
 
 template <int SCHEME, typename B>

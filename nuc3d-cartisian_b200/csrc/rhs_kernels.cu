@@ -1,10 +1,11 @@
-// Whole-box RHS + TVD-RK3 stage kernels for one periodic box.
+// Batched whole-box kernels: primitive recovery, dt, residual and the
+// directional WENO5 sweeps.
 //
-// One stage = k_prim -> [k_visc_flux] -> k_inviscid<x> -> k_inviscid<y> ->
-// k_inviscid<z> -> k_update.  The reference's per-direction rotated copies,
-// halo buffers and MPI self-messages (euler3d.cpp:307-387,
-// NaiverStokes3d.cpp:87-369, MPICommunicator.cpp:81-132) become periodic
-// index wraps inside the tile loads.
+// One RK stage = k_prim -> [k_visc_flux25] -> k_inviscid<x> -> k_inviscid<y>
+// -> k_inviscid<z> -> k_update25, each one launch for every box of a batch.
+// The reference's per-direction rotated copies, halo buffers and MPI
+// self-messages (euler3d.cpp:307-387, NaiverStokes3d.cpp:87-369,
+// MPICommunicator.cpp:81-132) become periodic index wraps in the tile loads.
 #include "nuc3d_device.cuh"
 #include "rhs_kernels.h"
 
@@ -12,28 +13,38 @@ namespace nuc3d {
 
 // ----------------------------------------------------------------- k_prim --
 // physicsModel::con2prim (physicsModel.cpp:324-356), FP64, plus the running
-// maxEigen of RiemannLF (physicsModel.cpp:546-547, 600-601, 653-654).
-__global__ void __launch_bounds__(256) k_prim(BoxParams bp, StateView q, PrimView w,
-                                              double *eig, int want_eig) {
+// maxEigen of RiemannLF (physicsModel.cpp:546-547, 600-601, 653-654).  A work
+// item is (box, first cell, cell count).
+__global__ void __launch_bounds__(256, 4) k_prim(const BoxDev *__restrict__ boxes,
+                                                 const WorkItem *__restrict__ items, int in_slot,
+                                                 int want_eig) {
+    const WorkItem it = items[blockIdx.x];
+    const BoxDev &bd = boxes[it.box];
+    if (!bd.active) return;
+    const BoxParams &bp = bd.p;
+    const long long np = bd.np;
+    const double *__restrict__ q = fieldU(bd, in_slot, 0);
+    double *__restrict__ w = fieldW(bd, 0);
     double lx = 0.0, ly = 0.0, lz = 0.0;
     const double gamma = bp.gamma, Mach = bp.mach;
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < bp.N;
-         n += (long long)gridDim.x * blockDim.x) {
-        double rho = q.q[0][n];
-        double u = q.q[1][n] / rho;
-        double v = q.q[2][n] / rho;
-        double ww = q.q[3][n] / rho;
-        double E = q.q[4][n];
+    const bool fabs_p = (bp.quirks & QK_FABS_PRESSURE) != 0;
+    const long long n0 = (long long)it.a * kPrimChunk, n1 = n0 + it.b;
+    for (long long n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
+        double rho = q[n];
+        double u = q[np + n] / rho;
+        double v = q[2 * np + n] / rho;
+        double ww = q[3 * np + n] / rho;
+        double E = q[4 * np + n];
         double p = (E - 0.5 * rho * (u * u + v * v + ww * ww)) * (gamma - 1.0);
-        if (bp.quirks & QK_FABS_PRESSURE) p = fabs(p);
+        if (fabs_p) p = fabs(p);
         double c = sqrt(gamma * p / rho);
         double T = gamma * Mach * Mach * p / rho;
-        w.w[0][n] = u;
-        w.w[1][n] = v;
-        w.w[2][n] = ww;
-        w.w[3][n] = p;
-        w.w[4][n] = c;
-        w.w[5][n] = T;
+        w[n] = u;
+        w[np + n] = v;
+        w[2 * np + n] = ww;
+        w[3 * np + n] = p;
+        w[4 * np + n] = c;
+        w[5 * np + n] = T;
         lx = fmax(fabs(u) + c, lx);
         ly = fmax(fabs(v) + c, ly);
         lz = fmax(fabs(ww) + c, lz);
@@ -62,124 +73,186 @@ __global__ void __launch_bounds__(256) k_prim(BoxParams bp, StateView q, PrimVie
             ly = fmax(ly, red[1][i]);
             lz = fmax(lz, red[2][i]);
         }
-        atomic_max_nonneg(&eig[0], lx);
-        atomic_max_nonneg(&eig[1], ly);
-        atomic_max_nonneg(&eig[2], lz);
+        atomic_max_nonneg(&bd.eig[0], lx);
+        atomic_max_nonneg(&bd.eig[1], ly);
+        atomic_max_nonneg(&bd.eig[2], lz);
     }
+}
+
+__global__ void k_clear_eig(const BoxDev *boxes, int nboxes) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nboxes || !boxes[b].active) return;
+    boxes[b].eig[0] = boxes[b].eig[1] = boxes[b].eig[2] = 0.0;
 }
 
 // -------------------------------------------------------------------- k_dt --
 // EulerData3D::getDt (euler3d.cpp:459-466) and PDEData3d::solve's
-// dt_global = dt_local * cfl (PDEData3d.cpp:161-165).  One thread.
-__global__ void k_dt(BoxParams bp, const double *eig, StepScalars *sc, int step) {
-    double dt_xi = bp.d[0] / eig[0];
-    double dt_eta = bp.d[1] / eig[1];
-    double dt_zeta = bp.d[2] / eig[2];
+// dt_global = dt_local * cfl (PDEData3d.cpp:161-165).  One thread per box.
+__global__ void k_dt(const BoxDev *boxes, int nboxes) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nboxes || !boxes[b].active) return;
+    const BoxDev &bd = boxes[b];
+    const double *eig = bd.eig;
+    double dt_xi = bd.p.d[0] / eig[0];
+    double dt_eta = bd.p.d[1] / eig[1];
+    double dt_zeta = bd.p.d[2] / eig[2];
     double dt_local = 1.0 / (1.0 / dt_xi + 1.0 / dt_eta + 1.0 / dt_zeta);
+    StepScalars *sc = bd.sc;
     sc->dt_local = dt_local;
-    sc->dt = dt_local * bp.cfl;
-    if (step >= 0) sc->dt_hist[step] = sc->dt;
+    sc->dt = dt_local * sc->cfl;
+    sc->dt_hist[sc->step % kHistory] = sc->dt;
+}
+
+// residual = sqrt(sum / (5 N)) / dt (PDEData3d.cpp:212); advances time and
+// the step counter.  One thread per box.
+__global__ void k_residual(const BoxDev *boxes, int nboxes) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nboxes || !boxes[b].active) return;
+    const BoxDev &bd = boxes[b];
+    StepScalars *sc = bd.sc;
+    double r = sqrt(*bd.res_acc / (double)(bd.p.N * 5)) / sc->dt;
+    sc->res_hist[sc->step % kHistory] = r;
+    sc->time += sc->dt;
+    sc->step += 1;
+    *bd.res_acc = 0.0;
 }
 
 // -------------------------------------------------------------- k_inviscid --
-// Tile geometry of the directional sweep kernel.
-template <int DIR, typename B>
-struct InvTile;
-template <typename B>
-struct InvTile<0, B> {  // sweep along x: tile = TL rows (j) x TC cells (x)
-    static constexpr int TL = 8, TC = 32;
-};
-// sweep along y / z: tile = TL columns (i) x TC cells along the sweep.  TL
-// columns of B make one full 128-byte row per load; FP64 uses 16 columns so
-// that four to five blocks fit per SM.
-template <typename B>
-struct InvTile<1, B> {
-    static constexpr int TL = 128 / sizeof(B), TC = 16;
-};
-template <typename B>
-struct InvTile<2, B> {
-    static constexpr int TL = 128 / sizeof(B), TC = 16;
-};
-
-template <int DIR, typename B>
+// Tile of the directional sweep: TL lines x TC cells along the sweep; every
+// thread owns one line and a run of R consecutive faces of it.
+//   DIR 0 (x): 16 lines (rows j) per tile; the 8 runs of a line sit in 8
+//              consecutive lanes.
+//   DIR 1/2:   TL = one 128-byte row of B (16 FP64 / 32 FP32 columns i) per
+//              tile; consecutive lanes are consecutive lines (coalesced).
+template <int DIR, typename B, int RUN>
 struct InvGeom {
-    static constexpr int TL = InvTile<DIR, B>::TL, TC = InvTile<DIR, B>::TC;
-    static constexpr int NF = TC + 6;  // cells staged (3-cell halo each side)
-    static constexpr int NH = TC + 1;  // faces
-    static constexpr int NT = TL * NH; // threads: one face per thread
-    // shared-memory index: thread-fast index is the position for DIR 0 and
-    // the line for DIR 1/2, so neighbouring threads touch neighbouring words
-    __device__ static int sf(int v, int l, int pc) {
-        return DIR == 0 ? (v * TL + l) * NF + pc : (v * NF + pc) * TL + l;
-    }
-    __device__ static int sh(int e, int l, int m) {
-        return DIR == 0 ? (e * TL + l) * NH + m : (e * NH + m) * TL + l;
-    }
-    __device__ static void item(int t, int span, int &l, int &p) {
+    static constexpr int R = RUN;               // faces per thread (1, 2 or 4)
+    static constexpr int NR = 32 / RUN;         // runs per line
+    static constexpr int TC = R * NR;           // cells per tile along the sweep (32)
+    static constexpr int TL = DIR == 0 ? 16 : 128 / (int)sizeof(B);
+    static constexpr int NF = TC + 6;           // staged cells (3-cell halo each side)
+    static constexpr int S = (NF + R - 1) / R;  // DIR 0 interleave stride
+    static constexpr int NT = TL * NR;          // threads
+    static constexpr int SF = DIR == 0 ? TL * R * S : NF * TL;  // staged values per flux
+    // thread -> (line, run)
+    __device__ static void thread(int t, int &l, int &r) {
         if (DIR == 0) {
-            l = t / span;
-            p = t - l * span;
+            l = t / NR;
+            r = t % NR;
         } else {
             l = t % TL;
-            p = t / TL;
+            r = t / TL;
+        }
+    }
+    // staged position pc (cell c0 - 3 + pc) of line l for flux v.  DIR 0
+    // interleaves positions so that the runs of a line (stride R) read
+    // consecutive words.
+    __device__ static int sf(int v, int l, int pc) {
+        return DIR == 0 ? v * SF + (l * R + pc % R) * S + pc / R : v * SF + pc * TL + l;
+    }
+    // staging loop: item t -> (line, position) with consecutive t reading
+    // consecutive addresses
+    __device__ static void stage_item(int t, int &l, int &pc) {
+        if (DIR == 0) {
+            l = t / NF;
+            pc = t - l * NF;
+        } else {
+            l = t % TL;
+            pc = t / TL;
         }
     }
 };
 
+// One direction's smoothness and candidate terms for a stencil whose second
+// differences d0, d1, d2 are already known (the run reuses them across faces).
+template <int SCHEME, typename B>
+__device__ __forceinline__ B weno_from(B f0, B f1, B f2, B f3, B f4, B d0, B d1, B d2) {
+    const B g0 = B(K::G0), g1 = B(K::G1);
+    B e0 = fma_(B(3), f2, fma_(B(-4), f1, f0));
+    B e1 = sub_(f1, f3);
+    B e2 = add_(fma_(B(-4), f3, mul_(B(3), f2)), f4);
+    B is0 = fma_(mul_(g0, d0), d0, mul_(mul_(g1, e0), e0));
+    B is1 = fma_(mul_(g0, d1), d1, mul_(mul_(g1, e1), e1));
+    B is2 = fma_(mul_(g0, d2), d2, mul_(mul_(g1, e2), e2));
+    B q0 = fma_(B(K::A02), f2, fma_(B(K::A01), f1, mul_(B(K::A00), f0)));
+    B q1 = fma_(B(K::A12), f3, fma_(B(K::A11), f2, mul_(B(K::A10), f1)));
+    B q2 = fma_(B(K::A22), f4, fma_(B(K::A21), f3, mul_(B(K::A20), f2)));
+    return weno_combine<SCHEME, B>(is0, is1, is2, q0, q1, q2);
+}
+
 // Inviscid flux derivative along DIR for all 5 equations (euler3d.cpp:307-387
 // + combineFluxLR :23-56 + setDerivatives*Inv :143-253), with the
 // Lax-Friedrichs split (physicsModel.cpp:546-565) done while staging.
-//   accumulate = 0: r = dF/dx ; 1: r += dG/dy (rhs order of
+//   accumulate = 0: R = dF/dx ; 1: R += dG/dy (the RHS summation order of
 //   NaiverStokes3d.cpp:396-446).
+// Work item: (box, a, b, c) = DIR 0: (x chunk, j group, k); DIR 1: (i group,
+// y chunk, k); DIR 2: (i group, j, z chunk).
+// Each thread computes F^ = F^+ + F^- on its R faces with a register sliding
+// window (the second differences of the smoothness indicators are carried
+// from face to face), takes the first face of the next run from a neighbour
+// through shared memory, and writes dF for its R cells.
 // Mixed precision (B = float): the split fluxes are formed in FP64 and each
 // line's value at the tile's first interior cell is subtracted before
 // rounding to FP32.  WENO5 commutes with adding a constant and the constant
 // cancels in the face difference, so this only removes rounding error.
-template <int SCHEME, int DIR, typename B>
-__global__ void __launch_bounds__(InvGeom<DIR, B>::NT)
-    k_inviscid(BoxParams bp, StateView q, PrimView w, BView<B> r, int accumulate) {
-    using G = InvGeom<DIR, B>;
-    constexpr int TL = G::TL, TC = G::TC, NF = G::NF, NH = G::NH;
+template <int SCHEME, int DIR, typename B, int RUN>
+__global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
+    k_inviscid(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, int in_slot,
+               int accumulate) {
+    using G = InvGeom<DIR, B, RUN>;
+    constexpr int TL = G::TL, TC = G::TC, NF = G::NF, R = G::R, NR = G::NR, NT = G::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    B *sF = reinterpret_cast<B *>(smem_raw);      // [10][..] split fluxes (+ e, then - e)
-    B *sH = sF + 10 * TL * NF;                     // [5][..] face fluxes F^+ + F^-
+    B *sF = reinterpret_cast<B *>(smem_raw);  // [10][SF] split fluxes (+ e, then - e)
+    B *xb = sF + 10 * G::SF;                  // [2][NT] first face of each run
     __shared__ double sRef[10][TL];
 
+    const WorkItem it = items[blockIdx.x];
+    const BoxDev &bd = boxes[it.box];
+    if (!bd.active) return;
+    const BoxParams &bp = bd.p;
+    const double *const qbase = fieldU(bd, in_slot, 0);
+    const double *const wbase = fieldW(bd, 0);
+    B *const rbase = fieldR<B>(bd, 0);
+    const long long np = bd.np;
     const int n = bp.n[DIR];
     int l0, c0, fixed;  // first line, first cell of the chunk, the third index
     if (DIR == 0) {
-        c0 = blockIdx.x * TC;
-        l0 = blockIdx.y * TL;
-        fixed = blockIdx.z;
+        c0 = it.a * TC;
+        l0 = it.b * TL;
+        fixed = it.c;
     } else if (DIR == 1) {
-        l0 = blockIdx.x * TL;
-        c0 = blockIdx.y * TC;
-        fixed = blockIdx.z;
+        l0 = it.a * TL;
+        c0 = it.b * TC;
+        fixed = it.c;
     } else {
-        l0 = blockIdx.x * TL;
-        fixed = blockIdx.y;
-        c0 = blockIdx.z * TC;
+        l0 = it.a * TL;
+        fixed = it.b;
+        c0 = it.c * TC;
     }
     const int nl = DIR == 0 ? bp.n[1] : bp.n[0];  // extent of the line index
+    const long long sy = bp.stride[1], sz = bp.stride[2];
     auto gidx = [&](int l, int pos) -> long long {
         int a = l0 + l;
-        if (DIR == 0) return pos + bp.stride[1] * (a + (long long)bp.n[1] * fixed);
-        if (DIR == 1) return a + bp.stride[1] * (pos + (long long)bp.n[1] * fixed);
-        return a + bp.n[0] * (long long)fixed + bp.stride[2] * pos;
+        if (DIR == 0) return pos + sy * a + sz * fixed;
+        if (DIR == 1) return a + sy * pos + sz * fixed;
+        return a + sy * fixed + sz * pos;
     };
     auto split = [&](long long g, double Fp[5], double Fm[5]) {
-        double Q[5] = {q.q[0][g], q.q[1][g], q.q[2][g], q.q[3][g], q.q[4][g]};
-        double un = w.w[DIR][g], p = w.w[3][g], c = w.w[4][g];
-        double lam = fabs(un) + c;
+        double Q[5];
+#pragma unroll
+        for (int e = 0; e < 5; ++e) Q[e] = qbase[e * np + g];
+        double un = wbase[DIR * np + g], p = wbase[3 * np + g], c = wbase[4 * np + g];
+        double lam = add_(fabs(un), c);
         double f[5];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) f[e] = un * Q[e];
-        f[1 + DIR] = un * Q[1 + DIR] + p;
-        f[4] = un * (Q[4] + p);
+        for (int e = 0; e < 4; ++e) f[e] = mul_(un, Q[e]);
+        f[1 + DIR] = fma_(un, Q[1 + DIR], p);
+        f[4] = mul_(un, add_(Q[4], p));
 #pragma unroll
         for (int e = 0; e < 5; ++e) {
-            Fp[e] = 0.5 * (f[e] + lam * Q[e]);
-            Fm[e] = 0.5 * (f[e] - lam * Q[e]);
+            double t = mul_(lam, Q[e]);
+            Fp[e] = mul_(0.5, add_(f[e], t));
+            Fm[e] = mul_(0.5, sub_(f[e], t));
         }
     };
     const bool mixed = sizeof(B) == sizeof(float);
@@ -202,9 +275,9 @@ __global__ void __launch_bounds__(InvGeom<DIR, B>::NT)
         __syncthreads();
     }
     // phase 1: stage the split fluxes of cells c0-3 .. c0+TC+2
-    for (int t = threadIdx.x; t < TL * NF; t += blockDim.x) {
+    for (int t = threadIdx.x; t < TL * NF; t += NT) {
         int l, pc;
-        G::item(t, NF, l, pc);
+        G::stage_item(t, l, pc);
         double Fp[5], Fm[5];
         if (l0 + l < nl) {
             int pos = ((c0 - 3 + pc) % n + n) % n;
@@ -216,8 +289,8 @@ __global__ void __launch_bounds__(InvGeom<DIR, B>::NT)
 #pragma unroll
         for (int e = 0; e < 5; ++e) {
             if (mixed) {
-                sF[G::sf(e, l, pc)] = B(Fp[e] - sRef[e][l]);
-                sF[G::sf(5 + e, l, pc)] = B(Fm[e] - sRef[5 + e][l]);
+                sF[G::sf(e, l, pc)] = B(sub_(Fp[e], sRef[e][l]));
+                sF[G::sf(5 + e, l, pc)] = B(sub_(Fm[e], sRef[5 + e][l]));
             } else {
                 sF[G::sf(e, l, pc)] = B(Fp[e]);
                 sF[G::sf(5 + e, l, pc)] = B(Fm[e]);
@@ -225,130 +298,188 @@ __global__ void __launch_bounds__(InvGeom<DIR, B>::NT)
         }
     }
     __syncthreads();
-    // phase 2: faces c0 .. c0+TC (face m lies between cells m-1 and m)
+    // phase 2: runs of faces.  Face m (local) lies between cells c0+m-1 and
+    // c0+m; '+' reads staged positions m..m+4, '-' reads m+5..m+1.
+    int l, r;
+    G::thread(threadIdx.x, l, r);
+    const int m0 = r * R;
+    const bool last = r == NR - 1;       // also computes face TC (next tile's first)
+    const bool line_ok = l0 + l < nl;
     const bool zq = SCHEME == SCHEME_Z && (bp.quirks & QK_WENOZ_BETA2);
-    for (int t = threadIdx.x; t < TL * NH; t += blockDim.x) {
-        int l, m;
-        G::item(t, NH, l, m);
-        int gm = c0 + m;
-        if (gm > n) continue;
-        // weno5z.cpp:80 applies on the inner faces 3..n-3 only
-        bool quirk = zq && gm >= 3 && gm <= n - 3;
-#pragma unroll 1
-        for (int e = 0; e < 5; ++e) {
-            // '+': cells gm-3..gm+1 -> pc m..m+4 ; '-': cells gm+2..gm-2 -> pc m+5..m+1
-            B fp = weno5_face<SCHEME, B>(sF[G::sf(e, l, m)], sF[G::sf(e, l, m + 1)],
-                                         sF[G::sf(e, l, m + 2)], sF[G::sf(e, l, m + 3)],
-                                         sF[G::sf(e, l, m + 4)], quirk);
-            B fm = weno5_face<SCHEME, B>(sF[G::sf(5 + e, l, m + 5)], sF[G::sf(5 + e, l, m + 4)],
-                                         sF[G::sf(5 + e, l, m + 3)], sF[G::sf(5 + e, l, m + 2)],
-                                         sF[G::sf(5 + e, l, m + 1)], false);
-            sH[G::sh(e, l, m)] = fp + fm;
-        }
-    }
-    __syncthreads();
-    // phase 3: dF/dx(cell) = (F^[m+1] - F^[m]) / delta
     const B inv_d = B(bp.inv_d[DIR]);
-    for (int t = threadIdx.x; t < TL * TC; t += blockDim.x) {
-        int l, m;
-        G::item(t, TC, l, m);
-        int gc = c0 + m;
-        if (gc >= n || l0 + l >= nl) continue;
-        long long g = gidx(l, gc);
+    int nbr_l, nbr_r = r + 1;            // the thread owning the next run
+    nbr_l = l;
+    const int nbr = DIR == 0 ? nbr_l * NR + nbr_r : nbr_r * TL + nbr_l;
+#pragma unroll 1
+    for (int e = 0; e < 5; ++e) {
+        B Fh[R + 1];
+        {  // '+' side: window f0..f4 = positions m..m+4
+            const int v = e;
+            B f0 = sF[G::sf(v, l, m0)], f1 = sF[G::sf(v, l, m0 + 1)], f2 = sF[G::sf(v, l, m0 + 2)];
+            B f3 = sF[G::sf(v, l, m0 + 3)], f4 = sF[G::sf(v, l, m0 + 4)];
+            B d0 = d2_(f0, f1, f2), d1 = d2_(f1, f2, f3);
 #pragma unroll
-        for (int e = 0; e < 5; ++e) {
-            B dfe = (sH[G::sh(e, l, m + 1)] - sH[G::sh(e, l, m)]) * inv_d;
-            if (accumulate)
-                r.f[e][g] += dfe;
-            else
-                r.f[e][g] = dfe;
+            for (int k = 0; k <= R; ++k) {
+                if (k == R && !last) break;
+                const int gm = c0 + m0 + k;
+                B d2 = d2_(f2, f3, f4);
+                // weno5z.cpp:80 on the inner '+' faces 3..n-3
+                B d2s = (zq && gm >= 3 && gm <= n - 3) ? d2_(f2, f3, f3) : d2;
+                Fh[k] = weno_from<SCHEME, B>(f0, f1, f2, f3, f4, d0, d1, d2s);
+                if (k < R) {
+                    f0 = f1;
+                    f1 = f2;
+                    f2 = f3;
+                    f3 = f4;
+                    f4 = sF[G::sf(v, l, m0 + k + 5)];
+                    d0 = d1;
+                    d1 = d2;
+                }
+            }
+        }
+        {  // '-' side: window f0..f4 = positions m+5..m+1
+            const int v = 5 + e;
+            B f0 = sF[G::sf(v, l, m0 + 5)], f1 = sF[G::sf(v, l, m0 + 4)], f2 = sF[G::sf(v, l, m0 + 3)];
+            B f3 = sF[G::sf(v, l, m0 + 2)], f4 = sF[G::sf(v, l, m0 + 1)];
+            B d1 = d2_(f1, f2, f3), d2 = d2_(f2, f3, f4);
+#pragma unroll
+            for (int k = 0; k <= R; ++k) {
+                if (k == R && !last) break;
+                B d0 = d2_(f0, f1, f2);
+                Fh[k] = add_(Fh[k], weno_from<SCHEME, B>(f0, f1, f2, f3, f4, d0, d1, d2));
+                if (k < R) {
+                    f4 = f3;
+                    f3 = f2;
+                    f2 = f1;
+                    f1 = f0;
+                    f0 = (m0 + k + 6 < NF) ? sF[G::sf(v, l, m0 + k + 6)] : B(0);
+                    d2 = d1;
+                    d1 = d0;
+                }
+            }
+        }
+        B *x = xb + (e & 1) * NT;
+        x[threadIdx.x] = Fh[0];
+        __syncthreads();
+        B next = last ? Fh[R] : x[nbr];
+        if (line_ok) {
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const int gc = c0 + m0 + k;
+                if (gc >= n) break;
+                B hi = (k + 1 < R) ? Fh[k + 1] : next;
+                B dfe = mul_(sub_(hi, Fh[k]), inv_d);
+                long long g = gidx(l, gc) + e * np;
+                rbase[g] = accumulate ? add_(rbase[g], dfe) : dfe;
+            }
         }
     }
-}
-
-// k_residual_final: residual = sqrt(sum / (5 N)) / dt (PDEData3d.cpp:212)
-__global__ void k_residual(BoxParams bp, StepScalars *sc, double *res_acc, int step) {
-    double r = sqrt(*res_acc / (double)(bp.N * 5)) / sc->dt;
-    if (step >= 0) sc->res_hist[step] = r;
-    sc->time += sc->dt;
-    *res_acc = 0.0;
 }
 
 // --------------------------------------------------------------- launches --
-static int grid_for(long long N, int sms) {
-    long long want = (N + 255) / 256;
-    long long cap = (long long)sms * 8;
-    return (int)(want < cap ? want : cap);
+template <int DIR, typename B, int RUN>
+static size_t inv_smem_t() {
+    using G = InvGeom<DIR, B, RUN>;
+    return sizeof(B) * (size_t)(10 * G::SF + 2 * G::NT);
 }
 
-template <typename B>
-static size_t inv_smem(int dir) {
-    auto f = [](int TL, int TC) { return sizeof(B) * (size_t)(10 * TL * (TC + 6) + 5 * TL * (TC + 1)); };
-    if (dir == 0) return f(InvTile<0, B>::TL, InvTile<0, B>::TC);
-    if (dir == 1) return f(InvTile<1, B>::TL, InvTile<1, B>::TC);
-    return f(InvTile<2, B>::TL, InvTile<2, B>::TC);
+InvTileDims inviscid_tile(int dir, bool mixed) {
+    // the tile shape is the same for every run length
+    if (dir == 0) return mixed ? InvTileDims{InvGeom<0, float, 1>::TL, InvGeom<0, float, 1>::TC}
+                               : InvTileDims{InvGeom<0, double, 1>::TL, InvGeom<0, double, 1>::TC};
+    return mixed ? InvTileDims{InvGeom<1, float, 1>::TL, InvGeom<1, float, 1>::TC}
+                 : InvTileDims{InvGeom<1, double, 1>::TL, InvGeom<1, double, 1>::TC};
 }
 
-template <int SCHEME, int DIR, typename B>
-static cudaError_t launch_inviscid_t(const BoxParams &bp, StateView q, PrimView w, BView<B> r,
-                                     int accumulate, cudaStream_t st) {
-    using G = InvGeom<DIR, B>;
-    size_t sm = inv_smem<B>(DIR);
-    auto kern = k_inviscid<SCHEME, DIR, B>;
-    static bool attr_set = false;  // per template instance
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
-    dim3 grid;
-    if (DIR == 0)
-        grid = dim3((bp.n[0] + G::TC - 1) / G::TC, (bp.n[1] + G::TL - 1) / G::TL, bp.n[2]);
-    else if (DIR == 1)
-        grid = dim3((bp.n[0] + G::TL - 1) / G::TL, (bp.n[1] + G::TC - 1) / G::TC, bp.n[2]);
-    else
-        grid = dim3((bp.n[0] + G::TL - 1) / G::TL, bp.n[1], (bp.n[2] + G::TC - 1) / G::TC);
-    kern<<<grid, G::NT, sm, st>>>(bp, q, w, r, accumulate);
+template <int SCHEME, int DIR, typename B, int RUN>
+static cudaError_t launch_t(const BoxDev *boxes, const WorkItem *items, int nitems, int in_slot,
+                            int accumulate, cudaStream_t st) {
+    using G = InvGeom<DIR, B, RUN>;
+    if (nitems <= 0) return cudaSuccess;
+    k_inviscid<SCHEME, DIR, B, RUN><<<nitems, G::NT, inv_smem_t<DIR, B, RUN>(), st>>>(
+        boxes, items, in_slot, accumulate);
     return cudaGetLastError();
 }
 
-template <typename B>
-cudaError_t launch_inviscid(const BoxParams &bp, int dir, StateView q, PrimView w, BView<B> r,
-                            int accumulate, cudaStream_t st) {
-    int s = bp.scheme[dir];
-    if (s == SCHEME_JS) {
-        if (dir == 0) return launch_inviscid_t<SCHEME_JS, 0, B>(bp, q, w, r, accumulate, st);
-        if (dir == 1) return launch_inviscid_t<SCHEME_JS, 1, B>(bp, q, w, r, accumulate, st);
-        return launch_inviscid_t<SCHEME_JS, 2, B>(bp, q, w, r, accumulate, st);
+template <int SCHEME, int DIR, typename B>
+static cudaError_t launch_v(int variant, const BoxDev *boxes, const WorkItem *items, int nitems,
+                            int in_slot, int accumulate, cudaStream_t st) {
+    switch (variant) {
+        case 0: return launch_t<SCHEME, DIR, B, 1>(boxes, items, nitems, in_slot, accumulate, st);
+        case 1: return launch_t<SCHEME, DIR, B, 2>(boxes, items, nitems, in_slot, accumulate, st);
+        default: return launch_t<SCHEME, DIR, B, 4>(boxes, items, nitems, in_slot, accumulate, st);
     }
-    if (s == SCHEME_Z) {
-        if (dir == 0) return launch_inviscid_t<SCHEME_Z, 0, B>(bp, q, w, r, accumulate, st);
-        if (dir == 1) return launch_inviscid_t<SCHEME_Z, 1, B>(bp, q, w, r, accumulate, st);
-        return launch_inviscid_t<SCHEME_Z, 2, B>(bp, q, w, r, accumulate, st);
+}
+
+template <typename B>
+cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxes,
+                            const WorkItem *items, int nitems, int in_slot, int accumulate,
+                            cudaStream_t st) {
+    if (scheme == SCHEME_JS) {
+        if (dir == 0) return launch_v<SCHEME_JS, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+        if (dir == 1) return launch_v<SCHEME_JS, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+        return launch_v<SCHEME_JS, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+    }
+    if (scheme == SCHEME_Z) {
+        if (dir == 0) return launch_v<SCHEME_Z, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+        if (dir == 1) return launch_v<SCHEME_Z, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+        return launch_v<SCHEME_Z, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
     }
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_prim(const BoxParams &bp, StateView q, PrimView w, double *eig, int want_eig,
-                        int sms, cudaStream_t st) {
-    k_prim<<<grid_for(bp.N, sms), 256, 0, st>>>(bp, q, w, eig, want_eig);
+template <int SCHEME, int DIR, typename B, int RUN>
+static cudaError_t prepare_t() {
+    return cudaFuncSetAttribute(k_inviscid<SCHEME, DIR, B, RUN>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)inv_smem_t<DIR, B, RUN>());
+}
+template <int SCHEME, int DIR, typename B>
+static cudaError_t prepare_runs() {
+    cudaError_t e[3] = {prepare_t<SCHEME, DIR, B, 1>(), prepare_t<SCHEME, DIR, B, 2>(),
+                        prepare_t<SCHEME, DIR, B, 4>()};
+    for (cudaError_t x : e)
+        if (x != cudaSuccess) return x;
+    return cudaSuccess;
+}
+template <typename B>
+static cudaError_t prepare_all() {
+    cudaError_t e[6] = {prepare_runs<SCHEME_JS, 0, B>(), prepare_runs<SCHEME_JS, 1, B>(),
+                        prepare_runs<SCHEME_JS, 2, B>(), prepare_runs<SCHEME_Z, 0, B>(),
+                        prepare_runs<SCHEME_Z, 1, B>(), prepare_runs<SCHEME_Z, 2, B>()};
+    for (cudaError_t x : e)
+        if (x != cudaSuccess) return x;
+    return cudaSuccess;
+}
+
+cudaError_t prepare_inviscid_kernels(bool mixed) {
+    return mixed ? prepare_all<float>() : prepare_all<double>();
+}
+
+cudaError_t launch_prim(const BoxDev *boxes, const WorkItem *items, int nitems, int in_slot,
+                        int want_eig, cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
+    k_prim<<<nitems, 256, 0, st>>>(boxes, items, in_slot, want_eig);
     return cudaGetLastError();
 }
 
-cudaError_t launch_dt(const BoxParams &bp, const double *eig, StepScalars *sc, int step,
-                      cudaStream_t st) {
-    k_dt<<<1, 1, 0, st>>>(bp, eig, sc, step);
+cudaError_t launch_clear_eig(const BoxDev *boxes, int nboxes, cudaStream_t st) {
+    k_clear_eig<<<(nboxes + 127) / 128, 128, 0, st>>>(boxes, nboxes);
     return cudaGetLastError();
 }
 
-cudaError_t launch_residual(const BoxParams &bp, StepScalars *sc, double *res_acc, int step,
-                            cudaStream_t st) {
-    k_residual<<<1, 1, 0, st>>>(bp, sc, res_acc, step);
+cudaError_t launch_dt(const BoxDev *boxes, int nboxes, cudaStream_t st) {
+    k_dt<<<(nboxes + 127) / 128, 128, 0, st>>>(boxes, nboxes);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_inviscid<double>(const BoxParams &, int, StateView, PrimView,
-                                             BView<double>, int, cudaStream_t);
-template cudaError_t launch_inviscid<float>(const BoxParams &, int, StateView, PrimView,
-                                            BView<float>, int, cudaStream_t);
+cudaError_t launch_residual(const BoxDev *boxes, int nboxes, cudaStream_t st) {
+    k_residual<<<(nboxes + 127) / 128, 128, 0, st>>>(boxes, nboxes);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_inviscid<double>(int, int, int, const BoxDev *, const WorkItem *, int,
+                                             int, int, cudaStream_t);
+template cudaError_t launch_inviscid<float>(int, int, int, const BoxDev *, const WorkItem *, int,
+                                            int, int, cudaStream_t);
 }  // namespace nuc3d

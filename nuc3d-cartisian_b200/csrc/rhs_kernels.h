@@ -1,6 +1,11 @@
-// Host-side launch interface of the whole-box kernels (rhs_kernels.cu,
-// crweno_kernels.cu).  Internal to the library; the public surface is the C
-// ABI in include/nuc3d_b200.h.
+// Launch interface of the whole-box kernels.  Internal to the library; the
+// public surface is the C ABI in include/nuc3d_b200.h.
+//
+// Every kernel is batched: it receives a device table of boxes (BoxDev: the
+// box's parameters and field pointers) and a list of work items, one per
+// thread block, each naming a box and a tile of it.  A batch of boxes of
+// different sizes therefore advances with one launch per kernel class, and a
+// single box is simply a batch of one.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -9,57 +14,114 @@
 
 namespace nuc3d {
 
-constexpr int kHistory = 1024;  // per-call step history kept on the device
+constexpr int kHistory = 1024;  // per-box step history kept on the device
 
+// Per-box scalars in device memory, so a step never waits on the host:
+// dt of the current step, simulated time, the step counter that indexes the
+// history (it lets a captured CUDA graph replay without new arguments).
+struct StepScalars {
+    double dt;
+    double dt_local;
+    double time;
+    double cfl;
+    long long step;
+    long long pad;
+    double dt_hist[kHistory];
+    double res_hist[kHistory];
+};
+
+// One box of a batch as the kernels see it.  U[s]: conserved state of RK
+// stage s (U[0] = u_n, updated in place by the last stage); W: u, v, w, p,
+// c, T (FP64); R: inviscid RHS accumulator and V: viscous fluxes
+// (tau_xx, tau_xy, tau_xz, tau_yy, tau_yz, tau_zz, E_x, E_y, E_z) in the bulk
+// type.
+struct BoxDev {
+    BoxParams p;
+    // All fields of the box live in one allocation at fixed offsets, so a
+    // kernel needs only this base and the padded field length np:
+    //   U[s][e] (stage s, equation e)  at base + (5 s + e) np   (FP64)
+    //   W[i]                            at base + (15 + i) np   (FP64)
+    //   R[e], V[i]  (bulk type B)       at (B *)(base + 21 np) + e np, + (5 + i) np
+    double *base;
+    long long np;
+    double *eig;      // [3] running max eigenvalues of the current step
+    double *res_acc;  // residual partial sum
+    unsigned *flags;  // bit 0: non-finite state seen
+    StepScalars *sc;
+    int active;       // 0: the box is skipped by every kernel
+    int pad;
+};
+
+__host__ __device__ __forceinline__ double *fieldU(const BoxDev &b, int s, int e) {
+    return b.base + (long long)(5 * s + e) * b.np;
+}
+__host__ __device__ __forceinline__ double *fieldW(const BoxDev &b, int i) {
+    return b.base + (long long)(15 + i) * b.np;
+}
+template <typename B>
+__host__ __device__ __forceinline__ B *fieldR(const BoxDev &b, int e) {
+    return reinterpret_cast<B *>(b.base + 21 * b.np) + (long long)e * b.np;
+}
+template <typename B>
+__host__ __device__ __forceinline__ B *fieldV(const BoxDev &b, int i) {
+    return reinterpret_cast<B *>(b.base + 21 * b.np) + (long long)(5 + i) * b.np;
+}
+
+// A work item: box index and up to three tile coordinates.
+struct WorkItem {
+    int box, a, b, c;
+};
+
+// Stage addressing: which U buffers are input/output of RK stage `stage`;
+// stage -1 evaluates the RHS of U[0] and writes it to `rhs_out`.
+struct StageArgs {
+    int stage;
+    int in_slot;             // U index read by the RHS (0, 1, 2)
+    int out_slot;            // U index written by the update (1, 2, 0)
+    double *const *rhs_out;  // device array of 5 pointers per box (stage -1 only)
+};
+
+// Tile geometry of the batched kernels (host and device agree on these).
+struct InvTileDims {
+    int TL, TC;  // lines per tile, cells per tile along the sweep
+};
+InvTileDims inviscid_tile(int dir, bool mixed);
+constexpr int kT25X = 32, kT25Y = 8, kT25Z = 32;  // 2.5-D tile of the stencil kernels
+constexpr int kPrimChunk = 4096;                  // cells per k_prim work item
+
+// Opt the inviscid kernels of one precision into their dynamic shared
+// memory size (once per device, before any launch or stream capture).
+cudaError_t prepare_inviscid_kernels(bool mixed);
+cudaError_t launch_prim(const BoxDev *boxes, const WorkItem *items, int nitems, int in_slot,
+                        int want_eig, cudaStream_t st);
+cudaError_t launch_dt(const BoxDev *boxes, int nboxes, cudaStream_t st);
+cudaError_t launch_residual(const BoxDev *boxes, int nboxes, cudaStream_t st);
+cudaError_t launch_clear_eig(const BoxDev *boxes, int nboxes, cudaStream_t st);
+// variant: run length of the sweep kernel, 0 -> 1 face per thread,
+// 1 -> 2, 2 -> 4 (picked per scheme and direction by the engine's autotuner)
+constexpr int kInvVariants = 3;
+template <typename B>
+cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxes,
+                            const WorkItem *items, int nitems, int in_slot, int accumulate,
+                            cudaStream_t st);
+template <typename B>
+cudaError_t launch_visc_flux(const BoxDev *boxes, const WorkItem *items, int nitems,
+                             cudaStream_t st);
+template <typename B>
+cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems, StageArgs sa,
+                          bool any_viscous, cudaStream_t st);
+
+// CRWENO5 sweep of one box (crweno_kernels.cu), launched per box.
 struct StateView {
     const double *q[5];
 };
-struct StateViewMut {
-    double *q[5];
-};
 struct PrimView {
-    double *w[6];  // u, v, w, p, c, T  (FP64)
+    double *w[6];
 };
 template <typename B>
 struct BView {
     B *f[5];
 };
-template <typename B>
-struct BView9 {
-    B *f[9];
-};
-
-// Per-box scalars that live in device memory so a step never waits on the
-// host: dt of the current step, accumulated time, and per-step history.
-struct StepScalars {
-    double dt;
-    double dt_local;
-    double time;
-    double pad;
-    double dt_hist[kHistory];
-    double res_hist[kHistory];
-};
-
-cudaError_t launch_prim(const BoxParams &bp, StateView q, PrimView w, double *eig, int want_eig,
-                        int sms, cudaStream_t st);
-cudaError_t launch_dt(const BoxParams &bp, const double *eig, StepScalars *sc, int step,
-                      cudaStream_t st);
-template <typename B>
-cudaError_t launch_inviscid(const BoxParams &bp, int dir, StateView q, PrimView w, BView<B> r,
-                            int accumulate, cudaStream_t st);
-template <typename B>
-cudaError_t launch_visc_flux(const BoxParams &bp, PrimView w, BView9<B> vf, int sms,
-                             cudaStream_t st);
-// stage 0..2: TVD-RK3 update into uout; stage -1: uout receives the total RHS.
-template <typename B>
-cudaError_t launch_update(const BoxParams &bp, BView<B> r, BView9<B> vf, StateView un,
-                          StateView uin, StateViewMut uout, int stage, const StepScalars *sc,
-                          double *res_acc, unsigned *flags, int sms, cudaStream_t st);
-cudaError_t launch_residual(const BoxParams &bp, StepScalars *sc, double *res_acc, int step,
-                            cudaStream_t st);
-
-// CRWENO5 whole-box sweep (crweno_kernels.cu).  scratch: 2 * lines * n bulk
-// values for the forward-sweep coefficients.
 template <typename B>
 cudaError_t launch_crweno(const BoxParams &bp, int dir, StateView q, PrimView w, BView<B> r,
                           int accumulate, B *scratch, cudaStream_t st, int *nlaunch);

@@ -13,7 +13,7 @@ namespace nuc3d {
 
 namespace {
 
-constexpr int TX = 32, TY = 8, KZ = 32;
+constexpr int TX = kT25X, TY = kT25Y, KZ = kT25Z;
 
 // Asynchronous global->shared copy of one element (cp.async, L1-allocating),
 // so a plane's halo tile streams in while the previous plane is computed.
@@ -41,12 +41,20 @@ __device__ __forceinline__ double cd6d(double m3, double m2, double m1, double p
 // solveGrads + solveViscousFlux (NaiverStokes3d.cpp:87-303): CD6 gradients
 // of u, v, w, T (FP64 differences), stresses and heat flux in the bulk type,
 // written as tau_xx, tau_xy, tau_xz, tau_yy, tau_yz, tau_zz, E_x, E_y, E_z.
+// Work item: (box, x tile, y tile, z chunk).
 template <typename B>
-__global__ void __launch_bounds__(TX *TY) k_visc_flux25(BoxParams bp, PrimView w, BView9<B> vf) {
+__global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items) {
     __shared__ double sP[2][4][TY + 6][TX + 6];
+    const WorkItem it = items[blockIdx.x];
+    const BoxDev &bd = boxes[it.box];
+    if (!bd.active || !bd.p.navier_stokes) return;
+    const BoxParams &bp = bd.p;
+    const long long np = bd.np;
+    const double *const wbase = fieldW(bd, 0);
+    B *const vbase = fieldV<B>(bd, 0);
     const int nx = bp.n[0], ny = bp.n[1], nz = bp.n[2];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
+    const int i0 = it.a * TX, j0 = it.b * TY, k0 = it.c * KZ;
     const int i = i0 + tx, j = j0 + ty;
     const bool active = i < nx && j < ny;
     const long long sz = bp.stride[2];
@@ -58,7 +66,7 @@ __global__ void __launch_bounds__(TX *TY) k_visc_flux25(BoxParams bp, PrimView w
             int yy = t / (TX + 6), xx = t - yy * (TX + 6);
             long long g = plane + pmod(i0 - 3 + xx, nx) + (long long)nx * pmod(j0 - 3 + yy, ny);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) cp_async_elem(&sP[buf][f][yy][xx], w.w[src[f]] + g);
+            for (int f = 0; f < 4; ++f) cp_async_elem(&sP[buf][f][yy][xx], wbase + src[f] * np + g);
         }
     };
     const int kend = min(k0 + KZ, nz);
@@ -69,7 +77,7 @@ __global__ void __launch_bounds__(TX *TY) k_visc_flux25(BoxParams bp, PrimView w
     for (int s = 0; s < 6; ++s) {
         long long g = col + sz * pmod(k0 - 3 + s, nz);
 #pragma unroll
-        for (int f = 0; f < 4; ++f) qz[f][s] = active ? w.w[src[f]][g] : 0.0;
+        for (int f = 0; f < 4; ++f) qz[f][s] = active ? wbase[src[f] * np + g] : 0.0;
     }
     const double ix = bp.inv_d[0], iy = bp.inv_d[1], iz = bp.inv_d[2];
     const B c23 = B(2.0 / 3.0);
@@ -81,7 +89,7 @@ __global__ void __launch_bounds__(TX *TY) k_visc_flux25(BoxParams bp, PrimView w
         {
             long long g = col + sz * pmod(k + 3, nz);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) qz[f][6] = active ? w.w[src[f]][g] : 0.0;
+            for (int f = 0; f < 4; ++f) qz[f][6] = active ? wbase[src[f] * np + g] : 0.0;
         }
         cp_async_wait1();
         __syncthreads();
@@ -113,15 +121,15 @@ __global__ void __launch_bounds__(TX *TY) k_visc_flux25(BoxParams bp, PrimView w
             B t_zz = miu0 * (B(2) * wz - c23 * grad);
             B u = B(qz[0][3]), v = B(qz[1][3]), ww = B(qz[2][3]);
             long long g = col + sz * k;
-            vf.f[0][g] = t_xx;
-            vf.f[1][g] = t_xy;
-            vf.f[2][g] = t_xz;
-            vf.f[3][g] = t_yy;
-            vf.f[4][g] = t_yz;
-            vf.f[5][g] = t_zz;
-            vf.f[6][g] = u * t_xx + v * t_xy + ww * t_xz + coeff0 * tx_;
-            vf.f[7][g] = u * t_xy + v * t_yy + ww * t_yz + coeff0 * ty_;
-            vf.f[8][g] = u * t_xz + v * t_yz + ww * t_zz + coeff0 * tz_;
+            vbase[0 * np + g] = t_xx;
+            vbase[1 * np + g] = t_xy;
+            vbase[2 * np + g] = t_xz;
+            vbase[3 * np + g] = t_yy;
+            vbase[4 * np + g] = t_yz;
+            vbase[5 * np + g] = t_zz;
+            vbase[6 * np + g] = u * t_xx + v * t_xy + ww * t_xz + coeff0 * tx_;
+            vbase[7 * np + g] = u * t_xy + v * t_yy + ww * t_yz + coeff0 * ty_;
+            vbase[8 * np + g] = u * t_xz + v * t_yz + ww * t_zz + coeff0 * tz_;
         }
         __syncthreads();
 #pragma unroll
@@ -136,20 +144,34 @@ __global__ void __launch_bounds__(TX *TY) k_visc_flux25(BoxParams bp, PrimView w
 // TVD-RK3 stage (TVD-RK3.cpp:76-196, dQ/dt = -RHS) in FP64; on the last stage
 // also the residual sum of PDEData3d::setRES (PDEData3d.cpp:178-213).  Every
 // new state value passes a finite check.  stage = -1 writes the total RHS.
-template <typename B, bool VIS>
-__global__ void __launch_bounds__(TX *TY)
-    k_update25(BoxParams bp, BView<B> r, BView9<B> vf, StateView un, StateView uin,
-               StateViewMut uout, int stage, const StepScalars *sc, double *res_acc,
-               unsigned *flags) {
+// Work item: (box, x tile, y tile, z chunk).  ANYVIS: some box of the batch
+// is viscous (sizes the shared tiles); per box the viscous part runs only for
+// Navier-Stokes boxes.
+template <typename B, bool ANYVIS>
+__global__ void __launch_bounds__(TX *TY, 2)
+    k_update25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, StageArgs sa) {
     // x stencils: tau_xx, tau_xy, tau_xz, E_x; y: tau_xy, tau_yy, tau_yz, E_y;
     // z: tau_xz, tau_yz, tau_zz, E_z
-    __shared__ B sX[2][VIS ? 4 : 1][TY][TX + 6];
-    __shared__ B sY[2][VIS ? 4 : 1][TY + 6][TX];
+    __shared__ B sX[2][4][TY][TX + 6];
+    __shared__ B sY[2][4][TY + 6][TX];
     __shared__ double red[TX * TY / 32];
     const int cx[4] = {0, 1, 2, 6}, cy[4] = {1, 3, 4, 7}, cz[4] = {2, 4, 5, 8};
+    const WorkItem it = items[blockIdx.x];
+    const BoxDev &bd = boxes[it.box];
+    if (!bd.active) return;
+    const BoxParams &bp = bd.p;
+    const bool VIS = ANYVIS && bp.navier_stokes;
+    const long long np = bd.np;
+    const B *const rbase = fieldR<B>(bd, 0);
+    const B *const vbase = fieldV<B>(bd, 0);
+    const int stage = sa.stage;
+    const double *const unb = fieldU(bd, 0, 0);
+    const double *const uinb = fieldU(bd, stage < 0 ? 0 : sa.in_slot, 0);
+    double *const uoutb = stage < 0 ? nullptr : fieldU(bd, sa.out_slot, 0);
+    const StepScalars *sc = bd.sc;
     const int nx = bp.n[0], ny = bp.n[1], nz = bp.n[2];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
+    const int i0 = it.a * TX, j0 = it.b * TY, k0 = it.c * KZ;
     const int i = i0 + tx, j = j0 + ty;
     const bool active = i < nx && j < ny;
     const long long sz = bp.stride[2];
@@ -163,13 +185,13 @@ __global__ void __launch_bounds__(TX *TY)
             int yy = t / (TX + 6), xx = t - yy * (TX + 6);
             long long g = plane + pmod(i0 - 3 + xx, nx) + (long long)nx * pmod(j0 + yy, ny);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) cp_async_elem(&sX[buf][f][yy][xx], vf.f[cx[f]] + g);
+            for (int f = 0; f < 4; ++f) cp_async_elem(&sX[buf][f][yy][xx], vbase + cx[f] * np + g);
         }
         for (int t = tid; t < (TY + 6) * TX; t += TX * TY) {
             int yy = t / TX, xx = t - yy * TX;
             long long g = plane + pmod(i0 + xx, nx) + (long long)nx * pmod(j0 - 3 + yy, ny);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) cp_async_elem(&sY[buf][f][yy][xx], vf.f[cy[f]] + g);
+            for (int f = 0; f < 4; ++f) cp_async_elem(&sY[buf][f][yy][xx], vbase + cy[f] * np + g);
         }
     };
     B qz[4][7];
@@ -180,7 +202,7 @@ __global__ void __launch_bounds__(TX *TY)
         for (int s = 0; s < 6; ++s) {
             long long g = col + sz * pmod(k0 - 3 + s, nz);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) qz[f][s] = active ? vf.f[cz[f]][g] : B(0);
+            for (int f = 0; f < 4; ++f) qz[f][s] = active ? vbase[cz[f] * np + g] : B(0);
         }
     }
     double res = 0.0;
@@ -193,7 +215,7 @@ __global__ void __launch_bounds__(TX *TY)
             cp_async_commit();
             long long g6 = col + sz * pmod(k + 3, nz);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) qz[f][6] = active ? vf.f[cz[f]][g6] : B(0);
+            for (int f = 0; f < 4; ++f) qz[f][6] = active ? vbase[cz[f] * np + g6] : B(0);
         }
         // pointwise operands, loaded before the wait so their latency overlaps
         B R[5];
@@ -201,9 +223,9 @@ __global__ void __launch_bounds__(TX *TY)
         if (active) {
 #pragma unroll
             for (int e = 0; e < 5; ++e) {
-                R[e] = r.f[e][g];
-                if (stage >= 0) ui[e] = uin.q[e][g];
-                if (stage >= 1) u_n[e] = un.q[e][g];
+                R[e] = rbase[e * np + g];
+                if (stage >= 0) ui[e] = uinb[e * np + g];
+                if (stage >= 1) u_n[e] = unb[e * np + g];
             }
         }
         if (VIS) {
@@ -230,7 +252,7 @@ __global__ void __launch_bounds__(TX *TY)
             }
             if (stage < 0) {
 #pragma unroll
-                for (int e = 0; e < 5; ++e) uout.q[e][g] = double(R[e]);
+                for (int e = 0; e < 5; ++e) sa.rhs_out[5 * it.box + e][g] = double(R[e]);
             } else {
 #pragma unroll
                 for (int e = 0; e < 5; ++e) {
@@ -246,7 +268,7 @@ __global__ void __launch_bounds__(TX *TY)
                         res += dd * dd;
                     }
                     bad |= !isfinite(out);
-                    uout.q[e][g] = out;
+                    uoutb[e * np + g] = out;
                 }
             }
         }
@@ -258,51 +280,41 @@ __global__ void __launch_bounds__(TX *TY)
                 for (int f = 0; f < 4; ++f) qz[f][s] = qz[f][s + 1];
         }
     }
-    if (bad) atomicOr(flags, 1u);
+    if (bad) atomicOr(bd.flags, 1u);
     if (stage != 2) return;
     for (int o = 16; o > 0; o >>= 1) res += __shfl_xor_sync(0xffffffffu, res, o);
     if ((tid & 31) == 0) red[tid >> 5] = res;
     __syncthreads();
     if (tid == 0) {
         for (int w = 1; w < TX * TY / 32; ++w) res += red[w];
-        atomicAdd(res_acc, res);
+        atomicAdd(bd.res_acc, res);
     }
 }
 
-static dim3 grid25(const BoxParams &bp) {
-    return dim3((bp.n[0] + TX - 1) / TX, (bp.n[1] + TY - 1) / TY, (bp.n[2] + KZ - 1) / KZ);
-}
-
 template <typename B>
-cudaError_t launch_visc_flux(const BoxParams &bp, PrimView w, BView9<B> vf, int, cudaStream_t st) {
-    k_visc_flux25<B><<<grid25(bp), dim3(TX, TY), 0, st>>>(bp, w, vf);
+cudaError_t launch_visc_flux(const BoxDev *boxes, const WorkItem *items, int nitems,
+                             cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
+    k_visc_flux25<B><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items);
     return cudaGetLastError();
 }
 
 template <typename B>
-cudaError_t launch_update(const BoxParams &bp, BView<B> r, BView9<B> vf, StateView un,
-                          StateView uin, StateViewMut uout, int stage, const StepScalars *sc,
-                          double *res_acc, unsigned *flags, int, cudaStream_t st) {
-    if (bp.navier_stokes)
-        k_update25<B, true><<<grid25(bp), dim3(TX, TY), 0, st>>>(bp, r, vf, un, uin, uout, stage,
-                                                                 sc, res_acc, flags);
+cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems, StageArgs sa,
+                          bool any_viscous, cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
+    if (any_viscous)
+        k_update25<B, true><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items, sa);
     else
-        k_update25<B, false><<<grid25(bp), dim3(TX, TY), 0, st>>>(bp, r, vf, un, uin, uout, stage,
-                                                                  sc, res_acc, flags);
+        k_update25<B, false><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items, sa);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_visc_flux<double>(const BoxParams &, PrimView, BView9<double>, int,
-                                              cudaStream_t);
-template cudaError_t launch_visc_flux<float>(const BoxParams &, PrimView, BView9<float>, int,
-                                             cudaStream_t);
-template cudaError_t launch_update<double>(const BoxParams &, BView<double>, BView9<double>,
-                                           StateView, StateView, StateViewMut, int,
-                                           const StepScalars *, double *, unsigned *, int,
+template cudaError_t launch_visc_flux<double>(const BoxDev *, const WorkItem *, int, cudaStream_t);
+template cudaError_t launch_visc_flux<float>(const BoxDev *, const WorkItem *, int, cudaStream_t);
+template cudaError_t launch_update<double>(const BoxDev *, const WorkItem *, int, StageArgs, bool,
                                            cudaStream_t);
-template cudaError_t launch_update<float>(const BoxParams &, BView<float>, BView9<float>,
-                                          StateView, StateView, StateViewMut, int,
-                                          const StepScalars *, double *, unsigned *, int,
+template cudaError_t launch_update<float>(const BoxDev *, const WorkItem *, int, StageArgs, bool,
                                           cudaStream_t);
 
 }  // namespace nuc3d

@@ -86,6 +86,28 @@ def lib() -> C.CDLL:
         L.nuc3d_launch_count.restype = C.c_longlong
         L.nuc3d_launch_count.argtypes = [C.c_void_p]
         L.nuc3d_probe_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+        L.nuc3d_batch_create.argtypes = [C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]
+        L.nuc3d_batch_destroy.argtypes = [C.c_void_p]
+        L.nuc3d_batch_add.argtypes = [C.c_void_p, C.POINTER(_Desc), C.POINTER(C.c_int)]
+        for fn in ("remove", "sync"):
+            getattr(L, f"nuc3d_batch_{fn}").argtypes = (
+                [C.c_void_p, C.c_int] if fn == "remove" else [C.c_void_p])
+        L.nuc3d_batch_set_active.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.nuc3d_batch_set_cfl.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        for fn in ("set_state_host", "get_state_host", "set_state_device", "get_state_device"):
+            getattr(L, f"nuc3d_batch_{fn}").argtypes = [C.c_void_p, C.c_int, _P5]
+        L.nuc3d_batch_step.argtypes = [C.c_void_p, C.c_int]
+        L.nuc3d_batch_history.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        L.nuc3d_batch_box_steps.restype = C.c_longlong
+        L.nuc3d_batch_box_steps.argtypes = [C.c_void_p, C.c_int]
+        L.nuc3d_batch_time.restype = C.c_double
+        L.nuc3d_batch_time.argtypes = [C.c_void_p, C.c_int]
+        L.nuc3d_batch_profile_enable.argtypes = [C.c_void_p, C.c_int]
+        L.nuc3d_batch_profile_read.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.nuc3d_batch_launch_count.restype = C.c_longlong
+        L.nuc3d_batch_launch_count.argtypes = [C.c_void_p]
+        L.nuc3d_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nuc3d_batch_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.nuc3d_reconstruct.argtypes = [C.c_int, C.c_int, C.c_uint, C.c_int, C.c_int, C.c_int,
                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p]
@@ -256,6 +278,121 @@ class Solver:
 
     def launch_count(self) -> int:
         return int(lib().nuc3d_launch_count(self._h))
+
+    def tuning(self):
+        return _tuning(lib().nuc3d_tuning, self._h)
+
+
+class Batch:
+    """Many periodic boxes advanced together (nuc3d_batch): one kernel launch
+    per kernel class for all boxes, the step replayed as a CUDA graph."""
+
+    def __init__(self, precision=FP64, stream=None):
+        h = C.c_void_p()
+        check(lib().nuc3d_batch_create(int(precision), _stream_handle(stream), C.byref(h)))
+        self._h = h
+        self.precision = precision
+        self.descs = {}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().nuc3d_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, desc: BoxDesc) -> int:
+        d = replace(desc, precision=self.precision).c_struct()
+        bid = C.c_int(-1)
+        check(lib().nuc3d_batch_add(self._h, C.byref(d), C.byref(bid)))
+        self.descs[bid.value] = replace(desc, precision=self.precision)
+        return bid.value
+
+    def remove(self, bid: int):
+        check(lib().nuc3d_batch_remove(self._h, bid))
+        self.descs.pop(bid, None)
+
+    def set_active(self, bid: int, on: bool):
+        check(lib().nuc3d_batch_set_active(self._h, bid, int(on)))
+
+    def set_cfl(self, bid: int, cfl: float):
+        check(lib().nuc3d_batch_set_cfl(self._h, bid, cfl))
+
+    def set_state(self, bid: int, q):
+        if hasattr(q[0], "is_cuda") and q[0].is_cuda:
+            check(lib().nuc3d_batch_set_state_device(self._h, bid, _ptrs5(q)))
+        else:
+            check(lib().nuc3d_batch_set_state_host(self._h, bid, _ptrs5(q)))
+
+    def get_state(self, bid: int, out=None):
+        import numpy as np
+        if out is None:
+            out = [np.zeros(self.descs[bid].shape) for _ in range(5)]
+        if hasattr(out[0], "is_cuda") and out[0].is_cuda:
+            check(lib().nuc3d_batch_get_state_device(self._h, bid, _ptrs5(out)))
+        else:
+            check(lib().nuc3d_batch_get_state_host(self._h, bid, _ptrs5(out)))
+        return out
+
+    def step(self, nsteps: int = 1):
+        check(lib().nuc3d_batch_step(self._h, nsteps))
+
+    def history(self, bid: int, n: int):
+        import numpy as np
+        dt = np.zeros(max(n, 1))
+        res = np.zeros(max(n, 1))
+        check(lib().nuc3d_batch_history(self._h, bid, n, dt.ctypes.data, res.ctypes.data))
+        return dt[:n], res[:n]
+
+    def sync(self):
+        check(lib().nuc3d_batch_sync(self._h))
+
+    def box_steps(self, bid: int) -> int:
+        return int(lib().nuc3d_batch_box_steps(self._h, bid))
+
+    def time(self, bid: int) -> float:
+        return lib().nuc3d_batch_time(self._h, bid)
+
+    def profile(self, on: bool):
+        check(lib().nuc3d_batch_profile_enable(self._h, int(on)))
+
+    def profile_read(self, reset: bool = True):
+        import numpy as np
+        ms = np.zeros(PROF_CLASSES)
+        n = np.zeros(PROF_CLASSES, dtype=np.int64)
+        check(lib().nuc3d_batch_profile_read(self._h, ms.ctypes.data, n.ctypes.data, int(reset)))
+        return {name: (float(ms[i]), int(n[i])) for i, name in enumerate(PROF_NAMES)}
+
+    def launch_count(self) -> int:
+        return int(lib().nuc3d_batch_launch_count(self._h))
+
+    def tuning(self):
+        return _tuning(lib().nuc3d_batch_tuning, self._h)
+
+
+def _tuning(fn, h):
+    """{(scheme, dir): (chosen run length, {run length: ms per launch})}"""
+    import numpy as np
+    rl = np.zeros(6, dtype=np.int32)
+    ms = np.zeros(18)
+    check(fn(h, rl.ctypes.data, ms.ctypes.data))
+    out = {}
+    for s, sname in enumerate(("weno5js", "weno5z")):
+        for d, dname in enumerate("xyz"):
+            if rl[s * 3 + d]:
+                out[f"{sname}_{dname}"] = (int(rl[s * 3 + d]), {
+                    L: round(float(ms[(s * 3 + d) * 3 + v]), 4) for v, L in enumerate((1, 2, 4))})
+    return out
 
 
 def probe_peak(precision=FP64) -> float:
