@@ -60,9 +60,22 @@ FLOPS_INV_Z = 5 * (2 * 76 + 1 + 2) + 33
 FLOPS_INV_JS = 5 * (2 * 68 + 1 + 2) + 33
 FLOPS_PER_CELL_STAGE = 3 * FLOPS_INV_Z + 20 + 156 + 111  # + prim, viscous flux, update
 STATE_BYTES_PER_CELL_UPDATE = 320  # compulsory FP64 state traffic of 3 RK stages
-# DRAM bytes per launch of the inviscid sweep at 256^3, from the ncu capture
-# summarised in profiles/k_inviscid_weno5z_256.md (None until captured).
-INV_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) per launch of the FP64 WENO5-Z sweep at 256^3,
+# mean of x, y, z: the ncu capture at 128^3 in
+# profiles/k_inviscid_weno5z_fp64_128.md (186.4, 270.9, 278.2 MB) scaled by the
+# cell count (x8); the traffic of a sweep is proportional to the cells it
+# covers (whole lines, no halo growth with size along the other axes).
+INV_TRAFFIC_BYTES = 8 * (186.44e6 + 270.89e6 + 278.18e6) / 3
+INV_TRAFFIC_NOTE = "ncu dram__bytes_read+write of the 128^3 capture x8 (cells), mean of x/y/z"
+
+
+def hbm_peak_gbs():
+    """Measured copy bandwidth of this pool's B200s (MEASURED_PEAKS.json)."""
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
 
 
 def env_int(name, default):
@@ -258,6 +271,8 @@ def run_b200(args, rank, world, local_rank):
         "frac": achieved / peak64,
         "peak_source": "FP64 FMA rate measured in this run (nuc3d_probe_peak)",
         "traffic": INV_TRAFFIC_BYTES,
+        "traffic_source": INV_TRAFFIC_NOTE,
+        "traffic_gbs": INV_TRAFFIC_BYTES / (inv_avg_ms * 1e-3) / 1e9,
         "flops_per_launch": FLOPS_INV_Z * cells,
         "avg_launch_ms": inv_avg_ms,
         "share_of_step": inv_ms / total_ms if total_ms else None,
@@ -265,7 +280,9 @@ def run_b200(args, rank, world, local_rank):
         "autotuned_run_length": tuning64,
         "step_fp64_tflops": FLOPS_PER_CELL_STAGE * 3 * cells / (ms_per_step * 1e-3) / 1e12,
         "hbm_state_frac": STATE_BYTES_PER_CELL_UPDATE * cells / (ms_per_step * 1e-3) / 1e9
-                          / 6550.7,
+                          / hbm_peak_gbs()[0],
+        "hbm_peak_gbs": hbm_peak_gbs()[0],
+        "hbm_peak_source": hbm_peak_gbs()[1],
     }
 
     # ---- e2e through the C ABI with host buffers

@@ -31,6 +31,8 @@ extern "C" {
 #define NUC3D_ERR_NOMEM (-3)       /* device allocation failed */
 #define NUC3D_ERR_UNSUPPORTED (-4) /* scheme / model not available */
 #define NUC3D_ERR_NONFINITE (-5)   /* the state went NaN/Inf (finite check) */
+#define NUC3D_ERR_TIMEOUT (-6)     /* nuc3d_serve_wait: not finished in time */
+#define NUC3D_ERR_CANCELLED (-7)   /* solve dropped by nuc3d_serve_destroy */
 
 /* Reconstruction schemes: the Method.in strings weno5js, weno5z, crweno5
  * (fieldOperator.cpp:152-166). */
@@ -193,6 +195,103 @@ NUC3D_API int nuc3d_probe_peak(int precision, double *tflops);
  * may be NULL. */
 NUC3D_API int nuc3d_tuning(const nuc3d_ctx *ctx, int *run_len, double *ms);
 NUC3D_API int nuc3d_batch_tuning(const nuc3d_batch *b, int *run_len, double *ms);
+
+/* ---- initial states generated on the device ------------------------------
+ * NUC3D_INIT_TGV: block::initial_taylorgreen (block.cpp:359-395) on the cell
+ *   centres with origin 0.
+ * NUC3D_INIT_HIT: block::initial_hit (block.cpp:397-551): random-phase
+ *   solenoidal velocity with E(k) ~ (k/k_peak)^4 exp(-2 (k/k_peak)^2), real
+ *   part of the unnormalised backward transform, rescaled to
+ *   u_rms = mach_t / (sqrt(3) M) (the reference writes mach_t / (sqrt(3) M^2);
+ *   equal at M = 1); rho = 1, p = 1 / (gamma M^2).  The reference's phases
+ *   come from an unseeded std::random_device; here phase c (0..2) of the mode
+ *   at FFT index idx = i + nx (j + ny k) is output number 3 idx + c + 1 of the
+ *   splitmix64 stream seeded with `seed`, times 2 pi, so a seed reproduces the
+ *   field.  re_lambda > 0 sets the box's Reynolds number to
+ *   re_lambda / (u_rms lambda), lambda the Taylor microscale of the generated
+ *   field (postproc.cpp:871-872, spectral derivatives, rho = T = 1). */
+#define NUC3D_INIT_TGV 1
+#define NUC3D_INIT_HIT 2
+typedef struct nuc3d_init_desc {
+    int kind;                 /* NUC3D_INIT_TGV or NUC3D_INIT_HIT */
+    unsigned long long seed;  /* HIT phase stream */
+    double k_peak;            /* HIT spectrum peak wavenumber */
+    double mach_t;            /* HIT turbulent Mach number */
+    double re_lambda;         /* HIT: > 0 sets the Reynolds number from it */
+} nuc3d_init_desc;
+/* h_info (3 doubles, may be NULL): u_rms, Taylor microscale, the box's
+ * Reynolds number after the call (NaN for the first two with TGV). */
+NUC3D_API int nuc3d_init_state(nuc3d_ctx *ctx, const nuc3d_init_desc *init, double *h_info);
+NUC3D_API int nuc3d_batch_init_state(nuc3d_batch *b, int box_id, const nuc3d_init_desc *init,
+                                     double *h_info);
+
+/* ---- serving: a request loop over a batch ---------------------------------
+ * No counterpart in the reference, which runs one solve per process
+ * (NUC3d.cpp main -> singleBlock::solve).  A server owns one batch (one
+ * precision) on the device current at creation and one worker thread.
+ * nuc3d_serve_submit queues a solve from any thread.  The worker admits
+ * queued solves in submission order while the sum of the resident solves'
+ * device bytes (nuc3d_ctx_bytes of each) fits the budget and fewer than
+ * max_resident are resident; it allocates the box, uploads h_q0 or generates
+ * the initial state, and advances all resident solves together in chunks of
+ * steps (the batch's CUDA graph replayed; a chunk is no longer than the
+ * shortest remaining solve and about chunk_ms long), so solves join and leave
+ * the running batch between chunks (continuous batching).  A finished solve's
+ * state is copied to h_q_out, its memory released and its result posted.
+ * A solve gives the same final state alone and in any mix: no arithmetic
+ * crosses boxes and every kernel variant rounds identically. */
+typedef struct nuc3d_server nuc3d_server;
+
+typedef struct nuc3d_serve_config {
+    int precision;            /* NUC3D_FP64 or NUC3D_MIXED */
+    long long budget_bytes;   /* device bytes for resident solves; <= 0: 90 % of free */
+    int max_resident;         /* <= 0: 256 */
+    int max_chunk_steps;      /* <= 0: 64 */
+    double chunk_ms;          /* target device time of one chunk; <= 0: 20 ms */
+} nuc3d_serve_config;
+
+typedef struct nuc3d_solve_request {
+    nuc3d_box_desc desc;      /* precision is replaced by the server's */
+    int nsteps;               /* TVD-RK3 steps */
+    double cfl;
+    nuc3d_init_desc init;     /* init.kind 0: the state comes from h_q0 */
+    const double *h_q0[5];    /* host; must stay valid until the result is collected */
+    double *h_q_out[5];       /* host, written at completion (all NULL: not copied) */
+    long long tag;            /* returned in the result */
+} nuc3d_solve_request;
+
+typedef struct nuc3d_solve_result {
+    long long ticket, tag;
+    int status;               /* NUC3D_OK or the solve's error code */
+    int pad;
+    long long steps, cells;
+    double sim_time, dt_last, res_last;
+    double reynolds;          /* Reynolds number the solve ran with */
+    double t_submit, t_admit, t_done;  /* seconds on the server's clock */
+    char error[160];
+} nuc3d_solve_result;
+
+typedef struct nuc3d_serve_stats {
+    long long submitted, completed, failed;
+    int queued, resident, peak_resident, pad;
+    long long resident_bytes, peak_resident_bytes, budget_bytes;
+    long long batch_steps, chunks, cell_updates, launches;
+    double busy_s;            /* wall time spent advancing resident solves */
+    double now_s;             /* the server's clock */
+} nuc3d_serve_stats;
+
+NUC3D_API void nuc3d_serve_config_default(nuc3d_serve_config *cfg);
+NUC3D_API int nuc3d_serve_create(const nuc3d_serve_config *cfg, nuc3d_server **out);
+/* Cancels queued and resident solves (status NUC3D_ERR_CANCELLED) and joins
+ * the worker. */
+NUC3D_API int nuc3d_serve_destroy(nuc3d_server *s);
+NUC3D_API int nuc3d_serve_submit(nuc3d_server *s, const nuc3d_solve_request *req,
+                                 long long *ticket);
+/* Waits for solve `ticket` (ticket < 0: the next solve to finish) and
+ * collects its result; timeout_s < 0 waits without limit. */
+NUC3D_API int nuc3d_serve_wait(nuc3d_server *s, long long ticket, double timeout_s,
+                               nuc3d_solve_result *out);
+NUC3D_API int nuc3d_serve_info(nuc3d_server *s, nuc3d_serve_stats *out);
 
 /* Simulated time advanced by this context so far (block.cpp:208-209). */
 NUC3D_API double nuc3d_ctx_time(const nuc3d_ctx *ctx);

@@ -2,7 +2,7 @@
 
     python nuc3d-cartisian_b200/build.py [--force]
 
-Each .cu under csrc/ is compiled with nvcc (-gencode arch=compute_100a,
+Each .cu / .cpp under csrc/ is compiled with nvcc (-gencode arch=compute_100a,
 code=sm_100a -lineinfo -O3) in parallel and linked into one shared library
 whose C ABI is include/nuc3d_b200.h.  The toolchain's g++ links libstdc++
 statically; the link hides those symbols (--exclude-libs,ALL) so the library
@@ -25,7 +25,7 @@ CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "lib" / "libnuc3d_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden,-pthread",
               "--expt-relaxed-constexpr", "-I", str(ROOT / "include"), "-I", str(CSRC)]
 
 
@@ -37,7 +37,7 @@ def nvcc() -> str:
 
 
 def sources():
-    return sorted(CSRC.glob("*.cu"))
+    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
 
 
 def _stale(src: Path, obj: Path) -> bool:
@@ -65,7 +65,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         tmp = LIB.with_suffix(".so.tmp")
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs),
-               "-Xcompiler", "-static-libstdc++", "-Xlinker", "--exclude-libs,ALL",
+               "-Xcompiler", "-static-libstdc++,-pthread", "-Xlinker", "--exclude-libs,ALL",
                "-cudart", "static"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

@@ -197,6 +197,11 @@ int nuc3d_rhs(nuc3d_ctx *c, double *const d_rhs[5], double *h_dt_local) {
 
 double nuc3d_ctx_time(const nuc3d_ctx *c) { return c ? c->eng->time(c->id) : NAN; }
 
+int nuc3d_init_state(nuc3d_ctx *c, const nuc3d_init_desc *init, double *h_info) {
+    if (!c || !init) return fail(NUC3D_ERR_INVALID, "null argument");
+    return c->eng->init_state(c->id, *init, h_info);
+}
+
 int nuc3d_profile_enable(nuc3d_ctx *c, int on) {
     if (!c) return fail(NUC3D_ERR_INVALID, "null context");
     int rc = c->eng->profile_flush();
@@ -246,6 +251,11 @@ int nuc3d_batch_set_active(nuc3d_batch *b, int box_id, int active) {
 int nuc3d_batch_set_cfl(nuc3d_batch *b, int box_id, double cfl) {
     if (!b) return fail(NUC3D_ERR_INVALID, "null batch");
     return b->eng->set_cfl(box_id, cfl);
+}
+int nuc3d_batch_init_state(nuc3d_batch *b, int box_id, const nuc3d_init_desc *init,
+                           double *h_info) {
+    if (!b || !init) return fail(NUC3D_ERR_INVALID, "null argument");
+    return b->eng->init_state(box_id, *init, h_info);
 }
 int nuc3d_batch_set_state_host(nuc3d_batch *b, int box_id, const double *const h_q[5]) {
     if (!b) return fail(NUC3D_ERR_INVALID, "null batch");

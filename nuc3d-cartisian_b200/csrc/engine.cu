@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 
+#include "init_kernels.h"
 #include "op_kernels.h"
 
 namespace nuc3d {
@@ -603,6 +604,70 @@ int Engine::rhs(int id, double *const d_rhs[5], double *h_dt_local) {
         ECK(cudaMemcpyAsync(h_dt_local, &boxes_[id].dev.sc->dt_local, sizeof(double),
                             cudaMemcpyDeviceToHost, stream_));
         ECK(cudaStreamSynchronize(stream_));
+    }
+    return NUC3D_OK;
+}
+
+int Engine::init_state(int id, const nuc3d_init_desc &in, double info[3]) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
+        return set_last_error(NUC3D_ERR_INVALID, "no such box");
+    EngineBox &b = boxes_[id];
+    const BoxParams &p = b.dev.p;
+    if (in.kind == NUC3D_INIT_TGV) {
+        ECK(launch_init_tgv(b.dev, stream_));
+        ECK(cudaStreamSynchronize(stream_));
+        if (info) {
+            info[0] = info[1] = NAN;
+            info[2] = p.reynolds;
+        }
+        return NUC3D_OK;
+    }
+    if (in.kind != NUC3D_INIT_HIT) return set_last_error(NUC3D_ERR_INVALID, "unknown initial state kind");
+    if (!(in.k_peak > 0.0) || !(in.mach_t > 0.0))
+        return set_last_error(NUC3D_ERR_INVALID, "HIT needs k_peak > 0 and mach_t > 0");
+    for (int d = 0; d < 3; ++d)
+        if (hit_axis(p.n[d], 1.0, in.k_peak).M > 512)
+            return set_last_error(NUC3D_ERR_INVALID, "HIT k_peak too large (at most 512 modes per axis)");
+    // u_rms from the turbulent Mach number sqrt(3) u_rms / c with c = 1/M
+    // (block.cpp:422 writes Mt / M^2 / sqrt(3): the same at M = 1)
+    const double u_rms = in.mach_t / p.mach / std::sqrt(3.0);
+    void *scratch = nullptr;
+    double *d_sums = nullptr;
+    const size_t bytes = hit_scratch_bytes(p, in.k_peak);
+    cudaError_t e = cudaMallocAsync(&scratch, bytes + 256, stream_);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_last_error(NUC3D_ERR_NOMEM, "device allocation of the HIT scratch failed");
+    }
+    d_sums = reinterpret_cast<double *>(static_cast<char *>(scratch) + bytes);
+    double sums[6] = {};
+    e = launch_hit_synthesis(b.dev, b.desc.lx, b.desc.ly, b.desc.lz, in.seed, in.k_peak, u_rms,
+                             scratch, d_sums, stream_);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(sums, d_sums, sizeof sums, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    const double n = (double)p.N;
+    const double cur = std::sqrt((sums[0] / n + sums[1] / n + sums[2] / n) / 3.0);
+    const double scale = u_rms / cur;
+    if (e == cudaSuccess) e = launch_hit_finalize(b.dev, scale, stream_);
+    cudaError_t e2 = cudaFreeAsync(scratch, stream_);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    ECK(e);
+    // Taylor microscale and Re_lambda as postproc.cpp:871-872 with rho = 1, T = 1
+    const double u2 = (sums[0] / n + sums[1] / n + sums[2] / n) / 3.0 * scale * scale;
+    const double d2 = (sums[3] / n + sums[4] / n + sums[5] / n) / 3.0 * scale * scale;
+    const double lam = std::sqrt(u2 / d2), urms = std::sqrt(u2);
+    if (in.re_lambda > 0.0) {
+        const double re = in.re_lambda / (urms * lam);
+        b.desc.reynolds = re;
+        b.dev.p.reynolds = re;
+        dirty_ = true;
+    }
+    if (info) {
+        info[0] = urms;
+        info[1] = lam;
+        info[2] = b.dev.p.reynolds;
     }
     return NUC3D_OK;
 }

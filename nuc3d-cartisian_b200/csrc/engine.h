@@ -41,9 +41,16 @@ public:
     // dt / residual history of the last `n` steps of box id into host arrays
     int history(int id, int n, double *h_dt, double *h_res);
     int rhs(int id, double *const d_rhs[5], double *h_dt_local);
+    // Initial state of box id generated on the device (Taylor-Green or HIT);
+    // info (may be null): u_rms, Taylor microscale, Reynolds number.  A HIT
+    // request with re_lambda > 0 also sets the box's Reynolds number.
+    int init_state(int id, const nuc3d_init_desc &in, double info[3]);
     int sync_and_check(int id_or_all);
     double time(int id);
     long long box_steps(int id) const;
+    double reynolds(int id) const {
+        return id >= 0 && id < (int)boxes_.size() && boxes_[id].live ? boxes_[id].dev.p.reynolds : 0.0;
+    }
     int nboxes() const { return (int)boxes_.size(); }
     int precision() const { return precision_; }
     cudaStream_t stream() const { return stream_; }

@@ -18,6 +18,8 @@ PKG_ROOT = Path(__file__).resolve().parents[2]
 LIB_PATH = PKG_ROOT / "lib" / "libnuc3d_b200.so"
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2, -3, -4, -5
+ERR_TIMEOUT, ERR_CANCELLED = -6, -7
+INIT_STATE, INIT_TGV, INIT_HIT = 0, 1, 2
 WENO5JS, WENO5Z, CRWENO5 = 0, 1, 2
 SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5}
 EULER3D, NAVIERSTOKES3D = 0, 1
@@ -54,7 +56,43 @@ class _Desc(C.Structure):
     ]
 
 
+class _Init(C.Structure):
+    _fields_ = [("kind", C.c_int), ("seed", C.c_ulonglong), ("k_peak", C.c_double),
+                ("mach_t", C.c_double), ("re_lambda", C.c_double)]
+
+
 _P5 = C.c_void_p * 5
+
+
+class _ServeConfig(C.Structure):
+    _fields_ = [("precision", C.c_int), ("budget_bytes", C.c_longlong),
+                ("max_resident", C.c_int), ("max_chunk_steps", C.c_int),
+                ("chunk_ms", C.c_double)]
+
+
+class _Request(C.Structure):
+    _fields_ = [("desc", _Desc), ("nsteps", C.c_int), ("cfl", C.c_double), ("init", _Init),
+                ("h_q0", _P5), ("h_q_out", _P5), ("tag", C.c_longlong)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("ticket", C.c_longlong), ("tag", C.c_longlong), ("status", C.c_int),
+                ("pad", C.c_int), ("steps", C.c_longlong), ("cells", C.c_longlong),
+                ("sim_time", C.c_double), ("dt_last", C.c_double), ("res_last", C.c_double),
+                ("reynolds", C.c_double), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_done", C.c_double), ("error", C.c_char * 160)]
+
+
+class _ServeStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong),
+                ("failed", C.c_longlong), ("queued", C.c_int), ("resident", C.c_int),
+                ("peak_resident", C.c_int), ("pad", C.c_int), ("resident_bytes", C.c_longlong),
+                ("peak_resident_bytes", C.c_longlong), ("budget_bytes", C.c_longlong),
+                ("batch_steps", C.c_longlong), ("chunks", C.c_longlong),
+                ("cell_updates", C.c_longlong), ("launches", C.c_longlong),
+                ("busy_s", C.c_double), ("now_s", C.c_double)]
+
+
 _lib = None
 
 
@@ -108,6 +146,15 @@ def lib() -> C.CDLL:
         L.nuc3d_batch_launch_count.argtypes = [C.c_void_p]
         L.nuc3d_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.nuc3d_batch_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nuc3d_init_state.argtypes = [C.c_void_p, C.POINTER(_Init), C.c_void_p]
+        L.nuc3d_batch_init_state.argtypes = [C.c_void_p, C.c_int, C.POINTER(_Init), C.c_void_p]
+        L.nuc3d_serve_config_default.argtypes = [C.POINTER(_ServeConfig)]
+        L.nuc3d_serve_config_default.restype = None
+        L.nuc3d_serve_create.argtypes = [C.POINTER(_ServeConfig), C.POINTER(C.c_void_p)]
+        L.nuc3d_serve_destroy.argtypes = [C.c_void_p]
+        L.nuc3d_serve_submit.argtypes = [C.c_void_p, C.POINTER(_Request), C.POINTER(C.c_longlong)]
+        L.nuc3d_serve_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_double, C.POINTER(_Result)]
+        L.nuc3d_serve_info.argtypes = [C.c_void_p, C.POINTER(_ServeStats)]
         L.nuc3d_reconstruct.argtypes = [C.c_int, C.c_int, C.c_uint, C.c_int, C.c_int, C.c_int,
                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p]
@@ -195,6 +242,31 @@ def _stream_handle(stream) -> int:
     return int(stream)
 
 
+def _init_struct(init) -> "_Init":
+    """init: "tgv", or a dict {"kind": "hit", "seed", "k_peak", "mach_t",
+    "re_lambda"} (nuc3d_init_desc)."""
+    d = _Init()
+    if init == "tgv" or (isinstance(init, dict) and init.get("kind") == "tgv"):
+        d.kind = INIT_TGV
+        return d
+    if not isinstance(init, dict) or init.get("kind") != "hit":
+        raise ValueError(f"unknown initial state {init!r}")
+    d.kind = INIT_HIT
+    d.seed = int(init.get("seed", 0)) & 0xFFFFFFFFFFFFFFFF
+    d.k_peak = float(init.get("k_peak", 4.0))
+    d.mach_t = float(init.get("mach_t", 0.3))
+    d.re_lambda = float(init.get("re_lambda", 0.0) or 0.0)
+    return d
+
+
+def _init_info(fn, *args):
+    import numpy as np
+    info = np.zeros(3)
+    check(fn(*args, info.ctypes.data))
+    return {"u_rms": float(info[0]), "taylor_microscale": float(info[1]),
+            "reynolds": float(info[2])}
+
+
 class Solver:
     """One periodic box resident on the current CUDA device (nuc3d_ctx)."""
 
@@ -242,6 +314,15 @@ class Solver:
         else:
             check(lib().nuc3d_get_state_host(self._h, _ptrs5(out)))
         return out
+
+    def init_state(self, init):
+        """Generate the initial state on the device (nuc3d_init_state); a HIT
+        init with re_lambda > 0 also sets the Reynolds number (desc is
+        updated).  Returns {u_rms, taylor_microscale, reynolds}."""
+        d = _init_struct(init)
+        info = _init_info(lib().nuc3d_init_state, self._h, C.byref(d))
+        self.desc = replace(self.desc, reynolds=info["reynolds"])
+        return info
 
     def step(self, nsteps: int, cfl: float, stats: bool = True):
         import numpy as np
@@ -344,6 +425,13 @@ class Batch:
             check(lib().nuc3d_batch_get_state_host(self._h, bid, _ptrs5(out)))
         return out
 
+    def init_state(self, bid: int, init):
+        """nuc3d_batch_init_state; see Solver.init_state."""
+        d = _init_struct(init)
+        info = _init_info(lib().nuc3d_batch_init_state, self._h, bid, C.byref(d))
+        self.descs[bid] = replace(self.descs[bid], reynolds=info["reynolds"])
+        return info
+
     def step(self, nsteps: int = 1):
         check(lib().nuc3d_batch_step(self._h, nsteps))
 
@@ -378,6 +466,89 @@ class Batch:
 
     def tuning(self):
         return _tuning(lib().nuc3d_batch_tuning, self._h)
+
+
+class Server:
+    """Request loop over a batch (nuc3d_serve_*): solves are admitted by
+    device-memory budget, advanced together in chunks (continuous batching)
+    by a worker thread inside the library, and collected with wait()."""
+
+    def __init__(self, precision=MIXED, budget_bytes=0, max_resident=256, max_chunk_steps=64,
+                 chunk_ms=20.0):
+        cfg = _ServeConfig()
+        lib().nuc3d_serve_config_default(C.byref(cfg))
+        cfg.precision = int(precision)
+        cfg.budget_bytes = int(budget_bytes)
+        cfg.max_resident = int(max_resident)
+        cfg.max_chunk_steps = int(max_chunk_steps)
+        cfg.chunk_ms = float(chunk_ms)
+        h = C.c_void_p()
+        check(lib().nuc3d_serve_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.precision = precision
+        self._pending = {}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().nuc3d_serve_destroy(self._h)
+            self._h = C.c_void_p()
+            self._pending.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, desc: BoxDesc, nsteps: int, cfl: float = 0.5, q0=None, init=None,
+               want_state: bool = False, tag: int = 0) -> int:
+        """Queue one solve; q0 (5 host float64 arrays) or init ("tgv" or a
+        HIT dict, see Solver.init_state) gives its initial state.  Returns the
+        ticket."""
+        import numpy as np
+        r = _Request()
+        r.desc = replace(desc, precision=self.precision).c_struct()
+        r.nsteps = int(nsteps)
+        r.cfl = float(cfl)
+        r.tag = int(tag)
+        keep = []
+        if q0 is not None:
+            q0 = [np.ascontiguousarray(a, dtype=np.float64) for a in q0]
+            r.init.kind = INIT_STATE
+            r.h_q0 = _ptrs5(q0)
+            keep.append(q0)
+        else:
+            r.init = _init_struct(init)
+        out = None
+        if want_state:
+            out = [np.empty(desc.shape) for _ in range(5)]
+            r.h_q_out = _ptrs5(out)
+        t = C.c_longlong(-1)
+        check(lib().nuc3d_serve_submit(self._h, C.byref(r), C.byref(t)))
+        self._pending[t.value] = (keep, out)
+        return t.value
+
+    def wait(self, ticket: int = -1, timeout: float | None = None) -> dict:
+        """Collect the result of `ticket` (-1: the next to finish)."""
+        res = _Result()
+        check(lib().nuc3d_serve_wait(self._h, int(ticket), -1.0 if timeout is None else float(timeout),
+                                     C.byref(res)))
+        _, out = self._pending.pop(res.ticket, (None, None))
+        d = {k: getattr(res, k) for k, _ in _Result._fields_ if k not in ("pad", "error")}
+        d["error"] = res.error.decode(errors="replace")
+        d["state"] = out if res.status == OK else None
+        return d
+
+    def stats(self) -> dict:
+        st = _ServeStats()
+        check(lib().nuc3d_serve_info(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _ServeStats._fields_ if k != "pad"}
 
 
 def _tuning(fn, h):

@@ -7,8 +7,13 @@
   E(k) = u_rms^2 * 16 sqrt(2/pi) (k/kp)^4 / kp * exp(-2 (k/kp)^2), built by
   the Craya-Herring projection and an unnormalised backward FFT, rescaled to
   the target rms velocity.  The reference draws its phases from an unseeded
-  std::random_device; here they come from a seeded numpy PCG64 stream, so the
-  field is reproducible (and, like the reference's, not pinned to it).
+  std::random_device + mt19937 (three per mode, in index order); here phase c
+  of the mode at FFT index idx is the splitmix64 output number 3*idx + c + 1
+  of the stream seeded with `seed` (Steele, Lea & Flood, "Fast splittable
+  pseudorandom number generators", OOPSLA 2014), mapped to [0, 2 pi).  A
+  counter-based stream lets the device generator draw the same phases in any
+  order, so the host and device fields agree to rounding; like the
+  reference's field, neither is pinned to the reference's own draws.
 """
 
 from __future__ import annotations
@@ -39,6 +44,20 @@ def taylor_green(desc, origin=(0.0, 0.0, 0.0)):
     return [np.ascontiguousarray(a) for a in (rho0, rho0 * u0, rho0 * v0, rho0 * w0, rhoE)]
 
 
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+
+
+def splitmix_uniform(seed, n):
+    """Uniform [0, 1) doubles: output number n (uint64 array, n >= 1) of the
+    splitmix64 stream seeded with `seed`, top 53 bits."""
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed & 0xFFFFFFFFFFFFFFFF) + np.asarray(n, dtype=np.uint64) * _GOLDEN
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
 def _wavenumbers(n):
     k = np.arange(n, dtype=np.float64)
     return np.where(k >= n / 2.0, k - n, k)  # block.cpp:472-474
@@ -56,8 +75,9 @@ def hit_velocity(desc, seed=0, k_peak=4.0, u_rms=0.1):
     pie = 4.0 * math.atan(1.0)
     ek = u_rms ** 2 * 16.0 * math.sqrt(2.0 / pie) * (kmag / k_peak) ** 4 / k_peak * np.exp(
         -2.0 * kmag * kmag / k_peak / k_peak)
-    rng = np.random.Generator(np.random.PCG64(seed))
-    phi = rng.uniform(0.0, 2.0 * pie, size=(3,) + kmag.shape)
+    idx = np.arange(kmag.size, dtype=np.uint64).reshape(kmag.shape)  # i + nx (j + ny k)
+    phi = np.stack([2.0 * pie * splitmix_uniform(seed, np.uint64(3) * idx + np.uint64(c + 1))
+                    for c in range(3)])
     amp = np.sqrt(2.0 * ek / kmag / kmag / 4.0 / pie)
     a = amp * np.exp(1j * phi[0]) * np.cos(phi[2])
     b = amp * np.exp(1j * phi[1]) * np.sin(phi[2])

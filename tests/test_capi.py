@@ -68,3 +68,52 @@ def test_ctx_create_rejects_bad_descriptions_without_device():
         assert L.nuc3d_ctx_create(C.byref(d), None, C.byref(h)) in (nb.ERR_INVALID,
                                                                     nb.ERR_UNSUPPORTED)
         assert not h.value
+
+
+def _c_layout(struct, fields):
+    """sizeof and offsetof of a header struct, from a gcc-compiled probe."""
+    import shutil
+    import subprocess
+    import tempfile
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not available")
+    lines = [f'printf("%zu\\n", sizeof({struct}));']
+    lines += [f'printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
+    src = ("#include <stddef.h>\n#include <stdio.h>\n#include \"nuc3d_b200.h\"\n"
+           "int main(void) {\n" + "\n".join(lines) + "\nreturn 0; }\n")
+    with tempfile.TemporaryDirectory() as d:
+        c = Path(d) / "probe.c"
+        exe = Path(d) / "probe"
+        c.write_text(src)
+        subprocess.run(["gcc", "-I", str(HEADER.parent), str(c), "-o", str(exe)], check=True)
+        out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    vals = [int(v) for v in out.split()]
+    return vals[0], vals[1:]
+
+
+@pytest.mark.parametrize("cname,ctype", [
+    ("nuc3d_box_desc", "_Desc"), ("nuc3d_init_desc", "_Init"),
+    ("nuc3d_serve_config", "_ServeConfig"), ("nuc3d_solve_request", "_Request"),
+    ("nuc3d_solve_result", "_Result"), ("nuc3d_serve_stats", "_ServeStats"),
+])
+def test_binding_structs_match_the_header(cname, ctype):
+    ct = getattr(nb, ctype)
+    names = [f for f, _ in ct._fields_]
+    size, offs = _c_layout(cname, names)
+    assert size == C.sizeof(ct)
+    assert offs == [getattr(ct, f).offset for f in names]
+
+
+def test_serve_and_init_validation_without_device():
+    L = nb.lib()
+    cfg = nb._ServeConfig()
+    L.nuc3d_serve_config_default(C.byref(cfg))
+    assert cfg.precision == nb.MIXED and cfg.max_resident == 256 and cfg.chunk_ms == 20.0
+    cfg.precision = 7
+    h = C.c_void_p()
+    assert L.nuc3d_serve_create(C.byref(cfg), C.byref(h)) == nb.ERR_UNSUPPORTED
+    assert not h.value
+    assert L.nuc3d_serve_submit(None, None, None) == nb.ERR_INVALID
+    assert L.nuc3d_serve_wait(None, 0, 0.0, None) == nb.ERR_INVALID
+    assert L.nuc3d_init_state(None, None, None) == nb.ERR_INVALID
+    assert L.nuc3d_serve_destroy(None) == nb.OK
