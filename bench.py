@@ -352,6 +352,7 @@ def run_b200(args, rank, world, local_rank):
 
     ensemble = None if args.skip_ensemble else run_ensemble(args, stream, barrier, max_over_ranks,
                                                             world, rank)
+    served = None if (args.skip_serve or world > 1) else run_served(args)
 
     if rank != 0:
         if dist is not None:
@@ -384,6 +385,7 @@ def run_b200(args, rank, world, local_rank):
         "clocks": clock_info,
         "mixed": mixed,
         "ensemble": ensemble,
+        "served": served,
         "cpu_baseline": cpu,
     }
     if dist is not None:
@@ -395,7 +397,8 @@ def run_b200(args, rank, world, local_rank):
 def ensemble_boxes(nboxes, seed0):
     """The batched-ensemble workload: box edges drawn from {32,48,64,96,128},
     turbulent Mach U[0.1,0.5], Re_lambda U[40,120], WENO5-JS or WENO5-Z per
-    box, seeded ICs (box b uses seed seed0 + b)."""
+    box, seeded HIT initial states generated on the device (box b uses seed
+    seed0 + b).  Returns (desc, init) pairs."""
     import numpy as np
     import nuc3d_b200 as nb
     rng = np.random.default_rng(2024 + seed0)
@@ -406,9 +409,8 @@ def ensemble_boxes(nboxes, seed0):
         rl = float(rng.uniform(40.0, 120.0))
         scheme = nb.WENO5JS if rng.uniform() < 0.5 else nb.WENO5Z
         d = nb.BoxDesc(n, n, n, mach=1.0, scheme=(scheme,) * 3)
-        q, re = nb.hit_field(d, seed=seed0 + b, k_peak=K_PEAK, mach_t=mt, re_lambda=rl)
-        d.reynolds = re
-        out.append((d, q))
+        out.append((d, {"kind": "hit", "seed": seed0 + b, "k_peak": K_PEAK, "mach_t": mt,
+                        "re_lambda": rl}))
     return out
 
 
@@ -425,8 +427,8 @@ def run_ensemble(args, stream, barrier, max_over_ranks, world, rank):
     for name, prec in (("mixed", nb.MIXED), ("fp64", nb.FP64)):
         with nb.Batch(prec, stream=stream) as B:
             ids = [B.add(d) for d, _ in boxes]
-            for i, (_, q) in zip(ids, boxes):
-                B.set_state(i, q)
+            for i, (_, init) in zip(ids, boxes):
+                B.init_state(i, init)
             B.step(args.warmup)
             B.sync()
             barrier()
@@ -443,6 +445,103 @@ def run_ensemble(args, stream, barrier, max_over_ranks, world, rank):
                          "ms_per_step": ms / args.steps,
                          "launches_per_step": (B.launch_count() - l0) / args.steps}
     res["mixed_speedup_vs_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    return res
+
+
+# ------------------------------------------------------------- serving -----
+def served_requests(nreq, seed, rate):
+    """The served stream: Poisson arrivals (mean `rate` per second), box edge
+    log-uniform in [32, 192], steps log-uniform in [50, 1000], turbulent Mach
+    U[0.1, 0.6], Re_lambda U[40, 120], scheme WENO5-JS / WENO5-Z / CRWENO5,
+    seeded HIT initial state generated on the device."""
+    import numpy as np
+    import nuc3d_b200 as nb
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    t -= t[0]
+    out = []
+    for i in range(nreq):
+        n = int(round(math.exp(rng.uniform(math.log(32), math.log(192)))))
+        steps = int(round(math.exp(rng.uniform(math.log(50), math.log(1000)))))
+        mt = float(rng.uniform(0.1, 0.6))
+        rl = float(rng.uniform(40.0, 120.0))
+        scheme = (nb.WENO5JS, nb.WENO5Z, nb.CRWENO5)[int(rng.integers(3))]
+        d = nb.BoxDesc(n, n, n, mach=1.0, scheme=(scheme,) * 3)
+        out.append((float(t[i]), d, steps,
+                    {"kind": "hit", "seed": seed * 1000 + i, "k_peak": K_PEAK, "mach_t": mt,
+                     "re_lambda": rl}))
+    return out
+
+
+def run_stream(reqs, precision, max_resident, budget_bytes):
+    """Submits the requests at their arrival times to a fresh server and
+    collects every result (final state copied to the host) on a second
+    thread.  Latency = completion - submission on the server's clock."""
+    import threading
+    import nuc3d_b200 as nb
+    srv = nb.Server(precision=precision, budget_bytes=budget_bytes, max_resident=max_resident)
+    results = []
+    submitted = threading.Semaphore(0)
+
+    def collect():
+        for _ in reqs:
+            submitted.acquire()  # a solve is outstanding
+            r = srv.wait()
+            r.pop("state", None)
+            results.append(r)
+
+    th = threading.Thread(target=collect)
+    th.start()
+    t0 = time.perf_counter()
+    for ta, d, steps, init in reqs:
+        delay = t0 + ta - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        srv.submit(d, steps, CFL, init=init, want_state=True)
+        submitted.release()
+    th.join()
+    st = srv.stats()
+    srv.close()
+    ok = [r for r in results if r["status"] == nb.OK]
+    lat = sorted(r["t_done"] - r["t_submit"] for r in ok)
+    span = max(r["t_done"] for r in results) - min(r["t_submit"] for r in results)
+    pct = lambda q: lat[min(len(lat) - 1, int(math.ceil(q * len(lat))) - 1)] if lat else None  # noqa: E731
+    return {
+        "solves_per_s": len(ok) / span,
+        "p50_latency_s": pct(0.50),
+        "p99_latency_s": pct(0.99),
+        "mean_queue_s": sum(r["t_admit"] - r["t_submit"] for r in ok) / max(len(ok), 1),
+        "cell_updates_per_s": st["cell_updates"] / span,
+        "span_s": span,
+        "completed": len(ok),
+        "failed": len(results) - len(ok),
+        "peak_resident": st["peak_resident"],
+        "peak_resident_gb": st["peak_resident_bytes"] / 1e9,
+        "chunks": st["chunks"],
+        "kernel_launches": st["launches"],
+    }
+
+
+def run_served(args):
+    import nuc3d_b200 as nb
+    reqs = served_requests(args.serve_requests, 5, args.serve_rate)
+    budget = int(150e9)
+    work = sum(d.cells * steps for _, d, steps, _ in reqs)
+    res = {
+        "workload": f"served stream: {len(reqs)} solves, Poisson arrivals at {args.serve_rate:g}/s, "
+                    "box edge log-uniform 32-192, 50-1000 steps (log-uniform), Mt U[0.1,0.6], "
+                    "Re_lambda U[40,120], scheme WENO5-JS/WENO5-Z/CRWENO5, seeded HIT on device, "
+                    "final state copied to the host; HBM budget 150 GB",
+        "requests": len(reqs),
+        "cell_updates_requested": work,
+        "schemes": {k: sum(1 for _, d, _, _ in reqs if d.scheme[0] == v)
+                    for k, v in (("weno5js", nb.WENO5JS), ("weno5z", nb.WENO5Z),
+                                 ("crweno5", nb.CRWENO5))},
+        "mixed_continuous": run_stream(reqs, nb.MIXED, 256, budget),
+        "fp64_serial": run_stream(reqs, nb.FP64, 1, budget),
+    }
+    res["solves_per_s_ratio"] = (res["mixed_continuous"]["solves_per_s"]
+                                 / res["fp64_serial"]["solves_per_s"])
     return res
 
 
@@ -484,6 +583,9 @@ def main():
     ap.add_argument("--skip-ensemble", action="store_true")
     ap.add_argument("--ensemble-boxes", type=int, default=64)
     ap.add_argument("--accuracy-steps", type=int, default=100)
+    ap.add_argument("--skip-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="mean arrivals per second")
     ap.add_argument("--cpu-n", type=int, default=48, help="box edge of the CPU sample")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-workers", type=int, default=0)

@@ -1,20 +1,28 @@
-// CRWENO5 whole-box sweep: one thread per (line, equation) solves that
-// line's tridiagonal systems for F^+ and F^- and writes dF/dx.
+// CRWENO5 directional sweep, batched over boxes: one block per tile of
+// kCrTL lines of one box, one warp per (line, sign) tridiagonal system.
 //
 // Reference system (crweno5.cpp:45-402, quirk bit QK_CRWENO_BOUNDED set): on
 // a line of n cells, faces 0..2 and n-2..n take explicit WENO5-JS values
 // from the halo (crweno5.cpp:425-837); faces 3..n-3 solve a tridiagonal
 // system whose first and last rows are identity rows holding WENO5-JS values
-// and whose inner rows are the compact-WENO relation
-//   a F^_{i} + b F^_{i+1} + c F^_{i+2} = d   (row of cell i, face i+1)
-// by the Thomas sweep of crweno5.cpp:208-219.
-//
+// and whose inner rows are the compact-WENO relation of cell i (face i+1)
+//   lo F^_i + b F^_{i+1} + hi F^_{i+2} = d          (crweno5.cpp:136-161)
+// ('-' swaps lo and hi, crweno5.cpp:335-338).  The reference solves it with
+// a Thomas sweep (crweno5.cpp:208-219).
 // Periodic system (bit cleared; not in the reference): every face 0..n-1 is
-// a compact row and the system wraps around; it is solved by Sherman-Morrison
-// on top of the same Thomas sweep.
+// a compact row and the system wraps around (cyclic tridiagonal).
 //
-// Forward-sweep coefficients and the F^+ face values go to a scratch buffer
-// laid out [slot][row][thread] so a warp's accesses are contiguous.
+// Per block and equation: the split fluxes F+ and F- of the tile's lines
+// (3-cell periodic halo) are staged in shared memory; each half-warp solves
+// one (line, sign) system by a partitioned method — lane l eliminates the
+// interior rows of its segment so that every row depends only on the
+// segment's first and last unknowns (rows kept at unit diagonal), the 2P
+// segment-end unknowns form a tridiagonal (cyclic for periodic lines) system
+// that the half-warp solves by parallel cyclic reduction with shuffles, and
+// each lane back-substitutes its interior rows.  The compact rows are used
+// without normalising the weights (a row may be scaled freely), so a row
+// costs one reciprocal.  The face values overwrite the staged fluxes, and
+// the block writes dF/dx.
 #include "nuc3d_device.cuh"
 #include "rhs_kernels.h"
 
@@ -22,247 +30,405 @@ namespace nuc3d {
 
 namespace {
 
-// One compact-WENO row from the upwind-oriented stencil f0..f4 of its cell
-// (crweno5.cpp:136-161): returns the upwind-side coupling lo, the diagonal b,
-// the downwind-side coupling hi and the right-hand side d.
-template <typename B>
-__device__ __forceinline__ void crweno_row(B f0, B f1, B f2, B f3, B f4, B &lo, B &b, B &hi,
-                                           B &d) {
-    B is0, is1, is2;
-    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
-    const B ss = B(1.0e-6);
-    B r0 = B(1) / (ss + is0), r1 = B(1) / (ss + is1), r2 = B(1) / (ss + is2);
-    B a0 = B(K::CR0) * r0 * r0, a1 = B(K::CR1) * r1 * r1, a2 = B(K::CR2) * r2 * r2;
-    B inv = B(1) / (a0 + a1 + a2);
-    B w0 = a0 * inv, w1 = a1 * inv, w2 = a2 * inv;
-    lo = B(2.0 / 3.0) * w0 + B(1.0 / 3.0) * w1;
-    b = B(1.0 / 3.0) * w0 + B(2.0 / 3.0) * (w1 + w2);
-    hi = B(1.0 / 3.0) * w2;
-    d = B(1.0 / 6.0) * w0 * f1 + (B(5) * (w0 + w1) + w2) * f2 / B(6) + (w1 + B(5) * w2) * f3 / B(6);
+constexpr int kCrTL = 4;         // lines per block
+constexpr int kCrWarps = kCrTL;  // one warp per line: half-warp 0 solves F+, 1 solves F-
+constexpr int kCrThreads = 32 * kCrWarps;
+constexpr int kCrLanes = 16;     // lanes per system
+
+// CRWENO5 weights up to a common positive factor (crweno5.cpp:136-150:
+// alpha_k = c_k / (eps + beta_k)^2, eps = 1e-6, c = 0.2, 0.5, 0.3).  A compact
+// row is linear in the weights, so the normalisation by their sum is left
+// out: FP64 multiplies alpha_k through by the product of the squares (no
+// division at all); FP32 uses fast reciprocals.
+__device__ __forceinline__ void cr_alpha(double is0, double is1, double is2, double &a0,
+                                         double &a1, double &a2) {
+    const double ss = 1.0e-6;
+    double s0 = add_(ss, is0), s1 = add_(ss, is1), s2 = add_(ss, is2);
+    s0 = mul_(s0, s0);
+    s1 = mul_(s1, s1);
+    s2 = mul_(s2, s2);
+    a0 = mul_(K::CR0, mul_(s1, s2));
+    a1 = mul_(K::CR1, mul_(s0, s2));
+    a2 = mul_(K::CR2, mul_(s0, s1));
+}
+__device__ __forceinline__ void cr_alpha(float is0, float is1, float is2, float &a0, float &a1,
+                                         float &a2) {
+    const float ss = 1.0e-6f;
+    const float r0 = frcp_fast(add_(ss, is0)), r1 = frcp_fast(add_(ss, is1)),
+                r2 = frcp_fast(add_(ss, is2));
+    a0 = mul_(mul_(float(K::CR0), r0), r0);
+    a1 = mul_(mul_(float(K::CR1), r1), r1);
+    a2 = mul_(mul_(float(K::CR2), r2), r2);
 }
 
-template <int DIR>
-struct LineMap {
-    // line id -> base index; positions advance by bp.stride[DIR]
-    __device__ static long long base(const BoxParams &bp, long long L) {
-        if (DIR == 0) return L * bp.n[0];  // (j,k) rows are contiguous blocks of nx
-        if (DIR == 1) {
-            long long i = L % bp.n[0], k = L / bp.n[0];
-            return i + bp.stride[2] * k;
-        }
-        return L;  // (i,j): base = i + nx*j = L
-    }
-    __device__ static long long count(const BoxParams &bp) {
-        if (DIR == 0) return (long long)bp.n[1] * bp.n[2];
-        if (DIR == 1) return (long long)bp.n[0] * bp.n[2];
-        return (long long)bp.n[0] * bp.n[1];
-    }
-};
+// One compact-WENO row (scaled by the weights' sum) from the upwind-oriented
+// stencil f0..f4 of its cell: the upwind-side coupling lo, the diagonal b,
+// the downwind-side coupling hi and the right-hand side d
+// (crweno5.cpp:151-161).
+template <typename B>
+__device__ __forceinline__ void cr_row(B f0, B f1, B f2, B f3, B f4, B &lo, B &b, B &hi, B &d) {
+    B is0, is1, is2, w0, w1, w2;
+    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
+    cr_alpha(is0, is1, is2, w0, w1, w2);
+    const B third = B(1.0 / 3.0), two3 = B(2.0 / 3.0), sixth = B(1.0 / 6.0);
+    lo = fma_(two3, w0, mul_(third, w1));
+    b = fma_(third, w0, mul_(two3, add_(w1, w2)));
+    hi = mul_(third, w2);
+    d = fma_(mul_(sixth, add_(w1, mul_(B(5), w2))), f3,
+             fma_(mul_(sixth, add_(mul_(B(5), add_(w0, w1)), w2)), f2, mul_(mul_(sixth, w0), f1)));
+}
+
+__device__ __forceinline__ double rcp_(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp_(float x) { return frcp_fast(x); }
+
+template <typename B>
+__device__ __forceinline__ B shfl(B v, int src) {
+    return __shfl_sync(0xffffffffu, v, src);
+}
+
+// PCR update of a unit-diagonal row (a, 1, c | d) with its unit-diagonal
+// neighbours m (row i - s) and p (row i + s); the result is normalised again.
+template <typename B>
+__device__ __forceinline__ void pcr_update(B &a, B &c, B &d, B ma, B mc, B md, B pa, B pc, B pd) {
+    const B r = rcp_(B(1) - a * mc - c * pa);
+    const B nd = (d - a * md - c * pd) * r;
+    a = -a * ma * r;
+    c = -c * pc * r;
+    d = nd;
+}
 
 }  // namespace
 
+int crweno_lanes(int n, bool bounded) {
+    const int N = bounded ? n - 5 : n;
+    int P = 1;
+    while (P < kCrLanes && 2 * P <= N / 2) P *= 2;
+    return P;
+}
+
+int crweno_segment_rows(int n, bool bounded) {
+    const int N = bounded ? n - 5 : n;
+    const int P = crweno_lanes(n, bounded);
+    return (N + P - 1) / P;
+}
+
+size_t crweno_smem_bytes(int nmax, int ms, bool mixed) {
+    const size_t bs = mixed ? sizeof(float) : sizeof(double);
+    return bs * ((size_t)2 * kCrTL * (nmax + 6) + (size_t)kCrWarps * 3 * ms * 32);
+}
+
+int crweno_tile_lines() { return kCrTL; }
+
+// Work item (box, a, b, -): DIR 0: lines j = a*TL.., k = b; DIR 1: lines
+// i = a*TL.., k = b; DIR 2: lines i = a*TL.., j = b.
 template <typename B, int DIR>
-__global__ void __launch_bounds__(128)
-    k_crweno(BoxParams bp, StateView q, PrimView w, BView<B> r, int accumulate, B *scratch,
-             long long line0, long long chunk, int periodic) {
-    const long long T = 5 * chunk;  // threads in this launch
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= T) return;
-    const int e = (int)(t / chunk);
-    const long long L = line0 + (t - (long long)e * chunk);
-    if (L >= LineMap<DIR>::count(bp)) return;
+__global__ void __launch_bounds__(kCrThreads)
+    k_crweno_lines(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items,
+                   int in_slot, int accumulate, int nmax, int ms) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ls = nmax + 6;                           // staged cells per line
+    B *sF = reinterpret_cast<B *>(smem_raw);           // [sign][line][ls]
+    B *sRow = sF + 2 * kCrTL * ls;                     // [warp][3][ms][32]
+    __shared__ double sRef[2][kCrTL];
+
+    const WorkItem it = items[blockIdx.x];
+    const BoxDev &bd = boxes[it.box];
+    if (!bd.active) return;
+    const BoxParams &bp = bd.p;
+    const double *const qbase = fieldU(bd, in_slot, 0);
+    const double *const wbase = fieldW(bd, 0);
+    B *const rbase = fieldR<B>(bd, 0);
+    const long long np = bd.np;
     const int n = bp.n[DIR];
-    const long long s = bp.stride[DIR];
-    const long long base = LineMap<DIR>::base(bp, L);
+    const int l0 = it.a * kCrTL, fixed = it.b;
+    const int nl = DIR == 0 ? bp.n[1] : bp.n[0];
+    const long long sy = bp.stride[1], sz = bp.stride[2];
+    auto gidx = [&](int l, int pos) -> long long {
+        const int a = l0 + l;
+        if (DIR == 0) return pos + sy * a + sz * fixed;
+        if (DIR == 1) return a + sy * pos + sz * fixed;
+        return a + sy * fixed + sz * pos;
+    };
+    // Lax-Friedrichs split of equation e at cell g (physicsModel.cpp:546-565)
+    auto split = [&](int e, long long g, double &fp, double &fm) {
+        const double qe = qbase[e * np + g];
+        const double un = wbase[DIR * np + g], p = wbase[3 * np + g], c = wbase[4 * np + g];
+        const double lam = add_(fabs(un), c);
+        double f;
+        if (e == 4)
+            f = mul_(un, add_(qe, p));
+        else if (e == 1 + DIR)
+            f = fma_(un, qe, p);
+        else
+            f = mul_(un, qe);
+        const double t = mul_(lam, qe);
+        fp = mul_(0.5, add_(f, t));
+        fm = mul_(0.5, sub_(f, t));
+    };
     const bool mixed = sizeof(B) == sizeof(float);
-
-    // split flux F^+ (sg=+1) or F^- (sg=-1) of equation e at periodic cell c
-    auto fsplit = [&](int c, int sg) -> double {
-        c = ((c % n) + n) % n;
-        long long g = base + s * c;
-        double Qe = q.q[e][g];
-        double un = w.w[DIR][g], p = w.w[3][g], cs = w.w[4][g];
-        double lam = fabs(un) + cs;
-        double f = (e == 4) ? un * (Qe + p) : (e == 1 + DIR ? un * Qe + p : un * Qe);
-        return sg > 0 ? 0.5 * (f + lam * Qe) : 0.5 * (f - lam * Qe);
-    };
-    double ref[2] = {0.0, 0.0};
-    if (mixed) {
-        ref[0] = fsplit(0, 1);
-        ref[1] = fsplit(0, -1);
-    }
-    auto fb = [&](int c, int sg) -> B { return B(fsplit(c, sg) - ref[sg > 0 ? 0 : 1]); };
-    // explicit WENO5-JS face (upwind-oriented stencil)
-    auto js = [&](int m, int sg) -> B {
-        if (sg > 0) return weno5js_face(fb(m - 3, 1), fb(m - 2, 1), fb(m - 1, 1), fb(m, 1), fb(m + 1, 1));
-        return weno5js_face(fb(m + 2, -1), fb(m + 1, -1), fb(m, -1), fb(m - 1, -1), fb(m - 2, -1));
-    };
-    B *sc_c = scratch;                         // c' per row
-    B *sc_d = scratch + (size_t)(n + 1) * T;   // d' per row
-    B *sc_h = scratch + 2 * (size_t)(n + 1) * T;  // F^+ per face
-    B *sc_z = scratch + 3 * (size_t)(n + 1) * T;  // Sherman-Morrison second solve (periodic)
-    auto at = [&](B *slot, int row) -> B & { return slot[(size_t)row * T + t]; };
-
+    const bool bounded = (bp.quirks & QK_CRWENO_BOUNDED) != 0;
+    const int N = bounded ? n - 5 : n;  // unknowns of the system
+    int P = 1;  // lanes per system
+    while (P < kCrLanes && 2 * P <= N / 2) P *= 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sg = lane >> 4, hl = lane & 15;  // sign (0: +, 1: -) and lane within the system
+    B *const myF = sF + (sg * kCrTL + warp) * ls;  // cell c at [c + 3]; later face m at [m]
+    B *const wA = sRow + (size_t)warp * 3 * ms * 32;  // [j][lane]
+    B *const wC = wA + ms * 32;
+    B *const wD = wC + ms * 32;
     const B inv_d = B(bp.inv_d[DIR]);
-    B prev = B(0);  // F^ at face m+1 while walking down
-    for (int sgi = 0; sgi < 2; ++sgi) {
-        const int sg = sgi == 0 ? 1 : -1;
-        // row coefficients for cell i (row of face i+1)
-        auto row = [&](int i, B &a, B &b, B &c, B &d) {
-            B lo, hi;
-            if (sg > 0) {
-                crweno_row(fb(i - 2, 1), fb(i - 1, 1), fb(i, 1), fb(i + 1, 1), fb(i + 2, 1), lo, b, hi, d);
-                a = lo;  // couples face i   (crweno5.cpp:156)
-                c = hi;  // couples face i+2
-            } else {
-                crweno_row(fb(i + 3, -1), fb(i + 2, -1), fb(i + 1, -1), fb(i, -1), fb(i - 1, -1), lo, b, hi, d);
-                c = lo;  // crweno5.cpp:335
-                a = hi;  // crweno5.cpp:337
+
+    for (int e = 0; e < 5; ++e) {
+        if (mixed) {  // per-line reference: the split flux at cell 0
+            if (threadIdx.x < kCrTL) {
+                double fp = 0.0, fm = 0.0;
+                if (l0 + (int)threadIdx.x < nl) split(e, gidx(threadIdx.x, 0), fp, fm);
+                sRef[0][threadIdx.x] = fp;
+                sRef[1][threadIdx.x] = fm;
             }
-        };
-        // out(face) consumer: '+' stores, '-' combines and differentiates
-        auto emit = [&](int m, B v) {
-            if (sg > 0) {
-                at(sc_h, m) = v;
-            } else {
-                B fh = at(sc_h, m) + v;
-                if (m < n) {
-                    long long g = base + s * m;
-                    B dfe = (prev - fh) * inv_d;
-                    if (accumulate)
-                        r.f[e][g] += dfe;
-                    else
-                        r.f[e][g] = dfe;
-                }
-                prev = fh;
-            }
-        };
-        if (!periodic) {
-            const int M = n - 5;  // rows for cells 2..n-4 (faces 3..n-3)
-            // forward sweep (crweno5.cpp:208-212); row 0 is an identity row
-            B cp = B(0), dp = js(3, sg);
-            at(sc_c, 0) = cp;
-            at(sc_d, 0) = dp;
-            for (int rr = 1; rr < M; ++rr) {
-                B a, b, c, d;
-                if (rr == M - 1) {
-                    a = B(0); b = B(1); c = B(0); d = js(rr + 3, sg);
-                } else {
-                    row(rr + 2, a, b, c, d);
-                }
-                B den = b - cp * a;
-                cp = c / den;
-                dp = (d - dp * a) / den;
-                at(sc_c, rr) = cp;
-                at(sc_d, rr) = dp;
-            }
-            // walk faces n .. 0
-            for (int m = n; m >= n - 2; --m) emit(m, js(m, sg));
-            B x = at(sc_d, M - 1);
-            emit(n - 3, x);
-            for (int rr = M - 2; rr >= 0; --rr) {
-                x = at(sc_d, rr) - at(sc_c, rr) * x;
-                emit(rr + 3, x);
-            }
-            for (int m = 2; m >= 0; --m) emit(m, js(m, sg));
-        } else {
-            // cyclic rows for faces 0..n-1: row of face m belongs to cell m-1.
-            // Sherman-Morrison: A = T + u v^T with corner terms moved into u,v.
-            B a0, b0, c0, d0, an, bn, cn, dn;
-            row(-1, a0, b0, c0, d0);       // face 0
-            row(n - 2, an, bn, cn, dn);    // face n-1
-            const B gam = -b0;
-            // forward sweep for rhs d and rhs u = (gam, 0..0, cn) together
-            B cp, dp, zp;
-            {
-                B bb = b0 - gam;
-                cp = c0 / bb;
-                dp = d0 / bb;
-                zp = gam / bb;
-                at(sc_c, 0) = cp;
-                at(sc_d, 0) = dp;
-                at(sc_z, 0) = zp;
-            }
-            for (int m = 1; m < n; ++m) {
-                B a, b, c, d;
-                if (m == n - 1) {
-                    a = an; b = bn - a0 * cn / gam; c = cn; d = dn;
-                } else {
-                    row(m - 1, a, b, c, d);
-                }
-                B den = b - a * cp;
-                B u = (m == n - 1) ? cn : B(0);
-                cp = c / den;
-                dp = (d - a * dp) / den;
-                zp = (u - a * zp) / den;
-                at(sc_c, m) = cp;
-                at(sc_d, m) = dp;
-                at(sc_z, m) = zp;
-            }
-            // back substitution of both solves; keep x0, z0, x_{n-1}, z_{n-1}
-            B x = dp, z = zp;
-            at(sc_d, n - 1) = x;
-            at(sc_z, n - 1) = z;
-            for (int m = n - 2; m >= 0; --m) {
-                B cpm = at(sc_c, m);
-                x = at(sc_d, m) - cpm * x;
-                z = at(sc_z, m) - cpm * z;
-                at(sc_d, m) = x;
-                at(sc_z, m) = z;
-            }
-            B xl = at(sc_d, n - 1), zl = at(sc_z, n - 1);
-            B fact = (x + a0 * xl / gam) / (B(1) + z + a0 * zl / gam);
-            emit(n, at(sc_d, 0) - fact * at(sc_z, 0));  // face n == face 0
-            for (int m = n - 1; m >= 0; --m) emit(m, at(sc_d, m) - fact * at(sc_z, m));
+            __syncthreads();
         }
+        // stage F+ / F- of cells -3 .. n+2
+        const int nst = n + 6;
+        for (int t = threadIdx.x; t < kCrTL * nst; t += kCrThreads) {
+            int l, pc;
+            if (DIR == 0) {
+                l = t / nst;
+                pc = t - l * nst;
+            } else {
+                l = t % kCrTL;
+                pc = t / kCrTL;
+            }
+            double fp = 0.0, fm = 0.0;
+            if (l0 + l < nl) {
+                int pos = pc - 3;
+                pos = pos < 0 ? pos + n : (pos >= n ? pos - n : pos);
+                split(e, gidx(l, pos), fp, fm);
+                if (mixed) {
+                    fp = sub_(fp, sRef[0][l]);
+                    fm = sub_(fm, sRef[1][l]);
+                }
+            }
+            sF[l * ls + pc] = B(fp);
+            sF[(kCrTL + l) * ls + pc] = B(fm);
+        }
+        __syncthreads();
+
+        if (l0 + warp < nl) {  // warp-uniform
+            auto F = [&](int c) -> B { return myF[c + 3]; };
+            auto js = [&](int m) -> B {
+                return sg == 0 ? weno5js_face(F(m - 3), F(m - 2), F(m - 1), F(m), F(m + 1))
+                               : weno5js_face(F(m + 2), F(m + 1), F(m), F(m - 1), F(m - 2));
+            };
+            // explicit faces of the bounded system: 0, 1, 2, n-2, n-1, n
+            int xm = -1;
+            B xv = B(0);
+            if (bounded && hl < 6) {
+                xm = hl < 3 ? hl : n - 5 + hl;
+                xv = js(xm);
+            }
+            // segment of this lane: rows r0 .. r1 (at least 2)
+            const bool act = hl < P;
+            const int r0 = act ? (hl * N) / P : 0;
+            const int r1 = act ? ((hl + 1) * N) / P - 1 : 1;
+            const int L = r1 - r0 + 1;
+            B fa = B(0), fc = B(0), fd = B(0);  // reduced unit-diagonal row of x_first
+            B la = B(0), lc = B(0), ld = B(0);  // reduced unit-diagonal row of x_last
+            if (act) {
+                // window w[k] = F(i - 2 + k) of the current row's cell i (face i + 1)
+                int i = bounded ? r0 + 2 : r0 - 1;
+                B w[6];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) w[k] = F(i - 2 + k);
+                auto gen = [&](int r, B &a, B &b, B &c, B &d) {
+                    if (bounded && (r == 0 || r == N - 1)) {
+                        a = B(0);
+                        b = B(1);
+                        c = B(0);
+                        d = js(r + 3);
+                    } else if (sg == 0) {
+                        cr_row(w[0], w[1], w[2], w[3], w[4], a, b, c, d);
+                    } else {
+                        B lo, hi;
+                        cr_row(w[5], w[4], w[3], w[2], w[1], lo, b, hi, d);
+                        a = hi;
+                        c = lo;
+                    }
+                };
+                auto advance = [&]() {
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) w[k] = w[k + 1];
+                    ++i;
+                    w[5] = F(i + 3);
+                };
+                B a0, b0, c0, d0;
+                gen(r0, a0, b0, c0, d0);
+                // forward: row j -> A x_first + x_j + C x_{j+1} = D
+                B Ap = B(0), Cp = B(0), Dp = B(0);
+                for (int j = 1; j < L; ++j) {
+                    advance();
+                    B a, b, c, d;
+                    gen(r0 + j, a, b, c, d);
+                    B bpv = b, An = a, Dn = d;
+                    if (j > 1) {
+                        bpv = b - a * Cp;
+                        An = -a * Ap;
+                        Dn = d - a * Dp;
+                    }
+                    const B r = rcp_(bpv);
+                    Ap = An * r;
+                    Cp = c * r;
+                    Dp = Dn * r;
+                    wA[j * 32 + lane] = Ap;
+                    wC[j * 32 + lane] = Cp;
+                    wD[j * 32 + lane] = Dp;
+                }
+                la = Ap;
+                lc = Cp;
+                ld = Dp;
+                // backward: row j -> A x_first + x_j + C x_last = D
+                B bf = b0, cf = c0, df = d0;
+                if (L >= 3) {
+                    B An = wA[(L - 2) * 32 + lane], Cn = wC[(L - 2) * 32 + lane];
+                    B Dn = wD[(L - 2) * 32 + lane];
+                    for (int j = L - 3; j >= 1; --j) {
+                        const B k = wC[j * 32 + lane];
+                        An = wA[j * 32 + lane] - k * An;
+                        Cn = -k * Cn;
+                        Dn = wD[j * 32 + lane] - k * Dn;
+                        wA[j * 32 + lane] = An;
+                        wC[j * 32 + lane] = Cn;
+                        wD[j * 32 + lane] = Dn;
+                    }
+                    // row 0 minus c0 x (row 1)
+                    bf = b0 - c0 * An;
+                    cf = -c0 * Cn;
+                    df = d0 - c0 * Dn;
+                }
+                const B r = rcp_(bf);
+                fa = a0 * r;
+                fc = cf * r;
+                fd = df * r;
+            }
+            // parallel cyclic reduction of the 2P segment-end unknowns
+            // (reduced row 2l: x_first of lane l, 2l+1: x_last) within the half-warp
+            const int base = sg << 4;
+            for (int s = 1; s < 2 * P; s <<= 1) {
+                B fma_a, fma_c, fma_d, fpa, fpc, fpd;  // first's neighbours
+                B lma, lmc, lmd, lpa, lpc, lpd;        // last's neighbours
+                bool fm_ok, fp_ok, lm_ok, lp_ok;
+                if (s == 1) {
+                    const int sm = base + (hl - 1 + P) % P, sp = base + (hl + 1) % P;
+                    fma_a = shfl(la, sm);
+                    fma_c = shfl(lc, sm);
+                    fma_d = shfl(ld, sm);
+                    lpa = shfl(fa, sp);
+                    lpc = shfl(fc, sp);
+                    lpd = shfl(fd, sp);
+                    fpa = la;
+                    fpc = lc;
+                    fpd = ld;
+                    lma = fa;
+                    lmc = fc;
+                    lmd = fd;
+                    fm_ok = !bounded || hl >= 1;
+                    lp_ok = !bounded || hl + 1 < P;
+                    fp_ok = lm_ok = true;
+                } else {
+                    const int h = s >> 1;
+                    const int sm = base + (hl - h + P) % P, sp = base + (hl + h) % P;
+                    fma_a = shfl(fa, sm);
+                    fma_c = shfl(fc, sm);
+                    fma_d = shfl(fd, sm);
+                    fpa = shfl(fa, sp);
+                    fpc = shfl(fc, sp);
+                    fpd = shfl(fd, sp);
+                    lma = shfl(la, sm);
+                    lmc = shfl(lc, sm);
+                    lmd = shfl(ld, sm);
+                    lpa = shfl(la, sp);
+                    lpc = shfl(lc, sp);
+                    lpd = shfl(ld, sp);
+                    fm_ok = lm_ok = !bounded || hl >= h;
+                    fp_ok = lp_ok = !bounded || hl + h < P;
+                }
+                if (!fm_ok) fma_a = fma_c = fma_d = B(0);
+                if (!fp_ok) fpa = fpc = fpd = B(0);
+                if (!lm_ok) lma = lmc = lmd = B(0);
+                if (!lp_ok) lpa = lpc = lpd = B(0);
+                pcr_update(fa, fc, fd, fma_a, fma_c, fma_d, fpa, fpc, fpd);
+                pcr_update(la, lc, ld, lma, lmc, lmd, lpa, lpc, lpd);
+            }
+            const B xf = fd * rcp_(B(1) + fa + fc), xl = ld * rcp_(B(1) + la + lc);
+            __syncwarp();  // every lane has read its staged fluxes
+            if (act) {
+                const int off = bounded ? 3 : 0;
+                myF[r0 + off] = xf;
+                myF[r1 + off] = xl;
+                for (int j = 1; j < L - 1; ++j)
+                    myF[r0 + j + off] =
+                        wD[j * 32 + lane] - wA[j * 32 + lane] * xf - wC[j * 32 + lane] * xl;
+                if (!bounded && hl == 0) myF[n] = xf;  // face n is face 0
+            }
+            if (xm >= 0) myF[xm] = xv;
+        }
+        __syncthreads();
+        // dF/dx of the tile's cells from F^ = F^+ + F^- (euler3d.cpp:23-56, 143-253)
+        for (int t = threadIdx.x; t < kCrTL * n; t += kCrThreads) {
+            int l, i;
+            if (DIR == 0) {
+                l = t / n;
+                i = t - l * n;
+            } else {
+                l = t % kCrTL;
+                i = t / kCrTL;
+            }
+            if (l0 + l >= nl) continue;
+            const B *fp = sF + l * ls, *fm = sF + (kCrTL + l) * ls;
+            const B dfe = mul_(sub_(add_(fp[i + 1], fm[i + 1]), add_(fp[i], fm[i])), inv_d);
+            B *r = rbase + (long long)e * np + gidx(l, i);
+            *r = accumulate ? add_(*r, dfe) : dfe;
+        }
+        __syncthreads();
     }
 }
 
-size_t crweno_scratch_elems(const BoxParams &bp) {
-    // 4 slots x (n+1) rows x threads-per-chunk; chunk sized to keep the
-    // scratch near L2-resident (~64 MiB of FP64)
-    int nmax = bp.n[0] > bp.n[1] ? bp.n[0] : bp.n[1];
-    nmax = nmax > bp.n[2] ? nmax : bp.n[2];
-    long long per_thread = 4LL * (nmax + 1);
-    long long threads = (64LL << 20) / 8 / per_thread;
-    if (threads < 5 * 128) threads = 5 * 128;
-    return (size_t)(per_thread * threads);
+cudaError_t prepare_crweno_kernels(bool mixed) {
+    const int max_smem = 200 * 1024;  // above the largest need (164 KB at 512 cells, FP64)
+    cudaError_t e;
+    if (mixed) {
+        e = cudaFuncSetAttribute(k_crweno_lines<float, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_crweno_lines<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_crweno_lines<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    } else {
+        e = cudaFuncSetAttribute(k_crweno_lines<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_crweno_lines<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_crweno_lines<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    }
+    return e;
 }
 
 template <typename B>
-cudaError_t launch_crweno(const BoxParams &bp, int dir, StateView q, PrimView w, BView<B> r,
-                          int accumulate, B *scratch, cudaStream_t st, int *nlaunch) {
-    int n = bp.n[dir];
-    *nlaunch = 0;
-    if (n < 8) return cudaErrorInvalidValue;
-    int nmax = bp.n[0] > bp.n[1] ? bp.n[0] : bp.n[1];
-    nmax = nmax > bp.n[2] ? nmax : bp.n[2];
-    long long per_thread = 4LL * (nmax + 1);
-    long long threads = (long long)crweno_scratch_elems(bp) / per_thread;
-    long long chunk = threads / 5;
-    long long lines = dir == 0 ? (long long)bp.n[1] * bp.n[2]
-                               : (dir == 1 ? (long long)bp.n[0] * bp.n[2] : (long long)bp.n[0] * bp.n[1]);
-    if (chunk > lines) chunk = lines;
-    int periodic = (bp.quirks & QK_CRWENO_BOUNDED) ? 0 : 1;
-    for (long long l0 = 0; l0 < lines; l0 += chunk) {
-        long long T = 5 * chunk;
-        unsigned grid = (unsigned)((T + 127) / 128);
-        if (dir == 0)
-            k_crweno<B, 0><<<grid, 128, 0, st>>>(bp, q, w, r, accumulate, scratch, l0, chunk, periodic);
-        else if (dir == 1)
-            k_crweno<B, 1><<<grid, 128, 0, st>>>(bp, q, w, r, accumulate, scratch, l0, chunk, periodic);
-        else
-            k_crweno<B, 2><<<grid, 128, 0, st>>>(bp, q, w, r, accumulate, scratch, l0, chunk, periodic);
-        cudaError_t err = cudaGetLastError();
-        if (err != cudaSuccess) return err;
-        ++*nlaunch;
-    }
-    return cudaSuccess;
+cudaError_t launch_crweno(int dir, const BoxDev *boxes, const WorkItem *items, int nitems,
+                          int in_slot, int accumulate, int nmax, int ms, cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
+    const size_t smem = crweno_smem_bytes(nmax, ms, sizeof(B) == sizeof(float));
+    if (dir == 0)
+        k_crweno_lines<B, 0><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot, accumulate, nmax, ms);
+    else if (dir == 1)
+        k_crweno_lines<B, 1><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot, accumulate, nmax, ms);
+    else
+        k_crweno_lines<B, 2><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot, accumulate, nmax, ms);
+    return cudaGetLastError();
 }
 
-template cudaError_t launch_crweno<double>(const BoxParams &, int, StateView, PrimView,
-                                           BView<double>, int, double *, cudaStream_t, int *);
-template cudaError_t launch_crweno<float>(const BoxParams &, int, StateView, PrimView,
-                                          BView<float>, int, float *, cudaStream_t, int *);
+template cudaError_t launch_crweno<double>(int, const BoxDev *, const WorkItem *, int, int, int,
+                                           int, int, cudaStream_t);
+template cudaError_t launch_crweno<float>(int, const BoxDev *, const WorkItem *, int, int, int,
+                                          int, int, cudaStream_t);
 
 }  // namespace nuc3d

@@ -17,11 +17,6 @@ long long pad32(long long n) { return (n + 31) / 32 * 32; }
 size_t bulk_size(int precision) { return precision == NUC3D_MIXED ? sizeof(float) : sizeof(double); }
 constexpr size_t kSmallBytes = 256 + sizeof(StepScalars);
 
-bool has_crweno(const nuc3d_box_desc &d) {
-    return d.scheme[0] == NUC3D_CRWENO5 || d.scheme[1] == NUC3D_CRWENO5 ||
-           d.scheme[2] == NUC3D_CRWENO5;
-}
-
 BoxParams make_params(const nuc3d_box_desc &d) {
     BoxParams bp{};
     bp.n[0] = d.nx;
@@ -74,6 +69,9 @@ int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
         if (d.scheme[i] < NUC3D_WENO5JS || d.scheme[i] > NUC3D_CRWENO5)
             return bad(NUC3D_ERR_UNSUPPORTED, "unknown reconstruction scheme");
     }
+    for (int i = 0; i < 3; ++i)
+        if (d.scheme[i] == NUC3D_CRWENO5 && n[i] > kCrMaxCells)
+            return bad(NUC3D_ERR_UNSUPPORTED, "CRWENO5 lines are limited to 512 cells");
     if ((long long)d.nx * d.ny * d.nz > (1LL << 31)) return bad(NUC3D_ERR_INVALID, "box larger than 2^31 cells");
     if (!(d.lx > 0 && d.ly > 0 && d.lz > 0)) return bad(NUC3D_ERR_INVALID, "box lengths must be > 0");
     if (d.pde_model != NUC3D_EULER3D && d.pde_model != NUC3D_NAVIERSTOKES3D)
@@ -92,9 +90,7 @@ long long Engine::box_bytes(const nuc3d_box_desc &d) {
     BoxParams bp = make_params(d);
     long long np = pad32(bp.N);
     long long bs = (long long)bulk_size(d.precision);
-    long long b = 21 * np * 8 + 14 * np * bs + (long long)kSmallBytes;
-    if (has_crweno(d)) b += (long long)crweno_scratch_elems(bp) * bs;
-    return b;
+    return 21 * np * 8 + 14 * np * bs + (long long)kSmallBytes;
 }
 
 Engine::Engine(int precision, cudaStream_t stream) : precision_(precision), stream_(stream) {}
@@ -104,7 +100,6 @@ Engine::~Engine() {
     invalidate_graph();
     for (auto &b : boxes_) {
         if (b.mem) cudaFreeAsync(b.mem, stream_);
-        if (b.scratch) cudaFreeAsync(b.scratch, stream_);
     }
     if (d_boxes_) cudaFreeAsync(d_boxes_, stream_);
     if (d_items_) cudaFreeAsync(d_items_, stream_);
@@ -134,10 +129,7 @@ int Engine::add_box(const nuc3d_box_desc &d, int *id) {
     const size_t bs = bulk_size(precision_);
     const size_t bytes = sizeof(double) * 21 * (size_t)np + bs * 14 * (size_t)np + kSmallBytes;
     cudaError_t e = cudaMallocAsync(&b.mem, bytes, stream_);
-    if (e == cudaSuccess && has_crweno(d))
-        e = cudaMallocAsync(&b.scratch, bs * crweno_scratch_elems(b.dev.p), stream_);
     if (e != cudaSuccess) {
-        if (b.mem) cudaFreeAsync(b.mem, stream_);
         cudaGetLastError();
         return set_last_error(NUC3D_ERR_NOMEM,
                               (std::string("device allocation failed: ") + cudaGetErrorString(e)).c_str());
@@ -179,7 +171,6 @@ int Engine::remove_box(int id) {
         return set_last_error(NUC3D_ERR_INVALID, "no such box");
     EngineBox &b = boxes_[id];
     ECK(cudaFreeAsync(b.mem, stream_));
-    if (b.scratch) ECK(cudaFreeAsync(b.scratch, stream_));
     b = EngineBox();
     dirty_ = true;
     return NUC3D_OK;
@@ -241,8 +232,9 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));
     const bool mixed = precision_ == NUC3D_MIXED;
     std::vector<BoxDev> table(boxes_.size());
-    std::vector<WorkItem> prim, st25, inv[2][3];
-    crweno_boxes_.clear();
+    std::vector<WorkItem> prim, st25, inv[2][3], cr[3];
+    const int crtl = crweno_tile_lines();
+    for (int d = 0; d < 3; ++d) cr_nmax_[d] = cr_ms_[d] = 0;
     any_visc_ = false;
     nactive_ = 0;
     for (size_t i = 0; i < boxes_.size(); ++i) {
@@ -259,11 +251,23 @@ int Engine::rebuild() {
         for (int z = 0; z < ceil_div(p.n[2], kT25Z); ++z)
             for (int y = 0; y < ceil_div(p.n[1], kT25Y); ++y)
                 for (int x = 0; x < ceil_div(p.n[0], kT25X); ++x) st25.push_back({id, x, y, z});
-        bool cr = false;
         for (int d = 0; d < 3; ++d) {
             int s = p.scheme[d];
             if (s == SCHEME_CR) {
-                cr = true;
+                const bool bounded = (p.quirks & QK_CRWENO_BOUNDED) != 0;
+                cr_nmax_[d] = std::max(cr_nmax_[d], p.n[d]);
+                cr_ms_[d] = std::max(cr_ms_[d], crweno_segment_rows(p.n[d], bounded));
+                auto &L = cr[d];
+                if (d == 0) {
+                    for (int k = 0; k < p.n[2]; ++k)
+                        for (int g = 0; g < ceil_div(p.n[1], crtl); ++g) L.push_back({id, g, k, 0});
+                } else if (d == 1) {
+                    for (int k = 0; k < p.n[2]; ++k)
+                        for (int g = 0; g < ceil_div(p.n[0], crtl); ++g) L.push_back({id, g, k, 0});
+                } else {
+                    for (int j = 0; j < p.n[1]; ++j)
+                        for (int g = 0; g < ceil_div(p.n[0], crtl); ++g) L.push_back({id, g, j, 0});
+                }
                 continue;
             }
             InvTileDims t = inviscid_tile(d, mixed);
@@ -282,7 +286,6 @@ int Engine::rebuild() {
                         for (int a = 0; a < ceil_div(p.n[0], t.TL); ++a) L.push_back({id, a, j, c});
             }
         }
-        if (cr) crweno_boxes_.push_back(id);
     }
     std::vector<WorkItem> all;
     auto append = [&](const std::vector<WorkItem> &v, Range &r) {
@@ -294,6 +297,7 @@ int Engine::rebuild() {
     append(st25, r_25d_);
     for (int s = 0; s < 2; ++s)
         for (int d = 0; d < 3; ++d) append(inv[s][d], r_inv_[s][d]);
+    for (int d = 0; d < 3; ++d) append(cr[d], r_cr_[d]);
     if ((int)boxes_.size() > d_boxes_cap_) {
         if (d_boxes_) ECK(cudaFreeAsync(d_boxes_, stream_));
         if (d_rhs_ptrs_) ECK(cudaFreeAsync(d_rhs_ptrs_, stream_));
@@ -314,10 +318,12 @@ int Engine::rebuild() {
                             cudaMemcpyHostToDevice, stream_));
     ECK(cudaStreamSynchronize(stream_));  // host vectors go out of scope
     ECK(prepare_inviscid_kernels(mixed));
+    ECK(prepare_crweno_kernels(mixed));
     int per_stage = (r_prim_.n > 0) + (any_visc_ && r_25d_.n > 0) + (r_25d_.n > 0);
     for (int s = 0; s < 2; ++s)
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d].n > 0;
-    launches_per_step_ = 3 * per_stage + 3;  // + clear_eig, dt, residual (crweno counted live)
+    for (int d = 0; d < 3; ++d) per_stage += r_cr_[d].n > 0;
+    launches_per_step_ = 3 * per_stage + 3;  // + clear_eig, dt, residual
     dirty_ = false;
     return NUC3D_OK;
 }
@@ -388,20 +394,8 @@ int Engine::enqueue_step_t(cudaStream_t st) {
             for (int s = 0; s < 2; ++s)
                 ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
                                         r_inv_[s][d].n, in, d > 0, st)));
-            for (int id : crweno_boxes_) {
-                const EngineBox &b = boxes_[id];
-                if (b.dev.p.scheme[d] != SCHEME_CR) continue;
-                StateView q;
-                PrimView w;
-                BView<B> r;
-                for (int e = 0; e < 5; ++e) q.q[e] = fieldU(b.dev, in, e);
-                for (int i = 0; i < 6; ++i) w.w[i] = fieldW(b.dev, i);
-                for (int e = 0; e < 5; ++e) r.f[e] = fieldR<B>(b.dev, e);
-                int nl = 0;
-                ECK((launch_crweno<B>(b.dev.p, d, q, w, r, d > 0, static_cast<B *>(b.scratch),
-                                      st, &nl)));
-                launches += nl;
-            }
+            ECK((launch_crweno<B>(d, d_boxes_, it + r_cr_[d].off, r_cr_[d].n, in, d > 0,
+                                  cr_nmax_[d], cr_ms_[d], st)));
         }
         {
             ProfScope ps(this, NUC3D_PROF_UPDATE);
@@ -514,8 +508,6 @@ int Engine::step(int nsteps) {
             ECK(e);
             graph_ = g;
             ECK(cudaGraphInstantiate(&exec_, graph_, 0));
-            // crweno launches are counted while enqueuing; count them per replay
-            launches_per_step_ += (int)(launches - before);
             launches = before;
         }
         for (int s = 0; s < nsteps; ++s) ECK(cudaGraphLaunch(exec_, stream_));
@@ -564,19 +556,8 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
         for (int s = 0; s < 2; ++s)
             ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
                                     r_inv_[s][d].n, 0, d > 0, stream_)));
-        for (int cid : crweno_boxes_) {
-            const EngineBox &b = boxes_[cid];
-            if (b.dev.p.scheme[d] != SCHEME_CR) continue;
-            StateView q;
-            PrimView w;
-            BView<B> r;
-            for (int e = 0; e < 5; ++e) q.q[e] = fieldU(b.dev, 0, e);
-            for (int i = 0; i < 6; ++i) w.w[i] = fieldW(b.dev, i);
-            for (int e = 0; e < 5; ++e) r.f[e] = fieldR<B>(b.dev, e);
-            int nl = 0;
-            ECK((launch_crweno<B>(b.dev.p, d, q, w, r, d > 0, static_cast<B *>(b.scratch), stream_,
-                                  &nl)));
-        }
+        ECK((launch_crweno<B>(d, d_boxes_, it + r_cr_[d].off, r_cr_[d].n, 0, d > 0, cr_nmax_[d],
+                              cr_ms_[d], stream_)));
     }
     StageArgs sa{-1, 0, 0, d_rhs_ptrs_};
     ECK((launch_update<B>(d_boxes_, it + r_25d_.off, r_25d_.n, sa, any_visc_, stream_)));

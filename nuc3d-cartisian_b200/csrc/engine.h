@@ -18,7 +18,6 @@ struct EngineBox {
     nuc3d_box_desc desc{};
     BoxDev dev{};          // host copy of the box's table entry
     void *mem = nullptr;   // one stream-ordered allocation holding all fields
-    void *scratch = nullptr;
     double cfl = 0.5;
     long long steps = 0;   // host mirror of the device step counter
     bool live = false;     // slot in use
@@ -97,7 +96,8 @@ private:
         int n = 0;
     };
     Range r_prim_, r_25d_, r_inv_[2][3];  // [scheme JS/Z][dir]
-    std::vector<int> crweno_boxes_;
+    Range r_cr_[3];                       // CRWENO5 line tiles per dir
+    int cr_nmax_[3] = {0, 0, 0}, cr_ms_[3] = {0, 0, 0};
     int launches_per_step_ = 0;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;

@@ -111,20 +111,18 @@ template <typename B>
 cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems, StageArgs sa,
                           bool any_viscous, cudaStream_t st);
 
-// CRWENO5 sweep of one box (crweno_kernels.cu), launched per box.
-struct StateView {
-    const double *q[5];
-};
-struct PrimView {
-    double *w[6];
-};
+// CRWENO5 sweep (crweno_kernels.cu), batched: one work item per tile of
+// crweno_tile_lines() lines of one box.  nmax is the longest line among the
+// launch's boxes and ms = crweno_segment_rows of it (rows per lane of the
+// partitioned line solve); they size the dynamic shared memory.
+cudaError_t prepare_crweno_kernels(bool mixed);
+int crweno_tile_lines();
+int crweno_lanes(int n, bool bounded);
+int crweno_segment_rows(int n, bool bounded);
+size_t crweno_smem_bytes(int nmax, int ms, bool mixed);
+constexpr int kCrMaxCells = 512;  // longest CRWENO5 line (shared-memory bound)
 template <typename B>
-struct BView {
-    B *f[5];
-};
-template <typename B>
-cudaError_t launch_crweno(const BoxParams &bp, int dir, StateView q, PrimView w, BView<B> r,
-                          int accumulate, B *scratch, cudaStream_t st, int *nlaunch);
-size_t crweno_scratch_elems(const BoxParams &bp);
+cudaError_t launch_crweno(int dir, const BoxDev *boxes, const WorkItem *items, int nitems,
+                          int in_slot, int accumulate, int nmax, int ms, cudaStream_t st);
 
 }  // namespace nuc3d

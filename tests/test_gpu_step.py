@@ -86,6 +86,25 @@ def test_textbook_variants_match_oracle(torch, scheme):
     assert max_rel_l2(qg, qo) < TOL_FP64
 
 
+@pytest.mark.parametrize("bounded", [True, False])
+@pytest.mark.parametrize("shape", [(150, 70, 9), (512, 8, 11)])
+def test_crweno_long_lines_match_oracle(torch, bounded, shape):
+    """CRWENO5 lines of 8 to 512 cells: every partition of the warp's line
+    solve (1 to 32 lanes, segments of 2 to 16 rows), bounded (reference) and
+    periodic systems, against the oracle's Thomas / Sherman-Morrison sweeps."""
+    quirks = QUIRKS_REFERENCE if bounded else QUIRKS_REFERENCE & ~Q_CRWENO_BOUNDED
+    box = Box(*shape, scheme=(CRWENO5,) * 3, quirks=quirks, mach=0.2, reynolds=500.0)
+    rng = np.random.default_rng(sum(shape))
+    O = Oracle()
+    q = [a * (1 + 0.05 * rng.standard_normal(a.shape)) for a in O.tgv(box, (0.3, -0.1, 0.2))]
+    ref, dref = O.rhs(box, q)
+    got, dgot = gpu_rhs(torch, box, q)
+    assert max_rel_l2(got, ref) < TOL_FP64
+    qo, _, _ = O.run_steps(box, 0.5, 2, q)
+    qg, _, _ = gpu_steps(box, q, 2)
+    assert max_rel_l2(qg, qo) < TOL_FP64
+
+
 def test_mixed_schemes_per_direction_match_oracle(torch):
     box = Box(18, 14, 10, scheme=(WENO5Z, CRWENO5, WENO5JS), mach=0.15)
     O = Oracle()
@@ -113,16 +132,26 @@ def test_conservation_at_64(torch, scheme):
 
 def test_mixed_precision_close_to_fp64(torch):
     """FP32 bulk / FP64 state against the FP64 path on decaying isotropic
-    turbulence (M = 1, Mt = 0.3), 100 steps."""
+    turbulence (M = 1, Mt = 0.3, Re_lambda = 100, k_peak = 4), 100 steps:
+    per-field relative L2 below 1e-6 and kinetic energy within 0.5 %.  At
+    128^3 the field is resolved like the 256^3 benchmark case; on coarser
+    grids (32^3) WENO weight switching at shocklets amplifies the FP32
+    rounding locally and the error can reach a few 1e-6."""
     import nuc3d_b200 as nb
-    desc = nb.BoxDesc(32, 32, 32, mach=1.0, scheme=(nb.WENO5Z,) * 3)
-    q, re = nb.hit_field(desc, seed=1, k_peak=4.0, mach_t=0.3, re_lambda=100.0)
-    box = Box(32, 32, 32, scheme=(WENO5Z,) * 3, mach=1.0, reynolds=re)
-    q64, dt64, _ = gpu_steps(box, q, 100, precision=0)
-    q32, dt32, _ = gpu_steps(box, q, 100, precision=1)
+    desc = nb.BoxDesc(128, 128, 128, mach=1.0, scheme=(nb.WENO5Z,) * 3)
+    init = {"kind": "hit", "seed": 1, "k_peak": 4.0, "mach_t": 0.3, "re_lambda": 100.0}
+    out = []
+    for precision in (nb.FP64, nb.MIXED):
+        with nb.Solver(nb.BoxDesc(**{**desc.__dict__, "precision": precision})) as s:
+            s.init_state(init)
+            s.step(100, 0.5, stats=False)
+            out.append(s.get_state())
+    q64, q32 = out
     err = max_rel_l2(q32, q64)
+    ke = [0.5 * float(np.sum((q[1] ** 2 + q[2] ** 2 + q[3] ** 2) / q[0])) for q in (q32, q64)]
     print(f"mixed vs fp64 after 100 steps: max per-field rel L2 = {err:.3e}")
     assert err < 1e-6
+    assert abs(ke[0] - ke[1]) <= 5e-3 * ke[1]
 
 
 def test_nonfinite_state_is_reported(torch):
