@@ -322,20 +322,30 @@ def run_b200(args, rank, world, local_rank):
         prof_m = sm.profile_read(reset=True)
         sm.profile(False)
         sm.close()
-        # accuracy: 100 steps from the same state, both precisions
+        # accuracy: 100 steps from the same state, both precisions, with the
+        # device statistics (FP64 reductions) logged every 25 steps
         nacc = args.accuracy_steps
-        a64 = nb.Solver(desc, stream=stream)
-        a64.set_state(q)
-        a64.step(nacc, CFL, stats=False)
-        r64 = a64.get_state()
-        a64.close()
-        a32 = nb.Solver(dm, stream=stream)
-        a32.set_state(q)
-        a32.step(nacc, CFL, stats=False)
-        r32 = a32.get_state()
-        a32.close()
+        logs = {}
+        finals = {}
+        for name, d in (("fp64", desc), ("mixed", dm)):
+            with nb.Solver(d, stream=stream) as a:
+                a.set_state(q)
+                log = [a.stats()]
+                done = 0
+                while done < nacc:
+                    k = min(25, nacc - done)
+                    a.step(k, CFL, stats=False)
+                    done += k
+                    log.append(a.stats())
+                logs[name] = log
+                finals[name] = a.get_state()
+        r64, r32 = finals["fp64"], finals["mixed"]
         errs = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(r32, r64)]
-        ke = [0.5 * float(np.sum((r[1] ** 2 + r[2] ** 2 + r[3] ** 2) / r[0])) for r in (r32, r64)]
+        ke = [logs["mixed"][-1]["kinetic"], logs["fp64"][-1]["kinetic"]]
+
+        def max_rel(key):
+            return max(abs(m[key] - f[key]) / abs(f[key])
+                       for m, f in zip(logs["mixed"], logs["fp64"]))
         mixed = {
             "value": world * cells / (ms_m / args.steps * 1e-3),
             "ms_per_step": ms_m / args.steps,
@@ -344,6 +354,11 @@ def run_b200(args, rank, world, local_rank):
             "rel_l2_vs_fp64": max(errs),
             "rel_l2_per_field": errs,
             "tke_rel_diff": abs(ke[0] - ke[1]) / ke[1],
+            "tke_max_rel_diff_over_run": max_rel("kinetic"),
+            "dissipation_max_rel_diff_over_run": max_rel("dissipation"),
+            "stats_every_steps": 25,
+            "fp64_stats": {k: [round(v[k], 10) for v in logs["fp64"]]
+                           for k in ("kinetic", "dissipation", "enstrophy", "re_lambda", "mach_t")},
             "accuracy_steps": nacc,
             "peak_fp32_tflops": peak32,
             "kernel_ms_per_step": {k: v[0] / 2 for k, v in prof_m.items()},

@@ -293,6 +293,29 @@ NUC3D_API int nuc3d_serve_wait(nuc3d_server *s, long long ticket, double timeout
                                nuc3d_solve_result *out);
 NUC3D_API int nuc3d_serve_info(nuc3d_server *s, nuc3d_serve_stats *out);
 
+/* ---- turbulence statistics on the device (FP64) ---------------------------
+ * postproc::solveQ (postproc.cpp:736-930) of the box's current state, single
+ * rank: CD6 velocity gradients of the primitives, then the 16 averages of
+ * enstrophy.dat (indices 0..15: du/dx, du/dy, du/dz, dv/dx, dv/dy, dv/dz,
+ * dw/dx, dw/dy, dw/dz, omega_x, omega_y, omega_z, enstrophy |omega|^2/2,
+ * Q, helicity, kinetic energy rho|u|^2/2) and the 9 values of turb_para.dat
+ * (16..24: u_rms, turbulent Mach, sqrt(<(du_i/dx_i)^2>/3), mean Sutherland
+ * viscosity, Re_lambda, Taylor microscale, mean density, eddy turnover time,
+ * velocity-derivative skewness).  Index 25, not in the reference: the viscous
+ * dissipation <mu (|omega|^2 + 4/3 (div u)^2)> with the box's viscosity model.
+ * Synchronises; h_out receives NUC3D_STATS doubles. */
+#define NUC3D_STATS 26
+#define NUC3D_STAT_ENSTROPHY 12
+#define NUC3D_STAT_KINETIC 15
+#define NUC3D_STAT_U_RMS 16
+#define NUC3D_STAT_MACH_T 17
+#define NUC3D_STAT_RE_LAMBDA 20
+#define NUC3D_STAT_LAMBDA 21
+#define NUC3D_STAT_SKEWNESS 24
+#define NUC3D_STAT_DISSIPATION 25
+NUC3D_API int nuc3d_stats(nuc3d_ctx *ctx, double *h_out);
+NUC3D_API int nuc3d_batch_stats(nuc3d_batch *b, int box_id, double *h_out);
+
 /* Simulated time advanced by this context so far (block.cpp:208-209). */
 NUC3D_API double nuc3d_ctx_time(const nuc3d_ctx *ctx);
 

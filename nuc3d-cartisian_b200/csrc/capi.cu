@@ -197,6 +197,15 @@ int nuc3d_rhs(nuc3d_ctx *c, double *const d_rhs[5], double *h_dt_local) {
 
 double nuc3d_ctx_time(const nuc3d_ctx *c) { return c ? c->eng->time(c->id) : NAN; }
 
+int nuc3d_stats(nuc3d_ctx *c, double *h_out) {
+    if (!c || !h_out) return fail(NUC3D_ERR_INVALID, "null argument");
+    return c->eng->stats(c->id, h_out);
+}
+int nuc3d_batch_stats(nuc3d_batch *b, int box_id, double *h_out) {
+    if (!b || !h_out) return fail(NUC3D_ERR_INVALID, "null argument");
+    return b->eng->stats(box_id, h_out);
+}
+
 int nuc3d_init_state(nuc3d_ctx *c, const nuc3d_init_desc *init, double *h_info) {
     if (!c || !init) return fail(NUC3D_ERR_INVALID, "null argument");
     return c->eng->init_state(c->id, *init, h_info);

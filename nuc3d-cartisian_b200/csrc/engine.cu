@@ -7,6 +7,7 @@
 #include <cstring>
 
 #include "init_kernels.h"
+#include "stats_kernels.h"
 #include "op_kernels.h"
 
 namespace nuc3d {
@@ -104,6 +105,7 @@ Engine::~Engine() {
     if (d_boxes_) cudaFreeAsync(d_boxes_, stream_);
     if (d_items_) cudaFreeAsync(d_items_, stream_);
     if (d_rhs_ptrs_) cudaFreeAsync(d_rhs_ptrs_, stream_);
+    if (d_stats_) cudaFreeAsync(d_stats_, stream_);
     cudaStreamSynchronize(stream_);
     for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
     if (cap_stream_) cudaStreamDestroy(cap_stream_);
@@ -238,7 +240,7 @@ int Engine::rebuild() {
     any_visc_ = false;
     nactive_ = 0;
     for (size_t i = 0; i < boxes_.size(); ++i) {
-        const EngineBox &b = boxes_[i];
+        EngineBox &b = boxes_[i];
         table[i] = b.dev;
         if (!b.live) table[i].active = 0;
         if (!b.live || !b.dev.active) continue;
@@ -246,8 +248,10 @@ int Engine::rebuild() {
         const BoxParams &p = b.dev.p;
         const int id = (int)i;
         any_visc_ = any_visc_ || p.navier_stokes;
+        boxes_[i].prim_off = (int)prim.size();
         for (long long c = 0; c * kPrimChunk < p.N; ++c)
             prim.push_back({id, (int)c, (int)std::min<long long>(kPrimChunk, p.N - c * kPrimChunk), 0});
+        boxes_[i].prim_n = (int)prim.size() - boxes_[i].prim_off;
         for (int z = 0; z < ceil_div(p.n[2], kT25Z); ++z)
             for (int y = 0; y < ceil_div(p.n[1], kT25Y); ++y)
                 for (int x = 0; x < ceil_div(p.n[0], kT25X); ++x) st25.push_back({id, x, y, z});
@@ -650,6 +654,27 @@ int Engine::init_state(int id, const nuc3d_init_desc &in, double info[3]) {
         info[1] = lam;
         info[2] = b.dev.p.reynolds;
     }
+    return NUC3D_OK;
+}
+
+int Engine::stats(int id, double out[26]) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
+        return set_last_error(NUC3D_ERR_INVALID, "no such box");
+    if (!out) return set_last_error(NUC3D_ERR_INVALID, "null argument");
+    if (dirty_) {
+        int rc = rebuild();
+        if (rc) return rc;
+    }
+    EngineBox &b = boxes_[id];
+    if (!b.dev.active) return set_last_error(NUC3D_ERR_INVALID, "box is not active");
+    if (!d_stats_) ECK(cudaMallocAsync(&d_stats_, sizeof(double) * stats_scratch_doubles(), stream_));
+    // primitives of U[0] into W (scratch between steps), then the sums
+    ECK(launch_prim(d_boxes_, d_items_ + r_prim_.off + b.prim_off, b.prim_n, 0, 0, stream_));
+    ECK(launch_stats(b.dev, d_stats_, stream_));
+    double sums[kStatsSums];
+    ECK(cudaMemcpyAsync(sums, d_stats_, sizeof sums, cudaMemcpyDeviceToHost, stream_));
+    ECK(cudaStreamSynchronize(stream_));
+    stats_finish(b.dev.p, sums, out);
     return NUC3D_OK;
 }
 

@@ -17,6 +17,7 @@ namespace nuc3d {
 struct EngineBox {
     nuc3d_box_desc desc{};
     BoxDev dev{};          // host copy of the box's table entry
+    int prim_off = 0, prim_n = 0;  // the box's k_prim work items (set by rebuild)
     void *mem = nullptr;   // one stream-ordered allocation holding all fields
     double cfl = 0.5;
     long long steps = 0;   // host mirror of the device step counter
@@ -44,6 +45,8 @@ public:
     // info (may be null): u_rms, Taylor microscale, Reynolds number.  A HIT
     // request with re_lambda > 0 also sets the box's Reynolds number.
     int init_state(int id, const nuc3d_init_desc &in, double info[3]);
+    // Turbulence statistics of box id's current state (NUC3D_STATS values).
+    int stats(int id, double out[26]);
     int sync_and_check(int id_or_all);
     double time(int id);
     long long box_steps(int id) const;
@@ -103,6 +106,7 @@ private:
     cudaGraphExec_t exec_ = nullptr;
     cudaStream_t cap_stream_ = nullptr;  // graphs cannot be captured on the legacy stream
     double **d_rhs_ptrs_ = nullptr;  // 5 per box, for stage -1
+    double *d_stats_ = nullptr;       // statistics scratch
     // profiling events
     std::vector<cudaEvent_t> ev_pool_;
     struct Mark {

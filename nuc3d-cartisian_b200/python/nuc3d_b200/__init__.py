@@ -32,6 +32,11 @@ QUIRK_FABS_PRESSURE = 0x8
 QUIRK_CRWENO_BOUNDED = 0x10
 QUIRKS_REFERENCE = 0x1F
 PROF_NAMES = ("prim", "dt", "visc", "inv_x", "inv_y", "inv_z", "update", "residual")
+# nuc3d_stats indices (postproc::solveQ averages, turb_para.dat values, dissipation)
+STAT_NAMES = ("dudx", "dudy", "dudz", "dvdx", "dvdy", "dvdz", "dwdx", "dwdy", "dwdz",
+              "omega_x", "omega_y", "omega_z", "enstrophy", "q_criterion", "helicity", "kinetic",
+              "u_rms", "mach_t", "div_rms", "mu_mean", "re_lambda", "taylor_microscale",
+              "rho_mean", "eddy_turnover", "skewness", "dissipation")
 PROF_CLASSES = len(PROF_NAMES)
 
 
@@ -146,6 +151,8 @@ def lib() -> C.CDLL:
         L.nuc3d_batch_launch_count.argtypes = [C.c_void_p]
         L.nuc3d_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.nuc3d_batch_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nuc3d_stats.argtypes = [C.c_void_p, C.c_void_p]
+        L.nuc3d_batch_stats.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.nuc3d_init_state.argtypes = [C.c_void_p, C.POINTER(_Init), C.c_void_p]
         L.nuc3d_batch_init_state.argtypes = [C.c_void_p, C.c_int, C.POINTER(_Init), C.c_void_p]
         L.nuc3d_serve_config_default.argtypes = [C.POINTER(_ServeConfig)]
@@ -259,6 +266,13 @@ def _init_struct(init) -> "_Init":
     return d
 
 
+def _stats(fn, *args):
+    import numpy as np
+    out = np.zeros(len(STAT_NAMES))
+    check(fn(*args, out.ctypes.data))
+    return dict(zip(STAT_NAMES, (float(v) for v in out)))
+
+
 def _init_info(fn, *args):
     import numpy as np
     info = np.zeros(3)
@@ -323,6 +337,10 @@ class Solver:
         info = _init_info(lib().nuc3d_init_state, self._h, C.byref(d))
         self.desc = replace(self.desc, reynolds=info["reynolds"])
         return info
+
+    def stats(self) -> dict:
+        """Turbulence statistics of the current state (nuc3d_stats)."""
+        return _stats(lib().nuc3d_stats, self._h)
 
     def step(self, nsteps: int, cfl: float, stats: bool = True):
         import numpy as np
@@ -431,6 +449,10 @@ class Batch:
         info = _init_info(lib().nuc3d_batch_init_state, self._h, bid, C.byref(d))
         self.descs[bid] = replace(self.descs[bid], reynolds=info["reynolds"])
         return info
+
+    def stats(self, bid: int) -> dict:
+        """Turbulence statistics of box bid (nuc3d_batch_stats)."""
+        return _stats(lib().nuc3d_batch_stats, self._h, bid)
 
     def step(self, nsteps: int = 1):
         check(lib().nuc3d_batch_step(self._h, nsteps))

@@ -647,3 +647,83 @@ void or_init_tgv(const or_box *b, double x0, double y0, double z0, double *const
                 q[4][idx] = p0 / (gamma - 1.0) + 0.5 * rho0 * (u0 * u0 + v0 * v0 + w0 * w0);
             }
 }
+
+/* ---------------------------------------------------------- statistics --- */
+/* postproc::solveQ (postproc.cpp:736-930).  Gradients are CD6 of the
+ * primitives (solveGrad -> the operator's differential scheme, periodic
+ * halos); the per-cell expressions and the (k, j, i) summation order follow
+ * postproc.cpp:805-853, the field averages MPICommunicator.cpp:161-185. */
+void or_stats(const or_box *b, const double *const q[5], double out[OR_NSTATS]) {
+    const long N = (long)b->nx * b->ny * b->nz;
+    double *prim[8], *g[9], *qf[16];
+    double *blk_prim = alloc_fields(8, N, prim);
+    double *blk_g = alloc_fields(9, N, g);
+    double *blk_q = alloc_fields(16, N, qf);
+    or_con2prim(b, q, prim);
+    const double *src[3] = {prim[1], prim[2], prim[3]};
+    for (int v = 0; v < 3; ++v)
+        for (int d = 0; d < 3; ++d) cd6_direction(b, d, src[v], g[v * 3 + d]);
+    const double non_dim_T_ref = b->t_ref / b->t_inf;
+    double u_rms_aver = 0.0, miu_aver = 0.0, rho_bar = 0.0, div_aver = 0.0, alpha_aver = 0.0;
+    double Skew2 = 0.0, Skew3 = 0.0, diss = 0.0;
+    for (int k = 0; k < b->nz; ++k)
+        for (int j = 0; j < b->ny; ++j)
+            for (int i = 0; i < b->nx; ++i) {
+                long n = i + (long)b->nx * (j + (long)b->ny * k);
+                double u0 = prim[1][n], u1 = prim[2][n], u2 = prim[3][n];
+                double ux = g[0][n], uy = g[1][n], uz = g[2][n];
+                double vx = g[3][n], vy = g[4][n], vz = g[5][n];
+                double wx = g[6][n], wy = g[7][n], wz = g[8][n];
+                double w0 = wy - vz, w1 = uz - wx, w2 = vx - uy;
+                double q0 = ux * vy + ux * wz + vy * wz - uy * vx - uz * wx - vz * wy;
+                for (int c = 0; c < 9; ++c) qf[c][n] = g[c][n];
+                qf[9][n] = w0;
+                qf[10][n] = w1;
+                qf[11][n] = w2;
+                qf[12][n] = (w0 * w0 + w1 * w1 + w2 * w2) * 0.5;
+                qf[13][n] = q0;
+                qf[14][n] = w0 * u0 + w1 * u1 + w2 * u2;
+                qf[15][n] = 0.5 * prim[0][n] * (u0 * u0 + u1 * u1 + u2 * u2);
+                u_rms_aver += (u0 * u0 + u1 * u1 + u2 * u2) / 3.0;
+                div_aver += (ux * ux + vy * vy + wz * wz) / 3.0;
+                Skew3 += (pow(ux, 3.0) + pow(vy, 3.0) + pow(wz, 3.0)) / 3.0;
+                Skew2 += (ux * ux + vy * vy + wz * wz) / 3.0;
+                alpha_aver += prim[7][n];
+                double T = prim[5][n];
+                miu_aver += (1.0 + non_dim_T_ref) / (T + non_dim_T_ref) * pow(T, 1.5);
+                rho_bar += prim[0][n];
+                double miu, coeff, th = ux + vy + wz;
+                viscosity(b, T, &miu, &coeff);
+                diss += miu * (w0 * w0 + w1 * w1 + w2 * w2 + 4.0 / 3.0 * th * th);
+            }
+    for (int c = 0; c < 16; ++c) {
+        double sum = 0.0;
+        for (long n = 0; n < N; ++n) sum += qf[c][n];
+        out[c] = sum / (double)(int)N;
+    }
+    const double NN = (double)(int)N;
+    u_rms_aver /= NN;
+    div_aver /= NN;
+    miu_aver /= NN;
+    rho_bar /= NN;
+    Skew3 /= NN;
+    Skew2 /= NN;
+    alpha_aver /= NN;
+    double skew = Skew3 / pow(Skew2, 1.5);
+    double lambda = sqrt(u_rms_aver / div_aver);
+    double Re_lambda = sqrt(u_rms_aver) * lambda * rho_bar / miu_aver * b->reynolds;
+    double tau_t = lambda / sqrt(u_rms_aver);
+    out[16] = sqrt(u_rms_aver);
+    out[17] = sqrt(u_rms_aver * 3.0) / alpha_aver;
+    out[18] = sqrt(div_aver);
+    out[19] = miu_aver;
+    out[20] = Re_lambda;
+    out[21] = lambda;
+    out[22] = rho_bar;
+    out[23] = tau_t;
+    out[24] = skew;
+    out[25] = diss / NN;
+    free(blk_prim);
+    free(blk_g);
+    free(blk_q);
+}

@@ -82,6 +82,16 @@ double or_rhs(const or_box *b, const double *const q[5], double *const rhs[5]);
 void or_run_steps(const or_box *b, double cfl, int nsteps, double *const q[5], double *dt,
                   double *res);
 
+/* postproc::solveQ (postproc.cpp:736-930) of a periodic box, single rank:
+ *   out[0..15]  the averages written to enstrophy.dat: du/dx, du/dy, du/dz,
+ *               dv/dx .. dw/dz, omega0..2, enstrophy, Q, helicity, kinetic
+ *   out[16..24] turb_para.dat: u_rms, Mt, sqrt(div_aver), mu_aver,
+ *               Re_lambda, lambda, rho_bar, tau_t, skewness
+ *   out[25]     viscous dissipation <mu (|omega|^2 + 4/3 (div u)^2)>, mu of
+ *               the box's viscosity model (not in the reference) */
+#define OR_NSTATS 26
+void or_stats(const or_box *b, const double *const q[5], double out[OR_NSTATS]);
+
 /* Taylor-Green initial state (block.cpp:103-140, 359-395); x0,y0,z0 origin. */
 void or_init_tgv(const or_box *b, double x0, double y0, double z0, double *const q[5]);
 

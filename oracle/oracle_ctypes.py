@@ -174,6 +174,14 @@ class Oracle:
         self.lib.or_run_steps(C.byref(b), C.c_double(cfl), nsteps, _ptrs(q), _ptr(dt), _ptr(res))
         return q, dt, res
 
+    def stats(self, box: Box, q):
+        """or_stats: postproc::solveQ's averages and turb_para values plus the
+        dissipation (26 values, see nuc3d_oracle.h)."""
+        out = np.zeros(26)
+        b = box.c_struct()
+        self.lib.or_stats(C.byref(b), _ptrs([np.ascontiguousarray(a) for a in q]), _ptr(out))
+        return out
+
     def tgv(self, box: Box, origin=(0.0, 0.0, 0.0)):
         q = [np.zeros(box.shape) for _ in range(5)]
         b = box.c_struct()
@@ -199,6 +207,10 @@ def write_decks(dirpath: Path, box: Box, cfl: float = 0.5):
         f"PDEModel {model}\nViscousModel {VISC_NAMES[box.visc_model]}\nForcing None\n"
         f"Reynolds {box.reynolds!r}\nMach {box.mach!r}\nPt {box.prandtl!r}\n"
         f"Gamma {box.gamma!r}\nT_ref {box.t_ref!r}\nT_inf {box.t_inf!r}\n")
+    # postproc.cpp:35-58: no averaging, simultaneous Q statistics, no files
+    (inp / "PostProc.in").write_text(
+        "AverageType 0\nAverageStartStep 0\nSimutaneousData 1\nAveragedSaveType 0\n"
+        "SimutaneousSaveType 0\nFFTPost 0\n")
 
 
 class Reference:
@@ -253,6 +265,19 @@ class Reference:
                              C.c_double(box.dy), C.c_double(box.dz), _ptrs(q), _ptrs(out),
                              C.byref(dtl))
         return out, dtl.value
+
+    def stats(self, box: Box, q):
+        """postproc::solveQ of the reference (25 values: the 16 averages of
+        enstrophy.dat and the 9 turb_para.dat values, printed with 12
+        significant digits)."""
+        out = np.zeros(25)
+        with tempfile.TemporaryDirectory() as td:
+            write_decks(Path(td), box)
+            rc = self.lib.ref_stats(str(td).encode(), box.nx, box.ny, box.nz, C.c_double(box.dx),
+                                    C.c_double(box.dy), C.c_double(box.dz),
+                                    _ptrs([np.ascontiguousarray(a) for a in q]), _ptr(out))
+        assert rc == 0, rc
+        return out
 
     def run_steps(self, box: Box, cfl, nsteps, q):
         q = [np.ascontiguousarray(a, dtype=np.float64).copy() for a in q]

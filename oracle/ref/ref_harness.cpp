@@ -17,6 +17,8 @@
 //                     (NaiverStokes3d.cpp:37-73, euler3d.cpp:260-277)
 //   ref_run_steps     block::solve's stage loop (block.cpp:191-215) for
 //                     nsteps steps, PDEData3d::solve (PDEData3d.cpp:155-213)
+//   ref_stats         postproc::solveQ (postproc.cpp:736-930): the averages it
+//                     keeps and the turb_para.dat line it writes
 //
 // The solver classes read their decks from ./inp relative to the working
 // directory (fieldOperator.cpp:34, physicsModel.cpp:67), so the whole-step
@@ -41,6 +43,14 @@
 #include "physicsModel.h"
 #include "weno5js.h"
 #include "weno5z.hpp"
+// solveQ is declared under `private:`; the harness calls it directly
+// (access only, the class layout is unchanged).
+#define private public
+#include "postproc.hpp"
+#undef private
+
+#include <cstdio>
+#include <fstream>
 
 using nuc3d::Field;
 using nuc3d::VectorField;
@@ -226,6 +236,33 @@ int ref_run_steps(const char *workdir, int nx, int ny, int nz, double dx, double
         res[n] = s.pde.getRes();
     }
     s.store(q);
+    return 0;
+}
+
+// postproc::solveQ on q (istep 0, time 0).  out[0..15]: the 16 field
+// averages of enstrophy.dat; out[16..24]: the turb_para.dat values; both read
+// back from the files solveQ writes (12 significant digits).  The workdir
+// needs inp/PostProc.in with SimutaneousData 1.
+int ref_stats(const char *workdir, int nx, int ny, int nz, double dx, double dy, double dz,
+              const double *const q[5], double *out) {
+    Cwd cwd(workdir);
+    RefSolver s(nx, ny, nz, dx, dy, dz);
+    s.load(q);
+    VectorField prim(5, Field(nx, ny, nz)), acou(3, Field(nx, ny, nz));
+    s.phys.getPrim(s.pde.getQ(), prim, acou);
+    nuc3d::postproc post(nx, ny, nz, dx, dy, dz);
+    std::remove("enstrophy.dat");
+    std::remove("turb_para.dat");
+    post.solveQ(prim, acou, s.phys, s.op, s.buffers, s.mpi, 0, 0.0);
+    double step, time;
+    std::ifstream fq("enstrophy.dat");
+    if (!(fq >> step >> time)) return -1;
+    for (int i = 0; i < 16; ++i)
+        if (!(fq >> out[i])) return -2;
+    std::ifstream f("turb_para.dat");
+    if (!(f >> step >> time)) return -3;
+    for (int i = 0; i < 9; ++i)
+        if (!(f >> out[16 + i])) return -4;
     return 0;
 }
 

@@ -91,7 +91,20 @@ def main():
     q0 = Oracle().tgv(box)
     qn, dt, res = R.run_steps(box, 0.5, 10, q0)
     np.savez_compressed(HERE / "tgv24_js_10.npz", q10=np.stack(qn), dt=dt, res=res)
+    stats_fixture(R)
     print("fixtures written to", HERE)
+
+
+def stats_fixture(R):
+    """postproc::solveQ of the reference (postproc.cpp:736-930) on a perturbed
+    non-cubic TGV: the 16 averages of enstrophy.dat and the 9 turb_para.dat
+    values (printed by the reference with 12 significant digits)."""
+    box = Box(24, 20, 16, scheme=(WENO5Z,) * 3, mach=0.3, reynolds=400.0)
+    q = perturbed_tgv(box, 3)
+    out = R.stats(box, q)
+    np.savez_compressed(HERE / "stats.npz", q=np.stack(q), stats=out,
+                        shape=np.array(box.shape), mach=box.mach, reynolds=box.reynolds,
+                        prandtl=box.prandtl)
 
 
 if __name__ == "__main__":

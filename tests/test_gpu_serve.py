@@ -151,3 +151,34 @@ def _alone_state(nb, d, q0, n, cfl):
         s.set_state(q0)
         s.step(n, cfl, stats=False)
         return s.get_state(), None
+
+
+def test_device_stats_match_reference_and_oracle(nb):
+    """nuc3d_stats against the reference's solveQ (golden, 12 printed digits)
+    and the oracle (dissipation, not in the reference)."""
+    from helpers import golden
+    from oracle_ctypes import Box, Oracle, WENO5Z
+    z = golden("stats.npz")
+    nz, ny, nx = (int(v) for v in z["shape"])
+    box = Box(nx, ny, nz, scheme=(WENO5Z,) * 3, mach=float(z["mach"]),
+              reynolds=float(z["reynolds"]), prandtl=float(z["prandtl"]))
+    d = nb.BoxDesc(nx, ny, nz, scheme=(nb.WENO5Z,) * 3, mach=box.mach, reynolds=box.reynolds,
+                   prandtl=box.prandtl)
+    q = [np.ascontiguousarray(a) for a in z["q"]]
+    with nb.Solver(d) as s:
+        s.set_state(q)
+        st = s.stats()
+    got = np.array([st[k] for k in nb.STAT_NAMES])
+    ref = z["stats"]
+    # the averages of the nine gradients and three vorticity components are
+    # summation noise around 0 (periodic box): compare them on the scale of
+    # the gradients themselves
+    # (so is the average of Q, a divergence): compare those on the scale of
+    # the gradients themselves
+    scale = float(ref[18])  # sqrt(<(du_i/dx_i)^2>/3)
+    assert np.all(np.abs(got[:12] - ref[:12]) <= 1e-13 * scale)
+    assert abs(got[13] - ref[13]) <= 1e-12 * scale * scale
+    keep = [12] + list(range(14, 25))
+    np.testing.assert_allclose(got[keep], ref[keep], rtol=1e-10)
+    o = Oracle().stats(box, q)
+    np.testing.assert_allclose(got[25], o[25], rtol=1e-12)

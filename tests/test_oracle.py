@@ -115,3 +115,16 @@ def test_oracle_weno_z_quirk_changes_only_inner_plus_faces(O):
     am = O.reconstruct_field(WENO5Z, -1, QUIRKS_REFERENCE, f, hl, hr)
     bm = O.reconstruct_field(WENO5Z, -1, QUIRKS_REFERENCE & ~Q_WENOZ_BETA2, f, hl, hr)
     assert np.array_equal(am, bm)
+
+
+def test_stats_match_reference_golden(O):
+    """postproc::solveQ (postproc.cpp:736-930): the oracle's restatement gives
+    the reference's enstrophy.dat averages and turb_para.dat values to the 12
+    significant digits the reference prints."""
+    z = golden("stats.npz")
+    nz, ny, nx = (int(v) for v in z["shape"])
+    box = Box(nx, ny, nz, scheme=(WENO5Z,) * 3, mach=float(z["mach"]),
+              reynolds=float(z["reynolds"]), prandtl=float(z["prandtl"]))
+    got = O.stats(box, list(z["q"]))
+    np.testing.assert_allclose(got[:25], z["stats"], rtol=1e-11, atol=0)
+    assert got[25] > 0  # dissipation (not in the reference)
