@@ -78,13 +78,6 @@ def hbm_peak_gbs():
         return 6650.0, "fallback"
 
 
-def env_int(name, default):
-    try:
-        return int(os.environ.get(name, default))
-    except ValueError:
-        return default
-
-
 def config_dict(n_gpus, reynolds):
     return {
         "workload": f"decaying isotropic turbulence {NX}^3 periodic box, seeded solenoidal "
@@ -192,14 +185,11 @@ def run_b200(args, rank, world, local_rank):
     import numpy as np
     import torch
     import nuc3d_b200 as nb
+    from nuc3d_b200.replicas import RankInfo, Replicas, whole_job_rate
 
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    reps = Replicas(RankInfo(rank, world, local_rank), backend="nccl", timeout_s=120.0, device=dev)
 
     desc = nb.BoxDesc(NX, NX, NX, mach=1.0, scheme=(nb.WENO5Z,) * 3)
     q, reynolds = nb.hit_field(desc, seed=SEED + rank, k_peak=K_PEAK, mach_t=MACH_T,
@@ -212,16 +202,9 @@ def run_b200(args, rank, world, local_rank):
     stream = torch.cuda.current_stream(dev)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
+        reps.barrier(lambda: torch.cuda.synchronize(dev))
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = reps.max
 
     def timed_steps(solver, k):
         barrier()
@@ -249,7 +232,7 @@ def run_b200(args, rank, world, local_rank):
     s64.sync()
     ms_max = max_over_ranks(ms)
     ms_per_step = ms_max / args.steps
-    value = world * cells / (ms_per_step * 1e-3)
+    value = whole_job_rate(cells, world, ms_per_step * 1e-3)
 
     tuning64 = s64.tuning()
     # ---- per-kernel event timing (separate short pass, same workload)
@@ -370,8 +353,7 @@ def run_b200(args, rank, world, local_rank):
     served = None if (args.skip_serve or world > 1) else run_served(args)
 
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
+        reps.close()
         return None
     cpu = None
     if args.cpu_result is not None:
@@ -403,8 +385,7 @@ def run_b200(args, rank, world, local_rank):
         "served": served,
         "cpu_baseline": cpu,
     }
-    if dist is not None:
-        dist.destroy_process_group()
+    reps.close()
     return line
 
 
@@ -610,9 +591,9 @@ def main():
         ap.error("--warmup must be >= 3")
     NX = args.n
     METRIC = METRIC.replace("256^3", f"{NX}^3")
-    rank = env_int("RANK", 0)
-    world = env_int("WORLD_SIZE", args.gpus)
-    local_rank = env_int("LOCAL_RANK", 0)
+    from nuc3d_b200.replicas import rank_info
+    ri = rank_info(default_world=args.gpus)
+    rank, world, local_rank = ri.rank, ri.world, ri.local_rank
 
     if args.impl == "reference":
         line = run_reference(args, rank, world)

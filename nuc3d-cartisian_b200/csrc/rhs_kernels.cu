@@ -280,7 +280,9 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
         G::stage_item(t, l, pc);
         double Fp[5], Fm[5];
         if (l0 + l < nl) {
-            int pos = ((c0 - 3 + pc) % n + n) % n;
+            int pos = c0 - 3 + pc;  // in [-3, n + NF): wrap without a division
+            if (pos < 0) pos += n;
+            while (pos >= n) pos -= n;
             split(gidx(l, pos), Fp, Fm);
         } else {
 #pragma unroll

@@ -45,6 +45,7 @@ __device__ __forceinline__ double cd6d(double m3, double m2, double m1, double p
 template <typename B>
 __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items) {
     __shared__ double sP[2][4][TY + 6][TX + 6];
+    __shared__ int sOff[(TY + 6) * (TX + 6)];  // in-plane offsets of the staged tile
     const WorkItem it = items[blockIdx.x];
     const BoxDev &bd = boxes[it.box];
     if (!bd.active || !bd.p.navier_stokes) return;
@@ -60,11 +61,16 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
     const long long sz = bp.stride[2];
     const long long col = active ? (long long)i + (long long)nx * j : 0;
     const int src[4] = {0, 1, 2, 5};  // u, v, w, T
+    for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
+        int yy = t / (TX + 6), xx = t - yy * (TX + 6);
+        sOff[t] = pmod(i0 - 3 + xx, nx) + nx * pmod(j0 - 3 + yy, ny);
+    }
+    __syncthreads();
     auto issue = [&](int k, int buf) {
         const long long plane = sz * k;
         for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
             int yy = t / (TX + 6), xx = t - yy * (TX + 6);
-            long long g = plane + pmod(i0 - 3 + xx, nx) + (long long)nx * pmod(j0 - 3 + yy, ny);
+            long long g = plane + sOff[t];
 #pragma unroll
             for (int f = 0; f < 4; ++f) cp_async_elem(&sP[buf][f][yy][xx], wbase + src[f] * np + g);
         }
