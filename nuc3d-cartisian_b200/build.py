@@ -4,7 +4,8 @@
 
 Each .cu / .cpp under csrc/ is compiled with nvcc (-gencode arch=compute_100a,
 code=sm_100a -lineinfo -O3) in parallel and linked into one shared library
-whose C ABI is include/nuc3d_b200.h.  The toolchain's g++ links libstdc++
+whose C ABI is include/nuc3d_b200.h, and host/nuc3d_run.cpp (the C++ case
+driver) into lib/nuc3d_run against it.  The toolchain's g++ links libstdc++
 statically; the link hides those symbols (--exclude-libs,ALL) so the library
 can share a process with other C++ runtimes (numpy, torch).
 """
@@ -24,6 +25,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "lib" / "libnuc3d_b200.so"
+DRIVER = PKG / "lib" / "nuc3d_run"  # host/nuc3d_run.cpp: the C++ case driver
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden,-pthread",
               "--expt-relaxed-constexpr", "-I", str(ROOT / "include"), "-I", str(CSRC)]
@@ -71,9 +73,24 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_driver(force)
     if verbose:
         print(f"built {LIB}")
     return LIB
+
+
+def build_driver(force: bool = False) -> Path:
+    """The C++ case driver, linked against the library (C ABI only)."""
+    src = PKG / "host" / "nuc3d_run.cpp"
+    if (force or not DRIVER.exists() or src.stat().st_mtime > DRIVER.stat().st_mtime
+            or LIB.stat().st_mtime > DRIVER.stat().st_mtime):
+        cxx = os.environ.get("CXX") or shutil.which("g++") or "g++"
+        cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-I", str(ROOT / "include"), str(src),
+               "-L", str(LIB.parent), "-lnuc3d_b200", "-Wl,-rpath,$ORIGIN", "-o", str(DRIVER)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"driver build failed:\n{r.stderr}")
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -1,0 +1,61 @@
+"""The C++ case driver end to end on the GPU: the reference's Taylor-Green
+case (decks, device initial state, 10 TVD-RK3 steps, restart file in the
+reference's binary layout, block.cpp:609-671) reproduces the reference's own
+10-step result, directly and across a restart."""
+
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from helpers import golden, max_rel_l2
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT / "nuc3d-cartisian_b200"))
+
+
+@pytest.fixture(scope="module")
+def driver():
+    import build as b
+    return b.build_driver()
+
+
+def tgv_case(tmp, **io):
+    import nuc3d_b200 as nb
+    d = nb.BoxDesc(24, 24, 24, mach=0.1, reynolds=1600.0, prandtl=0.71)
+    nb.write_decks(tmp, d, io=dict({"Benchmark": 2, "cfl": 0.5, "tl": 100.0, "postStep": 0}, **io))
+    return d
+
+
+def read_restart(path, shape):
+    raw = np.fromfile(path, dtype=np.float64)
+    n = int(np.prod(shape))
+    assert raw.size == 1 + 5 * n
+    return raw[0], [raw[1 + e * n:1 + (e + 1) * n].reshape(shape) for e in range(5)]
+
+
+def test_driver_tgv_10_steps_matches_reference(driver, tmp_path):
+    d = tgv_case(tmp_path, endStep=10, saveStep=10, postStep=5)
+    r = subprocess.run([str(driver), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.count("========step = ") == 10 and "Calculation finished!!" in r.stdout
+    z = golden("tgv24_js_10.npz")
+    t, q = read_restart(tmp_path / "flowData" / "NUC3d_step_10_ID_0.bin", d.shape)
+    assert max_rel_l2(q, z["q10"]) < 1e-12
+    assert abs(t - float(np.sum(z["dt"]))) <= 1e-13 * t
+    assert len((tmp_path / "enstrophy.dat").read_text().splitlines()) == 2  # steps 5 and 10
+
+
+def test_driver_restart_continues_bitwise(driver, tmp_path):
+    d = tgv_case(tmp_path, endStep=5, saveStep=5)
+    r = subprocess.run([str(driver), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    tgv_case(tmp_path, startStep=5, endStep=10, saveStep=10)
+    r = subprocess.run([str(driver), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    z = golden("tgv24_js_10.npz")
+    _, q = read_restart(tmp_path / "flowData" / "NUC3d_step_10_ID_0.bin", d.shape)
+    assert max_rel_l2(q, z["q10"]) < 1e-12
