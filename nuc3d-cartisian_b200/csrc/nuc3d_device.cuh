@@ -55,6 +55,7 @@ struct K {
     static constexpr double C0 = 0.1, C1 = 0.6, C2 = 0.3;      // WENO5 linear weights
     static constexpr double CR0 = 0.2, CR1 = 0.5, CR2 = 0.3;   // CRWENO5 linear weights
     static constexpr double G0 = 13.0 / 12.0, G1 = 1.0 / 4.0;
+    static constexpr double SG0 = 1.0408329997330663;  // sqrt(13/12)
     static constexpr double CD1 = 3.0 / 4.0, CD2 = -3.0 / 20.0, CD3 = 1.0 / 60.0;
 };
 
@@ -108,6 +109,15 @@ __device__ __forceinline__ B d2_(B f0, B f1, B f2) {
     return add_(fma_(B(-2), f1, f0), f2);
 }
 
+// sqrt(13/12) (f0 - 2 f1 + f2): with it and half the first-difference term
+// e, a smoothness indicator (schemes.hpp:33-34) is the two-operation
+// d^2 + e^2 (one multiply, one FMA)
+template <typename B>
+__device__ __forceinline__ B sd2_(B f0, B f1, B f2) {
+    const B c = B(K::SG0), m2c = B(-2.0 * K::SG0);
+    return fma_(c, f0, fma_(m2c, f1, mul_(c, f2)));
+}
+
 // Fast FP32 reciprocal (one MUFU op, ~1 ulp): the weights only need FP32
 // accuracy in the mixed path.
 __device__ __forceinline__ float frcp_fast(float x) {
@@ -118,7 +128,7 @@ __device__ __forceinline__ float frcp_fast(float x) {
 
 // WENO5-JS nonlinear combination (weno5js.cpp:97-108), eps = 1e-6, p = 2:
 // alpha_k = c_k/(eps+beta_k)^2 normalised by their sum.  FP64 writes it with a
-// single division by multiplying through with s0^2 s1^2 s2^2 (an exact
+// single reciprocal by multiplying through with s0^2 s1^2 s2^2 (an exact
 // rearrangement); FP32 uses fast reciprocals.
 __device__ __forceinline__ double weno_js_combine(double is0, double is1, double is2, double q0,
                                                   double q1, double q2) {
@@ -129,7 +139,7 @@ __device__ __forceinline__ double weno_js_combine(double is0, double is1, double
     s2 = mul_(s2, s2);
     double w0 = mul_(K::C0, mul_(s1, s2)), w1 = mul_(K::C1, mul_(s0, s2));
     double w2 = mul_(K::C2, mul_(s0, s1));
-    return __ddiv_rn(fma_(w2, q2, fma_(w1, q1, mul_(w0, q0))), add_(add_(w0, w1), w2));
+    return mul_(fma_(w2, q2, fma_(w1, q1, mul_(w0, q0))), __drcp_rn(add_(add_(w0, w1), w2)));
 }
 __device__ __forceinline__ float weno_js_combine(float is0, float is1, float is2, float q0,
                                                  float q1, float q2) {
@@ -155,7 +165,7 @@ __device__ __forceinline__ double weno_z_combine(double is0, double is1, double 
     double w0 = mul_(mul_(K::C0, add_(s0, t2)), mul_(s1, s2));
     double w1 = mul_(mul_(K::C1, add_(s1, t2)), mul_(s0, s2));
     double w2 = mul_(mul_(K::C2, add_(s2, t2)), mul_(s0, s1));
-    return __ddiv_rn(fma_(w2, q2, fma_(w1, q1, mul_(w0, q0))), add_(add_(w0, w1), w2));
+    return mul_(fma_(w2, q2, fma_(w1, q1, mul_(w0, q0))), __drcp_rn(add_(add_(w0, w1), w2)));
 }
 __device__ __forceinline__ float weno_z_combine(float is0, float is1, float is2, float q0, float q1,
                                                 float q2) {

@@ -163,17 +163,19 @@ struct InvGeom {
     }
 };
 
-// One direction's smoothness and candidate terms for a stencil whose second
-// differences d0, d1, d2 are already known (the run reuses them across faces).
+// One direction's smoothness and candidate terms for a stencil whose scaled
+// second differences d0, d1, d2 (sd2_) are already known (the run reuses
+// them across faces).  beta_k = 13/12 D_k^2 + 1/4 E_k^2 (schemes.hpp:33-34)
+// is formed as d_k^2 + e_k^2 with d = sqrt(13/12) D and e = E / 2.
 template <int SCHEME, typename B>
 __device__ __forceinline__ B weno_from(B f0, B f1, B f2, B f3, B f4, B d0, B d1, B d2) {
-    const B g0 = B(K::G0), g1 = B(K::G1);
-    B e0 = fma_(B(3), f2, fma_(B(-4), f1, f0));
-    B e1 = sub_(f1, f3);
-    B e2 = add_(fma_(B(-4), f3, mul_(B(3), f2)), f4);
-    B is0 = fma_(mul_(g0, d0), d0, mul_(mul_(g1, e0), e0));
-    B is1 = fma_(mul_(g0, d1), d1, mul_(mul_(g1, e1), e1));
-    B is2 = fma_(mul_(g0, d2), d2, mul_(mul_(g1, e2), e2));
+    const B h = B(0.5), th = B(1.5), m2 = B(-2), mh = B(-0.5);
+    B e0 = fma_(th, f2, fma_(m2, f1, mul_(h, f0)));
+    B e1 = fma_(h, f1, mul_(mh, f3));
+    B e2 = fma_(th, f2, fma_(m2, f3, mul_(h, f4)));
+    B is0 = fma_(d0, d0, mul_(e0, e0));
+    B is1 = fma_(d1, d1, mul_(e1, e1));
+    B is2 = fma_(d2, d2, mul_(e2, e2));
     B q0 = fma_(B(K::A02), f2, fma_(B(K::A01), f1, mul_(B(K::A00), f0)));
     B q1 = fma_(B(K::A12), f3, fma_(B(K::A11), f2, mul_(B(K::A10), f1)));
     B q2 = fma_(B(K::A22), f4, fma_(B(K::A21), f3, mul_(B(K::A20), f2)));
@@ -319,14 +321,14 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
             const int v = e;
             B f0 = sF[G::sf(v, l, m0)], f1 = sF[G::sf(v, l, m0 + 1)], f2 = sF[G::sf(v, l, m0 + 2)];
             B f3 = sF[G::sf(v, l, m0 + 3)], f4 = sF[G::sf(v, l, m0 + 4)];
-            B d0 = d2_(f0, f1, f2), d1 = d2_(f1, f2, f3);
+            B d0 = sd2_(f0, f1, f2), d1 = sd2_(f1, f2, f3);
 #pragma unroll
             for (int k = 0; k <= R; ++k) {
                 if (k == R && !last) break;
                 const int gm = c0 + m0 + k;
-                B d2 = d2_(f2, f3, f4);
+                B d2 = sd2_(f2, f3, f4);
                 // weno5z.cpp:80 on the inner '+' faces 3..n-3
-                B d2s = (zq && gm >= 3 && gm <= n - 3) ? d2_(f2, f3, f3) : d2;
+                B d2s = (zq && gm >= 3 && gm <= n - 3) ? sd2_(f2, f3, f3) : d2;
                 Fh[k] = weno_from<SCHEME, B>(f0, f1, f2, f3, f4, d0, d1, d2s);
                 if (k < R) {
                     f0 = f1;
@@ -343,11 +345,11 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
             const int v = 5 + e;
             B f0 = sF[G::sf(v, l, m0 + 5)], f1 = sF[G::sf(v, l, m0 + 4)], f2 = sF[G::sf(v, l, m0 + 3)];
             B f3 = sF[G::sf(v, l, m0 + 2)], f4 = sF[G::sf(v, l, m0 + 1)];
-            B d1 = d2_(f1, f2, f3), d2 = d2_(f2, f3, f4);
+            B d1 = sd2_(f1, f2, f3), d2 = sd2_(f2, f3, f4);
 #pragma unroll
             for (int k = 0; k <= R; ++k) {
                 if (k == R && !last) break;
-                B d0 = d2_(f0, f1, f2);
+                B d0 = sd2_(f0, f1, f2);
                 Fh[k] = add_(Fh[k], weno_from<SCHEME, B>(f0, f1, f2, f3, f4, d0, d1, d2));
                 if (k < R) {
                     f4 = f3;
