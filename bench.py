@@ -260,7 +260,7 @@ def run_b200(args, rank, world, local_rank):
         "avg_launch_ms": inv_avg_ms,
         "share_of_step": inv_ms / total_ms if total_ms else None,
         "kernel_ms_per_step": {k: v[0] / 2 for k, v in prof.items()},
-        "autotuned_run_length": tuning64,
+        "autotuned_sweep_variant": tuning64,
         "step_fp64_tflops": FLOPS_PER_CELL_STAGE * 3 * cells / (ms_per_step * 1e-3) / 1e12,
         "hbm_state_frac": STATE_BYTES_PER_CELL_UPDATE * cells / (ms_per_step * 1e-3) / 1e9
                           / hbm_peak_gbs()[0],
@@ -345,7 +345,7 @@ def run_b200(args, rank, world, local_rank):
             "accuracy_steps": nacc,
             "peak_fp32_tflops": peak32,
             "kernel_ms_per_step": {k: v[0] / 2 for k, v in prof_m.items()},
-            "autotuned_run_length": tuning32,
+            "autotuned_sweep_variant": tuning32,
         }
 
     ensemble = None if args.skip_ensemble else run_ensemble(args, stream, barrier, max_over_ranks,
