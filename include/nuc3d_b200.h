@@ -75,7 +75,16 @@ typedef struct nuc3d_box_desc {
     double powerlaw_exp;     /* exponent of NUC3D_VISC_POWERLAW */
     int precision;           /* NUC3D_FP64 or NUC3D_MIXED */
     unsigned quirks;         /* NUC3D_QUIRK_* mask */
+    /* PhysModel.in Forcing (physicsModel.cpp:50-56): NUC3D_FORCING_NONE or
+     * NUC3D_FORCING_CONST, the spectral shell forcing of AddForcing_Const
+     * (physicsModel.cpp:1368-1641) with Forcing_amplitude (target shell
+     * energy), Forcing_amplitude_hel (helical part) and Forcing_wave_k (shell
+     * radius, < 3.5). */
+    int forcing;
+    double forcing_amp, forcing_hel, forcing_k;
 } nuc3d_box_desc;
+#define NUC3D_FORCING_NONE 0
+#define NUC3D_FORCING_CONST 1
 
 typedef struct nuc3d_ctx nuc3d_ctx;
 

@@ -123,6 +123,10 @@ void nuc3d_box_desc_default(nuc3d_box_desc *d) {
     d->powerlaw_exp = 0.76;
     d->precision = NUC3D_FP64;
     d->quirks = NUC3D_QUIRKS_REFERENCE;
+    d->forcing = NUC3D_FORCING_NONE;
+    d->forcing_amp = 0.01;  // physicsModel.cpp:37-39
+    d->forcing_hel = 0.01;
+    d->forcing_k = 1.0;
 }
 
 long long nuc3d_ctx_bytes(const nuc3d_box_desc *d) { return d ? Engine::box_bytes(*d) : -1; }

@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 
+#include "forcing_kernels.h"
 #include "init_kernels.h"
 #include "stats_kernels.h"
 #include "op_kernels.h"
@@ -83,6 +84,15 @@ int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
         return bad(NUC3D_ERR_UNSUPPORTED, "unknown precision");
     if (!(d.gamma > 1.0) || !(d.mach > 0.0) || !(d.reynolds > 0.0) || !(d.prandtl > 0.0))
         return bad(NUC3D_ERR_INVALID, "gamma must be > 1 and Mach, Re, Pr > 0");
+    if (d.forcing != NUC3D_FORCING_NONE && d.forcing != NUC3D_FORCING_CONST)
+        return bad(NUC3D_ERR_UNSUPPORTED, "unknown forcing model");
+    if (d.forcing == NUC3D_FORCING_CONST) {
+        if (!(d.forcing_k > 0.0) || forcing_K(d.forcing_k) > kForceMaxK)
+            return bad(NUC3D_ERR_UNSUPPORTED, "forcing shell radius must be in (0, 3.5)");
+        for (int i = 0; i < 3; ++i)
+            if (2 * forcing_K(d.forcing_k) + 1 > n[i])
+                return bad(NUC3D_ERR_INVALID, "box too small for the forcing shell");
+    }
     return NUC3D_OK;
 }
 
@@ -91,7 +101,9 @@ long long Engine::box_bytes(const nuc3d_box_desc &d) {
     BoxParams bp = make_params(d);
     long long np = pad32(bp.N);
     long long bs = (long long)bulk_size(d.precision);
-    return 21 * np * 8 + 14 * np * bs + (long long)kSmallBytes;
+    long long b = 21 * np * 8 + 14 * np * bs + (long long)kSmallBytes;
+    if (d.forcing == NUC3D_FORCING_CONST) b += (long long)forcing_scratch_bytes(bp, d.forcing_k);
+    return b;
 }
 
 Engine::Engine(int precision, cudaStream_t stream) : precision_(precision), stream_(stream) {}
@@ -101,6 +113,7 @@ Engine::~Engine() {
     invalidate_graph();
     for (auto &b : boxes_) {
         if (b.mem) cudaFreeAsync(b.mem, stream_);
+        if (b.force_mem) cudaFreeAsync(b.force_mem, stream_);
     }
     if (d_boxes_) cudaFreeAsync(d_boxes_, stream_);
     if (d_items_) cudaFreeAsync(d_items_, stream_);
@@ -131,7 +144,10 @@ int Engine::add_box(const nuc3d_box_desc &d, int *id) {
     const size_t bs = bulk_size(precision_);
     const size_t bytes = sizeof(double) * 21 * (size_t)np + bs * 14 * (size_t)np + kSmallBytes;
     cudaError_t e = cudaMallocAsync(&b.mem, bytes, stream_);
+    if (e == cudaSuccess && d.forcing == NUC3D_FORCING_CONST)
+        e = cudaMallocAsync(&b.force_mem, forcing_scratch_bytes(b.dev.p, d.forcing_k), stream_);
     if (e != cudaSuccess) {
+        if (b.mem) cudaFreeAsync(b.mem, stream_);
         cudaGetLastError();
         return set_last_error(NUC3D_ERR_NOMEM,
                               (std::string("device allocation failed: ") + cudaGetErrorString(e)).c_str());
@@ -151,6 +167,9 @@ int Engine::add_box(const nuc3d_box_desc &d, int *id) {
     // sc->cfl = 0.5 (the stream-ordered memset above runs first)
     static const double half = 0.5;
     ECK(cudaMemcpyAsync(&b.dev.sc->cfl, &half, sizeof half, cudaMemcpyHostToDevice, stream_));
+    if (b.force_mem)
+        ECK(forcing_prepare(b.dev.p, d.forcing_k, forcing_layout(b.dev.p, d.forcing_k, b.force_mem),
+                            stream_));
     int slot = -1;
     for (size_t i = 0; i < boxes_.size(); ++i)
         if (!boxes_[i].live) {
@@ -173,6 +192,7 @@ int Engine::remove_box(int id) {
         return set_last_error(NUC3D_ERR_INVALID, "no such box");
     EngineBox &b = boxes_[id];
     ECK(cudaFreeAsync(b.mem, stream_));
+    if (b.force_mem) ECK(cudaFreeAsync(b.force_mem, stream_));
     b = EngineBox();
     dirty_ = true;
     return NUC3D_OK;
@@ -328,6 +348,8 @@ int Engine::rebuild() {
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d].n > 0;
     for (int d = 0; d < 3; ++d) per_stage += r_cr_[d].n > 0;
     launches_per_step_ = 3 * per_stage + 3;  // + clear_eig, dt, residual
+    for (const EngineBox &b : boxes_)
+        if (b.live && b.dev.active && b.force_mem) launches_per_step_ += 3 * 8;  // forcing passes
     dirty_ = false;
     return NUC3D_OK;
 }
@@ -401,6 +423,7 @@ int Engine::enqueue_step_t(cudaStream_t st) {
             ECK((launch_crweno<B>(d, d_boxes_, it + r_cr_[d].off, r_cr_[d].n, in, d > 0,
                                   cr_nmax_[d], cr_ms_[d], st)));
         }
+        ECK(enqueue_forcing<B>(st));
         {
             ProfScope ps(this, NUC3D_PROF_UPDATE);
             StageArgs sa{stage, in, out, nullptr};
@@ -412,6 +435,22 @@ int Engine::enqueue_step_t(cudaStream_t st) {
         ECK(launch_residual(d_boxes_, nb, st));
     }
     return NUC3D_OK;
+}
+
+// Spectral forcing of the forced boxes (physicsModel::solveSource after
+// the RHS assembly, NaiverStokes3d.cpp:58): uses this stage's primitives W,
+// subtracts from the inviscid accumulator R before the update.
+template <typename B>
+cudaError_t Engine::enqueue_forcing(cudaStream_t st) {
+    for (const EngineBox &b : boxes_) {
+        if (!b.live || !b.dev.active || !b.force_mem) continue;
+        ForceParams fp{b.desc.forcing_amp, b.desc.forcing_hel, b.desc.forcing_k,
+                       forcing_K(b.desc.forcing_k), 0};
+        cudaError_t e = launch_forcing<B>(b.dev, forcing_layout(b.dev.p, b.desc.forcing_k, b.force_mem),
+                                          fp, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 int Engine::enqueue_step(cudaStream_t s) {
@@ -563,6 +602,7 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
         ECK((launch_crweno<B>(d, d_boxes_, it + r_cr_[d].off, r_cr_[d].n, 0, d > 0, cr_nmax_[d],
                               cr_ms_[d], stream_)));
     }
+    ECK(enqueue_forcing<B>(stream_));
     StageArgs sa{-1, 0, 0, d_rhs_ptrs_};
     ECK((launch_update<B>(d_boxes_, it + r_25d_.off, r_25d_.n, sa, any_visc_, stream_)));
     ECK(cudaStreamSynchronize(stream_));  // ptrs is a host stack array

@@ -19,6 +19,7 @@ struct EngineBox {
     BoxDev dev{};          // host copy of the box's table entry
     int prim_off = 0, prim_n = 0;  // the box's k_prim work items (set by rebuild)
     void *mem = nullptr;   // one stream-ordered allocation holding all fields
+    void *force_mem = nullptr;  // spectral forcing scratch (forced boxes only)
     double cfl = 0.5;
     long long steps = 0;   // host mirror of the device step counter
     bool live = false;     // slot in use
@@ -80,6 +81,8 @@ private:
     int enqueue_step_t(cudaStream_t s);
     template <typename B>
     int enqueue_rhs_t(int id, double *const d_rhs[5]);
+    template <typename B>
+    cudaError_t enqueue_forcing(cudaStream_t st);
     void invalidate_graph();
     int autotune();
 

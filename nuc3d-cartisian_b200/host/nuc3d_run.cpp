@@ -14,6 +14,7 @@
 //
 // Only the C ABI in include/nuc3d_b200.h is used.  One process, one box,
 // periodic, process topology 1 1 1 (there is no MPI on this path).
+// PhysModel.in Forcing None or Const (the spectral shell forcing).
 //
 //   nuc3d_run [case_dir] [--precision fp64|mixed] [--seed S] [--check-decks]
 #include <chrono>
@@ -108,7 +109,9 @@ Case read_case(const std::string &dir) {
     if (p.size() < 12) die("PhysModel.in needs its six positional lines");
     const std::string riemann = p[5], model = p[7], visc = p[9], forcing = p[11];
     if (riemann != "LF") die("RiemannSolver " + riemann + ": only LF is on the B200 path");
-    if (forcing != "None") die("Forcing " + forcing + ": only None is on the B200 path");
+    if (forcing != "None" && forcing != "Const")
+        die("Forcing " + forcing + ": only None and Const are on the B200 path");
+    c.desc.forcing = forcing == "Const" ? NUC3D_FORCING_CONST : NUC3D_FORCING_NONE;
     if (model == "NavierStokes3d")
         c.desc.pde_model = NUC3D_NAVIERSTOKES3D;
     else if (model == "Euler3d")
@@ -135,6 +138,9 @@ Case read_case(const std::string &dir) {
     c.desc.gamma = c.phys["Gamma"];
     c.desc.t_ref = c.phys["T_ref"];
     c.desc.t_inf = c.phys["T_inf"];
+    c.desc.forcing_amp = c.phys["Forcing_amplitude"];
+    c.desc.forcing_hel = c.phys["Forcing_amplitude_hel"];
+    c.desc.forcing_k = c.phys["Forcing_wave_k"];
     // IOController.in key/value (IOcontroller.cpp:10-60)
     c.io = {{"startStep", 0}, {"endStep", 100000}, {"postStep", 1}, {"saveStep", 1000},
             {"postSaveStep", 100}, {"Benchmark", 0}, {"cfl", 0.5}, {"tl", 0.0}, {"dt", 0.01}};
@@ -204,7 +210,9 @@ int main(int argc, char **argv) {
                   << c.desc.scheme[2] << " pde " << c.desc.pde_model << " visc "
                   << c.desc.visc_model << " gamma " << c.desc.gamma << " mach " << c.desc.mach
                   << " reynolds " << c.desc.reynolds << " prandtl " << c.desc.prandtl
-                  << " t_ref " << c.desc.t_ref << " t_inf " << c.desc.t_inf << " cfl "
+                  << " t_ref " << c.desc.t_ref << " t_inf " << c.desc.t_inf << " forcing "
+                  << c.desc.forcing << " forcing_amp " << c.desc.forcing_amp << " forcing_hel "
+                  << c.desc.forcing_hel << " forcing_k " << c.desc.forcing_k << " cfl "
                   << c.io["cfl"] << " endStep " << c.io["endStep"] << " tl " << c.io["tl"]
                   << std::endl;
         return 0;

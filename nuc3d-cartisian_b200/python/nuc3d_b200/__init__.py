@@ -20,6 +20,7 @@ LIB_PATH = PKG_ROOT / "lib" / "libnuc3d_b200.so"
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2, -3, -4, -5
 ERR_TIMEOUT, ERR_CANCELLED = -6, -7
 INIT_STATE, INIT_TGV, INIT_HIT = 0, 1, 2
+FORCING_NONE, FORCING_CONST = 0, 1
 WENO5JS, WENO5Z, CRWENO5 = 0, 1, 2
 SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5}
 EULER3D, NAVIERSTOKES3D = 0, 1
@@ -58,6 +59,8 @@ class _Desc(C.Structure):
         ("powerlaw_exp", C.c_double),
         ("precision", C.c_int),
         ("quirks", C.c_uint),
+        ("forcing", C.c_int),
+        ("forcing_amp", C.c_double), ("forcing_hel", C.c_double), ("forcing_k", C.c_double),
     ]
 
 
@@ -201,6 +204,10 @@ class BoxDesc:
     powerlaw_exp: float = 0.76
     precision: int = FP64
     quirks: int = QUIRKS_REFERENCE
+    forcing: int = FORCING_NONE     # FORCING_CONST: physicsModel::AddForcing_Const
+    forcing_amp: float = 0.01       # PhysModel.in Forcing_amplitude
+    forcing_hel: float = 0.01       # Forcing_amplitude_hel
+    forcing_k: float = 1.0          # Forcing_wave_k
 
     @property
     def cells(self) -> int:
@@ -222,6 +229,8 @@ class BoxDesc:
         d.powerlaw_exp = self.powerlaw_exp
         d.precision = int(self.precision)
         d.quirks = int(self.quirks)
+        d.forcing = int(self.forcing)
+        d.forcing_amp, d.forcing_hel, d.forcing_k = self.forcing_amp, self.forcing_hel, self.forcing_k
         return d
 
     def device_bytes(self) -> int:

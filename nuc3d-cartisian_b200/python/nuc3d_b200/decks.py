@@ -11,7 +11,8 @@ from __future__ import annotations
 
 from pathlib import Path
 
-from . import (CONSTANT, EULER3D, NAVIERSTOKES3D, SCHEMES, SUTHERLAND, BoxDesc)
+from . import (CONSTANT, EULER3D, FORCING_CONST, FORCING_NONE, NAVIERSTOKES3D, SCHEMES,
+               SUTHERLAND, BoxDesc)
 
 _METHOD_DEFAULTS = {"scheme_time": "RK3", "scheme_x_ivs": "weno5js", "scheme_y_ivs": "weno5js",
                     "scheme_z_ivs": "weno5js", "scheme_x_vis": "cd6", "scheme_y_vis": "cd6",
@@ -44,8 +45,8 @@ def read_decks(dirpath):
     pos = [toks[2 * i + 1] for i in range(6)]  # Neqs EosName RiemannSolver PDEModel ViscousModel Forcing
     if pos[2] != "LF":
         raise ValueError(f"RiemannSolver {pos[2]}: only LF is on the B200 path")
-    if pos[5] not in ("None",):
-        raise ValueError(f"Forcing {pos[5]}: only None is on the B200 path")
+    if pos[5] not in ("None", "Const"):
+        raise ValueError(f"Forcing {pos[5]}: only None and Const are on the B200 path")
     phys = dict(_PHYS_DEFAULTS)
     for k, v in _pairs(" ".join(toks[12:])):
         if k in ("Coriolis", "Centrifugal"):
@@ -75,7 +76,10 @@ def read_decks(dirpath):
                    scheme=tuple(SCHEMES.get(method[f"scheme_{a}_ivs"], 0) for a in "xyz"),
                    pde_model=models[pos[3]], visc_model=visc, gamma=phys["Gamma"],
                    mach=phys["Mach"], reynolds=phys["Reynolds"], prandtl=phys["Pt"],
-                   t_ref=phys["T_ref"], t_inf=phys["T_inf"])
+                   t_ref=phys["T_ref"], t_inf=phys["T_inf"],
+                   forcing=FORCING_CONST if pos[5] == "Const" else FORCING_NONE,
+                   forcing_amp=phys["Forcing_amplitude"], forcing_hel=phys["Forcing_amplitude_hel"],
+                   forcing_k=phys["Forcing_wave_k"])
     return desc, io, phys
 
 
@@ -88,10 +92,13 @@ def write_decks(dirpath, desc, io=None):
         + "scheme_x_vis cd6\nscheme_y_vis cd6\nscheme_z_vis cd6\n")
     model = "NavierStokes3d" if desc.pde_model == NAVIERSTOKES3D else "Euler3d"
     visc = "Constant" if desc.visc_model == CONSTANT else "Sutherland"
+    forcing = "Const" if desc.forcing == FORCING_CONST else "None"
     (inp / "PhysModel.in").write_text(
         f"Neqs 5\nEosName IdealGas\nRiemannSolver LF\nPDEModel {model}\nViscousModel {visc}\n"
-        f"Forcing None\nReynolds {desc.reynolds!r}\nMach {desc.mach!r}\nPt {desc.prandtl!r}\n"
-        f"Gamma {desc.gamma!r}\nT_ref {desc.t_ref!r}\nT_inf {desc.t_inf!r}\n")
+        f"Forcing {forcing}\nReynolds {desc.reynolds!r}\nMach {desc.mach!r}\nPt {desc.prandtl!r}\n"
+        f"Gamma {desc.gamma!r}\nT_ref {desc.t_ref!r}\nT_inf {desc.t_inf!r}\n"
+        f"Forcing_amplitude {desc.forcing_amp!r}\nForcing_amplitude_hel {desc.forcing_hel!r}\n"
+        f"Forcing_wave_k {desc.forcing_k!r}\n")
     (inp / "block.in").write_text(
         f"1 1 1\n{desc.nx} {desc.ny} {desc.nz}\n{desc.lx!r} {desc.ly!r} {desc.lz!r}\n0.0 0.0 0.0\n")
     io = dict(_IO_DEFAULTS, **(io or {}))

@@ -182,3 +182,35 @@ def test_device_stats_match_reference_and_oracle(nb):
     np.testing.assert_allclose(got[keep], ref[keep], rtol=1e-10)
     o = Oracle().stats(box, q)
     np.testing.assert_allclose(got[25], o[25], rtol=1e-12)
+
+
+@pytest.mark.parametrize("kf,shape", [(1.0, (24, 20, 16)), (2.0, (32, 32, 32)), (2.6, (20, 24, 28))])
+def test_spectral_forcing_matches_restatement(nb, kf, shape):
+    """The device shell forcing (AddForcing_Const) against its numpy
+    restatement: the RHS with forcing minus the RHS without is the forcing."""
+    import torch
+    from oracle_ctypes import Oracle
+    from forcing_oracle import forcing_terms
+    base = nb.BoxDesc(*shape, mach=1.0, reynolds=300.0, scheme=(nb.WENO5Z,) * 3)
+    forced = nb.BoxDesc(**{**base.__dict__, "forcing": nb.FORCING_CONST, "forcing_amp": 0.05,
+                           "forcing_hel": 0.3, "forcing_k": kf})
+    with nb.Solver(base) as s:
+        s.init_state({"kind": "hit", "seed": 9, "k_peak": 2.0, "mach_t": 0.3})
+        q = s.get_state()
+    rhs = {}
+    for name, d in (("off", base), ("on", forced)):
+        with nb.Solver(d) as s:
+            s.set_state(q)
+            out = [torch.zeros(d.shape, dtype=torch.float64, device="cuda") for _ in range(5)]
+            s.rhs(out)
+            rhs[name] = [o.cpu().numpy() for o in out]
+    from oracle_ctypes import Box
+    prim = Oracle().con2prim(Box(*shape, mach=1.0), q)
+    terms, _ = forcing_terms(prim[1], prim[2], prim[3], 0.05, 0.3, kf)
+    assert np.array_equal(rhs["on"][0], rhs["off"][0])
+    for e in range(1, 5):
+        got = rhs["off"][e] - rhs["on"][e]
+        scale = np.max(np.abs(terms[e - 1]))
+        assert scale > 0
+        atol = 1e-12 * max(scale, np.max(np.abs(rhs["off"][e])))
+        np.testing.assert_allclose(got, terms[e - 1], rtol=0, atol=atol)
