@@ -84,6 +84,52 @@ static double weno5z_face(const double f[5], int beta2_quirk) {
     return omega0 * q30 + omega1 * q31 + omega2 * q32;
 }
 
+/* schemes.hpp:21-31 */
+static const double A7[4][4] = {{-3.0 / 12.0, 13.0 / 12.0, -23.0 / 12.0, 25.0 / 12.0},
+                                {1.0 / 12.0, -5.0 / 12.0, 13.0 / 12.0, 3.0 / 12.0},
+                                {-1.0 / 12.0, 7.0 / 12.0, 7.0 / 12.0, -1.0 / 12.0},
+                                {3.0 / 12.0, 13.0 / 12.0, -5.0 / 12.0, 1.0 / 12.0}};
+static const double C_W7[4] = {1.0 / 35.0, 12.0 / 35.0, 18.0 / 35.0, 4.0 / 35.0};
+
+/* The reference's weno7js: weno7js.cpp:79-126 (inner +), :179-226 (inner -),
+ * :316-371 and the other halo forms, all this expression on an
+ * upwind-oriented 7-cell stencil f[0..6].  Its weights are the Z form
+ * alpha_k = c_k (1 + (tau7/(eps+beta_k))^p), tau7 = |beta0 - beta3|,
+ * eps = 1e-20 (weno7js.cpp:14, :111-114; the JS form is commented out). */
+static double weno7_face(const double f[7]) {
+    const double ss = 1.0e-20;
+    double is0 = f[0] * (547.0 * f[0] - 3882.0 * f[1] + 4642.0 * f[2] - 1854.0 * f[3]) +
+                 f[1] * (7043.0 * f[1] - 17246.0 * f[2] + 7042.0 * f[3]) +
+                 f[2] * (11003.0 * f[2] - 9402.0 * f[3]) + 2107.0 * f[3] * f[3];
+    double is1 = f[1] * (267.0 * f[1] - 1642.0 * f[2] + 1602.0 * f[3] - 494.0 * f[4]) +
+                 f[2] * (2843.0 * f[2] - 5966.0 * f[3] + 1922.0 * f[4]) +
+                 f[3] * (3443.0 * f[3] - 2522.0 * f[4]) + 547.0 * f[4] * f[4];
+    double is2 = f[2] * (547.0 * f[2] - 2522.0 * f[3] + 1922.0 * f[4] - 494.0 * f[5]) +
+                 f[3] * (3443.0 * f[3] - 5966.0 * f[4] + 1602.0 * f[5]) +
+                 f[4] * (2843.0 * f[4] - 1642.0 * f[5]) + 267.0 * f[5] * f[5];
+    double is3 = f[3] * (2107.0 * f[3] - 9402.0 * f[4] + 7042.0 * f[5] - 1854.0 * f[6]) +
+                 f[4] * (11003.0 * f[4] - 17246.0 * f[5] + 4642.0 * f[6]) +
+                 f[5] * (7043.0 * f[5] - 3882.0 * f[6]) + 547.0 * f[6] * f[6];
+    double q40 = A7[0][0] * f[0] + A7[0][1] * f[1] + A7[0][2] * f[2] + A7[0][3] * f[3];
+    double q41 = A7[1][0] * f[1] + A7[1][1] * f[2] + A7[1][2] * f[3] + A7[1][3] * f[4];
+    double q42 = A7[2][0] * f[2] + A7[2][1] * f[3] + A7[2][2] * f[4] + A7[2][3] * f[5];
+    double q43 = A7[3][0] * f[3] + A7[3][1] * f[4] + A7[3][2] * f[5] + A7[3][3] * f[6];
+    double tau7 = fabs(is0 - is3);
+    double alpha0 = C_W7[0] * (1.0 + PW(tau7 / (ss + is0)));
+    double alpha1 = C_W7[1] * (1.0 + PW(tau7 / (ss + is1)));
+    double alpha2 = C_W7[2] * (1.0 + PW(tau7 / (ss + is2)));
+    double alpha3 = C_W7[3] * (1.0 + PW(tau7 / (ss + is3)));
+    double alphaSum = alpha0 + alpha1 + alpha2 + alpha3;
+    double omega0 = alpha0 / alphaSum;
+    double omega1 = alpha1 / alphaSum;
+    double omega2 = alpha2 / alphaSum;
+    double omega3 = alpha3 / alphaSum;
+    return omega0 * q40 + omega1 * q41 + omega2 * q42 + omega3 * q43;
+}
+
+/* buffer (halo) width of a scheme (fieldOperator.cpp:128-175) */
+static int halo_of(int scheme) { return scheme == OR_WENO7 ? 4 : 3; }
+
 /* One compact-WENO row (crweno5.cpp:131-162 for '+', :311-341 for '-').
  * f[0..4] is the upwind-oriented 5-cell stencil of the row's cell i
  * ('+': cells i-2..i+2; '-': cells i+3..i-1), so f[1], f[2], f[3] are the
@@ -138,6 +184,16 @@ static void thomas_ref(int M, double *a, double *b, double *c, double *d, double
 static void reconstruct_line_ref(int scheme, int upwind, unsigned quirks, int n,
                                  const double *line, double *out, double *work) {
     double f[5];
+    if (scheme == OR_WENO7) {
+        /* face m: '+' cells m-4..m+2 (weno7js.cpp:123 writes face i+1 from
+         * cells i-3..i+3), '-' cells m+3..m-3 */
+        double g[7];
+        for (int m = 0; m <= n; ++m) {
+            for (int k = 0; k < 7; ++k) g[k] = upwind > 0 ? line[m - 4 + k] : line[m + 3 - k];
+            out[m] = weno7_face(g);
+        }
+        return;
+    }
     if (scheme == OR_CRWENO5) {
         for (int m = 0; m <= 2 && m <= n; ++m) {
             face_stencil(line, m, upwind, f);
@@ -258,14 +314,15 @@ int or_reconstruct_field(int scheme, int upwind, unsigned quirks, int nx, int ny
                          const double *in, const double *halo_l, const double *halo_r,
                          double *out) {
     if (nx < 5 || (upwind != 1 && upwind != -1)) return -1;
-    double *buf = (double *)malloc(sizeof(double) * (size_t)(nx + 6));
+    const int H = halo_of(scheme);
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(nx + 2 * H));
     double *work = (double *)malloc(sizeof(double) * (size_t)(10 * (nx + 1)));
-    double *line = buf + 3;
+    double *line = buf + H;
     for (int k = 0; k < nz; ++k)
         for (int j = 0; j < ny; ++j) {
-            for (int c = 0; c < 3; ++c) {
-                line[c - 3] = halo_l[c + 3 * (j + ny * k)];
-                line[nx + c] = halo_r[c + 3 * (j + ny * k)];
+            for (int c = 0; c < H; ++c) {
+                line[c - H] = halo_l[c + H * (j + ny * k)];
+                line[nx + c] = halo_r[c + H * (j + ny * k)];
             }
             for (int i = 0; i < nx; ++i) line[i] = in[i + nx * (j + ny * k)];
             reconstruct_line_ref(scheme, upwind, quirks, nx, line,
@@ -405,7 +462,7 @@ static void line_counts(const or_box *b, int d, int *na, int *nc) {
 }
 
 static void gather_periodic(const double *src, long base, long stride, int n, double *line) {
-    for (int c = -3; c < n + 3; ++c) {
+    for (int c = -4; c < n + 4; ++c) {
         int cc = ((c % n) + n) % n;
         line[c] = src[base + (long)cc * stride];
     }
@@ -421,8 +478,8 @@ static void inviscid_direction(const or_box *b, int d, double *const fl[5], doub
     double delta = d == 0 ? b->dx : (d == 1 ? b->dy : b->dz);
     int na, nc;
     line_counts(b, d, &na, &nc);
-    double *buf = (double *)malloc(sizeof(double) * (size_t)(n + 6));
-    double *line = buf + 3;
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(n + 8));
+    double *line = buf + 4;
     double *rp = (double *)malloc(sizeof(double) * (size_t)(n + 1));
     double *rn = (double *)malloc(sizeof(double) * (size_t)(n + 1));
     double *work = (double *)malloc(sizeof(double) * (size_t)(10 * (n + 1)));
@@ -461,8 +518,8 @@ static void cd6_direction(const or_box *b, int d, const double *src, double *dst
     double delta = d == 0 ? b->dx : (d == 1 ? b->dy : b->dz);
     int na, nc;
     line_counts(b, d, &na, &nc);
-    double *buf = (double *)malloc(sizeof(double) * (size_t)(n + 6));
-    double *line = buf + 3;
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(n + 8));
+    double *line = buf + 4;
     for (int c = 0; c < nc; ++c)
         for (int a = 0; a < na; ++a) {
             long base = line_base(b, d, a, c);

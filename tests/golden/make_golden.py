@@ -19,9 +19,9 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT / "oracle"))
 
-from oracle_ctypes import (CRWENO5, WENO5JS, WENO5Z, Box, Oracle, Reference)  # noqa: E402
+from oracle_ctypes import (CRWENO5, WENO5JS, WENO5Z, WENO7, Box, Oracle, Reference)  # noqa: E402
 
-SCHEME_TAG = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr"}
+SCHEME_TAG = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr", WENO7: "w7"}
 
 
 def perturbed_tgv(box: Box, seed: int):
@@ -92,7 +92,34 @@ def main():
     qn, dt, res = R.run_steps(box, 0.5, 10, q0)
     np.savez_compressed(HERE / "tgv24_js_10.npz", q10=np.stack(qn), dt=dt, res=res)
     stats_fixture(R)
+    weno7_fixtures(R)
     print("fixtures written to", HERE)
+
+
+def weno7_fixtures(R):
+    """The reference's weno7js (bufferSize 4): both reconstruction directions
+    with 4-wide halos, and one RHS plus three steps, N-S and Euler."""
+    rng = np.random.default_rng(77)
+    out = {}
+    shape = (5, 4, 14)
+    for up in (1, -1):
+        f = rng.standard_normal(shape)
+        hl = rng.standard_normal(shape[:2] + (4,))
+        hr = rng.standard_normal(shape[:2] + (4,))
+        tag = f"w7_{'p' if up > 0 else 'm'}"
+        out[f"rec_{tag}_in"], out[f"rec_{tag}_hl"], out[f"rec_{tag}_hr"] = f, hl, hr
+        out[f"rec_{tag}_out"] = R.reconstruct_field(WENO7, up, f, hl, hr)
+    np.savez_compressed(HERE / "operators_w7.npz", **out)
+    for ns in (True, False):
+        box = Box(16, 12, 10, scheme=(WENO7,) * 3, navier_stokes=ns, mach=0.1, reynolds=1600.0,
+                  prandtl=0.71)
+        q = perturbed_tgv(box, 11 + WENO7)
+        rhs, dtl = R.rhs(box, q)
+        qn, dt, res = R.run_steps(box, 0.5, 3, q)
+        np.savez_compressed(HERE / f"step_w7_{'ns' if ns else 'eu'}.npz", q0=np.stack(q),
+                            rhs=np.stack(rhs), dt_local=np.array(dtl), q3=np.stack(qn), dt=dt,
+                            res=res, shape=np.array(box.shape), mach=box.mach,
+                            reynolds=box.reynolds, prandtl=box.prandtl)
 
 
 def stats_fixture(R):

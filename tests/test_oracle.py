@@ -11,7 +11,7 @@ import pytest
 
 from helpers import box_from_golden, golden
 from oracle_ctypes import (CRWENO5, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_WENOZ_BETA2, WENO5JS,
-                           WENO5Z, Box, Oracle, Reference)
+                           WENO5Z, WENO7, Box, Oracle, Reference)
 
 TAGS = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr"}
 
@@ -128,3 +128,24 @@ def test_stats_match_reference_golden(O):
     got = O.stats(box, list(z["q"]))
     np.testing.assert_allclose(got[:25], z["stats"], rtol=1e-11, atol=0)
     assert got[25] > 0  # dissipation (not in the reference)
+
+
+@pytest.mark.parametrize("up", [1, -1])
+def test_weno7_reconstruct_matches_reference_golden(O, up):
+    """The reference's weno7js (Z-form weights, eps 1e-20, 4-wide halos)."""
+    z = golden("operators_w7.npz")
+    tag = f"w7_{'p' if up > 0 else 'm'}"
+    out = O.reconstruct_field(WENO7, up, QUIRKS_REFERENCE, z[f"rec_{tag}_in"], z[f"rec_{tag}_hl"],
+                              z[f"rec_{tag}_hr"])
+    assert np.array_equal(out, z[f"rec_{tag}_out"])
+
+
+@pytest.mark.parametrize("ns", [True, False])
+def test_weno7_rhs_and_steps_match_reference_golden(O, ns):
+    z = golden(f"step_w7_{'ns' if ns else 'eu'}.npz")
+    box = box_from_golden(z, WENO7, ns)
+    rhs, dtl = O.rhs(box, list(z["q0"]))
+    assert np.array_equal(np.stack(rhs), z["rhs"]) and dtl == float(z["dt_local"])
+    q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
+    assert np.array_equal(np.stack(q3), z["q3"])
+    assert np.array_equal(dt, z["dt"]) and np.array_equal(res, z["res"])
