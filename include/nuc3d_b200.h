@@ -34,11 +34,13 @@ extern "C" {
 #define NUC3D_ERR_TIMEOUT (-6)     /* nuc3d_serve_wait: not finished in time */
 #define NUC3D_ERR_CANCELLED (-7)   /* solve dropped by nuc3d_serve_destroy */
 
-/* Reconstruction schemes: the Method.in strings weno5js, weno5z, crweno5
- * (fieldOperator.cpp:152-166). */
+/* Reconstruction schemes: the Method.in strings weno5js, weno5z, crweno5,
+ * weno7js (fieldOperator.cpp:152-175).  weno7js reads 4 halo cells per side
+ * (its bufferSize), the others 3. */
 #define NUC3D_WENO5JS 0
 #define NUC3D_WENO5Z 1
 #define NUC3D_CRWENO5 2
+#define NUC3D_WENO7JS 3
 
 /* PDEModel (block.cpp:146-157) */
 #define NUC3D_EULER3D 0
@@ -198,10 +200,13 @@ NUC3D_API int nuc3d_probe_peak(int precision, double *tflops);
 /* Autotuner result.  The directional WENO sweep has variants that give each
  * thread a run of 1, 2 or 4 consecutive faces; the first step after the set of
  * (scheme, direction) pairs changes times every variant on the live boxes and
- * keeps the fastest.  run_len[s*3+d] (s: 0 WENO5-JS, 1 WENO5-Z; d: x, y, z)
- * receives the chosen run length (0 = not tuned), ms[(s*3+d)*3+v] the measured
- * milliseconds per launch of variant v (run length 1, 2, 4).  Either pointer
- * may be NULL. */
+ * keeps the fastest.  run_len[s*3+d] (s: the scheme id, NUC3D_WENO5JS ..
+ * NUC3D_WENO7JS; d: x, y, z) receives the chosen run length (0 = not tuned;
+ * always 0 for CRWENO5, whose lines have no run variants),
+ * ms[(s*3+d)*3+v] the measured milliseconds per launch of variant v (run
+ * length 1, 2, 4).  run_len holds NUC3D_TUNING_SLOTS ints, ms
+ * 3*NUC3D_TUNING_SLOTS doubles; either pointer may be NULL. */
+#define NUC3D_TUNING_SLOTS 12
 NUC3D_API int nuc3d_tuning(const nuc3d_ctx *ctx, int *run_len, double *ms);
 NUC3D_API int nuc3d_batch_tuning(const nuc3d_batch *b, int *run_len, double *ms);
 
@@ -335,9 +340,11 @@ NUC3D_API double nuc3d_ctx_time(const nuc3d_ctx *ctx);
  *
  * nuc3d_reconstruct = interpolationInner + interpolationBoundaryL +
  *   interpolationBoundaryR of weno5js (weno5js.cpp:19-628), weno5z
- *   (weno5z.cpp:18-637) or crweno5 (crweno5.cpp:25-837) with tilesize 3.
- *   Along the fastest axis of an (nx,ny,nz) field; halo_l/halo_r are (3,ny,nz)
- *   (the received MPI buffers, bufferData.cpp:16-47); out is (nx+1,ny,nz),
+ *   (weno5z.cpp:18-637), crweno5 (crweno5.cpp:25-837) with tilesize 3, or
+ *   weno7js (weno7js.cpp:17-824) with tilesize 4.
+ *   Along the fastest axis of an (nx,ny,nz) field; halo_l/halo_r are (h,ny,nz)
+ *   with h = 4 for weno7js and 3 otherwise (the received MPI buffers,
+ *   bufferData.cpp:16-47); out is (nx+1,ny,nz),
  *   face m between cells m-1 and m.  upwind = +1 or -1.  crweno5 needs
  *   nx <= 4096.  quirks: NUC3D_QUIRK_WENOZ_BETA2 is honoured. */
 NUC3D_API int nuc3d_reconstruct(int scheme, int upwind, unsigned quirks, int nx, int ny, int nz,

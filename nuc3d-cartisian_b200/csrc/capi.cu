@@ -78,9 +78,11 @@ int read_profile(Engine *eng, double *ms, long long *launches, int reset) {
     return NUC3D_OK;
 }
 
+static_assert(kSchemes * 3 == NUC3D_TUNING_SLOTS, "tuning table layout");
+
 int read_tuning(const Engine *eng, int *run_len, double *ms) {
     static const int lens[kInvVariants] = {1, 2, 4};
-    for (int s = 0; s < 2; ++s)
+    for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) {
             int v = eng->inv_variant[s][d];
             if (run_len) run_len[s * 3 + d] = v < 0 ? 0 : lens[v];
@@ -318,7 +320,7 @@ long long nuc3d_batch_launch_count(const nuc3d_batch *b) { return b ? b->eng->la
 int nuc3d_reconstruct(int scheme, int upwind, unsigned quirks, int nx, int ny, int nz,
                       const double *in, const double *hl, const double *hr, double *out,
                       void *stream) {
-    if (scheme < NUC3D_WENO5JS || scheme > NUC3D_CRWENO5)
+    if (scheme < NUC3D_WENO5JS || scheme > NUC3D_WENO7JS)
         return fail(NUC3D_ERR_UNSUPPORTED, "weno error: no such scheme");
     if (upwind != 1 && upwind != -1) return fail(NUC3D_ERR_INVALID, "weno error: no such direction");
     if (nx < 8 || ny < 1 || nz < 1) return fail(NUC3D_ERR_INVALID, "need nx >= 8, ny, nz >= 1");

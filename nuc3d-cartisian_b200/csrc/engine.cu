@@ -68,7 +68,7 @@ int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
     const int n[3] = {d.nx, d.ny, d.nz};
     for (int i = 0; i < 3; ++i) {
         if (n[i] < 8) return bad(NUC3D_ERR_INVALID, "every box extent must be >= 8 cells");
-        if (d.scheme[i] < NUC3D_WENO5JS || d.scheme[i] > NUC3D_CRWENO5)
+        if (d.scheme[i] < NUC3D_WENO5JS || d.scheme[i] > NUC3D_WENO7JS)
             return bad(NUC3D_ERR_UNSUPPORTED, "unknown reconstruction scheme");
     }
     for (int i = 0; i < 3; ++i)
@@ -254,7 +254,7 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));
     const bool mixed = precision_ == NUC3D_MIXED;
     std::vector<BoxDev> table(boxes_.size());
-    std::vector<WorkItem> prim, st25, inv[2][3], cr[3];
+    std::vector<WorkItem> prim, st25, inv[kSchemes][3], cr[3];
     const int crtl = crweno_tile_lines();
     for (int d = 0; d < 3; ++d) cr_nmax_[d] = cr_ms_[d] = 0;
     any_visc_ = false;
@@ -319,7 +319,7 @@ int Engine::rebuild() {
     };
     append(prim, r_prim_);
     append(st25, r_25d_);
-    for (int s = 0; s < 2; ++s)
+    for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) append(inv[s][d], r_inv_[s][d]);
     for (int d = 0; d < 3; ++d) append(cr[d], r_cr_[d]);
     if ((int)boxes_.size() > d_boxes_cap_) {
@@ -344,7 +344,7 @@ int Engine::rebuild() {
     ECK(prepare_inviscid_kernels(mixed));
     ECK(prepare_crweno_kernels(mixed));
     int per_stage = (r_prim_.n > 0) + (any_visc_ && r_25d_.n > 0) + (r_25d_.n > 0);
-    for (int s = 0; s < 2; ++s)
+    for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d].n > 0;
     for (int d = 0; d < 3; ++d) per_stage += r_cr_[d].n > 0;
     launches_per_step_ = 3 * per_stage + 3;  // + clear_eig, dt, residual
@@ -417,7 +417,7 @@ int Engine::enqueue_step_t(cudaStream_t st) {
         }
         for (int d = 0; d < 3; ++d) {
             ProfScope ps(this, NUC3D_PROF_INV_X + d);
-            for (int s = 0; s < 2; ++s)
+            for (int s = 0; s < kSchemes; ++s)
                 ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
                                         r_inv_[s][d].n, in, d > 0, st)));
             ECK((launch_crweno<B>(d, d_boxes_, it + r_cr_[d].off, r_cr_[d].n, in, d > 0,
@@ -464,13 +464,13 @@ int Engine::enqueue_step(cudaStream_t s) {
 // live state changes nothing.
 int Engine::autotune() {
     bool need = false;
-    for (int s = 0; s < 2; ++s)
+    for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) need = need || (r_inv_[s][d].n > 0 && inv_variant[s][d] < 0);
     if (!need) return NUC3D_OK;
     // NUC3D_SWEEP_RUN=1|2|4 pins the run length (reproducibility studies)
     if (const char *pin = std::getenv("NUC3D_SWEEP_RUN")) {
         int v = std::atoi(pin) == 1 ? 0 : (std::atoi(pin) == 2 ? 1 : 2);
-        for (int s = 0; s < 2; ++s)
+        for (int s = 0; s < kSchemes; ++s)
             for (int d = 0; d < 3; ++d)
                 if (r_inv_[s][d].n > 0 && inv_variant[s][d] < 0) inv_variant[s][d] = v;
         invalidate_graph();
@@ -482,7 +482,7 @@ int Engine::autotune() {
     ECK(cudaEventCreate(&e1));
     const bool mixed = precision_ == NUC3D_MIXED;
     int rc = NUC3D_OK;
-    for (int s = 0; s < 2 && rc == NUC3D_OK; ++s)
+    for (int s = 0; s < kSchemes && rc == NUC3D_OK; ++s)
         for (int d = 0; d < 3 && rc == NUC3D_OK; ++d) {
             const Range &rg = r_inv_[s][d];
             if (rg.n <= 0 || inv_variant[s][d] >= 0) continue;
@@ -596,7 +596,7 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
     ECK(launch_dt(d_boxes_, nb, stream_));
     if (any_visc_) ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_.off, r_25d_.n, stream_)));
     for (int d = 0; d < 3; ++d) {
-        for (int s = 0; s < 2; ++s)
+        for (int s = 0; s < kSchemes; ++s)
             ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
                                     r_inv_[s][d].n, 0, d > 0, stream_)));
         ECK((launch_crweno<B>(d, d_boxes_, it + r_cr_[d].off, r_cr_[d].n, 0, d > 0, cr_nmax_[d],

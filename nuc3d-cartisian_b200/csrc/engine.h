@@ -66,8 +66,8 @@ public:
     int profile_flush();
     // autotuned run length per [scheme JS/Z][dir] (-1: not tuned yet) and the
     // measured milliseconds per launch of each variant
-    int inv_variant[2][3] = {{-1, -1, -1}, {-1, -1, -1}};
-    double inv_tune_ms[2][3][kInvVariants] = {};
+    int inv_variant[kSchemes][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
+    double inv_tune_ms[kSchemes][3][kInvVariants] = {};
 
     static long long box_bytes(const nuc3d_box_desc &d);
     static int validate(const nuc3d_box_desc &d, std::string *why);
@@ -101,7 +101,7 @@ private:
         size_t off = 0;
         int n = 0;
     };
-    Range r_prim_, r_25d_, r_inv_[2][3];  // [scheme JS/Z][dir]
+    Range r_prim_, r_25d_, r_inv_[kSchemes][3];  // [scheme JS/Z/-/W7][dir]
     Range r_cr_[3];                       // CRWENO5 line tiles per dir
     int cr_nmax_[3] = {0, 0, 0}, cr_ms_[3] = {0, 0, 0};
     int launches_per_step_ = 0;

@@ -18,7 +18,11 @@ enum : unsigned {
     QK_CRWENO_BOUNDED = 0x10u,
 };
 
-enum : int { SCHEME_JS = 0, SCHEME_Z = 1, SCHEME_CR = 2 };
+enum : int { SCHEME_JS = 0, SCHEME_Z = 1, SCHEME_CR = 2, SCHEME_W7 = 3 };
+
+// reconstruction stencil half-width (the reference's bufferSize,
+// fieldOperator.cpp:128-175): 4 cells for weno7js, 3 for the WENO5 family
+__host__ __device__ constexpr int scheme_halo(int scheme) { return scheme == SCHEME_W7 ? 4 : 3; }
 enum : int { VISC_SUTHERLAND = 0, VISC_CONSTANT = 1, VISC_POWERLAW = 2 };
 
 // Everything a kernel needs to know about one periodic box.
@@ -208,6 +212,98 @@ template <int SCHEME, typename B>
 __device__ __forceinline__ B weno5_face(B f0, B f1, B f2, B f3, B f4, bool beta2_quirk) {
     if (SCHEME == SCHEME_Z) return weno5z_face(f0, f1, f2, f3, f4, beta2_quirk);
     return weno5js_face(f0, f1, f2, f3, f4);
+}
+
+// ------------------------------------------------------------------ WENO7 --
+// The reference's weno7js face (weno7js.cpp:79-126 for '+', :179-226 for
+// '-'; the boundary forms :227-824 are the same expression on halo cells).
+// f[0..6] is the upwind-oriented 7-cell stencil (f[0] farthest upwind).
+// Smoothness indicators: Balsara-Shu integer quadratic forms of the four
+// 4-cell sub-stencils (weno7js.cpp:83-106); candidates: the four cubic
+// interpolants (coeff_weno7_alpha, schemes.hpp); weights of Z type,
+// alpha_k = c_k (1 + (tau7/(eps + beta_k))^2) with tau7 = |beta0 - beta3|,
+// eps = 1e-20 and c = {1, 12, 18, 4}/35 (weno7js.cpp:107-123).
+struct K7 {
+    static constexpr double C0 = 1.0 / 35.0, C1 = 12.0 / 35.0, C2 = 18.0 / 35.0, C3 = 4.0 / 35.0;
+};
+
+// beta of a 4-cell sub-stencil a, b, c, d in the reference's nested form
+// a(k00 a + k01 b + k02 c + k03 d) + b(k11 b + k12 c + k13 d) + c(k22 c + k23 d)
+// + k33 d^2, evaluated with FMAs.
+template <typename B>
+__device__ __forceinline__ B weno7_form(B a, B b, B c, B d, double k00, double k01, double k02,
+                                        double k03, double k11, double k12, double k13,
+                                        double k22, double k23, double k33) {
+    B ta = fma_(B(k00), a, fma_(B(k01), b, fma_(B(k02), c, mul_(B(k03), d))));
+    B tb = fma_(B(k11), b, fma_(B(k12), c, mul_(B(k13), d)));
+    B tc = fma_(B(k22), c, mul_(B(k23), d));
+    return fma_(a, ta, fma_(b, tb, fma_(c, tc, mul_(mul_(B(k33), d), d))));
+}
+
+template <typename B>
+__device__ __forceinline__ void weno7_parts(B f0, B f1, B f2, B f3, B f4, B f5, B f6, B is[4],
+                                            B q[4]) {
+    is[0] = weno7_form(f0, f1, f2, f3, 547.0, -3882.0, 4642.0, -1854.0, 7043.0, -17246.0,
+                       7042.0, 11003.0, -9402.0, 2107.0);
+    is[1] = weno7_form(f1, f2, f3, f4, 267.0, -1642.0, 1602.0, -494.0, 2843.0, -5966.0, 1922.0,
+                       3443.0, -2522.0, 547.0);
+    is[2] = weno7_form(f2, f3, f4, f5, 547.0, -2522.0, 1922.0, -494.0, 3443.0, -5966.0, 1602.0,
+                       2843.0, -1642.0, 267.0);
+    is[3] = weno7_form(f3, f4, f5, f6, 2107.0, -9402.0, 7042.0, -1854.0, 11003.0, -17246.0,
+                       4642.0, 7043.0, -3882.0, 547.0);
+    // cubic candidates (1/12)(...): rows of coeff_weno7_alpha
+    q[0] = fma_(B(-3.0 / 12.0), f0, fma_(B(13.0 / 12.0), f1, fma_(B(-23.0 / 12.0), f2,
+                                                                   mul_(B(25.0 / 12.0), f3))));
+    q[1] = fma_(B(1.0 / 12.0), f1, fma_(B(-5.0 / 12.0), f2, fma_(B(13.0 / 12.0), f3,
+                                                                  mul_(B(3.0 / 12.0), f4))));
+    q[2] = fma_(B(-1.0 / 12.0), f2, fma_(B(7.0 / 12.0), f3, fma_(B(7.0 / 12.0), f4,
+                                                                  mul_(B(-1.0 / 12.0), f5))));
+    q[3] = fma_(B(3.0 / 12.0), f3, fma_(B(13.0 / 12.0), f4, fma_(B(-5.0 / 12.0), f5,
+                                                                  mul_(B(1.0 / 12.0), f6))));
+}
+
+// FP64 weights multiplied through by s0^2 s1^2 s2^2 s3^2 (s_k = beta_k + eps),
+// an exact rearrangement that needs one reciprocal:
+// alpha_k * prod s^2 = c_k (s_k^2 + tau^2) prod_{j != k} s_j^2.
+__device__ __forceinline__ double weno7_combine(const double is[4], const double q[4]) {
+    const double ss = 1.0e-20;
+    double tau = fabs(sub_(is[0], is[3]));
+    double t2 = mul_(tau, tau);
+    double s0 = add_(ss, is[0]), s1 = add_(ss, is[1]), s2 = add_(ss, is[2]), s3 = add_(ss, is[3]);
+    s0 = mul_(s0, s0);
+    s1 = mul_(s1, s1);
+    s2 = mul_(s2, s2);
+    s3 = mul_(s3, s3);
+    double p01 = mul_(s0, s1), p23 = mul_(s2, s3);
+    double w0 = mul_(mul_(K7::C0, add_(s0, t2)), mul_(s1, p23));
+    double w1 = mul_(mul_(K7::C1, add_(s1, t2)), mul_(s0, p23));
+    double w2 = mul_(mul_(K7::C2, add_(s2, t2)), mul_(s3, p01));
+    double w3 = mul_(mul_(K7::C3, add_(s3, t2)), mul_(s2, p01));
+    double num = fma_(w3, q[3], fma_(w2, q[2], fma_(w1, q[1], mul_(w0, q[0]))));
+    return mul_(num, __drcp_rn(add_(add_(add_(w0, w1), w2), w3)));
+}
+// FP32: the ratio tau/(beta+eps) is capped so that its square stays finite
+// (a cap only binds where one sub-stencil is exactly smooth and its weight
+// already carries the whole face).
+__device__ __forceinline__ float weno7_combine(const float is[4], const float q[4]) {
+    const float ss = 1.0e-20f, cap = 1.0e18f;
+    float tau = fabsf(sub_(is[0], is[3]));
+    float a[4];
+    const float c[4] = {float(K7::C0), float(K7::C1), float(K7::C2), float(K7::C3)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float t = fminf(mul_(tau, frcp_fast(add_(ss, is[k]))), cap);
+        a[k] = mul_(c[k], fma_(t, t, 1.0f));
+    }
+    float num = fma_(a[3], q[3], fma_(a[2], q[2], fma_(a[1], q[1], mul_(a[0], q[0]))));
+    return mul_(num, frcp_fast(add_(add_(add_(a[0], a[1]), a[2]), a[3])));
+}
+
+template <typename B>
+__device__ __forceinline__ B weno7_face(B f0, B f1, B f2, B f3, B f4, B f5, B f6) {
+    B is[4], q[4];
+    weno7_parts(f0, f1, f2, f3, f4, f5, f6, is, q);
+    return weno7_combine(is, q);
 }
 
 // CD6 first derivative (centraldifference6th.cpp:44-46), times 1/dx.

@@ -3,8 +3,9 @@
 // (fieldOperator.h:13-81) on device buffers, with explicit halos.
 //
 // Convention (as the reference): the operator runs along the fastest axis of
-// an (nx,ny,nz) field; halo_l / halo_r are (3,ny,nz) arrays holding the three
-// cells beyond each end of every line; reconstruction output is (nx+1,ny,nz).
+// an (nx,ny,nz) field; halo_l / halo_r are (H,ny,nz) arrays holding the H
+// cells beyond each end of every line (H = 4 for weno7js, 3 otherwise);
+// reconstruction output is (nx+1,ny,nz).
 #include "nuc3d_device.cuh"
 #include "op_kernels.h"
 
@@ -12,11 +13,12 @@ namespace nuc3d {
 
 namespace {
 
-// value of cell c (-3 <= c < nx+3) of line (j,k)
+// value of cell c (-H <= c < nx+H) of line (j,k); the halos are (H,ny,nz)
+template <int H = 3>
 __device__ __forceinline__ double line_at(const double *in, const double *hl, const double *hr,
                                           int nx, long long line, int c) {
-    if (c < 0) return hl[3 * line + (c + 3)];
-    if (c >= nx) return hr[3 * line + (c - nx)];
+    if (c < 0) return hl[H * line + (c + H)];
+    if (c >= nx) return hr[H * line + (c - nx)];
     return in[(long long)nx * line + c];
 }
 
@@ -42,6 +44,24 @@ __global__ void k_op_weno(int upwind, unsigned quirks, int nx, long long lines, 
                  m <= nx - 3;
     out[t] = SCHEME == SCHEME_Z ? weno5z_face(f[0], f[1], f[2], f[3], f[4], quirk)
                                 : weno5js_face(f[0], f[1], f[2], f[3], f[4]);
+}
+
+// One thread per face of weno7js (weno7js.cpp:17-824): face m reads cells
+// m-4..m+2 ('+') or m+3..m-3 ('-'); the boundary faces use the same
+// expression on halo cells.
+__global__ void k_op_weno7(int upwind, int nx, long long lines, const double *in,
+                           const double *hl, const double *hr, double *out) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long total = (long long)(nx + 1) * lines;
+    if (t >= total) return;
+    long long line = t / (nx + 1);
+    int m = (int)(t - line * (nx + 1));
+    double f[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+        f[k] = upwind > 0 ? line_at<4>(in, hl, hr, nx, line, m - 4 + k)
+                          : line_at<4>(in, hl, hr, nx, line, m + 3 - k);
+    out[t] = weno7_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6]);
 }
 
 // One thread per line: crweno5.cpp:45-402 + halo faces :425-837.  scratch
@@ -148,7 +168,9 @@ cudaError_t op_reconstruct(int scheme, int upwind, unsigned quirks, int nx, long
     }
     long long total = (long long)(nx + 1) * lines;
     unsigned grid = (unsigned)((total + 255) / 256);
-    if (scheme == SCHEME_Z)
+    if (scheme == SCHEME_W7)
+        k_op_weno7<<<grid, 256, 0, st>>>(upwind, nx, lines, in, hl, hr, out);
+    else if (scheme == SCHEME_Z)
         k_op_weno<SCHEME_Z><<<grid, 256, 0, st>>>(upwind, quirks, nx, lines, in, hl, hr, out);
     else
         k_op_weno<SCHEME_JS><<<grid, 256, 0, st>>>(upwind, quirks, nx, lines, in, hl, hr, out);

@@ -1,5 +1,5 @@
 // Batched whole-box kernels: primitive recovery, dt, residual and the
-// directional WENO5 sweeps.
+// directional WENO5 / WENO7 sweeps.
 //
 // One RK stage = k_prim -> [k_visc_flux25] -> k_inviscid<x> -> k_inviscid<y>
 // -> k_inviscid<z> -> k_update25, each one launch for every box of a batch.
@@ -119,18 +119,19 @@ __global__ void k_residual(const BoxDev *boxes, int nboxes) {
 
 // -------------------------------------------------------------- k_inviscid --
 // Tile of the directional sweep: TL lines x TC cells along the sweep; every
-// thread owns one line and a run of R consecutive faces of it.
+// thread owns one line and a run of R consecutive faces of it.  H is the
+// stencil half-width (3 for WENO5, 4 for WENO7).
 //   DIR 0 (x): 16 lines (rows j) per tile; the 8 runs of a line sit in 8
 //              consecutive lanes.
 //   DIR 1/2:   TL = one 128-byte row of B (16 FP64 / 32 FP32 columns i) per
 //              tile; consecutive lanes are consecutive lines (coalesced).
-template <int DIR, typename B, int RUN>
+template <int DIR, typename B, int RUN, int H = 3>
 struct InvGeom {
     static constexpr int R = RUN;               // faces per thread (1, 2 or 4)
     static constexpr int NR = 32 / RUN;         // runs per line
     static constexpr int TC = R * NR;           // cells per tile along the sweep (32)
     static constexpr int TL = DIR == 0 ? 16 : 128 / (int)sizeof(B);
-    static constexpr int NF = TC + 6;           // staged cells (3-cell halo each side)
+    static constexpr int NF = TC + 2 * H;       // staged cells (H-cell halo each side)
     static constexpr int S = (NF + R - 1) / R;  // DIR 0 interleave stride
     static constexpr int NT = TL * NR;          // threads
     static constexpr int SF = DIR == 0 ? TL * R * S : NF * TL;  // staged values per flux
@@ -144,7 +145,7 @@ struct InvGeom {
             r = t / TL;
         }
     }
-    // staged position pc (cell c0 - 3 + pc) of line l for flux v.  DIR 0
+    // staged position pc (cell c0 - H + pc) of line l for flux v.  DIR 0
     // interleaves positions so that the runs of a line (stride R) read
     // consecutive words.
     __device__ static int sf(int v, int l, int pc) {
@@ -201,7 +202,8 @@ template <int SCHEME, int DIR, typename B, int RUN>
 __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
     k_inviscid(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, int in_slot,
                int accumulate) {
-    using G = InvGeom<DIR, B, RUN>;
+    constexpr int H = scheme_halo(SCHEME);
+    using G = InvGeom<DIR, B, RUN, H>;
     constexpr int TL = G::TL, TC = G::TC, NF = G::NF, R = G::R, NR = G::NR, NT = G::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     B *sF = reinterpret_cast<B *>(smem_raw);  // [10][SF] split fluxes (+ e, then - e)
@@ -276,13 +278,13 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
         }
         __syncthreads();
     }
-    // phase 1: stage the split fluxes of cells c0-3 .. c0+TC+2
+    // phase 1: stage the split fluxes of cells c0-H .. c0+TC+H-1
     for (int t = threadIdx.x; t < TL * NF; t += NT) {
         int l, pc;
         G::stage_item(t, l, pc);
         double Fp[5], Fm[5];
         if (l0 + l < nl) {
-            int pos = c0 - 3 + pc;  // in [-3, n + NF): wrap without a division
+            int pos = c0 - H + pc;  // in [-H, n + NF): wrap without a division (n >= 8 > H)
             if (pos < 0) pos += n;
             while (pos >= n) pos -= n;
             split(gidx(l, pos), Fp, Fm);
@@ -317,6 +319,35 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
 #pragma unroll 1
     for (int e = 0; e < 5; ++e) {
         B Fh[R + 1];
+        if constexpr (SCHEME == SCHEME_W7) {
+            // face m: '+' reads positions m..m+6 (cells m-4..m+2), '-' reads
+            // m+7..m+1 (cells m+3..m-3)
+            B f[7];
+#pragma unroll
+            for (int j = 0; j < 7; ++j) f[j] = sF[G::sf(e, l, m0 + j)];
+#pragma unroll
+            for (int k = 0; k <= R; ++k) {
+                if (k == R && !last) break;
+                Fh[k] = weno7_face<B>(f[0], f[1], f[2], f[3], f[4], f[5], f[6]);
+                if (k < R) {
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) f[j] = f[j + 1];
+                    f[6] = sF[G::sf(e, l, m0 + k + 7)];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 7; ++j) f[j] = sF[G::sf(5 + e, l, m0 + 7 - j)];
+#pragma unroll
+            for (int k = 0; k <= R; ++k) {
+                if (k == R && !last) break;
+                Fh[k] = add_(Fh[k], weno7_face<B>(f[0], f[1], f[2], f[3], f[4], f[5], f[6]));
+                if (k < R) {
+#pragma unroll
+                    for (int j = 6; j > 0; --j) f[j] = f[j - 1];
+                    f[0] = (m0 + k + 8 < NF) ? sF[G::sf(5 + e, l, m0 + k + 8)] : B(0);
+                }
+            }
+        } else {
         {  // '+' side: window f0..f4 = positions m..m+4
             const int v = e;
             B f0 = sF[G::sf(v, l, m0)], f1 = sF[G::sf(v, l, m0 + 1)], f2 = sF[G::sf(v, l, m0 + 2)];
@@ -362,6 +393,7 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
                 }
             }
         }
+        }
         B *x = xb + (e & 1) * NT;
         x[threadIdx.x] = Fh[0];
         __syncthreads();
@@ -381,9 +413,9 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
 }
 
 // --------------------------------------------------------------- launches --
-template <int DIR, typename B, int RUN>
+template <int SCHEME, int DIR, typename B, int RUN>
 static size_t inv_smem_t() {
-    using G = InvGeom<DIR, B, RUN>;
+    using G = InvGeom<DIR, B, RUN, scheme_halo(SCHEME)>;
     return sizeof(B) * (size_t)(10 * G::SF + 2 * G::NT);
 }
 
@@ -398,9 +430,9 @@ InvTileDims inviscid_tile(int dir, bool mixed) {
 template <int SCHEME, int DIR, typename B, int RUN>
 static cudaError_t launch_t(const BoxDev *boxes, const WorkItem *items, int nitems, int in_slot,
                             int accumulate, cudaStream_t st) {
-    using G = InvGeom<DIR, B, RUN>;
+    using G = InvGeom<DIR, B, RUN, scheme_halo(SCHEME)>;
     if (nitems <= 0) return cudaSuccess;
-    k_inviscid<SCHEME, DIR, B, RUN><<<nitems, G::NT, inv_smem_t<DIR, B, RUN>(), st>>>(
+    k_inviscid<SCHEME, DIR, B, RUN><<<nitems, G::NT, inv_smem_t<SCHEME, DIR, B, RUN>(), st>>>(
         boxes, items, in_slot, accumulate);
     return cudaGetLastError();
 }
@@ -419,6 +451,7 @@ template <typename B>
 cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxes,
                             const WorkItem *items, int nitems, int in_slot, int accumulate,
                             cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
     if (scheme == SCHEME_JS) {
         if (dir == 0) return launch_v<SCHEME_JS, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
         if (dir == 1) return launch_v<SCHEME_JS, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
@@ -429,6 +462,11 @@ cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxe
         if (dir == 1) return launch_v<SCHEME_Z, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
         return launch_v<SCHEME_Z, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
     }
+    if (scheme == SCHEME_W7) {
+        if (dir == 0) return launch_v<SCHEME_W7, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+        if (dir == 1) return launch_v<SCHEME_W7, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+        return launch_v<SCHEME_W7, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+    }
     return cudaErrorInvalidValue;
 }
 
@@ -436,7 +474,7 @@ template <int SCHEME, int DIR, typename B, int RUN>
 static cudaError_t prepare_t() {
     return cudaFuncSetAttribute(k_inviscid<SCHEME, DIR, B, RUN>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)inv_smem_t<DIR, B, RUN>());
+                                (int)inv_smem_t<SCHEME, DIR, B, RUN>());
 }
 template <int SCHEME, int DIR, typename B>
 static cudaError_t prepare_runs() {
@@ -448,9 +486,11 @@ static cudaError_t prepare_runs() {
 }
 template <typename B>
 static cudaError_t prepare_all() {
-    cudaError_t e[6] = {prepare_runs<SCHEME_JS, 0, B>(), prepare_runs<SCHEME_JS, 1, B>(),
+    cudaError_t e[9] = {prepare_runs<SCHEME_JS, 0, B>(), prepare_runs<SCHEME_JS, 1, B>(),
                         prepare_runs<SCHEME_JS, 2, B>(), prepare_runs<SCHEME_Z, 0, B>(),
-                        prepare_runs<SCHEME_Z, 1, B>(), prepare_runs<SCHEME_Z, 2, B>()};
+                        prepare_runs<SCHEME_Z, 1, B>(), prepare_runs<SCHEME_Z, 2, B>(),
+                        prepare_runs<SCHEME_W7, 0, B>(), prepare_runs<SCHEME_W7, 1, B>(),
+                        prepare_runs<SCHEME_W7, 2, B>()};
     for (cudaError_t x : e)
         if (x != cudaSuccess) return x;
     return cudaSuccess;

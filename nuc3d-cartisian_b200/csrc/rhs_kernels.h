@@ -100,6 +100,9 @@ cudaError_t launch_clear_eig(const BoxDev *boxes, int nboxes, cudaStream_t st);
 // variant: run length of the sweep kernel, 0 -> 1 face per thread,
 // 1 -> 2, 2 -> 4 (picked per scheme and direction by the engine's autotuner)
 constexpr int kInvVariants = 3;
+// scheme slots of the per-scheme sweep tables (indexed by scheme id; the
+// CRWENO5 slot stays empty, its lines run in launch_crweno)
+constexpr int kSchemes = 4;
 template <typename B>
 cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxes,
                             const WorkItem *items, int nitems, int in_slot, int accumulate,

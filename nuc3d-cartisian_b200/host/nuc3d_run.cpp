@@ -59,11 +59,19 @@ std::vector<std::string> words(const std::string &path, bool required) {
     return w;
 }
 
+// fieldOperator3d::setMethodIvs* (fieldOperator.cpp:128-180): a string the
+// reference does not know falls back to weno5js; the reference's other
+// schemes are not on this path and stop the run.
 int scheme_id(const std::string &s) {
     if (s == "weno5js") return NUC3D_WENO5JS;
     if (s == "weno5z") return NUC3D_WENO5Z;
     if (s == "crweno5") return NUC3D_CRWENO5;
-    die("reconstruction scheme '" + s + "' is not on the B200 path (weno5js, weno5z, crweno5)");
+    if (s == "weno7js") return NUC3D_WENO7JS;
+    for (const char *other : {"hccs", "hccs77", "hccs78", "weno3js", "upwind1st"})
+        if (s == other)
+            die("reconstruction scheme '" + s +
+                "' is not on the B200 path (weno5js, weno5z, crweno5, weno7js)");
+    return NUC3D_WENO5JS;
 }
 
 Case read_case(const std::string &dir) {

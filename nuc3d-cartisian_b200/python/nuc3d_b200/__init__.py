@@ -21,8 +21,9 @@ OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2
 ERR_TIMEOUT, ERR_CANCELLED = -6, -7
 INIT_STATE, INIT_TGV, INIT_HIT = 0, 1, 2
 FORCING_NONE, FORCING_CONST = 0, 1
-WENO5JS, WENO5Z, CRWENO5 = 0, 1, 2
-SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5}
+WENO5JS, WENO5Z, CRWENO5, WENO7JS = 0, 1, 2, 3
+SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5, "weno7js": WENO7JS}
+TUNING_SLOTS = 12  # NUC3D_TUNING_SLOTS: (scheme id, direction) pairs
 EULER3D, NAVIERSTOKES3D = 0, 1
 SUTHERLAND, CONSTANT, POWERLAW = 0, 1, 2
 FP64, MIXED = 0, 1
@@ -585,11 +586,11 @@ class Server:
 def _tuning(fn, h):
     """{(scheme, dir): (chosen run length, {run length: ms per launch})}"""
     import numpy as np
-    rl = np.zeros(6, dtype=np.int32)
-    ms = np.zeros(18)
+    rl = np.zeros(TUNING_SLOTS, dtype=np.int32)
+    ms = np.zeros(3 * TUNING_SLOTS)
     check(fn(h, rl.ctypes.data, ms.ctypes.data))
     out = {}
-    for s, sname in enumerate(("weno5js", "weno5z")):
+    for s, sname in enumerate(("weno5js", "weno5z", "crweno5", "weno7js")):
         for d, dname in enumerate("xyz"):
             if rl[s * 3 + d]:
                 out[f"{sname}_{dname}"] = (int(rl[s * 3 + d]), {

@@ -14,6 +14,18 @@ from pathlib import Path
 from . import (CONSTANT, EULER3D, FORCING_CONST, FORCING_NONE, NAVIERSTOKES3D, SCHEMES,
                SUTHERLAND, BoxDesc)
 
+_NOT_ON_PATH = ("hccs", "hccs77", "hccs78", "weno3js", "upwind1st")
+
+
+def _scheme(name: str) -> int:
+    """fieldOperator3d::setMethodIvs* (fieldOperator.cpp:128-180): unknown
+    strings fall back to weno5js; the reference's other schemes are refused."""
+    if name in _NOT_ON_PATH:
+        raise ValueError(f"reconstruction scheme {name!r} is not on the B200 path "
+                         f"({', '.join(SCHEMES)})")
+    return SCHEMES.get(name, SCHEMES["weno5js"])
+
+
 _METHOD_DEFAULTS = {"scheme_time": "RK3", "scheme_x_ivs": "weno5js", "scheme_y_ivs": "weno5js",
                     "scheme_z_ivs": "weno5js", "scheme_x_vis": "cd6", "scheme_y_vis": "cd6",
                     "scheme_z_vis": "cd6"}
@@ -73,7 +85,7 @@ def read_decks(dirpath):
         raise ValueError(f"Model Name:{pos[3]} does not exist!")
     visc = {"Sutherland": SUTHERLAND, "Constant": CONSTANT}.get(pos[4], SUTHERLAND)
     desc = BoxDesc(nx=nx, ny=ny, nz=nz, lx=lx, ly=ly, lz=lz,
-                   scheme=tuple(SCHEMES.get(method[f"scheme_{a}_ivs"], 0) for a in "xyz"),
+                   scheme=tuple(_scheme(method[f"scheme_{a}_ivs"]) for a in "xyz"),
                    pde_model=models[pos[3]], visc_model=visc, gamma=phys["Gamma"],
                    mach=phys["Mach"], reynolds=phys["Reynolds"], prandtl=phys["Pt"],
                    t_ref=phys["T_ref"], t_inf=phys["T_inf"],

@@ -34,6 +34,7 @@ def parsed(text):
     dict(nx=24, ny=20, nz=16, mach=0.1, reynolds=1600.0, prandtl=0.71),
     dict(nx=40, ny=32, nz=24, scheme=(1, 2, 0), pde_model=0, mach=0.3, reynolds=250.5),
     dict(nx=16, ny=16, nz=16, scheme=(2, 2, 2), visc_model=1, gamma=1.3, lx=1.5, ly=2.5, lz=3.5),
+    dict(nx=20, ny=18, nz=16, scheme=(3, 0, 3)),
     dict(nx=32, ny=32, nz=32, forcing=1, forcing_amp=0.02, forcing_hel=0.1, forcing_k=2.0),
 ])
 def test_driver_reads_decks_like_the_python_reader(driver, tmp_path, kw):
@@ -76,5 +77,10 @@ def test_driver_rejects_what_the_path_does_not_cover(driver, tmp_path):
     (inp / "PhysModel.in").write_text((inp / "PhysModel.in").read_text() + "Bogus 1.0\n")
     r = run(driver, tmp_path, "--check-decks")
     assert r.returncode != 0 and "word Bogus does not exist" in r.stderr
+    nb.write_decks(tmp_path, nb.BoxDesc(16, 16, 16))
+    text = (inp / "Method.in").read_text().replace("scheme_z_ivs weno5js", "scheme_z_ivs weno3js")
+    (inp / "Method.in").write_text(text)
+    r = run(driver, tmp_path, "--check-decks")
+    assert r.returncode != 0 and "weno3js" in r.stderr
     r = run(driver, "--help")
     assert r.returncode == 0 and "usage" in r.stdout

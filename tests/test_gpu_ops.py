@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from helpers import golden, rel_l2
-from oracle_ctypes import QUIRKS_REFERENCE, Q_WENOZ_BETA2, Oracle
+from oracle_ctypes import QUIRKS_REFERENCE, Q_WENOZ_BETA2, WENO7, Oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -56,6 +56,40 @@ def test_reconstruct_vs_oracle_larger(torch_cuda, scheme, up, quirks):
     ref = Oracle().reconstruct_field(scheme, up, quirks, f, hl, hr)
     out = torch.zeros(shape[:2] + (shape[2] + 1,), dtype=torch.float64, device="cuda")
     nb.reconstruct(scheme, up, quirks, to_dev(torch, f), to_dev(torch, hl), to_dev(torch, hr), out)
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), ref) < TOL_OP
+
+
+@pytest.mark.parametrize("up", [1, -1])
+def test_weno7_reconstruct_golden(torch_cuda, up):
+    """weno7js with its 4-cell halos against the reference's own outputs."""
+    import nuc3d_b200 as nb
+    torch = torch_cuda
+    z = golden("operators_w7.npz")
+    tag = f"w7_{'p' if up > 0 else 'm'}"
+    fin = to_dev(torch, z[f"rec_{tag}_in"])
+    out = torch.zeros(fin.shape[:2] + (fin.shape[2] + 1,), dtype=torch.float64, device="cuda")
+    nb.reconstruct(WENO7, up, QUIRKS_REFERENCE, fin, to_dev(torch, z[f"rec_{tag}_hl"]),
+                   to_dev(torch, z[f"rec_{tag}_hr"]), out)
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), z[f"rec_{tag}_out"]) < TOL_OP
+
+
+@pytest.mark.parametrize("up", [1, -1])
+def test_weno7_reconstruct_vs_oracle_larger(torch_cuda, up):
+    """Rough data (values spread over decades, so the Z weights switch) on
+    lines of 61 cells."""
+    import nuc3d_b200 as nb
+    torch = torch_cuda
+    rng = np.random.default_rng(70 + up)
+    shape = (7, 9, 61)
+    f = rng.standard_normal(shape) * np.exp(rng.standard_normal(shape))
+    hl = rng.standard_normal(shape[:2] + (4,))
+    hr = rng.standard_normal(shape[:2] + (4,))
+    ref = Oracle().reconstruct_field(WENO7, up, QUIRKS_REFERENCE, f, hl, hr)
+    out = torch.zeros(shape[:2] + (shape[2] + 1,), dtype=torch.float64, device="cuda")
+    nb.reconstruct(WENO7, up, QUIRKS_REFERENCE, to_dev(torch, f), to_dev(torch, hl),
+                   to_dev(torch, hr), out)
     torch.cuda.synchronize()
     assert rel_l2(out.cpu().numpy(), ref) < TOL_OP
 

@@ -11,12 +11,12 @@ import pytest
 
 from helpers import box_from_golden, desc_from_box, golden, max_rel_l2, rel_l2
 from oracle_ctypes import (CRWENO5, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_OFFDIAG_DIV,
-                           Q_WENOZ_BETA2, Q_ZETA_EIGEN, WENO5JS, WENO5Z, Box, Oracle)
+                           Q_WENOZ_BETA2, Q_ZETA_EIGEN, WENO5JS, WENO5Z, WENO7, Box, Oracle)
 
 pytestmark = pytest.mark.gpu
 
 TOL_FP64 = 1e-12
-TAGS = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr"}
+TAGS = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr", WENO7: "w7"}
 
 
 @pytest.fixture(scope="module")
@@ -46,7 +46,7 @@ def gpu_steps(box, q, nsteps, cfl=0.5, precision=0):
         return s.get_state(), dt, res
 
 
-@pytest.mark.parametrize("scheme", [WENO5JS, WENO5Z, CRWENO5])
+@pytest.mark.parametrize("scheme", [WENO5JS, WENO5Z, CRWENO5, WENO7])
 @pytest.mark.parametrize("ns", [True, False])
 def test_rhs_and_three_steps_match_reference(torch, scheme, ns):
     z = golden(f"step_{TAGS[scheme]}_{'ns' if ns else 'eu'}.npz")
@@ -68,7 +68,7 @@ def test_taylor_green_24_ten_steps_match_reference(torch):
     np.testing.assert_allclose(dt, z["dt"], rtol=1e-12)
 
 
-@pytest.mark.parametrize("scheme", [WENO5JS, WENO5Z, CRWENO5])
+@pytest.mark.parametrize("scheme", [WENO5JS, WENO5Z, CRWENO5, WENO7])
 def test_textbook_variants_match_oracle(torch, scheme):
     """Every quirk switched off (periodic CRWENO lines, textbook WENO5-Z beta2,
     no off-diagonal divergence, z eigenvalue kept) on a non-cubic box."""
@@ -105,8 +105,10 @@ def test_crweno_long_lines_match_oracle(torch, bounded, shape):
     assert max_rel_l2(qg, qo) < TOL_FP64
 
 
-def test_mixed_schemes_per_direction_match_oracle(torch):
-    box = Box(18, 14, 10, scheme=(WENO5Z, CRWENO5, WENO5JS), mach=0.15)
+@pytest.mark.parametrize("schemes", [(WENO5Z, CRWENO5, WENO5JS), (WENO7, WENO5Z, CRWENO5),
+                                     (CRWENO5, WENO7, WENO7)])
+def test_mixed_schemes_per_direction_match_oracle(torch, schemes):
+    box = Box(18, 14, 10, scheme=schemes, mach=0.15)
     O = Oracle()
     q = O.tgv(box)
     qo, _, _ = O.run_steps(box, 0.5, 3, q)
@@ -114,7 +116,7 @@ def test_mixed_schemes_per_direction_match_oracle(torch):
     assert max_rel_l2(qg, qo) < TOL_FP64
 
 
-@pytest.mark.parametrize("scheme", [WENO5JS, WENO5Z, CRWENO5])
+@pytest.mark.parametrize("scheme", [WENO5JS, WENO5Z, CRWENO5, WENO7])
 def test_conservation_at_64(torch, scheme):
     """Periodic conservative differencing: total mass, momentum and energy are
     invariant up to summation rounding (size-independent property)."""
@@ -152,6 +154,24 @@ def test_mixed_precision_close_to_fp64(torch):
     print(f"mixed vs fp64 after 100 steps: max per-field rel L2 = {err:.3e}")
     assert err < 1e-6
     assert abs(ke[0] - ke[1]) <= 5e-3 * ke[1]
+
+
+def test_weno7_mixed_precision_close_to_fp64(torch):
+    """WENO7 with FP32 bulk arithmetic against its FP64 path: decaying
+    turbulence at 64^3 (M = 1, Mt = 0.3, Re_lambda = 100, k_peak = 4), 50
+    steps, per-field relative L2 below 1e-6."""
+    import nuc3d_b200 as nb
+    desc = nb.BoxDesc(64, 64, 64, mach=1.0, scheme=(nb.WENO7JS,) * 3)
+    init = {"kind": "hit", "seed": 3, "k_peak": 4.0, "mach_t": 0.3, "re_lambda": 100.0}
+    out = []
+    for precision in (nb.FP64, nb.MIXED):
+        with nb.Solver(nb.BoxDesc(**{**desc.__dict__, "precision": precision})) as s:
+            s.init_state(init)
+            s.step(50, 0.5, stats=False)
+            out.append(s.get_state())
+    err = max_rel_l2(out[1], out[0])
+    print(f"weno7 mixed vs fp64 after 50 steps: max per-field rel L2 = {err:.3e}")
+    assert err < 1e-6
 
 
 def test_nonfinite_state_is_reported(torch):

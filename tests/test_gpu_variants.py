@@ -16,12 +16,12 @@ ROOT = Path(__file__).resolve().parents[1]
 SCRIPT = r"""
 import sys, numpy as np
 sys.path.insert(0, "oracle"); sys.path.insert(0, "nuc3d-cartisian_b200/python"); sys.path.insert(0, "tests")
-from oracle_ctypes import Box, Oracle, WENO5JS, WENO5Z
+from oracle_ctypes import Box, Oracle, WENO5JS, WENO5Z, WENO7
 from helpers import desc_from_box
 import nuc3d_b200 as nb
 prec = int(sys.argv[2])
 out = []
-for sch in (WENO5JS, WENO5Z):
+for sch in (WENO5JS, WENO5Z, WENO7):
     box = Box(40, 24, 36, scheme=(sch,) * 3, mach=0.3, reynolds=700.0)
     rng = np.random.default_rng(5)
     q = [np.ascontiguousarray(a * (1 + 0.02 * rng.standard_normal(a.shape))) for a in Oracle().tgv(box)]
