@@ -229,20 +229,23 @@ struct K7 {
 
 // beta of a 4-cell sub-stencil a, b, c, d in the reference's nested form
 // a(k00 a + k01 b + k02 c + k03 d) + b(k11 b + k12 c + k13 d) + c(k22 c + k23 d)
-// + k33 d^2, evaluated with FMAs.
-template <typename B>
-__device__ __forceinline__ B weno7_form(B a, B b, B c, B d, double k00, double k01, double k02,
-                                        double k03, double k11, double k12, double k13,
-                                        double k22, double k23, double k33) {
-    B ta = fma_(B(k00), a, fma_(B(k01), b, fma_(B(k02), c, mul_(B(k03), d))));
-    B tb = fma_(B(k11), b, fma_(B(k12), c, mul_(B(k13), d)));
-    B tc = fma_(B(k22), c, mul_(B(k23), d));
-    return fma_(a, ta, fma_(b, tb, fma_(c, tc, mul_(mul_(B(k33), d), d))));
+// + k33 d^2.  The form cancels heavily (its coefficients sum to zero, so
+// terms of size 1e4 f^2 cancel down to 1e2 (f' dx)^2): the rounding of each
+// operation shows in beta.  FP64 therefore evaluates it unfused, in the
+// reference's left-to-right order, which keeps the faces within ~1e-14 of
+// the reference where a fused evaluation drifts to ~1e-12 in the RHS.
+__device__ __forceinline__ double weno7_form(double a, double b, double c, double d, double k00,
+                                             double k01, double k02, double k03, double k11,
+                                             double k12, double k13, double k22, double k23,
+                                             double k33) {
+    double ta = add_(add_(add_(mul_(k00, a), mul_(k01, b)), mul_(k02, c)), mul_(k03, d));
+    double tb = add_(add_(mul_(k11, b), mul_(k12, c)), mul_(k13, d));
+    double tc = add_(mul_(k22, c), mul_(k23, d));
+    return add_(add_(add_(mul_(a, ta), mul_(b, tb)), mul_(c, tc)), mul_(mul_(k33, d), d));
 }
-
-template <typename B>
-__device__ __forceinline__ void weno7_parts(B f0, B f1, B f2, B f3, B f4, B f5, B f6, B is[4],
-                                            B q[4]) {
+__device__ __forceinline__ void weno7_parts(double f0, double f1, double f2, double f3, double f4,
+                                            double f5, double f6, double is[4], double q[4]) {
+    using B = double;
     is[0] = weno7_form(f0, f1, f2, f3, 547.0, -3882.0, 4642.0, -1854.0, 7043.0, -17246.0,
                        7042.0, 11003.0, -9402.0, 2107.0);
     is[1] = weno7_form(f1, f2, f3, f4, 267.0, -1642.0, 1602.0, -494.0, 2843.0, -5966.0, 1922.0,
@@ -282,28 +285,57 @@ __device__ __forceinline__ double weno7_combine(const double is[4], const double
     double num = fma_(w3, q[3], fma_(w2, q[2], fma_(w1, q[1], mul_(w0, q[0]))));
     return mul_(num, __drcp_rn(add_(add_(add_(w0, w1), w2), w3)));
 }
-// FP32: the ratio tau/(beta+eps) is capped so that its square stays finite
-// (a cap only binds where one sub-stencil is exactly smooth and its weight
-// already carries the whole face).
-__device__ __forceinline__ float weno7_combine(const float is[4], const float q[4]) {
+__device__ __forceinline__ double weno7_face(double f0, double f1, double f2, double f3, double f4,
+                                             double f5, double f6) {
+    double is[4], q[4];
+    weno7_parts(f0, f1, f2, f3, f4, f5, f6, is, q);
+    return weno7_combine(is, q);
+}
+
+// FP32 (mixed path): the same indicators and candidates rewritten exactly in
+// first and second differences, which removes the cancellation instead of
+// ordering it.  With delta_j = f_j - f_{j-1} and sigma_j = delta_j -
+// delta_{j-1}, sub-stencil k has u = delta_{k+2}, a = sigma_{k+2},
+// b = sigma_{k+3} and
+//   beta_k = 240 u^2 + p_k u a + r_k u b + s_k a^2 + t_k a b + v_k b^2
+// (the Balsara-Shu forms under that change of variables), and each cubic
+// candidate is f3 plus an integer combination of deltas over 12.  Smooth data
+// gives beta ~ 240 u^2 with small corrections, so FP32 rounding stays
+// relative to the differences, not to the flux itself.
+__device__ __forceinline__ float w7_beta(float u, float a, float b, float p, float r, float s,
+                                         float t, float v) {
+    float tu = fma_(r, b, fma_(p, a, mul_(240.0f, u)));
+    float ta = fma_(t, b, mul_(s, a));
+    return fma_(u, tu, fma_(a, ta, mul_(mul_(v, b), b)));
+}
+__device__ __forceinline__ float weno7_face(float f0, float f1, float f2, float f3, float f4,
+                                            float f5, float f6) {
+    float d1 = sub_(f1, f0), d2 = sub_(f2, f1), d3 = sub_(f3, f2);
+    float d4 = sub_(f4, f3), d5 = sub_(f5, f4), d6 = sub_(f6, f5);
+    float s2 = sub_(d2, d1), s3 = sub_(d3, d2), s4 = sub_(d4, d3), s5 = sub_(d5, d4),
+          s6 = sub_(d6, d5);
+    float is[4], r[4];
+    is[0] = w7_beta(d2, s2, s3, -160.0f, 880.0f, 547.0f, -1854.0f, 2107.0f);
+    is[1] = w7_beta(d3, s3, s4, 80.0f, 160.0f, 267.0f, -494.0f, 547.0f);
+    is[2] = w7_beta(d4, s4, s5, -160.0f, -80.0f, 547.0f, -494.0f, 267.0f);
+    is[3] = w7_beta(d5, s5, s6, -880.0f, 160.0f, 2107.0f, -1854.0f, 547.0f);
+    // 12 (q_k - f3)
+    r[0] = fma_(3.0f, d1, fma_(-10.0f, d2, mul_(13.0f, d3)));
+    r[1] = fma_(-1.0f, d2, fma_(4.0f, d3, mul_(3.0f, d4)));
+    r[2] = fma_(-1.0f, d5, fma_(6.0f, d4, d3));
+    r[3] = fma_(9.0f, d4, fma_(-4.0f, d5, d6));
     const float ss = 1.0e-20f, cap = 1.0e18f;
-    float tau = fabsf(sub_(is[0], is[3]));
-    float a[4];
     const float c[4] = {float(K7::C0), float(K7::C1), float(K7::C2), float(K7::C3)};
+    float tau = fabsf(sub_(is[0], is[3]));
+    float al[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         float t = fminf(mul_(tau, frcp_fast(add_(ss, is[k]))), cap);
-        a[k] = mul_(c[k], fma_(t, t, 1.0f));
+        al[k] = mul_(c[k], fma_(t, t, 1.0f));
     }
-    float num = fma_(a[3], q[3], fma_(a[2], q[2], fma_(a[1], q[1], mul_(a[0], q[0]))));
-    return mul_(num, frcp_fast(add_(add_(add_(a[0], a[1]), a[2]), a[3])));
-}
-
-template <typename B>
-__device__ __forceinline__ B weno7_face(B f0, B f1, B f2, B f3, B f4, B f5, B f6) {
-    B is[4], q[4];
-    weno7_parts(f0, f1, f2, f3, f4, f5, f6, is, q);
-    return weno7_combine(is, q);
+    float num = fma_(al[3], r[3], fma_(al[2], r[2], fma_(al[1], r[1], mul_(al[0], r[0]))));
+    float den = add_(add_(add_(al[0], al[1]), al[2]), al[3]);
+    return fma_(mul_(num, frcp_fast(den)), 1.0f / 12.0f, f3);
 }
 
 // CD6 first derivative (centraldifference6th.cpp:44-46), times 1/dx.

@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
 #pragma unroll
             for (int k = 0; k <= R; ++k) {
                 if (k == R && !last) break;
-                Fh[k] = weno7_face<B>(f[0], f[1], f[2], f[3], f[4], f[5], f[6]);
+                Fh[k] = weno7_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6]);
                 if (k < R) {
 #pragma unroll
                     for (int j = 0; j < 6; ++j) f[j] = f[j + 1];
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
 #pragma unroll
             for (int k = 0; k <= R; ++k) {
                 if (k == R && !last) break;
-                Fh[k] = add_(Fh[k], weno7_face<B>(f[0], f[1], f[2], f[3], f[4], f[5], f[6]));
+                Fh[k] = add_(Fh[k], weno7_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6]));
                 if (k < R) {
 #pragma unroll
                     for (int j = 6; j > 0; --j) f[j] = f[j - 1];

@@ -40,3 +40,19 @@ def desc_from_box(box, precision=0):
                       reynolds=box.reynolds, prandtl=box.prandtl, t_ref=box.t_ref,
                       t_inf=box.t_inf, powerlaw_exp=box.powerlaw_exp, precision=precision,
                       quirks=box.quirks)
+
+
+def rounding_sensitivity(box, q, nsteps, cfl=0.5, seed=0):
+    """How far the oracle's own state after `nsteps` moves when every input
+    value is moved by one ulp (max per-field relative L2).  The reference's
+    weno7js is ill-conditioned with respect to rounding (its expanded
+    Balsara-Shu indicators cancel terms of size 1e4 f^2), so two correct
+    implementations that round differently agree only to about this level;
+    WENO5 schemes give ~1e-13 here, weno7js ~1e-12 to 1e-9."""
+    from oracle_ctypes import Oracle
+    O = Oracle()
+    rng = np.random.default_rng(seed)
+    qp = [np.nextafter(a, np.where(rng.random(a.shape) < 0.5, -np.inf, np.inf)) for a in q]
+    a, _, _ = O.run_steps(box, cfl, nsteps, list(q))
+    b, _, _ = O.run_steps(box, cfl, nsteps, qp)
+    return max_rel_l2(a, b)
