@@ -348,6 +348,8 @@ def run_b200(args, rank, world, local_rank):
             "autotuned_sweep_variant": tuning32,
         }
 
+    schemes = None if args.skip_schemes else run_schemes(args, desc, q, stream, timed_steps,
+                                                         max_over_ranks)
     ensemble = None if args.skip_ensemble else run_ensemble(args, stream, barrier, max_over_ranks,
                                                             world, rank)
     served = None if (args.skip_serve or world > 1) else run_served(args)
@@ -381,12 +383,44 @@ def run_b200(args, rank, world, local_rank):
         "roofline": roofline,
         "clocks": clock_info,
         "mixed": mixed,
+        "schemes": schemes,
         "ensemble": ensemble,
         "served": served,
         "cpu_baseline": cpu,
     }
     reps.close()
     return line
+
+
+# ------------------------------------------------------------- schemes -----
+def run_schemes(args, desc, q, stream, timed_steps, max_over_ranks):
+    """Every reconstruction on the same 256^3 field, FP64 and mixed: ms per
+    step and the directional sweeps' share (WENO5-Z FP64 is the headline
+    above; this places the other Method.in schemes beside it)."""
+    import nuc3d_b200 as nb
+    k = max(3, min(args.steps, 10))
+    out = {"steps": k, "workload": f"{desc.nx}^3 HIT, CFL {CFL}"}
+    for name, sch in (("weno5js", nb.WENO5JS), ("weno5z", nb.WENO5Z), ("crweno5", nb.CRWENO5),
+                      ("weno7js", nb.WENO7JS)):
+        row = {}
+        for pname, prec in (("fp64", nb.FP64), ("mixed", nb.MIXED)):
+            d = nb.BoxDesc(**{**desc.__dict__, "scheme": (sch,) * 3, "precision": prec})
+            with nb.Solver(d, stream=stream) as s:
+                s.set_state(q)
+                s.step(args.warmup, CFL, stats=False)
+                s.sync()
+                ms = max_over_ranks(timed_steps(s, k)) / k
+                s.profile(True)
+                s.step(1, CFL, stats=False)
+                prof = s.profile_read(reset=True)
+                s.profile(False)
+            sweep = sum(prof[x][0] for x in ("inv_x", "inv_y", "inv_z"))
+            row[pname] = {"ms_per_step": ms, "cell_updates_per_s": desc.cells / (ms * 1e-3),
+                          "sweep_ms_per_step": sweep,
+                          "sweep_share": sweep / max(sum(v[0] for v in prof.values()), 1e-12)}
+        row["mixed_speedup"] = row["fp64"]["ms_per_step"] / row["mixed"]["ms_per_step"]
+        out[name] = row
+    return out
 
 
 # ------------------------------------------------------------ ensemble -----
@@ -577,6 +611,7 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--skip-mixed", action="store_true")
     ap.add_argument("--skip-ensemble", action="store_true")
+    ap.add_argument("--skip-schemes", action="store_true")
     ap.add_argument("--ensemble-boxes", type=int, default=64)
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--skip-serve", action="store_true")
