@@ -421,6 +421,71 @@ void or_lf_split(const or_box *b, const double *const q[5], const double *const 
     eig[2] = me[2];
 }
 
+/* physicsModel.cpp:1181-1278: the Mach-number and pressure splittings.
+ * AUSM squares with pow(x, 2) (an int exponent, promoted) and AUSMp with
+ * pow(x, 2.0): the same libm call. */
+static double ausm_mach_l(double mach) {
+    if (fabs(mach) < 1.0) return 0.25 * pow(mach + 1.0, 2.0) + 0.125 * pow(mach * mach - 1, 2.0);
+    return 0.50 * (mach + fabs(mach));
+}
+static double ausm_mach_r(double mach) {
+    if (fabs(mach) < 1.0) return -0.25 * pow(mach - 1.0, 2.0) - 0.125 * pow(mach * mach - 1, 2.0);
+    return 0.50 * (mach - fabs(mach));
+}
+static double ausm_p_l(double mach, double p) {
+    if (fabs(mach) < 1.0) return p * (mach + 1.0) / 2.0;
+    return 0.50 * p * (mach + fabs(mach)) / mach;
+}
+static double ausm_p_r(double mach, double p) {
+    if (fabs(mach) < 1.0) return -p * (mach - 1.0) / 2.0;
+    return 0.5 * p * (mach - fabs(mach)) / mach;
+}
+static double ausmp_p_l(double mach, double p) {
+    if (fabs(mach) < 1.0)
+        return p * (0.25 * pow(mach + 1.0, 2.0) * (2.0 - mach) +
+                    0.1875 * mach * pow(mach * mach - 1.0, 2.0));
+    return 0.50 * p * (mach + fabs(mach)) / mach;
+}
+static double ausmp_p_r(double mach, double p) {
+    if (fabs(mach) < 1.0)
+        return p * (0.25 * pow(mach - 1.0, 2.0) * (2.0 + mach) -
+                    0.1875 * mach * pow(mach * mach - 1.0, 2.0));
+    return 0.5 * p * (mach - fabs(mach)) / mach;
+}
+
+void or_ausm_split(const or_box *b, const double *const q[5], const double *const prim[8],
+                   double *const fl[3][5], double *const fr[3][5], double eig[3]) {
+    /* physicsModel.cpp:777-929 (AUSM), :1027-1178 (AUSMp): directions in the
+     * reference's order; (machp*alpha0)*Q evaluated left to right. */
+    const long N = (long)b->nx * b->ny * b->nz;
+    const int plus = b->riemann == OR_AUSMP;
+    double me[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < 3; ++d) {
+        for (long n = 0; n < N; ++n) {
+            double un = prim[1 + d][n];
+            double p0 = prim[4][n];
+            double alpha0 = prim[7][n];
+            double mach = un / alpha0;
+            double machp = ausm_mach_l(mach);
+            double machn = ausm_mach_r(mach);
+            double p_p = plus ? ausmp_p_l(mach, p0) : ausm_p_l(mach, p0);
+            double p_n = plus ? ausmp_p_r(mach, p0) : ausm_p_r(mach, p0);
+            me[d] = fmax(fabs(un) + alpha0, me[d]);
+            for (int e = 0; e < 4; ++e) {
+                fl[d][e][n] = machp * alpha0 * q[e][n];
+                fr[d][e][n] = machn * alpha0 * q[e][n];
+            }
+            fl[d][1 + d][n] = machp * alpha0 * q[1 + d][n] + p_p;
+            fr[d][1 + d][n] = machn * alpha0 * q[1 + d][n] + p_n;
+            fl[d][4][n] = machp * alpha0 * q[4][n] + machp * alpha0 * p0;
+            fr[d][4][n] = machn * alpha0 * q[4][n] + machn * alpha0 * p0;
+        }
+    }
+    eig[0] = me[0];
+    eig[1] = me[1];
+    eig[2] = me[2];
+}
+
 /* physicsModel.cpp:193-266 (+ an extra power-law model). */
 static void viscosity(const or_box *b, double T, double *miu, double *coeff) {
     double m;
@@ -550,7 +615,10 @@ double or_rhs(const or_box *b, const double *const q[5], double *const rhs[5]) {
         }
     double eig[3];
     or_con2prim(b, q, prim);                 /* NaiverStokes3d.cpp:46 */
-    or_lf_split(b, q, (const double *const *)prim, fl, fr, eig); /* :48 */
+    if (b->riemann == OR_LF) /* :48, physicsModel::solveRiemann */
+        or_lf_split(b, q, (const double *const *)prim, fl, fr, eig);
+    else
+        or_ausm_split(b, q, (const double *const *)prim, fl, fr, eig);
     for (int d = 0; d < 3; ++d) inviscid_direction(b, d, fl[d], fr[d], dinv + 5 * d); /* :52 */
 
     double *dvis[15] = {0};

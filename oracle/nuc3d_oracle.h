@@ -47,7 +47,11 @@ typedef struct {
     int visc_model;
     double gamma, mach, reynolds, prandtl, t_ref, t_inf, powerlaw_exp;
     unsigned quirks;
+    int riemann;        /* OR_LF, OR_AUSM, OR_AUSMP: PhysModel.in RiemannSolver */
 } or_box;
+
+/* flux splittings (physicsModel.cpp:16-20 map "LF", "AUSM", "AUSMp") */
+enum { OR_LF = 0, OR_AUSM = 1, OR_AUSMP = 2 };
 
 /* physicsModel::con2prim.  prim: rho,u,v,w,p,T,e,c (8 fields). */
 void or_con2prim(const or_box *b, const double *const q[5], double *const prim[8]);
@@ -57,6 +61,12 @@ void or_con2prim(const or_box *b, const double *const q[5], double *const prim[8
  * loop produces; with OR_Q_ZETA_EIGEN the z loop updates eig_eta instead. */
 void or_lf_split(const or_box *b, const double *const q[5], const double *const prim[8],
                  double *const fl[3][5], double *const fr[3][5], double eig[3]);
+
+/* physicsModel::RiemannAUSM / RiemannAUSMp (physicsModel.cpp:682-1278), the
+ * point-wise Mach-number splittings, same layout as or_lf_split.  No
+ * eigenvalue quirk: each direction's loop updates its own maxEigen. */
+void or_ausm_split(const or_box *b, const double *const q[5], const double *const prim[8],
+                   double *const fl[3][5], double *const fr[3][5], double eig[3]);
 
 /* The reference's per-field reconstruction interface
  * (interpolationInner + BoundaryL + BoundaryR): along the fastest axis of an

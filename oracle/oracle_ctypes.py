@@ -29,6 +29,8 @@ REF_SO = HERE / "_ref" / "libnuc3d_ref.so"
 WENO5JS, WENO5Z, CRWENO5, WENO7 = 0, 1, 2, 3
 SCHEME_NAMES = {WENO5JS: "weno5js", WENO5Z: "weno5z", CRWENO5: "crweno5", WENO7: "weno7js"}
 SUTHERLAND, CONSTANT, POWERLAW = 0, 1, 2
+LF, AUSM, AUSMP = 0, 1, 2
+RIEMANN_NAMES = {LF: "LF", AUSM: "AUSM", AUSMP: "AUSMp"}
 VISC_NAMES = {SUTHERLAND: "Sutherland", CONSTANT: "Constant"}
 
 Q_ZETA_EIGEN = 1 << 0
@@ -52,6 +54,7 @@ class _Box(C.Structure):
         ("prandtl", C.c_double), ("t_ref", C.c_double), ("t_inf", C.c_double),
         ("powerlaw_exp", C.c_double),
         ("quirks", C.c_uint),
+        ("riemann", C.c_int),
     ]
 
 
@@ -77,6 +80,7 @@ class Box:
     t_inf: float = 288.0
     powerlaw_exp: float = 0.76
     quirks: int = QUIRKS_REFERENCE
+    riemann: int = LF
 
     @property
     def dx(self):
@@ -106,6 +110,7 @@ class Box:
         b.prandtl, b.t_ref, b.t_inf = self.prandtl, self.t_ref, self.t_inf
         b.powerlaw_exp = self.powerlaw_exp
         b.quirks = int(self.quirks)
+        b.riemann = int(self.riemann)
         return b
 
 
@@ -155,6 +160,21 @@ class Oracle:
         self.lib.or_con2prim(C.byref(b), _ptrs(q), _ptrs(prim))
         return prim
 
+    def split(self, box: Box, q):
+        """con2prim + the box's flux splitting, x-fastest: (prim[8], fl[3][5],
+        fr[3][5], eig[3])."""
+        prim = self.con2prim(box, q)
+        fl = [[np.zeros(box.shape) for _ in range(5)] for _ in range(3)]
+        fr = [[np.zeros(box.shape) for _ in range(5)] for _ in range(3)]
+        arr15 = _DP * 5
+        FL = (arr15 * 3)(*[arr15(*[_ptr(a) for a in fl[d]]) for d in range(3)])
+        FR = (arr15 * 3)(*[arr15(*[_ptr(a) for a in fr[d]]) for d in range(3)])
+        eig = np.zeros(3)
+        b = box.c_struct()
+        fn = self.lib.or_lf_split if box.riemann == LF else self.lib.or_ausm_split
+        fn(C.byref(b), _ptrs(q), _ptrs(prim), FL, FR, _ptr(eig))
+        return prim, fl, fr, eig
+
     def rk3_stage(self, stage, dt, rhs, un, ui):
         n = rhs[0].size
         self.lib.or_rk3_stage(stage, C.c_long(n), C.c_double(dt), _ptrs(rhs), _ptrs(un),
@@ -203,7 +223,7 @@ def write_decks(dirpath: Path, box: Box, cfl: float = 0.5):
         "scheme_x_vis cd6\nscheme_y_vis cd6\nscheme_z_vis cd6\n")
     model = "NavierStokes3d" if box.navier_stokes else "Euler3d"
     (inp / "PhysModel.in").write_text(
-        "Neqs 5\nEosName IdealGas\nRiemannSolver LF\n"
+        f"Neqs 5\nEosName IdealGas\nRiemannSolver {RIEMANN_NAMES[box.riemann]}\n"
         f"PDEModel {model}\nViscousModel {VISC_NAMES[box.visc_model]}\nForcing None\n"
         f"Reynolds {box.reynolds!r}\nMach {box.mach!r}\nPt {box.prandtl!r}\n"
         f"Gamma {box.gamma!r}\nT_ref {box.t_ref!r}\nT_inf {box.t_inf!r}\n")

@@ -19,7 +19,8 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT / "oracle"))
 
-from oracle_ctypes import (CRWENO5, WENO5JS, WENO5Z, WENO7, Box, Oracle, Reference)  # noqa: E402
+from oracle_ctypes import (AUSM, AUSMP, CRWENO5, WENO5JS, WENO5Z, WENO7, Box, Oracle,  # noqa: E402
+                           Reference)
 
 SCHEME_TAG = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr", WENO7: "w7"}
 
@@ -93,7 +94,34 @@ def main():
     np.savez_compressed(HERE / "tgv24_js_10.npz", q10=np.stack(qn), dt=dt, res=res)
     stats_fixture(R)
     weno7_fixtures(R)
+    ausm_fixtures(R)
     print("fixtures written to", HERE)
+
+
+def ausm_fixtures(R):
+    """The reference's RiemannAUSM / RiemannAUSMp splittings
+    (physicsModel.cpp:682-1278): the split fluxes on a box whose local Mach
+    number crosses 1 (both branches of the Mach and pressure polynomials), and
+    one RHS plus three steps, N-S with WENO5-Z and Euler with WENO5-JS."""
+    dirs = ("xi", "eta", "zeta")
+    for rm, tag in ((AUSM, "ausm"), (AUSMP, "ausmp")):
+        box = Box(12, 10, 8, mach=1.5, reynolds=800.0, riemann=rm)
+        q = perturbed_tgv(box, 17 + rm)
+        prim, fl, fr, eig = R.split(box, q)
+        np.savez_compressed(HERE / f"split_{tag}.npz", q=np.stack(q), eig=eig, mach=box.mach,
+                            **{f"fl_{d}": np.stack(fl[5 * i:5 * i + 5]) for i, d in enumerate(dirs)},
+                            **{f"fr_{d}": np.stack(fr[5 * i:5 * i + 5]) for i, d in enumerate(dirs)})
+        for ns, scheme, mach in ((True, WENO5Z, 1.2), (False, WENO5JS, 0.3)):
+            box = Box(16, 12, 10, scheme=(scheme,) * 3, navier_stokes=ns, mach=mach,
+                      reynolds=1600.0, prandtl=0.71, riemann=rm)
+            q = perturbed_tgv(box, 23 + rm)
+            rhs, dtl = R.rhs(box, q)
+            qn, dt, res = R.run_steps(box, 0.5, 3, q)
+            np.savez_compressed(HERE / f"step_{tag}_{'ns' if ns else 'eu'}.npz", q0=np.stack(q),
+                                rhs=np.stack(rhs), dt_local=np.array(dtl), q3=np.stack(qn), dt=dt,
+                                res=res, shape=np.array(box.shape), mach=box.mach,
+                                reynolds=box.reynolds, prandtl=box.prandtl,
+                                scheme=np.array(scheme), riemann=np.array(rm))
 
 
 def weno7_fixtures(R):

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from helpers import box_from_golden, golden
-from oracle_ctypes import (CRWENO5, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_WENOZ_BETA2, WENO5JS,
+from oracle_ctypes import (AUSM, AUSMP, CRWENO5, LF, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_WENOZ_BETA2, WENO5JS,
                            WENO5Z, WENO7, Box, Oracle, Reference)
 
 TAGS = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr"}
@@ -144,6 +144,50 @@ def test_weno7_reconstruct_matches_reference_golden(O, up):
 def test_weno7_rhs_and_steps_match_reference_golden(O, ns):
     z = golden(f"step_w7_{'ns' if ns else 'eu'}.npz")
     box = box_from_golden(z, WENO7, ns)
+    rhs, dtl = O.rhs(box, list(z["q0"]))
+    assert np.array_equal(np.stack(rhs), z["rhs"]) and dtl == float(z["dt_local"])
+    q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
+    assert np.array_equal(np.stack(q3), z["q3"])
+    assert np.array_equal(dt, z["dt"]) and np.array_equal(res, z["res"])
+
+
+ROTATE = (lambda a: a, lambda a: a.transpose(2, 0, 1), lambda a: a.transpose(1, 2, 0))
+
+
+def _check_split(O, box, z):
+    q = [np.ascontiguousarray(a) for a in z["q"]]
+    _, fl, fr, eig = O.split(box, q)
+    for d, name in enumerate(("xi", "eta", "zeta")):
+        # the reference stores each direction in its rotated layout (euler3d.cpp:71-76)
+        assert np.array_equal(np.stack([ROTATE[d](a) for a in fl[d]]), z[f"fl_{name}"])
+        assert np.array_equal(np.stack([ROTATE[d](a) for a in fr[d]]), z[f"fr_{name}"])
+    assert np.array_equal(eig, z["eig"])
+
+
+def test_lf_split_fluxes_match_reference_golden(O):
+    _check_split(O, Box(12, 10, 8, mach=0.3, reynolds=800.0), golden("split.npz"))
+
+
+@pytest.mark.parametrize("riemann,tag", [(AUSM, "ausm"), (AUSMP, "ausmp")])
+def test_ausm_split_matches_reference_golden(O, riemann, tag):
+    """RiemannAUSM / RiemannAUSMp on a box whose local Mach number spans
+    1e-17 .. 17, so both branches of every splitting polynomial are used."""
+    z = golden(f"split_{tag}.npz")
+    _check_split(O, Box(12, 10, 8, mach=float(z["mach"]), reynolds=800.0, riemann=riemann), z)
+
+
+def ausm_box(z, ns):
+    nz, ny, nx = (int(v) for v in z["shape"])
+    return Box(nx, ny, nz, scheme=(int(z["scheme"]),) * 3, navier_stokes=ns,
+               mach=float(z["mach"]), reynolds=float(z["reynolds"]),
+               prandtl=float(z["prandtl"]), riemann=int(z["riemann"]))
+
+
+@pytest.mark.parametrize("tag", ["ausm", "ausmp"])
+@pytest.mark.parametrize("ns", [True, False])
+def test_ausm_rhs_and_steps_match_reference_golden(O, tag, ns):
+    z = golden(f"step_{tag}_{'ns' if ns else 'eu'}.npz")
+    box = ausm_box(z, ns)
     rhs, dtl = O.rhs(box, list(z["q0"]))
     assert np.array_equal(np.stack(rhs), z["rhs"]) and dtl == float(z["dt_local"])
     q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
