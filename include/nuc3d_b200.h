@@ -84,7 +84,16 @@ typedef struct nuc3d_box_desc {
      * radius, < 3.5). */
     int forcing;
     double forcing_amp, forcing_hel, forcing_k;
+    /* PhysModel.in RiemannSolver (physicsModel.cpp:16-20): NUC3D_RIEMANN_LF
+     * (RiemannLF, :436-680), NUC3D_RIEMANN_AUSM (RiemannAUSM, :682-930) or
+     * NUC3D_RIEMANN_AUSMP (RiemannAUSMp, :932-1179).  The quirk
+     * NUC3D_QUIRK_ZETA_EIGEN belongs to RiemannLF only: the AUSM loops keep
+     * each direction's own maximum eigenvalue. */
+    int riemann;
 } nuc3d_box_desc;
+#define NUC3D_RIEMANN_LF 0
+#define NUC3D_RIEMANN_AUSM 1
+#define NUC3D_RIEMANN_AUSMP 2
 #define NUC3D_FORCING_NONE 0
 #define NUC3D_FORCING_CONST 1
 

@@ -149,21 +149,12 @@ __global__ void __launch_bounds__(kCrThreads)
         if (DIR == 1) return a + sy * pos + sz * fixed;
         return a + sy * fixed + sz * pos;
     };
-    // Lax-Friedrichs split of equation e at cell g (physicsModel.cpp:546-565)
+    // the box's point-wise split (LF / AUSM / AUSMp) of equation e at cell g
+    const int riemann = bp.riemann;
     auto split = [&](int e, long long g, double &fp, double &fm) {
-        const double qe = qbase[e * np + g];
-        const double un = wbase[DIR * np + g], p = wbase[3 * np + g], c = wbase[4 * np + g];
-        const double lam = add_(fabs(un), c);
-        double f;
-        if (e == 4)
-            f = mul_(un, add_(qe, p));
-        else if (e == 1 + DIR)
-            f = fma_(un, qe, p);
-        else
-            f = mul_(un, qe);
-        const double t = mul_(lam, qe);
-        fp = mul_(0.5, add_(f, t));
-        fm = mul_(0.5, sub_(f, t));
+        SplitCell sc;
+        split_prepare(riemann, wbase[DIR * np + g], wbase[3 * np + g], wbase[4 * np + g], sc);
+        split_eq<DIR>(riemann, sc, e, qbase[e * np + g], fp, fm);
     };
     const bool mixed = sizeof(B) == sizeof(float);
     const bool bounded = (bp.quirks & QK_CRWENO_BOUNDED) != 0;

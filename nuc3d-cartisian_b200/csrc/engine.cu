@@ -43,6 +43,7 @@ BoxParams make_params(const nuc3d_box_desc &d) {
     bp.navier_stokes = d.pde_model == NUC3D_NAVIERSTOKES3D;
     bp.quirks = d.quirks;
     for (int i = 0; i < 3; ++i) bp.scheme[i] = d.scheme[i];
+    bp.riemann = d.riemann;
     return bp;
 }
 
@@ -84,6 +85,8 @@ int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
         return bad(NUC3D_ERR_UNSUPPORTED, "unknown precision");
     if (!(d.gamma > 1.0) || !(d.mach > 0.0) || !(d.reynolds > 0.0) || !(d.prandtl > 0.0))
         return bad(NUC3D_ERR_INVALID, "gamma must be > 1 and Mach, Re, Pr > 0");
+    if (d.riemann < NUC3D_RIEMANN_LF || d.riemann > NUC3D_RIEMANN_AUSMP)
+        return bad(NUC3D_ERR_UNSUPPORTED, "unknown Riemann solver (flux splitting)");
     if (d.forcing != NUC3D_FORCING_NONE && d.forcing != NUC3D_FORCING_CONST)
         return bad(NUC3D_ERR_UNSUPPORTED, "unknown forcing model");
     if (d.forcing == NUC3D_FORCING_CONST) {

@@ -24,6 +24,7 @@ enum : int { SCHEME_JS = 0, SCHEME_Z = 1, SCHEME_CR = 2, SCHEME_W7 = 3 };
 // fieldOperator.cpp:128-175): 4 cells for weno7js, 3 for the WENO5 family
 __host__ __device__ constexpr int scheme_halo(int scheme) { return scheme == SCHEME_W7 ? 4 : 3; }
 enum : int { VISC_SUTHERLAND = 0, VISC_CONSTANT = 1, VISC_POWERLAW = 2 };
+enum : int { RIEMANN_LF = 0, RIEMANN_AUSM = 1, RIEMANN_AUSMP = 2 };
 
 // Everything a kernel needs to know about one periodic box.
 struct BoxParams {
@@ -37,6 +38,7 @@ struct BoxParams {
     int visc_model, navier_stokes;
     unsigned quirks;
     int scheme[3];
+    int riemann;  // RIEMANN_LF / _AUSM / _AUSMP
 };
 
 // Field pointers of one box.  q: conserved state (double); w: primitives in
@@ -212,6 +214,87 @@ template <int SCHEME, typename B>
 __device__ __forceinline__ B weno5_face(B f0, B f1, B f2, B f3, B f4, bool beta2_quirk) {
     if (SCHEME == SCHEME_Z) return weno5z_face(f0, f1, f2, f3, f4, beta2_quirk);
     return weno5js_face(f0, f1, f2, f3, f4);
+}
+
+// --------------------------------------------------------- flux splitting --
+// Point-wise split of the DIR flux of one cell into F+ (reconstructed
+// upwind '+') and F- ('-').  FP64, each operation explicitly rounded in the
+// reference's order.
+//   LF    (physicsModel.cpp:546-565): F+- = (F(Q) +- lambda Q) / 2,
+//         lambda = |u_n| + c.
+//   AUSM  (:777-929), AUSMp (:1027-1178), with m = u_n / c:
+//         F+- = (M+-(m) c) Q + p+-(m) e_n + (M+-(m) c) p e_E, the Mach
+//         polynomials M+- and pressure weights p+- of :1181-1278.
+struct SplitCell {
+    double a[2];  // LF: u_n and lambda; AUSM: M+ c and M- c
+    double p;     // pressure
+    double pn[2]; // AUSM: p+ and p- (the normal-momentum terms)
+};
+
+__device__ __forceinline__ double sq_(double x) { return mul_(x, x); }
+
+__device__ __forceinline__ void split_prepare(int riemann, double un, double p, double c,
+                                              SplitCell &s) {
+    s.p = p;
+    if (riemann == RIEMANN_LF) {
+        s.a[0] = un;
+        s.a[1] = add_(fabs(un), c);
+        return;
+    }
+    const double m = un / c;  // IEEE division, as the reference
+    const double am = fabs(m);
+    double mp, mm, pp, pm;
+    if (am < 1.0) {
+        const double q2 = sq_(sub_(mul_(m, m), 1.0));
+        mp = add_(mul_(0.25, sq_(add_(m, 1.0))), mul_(0.125, q2));
+        mm = sub_(mul_(-0.25, sq_(sub_(m, 1.0))), mul_(0.125, q2));
+        if (riemann == RIEMANN_AUSM) {
+            pp = mul_(mul_(p, add_(m, 1.0)), 0.5);
+            pm = mul_(mul_(-p, sub_(m, 1.0)), 0.5);
+        } else {
+            const double t = mul_(mul_(0.1875, m), q2);
+            pp = mul_(p, add_(mul_(mul_(0.25, sq_(add_(m, 1.0))), sub_(2.0, m)), t));
+            pm = mul_(p, sub_(mul_(mul_(0.25, sq_(sub_(m, 1.0))), add_(2.0, m)), t));
+        }
+    } else {
+        mp = mul_(0.5, add_(m, am));
+        mm = mul_(0.5, sub_(m, am));
+        pp = mul_(mul_(0.5, p), add_(m, am)) / m;
+        pm = mul_(mul_(0.5, p), sub_(m, am)) / m;
+    }
+    s.a[0] = mul_(mp, c);
+    s.a[1] = mul_(mm, c);
+    s.pn[0] = pp;
+    s.pn[1] = pm;
+}
+
+// F+ and F- of equation e (0..4) of a cell with conserved value qe
+template <int DIR>
+__device__ __forceinline__ void split_eq(int riemann, const SplitCell &s, int e, double qe,
+                                         double &fp, double &fm) {
+    if (riemann == RIEMANN_LF) {
+        const double un = s.a[0], lam = s.a[1];
+        double f;
+        if (e == 4)
+            f = mul_(un, add_(qe, s.p));
+        else if (e == 1 + DIR)
+            f = fma_(un, qe, s.p);
+        else
+            f = mul_(un, qe);
+        const double t = mul_(lam, qe);
+        fp = mul_(0.5, add_(f, t));
+        fm = mul_(0.5, sub_(f, t));
+        return;
+    }
+    fp = mul_(s.a[0], qe);
+    fm = mul_(s.a[1], qe);
+    if (e == 1 + DIR) {
+        fp = add_(fp, s.pn[0]);
+        fm = add_(fm, s.pn[1]);
+    } else if (e == 4) {
+        fp = add_(fp, mul_(s.a[0], s.p));
+        fm = add_(fm, mul_(s.a[1], s.p));
+    }
 }
 
 // ------------------------------------------------------------------ WENO7 --

@@ -50,7 +50,9 @@ __global__ void __launch_bounds__(256, 4) k_prim(const BoxDev *__restrict__ boxe
         lz = fmax(fabs(ww) + c, lz);
     }
     if (!want_eig) return;
-    if (bp.quirks & QK_ZETA_EIGEN) {  // z loop writes MaxEigen_eta; zeta stays 0
+    if ((bp.quirks & QK_ZETA_EIGEN) && bp.riemann == RIEMANN_LF) {
+        // RiemannLF's z loop writes MaxEigen_eta; zeta stays 0 (the AUSM
+        // loops keep their own directions)
         ly = fmax(lz, ly);
         lz = 0.0;
     }
@@ -184,8 +186,9 @@ __device__ __forceinline__ B weno_from(B f0, B f1, B f2, B f3, B f4, B d0, B d1,
 }
 
 // Inviscid flux derivative along DIR for all 5 equations (euler3d.cpp:307-387
-// + combineFluxLR :23-56 + setDerivatives*Inv :143-253), with the
-// Lax-Friedrichs split (physicsModel.cpp:546-565) done while staging.
+// + combineFluxLR :23-56 + setDerivatives*Inv :143-253), with the box's
+// point-wise flux split (LF, AUSM or AUSMp; split_prepare) done while
+// staging.
 //   accumulate = 0: R = dF/dx ; 1: R += dG/dy (the RHS summation order of
 //   NaiverStokes3d.cpp:396-446).
 // Work item: (box, a, b, c) = DIR 0: (x chunk, j group, k); DIR 1: (i group,
@@ -241,23 +244,12 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
         if (DIR == 1) return a + sy * pos + sz * fixed;
         return a + sy * fixed + sz * pos;
     };
+    const int riemann = bp.riemann;
     auto split = [&](long long g, double Fp[5], double Fm[5]) {
-        double Q[5];
+        SplitCell sc;
+        split_prepare(riemann, wbase[DIR * np + g], wbase[3 * np + g], wbase[4 * np + g], sc);
 #pragma unroll
-        for (int e = 0; e < 5; ++e) Q[e] = qbase[e * np + g];
-        double un = wbase[DIR * np + g], p = wbase[3 * np + g], c = wbase[4 * np + g];
-        double lam = add_(fabs(un), c);
-        double f[5];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) f[e] = mul_(un, Q[e]);
-        f[1 + DIR] = fma_(un, Q[1 + DIR], p);
-        f[4] = mul_(un, add_(Q[4], p));
-#pragma unroll
-        for (int e = 0; e < 5; ++e) {
-            double t = mul_(lam, Q[e]);
-            Fp[e] = mul_(0.5, add_(f[e], t));
-            Fm[e] = mul_(0.5, sub_(f[e], t));
-        }
+        for (int e = 0; e < 5; ++e) split_eq<DIR>(riemann, sc, e, qbase[e * np + g], Fp[e], Fm[e]);
     };
     const bool mixed = sizeof(B) == sizeof(float);
     if (mixed) {  // per-line reference values (cell c0, always inside the box)

@@ -116,7 +116,16 @@ Case read_case(const std::string &dir) {
     auto p = words(inp + "PhysModel.in", true);
     if (p.size() < 12) die("PhysModel.in needs its six positional lines");
     const std::string riemann = p[5], model = p[7], visc = p[9], forcing = p[11];
-    if (riemann != "LF") die("RiemannSolver " + riemann + ": only LF is on the B200 path");
+    // physicsModel.cpp:16-20 names; an unknown name makes the reference warn
+    // and then compute no split at all (:88-93, :425-433), so it stops here
+    if (riemann == "LF")
+        c.desc.riemann = NUC3D_RIEMANN_LF;
+    else if (riemann == "AUSM")
+        c.desc.riemann = NUC3D_RIEMANN_AUSM;
+    else if (riemann == "AUSMp")
+        c.desc.riemann = NUC3D_RIEMANN_AUSMP;
+    else
+        die("Riemann Solver name " + riemann + " does not exist (LF, AUSM, AUSMp)");
     if (forcing != "None" && forcing != "Const")
         die("Forcing " + forcing + ": only None and Const are on the B200 path");
     c.desc.forcing = forcing == "Const" ? NUC3D_FORCING_CONST : NUC3D_FORCING_NONE;
@@ -220,7 +229,8 @@ int main(int argc, char **argv) {
                   << " reynolds " << c.desc.reynolds << " prandtl " << c.desc.prandtl
                   << " t_ref " << c.desc.t_ref << " t_inf " << c.desc.t_inf << " forcing "
                   << c.desc.forcing << " forcing_amp " << c.desc.forcing_amp << " forcing_hel "
-                  << c.desc.forcing_hel << " forcing_k " << c.desc.forcing_k << " cfl "
+                  << c.desc.forcing_hel << " forcing_k " << c.desc.forcing_k << " riemann "
+                  << c.desc.riemann << " cfl "
                   << c.io["cfl"] << " endStep " << c.io["endStep"] << " tl " << c.io["tl"]
                   << std::endl;
         return 0;

@@ -24,6 +24,8 @@ FORCING_NONE, FORCING_CONST = 0, 1
 WENO5JS, WENO5Z, CRWENO5, WENO7JS = 0, 1, 2, 3
 SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5, "weno7js": WENO7JS}
 TUNING_SLOTS = 12  # NUC3D_TUNING_SLOTS: (scheme id, direction) pairs
+RIEMANN_LF, RIEMANN_AUSM, RIEMANN_AUSMP = 0, 1, 2
+RIEMANNS = {"LF": RIEMANN_LF, "AUSM": RIEMANN_AUSM, "AUSMp": RIEMANN_AUSMP}
 EULER3D, NAVIERSTOKES3D = 0, 1
 SUTHERLAND, CONSTANT, POWERLAW = 0, 1, 2
 FP64, MIXED = 0, 1
@@ -62,6 +64,7 @@ class _Desc(C.Structure):
         ("quirks", C.c_uint),
         ("forcing", C.c_int),
         ("forcing_amp", C.c_double), ("forcing_hel", C.c_double), ("forcing_k", C.c_double),
+        ("riemann", C.c_int),
     ]
 
 
@@ -209,6 +212,7 @@ class BoxDesc:
     forcing_amp: float = 0.01       # PhysModel.in Forcing_amplitude
     forcing_hel: float = 0.01       # Forcing_amplitude_hel
     forcing_k: float = 1.0          # Forcing_wave_k
+    riemann: int = RIEMANN_LF       # PhysModel.in RiemannSolver: LF, AUSM, AUSMp
 
     @property
     def cells(self) -> int:
@@ -232,6 +236,7 @@ class BoxDesc:
         d.quirks = int(self.quirks)
         d.forcing = int(self.forcing)
         d.forcing_amp, d.forcing_hel, d.forcing_k = self.forcing_amp, self.forcing_hel, self.forcing_k
+        d.riemann = int(self.riemann)
         return d
 
     def device_bytes(self) -> int:

@@ -11,8 +11,8 @@ from __future__ import annotations
 
 from pathlib import Path
 
-from . import (CONSTANT, EULER3D, FORCING_CONST, FORCING_NONE, NAVIERSTOKES3D, SCHEMES,
-               SUTHERLAND, BoxDesc)
+from . import (CONSTANT, EULER3D, FORCING_CONST, FORCING_NONE, NAVIERSTOKES3D, RIEMANNS,
+               SCHEMES, SUTHERLAND, BoxDesc)
 
 _NOT_ON_PATH = ("hccs", "hccs77", "hccs78", "weno3js", "upwind1st")
 
@@ -55,8 +55,10 @@ def read_decks(dirpath):
     if len(toks) < 12:
         raise ValueError("PhysModel.in needs its six positional lines")
     pos = [toks[2 * i + 1] for i in range(6)]  # Neqs EosName RiemannSolver PDEModel ViscousModel Forcing
-    if pos[2] != "LF":
-        raise ValueError(f"RiemannSolver {pos[2]}: only LF is on the B200 path")
+    if pos[2] not in RIEMANNS:
+        # physicsModel.cpp:88-93 prints a warning and then computes no split
+        # at all (solveRiemann finds no such name); refuse instead
+        raise ValueError(f"Riemann Solver name {pos[2]} does not exist (LF, AUSM, AUSMp)")
     if pos[5] not in ("None", "Const"):
         raise ValueError(f"Forcing {pos[5]}: only None and Const are on the B200 path")
     phys = dict(_PHYS_DEFAULTS)
@@ -91,7 +93,7 @@ def read_decks(dirpath):
                    t_ref=phys["T_ref"], t_inf=phys["T_inf"],
                    forcing=FORCING_CONST if pos[5] == "Const" else FORCING_NONE,
                    forcing_amp=phys["Forcing_amplitude"], forcing_hel=phys["Forcing_amplitude_hel"],
-                   forcing_k=phys["Forcing_wave_k"])
+                   forcing_k=phys["Forcing_wave_k"], riemann=RIEMANNS[pos[2]])
     return desc, io, phys
 
 
@@ -105,8 +107,9 @@ def write_decks(dirpath, desc, io=None):
     model = "NavierStokes3d" if desc.pde_model == NAVIERSTOKES3D else "Euler3d"
     visc = "Constant" if desc.visc_model == CONSTANT else "Sutherland"
     forcing = "Const" if desc.forcing == FORCING_CONST else "None"
+    rname = {v: k for k, v in RIEMANNS.items()}[desc.riemann]
     (inp / "PhysModel.in").write_text(
-        f"Neqs 5\nEosName IdealGas\nRiemannSolver LF\nPDEModel {model}\nViscousModel {visc}\n"
+        f"Neqs 5\nEosName IdealGas\nRiemannSolver {rname}\nPDEModel {model}\nViscousModel {visc}\n"
         f"Forcing {forcing}\nReynolds {desc.reynolds!r}\nMach {desc.mach!r}\nPt {desc.prandtl!r}\n"
         f"Gamma {desc.gamma!r}\nT_ref {desc.t_ref!r}\nT_inf {desc.t_inf!r}\n"
         f"Forcing_amplitude {desc.forcing_amp!r}\nForcing_amplitude_hel {desc.forcing_hel!r}\n"

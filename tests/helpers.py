@@ -39,7 +39,7 @@ def desc_from_box(box, precision=0):
                       visc_model=box.visc_model, gamma=box.gamma, mach=box.mach,
                       reynolds=box.reynolds, prandtl=box.prandtl, t_ref=box.t_ref,
                       t_inf=box.t_inf, powerlaw_exp=box.powerlaw_exp, precision=precision,
-                      quirks=box.quirks)
+                      quirks=box.quirks, riemann=box.riemann)
 
 
 def rounding_sensitivity(box, q, nsteps, cfl=0.5, seed=0):

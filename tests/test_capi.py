@@ -65,7 +65,8 @@ def test_ctx_create_rejects_bad_descriptions_without_device():
     L = nb.lib()
     h = C.c_void_p()
     for bad in (nb.BoxDesc(4, 16, 16), nb.BoxDesc(16, 16, 16, scheme=(0, 5, 0)),
-                nb.BoxDesc(16, 16, 16, mach=-1.0), nb.BoxDesc(16, 16, 16, precision=3)):
+                nb.BoxDesc(16, 16, 16, mach=-1.0), nb.BoxDesc(16, 16, 16, precision=3),
+                nb.BoxDesc(16, 16, 16, riemann=3)):
         d = bad.c_struct()
         assert L.nuc3d_ctx_create(C.byref(d), None, C.byref(h)) in (nb.ERR_INVALID,
                                                                     nb.ERR_UNSUPPORTED)

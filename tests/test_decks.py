@@ -20,8 +20,8 @@ def test_decks_round_trip(tmp_path):
 def test_decks_reject_paths_off_the_gpu_route(tmp_path):
     nb.write_decks(tmp_path, nb.BoxDesc(16, 16, 16))
     p = tmp_path / "inp" / "PhysModel.in"
-    p.write_text(p.read_text().replace("RiemannSolver LF", "RiemannSolver AUSM"))
-    with pytest.raises(ValueError):
+    p.write_text(p.read_text().replace("RiemannSolver LF", "RiemannSolver Roe"))
+    with pytest.raises(ValueError, match="does not exist"):
         nb.read_decks(tmp_path)
     nb.write_decks(tmp_path, nb.BoxDesc(16, 16, 16))
     p.write_text(p.read_text() + "Bogus 1.0\n")
@@ -42,3 +42,12 @@ def test_scheme_strings_follow_the_reference(tmp_path):
     p.write_text(text.replace("scheme_y_ivs weno5z", "scheme_y_ivs hccs"))
     with pytest.raises(ValueError, match="not on the B200 path"):
         nb.read_decks(tmp_path)
+
+
+@pytest.mark.parametrize("riemann", [0, 1, 2])
+def test_riemann_solver_round_trip(tmp_path, riemann):
+    """PhysModel.in RiemannSolver LF / AUSM / AUSMp (physicsModel.cpp:16-20)."""
+    nb.write_decks(tmp_path, nb.BoxDesc(16, 16, 16, riemann=riemann))
+    text = (tmp_path / "inp" / "PhysModel.in").read_text()
+    assert f"RiemannSolver {['LF', 'AUSM', 'AUSMp'][riemann]}\n" in text
+    assert nb.read_decks(tmp_path)[0].riemann == riemann

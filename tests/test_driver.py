@@ -34,7 +34,8 @@ def parsed(text):
     dict(nx=24, ny=20, nz=16, mach=0.1, reynolds=1600.0, prandtl=0.71),
     dict(nx=40, ny=32, nz=24, scheme=(1, 2, 0), pde_model=0, mach=0.3, reynolds=250.5),
     dict(nx=16, ny=16, nz=16, scheme=(2, 2, 2), visc_model=1, gamma=1.3, lx=1.5, ly=2.5, lz=3.5),
-    dict(nx=20, ny=18, nz=16, scheme=(3, 0, 3)),
+    dict(nx=20, ny=18, nz=16, scheme=(3, 0, 3), riemann=1),
+    dict(nx=16, ny=16, nz=16, riemann=2, pde_model=0),
     dict(nx=32, ny=32, nz=32, forcing=1, forcing_amp=0.02, forcing_hel=0.1, forcing_k=2.0),
 ])
 def test_driver_reads_decks_like_the_python_reader(driver, tmp_path, kw):
@@ -55,6 +56,7 @@ def test_driver_reads_decks_like_the_python_reader(driver, tmp_path, kw):
         assert float(got[k]) == v
     assert float(got["endStep"]) == io["endStep"]
     assert int(got["forcing"]) == ref.forcing
+    assert int(got["riemann"]) == ref.riemann
     for k in ("forcing_amp", "forcing_hel", "forcing_k"):
         assert float(got[k]) == getattr(ref, k)
 

@@ -26,7 +26,7 @@ import pytest
 
 from helpers import (box_from_golden, desc_from_box, golden, max_rel_l2, rel_l2,
                      rounding_sensitivity)
-from oracle_ctypes import (CRWENO5, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_OFFDIAG_DIV,
+from oracle_ctypes import (AUSM, AUSMP, CRWENO5, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_OFFDIAG_DIV,
                            Q_WENOZ_BETA2, Q_ZETA_EIGEN, WENO5JS, WENO5Z, WENO7, Box, Oracle)
 
 pytestmark = pytest.mark.gpu
@@ -172,6 +172,66 @@ def test_mixed_precision_close_to_fp64(torch):
     print(f"mixed vs fp64 after 100 steps: max per-field rel L2 = {err:.3e}")
     assert err < 1e-6
     assert abs(ke[0] - ke[1]) <= 5e-3 * ke[1]
+
+
+def ausm_box(z, ns):
+    nz, ny, nx = (int(v) for v in z["shape"])
+    return Box(nx, ny, nz, scheme=(int(z["scheme"]),) * 3, navier_stokes=ns,
+               mach=float(z["mach"]), reynolds=float(z["reynolds"]),
+               prandtl=float(z["prandtl"]), riemann=int(z["riemann"]))
+
+
+@pytest.mark.parametrize("tag", ["ausm", "ausmp"])
+@pytest.mark.parametrize("ns", [True, False])
+def test_ausm_rhs_and_three_steps_match_reference(torch, tag, ns):
+    """RiemannAUSM / RiemannAUSMp (N-S with WENO5-Z at M 1.2, Euler with
+    WENO5-JS at M 0.3) against the reference's own outputs; dt checks that
+    the AUSM splits keep the z eigenvalue (no ZETA_EIGEN folding)."""
+    z = golden(f"step_{tag}_{'ns' if ns else 'eu'}.npz")
+    box = ausm_box(z, ns)
+    rhs, dtl = gpu_rhs(torch, box, z["q0"])
+    assert max_rel_l2(rhs, z["rhs"]) < TOL_FP64
+    assert abs(dtl - float(z["dt_local"])) <= 1e-14 * float(z["dt_local"])
+    q3, dt, res = gpu_steps(box, z["q0"], 3)
+    assert max_rel_l2(q3, z["q3"]) < TOL_FP64
+    np.testing.assert_allclose(dt, z["dt"], rtol=1e-13)
+    np.testing.assert_allclose(res, z["res"], rtol=1e-9)
+
+
+@pytest.mark.parametrize("riemann", [AUSM, AUSMP])
+def test_ausm_with_every_scheme_matches_oracle(torch, riemann):
+    """The AUSM splits feed every reconstruction (CRWENO5 lines and WENO7
+    sweeps included) on a transonic box (M 1.5: local Mach numbers on both
+    sides of 1)."""
+    box = Box(20, 16, 12, scheme=(CRWENO5, WENO7, WENO5Z), mach=1.5, reynolds=700.0,
+              riemann=riemann)
+    rng = np.random.default_rng(40 + riemann)
+    O = Oracle()
+    q = [a * (1 + 0.02 * rng.standard_normal(a.shape)) for a in O.tgv(box, (0.1, 0.2, -0.3))]
+    ref, dref = O.rhs(box, q)
+    got, dgot = gpu_rhs(torch, box, q)
+    assert max_rel_l2(got, ref) < TOL_FP64
+    assert abs(dgot - dref) <= 1e-14 * dref
+    qo, _, _ = O.run_steps(box, 0.5, 2, q)
+    qg, _, _ = gpu_steps(box, q, 2)
+    assert max_rel_l2(qg, qo) < step_tolerance(box, q, 2)
+
+
+def test_ausm_mixed_precision_close_to_fp64(torch):
+    """AUSMp with FP32 bulk arithmetic against its FP64 path: decaying
+    turbulence at 64^3, WENO5-Z, 50 steps."""
+    import nuc3d_b200 as nb
+    desc = nb.BoxDesc(64, 64, 64, mach=1.0, scheme=(nb.WENO5Z,) * 3, riemann=nb.RIEMANN_AUSMP)
+    init = {"kind": "hit", "seed": 5, "k_peak": 4.0, "mach_t": 0.3, "re_lambda": 100.0}
+    out = []
+    for precision in (nb.FP64, nb.MIXED):
+        with nb.Solver(nb.BoxDesc(**{**desc.__dict__, "precision": precision})) as s:
+            s.init_state(init)
+            s.step(50, 0.5, stats=False)
+            out.append(s.get_state())
+    err = max_rel_l2(out[1], out[0])
+    print(f"ausmp mixed vs fp64 after 50 steps: max per-field rel L2 = {err:.3e}")
+    assert err < 1e-6
 
 
 def test_weno7_mixed_precision_close_to_fp64(torch):
