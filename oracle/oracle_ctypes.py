@@ -299,6 +299,20 @@ class Reference:
         assert rc == 0, rc
         return out
 
+    def spectra(self, box: Box, q):
+        """postproc::solveFFT's nine shell spectra, shaped (9, kmax) in the
+        order kin, kinc, kins, kinl, kinr, hel, ens, den, pre (12 significant
+        digits, as the reference writes them)."""
+        kmax = min(box.nx, box.ny, box.nz) // 2
+        out = np.zeros((9, kmax))
+        with tempfile.TemporaryDirectory() as td:
+            write_decks(Path(td), box)
+            rc = self.lib.ref_spectra(str(td).encode(), box.nx, box.ny, box.nz,
+                                      C.c_double(box.dx), C.c_double(box.dy), C.c_double(box.dz),
+                                      _ptrs([np.ascontiguousarray(a) for a in q]), _ptr(out))
+        assert rc == 0, rc
+        return out
+
     def run_steps(self, box: Box, cfl, nsteps, q):
         q = [np.ascontiguousarray(a, dtype=np.float64).copy() for a in q]
         dt = np.zeros(nsteps)

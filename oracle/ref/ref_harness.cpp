@@ -19,12 +19,18 @@
 //                     nsteps steps, PDEData3d::solve (PDEData3d.cpp:155-213)
 //   ref_stats         postproc::solveQ (postproc.cpp:736-930): the averages it
 //                     keeps and the turb_para.dat line it writes
+//   ref_spectra       postproc::solveFFT (postproc.cpp:931-1184): the nine
+//                     shell spectra it writes (FFTs through the DFT stand-in)
 //
 // The solver classes read their decks from ./inp relative to the working
 // directory (fieldOperator.cpp:34, physicsModel.cpp:67), so the whole-step
 // entry points chdir into a caller-prepared directory first.
 
+#include <sys/stat.h>
 #include <unistd.h>
+
+#include <algorithm>
+#include <cerrno>
 
 #include <cstring>
 #include <memory>
@@ -92,6 +98,7 @@ struct RefSolver {
     RefSolver(int nx, int ny, int nz, double dx, double dy, double dz)
         : pde(nx, ny, nz, 5) {
         mpi.setTopo(1, 1, 1);
+        fft.initFFT(mpi, nx, ny, nz);  // block.cpp initialises it for every run
         if (phys.getMyModelName() == "NavierStokes3d")
             flux = std::make_shared<nuc3d::NaiverStokesData3d>(nx, ny, nz, 5, dx, dy, dz);
         else
@@ -270,6 +277,36 @@ int ref_stats(const char *workdir, int nx, int ny, int nz, double dx, double dy,
     if (!(f >> step >> time)) return -3;
     for (int i = 0; i < 9; ++i)
         if (!(f >> out[16 + i])) return -4;
+    return 0;
+}
+
+// postproc::solveTemporal's spectra (postproc.cpp:931-1184 with
+// fft.cpp:182-572) on q: solveQ for the enstrophy and helicity fields, then
+// solveFFT, which writes flowDataTemp/power_shell_0_<name>.dat per spectrum.
+// out[s*kmax + i] = shell i of spectrum s in the order kin, kinc, kins, kinl,
+// kinr, hel, ens, den, pre (12 significant digits, as written), kmax =
+// min(nx, ny, nz)/2.  The FFTs run through the DFT stand-in for FFTW.
+int ref_spectra(const char *workdir, int nx, int ny, int nz, double dx, double dy, double dz,
+                const double *const q[5], double *out) {
+    Cwd cwd(workdir);
+    if (mkdir("flowDataTemp", 0755) != 0 && errno != EEXIST) return -1;
+    RefSolver s(nx, ny, nz, dx, dy, dz);
+    s.load(q);
+    VectorField prim(5, Field(nx, ny, nz)), acou(3, Field(nx, ny, nz));
+    s.phys.getPrim(s.pde.getQ(), prim, acou);
+    nuc3d::postproc post(nx, ny, nz, dx, dy, dz);
+    post.solveQ(prim, acou, s.phys, s.op, s.buffers, s.mpi, 0, 0.0);
+    post.solveFFT(prim, acou, s.op, s.buffers, s.mpi, s.fft, 0, 0.0);
+    const int kmax = std::min(std::min(nx, ny), nz) / 2;
+    const char *names[9] = {"kin", "kinc", "kins", "kinl", "kinr", "hel", "ens", "den", "pre"};
+    for (int sp = 0; sp < 9; ++sp) {
+        std::ifstream f(std::string("flowDataTemp/power_shell_0_") + names[sp] + ".dat");
+        for (int i = 0; i < kmax; ++i) {
+            double idx, val, frac;
+            if (!(f >> idx >> val >> frac) || (int)idx != i) return -2 - sp;
+            out[sp * kmax + i] = val;
+        }
+    }
     return 0;
 }
 

@@ -95,7 +95,26 @@ def main():
     stats_fixture(R)
     weno7_fixtures(R)
     ausm_fixtures(R)
+    spectra_fixture(R)
     print("fixtures written to", HERE)
+
+
+def spectra_fixture(R):
+    """postproc::solveFFT's nine shell spectra (reference, FFTs through the
+    DFT stand-in for FFTW) of a perturbed Taylor-Green state with a mean flow
+    on a non-cubic box (kmax = 5), and of a 16^3 one."""
+    out = {}
+    for tag, shape in (("a", (16, 12, 10)), ("b", (16, 16, 16))):
+        box = Box(*shape, mach=0.5)
+        rng = np.random.default_rng(3 + len(tag) + shape[1])
+        q = [a * (1 + 0.05 * rng.standard_normal(a.shape))
+             for a in Oracle().tgv(box, (0.3, -0.2, 0.1))]
+        q[1] = q[1] + 0.1 * q[0]
+        out[f"{tag}_q"] = np.stack(q)
+        out[f"{tag}_spectra"] = R.spectra(box, q)
+        out[f"{tag}_shape"] = np.array(box.shape)
+        out[f"{tag}_mach"] = box.mach
+    np.savez_compressed(HERE / "spectra.npz", **out)
 
 
 def ausm_fixtures(R):

@@ -193,3 +193,19 @@ def test_ausm_rhs_and_steps_match_reference_golden(O, tag, ns):
     q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
     assert np.array_equal(np.stack(q3), z["q3"])
     assert np.array_equal(dt, z["dt"]) and np.array_equal(res, z["res"])
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_spectra_restatement_matches_reference_golden(tag):
+    """The numpy restatement of postproc::solveFFT against the reference's own
+    spectra (printed to 12 significant digits): folded kinetic spectra with
+    the k = 0 mode in shell 1, and the unfolded-octant scalar spectra."""
+    import spectra_oracle as so
+    z = golden("spectra.npz")
+    nz, ny, nx = (int(v) for v in z[f"{tag}_shape"])
+    box = Box(nx, ny, nz, mach=float(z[f"{tag}_mach"]))
+    got = so.spectra(list(z[f"{tag}_q"]), box.dx, box.dy, box.dz, box.gamma, box.mach)
+    ref = z[f"{tag}_spectra"]
+    assert got.shape == ref.shape == (9, min(nx, ny, nz) // 2)
+    assert np.all(ref[:5, 0] == 0.0)  # shell 0 of the kinetic spectra never fills
+    np.testing.assert_allclose(got, ref, rtol=1e-11, atol=1e-13 * np.abs(ref).max())
