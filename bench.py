@@ -310,6 +310,7 @@ def run_b200(args, rank, world, local_rank):
         nacc = args.accuracy_steps
         logs = {}
         finals = {}
+        spectra = {}
         for name, d in (("fp64", desc), ("mixed", dm)):
             with nb.Solver(d, stream=stream) as a:
                 a.set_state(q)
@@ -322,6 +323,7 @@ def run_b200(args, rank, world, local_rank):
                     log.append(a.stats())
                 logs[name] = log
                 finals[name] = a.get_state()
+                spectra[name] = a.spectra()
         r64, r32 = finals["fp64"], finals["mixed"]
         errs = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(r32, r64)]
         ke = [logs["mixed"][-1]["kinetic"], logs["fp64"][-1]["kinetic"]]
@@ -340,6 +342,10 @@ def run_b200(args, rank, world, local_rank):
             "tke_max_rel_diff_over_run": max_rel("kinetic"),
             "dissipation_max_rel_diff_over_run": max_rel("dissipation"),
             "stats_every_steps": 25,
+            # kinetic-energy spectrum (postproc::solveFFT "kin") after the run,
+            # shells holding at least 1e-10 of the energy
+            "spectrum_kin_max_rel_diff": spectrum_diff(spectra["mixed"][0], spectra["fp64"][0]),
+            "spectrum_kin_fp64": [float(v) for v in spectra["fp64"][0]],
             "fp64_stats": {k: [round(v[k], 10) for v in logs["fp64"]]
                            for k in ("kinetic", "dissipation", "enstrophy", "re_lambda", "mach_t")},
             "accuracy_steps": nacc,
@@ -390,6 +396,14 @@ def run_b200(args, rank, world, local_rank):
     }
     reps.close()
     return line
+
+
+def spectrum_diff(a, b):
+    """Max relative difference over the shells of spectrum b that hold at
+    least 1e-10 of its total."""
+    import numpy as np
+    on = b > 1e-10 * b.sum()
+    return float(np.max(np.abs(a[on] - b[on]) / b[on]))
 
 
 # ------------------------------------------------------------- schemes -----

@@ -339,6 +339,33 @@ NUC3D_API int nuc3d_serve_info(nuc3d_server *s, nuc3d_serve_stats *out);
 NUC3D_API int nuc3d_stats(nuc3d_ctx *ctx, double *h_out);
 NUC3D_API int nuc3d_batch_stats(nuc3d_batch *b, int box_id, double *h_out);
 
+/* Shell-binned spectra of the current state: postproc::solveFFT
+ * (postproc.cpp:931-1184) with fft.cpp:182-572, FP64, FFTs by cuFFT.
+ * h_out receives NUC3D_SPECTRA rows of kmax shells (row-major), kmax =
+ * min(nx, ny, nz)/2 written to *kmax; h_out may be NULL to query kmax.
+ * Rows, as the reference's power_shell_<step>_<name>.dat files:
+ *   kin, kinc, kins, kinl, kinr: 0.5 |u^|^2 of the velocity transform (normalised
+ *     by 1/N) and of its compressive, solenoidal and left/right helical parts,
+ *     binned over the folded |k| with |k| = 1 at k = 0 (the mean flow falls in
+ *     shell 1, shell 0 stays empty);
+ *   hel, ens, den, pre: |f^|^2 of the helicity field w.u, the enstrophy field
+ *     |w|^2/2, density and pressure, binned as fft.cpp:517-531 does: over the
+ *     unfolded i^2 + j^2 + k^2 (only the non-negative octant of wavenumbers).
+ * Shell i holds |k| in (i - 1/2, i + 1/2].  Allocates 112 bytes per cell of
+ * scratch for the call and synchronises the context's stream. */
+#define NUC3D_SPECTRA 9
+#define NUC3D_SPEC_KIN 0
+#define NUC3D_SPEC_KINC 1
+#define NUC3D_SPEC_KINS 2
+#define NUC3D_SPEC_KINL 3
+#define NUC3D_SPEC_KINR 4
+#define NUC3D_SPEC_HEL 5
+#define NUC3D_SPEC_ENS 6
+#define NUC3D_SPEC_DEN 7
+#define NUC3D_SPEC_PRE 8
+NUC3D_API int nuc3d_spectra(nuc3d_ctx *ctx, double *h_out, int *kmax);
+NUC3D_API int nuc3d_batch_spectra(nuc3d_batch *b, int box_id, double *h_out, int *kmax);
+
 /* Simulated time advanced by this context so far (block.cpp:208-209). */
 NUC3D_API double nuc3d_ctx_time(const nuc3d_ctx *ctx);
 

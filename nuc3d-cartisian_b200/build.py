@@ -27,6 +27,8 @@ OBJ = PKG / "_build"
 LIB = PKG / "lib" / "libnuc3d_b200.so"
 DRIVER = PKG / "lib" / "nuc3d_run"  # host/nuc3d_run.cpp: the C++ case driver
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# cuFFT (the spectra's transforms) is linked from the toolkit beside nvcc
+CUDA_LIB = str(Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "lib64")
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden,-pthread",
               "--expt-relaxed-constexpr", "-I", str(ROOT / "include"), "-I", str(CSRC)]
 
@@ -68,7 +70,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         tmp = LIB.with_suffix(".so.tmp")
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs),
                "-Xcompiler", "-static-libstdc++,-pthread", "-Xlinker", "--exclude-libs,ALL",
-               "-cudart", "static"]
+               "-cudart", "static", "-lcufft", "-Xlinker", "-rpath," + CUDA_LIB]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")

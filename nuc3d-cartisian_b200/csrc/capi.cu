@@ -207,6 +207,14 @@ int nuc3d_stats(nuc3d_ctx *c, double *h_out) {
     if (!c || !h_out) return fail(NUC3D_ERR_INVALID, "null argument");
     return c->eng->stats(c->id, h_out);
 }
+int nuc3d_spectra(nuc3d_ctx *c, double *h_out, int *kmax) {
+    if (!c) return fail(NUC3D_ERR_INVALID, "null context");
+    return c->eng->spectra(c->id, h_out, kmax);
+}
+int nuc3d_batch_spectra(nuc3d_batch *b, int box_id, double *h_out, int *kmax) {
+    if (!b) return fail(NUC3D_ERR_INVALID, "null batch");
+    return b->eng->spectra(box_id, h_out, kmax);
+}
 int nuc3d_batch_stats(nuc3d_batch *b, int box_id, double *h_out) {
     if (!b || !h_out) return fail(NUC3D_ERR_INVALID, "null argument");
     return b->eng->stats(box_id, h_out);

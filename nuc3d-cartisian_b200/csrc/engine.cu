@@ -8,6 +8,7 @@
 
 #include "forcing_kernels.h"
 #include "init_kernels.h"
+#include "spectra_kernels.h"
 #include "stats_kernels.h"
 #include "op_kernels.h"
 
@@ -719,6 +720,45 @@ int Engine::stats(int id, double out[26]) {
     ECK(cudaStreamSynchronize(stream_));
     stats_finish(b.dev.p, sums, out);
     return NUC3D_OK;
+}
+
+int Engine::spectra(int id, double *out, int *kmax_out) {
+    if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
+        return set_last_error(NUC3D_ERR_INVALID, "no such box");
+    if (!kmax_out) return set_last_error(NUC3D_ERR_INVALID, "null argument");
+    if (dirty_) {
+        int rc = rebuild();
+        if (rc) return rc;
+    }
+    EngineBox &b = boxes_[id];
+    const int kmax = spectra_kmax(b.dev.p);
+    *kmax_out = kmax;
+    if (!out) return NUC3D_OK;
+    if (!b.dev.active) return set_last_error(NUC3D_ERR_INVALID, "box is not active");
+    void *scratch = nullptr;
+    double *d_out = nullptr;
+    if (cudaMallocAsync(&scratch, spectra_scratch_bytes(b.dev.p), stream_) != cudaSuccess) {
+        cudaGetLastError();
+        return set_last_error(NUC3D_ERR_NOMEM, "no device memory for the spectra scratch");
+    }
+    int rc = NUC3D_OK;
+    int fft_status = 0;
+    cudaError_t e = cudaMallocAsync(&d_out, sizeof(double) * kSpectra * kmax, stream_);
+    if (e == cudaSuccess)
+        e = launch_prim(d_boxes_, d_items_ + r_prim_.off + b.prim_off, b.prim_n, 0, 0, stream_);
+    if (e == cudaSuccess) e = launch_spectra(b.dev, scratch, d_out, &fft_status, stream_);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, d_out, sizeof(double) * kSpectra * kmax, cudaMemcpyDeviceToHost,
+                            stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (fft_status != 0)
+        rc = set_last_error(NUC3D_ERR_CUDA, ("cuFFT failed with status " +
+                                             std::to_string(fft_status)).c_str());
+    else if (e != cudaSuccess)
+        rc = set_last_error(NUC3D_ERR_CUDA, cudaGetErrorString(e));
+    cudaFreeAsync(scratch, stream_);
+    if (d_out) cudaFreeAsync(d_out, stream_);
+    return rc;
 }
 
 int Engine::sync_and_check(int id) {

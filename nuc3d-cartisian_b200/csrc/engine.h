@@ -48,6 +48,9 @@ public:
     int init_state(int id, const nuc3d_init_desc &in, double info[3]);
     // Turbulence statistics of box id's current state (NUC3D_STATS values).
     int stats(int id, double out[26]);
+    // the nine shell spectra of box id into out[9 * kmax] (host); *kmax_out
+    // receives kmax = min(nx, ny, nz)/2.  out may be NULL to query kmax.
+    int spectra(int id, double *out, int *kmax_out);
     int sync_and_check(int id_or_all);
     double time(int id);
     long long box_steps(int id) const;

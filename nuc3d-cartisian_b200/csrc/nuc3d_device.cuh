@@ -427,6 +427,19 @@ __device__ __forceinline__ B cd6(B m3, B m2, B m1, B p1, B p2, B p3, B inv_dx) {
     return (B(K::CD3) * (p3 - m3) + B(K::CD2) * (p2 - m2) + B(K::CD1) * (p1 - m1)) * inv_dx;
 }
 
+// CD6 derivative of a whole-box field f at cell (i, j, k) along axis d with
+// the periodic wrap (centraldifference6th.cpp:44-46 on one rank), FP64; the
+// diagnostics' gradients (statistics, spectra).
+__device__ __forceinline__ double cd6_at(const double *f, const BoxParams &p, int i, int j, int k,
+                                         int d) {
+    const int n = p.n[d];
+    const int c = d == 0 ? i : (d == 1 ? j : k);
+    const long long base = (long long)i + p.stride[1] * j + p.stride[2] * k - p.stride[d] * c;
+    auto at = [&](int o) { return f[base + p.stride[d] * wrap(c + o, n)]; };
+    return (K::CD3 * (at(3) - at(-3)) + K::CD2 * (at(2) - at(-2)) + K::CD1 * (at(1) - at(-1))) /
+           p.d[d];
+}
+
 // Viscosity and heat-conduction coefficient (physicsModel.cpp:193-266).
 template <typename B>
 __device__ __forceinline__ void viscosity(const BoxParams &bp, B T, B &miu, B &coeff) {

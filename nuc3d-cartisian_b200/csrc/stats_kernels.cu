@@ -34,17 +34,6 @@ __device__ void block_sum(double (&v)[NV], double *out) {
     }
 }
 
-// CD6 derivative of f at cell (i, j, k) along axis d (centraldifference6th.cpp:44-46)
-__device__ __forceinline__ double cd6_at(const double *f, const BoxParams &p, int i, int j, int k,
-                                         int d) {
-    const int n = p.n[d];
-    const int c = d == 0 ? i : (d == 1 ? j : k);
-    const long long base = (long long)i + p.stride[1] * j + p.stride[2] * k - p.stride[d] * c;
-    auto at = [&](int o) { return f[base + p.stride[d] * wrap(c + o, n)]; };
-    return (K::CD3 * (at(3) - at(-3)) + K::CD2 * (at(2) - at(-2)) + K::CD1 * (at(1) - at(-1))) /
-           p.d[d];
-}
-
 __global__ void __launch_bounds__(kThreads) k_stats(BoxDev b, double *partials) {
     const BoxParams &p = b.p;
     const double *rho = fieldU(b, 0, 0);

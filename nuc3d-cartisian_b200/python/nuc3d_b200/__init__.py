@@ -160,6 +160,8 @@ def lib() -> C.CDLL:
         L.nuc3d_batch_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.nuc3d_stats.argtypes = [C.c_void_p, C.c_void_p]
         L.nuc3d_batch_stats.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.nuc3d_spectra.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
+        L.nuc3d_batch_spectra.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
         L.nuc3d_init_state.argtypes = [C.c_void_p, C.POINTER(_Init), C.c_void_p]
         L.nuc3d_batch_init_state.argtypes = [C.c_void_p, C.c_int, C.POINTER(_Init), C.c_void_p]
         L.nuc3d_serve_config_default.argtypes = [C.POINTER(_ServeConfig)]
@@ -357,6 +359,11 @@ class Solver:
         """Turbulence statistics of the current state (nuc3d_stats)."""
         return _stats(lib().nuc3d_stats, self._h)
 
+    def spectra(self):
+        """The nine shell spectra of the current state (nuc3d_spectra): a
+        (9, kmax) array, rows in SPECTRA_NAMES order."""
+        return _spectra(lib().nuc3d_spectra, self._h)
+
     def step(self, nsteps: int, cfl: float, stats: bool = True):
         import numpy as np
         if stats:
@@ -468,6 +475,10 @@ class Batch:
     def stats(self, bid: int) -> dict:
         """Turbulence statistics of box bid (nuc3d_batch_stats)."""
         return _stats(lib().nuc3d_batch_stats, self._h, bid)
+
+    def spectra(self, bid: int):
+        """The nine shell spectra of box bid (nuc3d_batch_spectra)."""
+        return _spectra(lib().nuc3d_batch_spectra, self._h, bid)
 
     def step(self, nsteps: int = 1):
         check(lib().nuc3d_batch_step(self._h, nsteps))
@@ -586,6 +597,18 @@ class Server:
         st = _ServeStats()
         check(lib().nuc3d_serve_info(self._h, C.byref(st)))
         return {k: getattr(st, k) for k, _ in _ServeStats._fields_ if k != "pad"}
+
+
+SPECTRA_NAMES = ("kin", "kinc", "kins", "kinl", "kinr", "hel", "ens", "den", "pre")
+
+
+def _spectra(fn, *args):
+    import numpy as np
+    kmax = C.c_int(0)
+    check(fn(*args, None, C.byref(kmax)))
+    out = np.zeros((len(SPECTRA_NAMES), kmax.value))
+    check(fn(*args, out.ctypes.data, C.byref(kmax)))
+    return out
 
 
 def _tuning(fn, h):
