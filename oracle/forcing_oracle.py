@@ -3,9 +3,11 @@
 the device forcing, never part of the product.
 
 The reference transforms with FFTW (fft.cpp:182-572: forward normalised by
-1/N, backward unnormalised), which is absent here, so its own forcing cannot
-run and this restatement is "parity unpinned" against it; every step below
-follows the cited lines, with numpy's FFTs under the same conventions.
+1/N, backward unnormalised).  FFTW is absent here; the compiled reference runs
+its own AddForcing_Const through a DFT stand-in for FFTW
+(oracle/ref/fftw_standin.cpp), and this restatement, with numpy's FFTs under
+the same conventions, is pinned to it (tests/test_oracle.py, golden
+forcing.npz: agreement to ~1e-14 of the forcing's scale).
 """
 
 from __future__ import annotations

@@ -81,6 +81,13 @@ class Box:
     powerlaw_exp: float = 0.76
     quirks: int = QUIRKS_REFERENCE
     riemann: int = LF
+    # PhysModel.in Forcing (physicsModel.cpp:50-56): 0 None, 1 Const.  Only
+    # the compiled reference runs it (the C restatement has no forcing; its
+    # numpy restatement is forcing_oracle.py).
+    forcing: int = 0
+    forcing_amp: float = 0.01
+    forcing_hel: float = 0.01
+    forcing_k: float = 1.0
 
     @property
     def dx(self):
@@ -181,6 +188,8 @@ class Oracle:
                               _ptrs(ui))
 
     def rhs(self, box: Box, q):
+        if box.forcing:
+            raise NotImplementedError("the C restatement has no forcing (forcing_oracle.py)")
         out = [np.zeros(box.shape) for _ in range(5)]
         b = box.c_struct()
         dt_local = self.lib.or_rhs(C.byref(b), _ptrs(q), _ptrs(out))
@@ -224,9 +233,12 @@ def write_decks(dirpath: Path, box: Box, cfl: float = 0.5):
     model = "NavierStokes3d" if box.navier_stokes else "Euler3d"
     (inp / "PhysModel.in").write_text(
         f"Neqs 5\nEosName IdealGas\nRiemannSolver {RIEMANN_NAMES[box.riemann]}\n"
-        f"PDEModel {model}\nViscousModel {VISC_NAMES[box.visc_model]}\nForcing None\n"
+        f"PDEModel {model}\nViscousModel {VISC_NAMES[box.visc_model]}\n"
+        f"Forcing {'Const' if box.forcing else 'None'}\n"
         f"Reynolds {box.reynolds!r}\nMach {box.mach!r}\nPt {box.prandtl!r}\n"
-        f"Gamma {box.gamma!r}\nT_ref {box.t_ref!r}\nT_inf {box.t_inf!r}\n")
+        f"Gamma {box.gamma!r}\nT_ref {box.t_ref!r}\nT_inf {box.t_inf!r}\n"
+        f"Forcing_amplitude {box.forcing_amp!r}\nForcing_amplitude_hel {box.forcing_hel!r}\n"
+        f"Forcing_wave_k {box.forcing_k!r}\n")
     # postproc.cpp:35-58: no averaging, simultaneous Q statistics, no files
     (inp / "PostProc.in").write_text(
         "AverageType 0\nAverageStartStep 0\nSimutaneousData 1\nAveragedSaveType 0\n"

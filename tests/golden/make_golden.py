@@ -96,7 +96,33 @@ def main():
     weno7_fixtures(R)
     ausm_fixtures(R)
     spectra_fixture(R)
+    forcing_fixture(R)
     print("fixtures written to", HERE)
+
+
+def forcing_fixture(R):
+    """physicsModel::AddForcing_Const (physicsModel.cpp:1368-1641) run by the
+    reference itself (FFTs through the DFT stand-in for FFTW): one RHS with
+    and without the shell forcing on a perturbed Taylor-Green state with a
+    mean flow, for shell radii 1 and 2 (helical part 0.3)."""
+    out = {}
+    for tag, shape, kf in (("a", (16, 12, 10), 1.0), ("b", (16, 16, 16), 2.0)):
+        box = Box(*shape, mach=0.5, reynolds=400.0, scheme=(WENO5Z,) * 3)
+        rng = np.random.default_rng(31 + shape[1])
+        q = [a * (1 + 0.05 * rng.standard_normal(a.shape))
+             for a in Oracle().tgv(box, (0.3, -0.2, 0.1))]
+        q[2] = q[2] + 0.05 * q[0]
+        off, _ = R.rhs(box, q)
+        forced = Box(**{**box.__dict__, "forcing": 1, "forcing_amp": 0.05, "forcing_hel": 0.3,
+                        "forcing_k": kf})
+        on, _ = R.rhs(forced, q)
+        out[f"{tag}_q"] = np.stack(q)
+        out[f"{tag}_rhs_off"] = np.stack(off)
+        out[f"{tag}_rhs_on"] = np.stack(on)
+        out[f"{tag}_shape"] = np.array(box.shape)
+        out[f"{tag}_kf"] = kf
+    out["mach"], out["reynolds"], out["amp"], out["hel"] = 0.5, 400.0, 0.05, 0.3
+    np.savez_compressed(HERE / "forcing.npz", **out)
 
 
 def spectra_fixture(R):

@@ -216,6 +216,28 @@ def test_spectral_forcing_matches_restatement(nb, kf, shape):
         np.testing.assert_allclose(got, terms[e - 1], rtol=0, atol=atol)
 
 
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_spectral_forcing_matches_reference_golden(nb, tag):
+    """The device forced RHS against the reference's own (AddForcing_Const run
+    by the compiled reference, FFTs through the DFT stand-in for FFTW)."""
+    import torch
+    from helpers import golden
+    z = golden("forcing.npz")
+    nz, ny, nx = (int(v) for v in z[f"{tag}_shape"])
+    desc = nb.BoxDesc(nx, ny, nz, mach=float(z["mach"]), reynolds=float(z["reynolds"]),
+                      prandtl=0.71, scheme=(nb.WENO5Z,) * 3, forcing=nb.FORCING_CONST,
+                      forcing_amp=float(z["amp"]), forcing_hel=float(z["hel"]),
+                      forcing_k=float(z[f"{tag}_kf"]))
+    with nb.Solver(desc) as s:
+        s.set_state([np.ascontiguousarray(a) for a in z[f"{tag}_q"]])
+        out = [torch.zeros(desc.shape, dtype=torch.float64, device="cuda") for _ in range(5)]
+        s.rhs(out)
+        got = [o.cpu().numpy() for o in out]
+    for e in range(5):
+        ref = z[f"{tag}_rhs_on"][e]
+        assert np.linalg.norm(got[e] - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
 def test_spectra_match_reference_golden(nb):
     """nuc3d_spectra (cuFFT transforms, device binning) against the
     reference's own postproc::solveFFT spectra (12 printed digits, FFTs

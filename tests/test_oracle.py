@@ -209,3 +209,23 @@ def test_spectra_restatement_matches_reference_golden(tag):
     assert got.shape == ref.shape == (9, min(nx, ny, nz) // 2)
     assert np.all(ref[:5, 0] == 0.0)  # shell 0 of the kinetic spectra never fills
     np.testing.assert_allclose(got, ref, rtol=1e-11, atol=1e-13 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_forcing_restatement_matches_reference_golden(tag):
+    """forcing_oracle.forcing_terms (numpy restatement of AddForcing_Const)
+    against the reference's own forced RHS minus its unforced RHS (the
+    reference's forcing run through the DFT stand-in for FFTW)."""
+    from forcing_oracle import forcing_terms
+    z = golden("forcing.npz")
+    nz, ny, nx = (int(v) for v in z[f"{tag}_shape"])
+    q = list(z[f"{tag}_q"])
+    prim = Oracle().con2prim(Box(nx, ny, nz, mach=float(z["mach"])), q)
+    terms, _ = forcing_terms(prim[1], prim[2], prim[3], float(z["amp"]), float(z["hel"]),
+                             float(z[f"{tag}_kf"]))
+    d = z[f"{tag}_rhs_off"] - z[f"{tag}_rhs_on"]
+    assert np.array_equal(d[0], np.zeros_like(d[0]))  # no mass source
+    for e in range(1, 5):
+        scale = np.abs(terms[e - 1]).max()
+        assert scale > 0
+        assert np.abs(d[e] - terms[e - 1]).max() <= 1e-12 * max(scale, np.abs(z[f"{tag}_rhs_off"][e]).max())
