@@ -10,7 +10,8 @@
 // iteration while time <= tl and step < endStep, the status line of
 // block::printStatus (block.cpp:217-220), restart files every saveStep
 // (block.cpp:609-638) and, every postStep, the solveQ statistics appended to
-// enstrophy.dat and turb_para.dat (postproc.cpp:888-927).
+// enstrophy.dat and turb_para.dat (postproc.cpp:888-927) and the solveFFT
+// shell spectra in flowDataTemp/power_shell_<step>_<name>.dat.
 //
 // Only the C ABI in include/nuc3d_b200.h is used.  One process, one box,
 // periodic, process topology 1 1 1 (there is no MPI on this path).
@@ -195,6 +196,29 @@ void check(int rc, const char *what) {
 
 }  // namespace
 
+// postproc::solveFFT's shell spectra (postproc.cpp:931-1184) written as
+// fft::solveShell writes them (fft.cpp:449-472): one file per spectrum,
+// flowDataTemp/power_shell_<step>_<name>.dat, lines "i E_i E_i/sum(E)".
+void write_spectra(nuc3d_ctx *ctx, const std::string &dir, long long step) {
+    static const char *names[NUC3D_SPECTRA] = {"kin", "kinc", "kins", "kinl", "kinr",
+                                               "hel", "ens", "den", "pre"};
+    int kmax = 0;
+    check(nuc3d_spectra(ctx, nullptr, &kmax), "nuc3d_spectra");
+    std::vector<double> sp((size_t)NUC3D_SPECTRA * kmax);
+    check(nuc3d_spectra(ctx, sp.data(), &kmax), "nuc3d_spectra");
+    mkdir((dir + "/flowDataTemp").c_str(), 0755);
+    for (int s = 0; s < NUC3D_SPECTRA; ++s) {
+        const double *e = sp.data() + (size_t)s * kmax;
+        double total = 0.0;
+        for (int i = 0; i < kmax; ++i) total += e[i];
+        std::ofstream f(dir + "/flowDataTemp/power_shell_" + std::to_string(step) + "_" +
+                        names[s] + ".dat");
+        for (int i = 0; i < kmax; ++i)
+            f << std::setprecision(12) << i << " " << e[i] << " " << e[i] / total << "\n";
+        f << std::endl;
+    }
+}
+
 int main(int argc, char **argv) {
     std::string dir = ".";
     int precision = NUC3D_FP64;
@@ -295,6 +319,7 @@ int main(int argc, char **argv) {
             ft << std::setprecision(12) << step << " " << time;
             for (int i = 16; i < 25; ++i) ft << " " << st[i];
             ft << "\n";
+            write_spectra(ctx, dir, step);
         }
         if (step % save == 0) output();
     }

@@ -47,6 +47,13 @@ def test_driver_tgv_10_steps_matches_reference(driver, tmp_path):
     assert max_rel_l2(q, z["q10"]) < 1e-12
     assert abs(t - float(np.sum(z["dt"]))) <= 1e-13 * t
     assert len((tmp_path / "enstrophy.dat").read_text().splitlines()) == 2  # steps 5 and 10
+    # spectra files as fft::solveShell writes them: "i E_i E_i/sum(E)" per shell
+    for name in ("kin", "kinc", "kins", "kinl", "kinr", "hel", "ens", "den", "pre"):
+        rows = np.loadtxt(tmp_path / "flowDataTemp" / f"power_shell_10_{name}.dat")
+        assert rows.shape == (12, 3) and np.array_equal(rows[:, 0], np.arange(12))
+        np.testing.assert_allclose(rows[:, 2], rows[:, 1] / rows[:, 1].sum(), rtol=1e-10)
+    kin = np.loadtxt(tmp_path / "flowDataTemp" / "power_shell_10_kin.dat")[:, 1]
+    assert kin[0] == 0.0 and kin[1] > 0.1 * kin.sum()  # the TGV's energy sits in shell 1
 
 
 def test_driver_restart_continues_bitwise(driver, tmp_path):
