@@ -152,9 +152,25 @@ __global__ void __launch_bounds__(kCrThreads)
     // the box's point-wise split (LF / AUSM / AUSMp) of equation e at cell g
     const int riemann = bp.riemann;
     auto split = [&](int e, long long g, double &fp, double &fm) {
-        SplitCell sc;
-        split_prepare(riemann, wbase[DIR * np + g], wbase[3 * np + g], wbase[4 * np + g], sc);
-        split_eq<DIR>(riemann, sc, e, qbase[e * np + g], fp, fm);
+        const double qe = qbase[e * np + g];
+        const double un = wbase[DIR * np + g], p = wbase[3 * np + g], c = wbase[4 * np + g];
+        if (riemann == RIEMANN_LF) {  // block-uniform; physicsModel.cpp:546-565
+            const double lam = add_(fabs(un), c);
+            double f;
+            if (e == 4)
+                f = mul_(un, add_(qe, p));
+            else if (e == 1 + DIR)
+                f = fma_(un, qe, p);
+            else
+                f = mul_(un, qe);
+            const double t = mul_(lam, qe);
+            fp = mul_(0.5, add_(f, t));
+            fm = mul_(0.5, sub_(f, t));
+        } else {
+            SplitCell sc;
+            split_prepare(riemann, un, p, c, sc);
+            split_eq<DIR>(riemann, sc, e, qe, fp, fm);
+        }
     };
     const bool mixed = sizeof(B) == sizeof(float);
     const bool bounded = (bp.quirks & QK_CRWENO_BOUNDED) != 0;
@@ -207,9 +223,14 @@ __global__ void __launch_bounds__(kCrThreads)
 
         if (l0 + warp < nl) {  // warp-uniform
             auto F = [&](int c) -> B { return myF[c + 3]; };
+            // the two half-warps run the same instructions: the sign only
+            // selects which cells feed a stencil ('+' reads upwind from the
+            // left, '-' from the right)
+            const int dir = sg == 0 ? 1 : -1;
             auto js = [&](int m) -> B {
-                return sg == 0 ? weno5js_face(F(m - 3), F(m - 2), F(m - 1), F(m), F(m + 1))
-                               : weno5js_face(F(m + 2), F(m + 1), F(m), F(m - 1), F(m - 2));
+                const int c0 = sg == 0 ? m - 3 : m + 2;
+                return weno5js_face(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
+                                    F(c0 + 4 * dir));
             };
             // explicit faces of the bounded system: 0, 1, 2, n-2, n-1, n
             int xm = -1;
@@ -237,13 +258,15 @@ __global__ void __launch_bounds__(kCrThreads)
                         b = B(1);
                         c = B(0);
                         d = js(r + 3);
-                    } else if (sg == 0) {
-                        cr_row(w[0], w[1], w[2], w[3], w[4], a, b, c, d);
                     } else {
+                        // '+': cells i-2..i+2 = w[0..4]; '-': cells i+3..i-1 = w[5..1]
+                        // with the off-diagonals swapped (crweno5.cpp:335-338)
+                        const bool m = sg != 0;
                         B lo, hi;
-                        cr_row(w[5], w[4], w[3], w[2], w[1], lo, b, hi, d);
-                        a = hi;
-                        c = lo;
+                        cr_row(m ? w[5] : w[0], m ? w[4] : w[1], m ? w[3] : w[2],
+                               m ? w[2] : w[3], m ? w[1] : w[4], lo, b, hi, d);
+                        a = m ? hi : lo;
+                        c = m ? lo : hi;
                     }
                 };
                 auto advance = [&]() {

@@ -241,7 +241,11 @@ __device__ __forceinline__ void split_prepare(int riemann, double un, double p, 
         s.a[1] = add_(fabs(un), c);
         return;
     }
-    const double m = un / c;  // IEEE division, as the reference
+    // m = u_n / c by a correctly rounded reciprocal (within an ulp of the
+    // reference's division); no division is inlined into the sweeps.  For
+    // |m| >= 1 the pressure weights 0.5 p (m +- |m|) / m are p or 0 exactly
+    // in real arithmetic (the reference's rounding of them is within an ulp).
+    const double m = mul_(un, __drcp_rn(c));
     const double am = fabs(m);
     double mp, mm, pp, pm;
     if (am < 1.0) {
@@ -259,8 +263,8 @@ __device__ __forceinline__ void split_prepare(int riemann, double un, double p, 
     } else {
         mp = mul_(0.5, add_(m, am));
         mm = mul_(0.5, sub_(m, am));
-        pp = mul_(mul_(0.5, p), add_(m, am)) / m;
-        pm = mul_(mul_(0.5, p), sub_(m, am)) / m;
+        pp = m > 0.0 ? p : 0.0;
+        pm = m > 0.0 ? 0.0 : p;
     }
     s.a[0] = mul_(mp, c);
     s.a[1] = mul_(mm, c);

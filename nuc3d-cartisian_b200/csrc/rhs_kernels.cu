@@ -246,10 +246,30 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
     };
     const int riemann = bp.riemann;
     auto split = [&](long long g, double Fp[5], double Fm[5]) {
-        SplitCell sc;
-        split_prepare(riemann, wbase[DIR * np + g], wbase[3 * np + g], wbase[4 * np + g], sc);
+        double Q[5];
 #pragma unroll
-        for (int e = 0; e < 5; ++e) split_eq<DIR>(riemann, sc, e, qbase[e * np + g], Fp[e], Fm[e]);
+        for (int e = 0; e < 5; ++e) Q[e] = qbase[e * np + g];
+        const double un = wbase[DIR * np + g], p = wbase[3 * np + g], c = wbase[4 * np + g];
+        if (riemann == RIEMANN_LF) {  // block-uniform
+            // physicsModel.cpp:546-565, spelt out for all five equations
+            const double lam = add_(fabs(un), c);
+            double f[5];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) f[e] = mul_(un, Q[e]);
+            f[1 + DIR] = fma_(un, Q[1 + DIR], p);
+            f[4] = mul_(un, add_(Q[4], p));
+#pragma unroll
+            for (int e = 0; e < 5; ++e) {
+                const double t = mul_(lam, Q[e]);
+                Fp[e] = mul_(0.5, add_(f[e], t));
+                Fm[e] = mul_(0.5, sub_(f[e], t));
+            }
+        } else {
+            SplitCell sc;
+            split_prepare(riemann, un, p, c, sc);
+#pragma unroll
+            for (int e = 0; e < 5; ++e) split_eq<DIR>(riemann, sc, e, Q[e], Fp[e], Fm[e]);
+        }
     };
     const bool mixed = sizeof(B) == sizeof(float);
     if (mixed) {  // per-line reference values (cell c0, always inside the box)
