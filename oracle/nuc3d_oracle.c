@@ -96,8 +96,14 @@ static const double C_W7[4] = {1.0 / 35.0, 12.0 / 35.0, 18.0 / 35.0, 4.0 / 35.0}
  * upwind-oriented 7-cell stencil f[0..6].  Its weights are the Z form
  * alpha_k = c_k (1 + (tau7/(eps+beta_k))^p), tau7 = |beta0 - beta3|,
  * eps = 1e-20 (weno7js.cpp:14, :111-114; the JS form is commented out). */
-static double weno7_face(const double f[7]) {
-    const double ss = 1.0e-20;
+static double weno7_face_eps(const double f[7], double ss, int literal_square);
+static double weno7_face(const double f[7]) { return weno7_face_eps(f, 1.0e-20, 0); }
+
+/* The same face with the caller's eps and squaring: hccs evaluates its WENO7
+ * faces with its own member ss = 1e-40 (hccs.cpp:13-17) and squares with
+ * std::pow(x, 2), a literal exponent the compiler turns into x*x, where
+ * weno7js raises to its runtime member p through libm's pow. */
+static double weno7_face_eps(const double f[7], double ss, int literal_square) {
     double is0 = f[0] * (547.0 * f[0] - 3882.0 * f[1] + 4642.0 * f[2] - 1854.0 * f[3]) +
                  f[1] * (7043.0 * f[1] - 17246.0 * f[2] + 7042.0 * f[3]) +
                  f[2] * (11003.0 * f[2] - 9402.0 * f[3]) + 2107.0 * f[3] * f[3];
@@ -115,10 +121,12 @@ static double weno7_face(const double f[7]) {
     double q42 = A7[2][0] * f[2] + A7[2][1] * f[3] + A7[2][2] * f[4] + A7[2][3] * f[5];
     double q43 = A7[3][0] * f[3] + A7[3][1] * f[4] + A7[3][2] * f[5] + A7[3][3] * f[6];
     double tau7 = fabs(is0 - is3);
-    double alpha0 = C_W7[0] * (1.0 + PW(tau7 / (ss + is0)));
-    double alpha1 = C_W7[1] * (1.0 + PW(tau7 / (ss + is1)));
-    double alpha2 = C_W7[2] * (1.0 + PW(tau7 / (ss + is2)));
-    double alpha3 = C_W7[3] * (1.0 + PW(tau7 / (ss + is3)));
+    double r0 = tau7 / (ss + is0), r1 = tau7 / (ss + is1), r2 = tau7 / (ss + is2),
+           r3 = tau7 / (ss + is3);
+    double alpha0 = C_W7[0] * (1.0 + (literal_square ? SQ(r0) : PW(r0)));
+    double alpha1 = C_W7[1] * (1.0 + (literal_square ? SQ(r1) : PW(r1)));
+    double alpha2 = C_W7[2] * (1.0 + (literal_square ? SQ(r2) : PW(r2)));
+    double alpha3 = C_W7[3] * (1.0 + (literal_square ? SQ(r3) : PW(r3)));
     double alphaSum = alpha0 + alpha1 + alpha2 + alpha3;
     double omega0 = alpha0 / alphaSum;
     double omega1 = alpha1 / alphaSum;
@@ -128,7 +136,7 @@ static double weno7_face(const double f[7]) {
 }
 
 /* buffer (halo) width of a scheme (fieldOperator.cpp:128-175) */
-static int halo_of(int scheme) { return scheme == OR_WENO7 ? 4 : 3; }
+static int halo_of(int scheme) { return (scheme == OR_WENO7 || scheme == OR_HCCS) ? 4 : 3; }
 
 /* One compact-WENO row (crweno5.cpp:131-162 for '+', :311-341 for '-').
  * f[0..4] is the upwind-oriented 5-cell stencil of the row's cell i
@@ -174,6 +182,49 @@ static void thomas_ref(int M, double *a, double *b, double *c, double *d, double
     for (int i = M - 2; i >= 0; i--) x[i] = d[i] - c[i] * x[i + 1];
 }
 
+/* schemes.hpp:30 coeff_upwindcompact_c */
+static const double C_UPC[3] = {2.0 / 7.0, 4.0 / 7.0, 1.0 / 7.0};
+
+/* One hybrid compact row of hccs (hccs.cpp:138-185 for '+', :375-420 for
+ * '-').  f[0..4] is the upwind-oriented 5-cell stencil of the row's cell i
+ * ('+': cells i-2..i+2; '-': cells i+3..i-1).  Returns the upwind-side
+ * coupling lo, the diagonal b, the downwind-side coupling hi and d:
+ *   WENO5-Z type weights with the CRWENO5 linear weights, eps = 1e-40,
+ *   theta = 1/(1 + (sum alpha - 1)^2); theta > 1/2 takes the linear upwind
+ *   compact row (2/7, 4/7, 1/7 | q7), otherwise the CRWENO5 row scaled by
+ *   (1 - theta)/theta plus the linear one.  Squares are std::pow(x, 2) with a
+ *   literal exponent in the reference, i.e. x*x. */
+static void hccs_row(const double f[5], double *lo, double *b, double *hi, double *d) {
+    const double ss = 1.0e-40;
+    double is0 = G0 * SQ(f[0] - 2.0 * f[1] + f[2]) + G1 * SQ(f[0] - 4.0 * f[1] + 3.0 * f[2]);
+    double is1 = G0 * SQ(f[1] - 2.0 * f[2] + f[3]) + G1 * SQ(f[1] - f[3]);
+    double is2 = G0 * SQ(f[2] - 2.0 * f[3] + f[4]) + G1 * SQ(3.0 * f[2] - 4.0 * f[3] + f[4]);
+    double q7 = (-f[0] + 19.0 * f[1] + 239.0 * f[2] + 159.0 * f[3] + 4.0 * f[4]) / 420.0;
+    double tau = fabs(is2 - is0);
+    double alpha0 = C_CR5[0] * (1.0 + SQ(tau / (is0 + ss)));
+    double alpha1 = C_CR5[1] * (1.0 + SQ(tau / (is1 + ss)));
+    double alpha2 = C_CR5[2] * (1.0 + SQ(tau / (is2 + ss)));
+    double alphaSum = alpha0 + alpha1 + alpha2;
+    double omega0 = alpha0 / alphaSum;
+    double omega1 = alpha1 / alphaSum;
+    double omega2 = alpha2 / alphaSum;
+    double theta = 1.0 / (1.0 + SQ(alphaSum - 1.0));
+    if (theta > 0.5) {
+        *lo = 2.0 / 7.0;
+        *b = 4.0 / 7.0;
+        *hi = 1.0 / 7.0;
+        *d = q7;
+    } else {
+        *lo = (2.0 / 3.0 * omega0 + 1.0 / 3.0 * omega1) * (1.0 - theta) / theta + C_UPC[0];
+        *b = (1.0 / 3.0 * omega0 + 2.0 / 3.0 * (omega1 + omega2)) * (1.0 - theta) / theta + C_UPC[1];
+        *hi = (1.0 / 3.0 * omega2) * (1.0 - theta) / theta + C_UPC[2];
+        *d = (1.0 / 6.0 * omega0 * f[1] + (5.0 * (omega0 + omega1) + omega2) * f[2] / 6.0 +
+              (omega1 + 5.0 * omega2) * f[3] / 6.0) *
+                 (1.0 - theta) / theta +
+             q7;
+    }
+}
+
 /* Reconstruct all n+1 faces of one line.  line[] covers cells -3..n+2 (index
  * with line[c], c may be negative).  out[m], m=0..n.  This is what
  * interpolationInner + interpolationBoundaryL + interpolationBoundaryR
@@ -192,6 +243,51 @@ static void reconstruct_line_ref(int scheme, int upwind, unsigned quirks, int n,
             for (int k = 0; k < 7; ++k) g[k] = upwind > 0 ? line[m - 4 + k] : line[m + 3 - k];
             out[m] = weno7_face(g);
         }
+        return;
+    }
+    if (scheme == OR_HCCS) {
+        /* hccs (hccs.cpp): faces 0..3 and n-3..n explicit WENO7 from the
+         * halos (:538-980); the rows of cells i = 3..n-5 (faces 4..n-4,
+         * :54-245 / :272-471) solved by the Thomas sweep (:232-245), the
+         * first and last rows identity rows holding WENO7 values.  Every
+         * WENO7 face here uses hccs's eps = 1e-40, not weno7js's 1e-20. */
+        double g[7];
+        for (int m = 0; m <= n; ++m) {
+            if (m >= 4 && m <= n - 4) continue;
+            for (int k = 0; k < 7; ++k) g[k] = upwind > 0 ? line[m - 4 + k] : line[m + 3 - k];
+            out[m] = weno7_face_eps(g, 1.0e-40, 1);
+        }
+        int ibeg = 3, iend = n - 4, M = iend - ibeg;
+        if (M < 2) return;
+        double *a = work, *b = work + M, *c = work + 2 * M, *d = work + 3 * M, *x = work + 4 * M;
+        for (int r = 0; r < M; ++r) {
+            int i = ibeg + r;
+            if (r == 0 || r == M - 1) {
+                for (int k = 0; k < 7; ++k)
+                    g[k] = upwind > 0 ? line[i + 1 - 4 + k] : line[i + 1 + 3 - k];
+                a[r] = 0.0;
+                b[r] = 1.0;
+                c[r] = 0.0;
+                d[r] = weno7_face_eps(g, 1.0e-40, 1);
+            } else {
+                double lo, bb, hi, dd;
+                if (upwind > 0) {
+                    for (int k = 0; k < 5; ++k) f[k] = line[i - 2 + k];
+                    hccs_row(f, &lo, &bb, &hi, &dd);
+                    a[r] = lo;
+                    c[r] = hi;
+                } else {
+                    for (int k = 0; k < 5; ++k) f[k] = line[i + 3 - k];
+                    hccs_row(f, &lo, &bb, &hi, &dd);
+                    c[r] = lo;
+                    a[r] = hi;
+                }
+                b[r] = bb;
+                d[r] = dd;
+            }
+        }
+        thomas_ref(M, a, b, c, d, x);
+        for (int r = 0; r < M; ++r) out[ibeg + 1 + r] = x[r];
         return;
     }
     if (scheme == OR_CRWENO5) {

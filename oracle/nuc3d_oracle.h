@@ -23,7 +23,7 @@ extern "C" {
 #endif
 
 /* scheme ids (fieldOperator.cpp:152-166 strings weno5js / weno5z / crweno5) */
-enum { OR_WENO5JS = 0, OR_WENO5Z = 1, OR_CRWENO5 = 2, OR_WENO7 = 3 };
+enum { OR_WENO5JS = 0, OR_WENO5Z = 1, OR_CRWENO5 = 2, OR_WENO7 = 3, OR_HCCS = 4 };
 /* viscosity models (physicsModel.cpp:44-49; power law is an extra model) */
 enum { OR_SUTHERLAND = 0, OR_CONSTANT = 1, OR_POWERLAW = 2 };
 
@@ -72,7 +72,8 @@ void or_ausm_split(const or_box *b, const double *const q[5], const double *cons
  * (interpolationInner + BoundaryL + BoundaryR): along the fastest axis of an
  * (nx,ny,nz) field with explicit halos of the scheme's buffer width (3 for
  * the 5-point schemes, 4 for OR_WENO7; fieldOperator.cpp:128-175), shaped
- * (width,ny,nz); out is (nx+1,ny,nz). */
+ * (width,ny,nz); out is (nx+1,ny,nz).  Widths: 3 for the 5-point schemes, 4
+ * for OR_WENO7 and OR_HCCS. */
 int or_reconstruct_field(int scheme, int upwind, unsigned quirks, int nx, int ny, int nz,
                          const double *in, const double *halo_l, const double *halo_r,
                          double *out);

@@ -5,7 +5,7 @@
 // product and never shipped.
 //
 // What each entry point drives (reference file:line):
-//   ref_reconstruct   weno5js / weno5z / crweno5 / weno7js ::interpolationInner +
+//   ref_reconstruct   weno5js / weno5z / crweno5 / weno7js / hccs ::interpolationInner +
 //                     interpolationBoundaryL/R          (weno5js.cpp:19-628,
 //                     weno5z.cpp:18-637, crweno5.cpp:25-837); output = n+1 faces
 //   ref_cd6           centraldifference6th::differentialInner/BoundaryL/R
@@ -46,6 +46,7 @@
 #include "euler3d.h"
 #include "fft.h"
 #include "fieldOperator.h"
+#include "hccs.hpp"
 #include "physicsModel.h"
 #include "weno5js.h"
 #include "weno5z.hpp"
@@ -124,12 +125,13 @@ struct RefSolver {
 
 extern "C" {
 
-// scheme: 0 = weno5js, 1 = weno5z, 2 = crweno5, 3 = weno7js.  in: (nx,ny,nz);
-// halos: (tile,ny,nz) with tile the scheme's bufferSize (3, or 4 for weno7js);
+// scheme: 0 = weno5js, 1 = weno5z, 2 = crweno5, 3 = weno7js, 4 = hccs.
+// in: (nx,ny,nz); halos: (tile,ny,nz) with tile the scheme's bufferSize (3,
+// or 4 for weno7js and hccs);
 // out: (nx+1,ny,nz).  Reconstruction runs along the fastest axis.
 int ref_reconstruct(int scheme, int upwind, int nx, int ny, int nz, const double *in,
                     const double *halo_l, const double *halo_r, double *out) {
-    const int tile = scheme == 3 ? 4 : 3;  // bufferSize (fieldOperator.cpp:131-175)
+    const int tile = scheme >= 3 ? 4 : 3;  // bufferSize (fieldOperator.cpp:131-175)
     Field fin(nx, ny, nz), fl(tile, ny, nz), fr(tile, ny, nz), fout(nx + 1, ny, nz);
     to_field(in, fin);
     to_field(halo_l, fl);
@@ -152,6 +154,11 @@ int ref_reconstruct(int scheme, int upwind, int nx, int ny, int nz, const double
         s.interpolationBoundaryR(fin, fr, upwind, fout, tile);
     } else if (scheme == 3) {
         nuc3d::weno7js s;
+        s.interpolationInner(fin, upwind, fout, tile);
+        s.interpolationBoundaryL(fin, fl, upwind, fout, tile);
+        s.interpolationBoundaryR(fin, fr, upwind, fout, tile);
+    } else if (scheme == 4) {
+        nuc3d::hccs s;
         s.interpolationInner(fin, upwind, fout, tile);
         s.interpolationBoundaryL(fin, fl, upwind, fout, tile);
         s.interpolationBoundaryR(fin, fr, upwind, fout, tile);

@@ -19,10 +19,10 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT / "oracle"))
 
-from oracle_ctypes import (AUSM, AUSMP, CRWENO5, WENO5JS, WENO5Z, WENO7, Box, Oracle,  # noqa: E402
-                           Reference)
+from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, WENO5JS, WENO5Z, WENO7, Box,  # noqa: E402
+                           Oracle, Reference)
 
-SCHEME_TAG = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr", WENO7: "w7"}
+SCHEME_TAG = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr", WENO7: "w7", HCCS: "hc"}
 
 
 def perturbed_tgv(box: Box, seed: int):
@@ -97,7 +97,42 @@ def main():
     ausm_fixtures(R)
     spectra_fixture(R)
     forcing_fixture(R)
+    hccs_fixtures(R)
     print("fixtures written to", HERE)
+
+
+def hccs_fixtures(R):
+    """The reference's hccs (hybrid compact scheme; its hccs.cpp compiled with
+    an injected declaration of the two names it uses before declaring them):
+    both directions on smooth lines (the linear compact rows) and rough ones
+    (the weighted rows), 4-wide halos; one RHS plus three steps, N-S and
+    Euler."""
+    rng = np.random.default_rng(44)
+    out = {}
+    shape = (5, 4, 20)
+    x = np.linspace(0.0, 2.0 * np.pi, shape[2], endpoint=False)
+    for up in (1, -1):
+        for kind in ("smooth", "rough"):
+            if kind == "smooth":
+                f = np.sin(x)[None, None, :] + 0.05 * rng.standard_normal(shape)
+            else:
+                f = rng.standard_normal(shape) * np.exp(rng.standard_normal(shape))
+            hl = rng.standard_normal(shape[:2] + (4,))
+            hr = rng.standard_normal(shape[:2] + (4,))
+            tag = f"hc_{kind}_{'p' if up > 0 else 'm'}"
+            out[f"rec_{tag}_in"], out[f"rec_{tag}_hl"], out[f"rec_{tag}_hr"] = f, hl, hr
+            out[f"rec_{tag}_out"] = R.reconstruct_field(HCCS, up, f, hl, hr)
+    np.savez_compressed(HERE / "operators_hc.npz", **out)
+    for ns in (True, False):
+        box = Box(16, 12, 10, scheme=(HCCS,) * 3, navier_stokes=ns, mach=0.3, reynolds=800.0,
+                  prandtl=0.71)
+        q = perturbed_tgv(box, 11 + HCCS)
+        rhs, dtl = R.rhs(box, q)
+        qn, dt, res = R.run_steps(box, 0.5, 3, q)
+        np.savez_compressed(HERE / f"step_hc_{'ns' if ns else 'eu'}.npz", q0=np.stack(q),
+                            rhs=np.stack(rhs), dt_local=np.array(dtl), q3=np.stack(qn), dt=dt,
+                            res=res, shape=np.array(box.shape), mach=box.mach,
+                            reynolds=box.reynolds, prandtl=box.prandtl)
 
 
 def forcing_fixture(R):

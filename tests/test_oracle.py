@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from helpers import box_from_golden, golden
-from oracle_ctypes import (AUSM, AUSMP, CRWENO5, LF, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_WENOZ_BETA2, WENO5JS,
+from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, LF, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_WENOZ_BETA2, WENO5JS,
                            WENO5Z, WENO7, Box, Oracle, Reference)
 
 TAGS = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr"}
@@ -229,3 +229,27 @@ def test_forcing_restatement_matches_reference_golden(tag):
         scale = np.abs(terms[e - 1]).max()
         assert scale > 0
         assert np.abs(d[e] - terms[e - 1]).max() <= 1e-12 * max(scale, np.abs(z[f"{tag}_rhs_off"][e]).max())
+
+
+@pytest.mark.parametrize("kind", ["smooth", "rough"])
+@pytest.mark.parametrize("up", [1, -1])
+def test_hccs_reconstruct_matches_reference_golden(O, kind, up):
+    """hccs: WENO7 end faces (eps 1e-40, literal squares), identity rows at
+    faces 4 and n-4, hybrid rows (linear upwind compact where theta > 1/2,
+    CRWENO5-weighted otherwise) solved by the reference's Thomas sweep."""
+    z = golden("operators_hc.npz")
+    tag = f"hc_{kind}_{'p' if up > 0 else 'm'}"
+    out = O.reconstruct_field(HCCS, up, QUIRKS_REFERENCE, z[f"rec_{tag}_in"], z[f"rec_{tag}_hl"],
+                              z[f"rec_{tag}_hr"])
+    assert np.array_equal(out, z[f"rec_{tag}_out"])
+
+
+@pytest.mark.parametrize("ns", [True, False])
+def test_hccs_rhs_and_steps_match_reference_golden(O, ns):
+    z = golden(f"step_hc_{'ns' if ns else 'eu'}.npz")
+    box = box_from_golden(z, HCCS, ns)
+    rhs, dtl = O.rhs(box, list(z["q0"]))
+    assert np.array_equal(np.stack(rhs), z["rhs"]) and dtl == float(z["dt_local"])
+    q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
+    assert np.array_equal(np.stack(q3), z["q3"])
+    assert np.array_equal(dt, z["dt"]) and np.array_equal(res, z["res"])
