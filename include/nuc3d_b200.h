@@ -35,12 +35,16 @@ extern "C" {
 #define NUC3D_ERR_CANCELLED (-7)   /* solve dropped by nuc3d_serve_destroy */
 
 /* Reconstruction schemes: the Method.in strings weno5js, weno5z, crweno5,
- * weno7js (fieldOperator.cpp:152-175).  weno7js reads 4 halo cells per side
- * (its bufferSize), the others 3. */
+ * weno7js, hccs (fieldOperator.cpp:128-175).  weno7js and hccs read 4 halo
+ * cells per side (their bufferSize), the others 3.  hccs is the hybrid
+ * compact scheme of hccs.cpp (WENO7 end faces, linear upwind compact rows
+ * blended with CRWENO5-weighted rows); its lines are bounded tridiagonal
+ * systems like crweno5's reference form. */
 #define NUC3D_WENO5JS 0
 #define NUC3D_WENO5Z 1
 #define NUC3D_CRWENO5 2
 #define NUC3D_WENO7JS 3
+#define NUC3D_HCCS 4
 
 /* PDEModel (block.cpp:146-157) */
 #define NUC3D_EULER3D 0
@@ -377,9 +381,9 @@ NUC3D_API double nuc3d_ctx_time(const nuc3d_ctx *ctx);
  * nuc3d_reconstruct = interpolationInner + interpolationBoundaryL +
  *   interpolationBoundaryR of weno5js (weno5js.cpp:19-628), weno5z
  *   (weno5z.cpp:18-637), crweno5 (crweno5.cpp:25-837) with tilesize 3, or
- *   weno7js (weno7js.cpp:17-824) with tilesize 4.
+ *   weno7js (weno7js.cpp:17-824) or hccs (hccs.cpp) with tilesize 4.
  *   Along the fastest axis of an (nx,ny,nz) field; halo_l/halo_r are (h,ny,nz)
- *   with h = 4 for weno7js and 3 otherwise (the received MPI buffers,
+ *   with h = 4 for weno7js and hccs and 3 otherwise (the received MPI buffers,
  *   bufferData.cpp:16-47); out is (nx+1,ny,nz),
  *   face m between cells m-1 and m.  upwind = +1 or -1.  crweno5 needs
  *   nx <= 4096.  quirks: NUC3D_QUIRK_WENOZ_BETA2 is honoured. */

@@ -1,5 +1,8 @@
-// CRWENO5 directional sweep, batched over boxes: one block per tile of
-// kCrTL lines of one box, one warp per (line, sign) tridiagonal system.
+// CRWENO5 and hccs directional sweeps, batched over boxes: one block per tile
+// of kCrTL lines of one box, one half-warp per (line, sign) tridiagonal
+// system.  hccs (hccs.cpp) has the same bounded structure with 4-cell ends:
+// faces 0..3 and n-3..n explicit WENO7 (eps 1e-40), identity rows at faces 4
+// and n-4, hybrid compact rows in between (hc_row).
 //
 // Reference system (crweno5.cpp:45-402, quirk bit QK_CRWENO_BOUNDED set): on
 // a line of n cells, faces 0..2 and n-2..n take explicit WENO5-JS values
@@ -99,34 +102,45 @@ __device__ __forceinline__ void pcr_update(B &a, B &c, B &d, B ma, B mc, B md, B
 
 }  // namespace
 
-int crweno_lanes(int n, bool bounded) {
-    const int N = bounded ? n - 5 : n;
+// unknowns of a line system: bounded lines solve faces H..n-H (the first and
+// last as identity rows), periodic ones faces 0..n-1
+static int line_unknowns(int sch, int n, bool bounded) {
+    const int H = scheme_halo(sch);
+    return bounded ? n - (2 * H - 1) : n;
+}
+
+int crweno_lanes(int sch, int n, bool bounded) {
+    const int N = line_unknowns(sch, n, bounded);
     int P = 1;
     while (P < kCrLanes && 2 * P <= N / 2) P *= 2;
     return P;
 }
 
-int crweno_segment_rows(int n, bool bounded) {
-    const int N = bounded ? n - 5 : n;
-    const int P = crweno_lanes(n, bounded);
+int crweno_segment_rows(int sch, int n, bool bounded) {
+    const int N = line_unknowns(sch, n, bounded);
+    const int P = crweno_lanes(sch, n, bounded);
     return (N + P - 1) / P;
 }
 
-size_t crweno_smem_bytes(int nmax, int ms, bool mixed) {
+size_t crweno_smem_bytes(int sch, int nmax, int ms, bool mixed) {
     const size_t bs = mixed ? sizeof(float) : sizeof(double);
-    return bs * ((size_t)2 * kCrTL * (nmax + 6) + (size_t)kCrWarps * 3 * ms * 32);
+    const int H = scheme_halo(sch);
+    return bs * ((size_t)2 * kCrTL * (nmax + 2 * H) + (size_t)kCrWarps * 3 * ms * 32);
 }
 
 int crweno_tile_lines() { return kCrTL; }
 
 // Work item (box, a, b, -): DIR 0: lines j = a*TL.., k = b; DIR 1: lines
 // i = a*TL.., k = b; DIR 2: lines i = a*TL.., j = b.
-template <typename B, int DIR>
+template <typename B, int DIR, int SCH>
 __global__ void __launch_bounds__(kCrThreads)
     k_crweno_lines(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items,
                    int in_slot, int accumulate, int nmax, int ms) {
+    // SCH: SCHEME_CR (crweno5) or SCHEME_HC (hccs).  H: staged halo, explicit
+    // faces per end and the first unknown face (3 for crweno5, 4 for hccs).
+    constexpr int H = scheme_halo(SCH);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int ls = nmax + 6;                           // staged cells per line
+    const int ls = nmax + 2 * H;                       // staged cells per line
     B *sF = reinterpret_cast<B *>(smem_raw);           // [sign][line][ls]
     B *sRow = sF + 2 * kCrTL * ls;                     // [warp][3][ms][32]
     __shared__ double sRef[2][kCrTL];
@@ -173,13 +187,15 @@ __global__ void __launch_bounds__(kCrThreads)
         }
     };
     const bool mixed = sizeof(B) == sizeof(float);
-    const bool bounded = (bp.quirks & QK_CRWENO_BOUNDED) != 0;
-    const int N = bounded ? n - 5 : n;  // unknowns of the system
+    // hccs lines are always bounded (the reference's form); crweno5 has the
+    // periodic form when the quirk bit is cleared
+    const bool bounded = SCH == SCHEME_HC || (bp.quirks & QK_CRWENO_BOUNDED) != 0;
+    const int N = bounded ? n - (2 * H - 1) : n;  // unknowns of the system
     int P = 1;  // lanes per system
     while (P < kCrLanes && 2 * P <= N / 2) P *= 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int sg = lane >> 4, hl = lane & 15;  // sign (0: +, 1: -) and lane within the system
-    B *const myF = sF + (sg * kCrTL + warp) * ls;  // cell c at [c + 3]; later face m at [m]
+    B *const myF = sF + (sg * kCrTL + warp) * ls;  // cell c at [c + H]; later face m at [m]
     B *const wA = sRow + (size_t)warp * 3 * ms * 32;  // [j][lane]
     B *const wC = wA + ms * 32;
     B *const wD = wC + ms * 32;
@@ -195,8 +211,8 @@ __global__ void __launch_bounds__(kCrThreads)
             }
             __syncthreads();
         }
-        // stage F+ / F- of cells -3 .. n+2
-        const int nst = n + 6;
+        // stage F+ / F- of cells -H .. n+H-1
+        const int nst = n + 2 * H;
         for (int t = threadIdx.x; t < kCrTL * nst; t += kCrThreads) {
             int l, pc;
             if (DIR == 0) {
@@ -208,7 +224,7 @@ __global__ void __launch_bounds__(kCrThreads)
             }
             double fp = 0.0, fm = 0.0;
             if (l0 + l < nl) {
-                int pos = pc - 3;
+                int pos = pc - H;
                 pos = pos < 0 ? pos + n : (pos >= n ? pos - n : pos);
                 split(e, gidx(l, pos), fp, fm);
                 if (mixed) {
@@ -222,21 +238,28 @@ __global__ void __launch_bounds__(kCrThreads)
         __syncthreads();
 
         if (l0 + warp < nl) {  // warp-uniform
-            auto F = [&](int c) -> B { return myF[c + 3]; };
+            auto F = [&](int c) -> B { return myF[c + H]; };
             // the two half-warps run the same instructions: the sign only
             // selects which cells feed a stencil ('+' reads upwind from the
             // left, '-' from the right)
             const int dir = sg == 0 ? 1 : -1;
+            // explicit face m: WENO5-JS (crweno5.cpp:425-837) or hccs's WENO7
+            // (hccs.cpp:538-980)
             auto js = [&](int m) -> B {
+                if (SCH == SCHEME_HC) {
+                    const int c0 = sg == 0 ? m - 4 : m + 3;
+                    return weno7_face_hc(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
+                                         F(c0 + 4 * dir), F(c0 + 5 * dir), F(c0 + 6 * dir));
+                }
                 const int c0 = sg == 0 ? m - 3 : m + 2;
                 return weno5js_face(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
                                     F(c0 + 4 * dir));
             };
-            // explicit faces of the bounded system: 0, 1, 2, n-2, n-1, n
+            // explicit faces of the bounded system: 0..H-1 and n-H+1..n
             int xm = -1;
             B xv = B(0);
-            if (bounded && hl < 6) {
-                xm = hl < 3 ? hl : n - 5 + hl;
+            if (bounded && hl < 2 * H) {
+                xm = hl < H ? hl : n - 2 * H + 1 + hl;
                 xv = js(xm);
             }
             // segment of this lane: rows r0 .. r1 (at least 2)
@@ -248,7 +271,7 @@ __global__ void __launch_bounds__(kCrThreads)
             B la = B(0), lc = B(0), ld = B(0);  // reduced unit-diagonal row of x_last
             if (act) {
                 // window w[k] = F(i - 2 + k) of the current row's cell i (face i + 1)
-                int i = bounded ? r0 + 2 : r0 - 1;
+                int i = bounded ? r0 + H - 1 : r0 - 1;
                 B w[6];
 #pragma unroll
                 for (int k = 0; k < 6; ++k) w[k] = F(i - 2 + k);
@@ -257,14 +280,18 @@ __global__ void __launch_bounds__(kCrThreads)
                         a = B(0);
                         b = B(1);
                         c = B(0);
-                        d = js(r + 3);
+                        d = js(r + H);
                     } else {
                         // '+': cells i-2..i+2 = w[0..4]; '-': cells i+3..i-1 = w[5..1]
                         // with the off-diagonals swapped (crweno5.cpp:335-338)
                         const bool m = sg != 0;
                         B lo, hi;
-                        cr_row(m ? w[5] : w[0], m ? w[4] : w[1], m ? w[3] : w[2],
-                               m ? w[2] : w[3], m ? w[1] : w[4], lo, b, hi, d);
+                        if (SCH == SCHEME_HC)
+                            hc_row(m ? w[5] : w[0], m ? w[4] : w[1], m ? w[3] : w[2],
+                                   m ? w[2] : w[3], m ? w[1] : w[4], lo, b, hi, d);
+                        else
+                            cr_row(m ? w[5] : w[0], m ? w[4] : w[1], m ? w[3] : w[2],
+                                   m ? w[2] : w[3], m ? w[1] : w[4], lo, b, hi, d);
                         a = m ? hi : lo;
                         c = m ? lo : hi;
                     }
@@ -376,7 +403,7 @@ __global__ void __launch_bounds__(kCrThreads)
             const B xf = fd * rcp_(B(1) + fa + fc), xl = ld * rcp_(B(1) + la + lc);
             __syncwarp();  // every lane has read its staged fluxes
             if (act) {
-                const int off = bounded ? 3 : 0;
+                const int off = bounded ? H : 0;
                 myF[r0 + off] = xf;
                 myF[r1 + off] = xl;
                 for (int j = 1; j < L - 1; ++j)
@@ -407,42 +434,56 @@ __global__ void __launch_bounds__(kCrThreads)
     }
 }
 
-cudaError_t prepare_crweno_kernels(bool mixed) {
-    const int max_smem = 200 * 1024;  // above the largest need (164 KB at 512 cells, FP64)
-    cudaError_t e;
-    if (mixed) {
-        e = cudaFuncSetAttribute(k_crweno_lines<float, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_crweno_lines<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_crweno_lines<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-    } else {
-        e = cudaFuncSetAttribute(k_crweno_lines<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_crweno_lines<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_crweno_lines<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-    }
+template <typename B, int SCH>
+static cudaError_t prepare_t() {
+    const int max_smem = 200 * 1024;  // above the largest need (166 KB at 512 cells, FP64)
+    cudaError_t e = cudaFuncSetAttribute(k_crweno_lines<B, 0, SCH>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_crweno_lines<B, 1, SCH>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_crweno_lines<B, 2, SCH>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
     return e;
 }
 
-template <typename B>
-cudaError_t launch_crweno(int dir, const BoxDev *boxes, const WorkItem *items, int nitems,
-                          int in_slot, int accumulate, int nmax, int ms, cudaStream_t st) {
-    if (nitems <= 0) return cudaSuccess;
-    const size_t smem = crweno_smem_bytes(nmax, ms, sizeof(B) == sizeof(float));
+cudaError_t prepare_crweno_kernels(bool mixed) {
+    cudaError_t e = mixed ? prepare_t<float, SCHEME_CR>() : prepare_t<double, SCHEME_CR>();
+    if (e == cudaSuccess) e = mixed ? prepare_t<float, SCHEME_HC>() : prepare_t<double, SCHEME_HC>();
+    return e;
+}
+
+template <typename B, int SCH>
+static void launch_t(int dir, const BoxDev *boxes, const WorkItem *items, int nitems, int in_slot,
+                     int accumulate, int nmax, int ms, size_t smem, cudaStream_t st) {
     if (dir == 0)
-        k_crweno_lines<B, 0><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot, accumulate, nmax, ms);
+        k_crweno_lines<B, 0, SCH><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot,
+                                                                    accumulate, nmax, ms);
     else if (dir == 1)
-        k_crweno_lines<B, 1><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot, accumulate, nmax, ms);
+        k_crweno_lines<B, 1, SCH><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot,
+                                                                    accumulate, nmax, ms);
     else
-        k_crweno_lines<B, 2><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot, accumulate, nmax, ms);
+        k_crweno_lines<B, 2, SCH><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot,
+                                                                    accumulate, nmax, ms);
+}
+
+template <typename B>
+cudaError_t launch_crweno(int sch, int dir, const BoxDev *boxes, const WorkItem *items,
+                          int nitems, int in_slot, int accumulate, int nmax, int ms,
+                          cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
+    const size_t smem = crweno_smem_bytes(sch, nmax, ms, sizeof(B) == sizeof(float));
+    if (sch == SCHEME_HC)
+        launch_t<B, SCHEME_HC>(dir, boxes, items, nitems, in_slot, accumulate, nmax, ms, smem, st);
+    else
+        launch_t<B, SCHEME_CR>(dir, boxes, items, nitems, in_slot, accumulate, nmax, ms, smem, st);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_crweno<double>(int, const BoxDev *, const WorkItem *, int, int, int,
-                                           int, int, cudaStream_t);
-template cudaError_t launch_crweno<float>(int, const BoxDev *, const WorkItem *, int, int, int,
-                                          int, int, cudaStream_t);
+template cudaError_t launch_crweno<double>(int, int, const BoxDev *, const WorkItem *, int, int,
+                                           int, int, int, cudaStream_t);
+template cudaError_t launch_crweno<float>(int, int, const BoxDev *, const WorkItem *, int, int,
+                                          int, int, int, cudaStream_t);
 
 }  // namespace nuc3d

@@ -70,12 +70,15 @@ int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
     const int n[3] = {d.nx, d.ny, d.nz};
     for (int i = 0; i < 3; ++i) {
         if (n[i] < 8) return bad(NUC3D_ERR_INVALID, "every box extent must be >= 8 cells");
-        if (d.scheme[i] < NUC3D_WENO5JS || d.scheme[i] > NUC3D_WENO7JS)
+        if (d.scheme[i] < NUC3D_WENO5JS || d.scheme[i] > NUC3D_HCCS)
             return bad(NUC3D_ERR_UNSUPPORTED, "unknown reconstruction scheme");
     }
     for (int i = 0; i < 3; ++i)
-        if (d.scheme[i] == NUC3D_CRWENO5 && n[i] > kCrMaxCells)
-            return bad(NUC3D_ERR_UNSUPPORTED, "CRWENO5 lines are limited to 512 cells");
+        if ((d.scheme[i] == NUC3D_CRWENO5 || d.scheme[i] == NUC3D_HCCS) && n[i] > kCrMaxCells)
+            return bad(NUC3D_ERR_UNSUPPORTED, "CRWENO5 / hccs lines are limited to 512 cells");
+    for (int i = 0; i < 3; ++i)
+        if (d.scheme[i] == NUC3D_HCCS && n[i] < 12)
+            return bad(NUC3D_ERR_INVALID, "hccs lines need at least 12 cells");
     if ((long long)d.nx * d.ny * d.nz > (1LL << 31)) return bad(NUC3D_ERR_INVALID, "box larger than 2^31 cells");
     if (!(d.lx > 0 && d.ly > 0 && d.lz > 0)) return bad(NUC3D_ERR_INVALID, "box lengths must be > 0");
     if (d.pde_model != NUC3D_EULER3D && d.pde_model != NUC3D_NAVIERSTOKES3D)
@@ -258,9 +261,10 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));
     const bool mixed = precision_ == NUC3D_MIXED;
     std::vector<BoxDev> table(boxes_.size());
-    std::vector<WorkItem> prim, st25, inv[kSchemes][3], cr[3];
+    std::vector<WorkItem> prim, st25, inv[kSchemes][3], cr[2][3];
     const int crtl = crweno_tile_lines();
-    for (int d = 0; d < 3; ++d) cr_nmax_[d] = cr_ms_[d] = 0;
+    for (int c = 0; c < 2; ++c)
+        for (int d = 0; d < 3; ++d) cr_nmax_[c][d] = cr_ms_[c][d] = 0;
     any_visc_ = false;
     nactive_ = 0;
     for (size_t i = 0; i < boxes_.size(); ++i) {
@@ -281,11 +285,12 @@ int Engine::rebuild() {
                 for (int x = 0; x < ceil_div(p.n[0], kT25X); ++x) st25.push_back({id, x, y, z});
         for (int d = 0; d < 3; ++d) {
             int s = p.scheme[d];
-            if (s == SCHEME_CR) {
-                const bool bounded = (p.quirks & QK_CRWENO_BOUNDED) != 0;
-                cr_nmax_[d] = std::max(cr_nmax_[d], p.n[d]);
-                cr_ms_[d] = std::max(cr_ms_[d], crweno_segment_rows(p.n[d], bounded));
-                auto &L = cr[d];
+            if (s == SCHEME_CR || s == SCHEME_HC) {
+                const int c = s == SCHEME_HC ? 1 : 0;
+                const bool bounded = s == SCHEME_HC || (p.quirks & QK_CRWENO_BOUNDED) != 0;
+                cr_nmax_[c][d] = std::max(cr_nmax_[c][d], p.n[d]);
+                cr_ms_[c][d] = std::max(cr_ms_[c][d], crweno_segment_rows(s, p.n[d], bounded));
+                auto &L = cr[c][d];
                 if (d == 0) {
                     for (int k = 0; k < p.n[2]; ++k)
                         for (int g = 0; g < ceil_div(p.n[1], crtl); ++g) L.push_back({id, g, k, 0});
@@ -325,7 +330,8 @@ int Engine::rebuild() {
     append(st25, r_25d_);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) append(inv[s][d], r_inv_[s][d]);
-    for (int d = 0; d < 3; ++d) append(cr[d], r_cr_[d]);
+    for (int c = 0; c < 2; ++c)
+        for (int d = 0; d < 3; ++d) append(cr[c][d], r_cr_[c][d]);
     if ((int)boxes_.size() > d_boxes_cap_) {
         if (d_boxes_) ECK(cudaFreeAsync(d_boxes_, stream_));
         if (d_rhs_ptrs_) ECK(cudaFreeAsync(d_rhs_ptrs_, stream_));
@@ -350,7 +356,8 @@ int Engine::rebuild() {
     int per_stage = (r_prim_.n > 0) + (any_visc_ && r_25d_.n > 0) + (r_25d_.n > 0);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d].n > 0;
-    for (int d = 0; d < 3; ++d) per_stage += r_cr_[d].n > 0;
+    for (int c = 0; c < 2; ++c)
+        for (int d = 0; d < 3; ++d) per_stage += r_cr_[c][d].n > 0;
     launches_per_step_ = 3 * per_stage + 3;  // + clear_eig, dt, residual
     for (const EngineBox &b : boxes_)
         if (b.live && b.dev.active && b.force_mem) launches_per_step_ += 3 * 8;  // forcing passes
@@ -424,8 +431,10 @@ int Engine::enqueue_step_t(cudaStream_t st) {
             for (int s = 0; s < kSchemes; ++s)
                 ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
                                         r_inv_[s][d].n, in, d > 0, st)));
-            ECK((launch_crweno<B>(d, d_boxes_, it + r_cr_[d].off, r_cr_[d].n, in, d > 0,
-                                  cr_nmax_[d], cr_ms_[d], st)));
+            for (int c = 0; c < 2; ++c)
+                ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_,
+                                      it + r_cr_[c][d].off, r_cr_[c][d].n, in, d > 0,
+                                      cr_nmax_[c][d], cr_ms_[c][d], st)));
         }
         ECK(enqueue_forcing<B>(st));
         {
@@ -603,8 +612,10 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
         for (int s = 0; s < kSchemes; ++s)
             ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
                                     r_inv_[s][d].n, 0, d > 0, stream_)));
-        ECK((launch_crweno<B>(d, d_boxes_, it + r_cr_[d].off, r_cr_[d].n, 0, d > 0, cr_nmax_[d],
-                              cr_ms_[d], stream_)));
+        for (int c = 0; c < 2; ++c)
+            ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_, it + r_cr_[c][d].off,
+                                  r_cr_[c][d].n, 0, d > 0, cr_nmax_[c][d], cr_ms_[c][d],
+                                  stream_)));
     }
     ECK(enqueue_forcing<B>(stream_));
     StageArgs sa{-1, 0, 0, d_rhs_ptrs_};

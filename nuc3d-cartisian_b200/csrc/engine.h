@@ -105,8 +105,10 @@ private:
         int n = 0;
     };
     Range r_prim_, r_25d_, r_inv_[kSchemes][3];  // [scheme JS/Z/-/W7][dir]
-    Range r_cr_[3];                       // CRWENO5 line tiles per dir
-    int cr_nmax_[3] = {0, 0, 0}, cr_ms_[3] = {0, 0, 0};
+    // line-solve tiles per [scheme: 0 crweno5, 1 hccs][dir], with the longest
+    // line and the rows per lane that size each launch's shared memory
+    Range r_cr_[2][3];
+    int cr_nmax_[2][3] = {}, cr_ms_[2][3] = {};
     int launches_per_step_ = 0;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;

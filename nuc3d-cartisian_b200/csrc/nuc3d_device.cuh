@@ -18,11 +18,14 @@ enum : unsigned {
     QK_CRWENO_BOUNDED = 0x10u,
 };
 
-enum : int { SCHEME_JS = 0, SCHEME_Z = 1, SCHEME_CR = 2, SCHEME_W7 = 3 };
+enum : int { SCHEME_JS = 0, SCHEME_Z = 1, SCHEME_CR = 2, SCHEME_W7 = 3, SCHEME_HC = 4 };
 
 // reconstruction stencil half-width (the reference's bufferSize,
-// fieldOperator.cpp:128-175): 4 cells for weno7js, 3 for the WENO5 family
-__host__ __device__ constexpr int scheme_halo(int scheme) { return scheme == SCHEME_W7 ? 4 : 3; }
+// fieldOperator.cpp:128-175): 4 cells for weno7js and hccs, 3 for the WENO5
+// family
+__host__ __device__ constexpr int scheme_halo(int scheme) {
+    return (scheme == SCHEME_W7 || scheme == SCHEME_HC) ? 4 : 3;
+}
 enum : int { VISC_SUTHERLAND = 0, VISC_CONSTANT = 1, VISC_POWERLAW = 2 };
 enum : int { RIEMANN_LF = 0, RIEMANN_AUSM = 1, RIEMANN_AUSMP = 2 };
 
@@ -379,6 +382,28 @@ __device__ __forceinline__ double weno7_face(double f0, double f1, double f2, do
     return weno7_combine(is, q);
 }
 
+// hccs's WENO7 faces (hccs.cpp:538-980 and its identity rows): the same
+// face with hccs's own eps = 1e-40.  FP64 forms the weights through
+// reciprocals (alpha_k = c_k (1 + (tau r_k)^2), r_k = 1/(eps + beta_k)): with
+// eps = 1e-40 the one-reciprocal product form would multiply four factors
+// as small as 1e-80 and underflow.
+__device__ __forceinline__ double weno7_face_hc(double f0, double f1, double f2, double f3,
+                                                double f4, double f5, double f6) {
+    double is[4], q[4];
+    weno7_parts(f0, f1, f2, f3, f4, f5, f6, is, q);
+    const double ss = 1.0e-40;
+    const double tau = fabs(sub_(is[0], is[3]));
+    const double c[4] = {K7::C0, K7::C1, K7::C2, K7::C3};
+    double a[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double r = mul_(tau, __drcp_rn(add_(ss, is[k])));
+        a[k] = mul_(c[k], fma_(r, r, 1.0));
+    }
+    const double num = fma_(a[3], q[3], fma_(a[2], q[2], fma_(a[1], q[1], mul_(a[0], q[0]))));
+    return mul_(num, __drcp_rn(add_(add_(add_(a[0], a[1]), a[2]), a[3])));
+}
+
 // FP32 (mixed path): the same indicators and candidates rewritten exactly in
 // first and second differences, which removes the cancellation instead of
 // ordering it.  With delta_j = f_j - f_{j-1} and sigma_j = delta_j -
@@ -395,8 +420,20 @@ __device__ __forceinline__ float w7_beta(float u, float a, float b, float p, flo
     float ta = fma_(t, b, mul_(s, a));
     return fma_(u, tu, fma_(a, ta, mul_(mul_(v, b), b)));
 }
+__device__ __forceinline__ float weno7_face_eps(float f0, float f1, float f2, float f3, float f4,
+                                                float f5, float f6, float ss);
 __device__ __forceinline__ float weno7_face(float f0, float f1, float f2, float f3, float f4,
                                             float f5, float f6) {
+    return weno7_face_eps(f0, f1, f2, f3, f4, f5, f6, 1.0e-20f);
+}
+// hccs's faces in FP32: 1e-40 is below FP32's normal range, 1e-30 stands in
+// (it only matters where a sub-stencil is exactly constant)
+__device__ __forceinline__ float weno7_face_hc(float f0, float f1, float f2, float f3, float f4,
+                                               float f5, float f6) {
+    return weno7_face_eps(f0, f1, f2, f3, f4, f5, f6, 1.0e-30f);
+}
+__device__ __forceinline__ float weno7_face_eps(float f0, float f1, float f2, float f3, float f4,
+                                                float f5, float f6, float ss) {
     float d1 = sub_(f1, f0), d2 = sub_(f2, f1), d3 = sub_(f3, f2);
     float d4 = sub_(f4, f3), d5 = sub_(f5, f4), d6 = sub_(f6, f5);
     float s2 = sub_(d2, d1), s3 = sub_(d3, d2), s4 = sub_(d4, d3), s5 = sub_(d5, d4),
@@ -411,7 +448,7 @@ __device__ __forceinline__ float weno7_face(float f0, float f1, float f2, float 
     r[1] = fma_(-1.0f, d2, fma_(4.0f, d3, mul_(3.0f, d4)));
     r[2] = fma_(-1.0f, d5, fma_(6.0f, d4, d3));
     r[3] = fma_(9.0f, d4, fma_(-4.0f, d5, d6));
-    const float ss = 1.0e-20f, cap = 1.0e18f;
+    const float cap = 1.0e18f;
     const float c[4] = {float(K7::C0), float(K7::C1), float(K7::C2), float(K7::C3)};
     float tau = fabsf(sub_(is[0], is[3]));
     float al[4];
@@ -423,6 +460,88 @@ __device__ __forceinline__ float weno7_face(float f0, float f1, float f2, float 
     float num = fma_(al[3], r[3], fma_(al[2], r[2], fma_(al[1], r[1], mul_(al[0], r[0]))));
     float den = add_(add_(add_(al[0], al[1]), al[2]), al[3]);
     return fma_(mul_(num, frcp_fast(den)), 1.0f / 12.0f, f3);
+}
+
+// One hybrid row of hccs (hccs.cpp:138-185; '-' mirrored, :375-420), scaled
+// by a positive factor.  WENO5-Z-type weights over the CRWENO5 linear
+// weights, alpha_k = c_k (1 + (tau/(beta_k + eps))^2), eps = 1e-40; with
+// x = sum alpha - 1 the blend is theta = 1/(1 + x^2).  theta > 1/2 (taken, as
+// the reference, as 1 + x^2 < 2) gives the linear upwind compact row
+// (2/7, 4/7, 1/7 | q7); otherwise the reference row
+//   (CRWENO5 row in omega) (1 - theta)/theta + (2/7, 4/7, 1/7 | q7)
+// is used multiplied by sum(alpha)/x^2, i.e. (CRWENO5 row in alpha) +
+// (2/7, 4/7, 1/7 | q7) sum(alpha)/x^2 (the two factors are equal in exact
+// arithmetic; this form stays finite for any x).
+//   FP64: the alphas multiplied through by P = s0 s1 s2, s_k = (beta_k +
+//   eps)^2 (at least 1e-80 each, so P does not underflow), x = (sum A - P)/P.
+//   FP32: reciprocal form with eps 1e-30 and tau/(beta + eps) capped.
+__device__ __forceinline__ void hc_row(double f0, double f1, double f2, double f3, double f4,
+                                       double &lo, double &b, double &hi, double &d) {
+    double is0, is1, is2;
+    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
+    const double q7 = mul_(fma_(4.0, f4, fma_(159.0, f3, fma_(239.0, f2, fma_(19.0, f1, -f0)))),
+                           1.0 / 420.0);
+    const double ss = 1.0e-40;
+    const double tau = fabs(sub_(is2, is0));
+    const double t2 = mul_(tau, tau);
+    double s0 = add_(is0, ss), s1 = add_(is1, ss), s2 = add_(is2, ss);
+    s0 = mul_(s0, s0);
+    s1 = mul_(s1, s1);
+    s2 = mul_(s2, s2);
+    const double P = mul_(mul_(s0, s1), s2);
+    const double A0 = mul_(mul_(K::CR0, add_(s0, t2)), mul_(s1, s2));
+    const double A1 = mul_(mul_(K::CR1, add_(s1, t2)), mul_(s0, s2));
+    const double A2 = mul_(mul_(K::CR2, add_(s2, t2)), mul_(s0, s1));
+    const double SA = add_(add_(A0, A1), A2);
+    const double x = mul_(sub_(SA, P), __drcp_rn(P));  // sum(alpha) - 1
+    if (add_(1.0, mul_(x, x)) < 2.0) {
+        lo = 2.0 / 7.0;
+        b = 4.0 / 7.0;
+        hi = 1.0 / 7.0;
+        d = q7;
+        return;
+    }
+    const double ix = mul_(P, __drcp_rn(sub_(SA, P)));  // 1/x
+    const double u = mul_(mul_(SA, ix), ix);            // P sum(alpha) / x^2
+    const double third = 1.0 / 3.0, two3 = 2.0 / 3.0, sixth = 1.0 / 6.0;
+    lo = fma_(2.0 / 7.0, u, fma_(two3, A0, mul_(third, A1)));
+    b = fma_(4.0 / 7.0, u, fma_(third, A0, mul_(two3, add_(A1, A2))));
+    hi = fma_(1.0 / 7.0, u, mul_(third, A2));
+    d = fma_(q7, u, fma_(mul_(sixth, add_(A1, mul_(5.0, A2))), f3,
+                         fma_(mul_(sixth, add_(mul_(5.0, add_(A0, A1)), A2)), f2,
+                              mul_(mul_(sixth, A0), f1))));
+}
+__device__ __forceinline__ void hc_row(float f0, float f1, float f2, float f3, float f4, float &lo,
+                                       float &b, float &hi, float &d) {
+    float is0, is1, is2;
+    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
+    const float q7 = mul_(fma_(4.0f, f4, fma_(159.0f, f3, fma_(239.0f, f2, fma_(19.0f, f1, -f0)))),
+                          float(1.0 / 420.0));
+    const float ss = 1.0e-30f, cap = 1.0e18f;
+    const float tau = fabsf(sub_(is2, is0));
+    const float r0 = fminf(mul_(tau, frcp_fast(add_(is0, ss))), cap);
+    const float r1 = fminf(mul_(tau, frcp_fast(add_(is1, ss))), cap);
+    const float r2 = fminf(mul_(tau, frcp_fast(add_(is2, ss))), cap);
+    const float A0 = mul_(float(K::CR0), fma_(r0, r0, 1.0f));
+    const float A1 = mul_(float(K::CR1), fma_(r1, r1, 1.0f));
+    const float A2 = mul_(float(K::CR2), fma_(r2, r2, 1.0f));
+    const float SA = add_(add_(A0, A1), A2);
+    const float x = sub_(SA, 1.0f);
+    if (add_(1.0f, mul_(x, x)) < 2.0f) {
+        lo = 2.0f / 7.0f;
+        b = 4.0f / 7.0f;
+        hi = 1.0f / 7.0f;
+        d = q7;
+        return;
+    }
+    const float u = mul_(SA, frcp_fast(mul_(x, x)));  // sum(alpha) / x^2 (0 if x^2 overflows)
+    const float third = 1.0f / 3.0f, two3 = 2.0f / 3.0f, sixth = 1.0f / 6.0f;
+    lo = fma_(2.0f / 7.0f, u, fma_(two3, A0, mul_(third, A1)));
+    b = fma_(4.0f / 7.0f, u, fma_(third, A0, mul_(two3, add_(A1, A2))));
+    hi = fma_(1.0f / 7.0f, u, mul_(third, A2));
+    d = fma_(q7, u, fma_(mul_(sixth, add_(A1, mul_(5.0f, A2))), f3,
+                         fma_(mul_(sixth, add_(mul_(5.0f, add_(A0, A1)), A2)), f2,
+                              mul_(mul_(sixth, A0), f1))));
 }
 
 // CD6 first derivative (centraldifference6th.cpp:44-46), times 1/dx.

@@ -123,6 +123,56 @@ __global__ void k_op_crweno(int upwind, int nx, long long lines, const double *i
     }
 }
 
+// One thread per line: hccs (hccs.cpp): faces 0..3 and nx-3..nx explicit
+// WENO7 with hccs's eps (:538-980), the system of faces 4..nx-4 (identity
+// rows at its ends, hybrid rows between, :54-245 / :272-471) by a Thomas
+// sweep.  scratch holds 2*nx values per line.
+__global__ void k_op_hccs(int upwind, int nx, long long lines, const double *in,
+                          const double *hl, const double *hr, double *out, double *scratch) {
+    long long line = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (line >= lines) return;
+    auto F = [&](int c) { return line_at<4>(in, hl, hr, nx, line, c); };
+    auto w7 = [&](int m) {
+        if (upwind > 0)
+            return weno7_face_hc(F(m - 4), F(m - 3), F(m - 2), F(m - 1), F(m), F(m + 1), F(m + 2));
+        return weno7_face_hc(F(m + 3), F(m + 2), F(m + 1), F(m), F(m - 1), F(m - 2), F(m - 3));
+    };
+    double *o = out + (long long)(nx + 1) * line;
+    for (int m = 0; m <= 3; ++m) o[m] = w7(m);
+    for (int m = nx - 3; m <= nx; ++m) o[m] = w7(m);
+    const int M = nx - 7;
+    double *cs = scratch + 2 * (long long)nx * line;
+    double *ds = cs + nx;
+    double cp = 0.0, dp = w7(4);
+    cs[0] = cp;
+    ds[0] = dp;
+    for (int r = 1; r < M; ++r) {
+        double a, b, c, d;
+        if (r == M - 1) {
+            a = 0.0; b = 1.0; c = 0.0; d = w7(r + 4);
+        } else {
+            const int i = r + 3;
+            double lo, hi;
+            if (upwind > 0)
+                hc_row(F(i - 2), F(i - 1), F(i), F(i + 1), F(i + 2), lo, b, hi, d);
+            else
+                hc_row(F(i + 3), F(i + 2), F(i + 1), F(i), F(i - 1), lo, b, hi, d);
+            if (upwind > 0) { a = lo; c = hi; } else { c = lo; a = hi; }
+        }
+        double den = b - cp * a;
+        cp = c / den;
+        dp = (d - dp * a) / den;
+        cs[r] = cp;
+        ds[r] = dp;
+    }
+    double x = ds[M - 1];
+    o[nx - 4] = x;
+    for (int r = M - 2; r >= 0; --r) {
+        x = ds[r] - cs[r] * x;
+        o[r + 4] = x;
+    }
+}
+
 // centraldifference6th.cpp:16-186: one thread per cell.
 __global__ void k_op_cd6(int nx, long long lines, double inv_dx, const double *in,
                          const double *hl, const double *hr, double *out) {
@@ -155,13 +205,16 @@ __global__ void k_op_rk3(int stage, long long n, double dt, RK5 rk) {
 cudaError_t op_reconstruct(int scheme, int upwind, unsigned quirks, int nx, long long lines,
                            const double *in, const double *hl, const double *hr, double *out,
                            cudaStream_t st) {
-    if (scheme == SCHEME_CR) {
+    if (scheme == SCHEME_CR || scheme == SCHEME_HC) {
         double *scratch = nullptr;
         size_t bytes = sizeof(double) * 2 * (size_t)nx * (size_t)lines;
         cudaError_t e = cudaMallocAsync(&scratch, bytes, st);
         if (e != cudaSuccess) return e;
         unsigned grid = (unsigned)((lines + 127) / 128);
-        k_op_crweno<<<grid, 128, 0, st>>>(upwind, nx, lines, in, hl, hr, out, scratch);
+        if (scheme == SCHEME_HC)
+            k_op_hccs<<<grid, 128, 0, st>>>(upwind, nx, lines, in, hl, hr, out, scratch);
+        else
+            k_op_crweno<<<grid, 128, 0, st>>>(upwind, nx, lines, in, hl, hr, out, scratch);
         e = cudaGetLastError();
         cudaError_t f = cudaFreeAsync(scratch, st);
         return e != cudaSuccess ? e : f;

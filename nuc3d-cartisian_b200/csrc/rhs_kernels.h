@@ -114,18 +114,20 @@ template <typename B>
 cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems, StageArgs sa,
                           bool any_viscous, cudaStream_t st);
 
-// CRWENO5 sweep (crweno_kernels.cu), batched: one work item per tile of
+// CRWENO5 / hccs sweeps (crweno_kernels.cu), batched: one work item per tile of
 // crweno_tile_lines() lines of one box.  nmax is the longest line among the
 // launch's boxes and ms = crweno_segment_rows of it (rows per lane of the
 // partitioned line solve); they size the dynamic shared memory.
+// sch: SCHEME_CR (crweno5) or SCHEME_HC (hccs, always the bounded system).
 cudaError_t prepare_crweno_kernels(bool mixed);
 int crweno_tile_lines();
-int crweno_lanes(int n, bool bounded);
-int crweno_segment_rows(int n, bool bounded);
-size_t crweno_smem_bytes(int nmax, int ms, bool mixed);
-constexpr int kCrMaxCells = 512;  // longest CRWENO5 line (shared-memory bound)
+int crweno_lanes(int sch, int n, bool bounded);
+int crweno_segment_rows(int sch, int n, bool bounded);
+size_t crweno_smem_bytes(int sch, int nmax, int ms, bool mixed);
+constexpr int kCrMaxCells = 512;  // longest CRWENO5 / hccs line (shared-memory bound)
 template <typename B>
-cudaError_t launch_crweno(int dir, const BoxDev *boxes, const WorkItem *items, int nitems,
-                          int in_slot, int accumulate, int nmax, int ms, cudaStream_t st);
+cudaError_t launch_crweno(int sch, int dir, const BoxDev *boxes, const WorkItem *items,
+                          int nitems, int in_slot, int accumulate, int nmax, int ms,
+                          cudaStream_t st);
 
 }  // namespace nuc3d

@@ -68,10 +68,11 @@ int scheme_id(const std::string &s) {
     if (s == "weno5z") return NUC3D_WENO5Z;
     if (s == "crweno5") return NUC3D_CRWENO5;
     if (s == "weno7js") return NUC3D_WENO7JS;
-    for (const char *other : {"hccs", "hccs77", "hccs78", "weno3js", "upwind1st"})
+    if (s == "hccs") return NUC3D_HCCS;
+    for (const char *other : {"hccs77", "hccs78", "weno3js", "upwind1st"})
         if (s == other)
             die("reconstruction scheme '" + s +
-                "' is not on the B200 path (weno5js, weno5z, crweno5, weno7js)");
+                "' is not on the B200 path (weno5js, weno5z, crweno5, weno7js, hccs)");
     return NUC3D_WENO5JS;
 }
 

@@ -21,8 +21,9 @@ OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2
 ERR_TIMEOUT, ERR_CANCELLED = -6, -7
 INIT_STATE, INIT_TGV, INIT_HIT = 0, 1, 2
 FORCING_NONE, FORCING_CONST = 0, 1
-WENO5JS, WENO5Z, CRWENO5, WENO7JS = 0, 1, 2, 3
-SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5, "weno7js": WENO7JS}
+WENO5JS, WENO5Z, CRWENO5, WENO7JS, HCCS = 0, 1, 2, 3, 4
+SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5, "weno7js": WENO7JS,
+           "hccs": HCCS}
 TUNING_SLOTS = 12  # NUC3D_TUNING_SLOTS: (scheme id, direction) pairs
 RIEMANN_LF, RIEMANN_AUSM, RIEMANN_AUSMP = 0, 1, 2
 RIEMANNS = {"LF": RIEMANN_LF, "AUSM": RIEMANN_AUSM, "AUSMp": RIEMANN_AUSMP}

@@ -14,7 +14,7 @@ from pathlib import Path
 from . import (CONSTANT, EULER3D, FORCING_CONST, FORCING_NONE, NAVIERSTOKES3D, RIEMANNS,
                SCHEMES, SUTHERLAND, BoxDesc)
 
-_NOT_ON_PATH = ("hccs", "hccs77", "hccs78", "weno3js", "upwind1st")
+_NOT_ON_PATH = ("hccs77", "hccs78", "weno3js", "upwind1st")
 
 
 def _scheme(name: str) -> int:

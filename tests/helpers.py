@@ -42,17 +42,30 @@ def desc_from_box(box, precision=0):
                       quirks=box.quirks, riemann=box.riemann)
 
 
+def _ulp_perturbed(q, seed):
+    rng = np.random.default_rng(seed)
+    return [np.nextafter(a, np.where(rng.random(a.shape) < 0.5, -np.inf, np.inf)) for a in q]
+
+
 def rounding_sensitivity(box, q, nsteps, cfl=0.5, seed=0):
     """How far the oracle's own state after `nsteps` moves when every input
     value is moved by one ulp (max per-field relative L2).  The reference's
-    weno7js is ill-conditioned with respect to rounding (its expanded
-    Balsara-Shu indicators cancel terms of size 1e4 f^2), so two correct
-    implementations that round differently agree only to about this level;
-    WENO5 schemes give ~1e-13 here, weno7js ~1e-12 to 1e-9."""
+    weno7js and hccs are ill-conditioned with respect to rounding (expanded
+    Balsara-Shu indicators that cancel terms of size 1e4 f^2, Z weights with
+    eps 1e-20 / 1e-40), so two correct implementations that round differently
+    agree only to about this level; WENO5 schemes give ~1e-13 here, weno7js
+    and hccs ~1e-12 to 1e-9."""
     from oracle_ctypes import Oracle
     O = Oracle()
-    rng = np.random.default_rng(seed)
-    qp = [np.nextafter(a, np.where(rng.random(a.shape) < 0.5, -np.inf, np.inf)) for a in q]
     a, _, _ = O.run_steps(box, cfl, nsteps, list(q))
-    b, _, _ = O.run_steps(box, cfl, nsteps, qp)
+    b, _, _ = O.run_steps(box, cfl, nsteps, _ulp_perturbed(q, seed))
+    return max_rel_l2(a, b)
+
+
+def rhs_rounding_sensitivity(box, q, seed=0):
+    """The same for one RHS evaluation."""
+    from oracle_ctypes import Oracle
+    O = Oracle()
+    a, _ = O.rhs(box, list(q))
+    b, _ = O.rhs(box, _ulp_perturbed(q, seed))
     return max_rel_l2(a, b)

@@ -30,7 +30,7 @@ def test_decks_reject_paths_off_the_gpu_route(tmp_path):
 
 
 def test_scheme_strings_follow_the_reference(tmp_path):
-    """fieldOperator.cpp:128-180: weno7js is read, an unknown string falls
+    """fieldOperator.cpp:128-180: weno7js and hccs are read, an unknown string falls
     back to weno5js, and the reference's schemes that this path does not
     build are refused rather than silently replaced."""
     nb.write_decks(tmp_path, nb.BoxDesc(16, 16, 16, scheme=(nb.WENO7JS, nb.WENO5Z, nb.WENO7JS)))
@@ -39,9 +39,11 @@ def test_scheme_strings_follow_the_reference(tmp_path):
     text = p.read_text()
     p.write_text(text.replace("scheme_y_ivs weno5z", "scheme_y_ivs nonesuch"))
     assert nb.read_decks(tmp_path)[0].scheme == (nb.WENO7JS, nb.WENO5JS, nb.WENO7JS)
-    p.write_text(text.replace("scheme_y_ivs weno5z", "scheme_y_ivs hccs"))
+    p.write_text(text.replace("scheme_y_ivs weno5z", "scheme_y_ivs hccs78"))
     with pytest.raises(ValueError, match="not on the B200 path"):
         nb.read_decks(tmp_path)
+    p.write_text(text.replace("scheme_y_ivs weno5z", "scheme_y_ivs hccs"))
+    assert nb.read_decks(tmp_path)[0].scheme == (nb.WENO7JS, nb.HCCS, nb.WENO7JS)
 
 
 @pytest.mark.parametrize("riemann", [0, 1, 2])

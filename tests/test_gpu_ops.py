@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from helpers import golden, rel_l2
-from oracle_ctypes import QUIRKS_REFERENCE, Q_WENOZ_BETA2, WENO7, Oracle
+from oracle_ctypes import HCCS, QUIRKS_REFERENCE, Q_WENOZ_BETA2, WENO7, Oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -92,6 +92,24 @@ def test_weno7_reconstruct_vs_oracle_larger(torch_cuda, up):
                    to_dev(torch, hr), out)
     torch.cuda.synchronize()
     assert rel_l2(out.cpu().numpy(), ref) < TOL_OP
+
+
+@pytest.mark.parametrize("kind", ["smooth", "rough"])
+@pytest.mark.parametrize("up", [1, -1])
+def test_hccs_reconstruct_golden(torch_cuda, kind, up):
+    """hccs (hybrid compact) with 4-cell halos against the reference's own
+    outputs; 1e-12 (the blend switches on a threshold and the Z weights use
+    eps 1e-40, so the scheme amplifies rounding more than WENO5)."""
+    import nuc3d_b200 as nb
+    torch = torch_cuda
+    z = golden("operators_hc.npz")
+    tag = f"hc_{kind}_{'p' if up > 0 else 'm'}"
+    fin = to_dev(torch, z[f"rec_{tag}_in"])
+    out = torch.zeros(fin.shape[:2] + (fin.shape[2] + 1,), dtype=torch.float64, device="cuda")
+    nb.reconstruct(HCCS, up, QUIRKS_REFERENCE, fin, to_dev(torch, z[f"rec_{tag}_hl"]),
+                   to_dev(torch, z[f"rec_{tag}_hr"]), out)
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), z[f"rec_{tag}_out"]) < 1e-12
 
 
 def test_cd6_and_rk3_golden(torch_cuda):
