@@ -334,7 +334,7 @@ int nuc3d_reconstruct(int scheme, int upwind, unsigned quirks, int nx, int ny, i
     if (nx < 8 || ny < 1 || nz < 1) return fail(NUC3D_ERR_INVALID, "need nx >= 8, ny, nz >= 1");
     if ((scheme == NUC3D_CRWENO5 || scheme == NUC3D_HCCS) && nx > 4096)
         return fail(NUC3D_ERR_INVALID, "crweno5 / hccs need nx <= 4096");
-    if (scheme == NUC3D_HCCS && nx < 12) return fail(NUC3D_ERR_INVALID, "hccs needs nx >= 12");
+    if (scheme == NUC3D_HCCS && nx < 9) return fail(NUC3D_ERR_INVALID, "hccs needs nx >= 9");
     if (!in || !hl || !hr || !out) return fail(NUC3D_ERR_INVALID, "null buffer");
     CK(op_reconstruct(scheme, upwind, quirks, nx, (long long)ny * nz, in, hl, hr, out,
                       static_cast<cudaStream_t>(stream)));

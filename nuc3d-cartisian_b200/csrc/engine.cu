@@ -77,8 +77,8 @@ int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
         if ((d.scheme[i] == NUC3D_CRWENO5 || d.scheme[i] == NUC3D_HCCS) && n[i] > kCrMaxCells)
             return bad(NUC3D_ERR_UNSUPPORTED, "CRWENO5 / hccs lines are limited to 512 cells");
     for (int i = 0; i < 3; ++i)
-        if (d.scheme[i] == NUC3D_HCCS && n[i] < 12)
-            return bad(NUC3D_ERR_INVALID, "hccs lines need at least 12 cells");
+        if (d.scheme[i] == NUC3D_HCCS && n[i] < 9)
+            return bad(NUC3D_ERR_INVALID, "hccs lines need at least 9 cells");
     if ((long long)d.nx * d.ny * d.nz > (1LL << 31)) return bad(NUC3D_ERR_INVALID, "box larger than 2^31 cells");
     if (!(d.lx > 0 && d.ly > 0 && d.lz > 0)) return bad(NUC3D_ERR_INVALID, "box lengths must be > 0");
     if (d.pde_model != NUC3D_EULER3D && d.pde_model != NUC3D_NAVIERSTOKES3D)

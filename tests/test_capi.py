@@ -50,7 +50,7 @@ def test_ctx_bytes_accounting():
 @pytest.mark.parametrize("args,code", [
     ((7, 1, 0, 16, 2, 2), nb.ERR_UNSUPPORTED),   # no such scheme
     ((5, 1, 0, 16, 2, 2), nb.ERR_UNSUPPORTED),   # one past hccs
-    ((4, 1, 0, 10, 2, 2), nb.ERR_INVALID),       # hccs line too short
+    ((4, 1, 0, 8, 2, 2), nb.ERR_INVALID),        # hccs line too short
     ((3, 1, 0, 5, 2, 2), nb.ERR_INVALID),        # weno7js line too short
     ((0, 2, 0, 16, 2, 2), nb.ERR_INVALID),       # no such direction
     ((0, 1, 0, 5, 2, 2), nb.ERR_INVALID),        # line too short

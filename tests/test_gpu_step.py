@@ -115,9 +115,9 @@ def test_textbook_variants_match_oracle(torch, scheme):
     assert max_rel_l2(qg, qo) < step_tolerance(box, q, 2)
 
 
-@pytest.mark.parametrize("shape", [(150, 70, 13), (512, 12, 14)])
+@pytest.mark.parametrize("shape", [(150, 70, 9), (512, 12, 14)])
 def test_hccs_long_lines_match_oracle(torch, shape):
-    """hccs lines of 12 to 512 cells (every partition of the warp's line
+    """hccs lines of 9 to 512 cells (every partition of the warp's line
     solve) against the oracle's Thomas sweep."""
     box = Box(*shape, scheme=(HCCS,) * 3, mach=0.2, reynolds=500.0)
     rng = np.random.default_rng(sum(shape) + 1)
@@ -130,7 +130,12 @@ def test_hccs_long_lines_match_oracle(torch, shape):
 
 def test_hccs_mixed_precision_close_to_fp64(torch):
     """hccs with FP32 bulk arithmetic against its FP64 path: decaying
-    turbulence at 64^3, 50 steps."""
+    turbulence at 64^3, 50 steps.  hccs switches each row between its linear
+    and its weighted form on a threshold (theta > 1/2), and the two forms do
+    not meet there, so FP32 rounding that moves a row across the threshold
+    changes that face by O(the local flux jump): the fields agree to ~1e-4
+    (held to 1e-3 here) and the kinetic energy to 0.5 %, where the WENO
+    schemes, which are continuous in their data, agree to ~1e-7."""
     import nuc3d_b200 as nb
     desc = nb.BoxDesc(64, 64, 64, mach=1.0, scheme=(nb.HCCS,) * 3)
     init = {"kind": "hit", "seed": 4, "k_peak": 4.0, "mach_t": 0.3, "re_lambda": 100.0}
@@ -141,8 +146,11 @@ def test_hccs_mixed_precision_close_to_fp64(torch):
             s.step(50, 0.5, stats=False)
             out.append(s.get_state())
     err = max_rel_l2(out[1], out[0])
-    print(f"hccs mixed vs fp64 after 50 steps: max per-field rel L2 = {err:.3e}")
-    assert err < 1e-6
+    ke = [0.5 * float(np.sum((q[1] ** 2 + q[2] ** 2 + q[3] ** 2) / q[0])) for q in out]
+    print(f"hccs mixed vs fp64 after 50 steps: max per-field rel L2 = {err:.3e}, "
+          f"kinetic energy rel diff {abs(ke[1] - ke[0]) / ke[0]:.2e}")
+    assert err < 1e-3
+    assert abs(ke[1] - ke[0]) <= 5e-3 * ke[0]
 
 
 @pytest.mark.parametrize("bounded", [True, False])
