@@ -1,6 +1,5 @@
 // CRWENO5 and hccs directional sweeps, batched over boxes: one block per tile
-// of kCrTL lines of one box, one half-warp per (line, sign) tridiagonal
-// system.  hccs (hccs.cpp) has the same bounded structure with 4-cell ends:
+// of kCrTL lines of one box, one warp per (line, sign) tridiagonal system.  hccs (hccs.cpp) has the same bounded structure with 4-cell ends:
 // faces 0..3 and n-3..n explicit WENO7 (eps 1e-40), identity rows at faces 4
 // and n-4, hybrid compact rows in between (hc_row).
 //
@@ -16,12 +15,12 @@
 // a compact row and the system wraps around (cyclic tridiagonal).
 //
 // Per block and equation: the split fluxes F+ and F- of the tile's lines
-// (3-cell periodic halo) are staged in shared memory; each half-warp solves
+// (3-cell periodic halo) are staged in shared memory; each warp solves
 // one (line, sign) system by a partitioned method — lane l eliminates the
 // interior rows of its segment so that every row depends only on the
 // segment's first and last unknowns (rows kept at unit diagonal), the 2P
 // segment-end unknowns form a tridiagonal (cyclic for periodic lines) system
-// that the half-warp solves by parallel cyclic reduction with shuffles, and
+// that the warp solves by parallel cyclic reduction with shuffles, and
 // each lane back-substitutes its interior rows.  The compact rows are used
 // without normalising the weights (a row may be scaled freely), so a row
 // costs one reciprocal.  The face values overwrite the staged fluxes, and
@@ -34,9 +33,9 @@ namespace nuc3d {
 namespace {
 
 constexpr int kCrTL = 4;         // lines per block
-constexpr int kCrWarps = kCrTL;  // one warp per line: half-warp 0 solves F+, 1 solves F-
+constexpr int kCrWarps = 2 * kCrTL;  // one warp per (line, sign) system
 constexpr int kCrThreads = 32 * kCrWarps;
-constexpr int kCrLanes = 16;     // lanes per system
+constexpr int kCrLanes = 32;          // lanes per system
 
 // CRWENO5 weights up to a common positive factor (crweno5.cpp:136-150:
 // alpha_k = c_k / (eps + beta_k)^2, eps = 1e-6, c = 0.2, 0.5, 0.3).  A compact
@@ -194,8 +193,9 @@ __global__ void __launch_bounds__(kCrThreads)
     int P = 1;  // lanes per system
     while (P < kCrLanes && 2 * P <= N / 2) P *= 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int sg = lane >> 4, hl = lane & 15;  // sign (0: +, 1: -) and lane within the system
-    B *const myF = sF + (sg * kCrTL + warp) * ls;  // cell c at [c + H]; later face m at [m]
+    // warp w solves line w/2 of the tile for sign w%2 (0: +, 1: -)
+    const int line = warp >> 1, sg = warp & 1, hl = lane;
+    B *const myF = sF + (sg * kCrTL + line) * ls;  // cell c at [c + H]; later face m at [m]
     B *const wA = sRow + (size_t)warp * 3 * ms * 32;  // [j][lane]
     B *const wC = wA + ms * 32;
     B *const wD = wC + ms * 32;
@@ -237,11 +237,10 @@ __global__ void __launch_bounds__(kCrThreads)
         }
         __syncthreads();
 
-        if (l0 + warp < nl) {  // warp-uniform
+        if (l0 + line < nl) {  // warp-uniform
             auto F = [&](int c) -> B { return myF[c + H]; };
-            // the two half-warps run the same instructions: the sign only
-            // selects which cells feed a stencil ('+' reads upwind from the
-            // left, '-' from the right)
+            // the sign (warp-uniform) only selects which cells feed a
+            // stencil ('+' reads upwind from the left, '-' from the right)
             const int dir = sg == 0 ? 1 : -1;
             // explicit face m: WENO5-JS (crweno5.cpp:425-837) or hccs's WENO7
             // (hccs.cpp:538-980)
@@ -352,8 +351,8 @@ __global__ void __launch_bounds__(kCrThreads)
                 fd = df * r;
             }
             // parallel cyclic reduction of the 2P segment-end unknowns
-            // (reduced row 2l: x_first of lane l, 2l+1: x_last) within the half-warp
-            const int base = sg << 4;
+            // (reduced row 2l: x_first of lane l, 2l+1: x_last) within the warp
+            const int base = 0;
             for (int s = 1; s < 2 * P; s <<= 1) {
                 B fma_a, fma_c, fma_d, fpa, fpc, fpd;  // first's neighbours
                 B lma, lmc, lmd, lpa, lpc, lpd;        // last's neighbours

@@ -179,8 +179,10 @@ __device__ __forceinline__ double weno_z_combine(double is0, double is1, double 
 __device__ __forceinline__ float weno_z_combine(float is0, float is1, float is2, float q0, float q1,
                                                 float q2) {
     // 1e-40 is below FP32's normal range; 1e-30 keeps the ratio finite and
-    // only differs where a sub-stencil is exactly constant.
-    const float ss = 1.0e-30f, cap = 1.0e18f;
+    // only differs where a sub-stencil is exactly constant.  The ratio is
+    // capped at 1e15 so that alpha (<= 1e30) times a candidate stays far
+    // below FP32's 3.4e38 (a capped weight carries the face anyway).
+    const float ss = 1.0e-30f, cap = 1.0e15f;
     float tau = fabsf(sub_(is2, is0));
     float t0 = fminf(mul_(tau, frcp_fast(add_(is0, ss))), cap);
     float t1 = fminf(mul_(tau, frcp_fast(add_(is1, ss))), cap);
@@ -443,12 +445,17 @@ __device__ __forceinline__ float weno7_face_eps(float f0, float f1, float f2, fl
     is[1] = w7_beta(d3, s3, s4, 80.0f, 160.0f, 267.0f, -494.0f, 547.0f);
     is[2] = w7_beta(d4, s4, s5, -160.0f, -80.0f, 547.0f, -494.0f, 267.0f);
     is[3] = w7_beta(d5, s5, s6, -880.0f, 160.0f, 2107.0f, -1854.0f, 547.0f);
+    // the forms are positive semi-definite; rounding can leave a flat
+    // sub-stencil's value a little below zero, which with eps 1e-30 would turn
+    // tau/(eps + beta) into a huge negative number
+#pragma unroll
+    for (int k = 0; k < 4; ++k) is[k] = fmaxf(is[k], 0.0f);
     // 12 (q_k - f3)
     r[0] = fma_(3.0f, d1, fma_(-10.0f, d2, mul_(13.0f, d3)));
     r[1] = fma_(-1.0f, d2, fma_(4.0f, d3, mul_(3.0f, d4)));
     r[2] = fma_(-1.0f, d5, fma_(6.0f, d4, d3));
     r[3] = fma_(9.0f, d4, fma_(-4.0f, d5, d6));
-    const float cap = 1.0e18f;
+    const float cap = 1.0e15f;
     const float c[4] = {float(K7::C0), float(K7::C1), float(K7::C2), float(K7::C3)};
     float tau = fabsf(sub_(is[0], is[3]));
     float al[4];
@@ -474,7 +481,9 @@ __device__ __forceinline__ float weno7_face_eps(float f0, float f1, float f2, fl
 // arithmetic; this form stays finite for any x).
 //   FP64: the alphas multiplied through by P = s0 s1 s2, s_k = (beta_k +
 //   eps)^2 (at least 1e-80 each, so P does not underflow), x = (sum A - P)/P.
-//   FP32: reciprocal form with eps 1e-30 and tau/(beta + eps) capped.
+//   FP32: reciprocal form with eps = 1e-30 + the stencil's FP32 noise floor
+//   and tau/(beta + eps) capped; the weighted row in normalised weights,
+//   scaled by 1/x^2.
 __device__ __forceinline__ void hc_row(double f0, double f1, double f2, double f3, double f4,
                                        double &lo, double &b, double &hi, double &d) {
     double is0, is1, is2;
@@ -517,7 +526,17 @@ __device__ __forceinline__ void hc_row(float f0, float f1, float f2, float f3, f
     weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
     const float q7 = mul_(fma_(4.0f, f4, fma_(159.0f, f3, fma_(239.0f, f2, fma_(19.0f, f1, -f0)))),
                           float(1.0 / 420.0));
-    const float ss = 1.0e-30f, cap = 1.0e18f;
+    // eps: the reference's 1e-40 is below FP32's range; in its place the
+    // stencil's own FP32 noise floor, (4e-6 max|f|)^2 (a second difference of
+    // FP32 values is only known to ~1e-6 of their size).  Indicators below it
+    // carry no information: a flat stretch far from the line's offset cell
+    // would otherwise get noise-driven, saturated weights, and two saturated
+    // neighbouring rows (omega2 = 1, then omega0 = 1) form a singular 2x2
+    // block of the line system.  With the floor such stencils take the linear
+    // row.
+    const float sc = mul_(4.0e-6f, fmaxf(fmaxf(fmaxf(fabsf(f0), fabsf(f1)), fmaxf(fabsf(f2), fabsf(f3))),
+                                         fabsf(f4)));
+    const float ss = fma_(sc, sc, 1.0e-30f), cap = 1.0e15f;
     const float tau = fabsf(sub_(is2, is0));
     const float r0 = fminf(mul_(tau, frcp_fast(add_(is0, ss))), cap);
     const float r1 = fminf(mul_(tau, frcp_fast(add_(is1, ss))), cap);
@@ -534,14 +553,19 @@ __device__ __forceinline__ void hc_row(float f0, float f1, float f2, float f3, f
         d = q7;
         return;
     }
-    const float u = mul_(SA, frcp_fast(mul_(x, x)));  // sum(alpha) / x^2 (0 if x^2 overflows)
+    // FP32 keeps the reference's normalised weights (alphas reach 1e36 here)
+    // and scales the row by 1/x^2 (<= 1; 0 if x^2 overflows): every term
+    // stays O(1)
+    const float is = frcp_fast(SA);
+    const float w0 = mul_(A0, is), w1 = mul_(A1, is), w2 = mul_(A2, is);
+    const float u = frcp_fast(mul_(x, x));
     const float third = 1.0f / 3.0f, two3 = 2.0f / 3.0f, sixth = 1.0f / 6.0f;
-    lo = fma_(2.0f / 7.0f, u, fma_(two3, A0, mul_(third, A1)));
-    b = fma_(4.0f / 7.0f, u, fma_(third, A0, mul_(two3, add_(A1, A2))));
-    hi = fma_(1.0f / 7.0f, u, mul_(third, A2));
-    d = fma_(q7, u, fma_(mul_(sixth, add_(A1, mul_(5.0f, A2))), f3,
-                         fma_(mul_(sixth, add_(mul_(5.0f, add_(A0, A1)), A2)), f2,
-                              mul_(mul_(sixth, A0), f1))));
+    lo = fma_(2.0f / 7.0f, u, fma_(two3, w0, mul_(third, w1)));
+    b = fma_(4.0f / 7.0f, u, fma_(third, w0, mul_(two3, add_(w1, w2))));
+    hi = fma_(1.0f / 7.0f, u, mul_(third, w2));
+    d = fma_(q7, u, fma_(mul_(sixth, add_(w1, mul_(5.0f, w2))), f3,
+                         fma_(mul_(sixth, add_(mul_(5.0f, add_(w0, w1)), w2)), f2,
+                              mul_(mul_(sixth, w0), f1))));
 }
 
 // CD6 first derivative (centraldifference6th.cpp:44-46), times 1/dx.
