@@ -29,16 +29,21 @@ __global__ void __launch_bounds__(256, 4) k_prim(const BoxDev *__restrict__ boxe
     const double gamma = bp.gamma, Mach = bp.mach;
     const bool fabs_p = (bp.quirks & QK_FABS_PRESSURE) != 0;
     const long long n0 = (long long)it.a * kPrimChunk, n1 = n0 + it.b;
+    const double gM2 = gamma * Mach * Mach;
     for (long long n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
+        // one correctly rounded reciprocal of rho in place of the reference's
+        // five divisions (results within an ulp of them)
         double rho = q[n];
-        double u = q[np + n] / rho;
-        double v = q[2 * np + n] / rho;
-        double ww = q[3 * np + n] / rho;
+        double ri = __drcp_rn(rho);
+        double u = q[np + n] * ri;
+        double v = q[2 * np + n] * ri;
+        double ww = q[3 * np + n] * ri;
         double E = q[4 * np + n];
         double p = (E - 0.5 * rho * (u * u + v * v + ww * ww)) * (gamma - 1.0);
         if (fabs_p) p = fabs(p);
-        double c = sqrt(gamma * p / rho);
-        double T = gamma * Mach * Mach * p / rho;
+        double pr = p * ri;
+        double c = sqrt(gamma * pr);
+        double T = gM2 * pr;
         w[n] = u;
         w[np + n] = v;
         w[2 * np + n] = ww;
