@@ -353,6 +353,7 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));  // host vectors go out of scope
     ECK(prepare_inviscid_kernels(mixed));
     ECK(prepare_crweno_kernels(mixed));
+    ECK(prepare_stencil_kernels(mixed));
     int per_stage = (r_prim_.n > 0) + (any_visc_ && r_25d_.n > 0) + (r_25d_.n > 0);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d].n > 0;

@@ -107,6 +107,8 @@ template <typename B>
 cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxes,
                             const WorkItem *items, int nitems, int in_slot, int accumulate,
                             cudaStream_t st);
+// raises the dynamic shared-memory limit of the viscous-flux kernel
+cudaError_t prepare_stencil_kernels(bool mixed);
 template <typename B>
 cudaError_t launch_visc_flux(const BoxDev *boxes, const WorkItem *items, int nitems,
                              cudaStream_t st);

@@ -44,8 +44,12 @@ __device__ __forceinline__ double cd6d(double m3, double m2, double m1, double p
 // Work item: (box, x tile, y tile, z chunk).
 template <typename B>
 __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items) {
-    __shared__ double sP[2][4][TY + 6][TX + 6];
-    __shared__ int sOff[(TY + 6) * (TX + 6)];  // in-plane offsets of the staged tile
+    // dynamic shared memory (visc_smem_bytes): the two plane tiles with their
+    // x/y halo, each column's plane k+3 (z-queue refill), the tile offsets
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto sP = reinterpret_cast<double (*)[4][TY + 6][TX + 6]>(smem_raw);
+    auto sZ = reinterpret_cast<double (*)[4][TX * TY]>(smem_raw + sizeof(double) * 2 * 4 * (TY + 6) * (TX + 6));
+    int *sOff = reinterpret_cast<int *>(smem_raw + sizeof(double) * 2 * 4 * ((TY + 6) * (TX + 6) + TX * TY));
     const WorkItem it = items[blockIdx.x];
     const BoxDev &bd = boxes[it.box];
     if (!bd.active || !bd.p.navier_stokes) return;
@@ -66,6 +70,8 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
         sOff[t] = pmod(i0 - 3 + xx, nx) + nx * pmod(j0 - 3 + yy, ny);
     }
     __syncthreads();
+    // plane k's halo tile, and each column's plane k+3 for the z-queue: both
+    // arrive while plane k-1 is computed
     auto issue = [&](int k, int buf) {
         const long long plane = sz * k;
         for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
@@ -73,6 +79,11 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
             long long g = plane + sOff[t];
 #pragma unroll
             for (int f = 0; f < 4; ++f) cp_async_elem(&sP[buf][f][yy][xx], wbase + src[f] * np + g);
+        }
+        if (active) {
+            const long long g6 = col + sz * pmod(k + 3, nz);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) cp_async_elem(&sZ[buf][f][tid], wbase + src[f] * np + g6);
         }
     };
     const int kend = min(k0 + KZ, nz);
@@ -92,13 +103,10 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
         const int buf = (k - k0) & 1;
         if (k + 1 < kend) issue(k + 1, buf ^ 1);
         cp_async_commit();
-        {
-            long long g = col + sz * pmod(k + 3, nz);
-#pragma unroll
-            for (int f = 0; f < 4; ++f) qz[f][6] = active ? wbase[src[f] * np + g] : 0.0;
-        }
         cp_async_wait1();
         __syncthreads();
+#pragma unroll
+        for (int f = 0; f < 4; ++f) qz[f][6] = active ? sZ[buf][f][tid] : 0.0;
         if (active) {
             B gr[4][3];
 #pragma unroll
@@ -158,6 +166,9 @@ __global__ void __launch_bounds__(TX *TY, 2)
     k_update25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, StageArgs sa) {
     // x stencils: tau_xx, tau_xy, tau_xz, E_x; y: tau_xy, tau_yy, tau_yz, E_y;
     // z: tau_xz, tau_yz, tau_zz, E_z
+    // x and y halo tiles of the fluxes each stencil direction needs.  (The
+    // z-queue refill stays a direct load here: routing it through shared
+    // memory as k_visc_flux25 does pushed this kernel into register spills.)
     __shared__ B sX[2][4][TY][TX + 6];
     __shared__ B sY[2][4][TY + 6][TX];
     __shared__ double red[TX * TY / 32];
@@ -297,11 +308,26 @@ __global__ void __launch_bounds__(TX *TY, 2)
     }
 }
 
+namespace {
+constexpr size_t visc_smem_bytes() {
+    return sizeof(double) * 2 * 4 * ((TY + 6) * (TX + 6) + TX * TY) + sizeof(int) * (TY + 6) * (TX + 6);
+}
+}  // namespace
+
+cudaError_t prepare_stencil_kernels(bool mixed) {
+    return mixed ? cudaFuncSetAttribute(k_visc_flux25<float>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)visc_smem_bytes())
+                 : cudaFuncSetAttribute(k_visc_flux25<double>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)visc_smem_bytes());
+}
+
 template <typename B>
 cudaError_t launch_visc_flux(const BoxDev *boxes, const WorkItem *items, int nitems,
                              cudaStream_t st) {
     if (nitems <= 0) return cudaSuccess;
-    k_visc_flux25<B><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items);
+    k_visc_flux25<B><<<nitems, dim3(TX, TY), visc_smem_bytes(), st>>>(boxes, items);
     return cudaGetLastError();
 }
 
