@@ -193,6 +193,92 @@ __device__ __forceinline__ float weno_z_combine(float is0, float is1, float is2,
     return mul_(fma_(a2, q2, fma_(a1, q1, mul_(a0, q0))), frcp_fast(add_(add_(a0, a1), a2)));
 }
 
+// The same combinations in offset form for the sweeps: with dq_k = q_k - f2
+// the face is f2 + sum(w_k dq_k) / sum(w_k), which saves the candidates'
+// common part and keeps the rounding relative to the local variation.
+// WENO5-Z's (beta + 1e-40)^2 is formed as beta^2 + 1e-80 (the cross term is
+// below 1e-40 of beta).
+__device__ __forceinline__ double weno_js_combine_dq(double is0, double is1, double is2,
+                                                     double dq0, double dq1, double dq2,
+                                                     double f2) {
+    const double ss = 1.0e-6;
+    double s0 = add_(ss, is0), s1 = add_(ss, is1), s2 = add_(ss, is2);
+    s0 = mul_(s0, s0);
+    s1 = mul_(s1, s1);
+    s2 = mul_(s2, s2);
+    double w0 = mul_(K::C0, mul_(s1, s2)), w1 = mul_(K::C1, mul_(s0, s2));
+    double w2 = mul_(K::C2, mul_(s0, s1));
+    return fma_(fma_(w2, dq2, fma_(w1, dq1, mul_(w0, dq0))),
+                __drcp_rn(add_(add_(w0, w1), w2)), f2);
+}
+__device__ __forceinline__ float weno_js_combine_dq(float is0, float is1, float is2, float dq0,
+                                                    float dq1, float dq2, float f2) {
+    const float ss = 1.0e-6f;
+    float r0 = frcp_fast(add_(ss, is0)), r1 = frcp_fast(add_(ss, is1)), r2 = frcp_fast(add_(ss, is2));
+    float a0 = mul_(mul_(float(K::C0), r0), r0), a1 = mul_(mul_(float(K::C1), r1), r1);
+    float a2 = mul_(mul_(float(K::C2), r2), r2);
+    return fma_(fma_(a2, dq2, fma_(a1, dq1, mul_(a0, dq0))), frcp_fast(add_(add_(a0, a1), a2)),
+                f2);
+}
+__device__ __forceinline__ double weno_z_combine_dq(double is0, double is1, double is2,
+                                                    double dq0, double dq1, double dq2,
+                                                    double f2) {
+    const double ss2 = 1.0e-80;  // eps^2, eps = 1e-40
+    double tau = fabs(sub_(is2, is0));
+    double t2 = mul_(tau, tau);
+    double s0 = fma_(is0, is0, ss2), s1 = fma_(is1, is1, ss2), s2 = fma_(is2, is2, ss2);
+    double w0 = mul_(mul_(K::C0, add_(s0, t2)), mul_(s1, s2));
+    double w1 = mul_(mul_(K::C1, add_(s1, t2)), mul_(s0, s2));
+    double w2 = mul_(mul_(K::C2, add_(s2, t2)), mul_(s0, s1));
+    return fma_(fma_(w2, dq2, fma_(w1, dq1, mul_(w0, dq0))),
+                __drcp_rn(add_(add_(w0, w1), w2)), f2);
+}
+__device__ __forceinline__ float weno_z_combine_dq(float is0, float is1, float is2, float dq0,
+                                                   float dq1, float dq2, float f2) {
+    const float ss = 1.0e-30f, cap = 1.0e15f;
+    float tau = fabsf(sub_(is2, is0));
+    float t0 = fminf(mul_(tau, frcp_fast(add_(is0, ss))), cap);
+    float t1 = fminf(mul_(tau, frcp_fast(add_(is1, ss))), cap);
+    float t2 = fminf(mul_(tau, frcp_fast(add_(is2, ss))), cap);
+    float a0 = mul_(float(K::C0), fma_(t0, t0, 1.0f));
+    float a1 = mul_(float(K::C1), fma_(t1, t1, 1.0f));
+    float a2 = mul_(float(K::C2), fma_(t2, t2, 1.0f));
+    return fma_(fma_(a2, dq2, fma_(a1, dq1, mul_(a0, dq0))), frcp_fast(add_(add_(a0, a1), a2)),
+                f2);
+}
+
+// One WENO5 face (either scheme) from the sliding window's differences:
+// a_ij = f_i - f_j of the upwind-oriented stencil f0..f4, the second
+// differences D0 = f0 - 2 f1 + f2 and D2 = f2 - 2 f3 + f4, and dd_k =
+// 13/12 D_k^2 (the indicators' first terms, carried from face to face).
+// With e_k the indicators' second terms halved (schemes.hpp:33-34 with the
+// 1/4 taken as (E/2)^2):
+//   e0 = D0/2 + a21,  e1 = -(a21 + a32)/2,  e2 = D2/2 - a32,
+//   beta_k = dd_k + e_k^2,
+// and the candidates (schemes.hpp:14-18) as f2 + dq_k:
+//   dq0 = D0/3 + a21/2,  dq1 = a21/6 + a32/3,  dq2 = 2 a32/3 - a43/6.
+template <int SCHEME, typename B>
+__device__ __forceinline__ B weno5_face_dq(B f2, B a21, B a32, B a43, B D0, B D2, B dd0, B dd1,
+                                           B dd2) {
+    const B h = B(0.5);
+    const B e0 = fma_(h, D0, a21);
+    const B e1 = mul_(B(-0.5), add_(a21, a32));
+    const B e2 = fma_(h, D2, -a32);
+    const B is0 = fma_(e0, e0, dd0), is1 = fma_(e1, e1, dd1), is2 = fma_(e2, e2, dd2);
+    const B dq0 = fma_(B(1.0 / 3.0), D0, mul_(h, a21));
+    const B dq1 = fma_(B(1.0 / 6.0), a21, mul_(B(1.0 / 3.0), a32));
+    const B dq2 = fma_(B(2.0 / 3.0), a32, mul_(B(-1.0 / 6.0), a43));
+    if (SCHEME == SCHEME_Z) return weno_z_combine_dq(is0, is1, is2, dq0, dq1, dq2, f2);
+    return weno_js_combine_dq(is0, is1, is2, dq0, dq1, dq2, f2);
+}
+
+// 13/12 D^2 as (sqrt(13/12) D)^2
+template <typename B>
+__device__ __forceinline__ B dd_of(B D) {
+    const B t = mul_(B(K::SG0), D);
+    return mul_(t, t);
+}
+
 template <int SCHEME, typename B>
 __device__ __forceinline__ B weno_combine(B is0, B is1, B is2, B q0, B q1, B q2) {
     if (SCHEME == SCHEME_Z) return weno_z_combine(is0, is1, is2, q0, q1, q2);

@@ -171,25 +171,6 @@ struct InvGeom {
     }
 };
 
-// One direction's smoothness and candidate terms for a stencil whose scaled
-// second differences d0, d1, d2 (sd2_) are already known (the run reuses
-// them across faces).  beta_k = 13/12 D_k^2 + 1/4 E_k^2 (schemes.hpp:33-34)
-// is formed as d_k^2 + e_k^2 with d = sqrt(13/12) D and e = E / 2.
-template <int SCHEME, typename B>
-__device__ __forceinline__ B weno_from(B f0, B f1, B f2, B f3, B f4, B d0, B d1, B d2) {
-    const B h = B(0.5), th = B(1.5), m2 = B(-2), mh = B(-0.5);
-    B e0 = fma_(th, f2, fma_(m2, f1, mul_(h, f0)));
-    B e1 = fma_(h, f1, mul_(mh, f3));
-    B e2 = fma_(th, f2, fma_(m2, f3, mul_(h, f4)));
-    B is0 = fma_(d0, d0, mul_(e0, e0));
-    B is1 = fma_(d1, d1, mul_(e1, e1));
-    B is2 = fma_(d2, d2, mul_(e2, e2));
-    B q0 = fma_(B(K::A02), f2, fma_(B(K::A01), f1, mul_(B(K::A00), f0)));
-    B q1 = fma_(B(K::A12), f3, fma_(B(K::A11), f2, mul_(B(K::A10), f1)));
-    B q2 = fma_(B(K::A22), f4, fma_(B(K::A21), f3, mul_(B(K::A20), f2)));
-    return weno_combine<SCHEME, B>(is0, is1, is2, q0, q1, q2);
-}
-
 // Inviscid flux derivative along DIR for all 5 equations (euler3d.cpp:307-387
 // + combineFluxLR :23-56 + setDerivatives*Inv :143-253), with the box's
 // point-wise flux split (LF, AUSM or AUSMp; split_prepare) done while
@@ -365,51 +346,73 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
                 }
             }
         } else {
-        {  // '+' side: window f0..f4 = positions m..m+4
-            const int v = e;
-            B f0 = sF[G::sf(v, l, m0)], f1 = sF[G::sf(v, l, m0 + 1)], f2 = sF[G::sf(v, l, m0 + 2)];
-            B f3 = sF[G::sf(v, l, m0 + 3)], f4 = sF[G::sf(v, l, m0 + 4)];
-            B d0 = sd2_(f0, f1, f2), d1 = sd2_(f1, f2, f3);
+            // WENO5: the window carries the first differences a_ij, the second
+            // differences D and dd = 13/12 D^2 of the current stencil, so each
+            // new face adds one value, one difference, one second difference
+            // and one square (weno5_face_dq).
+            {  // '+' side: stencil f0..f4 = positions m..m+4
+                const int v = e;
+                B f0 = sF[G::sf(v, l, m0)], f1 = sF[G::sf(v, l, m0 + 1)];
+                B f2 = sF[G::sf(v, l, m0 + 2)], f3 = sF[G::sf(v, l, m0 + 3)];
+                B f4 = sF[G::sf(v, l, m0 + 4)];
+                B a10 = sub_(f1, f0), a21 = sub_(f2, f1), a32 = sub_(f3, f2), a43 = sub_(f4, f3);
+                B D0 = sub_(a21, a10), D1 = sub_(a32, a21), D2 = sub_(a43, a32);
+                B dd0 = dd_of(D0), dd1 = dd_of(D1), dd2 = dd_of(D2);
 #pragma unroll
-            for (int k = 0; k <= R; ++k) {
-                if (k == R && !last) break;
-                const int gm = c0 + m0 + k;
-                B d2 = sd2_(f2, f3, f4);
-                // weno5z.cpp:80 on the inner '+' faces 3..n-3
-                B d2s = (zq && gm >= 3 && gm <= n - 3) ? sd2_(f2, f3, f3) : d2;
-                Fh[k] = weno_from<SCHEME, B>(f0, f1, f2, f3, f4, d0, d1, d2s);
-                if (k < R) {
-                    f0 = f1;
-                    f1 = f2;
-                    f2 = f3;
-                    f3 = f4;
-                    f4 = sF[G::sf(v, l, m0 + k + 5)];
-                    d0 = d1;
-                    d1 = d2;
+                for (int k = 0; k <= R; ++k) {
+                    if (k == R && !last) break;
+                    const int gm = c0 + m0 + k;
+                    // weno5z.cpp:80 on the inner '+' faces 3..n-3: beta2's first
+                    // term reads f2 - 2 f3 + f3 = -a32
+                    const B dd2s = (zq && gm >= 3 && gm <= n - 3) ? dd_of(a32) : dd2;
+                    Fh[k] = weno5_face_dq<SCHEME, B>(f2, a21, a32, a43, D0, D2, dd0, dd1, dd2s);
+                    if (k < R) {
+                        f2 = f3;
+                        f3 = f4;
+                        f4 = sF[G::sf(v, l, m0 + k + 5)];
+                        a21 = a32;
+                        a32 = a43;
+                        a43 = sub_(f4, f3);
+                        D0 = D1;
+                        D1 = D2;
+                        D2 = sub_(a43, a32);
+                        dd0 = dd1;
+                        dd1 = dd2;
+                        dd2 = dd_of(D2);
+                    }
                 }
             }
-        }
-        {  // '-' side: window f0..f4 = positions m+5..m+1
-            const int v = 5 + e;
-            B f0 = sF[G::sf(v, l, m0 + 5)], f1 = sF[G::sf(v, l, m0 + 4)], f2 = sF[G::sf(v, l, m0 + 3)];
-            B f3 = sF[G::sf(v, l, m0 + 2)], f4 = sF[G::sf(v, l, m0 + 1)];
-            B d1 = sd2_(f1, f2, f3), d2 = sd2_(f2, f3, f4);
+            {  // '-' side: stencil f0..f4 = positions m+5..m+1
+                const int v = 5 + e;
+                B f0 = sF[G::sf(v, l, m0 + 5)], f1 = sF[G::sf(v, l, m0 + 4)];
+                B f2 = sF[G::sf(v, l, m0 + 3)], f3 = sF[G::sf(v, l, m0 + 2)];
+                B f4 = sF[G::sf(v, l, m0 + 1)];
+                B a10 = sub_(f1, f0), a21 = sub_(f2, f1), a32 = sub_(f3, f2), a43 = sub_(f4, f3);
+                B D0 = sub_(a21, a10), D1 = sub_(a32, a21), D2 = sub_(a43, a32);
+                B dd0 = dd_of(D0), dd1 = dd_of(D1), dd2 = dd_of(D2);
 #pragma unroll
-            for (int k = 0; k <= R; ++k) {
-                if (k == R && !last) break;
-                B d0 = sd2_(f0, f1, f2);
-                Fh[k] = add_(Fh[k], weno_from<SCHEME, B>(f0, f1, f2, f3, f4, d0, d1, d2));
-                if (k < R) {
-                    f4 = f3;
-                    f3 = f2;
-                    f2 = f1;
-                    f1 = f0;
-                    f0 = (m0 + k + 6 < NF) ? sF[G::sf(v, l, m0 + k + 6)] : B(0);
-                    d2 = d1;
-                    d1 = d0;
+                for (int k = 0; k <= R; ++k) {
+                    if (k == R && !last) break;
+                    Fh[k] = add_(Fh[k], weno5_face_dq<SCHEME, B>(f2, a21, a32, a43, D0, D2, dd0,
+                                                                 dd1, dd2));
+                    if (k < R) {
+                        const B fn = (m0 + k + 6 < NF) ? sF[G::sf(v, l, m0 + k + 6)] : B(0);
+                        f2 = f1;
+                        f1 = f0;
+                        f0 = fn;
+                        a43 = a32;
+                        a32 = a21;
+                        a21 = a10;
+                        a10 = sub_(f1, f0);
+                        D2 = D1;
+                        D1 = D0;
+                        D0 = sub_(a21, a10);
+                        dd2 = dd1;
+                        dd1 = dd0;
+                        dd0 = dd_of(D0);
+                    }
                 }
             }
-        }
         }
         B *x = xb + (e & 1) * NT;
         x[threadIdx.x] = Fh[0];
