@@ -132,7 +132,7 @@ int crweno_tile_lines() { return kCrTL; }
 // Work item (box, a, b, -): DIR 0: lines j = a*TL.., k = b; DIR 1: lines
 // i = a*TL.., k = b; DIR 2: lines i = a*TL.., j = b.
 template <typename B, int DIR, int SCH>
-__global__ void __launch_bounds__(kCrThreads)
+__global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
     k_crweno_lines(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items,
                    int in_slot, int accumulate, int nmax, int ms) {
     // SCH: SCHEME_CR (crweno5) or SCHEME_HC (hccs).  H: staged halo, explicit
