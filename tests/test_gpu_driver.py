@@ -67,3 +67,12 @@ def test_driver_restart_continues_bitwise(driver, tmp_path):
     z = golden("tgv24_js_10.npz")
     _, q = read_restart(tmp_path / "flowData" / "NUC3d_step_10_ID_0.bin", d.shape)
     assert max_rel_l2(q, z["q10"]) < 1e-12
+
+
+def test_case_runner_module(capsys):
+    """python -m nuc3d_b200: one seeded HIT case on the device, one JSON line."""
+    import json
+    from nuc3d_b200.__main__ import main
+    main(["--n", "16", "--scheme", "crweno5", "--precision", "mixed", "--steps", "2"])
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert out["steps"] == 2 and out["dt_last"] > 0 and out["kinetic"] > 0
