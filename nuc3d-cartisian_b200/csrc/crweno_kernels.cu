@@ -168,17 +168,16 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
         const double qe = qbase[e * np + g];
         const double un = wbase[DIR * np + g], p = wbase[3 * np + g], c = wbase[4 * np + g];
         if (riemann == RIEMANN_LF) {  // block-uniform; physicsModel.cpp:546-565
-            const double lam = add_(fabs(un), c);
-            double f;
+            const double hun = mul_(0.5, un), hlam = mul_(0.5, add_(fabs(un), c));
+            double hf;
             if (e == 4)
-                f = mul_(un, add_(qe, p));
+                hf = mul_(hun, add_(qe, p));
             else if (e == 1 + DIR)
-                f = fma_(un, qe, p);
+                hf = fma_(hun, qe, mul_(0.5, p));
             else
-                f = mul_(un, qe);
-            const double t = mul_(lam, qe);
-            fp = mul_(0.5, add_(f, t));
-            fm = mul_(0.5, sub_(f, t));
+                hf = mul_(hun, qe);
+            fp = fma_(hlam, qe, hf);
+            fm = fma_(-hlam, qe, hf);
         } else {
             SplitCell sc;
             split_prepare(riemann, un, p, c, sc);
@@ -414,20 +413,33 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
         }
         __syncthreads();
         // dF/dx of the tile's cells from F^ = F^+ + F^- (euler3d.cpp:23-56, 143-253)
-        for (int t = threadIdx.x; t < kCrTL * n; t += kCrThreads) {
-            int l, i;
-            if (DIR == 0) {
-                l = t / n;
-                i = t - l * n;
-            } else {
-                l = t % kCrTL;
-                i = t / kCrTL;
+        // four cells per thread and pass, their RHS loads issued together
+        constexpr int U = 4;
+        for (int t0 = threadIdx.x; t0 < kCrTL * n; t0 += U * kCrThreads) {
+            long long gi[U];
+            B dfe[U], racc[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int t = t0 + u * kCrThreads;
+                int l, i;
+                if (DIR == 0) {
+                    l = t / n;
+                    i = t - l * n;
+                } else {
+                    l = t % kCrTL;
+                    i = t / kCrTL;
+                }
+                gi[u] = -1;
+                dfe[u] = racc[u] = B(0);
+                if (t >= kCrTL * n || l0 + l >= nl) continue;
+                const B *fp = sF + l * ls, *fm = sF + (kCrTL + l) * ls;
+                dfe[u] = mul_(sub_(add_(fp[i + 1], fm[i + 1]), add_(fp[i], fm[i])), inv_d);
+                gi[u] = (long long)e * np + gidx(l, i);
+                if (accumulate) racc[u] = rbase[gi[u]];
             }
-            if (l0 + l >= nl) continue;
-            const B *fp = sF + l * ls, *fm = sF + (kCrTL + l) * ls;
-            const B dfe = mul_(sub_(add_(fp[i + 1], fm[i + 1]), add_(fp[i], fm[i])), inv_d);
-            B *r = rbase + (long long)e * np + gidx(l, i);
-            *r = accumulate ? add_(*r, dfe) : dfe;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (gi[u] >= 0) rbase[gi[u]] = accumulate ? add_(racc[u], dfe[u]) : dfe[u];
         }
         __syncthreads();
     }

@@ -195,56 +195,56 @@ __device__ __forceinline__ float weno_z_combine(float is0, float is1, float is2,
 
 // The same combinations in offset form for the sweeps: with dq_k = q_k - f2
 // the face is f2 + sum(w_k dq_k) / sum(w_k), which saves the candidates'
-// common part and keeps the rounding relative to the local variation.
-// WENO5-Z's (beta + 1e-40)^2 is formed as beta^2 + 1e-80 (the cross term is
-// below 1e-40 of beta).
+// common part and keeps the rounding relative to the local variation.  The
+// linear weights are 0.1 (1, 6, 3); the 0.1 cancels in the ratio and the 6
+// and 3 go with the candidates, so the caller passes g = (dq0, 6 dq1, 3 dq2)
+// and the face is f2 + (w0 g0 + w1 g1 + w2 g2) / (w0 + 6 w1 + 3 w2) with w_k
+// the weights without their linear factor.  WENO5-Z's (beta + 1e-40)^2 is
+// formed as beta^2 + 1e-80 (the cross term is below 1e-40 of beta).
 __device__ __forceinline__ double weno_js_combine_dq(double is0, double is1, double is2,
-                                                     double dq0, double dq1, double dq2,
+                                                     double g0, double g1, double g2,
                                                      double f2) {
     const double ss = 1.0e-6;
     double s0 = add_(ss, is0), s1 = add_(ss, is1), s2 = add_(ss, is2);
     s0 = mul_(s0, s0);
     s1 = mul_(s1, s1);
     s2 = mul_(s2, s2);
-    double w0 = mul_(K::C0, mul_(s1, s2)), w1 = mul_(K::C1, mul_(s0, s2));
-    double w2 = mul_(K::C2, mul_(s0, s1));
-    return fma_(fma_(w2, dq2, fma_(w1, dq1, mul_(w0, dq0))),
-                __drcp_rn(add_(add_(w0, w1), w2)), f2);
+    const double w0 = mul_(s1, s2), w1 = mul_(s0, s2), w2 = mul_(s0, s1);
+    return fma_(fma_(w2, g2, fma_(w1, g1, mul_(w0, g0))),
+                __drcp_rn(fma_(6.0, w1, fma_(3.0, w2, w0))), f2);
 }
-__device__ __forceinline__ float weno_js_combine_dq(float is0, float is1, float is2, float dq0,
-                                                    float dq1, float dq2, float f2) {
+__device__ __forceinline__ float weno_js_combine_dq(float is0, float is1, float is2, float g0,
+                                                    float g1, float g2, float f2) {
     const float ss = 1.0e-6f;
     float r0 = frcp_fast(add_(ss, is0)), r1 = frcp_fast(add_(ss, is1)), r2 = frcp_fast(add_(ss, is2));
-    float a0 = mul_(mul_(float(K::C0), r0), r0), a1 = mul_(mul_(float(K::C1), r1), r1);
-    float a2 = mul_(mul_(float(K::C2), r2), r2);
-    return fma_(fma_(a2, dq2, fma_(a1, dq1, mul_(a0, dq0))), frcp_fast(add_(add_(a0, a1), a2)),
-                f2);
+    const float a0 = mul_(r0, r0), a1 = mul_(r1, r1), a2 = mul_(r2, r2);
+    return fma_(fma_(a2, g2, fma_(a1, g1, mul_(a0, g0))),
+                frcp_fast(fma_(6.0f, a1, fma_(3.0f, a2, a0))), f2);
 }
 __device__ __forceinline__ double weno_z_combine_dq(double is0, double is1, double is2,
-                                                    double dq0, double dq1, double dq2,
+                                                    double g0, double g1, double g2,
                                                     double f2) {
     const double ss2 = 1.0e-80;  // eps^2, eps = 1e-40
     double tau = fabs(sub_(is2, is0));
     double t2 = mul_(tau, tau);
     double s0 = fma_(is0, is0, ss2), s1 = fma_(is1, is1, ss2), s2 = fma_(is2, is2, ss2);
-    double w0 = mul_(mul_(K::C0, add_(s0, t2)), mul_(s1, s2));
-    double w1 = mul_(mul_(K::C1, add_(s1, t2)), mul_(s0, s2));
-    double w2 = mul_(mul_(K::C2, add_(s2, t2)), mul_(s0, s1));
-    return fma_(fma_(w2, dq2, fma_(w1, dq1, mul_(w0, dq0))),
-                __drcp_rn(add_(add_(w0, w1), w2)), f2);
+    // alpha_k / c_k * s0^2 s1^2 s2^2 = (s_k^2 + tau^2) prod_{j!=k} s_j^2
+    const double w0 = mul_(add_(s0, t2), mul_(s1, s2));
+    const double w1 = mul_(add_(s1, t2), mul_(s0, s2));
+    const double w2 = mul_(add_(s2, t2), mul_(s0, s1));
+    return fma_(fma_(w2, g2, fma_(w1, g1, mul_(w0, g0))),
+                __drcp_rn(fma_(6.0, w1, fma_(3.0, w2, w0))), f2);
 }
-__device__ __forceinline__ float weno_z_combine_dq(float is0, float is1, float is2, float dq0,
-                                                   float dq1, float dq2, float f2) {
+__device__ __forceinline__ float weno_z_combine_dq(float is0, float is1, float is2, float g0,
+                                                   float g1, float g2, float f2) {
     const float ss = 1.0e-30f, cap = 1.0e15f;
     float tau = fabsf(sub_(is2, is0));
     float t0 = fminf(mul_(tau, frcp_fast(add_(is0, ss))), cap);
     float t1 = fminf(mul_(tau, frcp_fast(add_(is1, ss))), cap);
     float t2 = fminf(mul_(tau, frcp_fast(add_(is2, ss))), cap);
-    float a0 = mul_(float(K::C0), fma_(t0, t0, 1.0f));
-    float a1 = mul_(float(K::C1), fma_(t1, t1, 1.0f));
-    float a2 = mul_(float(K::C2), fma_(t2, t2, 1.0f));
-    return fma_(fma_(a2, dq2, fma_(a1, dq1, mul_(a0, dq0))), frcp_fast(add_(add_(a0, a1), a2)),
-                f2);
+    const float a0 = fma_(t0, t0, 1.0f), a1 = fma_(t1, t1, 1.0f), a2 = fma_(t2, t2, 1.0f);
+    return fma_(fma_(a2, g2, fma_(a1, g1, mul_(a0, g0))),
+                frcp_fast(fma_(6.0f, a1, fma_(3.0f, a2, a0))), f2);
 }
 
 // One WENO5 face (either scheme) from the sliding window's differences:
@@ -256,7 +256,7 @@ __device__ __forceinline__ float weno_z_combine_dq(float is0, float is1, float i
 //   e0 = D0/2 + a21,  e1 = -(a21 + a32)/2,  e2 = D2/2 - a32,
 //   beta_k = dd_k + e_k^2,
 // and the candidates (schemes.hpp:14-18) as f2 + dq_k:
-//   dq0 = D0/3 + a21/2,  dq1 = a21/6 + a32/3,  dq2 = 2 a32/3 - a43/6.
+//   dq0 = D0/3 + a21/2,  6 dq1 = a21 + 2 a32,  3 dq2 = 2 a32 - a43/2.
 template <int SCHEME, typename B>
 __device__ __forceinline__ B weno5_face_dq(B f2, B a21, B a32, B a43, B D0, B D2, B dd0, B dd1,
                                            B dd2) {
@@ -265,11 +265,11 @@ __device__ __forceinline__ B weno5_face_dq(B f2, B a21, B a32, B a43, B D0, B D2
     const B e1 = mul_(B(-0.5), add_(a21, a32));
     const B e2 = fma_(h, D2, -a32);
     const B is0 = fma_(e0, e0, dd0), is1 = fma_(e1, e1, dd1), is2 = fma_(e2, e2, dd2);
-    const B dq0 = fma_(B(1.0 / 3.0), D0, mul_(h, a21));
-    const B dq1 = fma_(B(1.0 / 6.0), a21, mul_(B(1.0 / 3.0), a32));
-    const B dq2 = fma_(B(2.0 / 3.0), a32, mul_(B(-1.0 / 6.0), a43));
-    if (SCHEME == SCHEME_Z) return weno_z_combine_dq(is0, is1, is2, dq0, dq1, dq2, f2);
-    return weno_js_combine_dq(is0, is1, is2, dq0, dq1, dq2, f2);
+    const B g0 = fma_(B(1.0 / 3.0), D0, mul_(h, a21));
+    const B g1 = fma_(B(2), a32, a21);
+    const B g2 = fma_(B(2), a32, mul_(B(-0.5), a43));
+    if (SCHEME == SCHEME_Z) return weno_z_combine_dq(is0, is1, is2, g0, g1, g2, f2);
+    return weno_js_combine_dq(is0, is1, is2, g0, g1, g2, f2);
 }
 
 // 13/12 D^2 as (sqrt(13/12) D)^2
@@ -368,17 +368,17 @@ template <int DIR>
 __device__ __forceinline__ void split_eq(int riemann, const SplitCell &s, int e, double qe,
                                          double &fp, double &fm) {
     if (riemann == RIEMANN_LF) {
-        const double un = s.a[0], lam = s.a[1];
-        double f;
+        // F+- = F/2 +- (lambda/2) q, the halves taken first (exact)
+        const double hun = mul_(0.5, s.a[0]), hlam = mul_(0.5, s.a[1]);
+        double hf;
         if (e == 4)
-            f = mul_(un, add_(qe, s.p));
+            hf = mul_(hun, add_(qe, s.p));
         else if (e == 1 + DIR)
-            f = fma_(un, qe, s.p);
+            hf = fma_(hun, qe, mul_(0.5, s.p));
         else
-            f = mul_(un, qe);
-        const double t = mul_(lam, qe);
-        fp = mul_(0.5, add_(f, t));
-        fm = mul_(0.5, sub_(f, t));
+            hf = mul_(hun, qe);
+        fp = fma_(hlam, qe, hf);
+        fm = fma_(-hlam, qe, hf);
         return;
     }
     fp = mul_(s.a[0], qe);

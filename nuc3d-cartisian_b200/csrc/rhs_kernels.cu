@@ -142,6 +142,11 @@ struct InvGeom {
     static constexpr int S = (NF + R - 1) / R;  // DIR 0 interleave stride
     static constexpr int NT = TL * NR;          // threads
     static constexpr int SF = DIR == 0 ? TL * R * S : NF * TL;  // staged values per flux
+    // WENO5: the staged tile (~52 KB) admits 4 blocks per SM; blocks of up to
+    // 256 threads are held to the registers that keep all 4 resident, larger
+    // ones to 64 registers per thread.  WENO7's faces need more registers
+    // than that and are left unconstrained.
+    static constexpr int MINB = H > 3 ? 1 : (NT <= 256 ? 4 : 1024 / NT);
     // thread -> (line, run)
     __device__ static void thread(int t, int &l, int &r) {
         if (DIR == 0) {
@@ -188,9 +193,9 @@ struct InvGeom {
 // rounding to FP32.  WENO5 commutes with adding a constant and the constant
 // cancels in the face difference, so this only removes rounding error.
 template <int SCHEME, int DIR, typename B, int RUN>
-__global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
-    k_inviscid(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, int in_slot,
-               int accumulate) {
+__device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
+                                              const WorkItem *__restrict__ items, int in_slot,
+                                              int accumulate) {
     constexpr int H = scheme_halo(SCHEME);
     using G = InvGeom<DIR, B, RUN, H>;
     constexpr int TL = G::TL, TC = G::TC, NF = G::NF, R = G::R, NR = G::NR, NT = G::NT;
@@ -237,18 +242,18 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
         for (int e = 0; e < 5; ++e) Q[e] = qbase[e * np + g];
         const double un = wbase[DIR * np + g], p = wbase[3 * np + g], c = wbase[4 * np + g];
         if (riemann == RIEMANN_LF) {  // block-uniform
-            // physicsModel.cpp:546-565, spelt out for all five equations
-            const double lam = add_(fabs(un), c);
-            double f[5];
+            // physicsModel.cpp:546-565, spelt out for all five equations:
+            // F+- = F/2 +- (lambda/2) Q with the halves taken first (exact)
+            const double hun = mul_(0.5, un), hlam = mul_(0.5, add_(fabs(un), c));
+            double hf[5];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) f[e] = mul_(un, Q[e]);
-            f[1 + DIR] = fma_(un, Q[1 + DIR], p);
-            f[4] = mul_(un, add_(Q[4], p));
+            for (int e = 0; e < 4; ++e) hf[e] = mul_(hun, Q[e]);
+            hf[1 + DIR] = fma_(hun, Q[1 + DIR], mul_(0.5, p));
+            hf[4] = mul_(hun, add_(Q[4], p));
 #pragma unroll
             for (int e = 0; e < 5; ++e) {
-                const double t = mul_(lam, Q[e]);
-                Fp[e] = mul_(0.5, add_(f[e], t));
-                Fm[e] = mul_(0.5, sub_(f[e], t));
+                Fp[e] = fma_(hlam, Q[e], hf[e]);
+                Fm[e] = fma_(-hlam, Q[e], hf[e]);
             }
         } else {
             SplitCell sc;
@@ -316,6 +321,14 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
     const int nbr = DIR == 0 ? nbr_l * NR + nbr_r : nbr_r * TL + nbr_l;
 #pragma unroll 1
     for (int e = 0; e < 5; ++e) {
+        // the RHS values this equation adds to (y, z), loaded before the faces
+        // so that their latency hides behind the reconstruction
+        B racc[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const int gc = c0 + m0 + k;
+            racc[k] = (accumulate && line_ok && gc < n) ? rbase[gidx(l, gc) + e * np] : B(0);
+        }
         B Fh[R + 1];
         if constexpr (SCHEME == SCHEME_W7) {
             // face m: '+' reads positions m..m+6 (cells m-4..m+2), '-' reads
@@ -425,11 +438,35 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT)
                 if (gc >= n) break;
                 B hi = (k + 1 < R) ? Fh[k + 1] : next;
                 B dfe = mul_(sub_(hi, Fh[k]), inv_d);
-                long long g = gidx(l, gc) + e * np;
-                rbase[g] = accumulate ? add_(rbase[g], dfe) : dfe;
+                rbase[gidx(l, gc) + e * np] = accumulate ? add_(racc[k], dfe) : dfe;
             }
         }
     }
+}
+
+// The WENO5 sweeps carry a register cap (InvGeom::MINB); the WENO7 sweep is
+// compiled without one (its own kernel, so that the register allocation is
+// left to the compiler's default).
+template <int SCHEME, int DIR, typename B, int RUN>
+__global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT, InvGeom<DIR, B, RUN>::MINB)
+    k_inviscid(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, int in_slot,
+               int accumulate) {
+    inviscid_body<SCHEME, DIR, B, RUN>(boxes, items, in_slot, accumulate);
+}
+template <int DIR, typename B, int RUN>
+__global__ void __launch_bounds__(InvGeom<DIR, B, RUN, 4>::NT)
+    k_inviscid_w7(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items,
+                  int in_slot, int accumulate) {
+    inviscid_body<SCHEME_W7, DIR, B, RUN>(boxes, items, in_slot, accumulate);
+}
+
+using InvKernel = void (*)(const BoxDev *, const WorkItem *, int, int);
+template <int SCHEME, int DIR, typename B, int RUN>
+static InvKernel inv_kernel() {
+    if constexpr (SCHEME == SCHEME_W7)
+        return k_inviscid_w7<DIR, B, RUN>;
+    else
+        return k_inviscid<SCHEME, DIR, B, RUN>;
 }
 
 // --------------------------------------------------------------- launches --
@@ -452,7 +489,7 @@ static cudaError_t launch_t(const BoxDev *boxes, const WorkItem *items, int nite
                             int accumulate, cudaStream_t st) {
     using G = InvGeom<DIR, B, RUN, scheme_halo(SCHEME)>;
     if (nitems <= 0) return cudaSuccess;
-    k_inviscid<SCHEME, DIR, B, RUN><<<nitems, G::NT, inv_smem_t<SCHEME, DIR, B, RUN>(), st>>>(
+    inv_kernel<SCHEME, DIR, B, RUN>()<<<nitems, G::NT, inv_smem_t<SCHEME, DIR, B, RUN>(), st>>>(
         boxes, items, in_slot, accumulate);
     return cudaGetLastError();
 }
@@ -492,7 +529,7 @@ cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxe
 
 template <int SCHEME, int DIR, typename B, int RUN>
 static cudaError_t prepare_t() {
-    return cudaFuncSetAttribute(k_inviscid<SCHEME, DIR, B, RUN>,
+    return cudaFuncSetAttribute(inv_kernel<SCHEME, DIR, B, RUN>(),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)inv_smem_t<SCHEME, DIR, B, RUN>());
 }
