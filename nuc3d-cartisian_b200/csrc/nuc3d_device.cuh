@@ -689,6 +689,37 @@ __device__ __forceinline__ void viscosity(const BoxParams &bp, B T, B &miu, B &c
     coeff = m / B((bp.gamma - 1.0) * bp.mach * bp.mach * bp.prandtl);
 }
 
+// The same coefficients with the box's constants formed once per block:
+// Sutherland as ((1 + Tref)/Re) T sqrt(T) / (T + Tref) with one correctly
+// rounded reciprocal, and the divisions by Re and by (gamma-1) M^2 Pr as
+// multiplications by their reciprocals (each within an ulp or two of the
+// reference's divisions).
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+template <typename B>
+struct ViscConst {
+    int model;
+    B tr, suth, inv_re, pexp, heat;
+    __device__ explicit ViscConst(const BoxParams &bp)
+        : model(bp.visc_model),
+          tr(B(bp.tref_nd)),
+          suth(B((1.0 + bp.tref_nd) / bp.reynolds)),
+          inv_re(B(1.0 / bp.reynolds)),
+          pexp(B(bp.powerlaw_exp)),
+          heat(B(1.0 / ((bp.gamma - 1.0) * bp.mach * bp.mach * bp.prandtl))) {}
+    __device__ __forceinline__ void eval(B T, B &miu, B &coeff) const {
+        B m;
+        if (model == VISC_SUTHERLAND)
+            m = suth * (T * sqrt(T)) * rcp_rn(T + tr);
+        else if (model == VISC_CONSTANT)
+            m = inv_re;
+        else
+            m = pow(T, pexp) * inv_re;
+        miu = m;
+        coeff = m * heat;
+    }
+};
+
 // atomic max of a non-negative double (its bit pattern orders as an integer)
 __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
     atomicMax(reinterpret_cast<unsigned long long *>(addr),

@@ -30,20 +30,33 @@ __global__ void __launch_bounds__(256, 4) k_prim(const BoxDev *__restrict__ boxe
     const bool fabs_p = (bp.quirks & QK_FABS_PRESSURE) != 0;
     const long long n0 = (long long)it.a * kPrimChunk, n1 = n0 + it.b;
     const double gM2 = gamma * Mach * Mach;
-    for (long long n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
+    // the next cell's state is loaded while the current one is converted
+    long long n = n0 + threadIdx.x;
+    double Qn[5];
+#pragma unroll
+    for (int e = 0; e < 5; ++e) Qn[e] = n < n1 ? q[e * np + n] : 1.0;
+    for (; n < n1; n += blockDim.x) {
+        double Q[5];
+#pragma unroll
+        for (int e = 0; e < 5; ++e) Q[e] = Qn[e];
+        const long long nxt = n + blockDim.x;
+        if (nxt < n1) {
+#pragma unroll
+            for (int e = 0; e < 5; ++e) Qn[e] = q[e * np + nxt];
+        }
         // one correctly rounded reciprocal of rho in place of the reference's
         // five divisions (results within an ulp of them)
-        double rho = q[n];
-        double ri = __drcp_rn(rho);
-        double u = q[np + n] * ri;
-        double v = q[2 * np + n] * ri;
-        double ww = q[3 * np + n] * ri;
-        double E = q[4 * np + n];
+        const double rho = Q[0];
+        const double ri = __drcp_rn(rho);
+        const double u = Q[1] * ri;
+        const double v = Q[2] * ri;
+        const double ww = Q[3] * ri;
+        const double E = Q[4];
         double p = (E - 0.5 * rho * (u * u + v * v + ww * ww)) * (gamma - 1.0);
         if (fabs_p) p = fabs(p);
-        double pr = p * ri;
-        double c = sqrt(gamma * pr);
-        double T = gM2 * pr;
+        const double pr = p * ri;
+        const double c = sqrt(gamma * pr);
+        const double T = gM2 * pr;
         w[n] = u;
         w[np + n] = v;
         w[2 * np + n] = ww;
@@ -144,9 +157,9 @@ struct InvGeom {
     static constexpr int SF = DIR == 0 ? TL * R * S : NF * TL;  // staged values per flux
     // WENO5: the staged tile (~52 KB) admits 4 blocks per SM; blocks of up to
     // 256 threads are held to the registers that keep all 4 resident, larger
-    // ones to 64 registers per thread.  WENO7's faces need more registers
-    // than that and are left unconstrained.
-    static constexpr int MINB = H > 3 ? 1 : (NT <= 256 ? 4 : 1024 / NT);
+    // ones to 64 registers per thread.  (WENO7's sweep has its own kernel
+    // without a register cap.)
+    static constexpr int MINB = NT <= 256 ? 4 : 1024 / NT;
     // thread -> (line, run)
     __device__ static void thread(int t, int &l, int &r) {
         if (DIR == 0) {
@@ -282,19 +295,7 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
         __syncthreads();
     }
     // phase 1: stage the split fluxes of cells c0-H .. c0+TC+H-1
-    for (int t = threadIdx.x; t < TL * NF; t += NT) {
-        int l, pc;
-        G::stage_item(t, l, pc);
-        double Fp[5], Fm[5];
-        if (l0 + l < nl) {
-            int pos = c0 - H + pc;  // in [-H, n + NF): wrap without a division (n >= 8 > H)
-            if (pos < 0) pos += n;
-            while (pos >= n) pos -= n;
-            split(gidx(l, pos), Fp, Fm);
-        } else {
-#pragma unroll
-            for (int e = 0; e < 5; ++e) Fp[e] = Fm[e] = 0.0;
-        }
+    auto stage_store = [&](int l, int pc, const double Fp[5], const double Fm[5]) {
 #pragma unroll
         for (int e = 0; e < 5; ++e) {
             if (mixed) {
@@ -305,6 +306,26 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
                 sF[G::sf(5 + e, l, pc)] = B(Fm[e]);
             }
         }
+    };
+    // position of staged cell pc in the box: in [-H, n + NF), wrapped
+    // without a division (n >= 8 > H)
+    auto stage_pos = [&](int pc) {
+        int pos = c0 - H + pc;
+        if (pos < 0) pos += n;
+        while (pos >= n) pos -= n;
+        return pos;
+    };
+    for (int t = threadIdx.x; t < TL * NF; t += NT) {
+        int l, pc;
+        G::stage_item(t, l, pc);
+        double Fp[5], Fm[5];
+        if (l0 + l < nl) {
+            split(gidx(l, stage_pos(pc)), Fp, Fm);
+        } else {
+#pragma unroll
+            for (int e = 0; e < 5; ++e) Fp[e] = Fm[e] = 0.0;
+        }
+        stage_store(l, pc, Fp, Fm);
     }
     __syncthreads();
     // phase 2: runs of faces.  Face m (local) lies between cells c0+m-1 and
@@ -359,70 +380,153 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
                 }
             }
         } else {
-            // WENO5: the window carries the first differences a_ij, the second
-            // differences D and dd = 13/12 D^2 of the current stencil, so each
-            // new face adds one value, one difference, one second difference
-            // and one square (weno5_face_dq).
-            {  // '+' side: stencil f0..f4 = positions m..m+4
-                const int v = e;
-                B f0 = sF[G::sf(v, l, m0)], f1 = sF[G::sf(v, l, m0 + 1)];
-                B f2 = sF[G::sf(v, l, m0 + 2)], f3 = sF[G::sf(v, l, m0 + 3)];
-                B f4 = sF[G::sf(v, l, m0 + 4)];
-                B a10 = sub_(f1, f0), a21 = sub_(f2, f1), a32 = sub_(f3, f2), a43 = sub_(f4, f3);
-                B D0 = sub_(a21, a10), D1 = sub_(a32, a21), D2 = sub_(a43, a32);
-                B dd0 = dd_of(D0), dd1 = dd_of(D1), dd2 = dd_of(D2);
-#pragma unroll
-                for (int k = 0; k <= R; ++k) {
-                    if (k == R && !last) break;
+            // FP64 runs of 4 faces step both windows together; the others step
+            // them one after the other (measured faster for FP32, and the joint
+            // form does not fit the 64-register budget of FP64 runs of 1 or 2)
+            constexpr bool joint = sizeof(B) == 8 && R == 4;
+            if constexpr (joint) {
+                // WENO5: each window carries the first differences a_ij, the second
+                // differences D and dd = 13/12 D^2 of its current stencil, so each
+                // new face adds one value, one difference, one second difference
+                // and one square (weno5_face_dq).  The '+' stencil of face m is
+                // positions m..m+4, the '-' stencil m+5..m+1; both windows step
+                // together so that each face offers two independent chains.
+                const int vp = e, vm = 5 + e;
+                B p2 = sF[G::sf(vp, l, m0 + 2)], p3 = sF[G::sf(vp, l, m0 + 3)];
+                B p4 = sF[G::sf(vp, l, m0 + 4)];
+                B pa21, pa32, pa43, pD0, pD1, pD2;
+                {
+                    const B p0 = sF[G::sf(vp, l, m0)], p1 = sF[G::sf(vp, l, m0 + 1)];
+                    const B pa10 = sub_(p1, p0);
+                    pa21 = sub_(p2, p1);
+                    pa32 = sub_(p3, p2);
+                    pa43 = sub_(p4, p3);
+                    pD0 = sub_(pa21, pa10);
+                    pD1 = sub_(pa32, pa21);
+                    pD2 = sub_(pa43, pa32);
+                }
+                B pdd0 = dd_of(pD0), pdd1 = dd_of(pD1), pdd2 = dd_of(pD2);
+                B q0 = sF[G::sf(vm, l, m0 + 5)], q1 = sF[G::sf(vm, l, m0 + 4)];
+                B q2 = sF[G::sf(vm, l, m0 + 3)];
+                B qa10, qa21, qa32, qa43, qD0, qD1, qD2;
+                {
+                    const B q3 = sF[G::sf(vm, l, m0 + 2)], q4 = sF[G::sf(vm, l, m0 + 1)];
+                    qa10 = sub_(q1, q0);
+                    qa21 = sub_(q2, q1);
+                    qa32 = sub_(q3, q2);
+                    qa43 = sub_(q4, q3);
+                    qD0 = sub_(qa21, qa10);
+                    qD1 = sub_(qa32, qa21);
+                    qD2 = sub_(qa43, qa32);
+                }
+                B qdd0 = dd_of(qD0), qdd1 = dd_of(qD1), qdd2 = dd_of(qD2);
+                auto face = [&](int k) {
                     const int gm = c0 + m0 + k;
                     // weno5z.cpp:80 on the inner '+' faces 3..n-3: beta2's first
                     // term reads f2 - 2 f3 + f3 = -a32
-                    const B dd2s = (zq && gm >= 3 && gm <= n - 3) ? dd_of(a32) : dd2;
-                    Fh[k] = weno5_face_dq<SCHEME, B>(f2, a21, a32, a43, D0, D2, dd0, dd1, dd2s);
-                    if (k < R) {
-                        f2 = f3;
-                        f3 = f4;
-                        f4 = sF[G::sf(v, l, m0 + k + 5)];
-                        a21 = a32;
-                        a32 = a43;
-                        a43 = sub_(f4, f3);
-                        D0 = D1;
-                        D1 = D2;
-                        D2 = sub_(a43, a32);
-                        dd0 = dd1;
-                        dd1 = dd2;
-                        dd2 = dd_of(D2);
+                    const B dd2s = (zq && gm >= 3 && gm <= n - 3) ? dd_of(pa32) : pdd2;
+                    const B fp = weno5_face_dq<SCHEME, B>(p2, pa21, pa32, pa43, pD0, pD2, pdd0, pdd1, dd2s);
+                    const B fm = weno5_face_dq<SCHEME, B>(q2, qa21, qa32, qa43, qD0, qD2, qdd0, qdd1, qdd2);
+                    return add_(fp, fm);
+                };
+    #pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    Fh[k] = face(k);
+                    // '+' gains position m0+k+5, '-' gains position m0+k+6
+                    p2 = p3;
+                    p3 = p4;
+                    p4 = sF[G::sf(vp, l, m0 + k + 5)];
+                    pa21 = pa32;
+                    pa32 = pa43;
+                    pa43 = sub_(p4, p3);
+                    pD0 = pD1;
+                    pD1 = pD2;
+                    pD2 = sub_(pa43, pa32);
+                    pdd0 = pdd1;
+                    pdd1 = pdd2;
+                    pdd2 = dd_of(pD2);
+                    const B qn = (m0 + k + 6 < NF) ? sF[G::sf(vm, l, m0 + k + 6)] : B(0);
+                    q2 = q1;
+                    q1 = q0;
+                    q0 = qn;
+                    qa43 = qa32;
+                    qa32 = qa21;
+                    qa21 = qa10;
+                    qa10 = sub_(q1, q0);
+                    qD2 = qD1;
+                    qD1 = qD0;
+                    qD0 = sub_(qa21, qa10);
+                    qdd2 = qdd1;
+                    qdd1 = qdd0;
+                    qdd0 = dd_of(qD0);
+                }
+                if (last) Fh[R] = face(R);
+            } else {
+                // WENO5: the window carries the first differences a_ij, the second
+                // differences D and dd = 13/12 D^2 of the current stencil, so each
+                // new face adds one value, one difference, one second difference
+                // and one square (weno5_face_dq).
+                {  // '+' side: stencil f0..f4 = positions m..m+4
+                    const int v = e;
+                    B f0 = sF[G::sf(v, l, m0)], f1 = sF[G::sf(v, l, m0 + 1)];
+                    B f2 = sF[G::sf(v, l, m0 + 2)], f3 = sF[G::sf(v, l, m0 + 3)];
+                    B f4 = sF[G::sf(v, l, m0 + 4)];
+                    B a10 = sub_(f1, f0), a21 = sub_(f2, f1), a32 = sub_(f3, f2), a43 = sub_(f4, f3);
+                    B D0 = sub_(a21, a10), D1 = sub_(a32, a21), D2 = sub_(a43, a32);
+                    B dd0 = dd_of(D0), dd1 = dd_of(D1), dd2 = dd_of(D2);
+    #pragma unroll
+                    for (int k = 0; k <= R; ++k) {
+                        if (k == R && !last) break;
+                        const int gm = c0 + m0 + k;
+                        // weno5z.cpp:80 on the inner '+' faces 3..n-3: beta2's first
+                        // term reads f2 - 2 f3 + f3 = -a32
+                        const B dd2s = (zq && gm >= 3 && gm <= n - 3) ? dd_of(a32) : dd2;
+                        Fh[k] = weno5_face_dq<SCHEME, B>(f2, a21, a32, a43, D0, D2, dd0, dd1, dd2s);
+                        if (k < R) {
+                            f2 = f3;
+                            f3 = f4;
+                            f4 = sF[G::sf(v, l, m0 + k + 5)];
+                            a21 = a32;
+                            a32 = a43;
+                            a43 = sub_(f4, f3);
+                            D0 = D1;
+                            D1 = D2;
+                            D2 = sub_(a43, a32);
+                            dd0 = dd1;
+                            dd1 = dd2;
+                            dd2 = dd_of(D2);
+                        }
                     }
                 }
-            }
-            {  // '-' side: stencil f0..f4 = positions m+5..m+1
-                const int v = 5 + e;
-                B f0 = sF[G::sf(v, l, m0 + 5)], f1 = sF[G::sf(v, l, m0 + 4)];
-                B f2 = sF[G::sf(v, l, m0 + 3)], f3 = sF[G::sf(v, l, m0 + 2)];
-                B f4 = sF[G::sf(v, l, m0 + 1)];
-                B a10 = sub_(f1, f0), a21 = sub_(f2, f1), a32 = sub_(f3, f2), a43 = sub_(f4, f3);
-                B D0 = sub_(a21, a10), D1 = sub_(a32, a21), D2 = sub_(a43, a32);
-                B dd0 = dd_of(D0), dd1 = dd_of(D1), dd2 = dd_of(D2);
-#pragma unroll
-                for (int k = 0; k <= R; ++k) {
-                    if (k == R && !last) break;
-                    Fh[k] = add_(Fh[k], weno5_face_dq<SCHEME, B>(f2, a21, a32, a43, D0, D2, dd0,
-                                                                 dd1, dd2));
-                    if (k < R) {
-                        const B fn = (m0 + k + 6 < NF) ? sF[G::sf(v, l, m0 + k + 6)] : B(0);
-                        f2 = f1;
-                        f1 = f0;
-                        f0 = fn;
-                        a43 = a32;
-                        a32 = a21;
-                        a21 = a10;
-                        a10 = sub_(f1, f0);
-                        D2 = D1;
-                        D1 = D0;
-                        D0 = sub_(a21, a10);
-                        dd2 = dd1;
-                        dd1 = dd0;
-                        dd0 = dd_of(D0);
+                {  // '-' side: stencil f0..f4 = positions m+5..m+1
+                    const int v = 5 + e;
+                    B f0 = sF[G::sf(v, l, m0 + 5)], f1 = sF[G::sf(v, l, m0 + 4)];
+                    B f2 = sF[G::sf(v, l, m0 + 3)], f3 = sF[G::sf(v, l, m0 + 2)];
+                    B f4 = sF[G::sf(v, l, m0 + 1)];
+                    B a10 = sub_(f1, f0), a21 = sub_(f2, f1), a32 = sub_(f3, f2), a43 = sub_(f4, f3);
+                    B D0 = sub_(a21, a10), D1 = sub_(a32, a21), D2 = sub_(a43, a32);
+                    B dd0 = dd_of(D0), dd1 = dd_of(D1), dd2 = dd_of(D2);
+    #pragma unroll
+                    for (int k = 0; k <= R; ++k) {
+                        if (k == R && !last) break;
+                        Fh[k] = add_(Fh[k], weno5_face_dq<SCHEME, B>(f2, a21, a32, a43, D0, D2, dd0,
+                                                                     dd1, dd2));
+                        if (k < R) {
+                            const B fn = (m0 + k + 6 < NF) ? sF[G::sf(v, l, m0 + k + 6)] : B(0);
+                            f2 = f1;
+                            f1 = f0;
+                            f0 = fn;
+                            a43 = a32;
+                            a32 = a21;
+                            a21 = a10;
+                            a10 = sub_(f1, f0);
+                            D2 = D1;
+                            D1 = D0;
+                            D0 = sub_(a21, a10);
+                            dd2 = dd1;
+                            dd1 = dd0;
+                            dd0 = dd_of(D0);
+                        }
                     }
                 }
             }

@@ -99,57 +99,66 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
     const double ix = bp.inv_d[0], iy = bp.inv_d[1], iz = bp.inv_d[2];
     const B c23 = B(2.0 / 3.0);
     const bool od = (bp.quirks & QK_OFFDIAG_DIV) != 0;
-    for (int k = k0; k < kend; ++k) {
-        const int buf = (k - k0) & 1;
-        if (k + 1 < kend) issue(k + 1, buf ^ 1);
-        cp_async_commit();
-        cp_async_wait1();
-        __syncthreads();
+    const ViscConst<B> vc(bp);
+    // The z queue is a ring of 7 register slots: plane k+s-3 sits in slot
+    // (k-k0+s) % 7.  The plane loop is unrolled by 7 so that every slot index
+    // is a constant and the ring turns without register moves.
+    for (int kb = k0; kb < kend; kb += 7) {
 #pragma unroll
-        for (int f = 0; f < 4; ++f) qz[f][6] = active ? sZ[buf][f][tid] : 0.0;
-        if (active) {
-            B gr[4][3];
+        for (int u = 0; u < 7; ++u) {
+            const int k = kb + u;
+            if (k >= kend) break;  // block-uniform
+            const int buf = (k - k0) & 1;
+            if (k + 1 < kend) issue(k + 1, buf ^ 1);
+            cp_async_commit();
+            cp_async_wait1();
+            __syncthreads();
+            // slot of plane k+s-3 (kb - k0 is a multiple of 7)
+#define QZ(f, s) qz[f][(u + (s)) % 7]
 #pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                const int r = ty + 3, c = tx + 3;
-                const double(*P)[TX + 6] = sP[buf][f];
-                gr[f][0] = B(cd6d(P[r][c - 3], P[r][c - 2], P[r][c - 1], P[r][c + 1], P[r][c + 2],
-                                  P[r][c + 3], ix));
-                gr[f][1] = B(cd6d(P[r - 3][c], P[r - 2][c], P[r - 1][c], P[r + 1][c], P[r + 2][c],
-                                  P[r + 3][c], iy));
-                gr[f][2] = B(cd6d(qz[f][0], qz[f][1], qz[f][2], qz[f][4], qz[f][5], qz[f][6], iz));
+            for (int f = 0; f < 4; ++f) QZ(f, 6) = active ? sZ[buf][f][tid] : 0.0;
+            if (active) {
+                B gr[4][3];
+#pragma unroll
+                for (int f = 0; f < 4; ++f) {
+                    const int r = ty + 3, c = tx + 3;
+                    const double(*P)[TX + 6] = sP[buf][f];
+                    gr[f][0] = B(cd6d(P[r][c - 3], P[r][c - 2], P[r][c - 1], P[r][c + 1],
+                                      P[r][c + 2], P[r][c + 3], ix));
+                    gr[f][1] = B(cd6d(P[r - 3][c], P[r - 2][c], P[r - 1][c], P[r + 1][c],
+                                      P[r + 2][c], P[r + 3][c], iy));
+                    gr[f][2] = B(cd6d(QZ(f, 0), QZ(f, 1), QZ(f, 2), QZ(f, 4), QZ(f, 5), QZ(f, 6),
+                                      iz));
+                }
+                B ux = gr[0][0], uy = gr[0][1], uz = gr[0][2];
+                B vx = gr[1][0], vy = gr[1][1], vz = gr[1][2];
+                B wx = gr[2][0], wy = gr[2][1], wz = gr[2][2];
+                B tx_ = gr[3][0], ty_ = gr[3][1], tz_ = gr[3][2];
+                B grad = ux + vy + wz;
+                B miu0, coeff0;
+                vc.eval(B(QZ(3, 3)), miu0, coeff0);
+                B dv = od ? c23 * grad : B(0);
+                B t_xx = miu0 * (B(2) * ux - c23 * grad);
+                B t_xy = miu0 * (uy + vx - dv);
+                B t_xz = miu0 * (uz + wx - dv);
+                B t_yy = miu0 * (B(2) * vy - c23 * grad);
+                B t_yz = miu0 * (vz + wy - dv);
+                B t_zz = miu0 * (B(2) * wz - c23 * grad);
+                B uu = B(QZ(0, 3)), v = B(QZ(1, 3)), ww = B(QZ(2, 3));
+#undef QZ
+                long long g = col + sz * k;
+                vbase[0 * np + g] = t_xx;
+                vbase[1 * np + g] = t_xy;
+                vbase[2 * np + g] = t_xz;
+                vbase[3 * np + g] = t_yy;
+                vbase[4 * np + g] = t_yz;
+                vbase[5 * np + g] = t_zz;
+                vbase[6 * np + g] = uu * t_xx + v * t_xy + ww * t_xz + coeff0 * tx_;
+                vbase[7 * np + g] = uu * t_xy + v * t_yy + ww * t_yz + coeff0 * ty_;
+                vbase[8 * np + g] = uu * t_xz + v * t_yz + ww * t_zz + coeff0 * tz_;
             }
-            B ux = gr[0][0], uy = gr[0][1], uz = gr[0][2];
-            B vx = gr[1][0], vy = gr[1][1], vz = gr[1][2];
-            B wx = gr[2][0], wy = gr[2][1], wz = gr[2][2];
-            B tx_ = gr[3][0], ty_ = gr[3][1], tz_ = gr[3][2];
-            B grad = ux + vy + wz;
-            B miu0, coeff0;
-            viscosity<B>(bp, B(qz[3][3]), miu0, coeff0);
-            B dv = od ? c23 * grad : B(0);
-            B t_xx = miu0 * (B(2) * ux - c23 * grad);
-            B t_xy = miu0 * (uy + vx - dv);
-            B t_xz = miu0 * (uz + wx - dv);
-            B t_yy = miu0 * (B(2) * vy - c23 * grad);
-            B t_yz = miu0 * (vz + wy - dv);
-            B t_zz = miu0 * (B(2) * wz - c23 * grad);
-            B u = B(qz[0][3]), v = B(qz[1][3]), ww = B(qz[2][3]);
-            long long g = col + sz * k;
-            vbase[0 * np + g] = t_xx;
-            vbase[1 * np + g] = t_xy;
-            vbase[2 * np + g] = t_xz;
-            vbase[3 * np + g] = t_yy;
-            vbase[4 * np + g] = t_yz;
-            vbase[5 * np + g] = t_zz;
-            vbase[6 * np + g] = u * t_xx + v * t_xy + ww * t_xz + coeff0 * tx_;
-            vbase[7 * np + g] = u * t_xy + v * t_yy + ww * t_yz + coeff0 * ty_;
-            vbase[8 * np + g] = u * t_xz + v * t_yz + ww * t_zz + coeff0 * tz_;
+            __syncthreads();
         }
-        __syncthreads();
-#pragma unroll
-        for (int s = 0; s < 6; ++s)
-#pragma unroll
-            for (int f = 0; f < 4; ++f) qz[f][s] = qz[f][s + 1];
     }
 }
 
