@@ -261,7 +261,7 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));
     const bool mixed = precision_ == NUC3D_MIXED;
     std::vector<BoxDev> table(boxes_.size());
-    std::vector<WorkItem> prim, st25, inv[kSchemes][3], cr[2][3];
+    std::vector<WorkItem> prim, prim_step, st25, inv[kSchemes][3], cr[2][3];
     const int crtl = crweno_tile_lines();
     for (int c = 0; c < 2; ++c)
         for (int d = 0; d < 3; ++d) cr_nmax_[c][d] = cr_ms_[c][d] = 0;
@@ -280,6 +280,8 @@ int Engine::rebuild() {
         for (long long c = 0; c * kPrimChunk < p.N; ++c)
             prim.push_back({id, (int)c, (int)std::min<long long>(kPrimChunk, p.N - c * kPrimChunk), 0});
         boxes_[i].prim_n = (int)prim.size() - boxes_[i].prim_off;
+        if (p.scheme[0] == SCHEME_CR || p.scheme[0] == SCHEME_HC)
+            prim_step.insert(prim_step.end(), prim.end() - boxes_[i].prim_n, prim.end());
         for (int z = 0; z < ceil_div(p.n[2], kT25Z); ++z)
             for (int y = 0; y < ceil_div(p.n[1], kT25Y); ++y)
                 for (int x = 0; x < ceil_div(p.n[0], kT25X); ++x) st25.push_back({id, x, y, z});
@@ -327,6 +329,7 @@ int Engine::rebuild() {
         all.insert(all.end(), v.begin(), v.end());
     };
     append(prim, r_prim_);
+    append(prim_step, r_prim_step_);
     append(st25, r_25d_);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) append(inv[s][d], r_inv_[s][d]);
@@ -354,7 +357,7 @@ int Engine::rebuild() {
     ECK(prepare_inviscid_kernels(mixed));
     ECK(prepare_crweno_kernels(mixed));
     ECK(prepare_stencil_kernels(mixed));
-    int per_stage = (r_prim_.n > 0) + (any_visc_ && r_25d_.n > 0) + (r_25d_.n > 0);
+    int per_stage = (r_prim_step_.n > 0) + (any_visc_ && r_25d_.n > 0) + (r_25d_.n > 0);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d].n > 0;
     for (int c = 0; c < 2; ++c)
@@ -415,10 +418,26 @@ int Engine::enqueue_step_t(cudaStream_t st) {
     }
     for (int stage = 0; stage < 3; ++stage) {
         const int in = stage, out = (stage + 1) % 3;
-        {
+        // primitives of the boxes whose x lines run the line kernel; the x
+        // sweep recovers those of the other boxes (and their eigenvalues on
+        // the first stage) while staging
+        if (r_prim_step_.n > 0) {
             ProfScope ps(this, NUC3D_PROF_PRIM);
-            ECK(launch_prim(d_boxes_, it + r_prim_.off, r_prim_.n, in, stage == 0, st));
+            ECK(launch_prim(d_boxes_, it + r_prim_step_.off, r_prim_step_.n, in, stage == 0, st));
         }
+        auto sweeps = [&](int d) -> int {
+            ProfScope ps(this, NUC3D_PROF_INV_X + d);
+            for (int s = 0; s < kSchemes; ++s)
+                ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
+                                        r_inv_[s][d].n, in, d > 0,
+                                        d == 0 ? (stage == 0 ? 2 : 1) : 0, st)));
+            for (int c = 0; c < 2; ++c)
+                ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_,
+                                      it + r_cr_[c][d].off, r_cr_[c][d].n, in, d > 0,
+                                      cr_nmax_[c][d], cr_ms_[c][d], st)));
+            return NUC3D_OK;
+        };
+        if (int rc = sweeps(0)) return rc;
         if (stage == 0) {
             ProfScope ps(this, NUC3D_PROF_DT);
             ECK(launch_dt(d_boxes_, nb, st));
@@ -427,16 +446,8 @@ int Engine::enqueue_step_t(cudaStream_t st) {
             ProfScope ps(this, NUC3D_PROF_VISC);
             ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_.off, r_25d_.n, st)));
         }
-        for (int d = 0; d < 3; ++d) {
-            ProfScope ps(this, NUC3D_PROF_INV_X + d);
-            for (int s = 0; s < kSchemes; ++s)
-                ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
-                                        r_inv_[s][d].n, in, d > 0, st)));
-            for (int c = 0; c < 2; ++c)
-                ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_,
-                                      it + r_cr_[c][d].off, r_cr_[c][d].n, in, d > 0,
-                                      cr_nmax_[c][d], cr_ms_[c][d], st)));
-        }
+        for (int d = 1; d < 3; ++d)
+            if (int rc = sweeps(d)) return rc;
         ECK(enqueue_forcing<B>(st));
         {
             ProfScope ps(this, NUC3D_PROF_UPDATE);
@@ -504,9 +515,9 @@ int Engine::autotune() {
             for (int v = 0; v < kInvVariants; ++v) {
                 auto go = [&]() {
                     return mixed ? launch_inviscid<float>(s, d, v, d_boxes_, d_items_ + rg.off, rg.n,
-                                                          0, d > 0, stream_)
+                                                          0, d > 0, 0, stream_)
                                  : launch_inviscid<double>(s, d, v, d_boxes_, d_items_ + rg.off,
-                                                           rg.n, 0, d > 0, stream_);
+                                                           rg.n, 0, d > 0, 0, stream_);
                 };
                 cudaError_t err = go();  // warm-up
                 err = err == cudaSuccess ? cudaEventRecord(e0, stream_) : err;
@@ -612,7 +623,7 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
     for (int d = 0; d < 3; ++d) {
         for (int s = 0; s < kSchemes; ++s)
             ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
-                                    r_inv_[s][d].n, 0, d > 0, stream_)));
+                                    r_inv_[s][d].n, 0, d > 0, 0, stream_)));
         for (int c = 0; c < 2; ++c)
             ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_, it + r_cr_[c][d].off,
                                   r_cr_[c][d].n, 0, d > 0, cr_nmax_[c][d], cr_ms_[c][d],

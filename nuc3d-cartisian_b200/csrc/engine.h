@@ -105,6 +105,9 @@ private:
         int n = 0;
     };
     Range r_prim_, r_25d_, r_inv_[kSchemes][3];  // [scheme JS/Z/-/W7][dir]
+    // k_prim items of the boxes whose x direction runs the line kernel; the
+    // x sweep (k_inviscid) recovers the primitives of the other boxes itself
+    Range r_prim_step_;
     // line-solve tiles per [scheme: 0 crweno5, 1 hccs][dir], with the longest
     // line and the rows per lane that size each launch's shared memory
     Range r_cr_[2][3];

@@ -12,62 +12,49 @@
 namespace nuc3d {
 
 // ----------------------------------------------------------------- k_prim --
-// physicsModel::con2prim (physicsModel.cpp:324-356), FP64, plus the running
-// maxEigen of RiemannLF (physicsModel.cpp:546-547, 600-601, 653-654).  A work
-// item is (box, first cell, cell count).
-__global__ void __launch_bounds__(256, 4) k_prim(const BoxDev *__restrict__ boxes,
-                                                 const WorkItem *__restrict__ items, int in_slot,
-                                                 int want_eig) {
-    const WorkItem it = items[blockIdx.x];
-    const BoxDev &bd = boxes[it.box];
-    if (!bd.active) return;
-    const BoxParams &bp = bd.p;
+// physicsModel::con2prim (physicsModel.cpp:324-356) of one cell, FP64, with
+// one correctly rounded reciprocal of rho in place of the reference's five
+// divisions (each result within an ulp or two of the reference's).  k_prim
+// and the x sweep (which recovers the primitives of its tile while staging)
+// share it, so both give bitwise the same W.
+struct PrimConst {
+    double gamma, gm1, gM2;
+    bool fabs_p;
+    __device__ explicit PrimConst(const BoxParams &bp)
+        : gamma(bp.gamma), gm1(bp.gamma - 1.0), gM2(bp.gamma * bp.mach * bp.mach),
+          fabs_p((bp.quirks & QK_FABS_PRESSURE) != 0) {}
+};
+struct PrimCell {
+    double u, v, w, p, c, T;
+};
+__device__ __forceinline__ void prim_cell(const PrimConst &k, const double Q[5], PrimCell &o) {
+    const double ri = __drcp_rn(Q[0]);
+    o.u = mul_(Q[1], ri);
+    o.v = mul_(Q[2], ri);
+    o.w = mul_(Q[3], ri);
+    // p = (E - rho/2 (u^2 + v^2 + w^2)) (gamma - 1)
+    const double q2 = fma_(o.w, o.w, fma_(o.v, o.v, mul_(o.u, o.u)));
+    double p = mul_(fma_(mul_(-0.5, Q[0]), q2, Q[4]), k.gm1);
+    if (k.fabs_p) p = fabs(p);
+    o.p = p;
+    const double pr = mul_(p, ri);
+    o.c = sqrt(mul_(k.gamma, pr));
+    o.T = mul_(k.gM2, pr);
+}
+__device__ __forceinline__ void prim_store(const BoxDev &bd, long long g, const PrimCell &o) {
+    double *const w = fieldW(bd, 0);
     const long long np = bd.np;
-    const double *__restrict__ q = fieldU(bd, in_slot, 0);
-    double *__restrict__ w = fieldW(bd, 0);
-    double lx = 0.0, ly = 0.0, lz = 0.0;
-    const double gamma = bp.gamma, Mach = bp.mach;
-    const bool fabs_p = (bp.quirks & QK_FABS_PRESSURE) != 0;
-    const long long n0 = (long long)it.a * kPrimChunk, n1 = n0 + it.b;
-    const double gM2 = gamma * Mach * Mach;
-    // the next cell's state is loaded while the current one is converted
-    long long n = n0 + threadIdx.x;
-    double Qn[5];
-#pragma unroll
-    for (int e = 0; e < 5; ++e) Qn[e] = n < n1 ? q[e * np + n] : 1.0;
-    for (; n < n1; n += blockDim.x) {
-        double Q[5];
-#pragma unroll
-        for (int e = 0; e < 5; ++e) Q[e] = Qn[e];
-        const long long nxt = n + blockDim.x;
-        if (nxt < n1) {
-#pragma unroll
-            for (int e = 0; e < 5; ++e) Qn[e] = q[e * np + nxt];
-        }
-        // one correctly rounded reciprocal of rho in place of the reference's
-        // five divisions (results within an ulp of them)
-        const double rho = Q[0];
-        const double ri = __drcp_rn(rho);
-        const double u = Q[1] * ri;
-        const double v = Q[2] * ri;
-        const double ww = Q[3] * ri;
-        const double E = Q[4];
-        double p = (E - 0.5 * rho * (u * u + v * v + ww * ww)) * (gamma - 1.0);
-        if (fabs_p) p = fabs(p);
-        const double pr = p * ri;
-        const double c = sqrt(gamma * pr);
-        const double T = gM2 * pr;
-        w[n] = u;
-        w[np + n] = v;
-        w[2 * np + n] = ww;
-        w[3 * np + n] = p;
-        w[4 * np + n] = c;
-        w[5 * np + n] = T;
-        lx = fmax(fabs(u) + c, lx);
-        ly = fmax(fabs(v) + c, ly);
-        lz = fmax(fabs(ww) + c, lz);
-    }
-    if (!want_eig) return;
+    w[g] = o.u;
+    w[np + g] = o.v;
+    w[2 * np + g] = o.w;
+    w[3 * np + g] = o.p;
+    w[4 * np + g] = o.c;
+    w[5 * np + g] = o.T;
+}
+// the running maxEigen of RiemannLF (physicsModel.cpp:546-547, 600-601,
+// 653-654) reduced over a block and folded into the box's maxima
+__device__ __forceinline__ void eig_block_max(const BoxDev &bd, double lx, double ly, double lz) {
+    const BoxParams &bp = bd.p;
     if ((bp.quirks & QK_ZETA_EIGEN) && bp.riemann == RIEMANN_LF) {
         // RiemannLF's z loop writes MaxEigen_eta; zeta stays 0 (the AUSM
         // loops keep their own directions)
@@ -79,8 +66,8 @@ __global__ void __launch_bounds__(256, 4) k_prim(const BoxDev *__restrict__ boxe
         ly = fmax(ly, __shfl_xor_sync(0xffffffffu, ly, o));
         lz = fmax(lz, __shfl_xor_sync(0xffffffffu, lz, o));
     }
-    __shared__ double red[3][8];
-    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ double red[3][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (lane == 0) {
         red[0][warp] = lx;
         red[1][warp] = ly;
@@ -97,6 +84,43 @@ __global__ void __launch_bounds__(256, 4) k_prim(const BoxDev *__restrict__ boxe
         atomic_max_nonneg(&bd.eig[1], ly);
         atomic_max_nonneg(&bd.eig[2], lz);
     }
+}
+
+// A work item is (box, first cell chunk, cell count).
+__global__ void __launch_bounds__(256, 4) k_prim(const BoxDev *__restrict__ boxes,
+                                                 const WorkItem *__restrict__ items, int in_slot,
+                                                 int want_eig) {
+    const WorkItem it = items[blockIdx.x];
+    const BoxDev &bd = boxes[it.box];
+    if (!bd.active) return;
+    const long long np = bd.np;
+    const double *__restrict__ q = fieldU(bd, in_slot, 0);
+    const PrimConst pk(bd.p);
+    double lx = 0.0, ly = 0.0, lz = 0.0;
+    const long long n0 = (long long)it.a * kPrimChunk, n1 = n0 + it.b;
+    // the next cell's state is loaded while the current one is converted
+    long long n = n0 + threadIdx.x;
+    double Qn[5];
+#pragma unroll
+    for (int e = 0; e < 5; ++e) Qn[e] = n < n1 ? q[e * np + n] : 1.0;
+    for (; n < n1; n += blockDim.x) {
+        double Q[5];
+#pragma unroll
+        for (int e = 0; e < 5; ++e) Q[e] = Qn[e];
+        const long long nxt = n + blockDim.x;
+        if (nxt < n1) {
+#pragma unroll
+            for (int e = 0; e < 5; ++e) Qn[e] = q[e * np + nxt];
+        }
+        PrimCell o;
+        prim_cell(pk, Q, o);
+        prim_store(bd, n, o);
+        lx = fmax(add_(fabs(o.u), o.c), lx);
+        ly = fmax(add_(fabs(o.v), o.c), ly);
+        lz = fmax(add_(fabs(o.w), o.c), lz);
+    }
+    if (!want_eig) return;
+    eig_block_max(bd, lx, ly, lz);
 }
 
 __global__ void k_clear_eig(const BoxDev *boxes, int nboxes) {
@@ -208,7 +232,7 @@ struct InvGeom {
 template <int SCHEME, int DIR, typename B, int RUN>
 __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
                                               const WorkItem *__restrict__ items, int in_slot,
-                                              int accumulate) {
+                                              int accumulate, int prim_mode) {
     constexpr int H = scheme_halo(SCHEME);
     using G = InvGeom<DIR, B, RUN, H>;
     constexpr int TL = G::TL, TC = G::TC, NF = G::NF, R = G::R, NR = G::NR, NT = G::NT;
@@ -249,11 +273,35 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
         return a + sy * fixed + sz * pos;
     };
     const int riemann = bp.riemann;
-    auto split = [&](long long g, double Fp[5], double Fm[5]) {
+    // prim_mode (x sweep only): 0 reads u_n, p, c from W; 1 recovers the
+    // primitives from the state (prim_cell) and writes W for the tile's own
+    // cells; 2 also folds their eigenvalues into the box's maxima
+    const bool own_prim = DIR == 0 && prim_mode != 0;
+    const PrimConst pk(bp);
+    double eg[3] = {0.0, 0.0, 0.0};
+    // split fluxes of cell g; store: g is one of the tile's own cells
+    auto split = [&](long long g, double Fp[5], double Fm[5], bool store) {
         double Q[5];
 #pragma unroll
         for (int e = 0; e < 5; ++e) Q[e] = qbase[e * np + g];
-        const double un = wbase[DIR * np + g], p = wbase[3 * np + g], c = wbase[4 * np + g];
+        double un, p, c;
+        if (own_prim) {
+            PrimCell o;
+            prim_cell(pk, Q, o);
+            un = o.u;
+            p = o.p;
+            c = o.c;
+            if (store) {
+                prim_store(bd, g, o);
+                eg[0] = fmax(add_(fabs(o.u), o.c), eg[0]);
+                eg[1] = fmax(add_(fabs(o.v), o.c), eg[1]);
+                eg[2] = fmax(add_(fabs(o.w), o.c), eg[2]);
+            }
+        } else {
+            un = wbase[DIR * np + g];
+            p = wbase[3 * np + g];
+            c = wbase[4 * np + g];
+        }
         if (riemann == RIEMANN_LF) {  // block-uniform
             // physicsModel.cpp:546-565, spelt out for all five equations:
             // F+- = F/2 +- (lambda/2) Q with the halves taken first (exact)
@@ -281,7 +329,7 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
             int l = threadIdx.x;
             double Fp[5], Fm[5];
             if (l0 + l < nl) {
-                split(gidx(l, c0), Fp, Fm);
+                split(gidx(l, c0), Fp, Fm, false);
             } else {
 #pragma unroll
                 for (int e = 0; e < 5; ++e) Fp[e] = Fm[e] = 0.0;
@@ -320,7 +368,9 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
         G::stage_item(t, l, pc);
         double Fp[5], Fm[5];
         if (l0 + l < nl) {
-            split(gidx(l, stage_pos(pc)), Fp, Fm);
+            // the tile's own cells: staged positions H .. H+TC-1 inside the box
+            const bool own = pc >= H && pc < H + TC && c0 + pc - H < n;
+            split(gidx(l, stage_pos(pc)), Fp, Fm, own);
         } else {
 #pragma unroll
             for (int e = 0; e < 5; ++e) Fp[e] = Fm[e] = 0.0;
@@ -546,6 +596,7 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
             }
         }
     }
+    if (own_prim && prim_mode == 2) eig_block_max(bd, eg[0], eg[1], eg[2]);
 }
 
 // The WENO5 sweeps carry a register cap (InvGeom::MINB); the WENO7 sweep is
@@ -554,17 +605,17 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
 template <int SCHEME, int DIR, typename B, int RUN>
 __global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT, InvGeom<DIR, B, RUN>::MINB)
     k_inviscid(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, int in_slot,
-               int accumulate) {
-    inviscid_body<SCHEME, DIR, B, RUN>(boxes, items, in_slot, accumulate);
+               int accumulate, int prim_mode) {
+    inviscid_body<SCHEME, DIR, B, RUN>(boxes, items, in_slot, accumulate, prim_mode);
 }
 template <int DIR, typename B, int RUN>
 __global__ void __launch_bounds__(InvGeom<DIR, B, RUN, 4>::NT)
     k_inviscid_w7(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items,
-                  int in_slot, int accumulate) {
-    inviscid_body<SCHEME_W7, DIR, B, RUN>(boxes, items, in_slot, accumulate);
+                  int in_slot, int accumulate, int prim_mode) {
+    inviscid_body<SCHEME_W7, DIR, B, RUN>(boxes, items, in_slot, accumulate, prim_mode);
 }
 
-using InvKernel = void (*)(const BoxDev *, const WorkItem *, int, int);
+using InvKernel = void (*)(const BoxDev *, const WorkItem *, int, int, int);
 template <int SCHEME, int DIR, typename B, int RUN>
 static InvKernel inv_kernel() {
     if constexpr (SCHEME == SCHEME_W7)
@@ -590,43 +641,43 @@ InvTileDims inviscid_tile(int dir, bool mixed) {
 
 template <int SCHEME, int DIR, typename B, int RUN>
 static cudaError_t launch_t(const BoxDev *boxes, const WorkItem *items, int nitems, int in_slot,
-                            int accumulate, cudaStream_t st) {
+                            int accumulate, int prim_mode, cudaStream_t st) {
     using G = InvGeom<DIR, B, RUN, scheme_halo(SCHEME)>;
     if (nitems <= 0) return cudaSuccess;
     inv_kernel<SCHEME, DIR, B, RUN>()<<<nitems, G::NT, inv_smem_t<SCHEME, DIR, B, RUN>(), st>>>(
-        boxes, items, in_slot, accumulate);
+        boxes, items, in_slot, accumulate, prim_mode);
     return cudaGetLastError();
 }
 
 template <int SCHEME, int DIR, typename B>
 static cudaError_t launch_v(int variant, const BoxDev *boxes, const WorkItem *items, int nitems,
-                            int in_slot, int accumulate, cudaStream_t st) {
+                            int in_slot, int accumulate, int prim_mode, cudaStream_t st) {
     switch (variant) {
-        case 0: return launch_t<SCHEME, DIR, B, 1>(boxes, items, nitems, in_slot, accumulate, st);
-        case 1: return launch_t<SCHEME, DIR, B, 2>(boxes, items, nitems, in_slot, accumulate, st);
-        default: return launch_t<SCHEME, DIR, B, 4>(boxes, items, nitems, in_slot, accumulate, st);
+        case 0: return launch_t<SCHEME, DIR, B, 1>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        case 1: return launch_t<SCHEME, DIR, B, 2>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        default: return launch_t<SCHEME, DIR, B, 4>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
     }
 }
 
 template <typename B>
 cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxes,
                             const WorkItem *items, int nitems, int in_slot, int accumulate,
-                            cudaStream_t st) {
+                            int prim_mode, cudaStream_t st) {
     if (nitems <= 0) return cudaSuccess;
     if (scheme == SCHEME_JS) {
-        if (dir == 0) return launch_v<SCHEME_JS, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
-        if (dir == 1) return launch_v<SCHEME_JS, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
-        return launch_v<SCHEME_JS, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+        if (dir == 0) return launch_v<SCHEME_JS, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        if (dir == 1) return launch_v<SCHEME_JS, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        return launch_v<SCHEME_JS, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
     }
     if (scheme == SCHEME_Z) {
-        if (dir == 0) return launch_v<SCHEME_Z, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
-        if (dir == 1) return launch_v<SCHEME_Z, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
-        return launch_v<SCHEME_Z, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+        if (dir == 0) return launch_v<SCHEME_Z, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        if (dir == 1) return launch_v<SCHEME_Z, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        return launch_v<SCHEME_Z, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
     }
     if (scheme == SCHEME_W7) {
-        if (dir == 0) return launch_v<SCHEME_W7, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
-        if (dir == 1) return launch_v<SCHEME_W7, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
-        return launch_v<SCHEME_W7, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, st);
+        if (dir == 0) return launch_v<SCHEME_W7, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        if (dir == 1) return launch_v<SCHEME_W7, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        return launch_v<SCHEME_W7, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -684,7 +735,7 @@ cudaError_t launch_residual(const BoxDev *boxes, int nboxes, cudaStream_t st) {
 }
 
 template cudaError_t launch_inviscid<double>(int, int, int, const BoxDev *, const WorkItem *, int,
-                                             int, int, cudaStream_t);
+                                             int, int, int, cudaStream_t);
 template cudaError_t launch_inviscid<float>(int, int, int, const BoxDev *, const WorkItem *, int,
-                                            int, int, cudaStream_t);
+                                            int, int, int, cudaStream_t);
 }  // namespace nuc3d

@@ -103,10 +103,14 @@ constexpr int kInvVariants = 3;
 // scheme slots of the per-scheme sweep tables (indexed by scheme id; the
 // CRWENO5 slot stays empty, its lines run in launch_crweno)
 constexpr int kSchemes = 4;
+// prim_mode (x sweep only): 0 reads the primitives W; 1 recovers them from
+// the state while staging and writes W for the tile's own cells (k_prim's
+// work, bitwise the same); 2 also folds their eigenvalues into the boxes'
+// running maxima (k_prim with want_eig)
 template <typename B>
 cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxes,
                             const WorkItem *items, int nitems, int in_slot, int accumulate,
-                            cudaStream_t st);
+                            int prim_mode, cudaStream_t st);
 // raises the dynamic shared-memory limit of the viscous-flux kernel
 cudaError_t prepare_stencil_kernels(bool mixed);
 template <typename B>
