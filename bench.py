@@ -58,14 +58,18 @@ CFL = 0.5
 # (2 WENO5-Z faces of 76 flops + F^+ + F^- add + difference 2) + LF split 33.
 FLOPS_INV_Z = 5 * (2 * 76 + 1 + 2) + 33
 FLOPS_INV_JS = 5 * (2 * 68 + 1 + 2) + 33
-FLOPS_PER_CELL_STAGE = 3 * FLOPS_INV_Z + 20 + 156 + 111  # + prim, viscous flux, update
+FLOPS_PRIM = 20  # con2prim + eigenvalues, done by the x sweep while staging
+FLOPS_PER_CELL_STAGE = 3 * FLOPS_INV_Z + FLOPS_PRIM + 156 + 111  # + viscous flux, update
+# algorithmic flops of the average sweep launch (x, y, z; x carries con2prim)
+FLOPS_INV_LAUNCH = FLOPS_INV_Z + FLOPS_PRIM / 3
 STATE_BYTES_PER_CELL_UPDATE = 320  # compulsory FP64 state traffic of 3 RK stages
 # DRAM bytes (read + write) per launch of the FP64 WENO5-Z sweep at 256^3,
 # mean of x, y, z: the ncu capture at 128^3 in
-# profiles/k_inviscid_weno5z_fp64_128.md (186.4, 270.9, 278.2 MB) scaled by the
-# cell count (x8); the traffic of a sweep is proportional to the cells it
-# covers (whole lines, no halo growth with size along the other axes).
-INV_TRAFFIC_BYTES = 8 * (186.44e6 + 270.89e6 + 278.18e6) / 3
+# profiles/k_inviscid_weno5z_fp64_128.md (212.5, 270.0, 277.6 MB; the x sweep
+# reads the state only and writes the primitives as well as its RHS) scaled
+# by the cell count (x8); the traffic of a sweep is proportional to the cells
+# it covers (whole lines, no halo growth with size along the other axes).
+INV_TRAFFIC_BYTES = 8 * (212.489472e6 + 270.013184e6 + 277.586176e6) / 3
 INV_TRAFFIC_NOTE = "ncu dram__bytes_read+write of the 128^3 capture x8 (cells), mean of x/y/z"
 
 
@@ -244,10 +248,10 @@ def run_b200(args, rank, world, local_rank):
     inv_n = sum(prof[k][1] for k in ("inv_x", "inv_y", "inv_z"))
     total_ms = sum(v[0] for v in prof.values())
     inv_avg_ms = inv_ms / max(inv_n, 1)
-    achieved = FLOPS_INV_Z * cells / (inv_avg_ms * 1e-3) / 1e12
+    achieved = FLOPS_INV_LAUNCH * cells / (inv_avg_ms * 1e-3) / 1e12
     roofline = {
         "bound": "fp64",
-        "kernel": "k_inviscid<WENO5-Z, FP64> (directional sweep, x/y/z)",
+        "kernel": "k_inviscid<WENO5-Z, FP64> (directional sweep, x/y/z; x also recovers the primitives)",
         "achieved": achieved,
         "peak": peak64,
         "unit": "TFLOP/s",
@@ -256,7 +260,7 @@ def run_b200(args, rank, world, local_rank):
         "traffic": INV_TRAFFIC_BYTES,
         "traffic_source": INV_TRAFFIC_NOTE,
         "traffic_gbs": INV_TRAFFIC_BYTES / (inv_avg_ms * 1e-3) / 1e9,
-        "flops_per_launch": FLOPS_INV_Z * cells,
+        "flops_per_launch": FLOPS_INV_LAUNCH * cells,
         "avg_launch_ms": inv_avg_ms,
         "share_of_step": inv_ms / total_ms if total_ms else None,
         "kernel_ms_per_step": {k: v[0] / 2 for k, v in prof.items()},

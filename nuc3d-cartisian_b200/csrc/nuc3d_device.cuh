@@ -199,12 +199,15 @@ __device__ __forceinline__ float weno_z_combine(float is0, float is1, float is2,
 // linear weights are 0.1 (1, 6, 3); the 0.1 cancels in the ratio and the 6
 // and 3 go with the candidates, so the caller passes g = (dq0, 6 dq1, 3 dq2)
 // and the face is f2 + (w0 g0 + w1 g1 + w2 g2) / (w0 + 6 w1 + 3 w2) with w_k
-// the weights without their linear factor.  WENO5-Z's (beta + 1e-40)^2 is
-// formed as beta^2 + 1e-80 (the cross term is below 1e-40 of beta).
+// the weights without their linear factor.  The indicators arrive scaled by
+// 4 (is_k = 4 beta_k, see weno5_face_dq) and eps with them, an exact scaling
+// that leaves every weight ratio bitwise unchanged.  WENO5-Z's
+// (beta + 1e-40)^2 is formed as beta^2 + 1e-80 (the cross term is below
+// 1e-40 of beta).
 __device__ __forceinline__ double weno_js_combine_dq(double is0, double is1, double is2,
                                                      double g0, double g1, double g2,
                                                      double f2) {
-    const double ss = 1.0e-6;
+    const double ss = 4.0 * 1.0e-6;  // 4 eps
     double s0 = add_(ss, is0), s1 = add_(ss, is1), s2 = add_(ss, is2);
     s0 = mul_(s0, s0);
     s1 = mul_(s1, s1);
@@ -215,7 +218,7 @@ __device__ __forceinline__ double weno_js_combine_dq(double is0, double is1, dou
 }
 __device__ __forceinline__ float weno_js_combine_dq(float is0, float is1, float is2, float g0,
                                                     float g1, float g2, float f2) {
-    const float ss = 1.0e-6f;
+    const float ss = 4.0f * 1.0e-6f;  // 4 eps
     float r0 = frcp_fast(add_(ss, is0)), r1 = frcp_fast(add_(ss, is1)), r2 = frcp_fast(add_(ss, is2));
     const float a0 = mul_(r0, r0), a1 = mul_(r1, r1), a2 = mul_(r2, r2);
     return fma_(fma_(a2, g2, fma_(a1, g1, mul_(a0, g0))),
@@ -224,7 +227,7 @@ __device__ __forceinline__ float weno_js_combine_dq(float is0, float is1, float 
 __device__ __forceinline__ double weno_z_combine_dq(double is0, double is1, double is2,
                                                     double g0, double g1, double g2,
                                                     double f2) {
-    const double ss2 = 1.0e-80;  // eps^2, eps = 1e-40
+    const double ss2 = 16.0 * 1.0e-80;  // (4 eps)^2, eps = 1e-40
     double tau = fabs(sub_(is2, is0));
     double t2 = mul_(tau, tau);
     double s0 = fma_(is0, is0, ss2), s1 = fma_(is1, is1, ss2), s2 = fma_(is2, is2, ss2);
@@ -237,7 +240,7 @@ __device__ __forceinline__ double weno_z_combine_dq(double is0, double is1, doub
 }
 __device__ __forceinline__ float weno_z_combine_dq(float is0, float is1, float is2, float g0,
                                                    float g1, float g2, float f2) {
-    const float ss = 1.0e-30f, cap = 1.0e15f;
+    const float ss = 4.0f * 1.0e-30f, cap = 1.0e15f;  // 4 eps
     float tau = fabsf(sub_(is2, is0));
     float t0 = fminf(mul_(tau, frcp_fast(add_(is0, ss))), cap);
     float t1 = fminf(mul_(tau, frcp_fast(add_(is1, ss))), cap);
@@ -249,21 +252,20 @@ __device__ __forceinline__ float weno_z_combine_dq(float is0, float is1, float i
 
 // One WENO5 face (either scheme) from the sliding window's differences:
 // a_ij = f_i - f_j of the upwind-oriented stencil f0..f4, the second
-// differences D0 = f0 - 2 f1 + f2 and D2 = f2 - 2 f3 + f4, and dd_k =
-// 13/12 D_k^2 (the indicators' first terms, carried from face to face).
-// With e_k the indicators' second terms halved (schemes.hpp:33-34 with the
-// 1/4 taken as (E/2)^2):
-//   e0 = D0/2 + a21,  e1 = -(a21 + a32)/2,  e2 = D2/2 - a32,
-//   beta_k = dd_k + e_k^2,
+// differences D0 = f0 - 2 f1 + f2 and D2 = f2 - 2 f3 + f4, and dd_k (the
+// indicators' first terms, carried from face to face).  The indicators are formed times 4 (schemes.hpp:33-34 with the 1/4 of the
+// second term absorbed): with E_k the second terms' differences,
+//   E0 = D0 + 2 a21,  E1 = -(a21 + a32) (its sign drops in the square),
+//   E2 = D2 - 2 a32,   4 beta_k = dd_k + E_k^2,  dd_k = 4 (13/12) D_k^2,
 // and the candidates (schemes.hpp:14-18) as f2 + dq_k:
 //   dq0 = D0/3 + a21/2,  6 dq1 = a21 + 2 a32,  3 dq2 = 2 a32 - a43/2.
 template <int SCHEME, typename B>
 __device__ __forceinline__ B weno5_face_dq(B f2, B a21, B a32, B a43, B D0, B D2, B dd0, B dd1,
                                            B dd2) {
     const B h = B(0.5);
-    const B e0 = fma_(h, D0, a21);
-    const B e1 = mul_(B(-0.5), add_(a21, a32));
-    const B e2 = fma_(h, D2, -a32);
+    const B e0 = fma_(B(2), a21, D0);
+    const B e1 = add_(a21, a32);
+    const B e2 = fma_(B(-2), a32, D2);
     const B is0 = fma_(e0, e0, dd0), is1 = fma_(e1, e1, dd1), is2 = fma_(e2, e2, dd2);
     const B g0 = fma_(B(1.0 / 3.0), D0, mul_(h, a21));
     const B g1 = fma_(B(2), a32, a21);
@@ -272,10 +274,11 @@ __device__ __forceinline__ B weno5_face_dq(B f2, B a21, B a32, B a43, B D0, B D2
     return weno_js_combine_dq(is0, is1, is2, g0, g1, g2, f2);
 }
 
-// 13/12 D^2 as (sqrt(13/12) D)^2
+// 4 (13/12) D^2 as (2 sqrt(13/12) D)^2 (the sweeps' indicators are formed
+// times 4)
 template <typename B>
 __device__ __forceinline__ B dd_of(B D) {
-    const B t = mul_(B(K::SG0), D);
+    const B t = mul_(B(2.0 * K::SG0), D);
     return mul_(t, t);
 }
 

@@ -1,8 +1,11 @@
 // Batched whole-box kernels: primitive recovery, dt, residual and the
 // directional WENO5 / WENO7 sweeps.
 //
-// One RK stage = k_prim -> [k_visc_flux25] -> k_inviscid<x> -> k_inviscid<y>
-// -> k_inviscid<z> -> k_update25, each one launch for every box of a batch.
+// One RK stage = k_inviscid<x> (which recovers the primitives of its tiles:
+// k_prim's work; k_prim itself runs first for boxes whose x lines use the
+// line kernel) -> [k_dt on the first stage] -> [k_visc_flux25] ->
+// k_inviscid<y> -> k_inviscid<z> -> k_update25, each one launch for every
+// box of a batch.
 // The reference's per-direction rotated copies, halo buffers and MPI
 // self-messages (euler3d.cpp:307-387, NaiverStokes3d.cpp:87-369,
 // MPICommunicator.cpp:81-132) become periodic index wraps in the tile loads.
@@ -436,7 +439,7 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
             constexpr bool joint = sizeof(B) == 8 && R == 4;
             if constexpr (joint) {
                 // WENO5: each window carries the first differences a_ij, the second
-                // differences D and dd = 13/12 D^2 of its current stencil, so each
+                // differences D and dd = 4 (13/12) D^2 of its current stencil, so each
                 // new face adds one value, one difference, one second difference
                 // and one square (weno5_face_dq).  The '+' stencil of face m is
                 // positions m..m+4, the '-' stencil m+5..m+1; both windows step
@@ -513,7 +516,7 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
                 if (last) Fh[R] = face(R);
             } else {
                 // WENO5: the window carries the first differences a_ij, the second
-                // differences D and dd = 13/12 D^2 of the current stencil, so each
+                // differences D and dd = 4 (13/12) D^2 of the current stencil, so each
                 // new face adds one value, one difference, one second difference
                 // and one square (weno5_face_dq).
                 {  // '+' side: stencil f0..f4 = positions m..m+4
