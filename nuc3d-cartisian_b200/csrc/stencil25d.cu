@@ -181,6 +181,12 @@ __global__ void __launch_bounds__(TX *TY, 2)
     __shared__ B sX[2][4][TY][TX + 6];
     __shared__ B sY[2][4][TY + 6][TX];
     __shared__ double red[TX * TY / 32];
+    // periodic wraps of the tile's columns and rows with their 3-cell halos
+    // (x: i index; y: row offset j nx), resolved once per block.  FP32 only:
+    // in the FP64 instance (at its register limit) the table lookups cost
+    // register spills that outweigh the remainders they save.
+    constexpr bool wrap_table = sizeof(B) == 4;
+    __shared__ int sWx[TX + 6], sWy[TY + 6];
     const int cx[4] = {0, 1, 2, 6}, cy[4] = {1, 3, 4, 7}, cz[4] = {2, 4, 5, 8};
     const WorkItem it = items[blockIdx.x];
     const BoxDev &bd = boxes[it.box];
@@ -205,17 +211,29 @@ __global__ void __launch_bounds__(TX *TY, 2)
     const double dt = sc->dt;
     const B ixb = B(bp.inv_d[0]), iyb = B(bp.inv_d[1]), izb = B(bp.inv_d[2]);
     const int kend = min(k0 + KZ, nz);
+    if constexpr (wrap_table) {
+        if (tid < TX + 6) sWx[tid] = pmod(i0 - 3 + tid, nx);
+        if (tid < TY + 6) sWy[tid] = nx * pmod(j0 - 3 + tid, ny);
+        __syncthreads();
+    }
+    // in-plane offset of tile position (xx, yy) relative to (i0 - 3, j0 - 3)
+    auto wxy = [&](int xx, int yy) -> long long {
+        if constexpr (wrap_table)
+            return sWx[xx] + sWy[yy];
+        else
+            return pmod(i0 - 3 + xx, nx) + (long long)nx * pmod(j0 - 3 + yy, ny);
+    };
     auto issue = [&](int k, int buf) {
         const long long plane = sz * k;
         for (int t = tid; t < TY * (TX + 6); t += TX * TY) {
             int yy = t / (TX + 6), xx = t - yy * (TX + 6);
-            long long g = plane + pmod(i0 - 3 + xx, nx) + (long long)nx * pmod(j0 + yy, ny);
+            long long g = plane + wxy(xx, yy + 3);
 #pragma unroll
             for (int f = 0; f < 4; ++f) cp_async_elem(&sX[buf][f][yy][xx], vbase + cx[f] * np + g);
         }
         for (int t = tid; t < (TY + 6) * TX; t += TX * TY) {
             int yy = t / TX, xx = t - yy * TX;
-            long long g = plane + pmod(i0 + xx, nx) + (long long)nx * pmod(j0 - 3 + yy, ny);
+            long long g = plane + wxy(xx + 3, yy);
 #pragma unroll
             for (int f = 0; f < 4; ++f) cp_async_elem(&sY[buf][f][yy][xx], vbase + cy[f] * np + g);
         }
