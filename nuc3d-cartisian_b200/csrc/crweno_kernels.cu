@@ -25,6 +25,8 @@
 // without normalising the weights (a row may be scaled freely), so a row
 // costs one reciprocal.  The face values overwrite the staged fluxes, and
 // the block writes dF/dx.
+#include <type_traits>
+
 #include "nuc3d_device.cuh"
 #include "rhs_kernels.h"
 
@@ -237,29 +239,9 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
         __syncthreads();
 
         if (l0 + line < nl) {  // warp-uniform
-            auto F = [&](int c) -> B { return myF[c + H]; };
-            // the sign (warp-uniform) only selects which cells feed a
-            // stencil ('+' reads upwind from the left, '-' from the right)
-            const int dir = sg == 0 ? 1 : -1;
-            // explicit face m: WENO5-JS (crweno5.cpp:425-837) or hccs's WENO7
-            // (hccs.cpp:538-980)
-            auto js = [&](int m) -> B {
-                if (SCH == SCHEME_HC) {
-                    const int c0 = sg == 0 ? m - 4 : m + 3;
-                    return weno7_face_hc(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
-                                         F(c0 + 4 * dir), F(c0 + 5 * dir), F(c0 + 6 * dir));
-                }
-                const int c0 = sg == 0 ? m - 3 : m + 2;
-                return weno5js_face(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
-                                    F(c0 + 4 * dir));
-            };
             // explicit faces of the bounded system: 0..H-1 and n-H+1..n
             int xm = -1;
             B xv = B(0);
-            if (bounded && hl < 2 * H) {
-                xm = hl < H ? hl : n - 2 * H + 1 + hl;
-                xv = js(xm);
-            }
             // segment of this lane: rows r0 .. r1 (at least 2)
             const bool act = hl < P;
             const int r0 = act ? (hl * N) / P : 0;
@@ -267,88 +249,117 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
             const int L = r1 - r0 + 1;
             B fa = B(0), fc = B(0), fd = B(0);  // reduced unit-diagonal row of x_first
             B la = B(0), lc = B(0), ld = B(0);  // reduced unit-diagonal row of x_last
-            if (act) {
-                // window w[k] = F(i - 2 + k) of the current row's cell i (face i + 1)
-                int i = bounded ? r0 + H - 1 : r0 - 1;
-                B w[6];
-#pragma unroll
-                for (int k = 0; k < 6; ++k) w[k] = F(i - 2 + k);
-                auto gen = [&](int r, B &a, B &b, B &c, B &d) {
-                    if (bounded && (r == 0 || r == N - 1)) {
-                        a = B(0);
-                        b = B(1);
-                        c = B(0);
-                        d = js(r + H);
-                    } else {
-                        // '+': cells i-2..i+2 = w[0..4]; '-': cells i+3..i-1 = w[5..1]
-                        // with the off-diagonals swapped (crweno5.cpp:335-338)
-                        const bool m = sg != 0;
-                        B lo, hi;
-                        if (SCH == SCHEME_HC)
-                            hc_row(m ? w[5] : w[0], m ? w[4] : w[1], m ? w[3] : w[2],
-                                   m ? w[2] : w[3], m ? w[1] : w[4], lo, b, hi, d);
-                        else
-                            cr_row(m ? w[5] : w[0], m ? w[4] : w[1], m ? w[3] : w[2],
-                                   m ? w[2] : w[3], m ? w[1] : w[4], lo, b, hi, d);
-                        a = m ? hi : lo;
-                        c = m ? lo : hi;
+            // the row work of one sign; the sign (warp-uniform) is a compile-time
+            // constant inside, so each warp runs code without sign selects
+            auto segment = [&](auto sign) {
+                constexpr int S = decltype(sign)::value;
+                auto F = [&](int c) -> B { return myF[c + H]; };
+                // the sign (warp-uniform) only selects which cells feed a
+                // stencil ('+' reads upwind from the left, '-' from the right)
+                constexpr int dir = S == 0 ? 1 : -1;
+                // explicit face m: WENO5-JS (crweno5.cpp:425-837) or hccs's WENO7
+                // (hccs.cpp:538-980)
+                auto js = [&](int m) -> B {
+                    if (SCH == SCHEME_HC) {
+                        const int c0 = S == 0 ? m - 4 : m + 3;
+                        return weno7_face_hc(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
+                                             F(c0 + 4 * dir), F(c0 + 5 * dir), F(c0 + 6 * dir));
                     }
+                    const int c0 = S == 0 ? m - 3 : m + 2;
+                    return weno5js_face(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
+                                        F(c0 + 4 * dir));
                 };
-                auto advance = [&]() {
-#pragma unroll
-                    for (int k = 0; k < 5; ++k) w[k] = w[k + 1];
-                    ++i;
-                    w[5] = F(i + 3);
-                };
-                B a0, b0, c0, d0;
-                gen(r0, a0, b0, c0, d0);
-                // forward: row j -> A x_first + x_j + C x_{j+1} = D
-                B Ap = B(0), Cp = B(0), Dp = B(0);
-                for (int j = 1; j < L; ++j) {
-                    advance();
-                    B a, b, c, d;
-                    gen(r0 + j, a, b, c, d);
-                    B bpv = b, An = a, Dn = d;
-                    if (j > 1) {
-                        bpv = b - a * Cp;
-                        An = -a * Ap;
-                        Dn = d - a * Dp;
-                    }
-                    const B r = rcp_(bpv);
-                    Ap = An * r;
-                    Cp = c * r;
-                    Dp = Dn * r;
-                    wA[j * 32 + lane] = Ap;
-                    wC[j * 32 + lane] = Cp;
-                    wD[j * 32 + lane] = Dp;
+                if (bounded && hl < 2 * H) {
+                    xm = hl < H ? hl : n - 2 * H + 1 + hl;
+                    xv = js(xm);
                 }
-                la = Ap;
-                lc = Cp;
-                ld = Dp;
-                // backward: row j -> A x_first + x_j + C x_last = D
-                B bf = b0, cf = c0, df = d0;
-                if (L >= 3) {
-                    B An = wA[(L - 2) * 32 + lane], Cn = wC[(L - 2) * 32 + lane];
-                    B Dn = wD[(L - 2) * 32 + lane];
-                    for (int j = L - 3; j >= 1; --j) {
-                        const B k = wC[j * 32 + lane];
-                        An = wA[j * 32 + lane] - k * An;
-                        Cn = -k * Cn;
-                        Dn = wD[j * 32 + lane] - k * Dn;
-                        wA[j * 32 + lane] = An;
-                        wC[j * 32 + lane] = Cn;
-                        wD[j * 32 + lane] = Dn;
+                if (act) {
+                    // window w[k] = F(i - 2 + k) of the current row's cell i (face i + 1)
+                    int i = bounded ? r0 + H - 1 : r0 - 1;
+                    B w[6];
+    #pragma unroll
+                    for (int k = 0; k < 6; ++k) w[k] = F(i - 2 + k);
+                    auto gen = [&](int r, B &a, B &b, B &c, B &d) {
+                        if (bounded && (r == 0 || r == N - 1)) {
+                            a = B(0);
+                            b = B(1);
+                            c = B(0);
+                            d = js(r + H);
+                        } else {
+                            // '+': cells i-2..i+2 = w[0..4]; '-': cells i+3..i-1 = w[5..1]
+                            // with the off-diagonals swapped (crweno5.cpp:335-338)
+                            constexpr bool m = S != 0;
+                            B lo, hi;
+                            if (SCH == SCHEME_HC)
+                                hc_row(m ? w[5] : w[0], m ? w[4] : w[1], m ? w[3] : w[2],
+                                       m ? w[2] : w[3], m ? w[1] : w[4], lo, b, hi, d);
+                            else
+                                cr_row(m ? w[5] : w[0], m ? w[4] : w[1], m ? w[3] : w[2],
+                                       m ? w[2] : w[3], m ? w[1] : w[4], lo, b, hi, d);
+                            a = m ? hi : lo;
+                            c = m ? lo : hi;
+                        }
+                    };
+                    auto advance = [&]() {
+    #pragma unroll
+                        for (int k = 0; k < 5; ++k) w[k] = w[k + 1];
+                        ++i;
+                        w[5] = F(i + 3);
+                    };
+                    B a0, b0, c0, d0;
+                    gen(r0, a0, b0, c0, d0);
+                    // forward: row j -> A x_first + x_j + C x_{j+1} = D
+                    B Ap = B(0), Cp = B(0), Dp = B(0);
+                    for (int j = 1; j < L; ++j) {
+                        advance();
+                        B a, b, c, d;
+                        gen(r0 + j, a, b, c, d);
+                        B bpv = b, An = a, Dn = d;
+                        if (j > 1) {
+                            bpv = b - a * Cp;
+                            An = -a * Ap;
+                            Dn = d - a * Dp;
+                        }
+                        const B r = rcp_(bpv);
+                        Ap = An * r;
+                        Cp = c * r;
+                        Dp = Dn * r;
+                        wA[j * 32 + lane] = Ap;
+                        wC[j * 32 + lane] = Cp;
+                        wD[j * 32 + lane] = Dp;
                     }
-                    // row 0 minus c0 x (row 1)
-                    bf = b0 - c0 * An;
-                    cf = -c0 * Cn;
-                    df = d0 - c0 * Dn;
+                    la = Ap;
+                    lc = Cp;
+                    ld = Dp;
+                    // backward: row j -> A x_first + x_j + C x_last = D
+                    B bf = b0, cf = c0, df = d0;
+                    if (L >= 3) {
+                        B An = wA[(L - 2) * 32 + lane], Cn = wC[(L - 2) * 32 + lane];
+                        B Dn = wD[(L - 2) * 32 + lane];
+                        for (int j = L - 3; j >= 1; --j) {
+                            const B k = wC[j * 32 + lane];
+                            An = wA[j * 32 + lane] - k * An;
+                            Cn = -k * Cn;
+                            Dn = wD[j * 32 + lane] - k * Dn;
+                            wA[j * 32 + lane] = An;
+                            wC[j * 32 + lane] = Cn;
+                            wD[j * 32 + lane] = Dn;
+                        }
+                        // row 0 minus c0 x (row 1)
+                        bf = b0 - c0 * An;
+                        cf = -c0 * Cn;
+                        df = d0 - c0 * Dn;
+                    }
+                    const B r = rcp_(bf);
+                    fa = a0 * r;
+                    fc = cf * r;
+                    fd = df * r;
                 }
-                const B r = rcp_(bf);
-                fa = a0 * r;
-                fc = cf * r;
-                fd = df * r;
-            }
+            };
+            if (sg == 0)
+                segment(std::integral_constant<int, 0>{});
+            else
+                segment(std::integral_constant<int, 1>{});
             // parallel cyclic reduction of the 2P segment-end unknowns
             // (reduced row 2l: x_first of lane l, 2l+1: x_last) within the warp
             const int base = 0;

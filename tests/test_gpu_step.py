@@ -325,3 +325,35 @@ def test_oversized_box_fails_cleanly(torch):
     box = Box(16, 16, 16)
     q, _, _ = gpu_steps(box, Oracle().tgv(box), 1)
     assert np.isfinite(q[4]).all()
+
+
+@pytest.mark.parametrize("scheme", [WENO5Z, WENO7, CRWENO5])
+def test_step_equals_rhs_calls_and_rk_stages(torch, scheme):
+    """A step recovers the primitives inside its x sweep (k_prim only runs for
+    boxes whose x lines use the line kernel), while nuc3d_rhs runs k_prim
+    first.  Both use the same con2prim code, so one step equals three
+    nuc3d_rhs calls chained by nuc3d_tvdrk3_stage: the same dt bit for bit,
+    and the same state up to the RK stage's own rounding (the step's update
+    kernel and the stage kernel evaluate the same expressions)."""
+    import nuc3d_b200 as nb
+    box = Box(24, 20, 16, mach=1.0, reynolds=400.0, scheme=(scheme,) * 3)
+    with solver_for(box) as s:
+        s.init_state({"kind": "hit", "seed": 3, "k_peak": 3.0, "mach_t": 0.3})
+        q0 = s.get_state()
+        dt, _ = s.step(1, 0.5)
+        q1 = s.get_state()
+    un = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in q0]
+    ui = [a.clone() for a in un]
+    rhs = [torch.zeros(box.shape, dtype=torch.float64, device="cuda") for _ in range(5)]
+    with solver_for(box) as s:
+        for stage in range(3):
+            s.set_state([a.cpu().numpy() for a in ui])
+            dtl = s.rhs(rhs)
+            if stage == 0:
+                assert dtl * 0.5 == dt[0]
+            nb.tvdrk3_stage(stage, float(dt[0]), rhs, un, ui)
+    torch.cuda.synchronize()
+    got = [a.cpu().numpy() for a in ui]
+    for e in range(5):
+        scale = np.max(np.abs(q1[e]))
+        assert np.max(np.abs(got[e] - q1[e])) <= 4e-16 * scale, e
