@@ -584,10 +584,19 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
                 }
             }
         }
-        B *x = xb + (e & 1) * NT;
-        x[threadIdx.x] = Fh[0];
-        __syncthreads();
-        B next = last ? Fh[R] : x[nbr];
+        // the first face of the next run: in the x sweep the runs of a line
+        // are consecutive lanes of one warp (a shuffle, no barrier); in y/z
+        // the next run may sit in another warp (shared memory)
+        B next;
+        if constexpr (DIR == 0) {
+            const B nb = __shfl_down_sync(0xffffffffu, Fh[0], 1);
+            next = last ? Fh[R] : nb;
+        } else {
+            B *x = xb + (e & 1) * NT;
+            x[threadIdx.x] = Fh[0];
+            __syncthreads();
+            next = last ? Fh[R] : x[nbr];
+        }
         if (line_ok) {
 #pragma unroll
             for (int k = 0; k < R; ++k) {
