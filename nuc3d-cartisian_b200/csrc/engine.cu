@@ -1,6 +1,9 @@
 // Engine: host side of the batched solver (see engine.h).
 #include "engine.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -18,7 +21,58 @@ namespace {
 
 long long pad32(long long n) { return (n + 31) / 32 * 32; }
 size_t bulk_size(int precision) { return precision == NUC3D_MIXED ? sizeof(float) : sizeof(double); }
-constexpr size_t kSmallBytes = 256 + sizeof(StepScalars);
+// the box's small area: eig, residual sum, flags, StepScalars, then the
+// viscous-flux kernel's 8 TMA tensor maps (128-byte aligned)
+constexpr size_t kTmaOff = (256 + sizeof(StepScalars) + 127) / 128 * 128;
+constexpr size_t kSmallBytes = kTmaOff + 8 * sizeof(CUtensorMap);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); null when unavailable
+PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// Tensor maps of u, v, w, T for k_visc_flux25's TMA loads: [0..3] the tile's
+// plane with its halo (kViscTmaHaloX x kViscTmaHaloY), [4..7] the tile's own
+// columns (kViscTmaTileX x kViscTmaTileY), one plane deep.  A row must be a
+// multiple of 16 bytes (nx even); NUC3D_VISC_TMA=0 keeps the element-wise
+// cp.async loads for every tile.
+bool encode_visc_maps(const BoxDev &d, CUtensorMap out[8]) {
+    const BoxParams &p = d.p;
+    if (p.n[0] % 2 != 0) return false;
+    if (const char *env = std::getenv("NUC3D_VISC_TMA"))
+        if (std::atoi(env) == 0) return false;
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encoder();
+    if (!enc) return false;
+    const int src[4] = {0, 1, 2, 5};  // u, v, w, T
+    const cuuint64_t dims[3] = {(cuuint64_t)p.n[0], (cuuint64_t)p.n[1], (cuuint64_t)p.n[2]};
+    const cuuint64_t strides[2] = {(cuuint64_t)p.stride[1] * 8, (cuuint64_t)p.stride[2] * 8};
+    const cuuint32_t es[3] = {1, 1, 1};
+    for (int kind = 0; kind < 2; ++kind) {
+        const cuuint32_t box[3] = {(cuuint32_t)(kind ? kViscTmaTileX : kViscTmaHaloX),
+                                   (cuuint32_t)(kind ? kViscTmaTileY : kViscTmaHaloY), 1};
+        for (int f = 0; f < 4; ++f) {
+            CUresult r = enc(&out[4 * kind + f], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                             static_cast<void *>(fieldW(d, src[f])), dims, strides, box, es,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return false;
+        }
+    }
+    return true;
+}
 
 BoxParams make_params(const nuc3d_box_desc &d) {
     BoxParams bp{};
@@ -177,6 +231,16 @@ int Engine::add_box(const nuc3d_box_desc &d, int *id) {
     if (b.force_mem)
         ECK(forcing_prepare(b.dev.p, d.forcing_k, forcing_layout(b.dev.p, d.forcing_k, b.force_mem),
                             stream_));
+    b.dev.tmw = nullptr;
+    if (b.dev.p.navier_stokes) {
+        CUtensorMap maps[8];
+        if (encode_visc_maps(b.dev, maps)) {
+            void *dst = sm + kTmaOff;
+            ECK(cudaMemcpyAsync(dst, maps, sizeof maps, cudaMemcpyHostToDevice, stream_));
+            ECK(cudaStreamSynchronize(stream_));  // maps is a host stack array
+            b.dev.tmw = dst;
+        }
+    }
     int slot = -1;
     for (size_t i = 0; i < boxes_.size(); ++i)
         if (!boxes_[i].live) {
@@ -790,7 +854,9 @@ int Engine::sync_and_check(int id) {
         if (!boxes_[i].live || (id >= 0 && (int)i != id)) continue;
         unsigned f = 0;
         ECK(cudaMemcpy(&f, boxes_[i].dev.flags, sizeof f, cudaMemcpyDeviceToHost));
-        if (f & 1u) return set_last_error(NUC3D_ERR_NONFINITE, "state became non-finite (NaN/Inf)");
+        if (f & kFlagWaitTimeout)
+            return set_last_error(NUC3D_ERR_CUDA, "a bounded device wait timed out (viscous-flux TMA load)");
+        if (f & kFlagNonFinite) return set_last_error(NUC3D_ERR_NONFINITE, "state became non-finite (NaN/Inf)");
     }
     return NUC3D_OK;
 }

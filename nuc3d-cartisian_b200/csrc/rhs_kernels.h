@@ -46,11 +46,22 @@ struct BoxDev {
     long long np;
     double *eig;      // [3] running max eigenvalues of the current step
     double *res_acc;  // residual partial sum
-    unsigned *flags;  // bit 0: non-finite state seen
+    unsigned *flags;  // bit 0: non-finite state seen; bit 1: a bounded device wait timed out
     StepScalars *sc;
     int active;       // 0: the box is skipped by every kernel
     int pad;
+    // TMA tensor maps (CUtensorMap, 128 B each, in the box's allocation) of
+    // the primitives u, v, w, T: [0..3] halo-plane boxes, [4..7] tile boxes
+    // (kViscTmaBox*); null when the box's rows are not TMA-aligned (odd nx)
+    // or the box is inviscid
+    const void *tmw;
 };
+
+constexpr unsigned kFlagNonFinite = 1u, kFlagWaitTimeout = 2u;
+// boxes of the viscous-flux kernel's TMA loads (elements x, y, z): the
+// tile's plane with a 3-cell halo, x widened to start on a 32-byte boundary,
+// and the tile's own columns
+constexpr int kViscTmaHaloX = 40, kViscTmaHaloY = 14, kViscTmaTileX = 32, kViscTmaTileY = 8;
 
 __host__ __device__ __forceinline__ double *fieldU(const BoxDev &b, int s, int e) {
     return b.base + (long long)(5 * s + e) * b.np;

@@ -15,6 +15,12 @@ namespace {
 
 constexpr int TX = kT25X, TY = kT25Y, KZ = kT25Z;
 
+// a TMA tensor map as the kernels see it: 128 opaque, 64-byte aligned bytes
+// (the host encodes CUtensorMap values into the box's allocation)
+struct alignas(64) CUtensorMapLike {
+    unsigned long long opaque[16];
+};
+
 // Asynchronous global->shared copy of one element (cp.async, L1-allocating),
 // so a plane's halo tile streams in while the previous plane is computed.
 template <typename T>
@@ -25,6 +31,45 @@ __device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// ---- TMA (cp.async.bulk.tensor) loads completed on an mbarrier ----
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// waits for the completion of phase `parity` of the barrier for at most
+// ~2^31 clock cycles (about a second); false on timeout
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+    const long long t0 = clock64();
+    while (true) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > (1ll << 31)) return false;
+    }
+}
+// one 3-D tile of a tensor map (coordinates x, y, z in elements) into shared
+// memory, completing on the barrier
+__device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, int x, int y, int z,
+                                            unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_u32(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
 
 __device__ __forceinline__ int pmod(int c, int n) {
     int r = c % n;
@@ -45,11 +90,21 @@ __device__ __forceinline__ double cd6d(double m3, double m2, double m1, double p
 template <typename B>
 __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items) {
     // dynamic shared memory (visc_smem_bytes): the two plane tiles with their
-    // x/y halo, each column's plane k+3 (z-queue refill), the tile offsets
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto sP = reinterpret_cast<double (*)[4][TY + 6][TX + 6]>(smem_raw);
-    auto sZ = reinterpret_cast<double (*)[4][TX * TY]>(smem_raw + sizeof(double) * 2 * 4 * (TY + 6) * (TX + 6));
-    int *sOff = reinterpret_cast<int *>(smem_raw + sizeof(double) * 2 * 4 * ((TY + 6) * (TX + 6) + TX * TY));
+    // x/y halo (row pitch TX + 8: column 0 is cell i0 - 4, so that a TMA box
+    // starts on a 32-byte boundary), each column's plane k+3 (z-queue
+    // refill), the tile offsets, two mbarriers
+    static_assert(kViscTmaHaloX == TX + 8 && kViscTmaHaloY == TY + 6, "TMA halo box");
+    static_assert(kViscTmaTileX == TX && kViscTmaTileY == TY, "TMA tile box");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // TMA destinations must start on 128-byte boundaries: the layout starts
+    // at the first such boundary of the window (128 bytes are reserved)
+    unsigned char *const sbase = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
+    constexpr int PX = TX + 8;
+    auto sP = reinterpret_cast<double (*)[4][TY + 6][PX]>(sbase);
+    auto sZ = reinterpret_cast<double (*)[4][TX * TY]>(sbase + sizeof(double) * 2 * 4 * (TY + 6) * PX);
+    int *sOff = reinterpret_cast<int *>(sbase + sizeof(double) * 2 * 4 * ((TY + 6) * PX + TX * TY));
+    auto mbar = reinterpret_cast<unsigned long long *>(
+        sbase + sizeof(double) * 2 * 4 * ((TY + 6) * PX + TX * TY) + 16 * ((TY + 6) * (TX + 6) * 4 / 16 + 1));
     const WorkItem it = items[blockIdx.x];
     const BoxDev &bd = boxes[it.box];
     if (!bd.active || !bd.p.navier_stokes) return;
@@ -65,26 +120,70 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
     const long long sz = bp.stride[2];
     const long long col = active ? (long long)i + (long long)nx * j : 0;
     const int src[4] = {0, 1, 2, 5};  // u, v, w, T
-    for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
-        int yy = t / (TX + 6), xx = t - yy * (TX + 6);
-        sOff[t] = pmod(i0 - 3 + xx, nx) + nx * pmod(j0 - 3 + yy, ny);
+    // A tile whose halo plane lies inside the box (no periodic wrap) loads
+    // each plane with TMA: one thread issues 8 tile copies (halo plane and
+    // plane k+3 of u, v, w, T) completing on the buffer's mbarrier.  Other
+    // tiles copy element by element with cp.async through the wrapped offset
+    // table.
+    const CUtensorMapLike *tm = static_cast<const CUtensorMapLike *>(bd.tmw);
+    const bool tma = tm != nullptr && i0 >= 4 && i0 + TX + 4 <= nx && j0 >= 3 && j0 + TY + 3 <= ny;
+    if (tma) {
+        if (tid == 0) {
+            mbar_init(&mbar[0], 1);
+            mbar_init(&mbar[1], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+    } else {
+        for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
+            int yy = t / (TX + 6), xx = t - yy * (TX + 6);
+            sOff[t] = pmod(i0 - 3 + xx, nx) + nx * pmod(j0 - 3 + yy, ny);
+        }
     }
     __syncthreads();
+    constexpr unsigned kTmaBytes = 4 * sizeof(double) * ((TY + 6) * PX + TX * TY);
     // plane k's halo tile, and each column's plane k+3 for the z-queue: both
     // arrive while plane k-1 is computed
     auto issue = [&](int k, int buf) {
+        const int kz = k + 3 < nz ? k + 3 : k + 3 - nz;  // nz >= 8
+        if (tma) {
+            if (tid == 0) {
+                // the buffer's previous contents were read before the block's
+                // last barrier; order those reads before the async writes
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                mbar_arrive_expect_tx(&mbar[buf], kTmaBytes);
+#pragma unroll
+                for (int f = 0; f < 4; ++f) {
+                    tma_load_3d(&sP[buf][f][0][0], &tm[f], i0 - 4, j0 - 3, k, &mbar[buf]);
+                    tma_load_3d(&sZ[buf][f][0], &tm[4 + f], i0, j0, kz, &mbar[buf]);
+                }
+            }
+            return;
+        }
         const long long plane = sz * k;
         for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
             int yy = t / (TX + 6), xx = t - yy * (TX + 6);
             long long g = plane + sOff[t];
 #pragma unroll
-            for (int f = 0; f < 4; ++f) cp_async_elem(&sP[buf][f][yy][xx], wbase + src[f] * np + g);
+            for (int f = 0; f < 4; ++f)
+                cp_async_elem(&sP[buf][f][yy][xx + 1], wbase + src[f] * np + g);
         }
         if (active) {
-            const long long g6 = col + sz * pmod(k + 3, nz);
+            const long long g6 = col + sz * kz;
 #pragma unroll
             for (int f = 0; f < 4; ++f) cp_async_elem(&sZ[buf][f][tid], wbase + src[f] * np + g6);
         }
+    };
+    // plane k's buffer is ready: TMA tiles wait on the buffer's barrier (its
+    // (k-k0)/2-th completion), cp.async tiles on their own copies and then
+    // the block.  False when a TMA wait timed out (the block then stops).
+    auto ready = [&](int k, int buf) -> bool {
+        if (tma) {
+            const bool ok = mbar_wait(&mbar[buf], ((k - k0) >> 1) & 1);
+            return !__syncthreads_or(!ok);
+        }
+        cp_async_wait1();
+        __syncthreads();
+        return true;
     };
     const int kend = min(k0 + KZ, nz);
     issue(k0, 0);
@@ -111,8 +210,15 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
             const int buf = (k - k0) & 1;
             if (k + 1 < kend) issue(k + 1, buf ^ 1);
             cp_async_commit();
-            cp_async_wait1();
-            __syncthreads();
+            if (!ready(k, buf)) {
+                // a TMA wait timed out: report it, let the copies still in
+                // flight land (bounded), and stop
+                if (tid == 0) {
+                    atomicOr(bd.flags, kFlagWaitTimeout);
+                    if (k + 1 < kend) mbar_wait(&mbar[buf ^ 1], ((k + 1 - k0) >> 1) & 1);
+                }
+                return;
+            }
             // slot of plane k+s-3 (kb - k0 is a multiple of 7)
 #define QZ(f, s) qz[f][(u + (s)) % 7]
 #pragma unroll
@@ -121,8 +227,8 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
                 B gr[4][3];
 #pragma unroll
                 for (int f = 0; f < 4; ++f) {
-                    const int r = ty + 3, c = tx + 3;
-                    const double(*P)[TX + 6] = sP[buf][f];
+                    const int r = ty + 3, c = tx + 4;
+                    const double(*P)[PX] = sP[buf][f];
                     gr[f][0] = B(cd6d(P[r][c - 3], P[r][c - 2], P[r][c - 1], P[r][c + 1],
                                       P[r][c + 2], P[r][c + 3], ix));
                     gr[f][1] = B(cd6d(P[r - 3][c], P[r - 2][c], P[r - 1][c], P[r + 1][c],
@@ -257,7 +363,7 @@ __global__ void __launch_bounds__(TX *TY, 2)
         if (VIS) {
             if (k + 1 < kend) issue(k + 1, buf ^ 1);
             cp_async_commit();
-            long long g6 = col + sz * pmod(k + 3, nz);
+            long long g6 = col + sz * (k + 3 < nz ? k + 3 : k + 3 - nz);  // nz >= 8
 #pragma unroll
             for (int f = 0; f < 4; ++f) qz[f][6] = active ? vbase[cz[f] * np + g6] : B(0);
         }
@@ -337,7 +443,10 @@ __global__ void __launch_bounds__(TX *TY, 2)
 
 namespace {
 constexpr size_t visc_smem_bytes() {
-    return sizeof(double) * 2 * 4 * ((TY + 6) * (TX + 6) + TX * TY) + sizeof(int) * (TY + 6) * (TX + 6);
+    // planes (row pitch TX + 8) and z refills, the offset table rounded up to
+    // 16 bytes, two mbarriers, and the 128 bytes of alignment slack
+    return sizeof(double) * 2 * 4 * ((TY + 6) * (TX + 8) + TX * TY) +
+           16 * ((TY + 6) * (TX + 6) * 4 / 16 + 1) + 2 * sizeof(unsigned long long) + 128;
 }
 }  // namespace
 
