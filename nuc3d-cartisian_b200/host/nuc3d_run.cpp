@@ -9,7 +9,9 @@
 // singleBlock::solvePDE's loop (singleBlock.cpp:50-68): one TVD-RK3 step per
 // iteration while time <= tl and step < endStep, the status line of
 // block::printStatus (block.cpp:217-220), restart files every saveStep
-// (block.cpp:609-638) and, every postStep, the solveQ statistics appended to
+// (block.cpp:609-638; with IOController "Tecplot yes" also the Tecplot file
+// flowData/NUC3d_step_<step>_id_0.dat, block.cpp:553-607) and, every
+// postStep, the solveQ statistics appended to
 // enstrophy.dat and turb_para.dat (postproc.cpp:888-927) and the solveFFT
 // shell spectra in flowDataTemp/power_shell_<step>_<name>.dat.
 //
@@ -39,6 +41,7 @@ namespace {
 struct Case {
     nuc3d_box_desc desc{};
     std::map<std::string, double> io;    // IOController.in
+    std::map<std::string, std::string> out;  // IOController.in output switches (yes/no)
     std::map<std::string, double> phys;  // PhysModel.in key/value part
     double x0 = 0, y0 = 0, z0 = 0;
 };
@@ -163,9 +166,15 @@ Case read_case(const std::string &dir) {
     // IOController.in key/value (IOcontroller.cpp:10-60)
     c.io = {{"startStep", 0}, {"endStep", 100000}, {"postStep", 1}, {"saveStep", 1000},
             {"postSaveStep", 100}, {"Benchmark", 0}, {"cfl", 0.5}, {"tl", 0.0}, {"dt", 0.01}};
+    // block::Output's switches (block.cpp:241-262); the restart file is
+    // written at every save whatever "Binary" says (this driver restarts
+    // from it), the Tecplot file only when "Tecplot" is "yes"
+    c.out = {{"Binary", "no"}, {"Tecplot", "yes"}, {"PostProc", "no"}};
     auto io = words(inp + "IOController.in", false);
-    for (size_t i = 0; i + 1 < io.size(); i += 2)
+    for (size_t i = 0; i + 1 < io.size(); i += 2) {
         if (c.io.count(io[i])) c.io[io[i]] = std::atof(io[i + 1].c_str());
+        if (c.out.count(io[i])) c.out[io[i]] = io[i + 1];
+    }
     return c;
 }
 
@@ -189,6 +198,55 @@ double read_restart(const std::string &path, std::vector<double> &q, long long n
     f.read(reinterpret_cast<char *>(q.data()), (std::streamsize)(sizeof(double) * 5 * n));
     if (!f) die("restart file '" + path + "' is shorter than the mesh");
     return time;
+}
+
+// block::outputQ_tecplot (block.cpp:553-607): Tecplot ASCII, BLOCK packing;
+// the mesh vertices x, y, z ((nx+1)(ny+1)(nz+1) each, block::getXYZ,
+// block.cpp:103-140) then the cell-centred rho, u, v, w, pressure,
+// temperature, e, sound_speed of physicsModel::con2prim
+// (physicsModel.cpp:324-356), x fastest, one value per line with 12
+// significant digits (utilities.cpp:47-61).
+void write_tecplot(const std::string &path, const Case &c, const std::vector<double> &q,
+                   long long n) {
+    std::ofstream f(path);
+    if (!f) die("cannot write " + path);
+    const int nx = c.desc.nx, ny = c.desc.ny, nz = c.desc.nz;
+    const char *names[8] = {"rho", "u", "v", "w", "pressure", "temperature", "e", "sound_speed"};
+    f << "title=NUC3d\n"
+      << "variables=x,y,z";
+    for (const char *v : names) f << "," << v;
+    f << "\n Zone I = " << nx + 1 << ", J= " << ny + 1 << ", K=" << nz + 1
+      << "\n DATAPACKING=BLOCK, VARLOCATION=([4-11]=CELLCENTERED)\n";
+    f << std::setprecision(12);
+    const double d[3] = {c.desc.lx / nx, c.desc.ly / ny, c.desc.lz / nz};
+    const double o[3] = {c.x0, c.y0, c.z0};
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k <= nz; ++k)
+            for (int j = 0; j <= ny; ++j)
+                for (int i = 0; i <= nx; ++i) {
+                    const int ijk[3] = {i, j, k};
+                    f << d[a] * ijk[a] - o[a] << "\n";
+                }
+    const double gamma = c.desc.gamma, mach = c.desc.mach;
+    for (int v = 0; v < 8; ++v)
+        for (long long m = 0; m < n; ++m) {
+            const double rho = q[m], u = q[n + m] / rho, vv = q[2 * n + m] / rho,
+                         w = q[3 * n + m] / rho, E = q[4 * n + m];
+            const double p = std::fabs((E - 0.5 * rho * (u * u + vv * vv + w * w)) * (gamma - 1.0));
+            double val;
+            switch (v) {
+                case 0: val = rho; break;
+                case 1: val = u; break;
+                case 2: val = vv; break;
+                case 3: val = w; break;
+                case 4: val = p; break;
+                case 5: val = gamma * mach * mach * p / rho; break;
+                case 6: val = p / rho / (gamma - 1.0); break;
+                default: val = std::sqrt(gamma * p / rho); break;
+            }
+            f << val << "\n";
+        }
+    if (!f) die("write failed: " + path);
 }
 
 void check(int rc, const char *what) {
@@ -298,6 +356,9 @@ int main(int argc, char **argv) {
     auto output = [&]() {
         check(nuc3d_get_state_host(ctx, qp), "nuc3d_get_state_host");
         write_restart(restart_name(dir, step), time, q, n);
+        if (c.out["Tecplot"] == "yes")
+            write_tecplot(dir + "/flowData/NUC3d_step_" + std::to_string(step) + "_id_0.dat", c,
+                          q, n);
     };
     std::cout << "Start solving......\n";
     while (time <= tl && step < end) {

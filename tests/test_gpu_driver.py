@@ -69,6 +69,41 @@ def test_driver_restart_continues_bitwise(driver, tmp_path):
     assert max_rel_l2(q, z["q10"]) < 1e-12
 
 
+def test_driver_tecplot_file(driver, tmp_path):
+    """IOController "Tecplot yes": block::outputQ_tecplot's ASCII file beside
+    the restart file: header, BLOCK-packed mesh vertices, then the
+    cell-centred primitives of con2prim, 12 significant digits."""
+    d = tgv_case(tmp_path, endStep=2, saveStep=2, Tecplot="yes")
+    r = subprocess.run([str(driver), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = (tmp_path / "flowData" / "NUC3d_step_2_id_0.dat").read_text().splitlines()
+    assert lines[0] == "title=NUC3d"
+    assert lines[1] == "variables=x,y,z,rho,u,v,w,pressure,temperature,e,sound_speed"
+    assert lines[2] == " Zone I = 25, J= 25, K=25"
+    assert lines[3] == " DATAPACKING=BLOCK, VARLOCATION=([4-11]=CELLCENTERED)"
+    vals = np.array([float(v) for v in lines[4:]])
+    nv, nc = 25 ** 3, 24 ** 3
+    assert vals.size == 3 * nv + 8 * nc
+    h = 2.0 * np.pi / 24
+    k, j, i = np.meshgrid(np.arange(25), np.arange(25), np.arange(25), indexing="ij")
+    for a, idx in enumerate((i, j, k)):
+        np.testing.assert_allclose(vals[a * nv:(a + 1) * nv], (h * idx).ravel(), rtol=1e-11, atol=1e-12)
+    _, q = read_restart(tmp_path / "flowData" / "NUC3d_step_2_ID_0.bin", d.shape)
+    rho, u, v, w = q[0], q[1] / q[0], q[2] / q[0], q[3] / q[0]
+    g, m = d.gamma, d.mach
+    p = np.abs((q[4] - 0.5 * rho * (u * u + v * v + w * w)) * (g - 1.0))
+    want = [rho, u, v, w, p, g * m * m * p / rho, p / rho / (g - 1.0), np.sqrt(g * p / rho)]
+    cells = vals[3 * nv:].reshape(8, -1)
+    for f in range(8):  # 12 significant digits: within 5e-12 of the value
+        np.testing.assert_allclose(cells[f], want[f].ravel(), rtol=1e-11, atol=1e-13)
+    # "Tecplot no" writes none
+    tgv_case(tmp_path, endStep=2, saveStep=2, Tecplot="no")
+    (tmp_path / "flowData" / "NUC3d_step_2_id_0.dat").unlink()
+    r = subprocess.run([str(driver), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert not (tmp_path / "flowData" / "NUC3d_step_2_id_0.dat").exists()
+
+
 def test_case_runner_module(capsys):
     """python -m nuc3d_b200: one seeded HIT case on the device, one JSON line."""
     import json
