@@ -591,15 +591,17 @@ __device__ __forceinline__ void hc_row(double f0, double f1, double f2, double f
     const double A1 = mul_(mul_(K::CR1, add_(s1, t2)), mul_(s0, s2));
     const double A2 = mul_(mul_(K::CR2, add_(s2, t2)), mul_(s0, s1));
     const double SA = add_(add_(A0, A1), A2);
-    const double x = mul_(sub_(SA, P), __drcp_rn(P));  // sum(alpha) - 1
-    if (add_(1.0, mul_(x, x)) < 2.0) {
+    // theta = 1/(1 + x^2) > 1/2 with x = sum(alpha) - 1 = (SA - P)/P, i.e.
+    // |SA - P| < P: decided without a division
+    const double dSP = sub_(SA, P);
+    if (fabs(dSP) < P) {
         lo = 2.0 / 7.0;
         b = 4.0 / 7.0;
         hi = 1.0 / 7.0;
         d = q7;
         return;
     }
-    const double ix = mul_(P, __drcp_rn(sub_(SA, P)));  // 1/x
+    const double ix = mul_(P, __drcp_rn(dSP));  // 1/x
     const double u = mul_(mul_(SA, ix), ix);            // P sum(alpha) / x^2
     const double third = 1.0 / 3.0, two3 = 2.0 / 3.0, sixth = 1.0 / 6.0;
     lo = fma_(2.0 / 7.0, u, fma_(two3, A0, mul_(third, A1)));
