@@ -69,21 +69,6 @@ __device__ __forceinline__ void cr_p(float is0, float is1, float is2, float &p0,
     p2 = mul_(r2, r2);
 }
 
-// WENO5 smoothness indicators times 4 of the upwind-oriented stencil
-// f0..f4 (schemes.hpp:33-34), from first and second differences:
-// 4 beta_k = 4 (13/12) D_k^2 + E_k^2 with D_k the sub-stencil's second
-// difference and E0 = D0 + 2 (f2 - f1), E1 = (f2 - f1) + (f3 - f2),
-// E2 = D2 - 2 (f3 - f2).
-template <typename B>
-__device__ __forceinline__ void cr_beta4(B f0, B f1, B f2, B f3, B f4, B &is0, B &is1, B &is2) {
-    const B a10 = sub_(f1, f0), a21 = sub_(f2, f1), a32 = sub_(f3, f2), a43 = sub_(f4, f3);
-    const B D0 = sub_(a21, a10), D1 = sub_(a32, a21), D2 = sub_(a43, a32);
-    const B e0 = fma_(B(2), a21, D0), e1 = add_(a21, a32), e2 = fma_(B(-2), a32, D2);
-    is0 = fma_(e0, e0, dd_of(D0));
-    is1 = fma_(e1, e1, dd_of(D1));
-    is2 = fma_(e2, e2, dd_of(D2));
-}
-
 // One compact-WENO row from the upwind-oriented stencil f0..f4 of its cell:
 // the upwind-side coupling lo, the diagonal b, the downwind-side coupling hi
 // and the right-hand side d (crweno5.cpp:151-161), all times 60 / (0.1 sum p)
@@ -96,7 +81,7 @@ __device__ __forceinline__ void cr_beta4(B f0, B f1, B f2, B f3, B f4, B &is0, B
 template <typename B>
 __device__ __forceinline__ void cr_row(B f0, B f1, B f2, B f3, B f4, B &lo, B &b, B &hi, B &d) {
     B is0, is1, is2, p0, p1, p2;
-    cr_beta4(f0, f1, f2, f3, f4, is0, is1, is2);
+    weno5_beta4(f0, f1, f2, f3, f4, is0, is1, is2);
     cr_p(is0, is1, is2, p0, p1, p2);
     lo = fma_(B(8), p0, mul_(B(10), p1));
     b = fma_(B(4), p0, fma_(B(20), p1, mul_(B(12), p2)));

@@ -282,6 +282,21 @@ __device__ __forceinline__ B dd_of(B D) {
     return mul_(t, t);
 }
 
+// WENO5 smoothness indicators times 4 of the upwind-oriented stencil
+// f0..f4 (schemes.hpp:33-34), from first and second differences:
+// 4 beta_k = 4 (13/12) D_k^2 + E_k^2 with D_k the sub-stencil's second
+// difference and E0 = D0 + 2 (f2 - f1), E1 = (f2 - f1) + (f3 - f2),
+// E2 = D2 - 2 (f3 - f2).
+template <typename B>
+__device__ __forceinline__ void weno5_beta4(B f0, B f1, B f2, B f3, B f4, B &is0, B &is1, B &is2) {
+    const B a10 = sub_(f1, f0), a21 = sub_(f2, f1), a32 = sub_(f3, f2), a43 = sub_(f4, f3);
+    const B D0 = sub_(a21, a10), D1 = sub_(a32, a21), D2 = sub_(a43, a32);
+    const B e0 = fma_(B(2), a21, D0), e1 = add_(a21, a32), e2 = fma_(B(-2), a32, D2);
+    is0 = fma_(e0, e0, dd_of(D0));
+    is1 = fma_(e1, e1, dd_of(D1));
+    is2 = fma_(e2, e2, dd_of(D2));
+}
+
 template <int SCHEME, typename B>
 __device__ __forceinline__ B weno_combine(B is0, B is1, B is2, B q0, B q1, B q2) {
     if (SCHEME == SCHEME_Z) return weno_z_combine(is0, is1, is2, q0, q1, q2);
@@ -575,11 +590,14 @@ __device__ __forceinline__ float weno7_face_eps(float f0, float f1, float f2, fl
 //   scaled by 1/x^2.
 __device__ __forceinline__ void hc_row(double f0, double f1, double f2, double f3, double f4,
                                        double &lo, double &b, double &hi, double &d) {
+    // indicators times 4 (weno5_beta4) with eps alike: every alpha and the
+    // products below scale by 16^3, which leaves x and the row's ratios as
+    // they are (a row may be scaled freely)
     double is0, is1, is2;
-    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
+    weno5_beta4(f0, f1, f2, f3, f4, is0, is1, is2);
     const double q7 = mul_(fma_(4.0, f4, fma_(159.0, f3, fma_(239.0, f2, fma_(19.0, f1, -f0)))),
                            1.0 / 420.0);
-    const double ss = 1.0e-40;
+    const double ss = 4.0 * 1.0e-40;
     const double tau = fabs(sub_(is2, is0));
     const double t2 = mul_(tau, tau);
     double s0 = add_(is0, ss), s1 = add_(is1, ss), s2 = add_(is2, ss);
@@ -613,8 +631,10 @@ __device__ __forceinline__ void hc_row(double f0, double f1, double f2, double f
 }
 __device__ __forceinline__ void hc_row(float f0, float f1, float f2, float f3, float f4, float &lo,
                                        float &b, float &hi, float &d) {
+    // indicators times 4 (weno5_beta4); tau and eps scale alike, so the
+    // ratios r_k below are unchanged
     float is0, is1, is2;
-    weno5_beta(f0, f1, f2, f3, f4, is0, is1, is2, false);
+    weno5_beta4(f0, f1, f2, f3, f4, is0, is1, is2);
     const float q7 = mul_(fma_(4.0f, f4, fma_(159.0f, f3, fma_(239.0f, f2, fma_(19.0f, f1, -f0)))),
                           float(1.0 / 420.0));
     // eps: the reference's 1e-40 is below FP32's range; in its place the
@@ -625,9 +645,9 @@ __device__ __forceinline__ void hc_row(float f0, float f1, float f2, float f3, f
     // neighbouring rows (omega2 = 1, then omega0 = 1) form a singular 2x2
     // block of the line system.  With the floor such stencils take the linear
     // row.
-    const float sc = mul_(4.0e-6f, fmaxf(fmaxf(fmaxf(fabsf(f0), fabsf(f1)), fmaxf(fabsf(f2), fabsf(f3))),
-                                         fabsf(f4)));
-    const float ss = fma_(sc, sc, 1.0e-30f), cap = 1.0e15f;
+    const float sc = mul_(2.0f * 4.0e-6f, fmaxf(fmaxf(fmaxf(fabsf(f0), fabsf(f1)), fmaxf(fabsf(f2), fabsf(f3))),
+                                                fabsf(f4)));
+    const float ss = fma_(sc, sc, 4.0f * 1.0e-30f), cap = 1.0e15f;  // 4 (eps + floor^2)
     const float tau = fabsf(sub_(is2, is0));
     const float r0 = fminf(mul_(tau, frcp_fast(add_(is0, ss))), cap);
     const float r1 = fminf(mul_(tau, frcp_fast(add_(is1, ss))), cap);

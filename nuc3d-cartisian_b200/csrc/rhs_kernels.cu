@@ -184,9 +184,11 @@ struct InvGeom {
     static constexpr int SF = DIR == 0 ? TL * R * S : NF * TL;  // staged values per flux
     // WENO5: the staged tile (~52 KB) admits 4 blocks per SM; blocks of up to
     // 256 threads are held to the registers that keep all 4 resident, larger
-    // ones to 64 registers per thread.  (WENO7's sweep has its own kernel
+    // ones to 64 registers per thread.  The FP32 4-face x tile (28 KB) is held
+    // to 6 blocks (80 registers; measured faster than 4 or 8).  (WENO7's sweep has its own kernel
     // without a register cap.)
-    static constexpr int MINB = NT <= 256 ? 4 : 1024 / NT;
+    static constexpr int MINB =
+        NT <= 256 ? ((DIR == 0 && sizeof(B) == 4 && NT == 128) ? 6 : 4) : 1024 / NT;
     // thread -> (line, run)
     __device__ static void thread(int t, int &l, int &r) {
         if (DIR == 0) {
