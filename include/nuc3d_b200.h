@@ -85,7 +85,15 @@ typedef struct nuc3d_box_desc {
      * NUC3D_FORCING_CONST, the spectral shell forcing of AddForcing_Const
      * (physicsModel.cpp:1368-1641) with Forcing_amplitude (target shell
      * energy), Forcing_amplitude_hel (helical part) and Forcing_wave_k (shell
-     * radius, < 3.5). */
+     * radius, < 3.5).
+     * NUC3D_FORCING_BAND (no counterpart in the reference, which has only
+     * the shell forcing): band-limited forcing at a fixed energy-injection
+     * rate.  On every RHS evaluation the solenoidal part s(k) of the
+     * velocity's Fourier modes with 0 < |k| <= forcing_k (< 3.5) is forced
+     * as f(k) = P s(k) / (2 E_b), E_b = sum over the band of |s(k)|^2 / 2,
+     * P = forcing_amp, so that the mean kinetic-energy input <f.u> is
+     * exactly P; forcing_hel is ignored.  It enters the RHS as the shell
+     * forcing does (density taken as 1; energy equation gets f.u - <f.u>). */
     int forcing;
     double forcing_amp, forcing_hel, forcing_k;
     /* PhysModel.in RiemannSolver (physicsModel.cpp:16-20): NUC3D_RIEMANN_LF
@@ -100,6 +108,7 @@ typedef struct nuc3d_box_desc {
 #define NUC3D_RIEMANN_AUSMP 2
 #define NUC3D_FORCING_NONE 0
 #define NUC3D_FORCING_CONST 1
+#define NUC3D_FORCING_BAND 2
 
 typedef struct nuc3d_ctx nuc3d_ctx;
 
@@ -398,10 +407,13 @@ NUC3D_API int nuc3d_reconstruct(int scheme, int upwind, unsigned quirks, int nx,
  * results as nuc3d_reconstruct(NUC3D_CRWENO5, ...), but the Thomas-sweep
  * scratch is a fixed 4 MiB array in the library's device image (held by
  * every GPU that loads the library until exit), so 2*nx*ny*nz must not
- * exceed 524288; larger calls return NUC3D_ERR_INVALID.  The first call on
- * each device looks up the array's device address (cudaGetSymbolAddress)
- * and should come before any stream capture.  All calls share the array:
- * calls that overlap on the GPU race and must be serialised. */
+ * exceed 524288 (and nx must not exceed 4096, as for nuc3d_reconstruct);
+ * larger calls return NUC3D_ERR_INVALID.  Every call looks up the array's
+ * address on the current device (cudaGetSymbolAddress, which allocates
+ * nothing), so a device reset in the same process is harmless; the first
+ * call on each device also loads the library's device code there and should
+ * come before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised. */
 NUC3D_API int nuc3d_reconstruct_crweno5_noalloc(int upwind, int nx, int ny, int nz,
                                                 const double *d_in, const double *d_halo_l,
                                                 const double *d_halo_r, double *d_out,

@@ -145,11 +145,14 @@ int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
         return bad(NUC3D_ERR_INVALID, "gamma must be > 1 and Mach, Re, Pr > 0");
     if (d.riemann < NUC3D_RIEMANN_LF || d.riemann > NUC3D_RIEMANN_AUSMP)
         return bad(NUC3D_ERR_UNSUPPORTED, "unknown Riemann solver (flux splitting)");
-    if (d.forcing != NUC3D_FORCING_NONE && d.forcing != NUC3D_FORCING_CONST)
+    if (d.forcing != NUC3D_FORCING_NONE && d.forcing != NUC3D_FORCING_CONST &&
+        d.forcing != NUC3D_FORCING_BAND)
         return bad(NUC3D_ERR_UNSUPPORTED, "unknown forcing model");
-    if (d.forcing == NUC3D_FORCING_CONST) {
+    if (d.forcing != NUC3D_FORCING_NONE) {
         if (!(d.forcing_k > 0.0) || forcing_K(d.forcing_k) > kForceMaxK)
             return bad(NUC3D_ERR_UNSUPPORTED, "forcing shell radius must be in (0, 3.5)");
+        if (d.forcing == NUC3D_FORCING_BAND && !(d.forcing_amp >= 0.0))
+            return bad(NUC3D_ERR_INVALID, "band forcing needs an injection rate >= 0");
         for (int i = 0; i < 3; ++i)
             if (2 * forcing_K(d.forcing_k) + 1 > n[i])
                 return bad(NUC3D_ERR_INVALID, "box too small for the forcing shell");
@@ -163,7 +166,7 @@ long long Engine::box_bytes(const nuc3d_box_desc &d) {
     long long np = pad32(bp.N);
     long long bs = (long long)bulk_size(d.precision);
     long long b = 21 * np * 8 + 14 * np * bs + (long long)kSmallBytes;
-    if (d.forcing == NUC3D_FORCING_CONST) b += (long long)forcing_scratch_bytes(bp, d.forcing_k);
+    if (d.forcing != NUC3D_FORCING_NONE) b += (long long)forcing_scratch_bytes(bp, d.forcing_k);
     return b;
 }
 
@@ -205,7 +208,7 @@ int Engine::add_box(const nuc3d_box_desc &d, int *id) {
     const size_t bs = bulk_size(precision_);
     const size_t bytes = sizeof(double) * 21 * (size_t)np + bs * 14 * (size_t)np + kSmallBytes;
     cudaError_t e = cudaMallocAsync(&b.mem, bytes, stream_);
-    if (e == cudaSuccess && d.forcing == NUC3D_FORCING_CONST)
+    if (e == cudaSuccess && d.forcing != NUC3D_FORCING_NONE)
         e = cudaMallocAsync(&b.force_mem, forcing_scratch_bytes(b.dev.p, d.forcing_k), stream_);
     if (e != cudaSuccess) {
         if (b.mem) cudaFreeAsync(b.mem, stream_);
@@ -534,7 +537,7 @@ cudaError_t Engine::enqueue_forcing(cudaStream_t st) {
     for (const EngineBox &b : boxes_) {
         if (!b.live || !b.dev.active || !b.force_mem) continue;
         ForceParams fp{b.desc.forcing_amp, b.desc.forcing_hel, b.desc.forcing_k,
-                       forcing_K(b.desc.forcing_k), 0};
+                       forcing_K(b.desc.forcing_k), b.desc.forcing == NUC3D_FORCING_BAND ? 1 : 0};
         cudaError_t e = launch_forcing<B>(b.dev, forcing_layout(b.dev.p, b.desc.forcing_k, b.force_mem),
                                           fp, st);
         if (e != cudaSuccess) return e;

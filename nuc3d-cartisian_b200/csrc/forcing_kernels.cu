@@ -17,6 +17,12 @@
 // (kmag unmodified, so k = 0 counts in E_s but is not forced).  In physical
 // space (rho taken as 1, physicsModel.cpp:1617-1640):
 //   R[1..3] -= f,   R[4] -= f.u - <f.u>.
+//
+// The band forcing at a fixed injection rate (NUC3D_FORCING_BAND, not in the
+// reference) shares every pass: on the modes with 0 < |k| <= k_f it forces
+// the solenoidal part s (no helical term) as f = s P / (2 E_b), E_b the band's
+// solenoidal energy sum |s|^2 / 2.  Since s is orthogonal to the compressive
+// part, sum Re(f . conj(u^)) = P: the mean power <f.u> is P.
 #include "forcing_kernels.h"
 
 namespace nuc3d {
@@ -108,6 +114,10 @@ __global__ void k_force_fy(const double2 *A, const double2 *Ty, double2 *B, int 
     }
 }
 
+__device__ __forceinline__ double kmag0_of(double kx, double ky, double kz) {
+    return sqrt(kx * kx + ky * ky + kz * kz);
+}
+
 // forward z + mode algebra + shell energies + forcing spectrum (one block).
 // scal: [0] E_s, [1] E_c, [2] theta, [3] <f.u> (set later)
 __global__ void __launch_bounds__(kThreads)
@@ -141,6 +151,14 @@ __global__ void __launch_bounds__(kThreads)
             s[c] = make_double2(uh[c].x - ku_re * kk[c] / kmag, uh[c].y - ku_im * kk[c] / kmag);
             cc[c] = make_double2(uh[c].x - s[c].x, uh[c].y - s[c].y);
         }
+        if (fp.band) {
+            // band forcing: the solenoidal part alone, energy over 0 < |k| <= k_f
+            if (kmag0_of(kx0, ky0, kz0) > 0.0 && kmag0_of(kx0, ky0, kz0) <= fp.k + 1e-12)
+                e2[0] += 0.5 * (s[0].x * s[0].x + s[1].x * s[1].x + s[2].x * s[2].x +
+                                s[0].y * s[0].y + s[1].y * s[1].y + s[2].y * s[2].y);
+            for (int c = 0; c < 3; ++c) sS[mode * 3 + c] = s[c];
+            continue;
+        }
         // helical term (physicsModel.cpp:1512-1526)
         const double kxu0_re = -(ky0 * s[2].y - kz0 * s[1].y) / kmag;
         const double kxu1_re = (kx0 * s[2].y - kz0 * s[0].y) / kmag;
@@ -161,21 +179,23 @@ __global__ void __launch_bounds__(kThreads)
     }
     __shared__ double tot[2];
     block_sum<2>(e2, tot);
-    const double theta = sqrt(fabs(fp.amp - tot[1]) / tot[0]);
+    // shell: theta - 1 multiplies the shell's modes; band: the gain P / (2 E_b)
+    // (zero for a band without energy)
+    const double theta = fp.band ? 0.0 : sqrt(fabs(fp.amp - tot[1]) / tot[0]);
+    const double gain = fp.band ? (tot[0] > 0.0 ? fp.amp / (2.0 * tot[0]) : 0.0) : theta - 1.0;
     if (threadIdx.x == 0) {
         scal[0] = tot[0];
         scal[1] = tot[1];
-        scal[2] = theta;
+        scal[2] = fp.band ? gain : theta;
     }
     for (int mode = threadIdx.x; mode < M3; mode += blockDim.x) {
         const int mx = mode % M, my = (mode / M) % M, mz = mode / (M * M);
         const double kx0 = mx - K, ky0 = my - K, kz0 = mz - K;
-        const double kmag = sqrt(kx0 * kx0 + ky0 * ky0 + kz0 * kz0);  // unmodified at k = 0
-        const bool on = fabs(kmag - fp.k) < 0.5;
+        const double kmag = kmag0_of(kx0, ky0, kz0);  // unmodified at k = 0
+        const bool on = fp.band ? (kmag > 0.0 && kmag <= fp.k + 1e-12) : fabs(kmag - fp.k) < 0.5;
         for (int c = 0; c < 3; ++c) {
             const double2 s = sS[mode * 3 + c];
-            Fh[c * M3 + mode] = on ? make_double2(s.x * (theta - 1.0), s.y * (theta - 1.0))
-                                   : make_double2(0.0, 0.0);
+            Fh[c * M3 + mode] = on ? make_double2(s.x * gain, s.y * gain) : make_double2(0.0, 0.0);
         }
     }
 }

@@ -11,10 +11,12 @@ namespace nuc3d {
 
 // PhysModel.in Forcing_amplitude, Forcing_amplitude_hel, Forcing_wave_k
 // (physicsModel.cpp:1422-1424); K = floor(k + 1/2) bounds |k_d| of the shell.
+// band = 1: the band forcing at a fixed injection rate (NUC3D_FORCING_BAND):
+// amp is the injection rate P and k the band radius.
 struct ForceParams {
     double amp, hel, k;
     int K;
-    int pad;
+    int band;
 };
 
 // Device scratch of one forced box (one allocation, laid out by forcing_layout).
@@ -22,7 +24,7 @@ struct ForceScratch {
     double2 *tx, *ty, *tz;  // twiddles exp(+i 2 pi k j / n), k = -K..K
     double2 *a, *b, *fh;    // transform passes and the forcing spectrum
     double *partials;       // per-line sums of f.u
-    double *scal;           // E_s, E_c, theta, <f.u>
+    double *scal;           // E_s, E_c, theta (band: the gain P / (2 E_b)), <f.u>
 };
 
 constexpr int kForceMaxK = 3;  // shells up to k_f < 3.5

@@ -13,10 +13,15 @@
 //    loads the library holds it until the process exits.  Calls needing
 //    more than 2 * nx * ny * nz > kNoAllocScratchDoubles are rejected with
 //    NUC3D_ERR_INVALID.
-//  * the array's host-side name is not a device address, so its device
-//    address is looked up with cudaGetSymbolAddress once per device, with
-//    that device current, on the first call made on that device.  Make that
+//  * the array's host-side name is not a device address.  Every call looks
+//    up the array's address on the current device with
+//    cudaGetSymbolAddress (a host-side lookup that allocates nothing) and
+//    checks the result, so a cudaDeviceReset or a re-created primary context
+//    in the same process never leaves a stale address behind.  The first
+//    call on a device also loads the library's device code there; make that
 //    first call before any stream capture.
+//  * the same argument rules as nuc3d_reconstruct(NUC3D_CRWENO5, ...),
+//    nx <= 4096 included.
 //  * all calls share one array per device and it keeps the last call's
 //    contents.  Nothing in it has to start at zero: the kernel writes every
 //    entry it reads before reading it.  Calls whose executions overlap on
@@ -25,8 +30,6 @@
 //  * no cudaMalloc, cudaFree or allocating library routine is called.
 #include <cuda_runtime.h>
 
-#include <mutex>
-
 #include "nuc3d_b200.h"
 #include "op_kernels.h"
 
@@ -34,10 +37,6 @@ namespace {
 
 constexpr size_t kNoAllocScratchDoubles = size_t(1) << 19;  // 4 MiB of FP64
 __device__ __align__(256) double g_crweno_scratch[kNoAllocScratchDoubles];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-double *g_scratch_ptr[kMaxDevices] = {};
 
 }  // namespace
 
@@ -51,6 +50,7 @@ extern "C" NUC3D_API int nuc3d_reconstruct_crweno5_noalloc(int upwind, int nx, i
         return set_last_error(NUC3D_ERR_INVALID, "weno error: no such direction");
     if (nx < 8 || ny < 1 || nz < 1)
         return set_last_error(NUC3D_ERR_INVALID, "need nx >= 8, ny, nz >= 1");
+    if (nx > 4096) return set_last_error(NUC3D_ERR_INVALID, "crweno5 / hccs need nx <= 4096");
     if (!d_in || !d_halo_l || !d_halo_r || !d_out)
         return set_last_error(NUC3D_ERR_INVALID, "null buffer");
     const long long lines = (long long)ny * nz;
@@ -59,24 +59,17 @@ extern "C" NUC3D_API int nuc3d_reconstruct_crweno5_noalloc(int upwind, int nx, i
         return set_last_error(NUC3D_ERR_INVALID,
                               "crweno5 no-alloc: 2*nx*ny*nz exceeds the 524288-double "
                               "(4 MiB) static scratch; use nuc3d_reconstruct");
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-        return set_last_error(NUC3D_ERR_CUDA, "crweno5 no-alloc: no usable current device");
-    double *scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratch_ptr[dev]) {
-            void *p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_crweno_scratch);
-            if (e != cudaSuccess || !p)
-                return set_last_error(NUC3D_ERR_CUDA,
-                                      "crweno5 no-alloc: cudaGetSymbolAddress failed");
-            g_scratch_ptr[dev] = static_cast<double *>(p);
-        }
-        scratch = g_scratch_ptr[dev];
-    }
-    cudaError_t e = nuc3d::op_crweno_into(upwind, nx, lines, d_in, d_halo_l, d_halo_r, d_out,
-                                          scratch, static_cast<cudaStream_t>(stream));
+    // the device address of the array in the current context (never cached:
+    // a reset device reloads the module and the array may move)
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_crweno_scratch);
+    if (e != cudaSuccess || !p)
+        return set_last_error(NUC3D_ERR_CUDA, e != cudaSuccess
+                                                  ? cudaGetErrorString(e)
+                                                  : "crweno5 no-alloc: no scratch address");
+    double *const scratch = static_cast<double *>(p);
+    e = nuc3d::op_crweno_into(upwind, nx, lines, d_in, d_halo_l, d_halo_r, d_out, scratch,
+                              static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return set_last_error(NUC3D_ERR_CUDA, cudaGetErrorString(e));
     return NUC3D_OK;
 }

@@ -65,7 +65,10 @@ __global__ void k_op_weno7(int upwind, int nx, long long lines, const double *in
 }
 
 // One thread per line: crweno5.cpp:45-402 + halo faces :425-837.  scratch
-// holds 2*(nx) values per line (c' and d' of the Thomas sweep).
+// holds 2*nx values per line (c' and d' of the Thomas sweep), interleaved
+// with the line index fastest (row r of line l at r*lines + l, d' rows after
+// the nx c' rows), so that the consecutive lines of a warp touch consecutive
+// words.
 __global__ void k_op_crweno(int upwind, int nx, long long lines, const double *in,
                             const double *hl, const double *hr, double *out, double *scratch) {
     long long line = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -79,8 +82,8 @@ __global__ void k_op_crweno(int upwind, int nx, long long lines, const double *i
     for (int m = 0; m <= 2; ++m) o[m] = js(m);
     for (int m = nx - 2; m <= nx; ++m) o[m] = js(m);
     const int M = nx - 5;
-    double *cs = scratch + 2 * (long long)nx * line;
-    double *ds = cs + nx;
+    double *cs = scratch + line;                    // c' of row r at cs[r * lines]
+    double *ds = scratch + (long long)nx * lines + line;  // d' of row r at ds[r * lines]
     double cp = 0.0, dp = js(3);
     cs[0] = cp;
     ds[0] = dp;
@@ -112,13 +115,13 @@ __global__ void k_op_crweno(int upwind, int nx, long long lines, const double *i
         double den = b - cp * a;
         cp = c / den;
         dp = (d - dp * a) / den;
-        cs[r] = cp;
-        ds[r] = dp;
+        cs[r * lines] = cp;
+        ds[r * lines] = dp;
     }
-    double x = ds[M - 1];
+    double x = ds[(M - 1) * lines];
     o[nx - 3] = x;
     for (int r = M - 2; r >= 0; --r) {
-        x = ds[r] - cs[r] * x;
+        x = ds[r * lines] - cs[r * lines] * x;
         o[r + 3] = x;
     }
 }
@@ -126,7 +129,8 @@ __global__ void k_op_crweno(int upwind, int nx, long long lines, const double *i
 // One thread per line: hccs (hccs.cpp): faces 0..3 and nx-3..nx explicit
 // WENO7 with hccs's eps (:538-980), the system of faces 4..nx-4 (identity
 // rows at its ends, hybrid rows between, :54-245 / :272-471) by a Thomas
-// sweep.  scratch holds 2*nx values per line.
+// sweep.  scratch holds 2*nx values per line, interleaved as in
+// k_op_crweno.
 __global__ void k_op_hccs(int upwind, int nx, long long lines, const double *in,
                           const double *hl, const double *hr, double *out, double *scratch) {
     long long line = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -141,8 +145,8 @@ __global__ void k_op_hccs(int upwind, int nx, long long lines, const double *in,
     for (int m = 0; m <= 3; ++m) o[m] = w7(m);
     for (int m = nx - 3; m <= nx; ++m) o[m] = w7(m);
     const int M = nx - 7;
-    double *cs = scratch + 2 * (long long)nx * line;
-    double *ds = cs + nx;
+    double *cs = scratch + line;                    // interleaved as in k_op_crweno
+    double *ds = scratch + (long long)nx * lines + line;
     double cp = 0.0, dp = w7(4);
     cs[0] = cp;
     ds[0] = dp;
@@ -162,13 +166,13 @@ __global__ void k_op_hccs(int upwind, int nx, long long lines, const double *in,
         double den = b - cp * a;
         cp = c / den;
         dp = (d - dp * a) / den;
-        cs[r] = cp;
-        ds[r] = dp;
+        cs[r * lines] = cp;
+        ds[r * lines] = dp;
     }
-    double x = ds[M - 1];
+    double x = ds[(M - 1) * lines];
     o[nx - 4] = x;
     for (int r = M - 2; r >= 0; --r) {
-        x = ds[r] - cs[r] * x;
+        x = ds[r * lines] - cs[r * lines] * x;
         o[r + 4] = x;
     }
 }

@@ -293,7 +293,10 @@ private:
                 chunk = 1;  // measure the new composition first
             const double t_a = now();
             int rc = eng->step((int)chunk);
-            if (!rc) rc = cudaStreamSynchronize(st) == cudaSuccess ? NUC3D_OK : NUC3D_ERR_CUDA;
+            if (!rc) {
+                const cudaError_t se = cudaStreamSynchronize(st);
+                if (se != cudaSuccess) rc = set_last_error(NUC3D_ERR_CUDA, cudaGetErrorString(se));
+            }
             const double dt_chunk = now() - t_a;
             if (rc) {
                 // a failed step leaves every resident solve undefined

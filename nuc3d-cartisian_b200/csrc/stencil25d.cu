@@ -211,10 +211,13 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
             if (k + 1 < kend) issue(k + 1, buf ^ 1);
             cp_async_commit();
             if (!ready(k, buf)) {
-                // a TMA wait timed out: report it, let the copies still in
-                // flight land (bounded), and stop
+                // a TMA wait timed out: report it, give the copies still in
+                // flight into both buffers one more bounded wait each, and
+                // stop.  The box's state is undefined from here on: the host
+                // treats the flag as fatal (NUC3D_ERR_CUDA).
                 if (tid == 0) {
                     atomicOr(bd.flags, kFlagWaitTimeout);
+                    mbar_wait(&mbar[buf], ((k - k0) >> 1) & 1);
                     if (k + 1 < kend) mbar_wait(&mbar[buf ^ 1], ((k + 1 - k0) >> 1) & 1);
                 }
                 return;

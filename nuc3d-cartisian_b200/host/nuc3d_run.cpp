@@ -17,7 +17,8 @@
 //
 // Only the C ABI in include/nuc3d_b200.h is used.  One process, one box,
 // periodic, process topology 1 1 1 (there is no MPI on this path).
-// PhysModel.in Forcing None or Const (the spectral shell forcing).
+// PhysModel.in Forcing None, Const (the spectral shell forcing) or Band (the
+// band forcing at a fixed injection rate, this library's own keyword).
 //
 //   nuc3d_run [case_dir] [--precision fp64|mixed] [--seed S] [--check-decks]
 #include <chrono>
@@ -131,9 +132,13 @@ Case read_case(const std::string &dir) {
         c.desc.riemann = NUC3D_RIEMANN_AUSMP;
     else
         die("Riemann Solver name " + riemann + " does not exist (LF, AUSM, AUSMp)");
-    if (forcing != "None" && forcing != "Const")
-        die("Forcing " + forcing + ": only None and Const are on the B200 path");
-    c.desc.forcing = forcing == "Const" ? NUC3D_FORCING_CONST : NUC3D_FORCING_NONE;
+    // "Band" is this library's band forcing at a fixed injection rate (not a
+    // reference keyword)
+    if (forcing != "None" && forcing != "Const" && forcing != "Band")
+        die("Forcing " + forcing + ": only None, Const and Band are on the B200 path");
+    c.desc.forcing = forcing == "Const"  ? NUC3D_FORCING_CONST
+                     : forcing == "Band" ? NUC3D_FORCING_BAND
+                                         : NUC3D_FORCING_NONE;
     if (model == "NavierStokes3d")
         c.desc.pde_model = NUC3D_NAVIERSTOKES3D;
     else if (model == "Euler3d")

@@ -20,7 +20,7 @@ LIB_PATH = PKG_ROOT / "lib" / "libnuc3d_b200.so"
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2, -3, -4, -5
 ERR_TIMEOUT, ERR_CANCELLED = -6, -7
 INIT_STATE, INIT_TGV, INIT_HIT = 0, 1, 2
-FORCING_NONE, FORCING_CONST = 0, 1
+FORCING_NONE, FORCING_CONST, FORCING_BAND = 0, 1, 2
 WENO5JS, WENO5Z, CRWENO5, WENO7JS, HCCS = 0, 1, 2, 3, 4
 SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5, "weno7js": WENO7JS,
            "hccs": HCCS}
@@ -211,7 +211,7 @@ class BoxDesc:
     powerlaw_exp: float = 0.76
     precision: int = FP64
     quirks: int = QUIRKS_REFERENCE
-    forcing: int = FORCING_NONE     # FORCING_CONST: physicsModel::AddForcing_Const
+    forcing: int = FORCING_NONE     # FORCING_CONST: physicsModel::AddForcing_Const; FORCING_BAND
     forcing_amp: float = 0.01       # PhysModel.in Forcing_amplitude
     forcing_hel: float = 0.01       # Forcing_amplitude_hel
     forcing_k: float = 1.0          # Forcing_wave_k

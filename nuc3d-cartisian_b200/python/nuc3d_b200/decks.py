@@ -11,8 +11,10 @@ from __future__ import annotations
 
 from pathlib import Path
 
-from . import (CONSTANT, EULER3D, FORCING_CONST, FORCING_NONE, NAVIERSTOKES3D, RIEMANNS,
+from . import (CONSTANT, EULER3D, FORCING_BAND, FORCING_CONST, FORCING_NONE, NAVIERSTOKES3D, RIEMANNS,
                SCHEMES, SUTHERLAND, BoxDesc)
+
+_FORCINGS = {"None": FORCING_NONE, "Const": FORCING_CONST, "Band": FORCING_BAND}
 
 _NOT_ON_PATH = ("hccs77", "hccs78", "weno3js", "upwind1st")
 
@@ -59,8 +61,11 @@ def read_decks(dirpath):
         # physicsModel.cpp:88-93 prints a warning and then computes no split
         # at all (solveRiemann finds no such name); refuse instead
         raise ValueError(f"Riemann Solver name {pos[2]} does not exist (LF, AUSM, AUSMp)")
-    if pos[5] not in ("None", "Const"):
-        raise ValueError(f"Forcing {pos[5]}: only None and Const are on the B200 path")
+    # "Band" (band-limited forcing at a fixed injection rate Forcing_amplitude
+    # over 0 < |k| <= Forcing_wave_k) is this library's own keyword; the
+    # reference knows None, Const, ABC and TG
+    if pos[5] not in _FORCINGS:
+        raise ValueError(f"Forcing {pos[5]}: only None, Const and Band are on the B200 path")
     phys = dict(_PHYS_DEFAULTS)
     for k, v in _pairs(" ".join(toks[12:])):
         if k in ("Coriolis", "Centrifugal"):
@@ -91,7 +96,7 @@ def read_decks(dirpath):
                    pde_model=models[pos[3]], visc_model=visc, gamma=phys["Gamma"],
                    mach=phys["Mach"], reynolds=phys["Reynolds"], prandtl=phys["Pt"],
                    t_ref=phys["T_ref"], t_inf=phys["T_inf"],
-                   forcing=FORCING_CONST if pos[5] == "Const" else FORCING_NONE,
+                   forcing=_FORCINGS[pos[5]],
                    forcing_amp=phys["Forcing_amplitude"], forcing_hel=phys["Forcing_amplitude_hel"],
                    forcing_k=phys["Forcing_wave_k"], riemann=RIEMANNS[pos[2]])
     return desc, io, phys
@@ -106,7 +111,7 @@ def write_decks(dirpath, desc, io=None):
         + "scheme_x_vis cd6\nscheme_y_vis cd6\nscheme_z_vis cd6\n")
     model = "NavierStokes3d" if desc.pde_model == NAVIERSTOKES3D else "Euler3d"
     visc = "Constant" if desc.visc_model == CONSTANT else "Sutherland"
-    forcing = "Const" if desc.forcing == FORCING_CONST else "None"
+    forcing = {v: k for k, v in _FORCINGS.items()}[desc.forcing]
     rname = {v: k for k, v in RIEMANNS.items()}[desc.riemann]
     (inp / "PhysModel.in").write_text(
         f"Neqs 5\nEosName IdealGas\nRiemannSolver {rname}\nPDEModel {model}\nViscousModel {visc}\n"

@@ -50,3 +50,30 @@ def forcing_terms(u, v, w, amp, hel, kf):
     fu = f[0] * u + f[1] * v + f[2] * w  # rho0 = 1
     a_aver = float(np.mean(fu))
     return [f[0], f[1], f[2], fu - a_aver], (e_s, e_c, float(theta))
+
+
+def band_forcing_terms(u, v, w, rate, kf):
+    """The amounts the band forcing at a fixed injection rate subtracts from
+    RHS[1..4] (NUC3D_FORCING_BAND, this library's own model: the reference
+    has only the shell forcing above), and (E_b, gain).  The solenoidal part
+    s of every mode with 0 < |k| <= kf is forced as f = s * rate / (2 E_b),
+    E_b = sum over the band of |s|^2 / 2; in physical space with the shell
+    forcing's conventions (density 1, energy equation f.u - <f.u>)."""
+    nz, ny, nx = u.shape
+    n = nx * ny * nz
+    U = [np.fft.fftn(f) / n for f in (u, v, w)]
+    kx = _wavenumbers(nx)[None, None, :]
+    ky = _wavenumbers(ny)[None, :, None]
+    kz = _wavenumbers(nz)[:, None, None]
+    kx, ky, kz = np.broadcast_arrays(kx, ky, kz)
+    kmag0 = np.sqrt(kx * kx + ky * ky + kz * kz)
+    kmag = np.where(kmag0 < 1e-6, 1.0, kmag0)
+    ku = (kx * U[0] + ky * U[1] + kz * U[2]) / kmag
+    s = [U[0] - ku * kx / kmag, U[1] - ku * ky / kmag, U[2] - ku * kz / kmag]
+    band = (kmag0 > 0.0) & (kmag0 <= kf + 1e-12)
+    e_b = float(np.sum(0.5 * sum(np.abs(a) ** 2 for a in s)[band]))
+    gain = rate / (2.0 * e_b) if e_b > 0.0 else 0.0
+    F = [np.where(band, a * gain, 0.0) for a in s]
+    f = [np.fft.ifftn(a).real * n for a in F]
+    fu = f[0] * u + f[1] * v + f[2] * w
+    return [f[0], f[1], f[2], fu - float(np.mean(fu))], (e_b, gain)

@@ -12,12 +12,22 @@
  *     scheme's int member p is a libm pow() call, which differs from x*x by
  *     one ulp for about 0.1% of inputs.  SQ() and PW() below keep them apart.
  *   - Sutherland's T^1.5 is libm pow(T, 1.5) (physicsModel.cpp:220).
+ *
+ * The RHS and the RK stage run their independent lines and cells on POSIX
+ * threads (NUC3D_ORACLE_THREADS, default: the online cores).  Every line and
+ * cell is computed exactly as in a serial run, the running maxima are
+ * combined with fmax (associative; it ignores a NaN operand in any order)
+ * and the residual sum stays serial, so the results are bitwise the same for
+ * any thread count.
  */
+#define _POSIX_C_SOURCE 200809L
 #include "nuc3d_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 /* The reference's schemes hold p = 2 as a runtime member (weno5js.cpp:9,
  * weno5z.cpp:8, crweno5.cpp:15).  Keeping it in a global stops the compiler
@@ -26,6 +36,60 @@ int or_weno_p = 2;
 
 #define SQ(x) ((x) * (x))
 #define PW(x) pow((x), (double)or_weno_p)
+
+/* ------------------------------------------------------------ threads ---- */
+
+#define OR_MAX_THREADS 64
+
+typedef void (*or_range_fn)(void *ctx, int part, long lo, long hi);
+
+typedef struct {
+    or_range_fn fn;
+    void *ctx;
+    int part;
+    long lo, hi;
+} or_task;
+
+static int or_thread_count(void) {
+    const char *e = getenv("NUC3D_ORACLE_THREADS");
+    long t = e ? atol(e) : sysconf(_SC_NPROCESSORS_ONLN);
+    if (t < 1) t = 1;
+    if (t > OR_MAX_THREADS) t = OR_MAX_THREADS;
+    return (int)t;
+}
+
+static void *or_task_main(void *arg) {
+    or_task *t = (or_task *)arg;
+    t->fn(t->ctx, t->part, t->lo, t->hi);
+    return NULL;
+}
+
+/* Runs fn over [0, n) in contiguous parts, one per thread (part 0 on the
+ * calling thread; a part whose thread cannot be started runs on the calling
+ * thread too).  Returns the number of parts. */
+static int or_parallel(long n, or_range_fn fn, void *ctx) {
+    int T = or_thread_count();
+    if (n < T) T = n > 0 ? (int)n : 1;
+    or_task task[OR_MAX_THREADS];
+    pthread_t th[OR_MAX_THREADS];
+    int started[OR_MAX_THREADS] = {0};
+    for (int i = 0; i < T; ++i) {
+        task[i].fn = fn;
+        task[i].ctx = ctx;
+        task[i].part = i;
+        task[i].lo = n * i / T;
+        task[i].hi = n * (i + 1) / T;
+    }
+    for (int i = 1; i < T; ++i) started[i] = pthread_create(&th[i], NULL, or_task_main, &task[i]) == 0;
+    or_task_main(&task[0]);
+    for (int i = 1; i < T; ++i) {
+        if (started[i])
+            pthread_join(th[i], NULL);
+        else
+            or_task_main(&task[i]);
+    }
+    return T;
+}
 
 /* schemes.hpp:14-36 */
 static const double A[3][3] = {{1.0 / 3.0, -7.0 / 6.0, 11.0 / 6.0},
@@ -457,11 +521,21 @@ int or_cd6_field(int nx, int ny, int nz, double dx, const double *in, const doub
 
 /* ------------------------------------------------------------ physics ---- */
 
-void or_con2prim(const or_box *b, const double *const q[5], double *const prim[8]) {
+typedef struct {
+    const or_box *b;
+    const double *const *q;
+    double *const *prim;
+} c2p_ctx;
+
+static void c2p_range(void *vc, int part, long lo, long hi) {
     /* physicsModel.cpp:317-356 */
+    const c2p_ctx *x = (const c2p_ctx *)vc;
+    const or_box *b = x->b;
+    const double *const *q = x->q;
+    double *const *prim = x->prim;
     const double gamma = b->gamma, Mach = b->mach;
-    const long N = (long)b->nx * b->ny * b->nz;
-    for (long n = 0; n < N; ++n) {
+    (void)part;
+    for (long n = lo; n < hi; ++n) {
         double rho = q[0][n];
         double u = q[1][n] / rho;
         double v = q[2][n] / rho;
@@ -483,34 +557,75 @@ void or_con2prim(const or_box *b, const double *const q[5], double *const prim[8
     }
 }
 
+void or_con2prim(const or_box *b, const double *const q[5], double *const prim[8]) {
+    const long N = (long)b->nx * b->ny * b->nz;
+    c2p_ctx x = {b, q, prim};
+    or_parallel(N, c2p_range, &x);
+}
+
+typedef struct {
+    const or_box *b;
+    const double *const *q;
+    const double *const *prim;
+    double *const *fl, *const *fr;
+    int d;
+    double mpart[OR_MAX_THREADS];
+} split_ctx;
+
+static void lf_range(void *vc, int part, long lo, long hi) {
+    split_ctx *x = (split_ctx *)vc;
+    const int d = x->d;
+    const double *const *q = x->q;
+    const double *const *prim = x->prim;
+    double m = x->mpart[part];
+    for (long n = lo; n < hi; ++n) {
+        double un = prim[1 + d][n];
+        double p0 = prim[4][n];
+        double alpha0 = prim[7][n];
+        double Q[5] = {q[0][n], q[1][n], q[2][n], q[3][n], q[4][n]};
+        double lam = fabs(un) + alpha0;
+        m = fmax(lam, m);
+        double flux[5];
+        flux[0] = un * Q[0];
+        flux[1] = un * Q[1];
+        flux[2] = un * Q[2];
+        flux[3] = un * Q[3];
+        flux[1 + d] = un * Q[1 + d] + p0;
+        flux[4] = un * (Q[4] + p0);
+        for (int e = 0; e < 5; ++e) {
+            x->fl[e][n] = 0.5 * (flux[e] + lam * Q[e]);
+            x->fr[e][n] = 0.5 * (flux[e] - lam * Q[e]);
+        }
+    }
+    x->mpart[part] = m;
+}
+
+/* one direction of a split over all cells; the running maximum `run` is
+ * continued part by part with fmax */
+static double split_direction(split_ctx *x, or_range_fn fn, long N, double run) {
+    for (int i = 0; i < OR_MAX_THREADS; ++i) x->mpart[i] = run;
+    int T = or_parallel(N, fn, x);
+    for (int i = 0; i < T; ++i) run = fmax(x->mpart[i], run);
+    return run;
+}
+
 void or_lf_split(const or_box *b, const double *const q[5], const double *const prim[8],
                  double *const fl[3][5], double *const fr[3][5], double eig[3]) {
     /* physicsModel.cpp:520-679.  The three loops run in the reference's order
      * (xi, eta, zeta) so the running fmax values match. */
     const long N = (long)b->nx * b->ny * b->nz;
     double me[3] = {0.0, 0.0, 0.0};
+    split_ctx x;
+    x.b = b;
+    x.q = q;
+    x.prim = prim;
     for (int d = 0; d < 3; ++d) {
         int slot = d;
         if (d == 2 && (b->quirks & OR_Q_ZETA_EIGEN)) slot = 1; /* :653-654 */
-        for (long n = 0; n < N; ++n) {
-            double un = prim[1 + d][n];
-            double p0 = prim[4][n];
-            double alpha0 = prim[7][n];
-            double Q[5] = {q[0][n], q[1][n], q[2][n], q[3][n], q[4][n]};
-            double lam = fabs(un) + alpha0;
-            me[slot] = fmax(lam, me[slot]);
-            double flux[5];
-            flux[0] = un * Q[0];
-            flux[1] = un * Q[1];
-            flux[2] = un * Q[2];
-            flux[3] = un * Q[3];
-            flux[1 + d] = un * Q[1 + d] + p0;
-            flux[4] = un * (Q[4] + p0);
-            for (int e = 0; e < 5; ++e) {
-                fl[d][e][n] = 0.5 * (flux[e] + lam * Q[e]);
-                fr[d][e][n] = 0.5 * (flux[e] - lam * Q[e]);
-            }
-        }
+        x.fl = fl[d];
+        x.fr = fr[d];
+        x.d = d;
+        me[slot] = split_direction(&x, lf_range, N, me[slot]);
     }
     eig[0] = me[0];
     eig[1] = me[1];
@@ -549,33 +664,51 @@ static double ausmp_p_r(double mach, double p) {
     return 0.5 * p * (mach - fabs(mach)) / mach;
 }
 
+static void ausm_range(void *vc, int part, long lo, long hi) {
+    split_ctx *x = (split_ctx *)vc;
+    const int d = x->d;
+    const int plus = x->b->riemann == OR_AUSMP;
+    const double *const *q = x->q;
+    const double *const *prim = x->prim;
+    double *const *fl = x->fl, *const *fr = x->fr;
+    double m = x->mpart[part];
+    for (long n = lo; n < hi; ++n) {
+        double un = prim[1 + d][n];
+        double p0 = prim[4][n];
+        double alpha0 = prim[7][n];
+        double mach = un / alpha0;
+        double machp = ausm_mach_l(mach);
+        double machn = ausm_mach_r(mach);
+        double p_p = plus ? ausmp_p_l(mach, p0) : ausm_p_l(mach, p0);
+        double p_n = plus ? ausmp_p_r(mach, p0) : ausm_p_r(mach, p0);
+        m = fmax(fabs(un) + alpha0, m);
+        for (int e = 0; e < 4; ++e) {
+            fl[e][n] = machp * alpha0 * q[e][n];
+            fr[e][n] = machn * alpha0 * q[e][n];
+        }
+        fl[1 + d][n] = machp * alpha0 * q[1 + d][n] + p_p;
+        fr[1 + d][n] = machn * alpha0 * q[1 + d][n] + p_n;
+        fl[4][n] = machp * alpha0 * q[4][n] + machp * alpha0 * p0;
+        fr[4][n] = machn * alpha0 * q[4][n] + machn * alpha0 * p0;
+    }
+    x->mpart[part] = m;
+}
+
 void or_ausm_split(const or_box *b, const double *const q[5], const double *const prim[8],
                    double *const fl[3][5], double *const fr[3][5], double eig[3]) {
     /* physicsModel.cpp:777-929 (AUSM), :1027-1178 (AUSMp): directions in the
      * reference's order; (machp*alpha0)*Q evaluated left to right. */
     const long N = (long)b->nx * b->ny * b->nz;
-    const int plus = b->riemann == OR_AUSMP;
     double me[3] = {0.0, 0.0, 0.0};
+    split_ctx x;
+    x.b = b;
+    x.q = q;
+    x.prim = prim;
     for (int d = 0; d < 3; ++d) {
-        for (long n = 0; n < N; ++n) {
-            double un = prim[1 + d][n];
-            double p0 = prim[4][n];
-            double alpha0 = prim[7][n];
-            double mach = un / alpha0;
-            double machp = ausm_mach_l(mach);
-            double machn = ausm_mach_r(mach);
-            double p_p = plus ? ausmp_p_l(mach, p0) : ausm_p_l(mach, p0);
-            double p_n = plus ? ausmp_p_r(mach, p0) : ausm_p_r(mach, p0);
-            me[d] = fmax(fabs(un) + alpha0, me[d]);
-            for (int e = 0; e < 4; ++e) {
-                fl[d][e][n] = machp * alpha0 * q[e][n];
-                fr[d][e][n] = machn * alpha0 * q[e][n];
-            }
-            fl[d][1 + d][n] = machp * alpha0 * q[1 + d][n] + p_p;
-            fr[d][1 + d][n] = machn * alpha0 * q[1 + d][n] + p_n;
-            fl[d][4][n] = machp * alpha0 * q[4][n] + machp * alpha0 * p0;
-            fr[d][4][n] = machn * alpha0 * q[4][n] + machn * alpha0 * p0;
-        }
+        x.fl = fl[d];
+        x.fr = fr[d];
+        x.d = d;
+        me[d] = split_direction(&x, ausm_range, N, me[d]);
     }
     eig[0] = me[0];
     eig[1] = me[1];
@@ -629,71 +762,192 @@ static void gather_periodic(const double *src, long base, long stride, int n, do
     }
 }
 
-/* Inviscid derivative of one direction (euler3d.cpp:307-387 solveInv,
- * :23-56 combineFluxLR, :143-253 setDerivatives*Inv): for every equation,
- * F^ = F^+(face) + F^-(face), dF/dx(cell i) = (F^[i+1] - F^[i]) / delta. */
-static void inviscid_direction(const or_box *b, int d, double *const fl[5], double *const fr[5],
-                               double *const df[5]) {
-    int n = dir_len(b, d);
-    long s = dir_stride(b, d);
-    double delta = d == 0 ? b->dx : (d == 1 ? b->dy : b->dz);
-    int na, nc;
-    line_counts(b, d, &na, &nc);
+typedef struct {
+    const or_box *b;
+    int d, n, na, nc, periodic_cr;
+    long s;
+    double delta;
+    double *const *fl, *const *fr, *const *df;
+} inv_ctx;
+
+/* lines lo..hi-1 of the 5 * nc * na (equation, c, a) lines of a direction */
+static void inv_range(void *vc, int part, long lo, long hi) {
+    const inv_ctx *x = (const inv_ctx *)vc;
+    const or_box *b = x->b;
+    const int d = x->d, n = x->n;
+    const long s = x->s;
+    (void)part;
     double *buf = (double *)malloc(sizeof(double) * (size_t)(n + 8));
     double *line = buf + 4;
     double *rp = (double *)malloc(sizeof(double) * (size_t)(n + 1));
     double *rn = (double *)malloc(sizeof(double) * (size_t)(n + 1));
     double *work = (double *)malloc(sizeof(double) * (size_t)(10 * (n + 1)));
-    int periodic_cr = b->scheme[d] == OR_CRWENO5 && !(b->quirks & OR_Q_CRWENO_BOUNDED);
-    for (int e = 0; e < 5; ++e)
-        for (int c = 0; c < nc; ++c)
-            for (int a = 0; a < na; ++a) {
-                long base = line_base(b, d, a, c);
-                gather_periodic(fl[e], base, s, n, line);
-                if (periodic_cr)
-                    reconstruct_line_periodic_crweno(1, n, line, rp, work);
-                else
-                    reconstruct_line_ref(b->scheme[d], 1, b->quirks, n, line, rp, work);
-                gather_periodic(fr[e], base, s, n, line);
-                if (periodic_cr)
-                    reconstruct_line_periodic_crweno(-1, n, line, rn, work);
-                else
-                    reconstruct_line_ref(b->scheme[d], -1, b->quirks, n, line, rn, work);
-                for (int m = 0; m <= n; ++m) rp[m] = rp[m] + rn[m];
-                for (int i = 1; i <= n; ++i) {
-                    double df_loc = rp[i] - rp[i - 1];
-                    df[e][base + (long)(i - 1) * s] = df_loc / delta;
-                }
-            }
+    const long per_e = (long)x->nc * x->na;
+    for (long L = lo; L < hi; ++L) {
+        const int e = (int)(L / per_e);
+        const long r = L - e * per_e;
+        const int c = (int)(r / x->na), a = (int)(r - (long)c * x->na);
+        long base = line_base(b, d, a, c);
+        gather_periodic(x->fl[e], base, s, n, line);
+        if (x->periodic_cr)
+            reconstruct_line_periodic_crweno(1, n, line, rp, work);
+        else
+            reconstruct_line_ref(b->scheme[d], 1, b->quirks, n, line, rp, work);
+        gather_periodic(x->fr[e], base, s, n, line);
+        if (x->periodic_cr)
+            reconstruct_line_periodic_crweno(-1, n, line, rn, work);
+        else
+            reconstruct_line_ref(b->scheme[d], -1, b->quirks, n, line, rn, work);
+        for (int m = 0; m <= n; ++m) rp[m] = rp[m] + rn[m];
+        for (int i = 1; i <= n; ++i) {
+            double df_loc = rp[i] - rp[i - 1];
+            x->df[e][base + (long)(i - 1) * s] = df_loc / x->delta;
+        }
+    }
     free(buf);
     free(rp);
     free(rn);
     free(work);
 }
 
+/* Inviscid derivative of one direction (euler3d.cpp:307-387 solveInv,
+ * :23-56 combineFluxLR, :143-253 setDerivatives*Inv): for every equation,
+ * F^ = F^+(face) + F^-(face), dF/dx(cell i) = (F^[i+1] - F^[i]) / delta. */
+static void inviscid_direction(const or_box *b, int d, double *const fl[5], double *const fr[5],
+                               double *const df[5]) {
+    inv_ctx x;
+    x.b = b;
+    x.d = d;
+    x.n = dir_len(b, d);
+    x.s = dir_stride(b, d);
+    x.delta = d == 0 ? b->dx : (d == 1 ? b->dy : b->dz);
+    line_counts(b, d, &x.na, &x.nc);
+    x.periodic_cr = b->scheme[d] == OR_CRWENO5 && !(b->quirks & OR_Q_CRWENO_BOUNDED);
+    x.fl = fl;
+    x.fr = fr;
+    x.df = df;
+    or_parallel(5L * x.nc * x.na, inv_range, &x);
+}
+
+typedef struct {
+    const or_box *b;
+    int d, n, na;
+    long s;
+    double delta;
+    const double *src;
+    double *dst;
+} cd6_ctx;
+
+static void cd6_range(void *vc, int part, long lo, long hi) {
+    const cd6_ctx *x = (const cd6_ctx *)vc;
+    const int n = x->n;
+    (void)part;
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(n + 8));
+    double *line = buf + 4;
+    for (long L = lo; L < hi; ++L) {
+        const int c = (int)(L / x->na), a = (int)(L - (long)c * x->na);
+        long base = line_base(x->b, x->d, a, c);
+        gather_periodic(x->src, base, x->s, n, line);
+        for (int i = 0; i < n; ++i) x->dst[base + (long)i * x->s] = cd6_at(line, i, x->delta);
+    }
+    free(buf);
+}
+
 /* CD6 along direction d of a periodic field (the halo exchange with one
  * rank is the periodic wrap). */
 static void cd6_direction(const or_box *b, int d, const double *src, double *dst) {
-    int n = dir_len(b, d);
-    long s = dir_stride(b, d);
-    double delta = d == 0 ? b->dx : (d == 1 ? b->dy : b->dz);
-    int na, nc;
-    line_counts(b, d, &na, &nc);
-    double *buf = (double *)malloc(sizeof(double) * (size_t)(n + 8));
-    double *line = buf + 4;
-    for (int c = 0; c < nc; ++c)
-        for (int a = 0; a < na; ++a) {
-            long base = line_base(b, d, a, c);
-            gather_periodic(src, base, s, n, line);
-            for (int i = 0; i < n; ++i) dst[base + (long)i * s] = cd6_at(line, i, delta);
-        }
-    free(buf);
+    cd6_ctx x;
+    int nc;
+    x.b = b;
+    x.d = d;
+    x.n = dir_len(b, d);
+    x.s = dir_stride(b, d);
+    x.delta = d == 0 ? b->dx : (d == 1 ? b->dy : b->dz);
+    line_counts(b, d, &x.na, &nc);
+    x.src = src;
+    x.dst = dst;
+    or_parallel((long)nc * x.na, cd6_range, &x);
 }
 
 static double *alloc_fields(int count, long N, double **ptrs) {
     double *blk = (double *)calloc((size_t)count * (size_t)N, sizeof(double));
     for (int i = 0; i < count; ++i) ptrs[i] = blk + (size_t)i * N;
     return blk;
+}
+
+typedef struct {
+    const or_box *b;
+    const double *const *g;
+    const double *const *prim;
+    double *const *fv;
+} visc_ctx;
+
+/* solveViscousFlux (NaiverStokes3d.cpp:177-303) for cells lo..hi-1 */
+static void visc_range(void *vc, int part, long lo, long hi) {
+    const visc_ctx *x = (const visc_ctx *)vc;
+    const or_box *b = x->b;
+    const double *const *g = x->g;
+    const double *const *prim = x->prim;
+    double *const *fv = x->fv;
+    const double c23 = 2.0 / 3.0;
+    int offdiag = (b->quirks & OR_Q_OFFDIAG_DIV) != 0;
+    (void)part;
+    for (long n = lo; n < hi; ++n) {
+        double ux = g[0][n], uy = g[1][n], uz = g[2][n];
+        double vx = g[3][n], vy = g[4][n], vz = g[5][n];
+        double wx = g[6][n], wy = g[7][n], wz = g[8][n];
+        double tx = g[9][n], ty = g[10][n], tz = g[11][n];
+        double grad = ux + vy + wz;
+        double miu0, coeff0;
+        viscosity(b, prim[5][n], &miu0, &coeff0);
+        double tau_xx = miu0 * (2.0 * ux - c23 * grad);
+        double tau_xy = offdiag ? miu0 * (uy + vx - c23 * grad) : miu0 * (uy + vx);
+        double tau_xz = offdiag ? miu0 * (uz + wx - c23 * grad) : miu0 * (uz + wx);
+        double tau_yy = miu0 * (2.0 * vy - c23 * grad);
+        double tau_yz = offdiag ? miu0 * (vz + wy - c23 * grad) : miu0 * (vz + wy);
+        double tau_zz = miu0 * (2.0 * wz - c23 * grad);
+        double tau_tx = coeff0 * tx, tau_ty = coeff0 * ty, tau_tz = coeff0 * tz;
+        double u = prim[1][n], v = prim[2][n], w = prim[3][n];
+        fv[0][n] = 0.0;
+        fv[1][n] = tau_xx;
+        fv[2][n] = tau_xy;
+        fv[3][n] = tau_xz;
+        fv[4][n] = u * tau_xx + v * tau_xy + w * tau_xz + tau_tx;
+        fv[5][n] = 0.0;
+        fv[6][n] = tau_xy;
+        fv[7][n] = tau_yy;
+        fv[8][n] = tau_yz;
+        fv[9][n] = u * tau_xy + v * tau_yy + w * tau_yz + tau_ty;
+        fv[10][n] = 0.0;
+        fv[11][n] = tau_xz;
+        fv[12][n] = tau_yz;
+        fv[13][n] = tau_zz;
+        fv[14][n] = u * tau_xz + v * tau_yz + w * tau_zz + tau_tz;
+    }
+}
+
+typedef struct {
+    int navier_stokes;
+    double *const *dinv, *const *dvis, *const *rhs;
+} sum_ctx;
+
+/* solveRHS (NaiverStokes3d.cpp:385-499 / euler3d.cpp:389-457) for cells
+ * lo..hi-1, in the reference's summation order */
+static void sum_range(void *vc, int part, long lo, long hi) {
+    const sum_ctx *x = (const sum_ctx *)vc;
+    (void)part;
+    for (int e = 0; e < 5; ++e)
+        for (long n = lo; n < hi; ++n) {
+            double r = x->dinv[e][n];
+            r += x->dinv[5 + e][n];
+            r += x->dinv[10 + e][n];
+            if (x->navier_stokes) {
+                r -= x->dvis[e][n];
+                r -= x->dvis[5 + e][n];
+                r -= x->dvis[10 + e][n];
+            }
+            x->rhs[e][n] = r;
+        }
 }
 
 double or_rhs(const or_box *b, const double *const q[5], double *const rhs[5]) {
@@ -716,6 +970,9 @@ double or_rhs(const or_box *b, const double *const q[5], double *const rhs[5]) {
     else
         or_ausm_split(b, q, (const double *const *)prim, fl, fr, eig);
     for (int d = 0; d < 3; ++d) inviscid_direction(b, d, fl[d], fr[d], dinv + 5 * d); /* :52 */
+    free(blk_fl); /* the split fluxes are not needed again */
+    free(blk_fr);
+    blk_fl = blk_fr = NULL;
 
     double *dvis[15] = {0};
     double *blk_v = NULL;
@@ -729,60 +986,18 @@ double or_rhs(const or_box *b, const double *const q[5], double *const rhs[5]) {
         /* solveViscousFlux (NaiverStokes3d.cpp:177-303) */
         double *fv[15];
         double *blk_fv = alloc_fields(15, N, fv);
-        const double c23 = 2.0 / 3.0;
-        int offdiag = (b->quirks & OR_Q_OFFDIAG_DIV) != 0;
-        for (long n = 0; n < N; ++n) {
-            double ux = g[0][n], uy = g[1][n], uz = g[2][n];
-            double vx = g[3][n], vy = g[4][n], vz = g[5][n];
-            double wx = g[6][n], wy = g[7][n], wz = g[8][n];
-            double tx = g[9][n], ty = g[10][n], tz = g[11][n];
-            double grad = ux + vy + wz;
-            double miu0, coeff0;
-            viscosity(b, prim[5][n], &miu0, &coeff0);
-            double tau_xx = miu0 * (2.0 * ux - c23 * grad);
-            double tau_xy = offdiag ? miu0 * (uy + vx - c23 * grad) : miu0 * (uy + vx);
-            double tau_xz = offdiag ? miu0 * (uz + wx - c23 * grad) : miu0 * (uz + wx);
-            double tau_yy = miu0 * (2.0 * vy - c23 * grad);
-            double tau_yz = offdiag ? miu0 * (vz + wy - c23 * grad) : miu0 * (vz + wy);
-            double tau_zz = miu0 * (2.0 * wz - c23 * grad);
-            double tau_tx = coeff0 * tx, tau_ty = coeff0 * ty, tau_tz = coeff0 * tz;
-            double u = prim[1][n], v = prim[2][n], w = prim[3][n];
-            fv[0][n] = 0.0;
-            fv[1][n] = tau_xx;
-            fv[2][n] = tau_xy;
-            fv[3][n] = tau_xz;
-            fv[4][n] = u * tau_xx + v * tau_xy + w * tau_xz + tau_tx;
-            fv[5][n] = 0.0;
-            fv[6][n] = tau_xy;
-            fv[7][n] = tau_yy;
-            fv[8][n] = tau_yz;
-            fv[9][n] = u * tau_xy + v * tau_yy + w * tau_yz + tau_ty;
-            fv[10][n] = 0.0;
-            fv[11][n] = tau_xz;
-            fv[12][n] = tau_yz;
-            fv[13][n] = tau_zz;
-            fv[14][n] = u * tau_xz + v * tau_yz + w * tau_zz + tau_tz;
-        }
+        visc_ctx vx_ = {b, (const double *const *)g, (const double *const *)prim, fv};
+        or_parallel(N, visc_range, &vx_);
+        free(blk_g);
         /* setDerivativesVis (NaiverStokes3d.cpp:305-369) */
         blk_v = alloc_fields(15, N, dvis);
         for (int d = 0; d < 3; ++d)
             for (int e = 0; e < 5; ++e) cd6_direction(b, d, fv[d * 5 + e], dvis[d * 5 + e]);
-        free(blk_g);
         free(blk_fv);
     }
     /* solveRHS: NaiverStokes3d.cpp:385-499 / euler3d.cpp:389-457 */
-    for (int e = 0; e < 5; ++e)
-        for (long n = 0; n < N; ++n) {
-            double r = dinv[e][n];
-            r += dinv[5 + e][n];
-            r += dinv[10 + e][n];
-            if (b->navier_stokes) {
-                r -= dvis[e][n];
-                r -= dvis[5 + e][n];
-                r -= dvis[10 + e][n];
-            }
-            rhs[e][n] = r;
-        }
+    sum_ctx sx = {b->navier_stokes, dinv, dvis, rhs};
+    or_parallel(N, sum_range, &sx);
     free(blk_prim);
     free(blk_fl);
     free(blk_fr);
@@ -797,22 +1012,38 @@ double or_rhs(const or_box *b, const double *const q[5], double *const rhs[5]) {
 
 /* ------------------------------------------------------------- RK3 ------- */
 
-void or_rk3_stage(int stage, long n, double dt, const double *const rhs[5],
-                  const double *const un[5], double *const ui[5]) {
+typedef struct {
+    int stage;
+    double dt;
+    const double *const *rhs, *const *un;
+    double *const *ui;
+} rk_ctx;
+
+static void rk_range(void *vc, int part, long lo, long hi) {
     /* TVD-RK3.h:9-12 coefficients; TVD-RK3.cpp:76-196 */
     static const double c[3][2] = {{1.0, 1.0}, {3.0 / 4.0, 1.0 / 4.0}, {1.0 / 3.0, 2.0 / 3.0}};
+    const rk_ctx *x = (const rk_ctx *)vc;
+    const int stage = x->stage;
+    const double dt = x->dt;
+    (void)part;
     for (int e = 0; e < 5; ++e)
-        for (long i = 0; i < n; ++i) {
-            double r = -rhs[e][i];
+        for (long i = lo; i < hi; ++i) {
+            double r = -x->rhs[e][i];
             if (stage == 0) {
-                double u = ui[e][i];
-                ui[e][i] = c[0][0] * u + c[0][1] * r * dt;
+                double u = x->ui[e][i];
+                x->ui[e][i] = c[0][0] * u + c[0][1] * r * dt;
             } else {
-                double u = un[e][i];
-                double uk = ui[e][i];
-                ui[e][i] = c[stage][0] * u + c[stage][1] * (r * dt + uk);
+                double u = x->un[e][i];
+                double uk = x->ui[e][i];
+                x->ui[e][i] = c[stage][0] * u + c[stage][1] * (r * dt + uk);
             }
         }
+}
+
+void or_rk3_stage(int stage, long n, double dt, const double *const rhs[5],
+                  const double *const un[5], double *const ui[5]) {
+    rk_ctx x = {stage, dt, rhs, un, ui};
+    or_parallel(n, rk_range, &x);
 }
 
 void or_run_steps(const or_box *b, double cfl, int nsteps, double *const q[5], double *dt,

@@ -38,6 +38,7 @@ def parsed(text):
     dict(nx=16, ny=16, nz=16, riemann=2, pde_model=0),
     dict(nx=24, ny=16, nz=12, scheme=(4, 2, 4)),
     dict(nx=32, ny=32, nz=32, forcing=1, forcing_amp=0.02, forcing_hel=0.1, forcing_k=2.0),
+    dict(nx=32, ny=32, nz=32, forcing=2, forcing_amp=0.3, forcing_k=2.0),
 ])
 def test_driver_reads_decks_like_the_python_reader(driver, tmp_path, kw):
     import nuc3d_b200 as nb

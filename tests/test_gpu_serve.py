@@ -216,6 +216,44 @@ def test_spectral_forcing_matches_restatement(nb, kf, shape):
         np.testing.assert_allclose(got, terms[e - 1], rtol=0, atol=atol)
 
 
+@pytest.mark.parametrize("kf,shape,prec", [(2.0, (32, 32, 32), 0), (1.5, (24, 20, 28), 0),
+                                           (2.0, (32, 32, 32), 1)])
+def test_band_forcing_matches_restatement(nb, kf, shape, prec):
+    """The band forcing at a fixed injection rate (NUC3D_FORCING_BAND) against
+    its numpy restatement (forcing_oracle.band_forcing_terms): the RHS with
+    forcing minus the RHS without is the forcing, in FP64 and (forcing in
+    FP64, RHS in FP32) in mixed precision."""
+    import torch
+    from oracle_ctypes import Box, Oracle
+    from forcing_oracle import band_forcing_terms
+    base = nb.BoxDesc(*shape, mach=1.0, reynolds=300.0, scheme=(nb.WENO5Z,) * 3, precision=prec)
+    forced = nb.BoxDesc(**{**base.__dict__, "forcing": nb.FORCING_BAND, "forcing_amp": 0.2,
+                           "forcing_k": kf})
+    with nb.Solver(nb.BoxDesc(*shape, mach=1.0)) as s:
+        s.init_state({"kind": "hit", "seed": 4, "k_peak": 2.0, "mach_t": 0.4})
+        q = s.get_state()
+    rhs = {}
+    for name, d in (("off", base), ("on", forced)):
+        with nb.Solver(d) as s:
+            s.set_state(q)
+            out = [torch.zeros(d.shape, dtype=torch.float64, device="cuda") for _ in range(5)]
+            s.rhs(out)
+            rhs[name] = [o.cpu().numpy() for o in out]
+    prim = Oracle().con2prim(Box(*shape, mach=1.0), q)
+    terms, (e_b, gain) = band_forcing_terms(prim[1], prim[2], prim[3], 0.2, kf)
+    assert e_b > 0 and gain > 0
+    assert np.array_equal(rhs["on"][0], rhs["off"][0])
+    # FP64: the forcing to 1e-12 of the larger of the forcing and the RHS;
+    # mixed: the RHS is held in FP32, so its rounding (1e-7 of the RHS) shows
+    rel = 1e-12 if prec == 0 else 3e-7
+    for e in range(1, 5):
+        got = rhs["off"][e] - rhs["on"][e]
+        scale = np.max(np.abs(terms[e - 1]))
+        assert scale > 0
+        atol = rel * max(scale, np.max(np.abs(rhs["off"][e])))
+        np.testing.assert_allclose(got, terms[e - 1], rtol=0, atol=atol)
+
+
 @pytest.mark.parametrize("tag", ["a", "b"])
 def test_spectral_forcing_matches_reference_golden(nb, tag):
     """The device forced RHS against the reference's own (AddForcing_Const run

@@ -231,6 +231,35 @@ def test_forcing_restatement_matches_reference_golden(tag):
         assert np.abs(d[e] - terms[e - 1]).max() <= 1e-12 * max(scale, np.abs(z[f"{tag}_rhs_off"][e]).max())
 
 
+def test_band_forcing_restatement_injects_its_rate():
+    """forcing_oracle.band_forcing_terms (the band forcing at a fixed
+    injection rate, a model the reference does not have: its parity is pinned
+    to this restatement only) checked by its defining properties: the mean
+    power <f.u> equals the rate, the force is solenoidal and band-limited
+    (0 < |k| <= k_f), and the energy source has zero mean."""
+    from forcing_oracle import band_forcing_terms
+    rng = np.random.default_rng(5)
+    nz, ny, nx = 12, 10, 16
+    u, v, w = (rng.standard_normal((nz, ny, nx)) for _ in range(3))
+    rate, kf = 0.37, 2.0
+    terms, (e_b, gain) = band_forcing_terms(u, v, w, rate, kf)
+    f = terms[:3]
+    assert abs(np.mean(f[0] * u + f[1] * v + f[2] * w) - rate) <= 1e-13 * rate
+    assert abs(np.mean(terms[3])) <= 1e-14 * np.abs(terms[3]).max()
+    F = [np.fft.fftn(a) for a in f]
+    kx = np.fft.fftfreq(nx, 1.0 / nx)[None, None, :]
+    ky = np.fft.fftfreq(ny, 1.0 / ny)[None, :, None]
+    kz = np.fft.fftfreq(nz, 1.0 / nz)[:, None, None]
+    kx, ky, kz = np.broadcast_arrays(kx, ky, kz)
+    kmag = np.sqrt(kx * kx + ky * ky + kz * kz)
+    big = max(np.abs(a).max() for a in F)
+    outside = (kmag == 0) | (kmag > kf + 1e-9)
+    assert all(np.abs(a[outside]).max() <= 1e-12 * big for a in F)
+    div = kx * F[0] + ky * F[1] + kz * F[2]
+    assert np.abs(div).max() <= 1e-12 * big * kf
+    assert e_b > 0 and np.isclose(gain, rate / (2.0 * e_b))
+
+
 @pytest.mark.parametrize("kind", ["smooth", "rough"])
 @pytest.mark.parametrize("up", [1, -1])
 def test_hccs_reconstruct_matches_reference_golden(O, kind, up):

@@ -61,3 +61,10 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     p = dummy.data_ptr()
     assert fn(1, nx, ny, nz, p, p, p, p, None) == nb.ERR_INVALID
     assert b"static scratch" in nb.lib().nuc3d_last_error()
+    # the allocating entry point's line-length rule holds here too: nx = 4097
+    # fits the scratch (2*4097 doubles) but is refused by both entry points
+    assert fn(1, 4097, 1, 1, p, p, p, p, None) == nb.ERR_INVALID
+    assert b"nx <= 4096" in nb.lib().nuc3d_last_error()
+    assert nb.lib().nuc3d_reconstruct(nb.CRWENO5, 1, 0, 4097, 1, 1, C.c_void_p(p),
+                                      C.c_void_p(p), C.c_void_p(p), C.c_void_p(p),
+                                      None) == nb.ERR_INVALID
