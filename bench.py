@@ -11,8 +11,10 @@ CFL 0.5.  One "step" is one TVD-RK3 step (3 RHS evaluations) of every box.
 The metric is cell-updates/s (cells x steps / s) over the whole job.
 
 * ``value``: FP64 path, state resident in HBM, device-timed with CUDA events
-  (max over ranks).  The state (671 MB per box) is larger than the 126 MB L2,
-  so no flush is needed between steps.
+  (max over ranks), the median of --repeats timed regions of exactly --steps
+  steps each.  The state (671 MB per box) is larger than the 126 MB L2, so
+  no flush is needed between steps.  ``clocks``: NVML samples every 10 ms
+  over the timed regions.
 * ``e2e``: the same metric through the C ABI with host buffers: each step
   uploads the state from pinned host memory (nuc3d_set_state_host), advances
   one step with the dt/residual read back (nuc3d_step), and downloads the
@@ -22,6 +24,13 @@ The metric is cell-updates/s (cells x steps / s) over the whole job.
 * ``roofline``: the dominant kernel (inviscid WENO sweep), algorithmic FP64
   flops per launch over its event-timed average launch duration, against the
   FP64 FMA rate measured in the same run (nuc3d_probe_peak).
+* ``long_horizon``: FP64 and mixed advanced 2000 steps from the same state,
+  TKE, dissipation and spectrum compared over the run.
+* ``config3``: forced HIT at 384^3, turbulent Mach 0.6, band forcing at a
+  fixed injection rate, hccs and CRWENO5, FP64 and mixed (CFL 0.4).
+* ``ensemble`` / ``served``: the batched 64-box ensemble and the served
+  request stream (continuous batching vs a serial FP64 queue, with the same
+  mix run as one batch as its ceiling).
 * ``cpu_baseline``: the reference's own code (oracle/_ref) on host cores.
 
 With --gpus N > 1 (torchrun), every rank advances its own box (independent
@@ -93,6 +102,7 @@ def config_dict(n_gpus, reynolds):
         "parallelism": f"replicas x{n_gpus} (one box per GPU, no collective)",
         "l2_flush": (f"not needed: {40 * NX ** 3 / 1e6:.0f} MB FP64 state per box > 126 MB L2"
                      if 40 * NX ** 3 > 126e6 else "state smaller than L2 (profiling size only)"),
+        "timing": "median of the repeats, each exactly `steps` steps between barriers",
     }
 
 
@@ -140,48 +150,98 @@ def cpu_sample(n, steps, warm, reynolds, workers):
 
 
 # ------------------------------------------------------------ clocks -------
-class ClockSampler:
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+_REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+            ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, gpu_index):
-        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+
+class ClockSampler:
+    """SM clock, power and throttle reasons of one GPU sampled while a timed
+    region runs (read only: NVML queries, every 10 ms, on a thread; nvidia-smi
+    at 200 ms where NVML is unavailable).  The GPU is matched by PCI bus id,
+    so CUDA_VISIBLE_DEVICES does not shift it."""
+
+    def __init__(self, dev_index):
+        import threading
+        self.samples = []  # (sm_mhz, power_w, reasons bitmask)
+        self.smax = None
         self.proc = None
+        self.path = None
+        self._stop = threading.Event()
+        self._thread = None
+        self.source = "nvml"
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(dev_index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            try:
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except pynvml.NVMLError:
+                h = pynvml.nvmlDeviceGetHandleByIndex(dev_index)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append((
+                            float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)),
+                            pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0,
+                            int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                    except pynvml.NVMLError:
+                        pass
+                    self._stop.wait(0.01)
+            self._thread = threading.Thread(target=run, daemon=True)
+            self._thread.start()
+        except Exception:
+            self._start_smi(dev_index)
+
+    def _start_smi(self, gpu_index):
+        self.source = "nvidia-smi"
+        fields = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_power_cap")
+        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
+                ["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={fields}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, power, reasons = [], None, [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.path.read_text().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 7:
-                continue
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
+        elif self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(parts[0]))
-                smax = float(parts[1])
-                power.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[3:7]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "power_w_median": statistics.median(power) if power else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            for line in self.path.read_text().splitlines():
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 7:
+                    continue
+                try:
+                    sm, self.smax, pw = float(parts[0]), float(parts[1]), float(parts[2])
+                except ValueError:
+                    continue
+                mask = sum(bit for (nm, bit), v in zip(_REASONS[:4], parts[3:7])
+                           if v.lower() == "active")
+                self.samples.append((sm, pw, mask))
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        sm = [a for a, _, _ in self.samples]
+        pw = [b for _, b, _ in self.samples]
+        reasons = sorted({nm for _, _, m in self.samples for nm, bit in _REASONS if m & bit})
+        counts = {nm: sum(1 for _, _, m in self.samples if m & bit) for nm, bit in _REASONS}
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                "sm_mhz_min": min(sm) if sm else None,
+                "power_w_median": statistics.median(pw) if pw else None,
+                "samples": len(sm), "source": self.source, "reasons": reasons,
+                "reason_samples": {k: v for k, v in counts.items() if v}}
 
 
 # ------------------------------------------------------------ GPU arm ------
@@ -220,6 +280,12 @@ def run_b200(args, rank, world, local_rank):
         barrier()
         return e0.elapsed_time(e1)
 
+    def timed_repeats(solver, k, repeats):
+        """`repeats` timed regions of exactly k steps each (barrier + device
+        sync on both sides, CUDA events on the launching stream); the max
+        over ranks of each."""
+        return [max_over_ranks(timed_steps(solver, k)) for _ in range(repeats)]
+
     peak64 = nb.probe_peak(nb.FP64)
     peak32 = nb.probe_peak(nb.MIXED)
 
@@ -230,13 +296,16 @@ def run_b200(args, rank, world, local_rank):
     s64.sync()
     clocks = ClockSampler(local_rank)
     launches0 = s64.launch_count()
-    ms = timed_steps(s64, args.steps)
-    launches = s64.launch_count() - launches0
+    reps_ms = timed_repeats(s64, args.steps, args.repeats)
+    launches = (s64.launch_count() - launches0) // args.repeats
     clock_info = clocks.stop()
     s64.sync()
-    ms_max = max_over_ranks(ms)
+    ms_max = statistics.median(reps_ms)
     ms_per_step = ms_max / args.steps
     value = whole_job_rate(cells, world, ms_per_step * 1e-3)
+    timing = {"repeats": args.repeats, "steps_per_repeat": args.steps,
+              "ms_per_step_each": [m / args.steps for m in reps_ms],
+              "value_from": "median repeat", "timed_s_total": sum(reps_ms) / 1e3}
 
     tuning64 = s64.tuning()
     # ---- per-kernel event timing (separate short pass, same workload)
@@ -302,7 +371,7 @@ def run_b200(args, rank, world, local_rank):
         sm.set_state(q)
         sm.step(args.warmup, CFL, stats=False)
         sm.sync()
-        ms_m = max_over_ranks(timed_steps(sm, args.steps))
+        ms_m = statistics.median(timed_repeats(sm, args.steps, args.repeats))
         tuning32 = sm.tuning()
         sm.profile(True)
         sm.step(2, CFL, stats=False)
@@ -360,6 +429,9 @@ def run_b200(args, rank, world, local_rank):
 
     schemes = None if args.skip_schemes else run_schemes(args, desc, q, stream, timed_steps,
                                                          max_over_ranks)
+    long_horizon = None if (args.skip_long or args.skip_mixed) else run_long_horizon(
+        args, desc, q, stream)
+    config3 = None if args.skip_config3 else run_config3(args, stream)
     ensemble = None if args.skip_ensemble else run_ensemble(args, stream, barrier, max_over_ranks,
                                                             world, rank)
     served = None if (args.skip_serve or world > 1) else run_served(args)
@@ -390,10 +462,13 @@ def run_b200(args, rank, world, local_rank):
                 "resident": {"value": world * cells * e2e_steps / res_s, "unit": UNIT,
                              "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 16}},
         "gpu_launches": launches,
+        "timing": timing,
         "roofline": roofline,
         "clocks": clock_info,
         "mixed": mixed,
         "schemes": schemes,
+        "long_horizon": long_horizon,
+        "config3": config3,
         "ensemble": ensemble,
         "served": served,
         "cpu_baseline": cpu,
@@ -408,6 +483,152 @@ def spectrum_diff(a, b):
     import numpy as np
     on = b > 1e-10 * b.sum()
     return float(np.max(np.abs(a[on] - b[on]) / b[on]))
+
+
+# -------------------------------------------------------- long horizon -----
+LONG_KEYS = ("kinetic", "dissipation", "enstrophy", "re_lambda", "mach_t", "u_rms")
+
+
+def run_long_horizon(args, desc, q, stream):
+    """The 256^3 decaying HIT advanced --long-steps steps in FP64 and in mixed
+    precision from the same state, with the device statistics (FP64
+    reductions, postproc::solveQ) every --long-every steps and the
+    kinetic-energy spectrum (postproc::solveFFT) at the middle and the end:
+    how far the mixed form's TKE, dissipation and spectrum move from the
+    FP64 path's over the run."""
+    import numpy as np
+    import torch
+    import nuc3d_b200 as nb
+    nsteps, every = args.long_steps, args.long_every
+    logs, spectra, dev_ms, times = {}, {}, {}, {}
+    for name, prec in (("fp64", nb.FP64), ("mixed", nb.MIXED)):
+        d = nb.BoxDesc(**{**desc.__dict__, "precision": prec})
+        with nb.Solver(d, stream=stream) as a:
+            a.set_state(q)
+            log, spec, ms = [a.stats()], {}, 0.0
+            done = 0
+            while done < nsteps:
+                k = min(every, nsteps - done)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                a.step(k, CFL, stats=False)
+                e1.record(stream)
+                a.sync()
+                ms += e0.elapsed_time(e1)
+                done += k
+                log.append(a.stats())
+                if done == nsteps // 2 or done == nsteps:
+                    spec[done] = a.spectra()[0]
+            logs[name], spectra[name], dev_ms[name], times[name] = log, spec, ms, a.time()
+    rel = {key: [abs(m[key] - f[key]) / abs(f[key]) for m, f in zip(logs["mixed"], logs["fp64"])]
+           for key in LONG_KEYS}
+
+    def first_over(key, bar=0.005):
+        for i, v in enumerate(rel[key]):
+            if v > bar:
+                return i * every
+        return None
+    ke0 = logs["fp64"][0]
+    tau = ke0["eddy_turnover"]
+    return {
+        "workload": f"{desc.nx}^3 decaying HIT (the headline field), WENO5-Z, CFL {CFL}, "
+                    f"{nsteps} steps FP64 and mixed from the same state",
+        "steps": nsteps, "stats_every_steps": every,
+        "sim_time": times["fp64"],
+        "eddy_turnover_time_initial": tau,
+        "eddy_turnovers": times["fp64"] / tau if tau else None,
+        "ms_per_step": {k: v / nsteps for k, v in dev_ms.items()},
+        "cell_updates_per_s": {k: desc.cells * nsteps / (v * 1e-3) for k, v in dev_ms.items()},
+        "tke_max_rel_diff": max(rel["kinetic"]),
+        "dissipation_max_rel_diff": max(rel["dissipation"]),
+        "max_rel_diff": {k: max(v) for k, v in rel.items()},
+        "first_step_over_0.5pct": {k: first_over(k) for k in ("kinetic", "dissipation")},
+        "spectrum_kin_max_rel_diff": {str(k): spectrum_diff(spectra["mixed"][k], spectra["fp64"][k])
+                                      for k in spectra["fp64"]},
+        "tke_decay": logs["fp64"][-1]["kinetic"] / ke0["kinetic"],
+        "fp64_series": {k: [round(v[k], 10) for v in logs["fp64"]] for k in LONG_KEYS},
+        "mixed_series": {k: [round(v[k], 10) for v in logs["mixed"]] for k in ("kinetic", "dissipation")},
+        "spectrum_kin_fp64_end": [float(v) for v in spectra["fp64"][nsteps]],
+    }
+
+
+# ------------------------------------------------------------- config 3 ----
+def run_config3(args, stream):
+    """Forced isotropic turbulence with shocklets: --c3-n^3 (384) periodic
+    box, seeded solenoidal field of the headline's spectrum at turbulent Mach
+    0.6 (M 1, Re from Re_lambda 100), the band forcing on 0 < |k| <= 2 at a
+    fixed injection rate equal to the initial dissipation rate, CFL 0.4.
+    hccs (the reference's hybrid compact-WENO switch, CRWENO5 rows with linear
+    compact rows where smooth) and plain CRWENO5, FP64 and mixed: device-timed
+    steps, the mixed form's per-field relative L2 from FP64 after --c3-steps
+    steps, and the mixed hccs run continued to --c3-long steps, checked finite
+    every 100."""
+    import numpy as np
+    import torch
+    import nuc3d_b200 as nb
+    n = args.c3_n
+    cfl = 0.4
+    init = {"kind": "hit", "seed": 0, "k_peak": K_PEAK, "mach_t": 0.6, "re_lambda": RE_LAMBDA}
+    with nb.Solver(nb.BoxDesc(n, n, n, mach=1.0), stream=stream) as s0:
+        info = s0.init_state(init)
+        st0 = s0.stats()
+    rate = st0["dissipation"]
+    out = {"workload": f"forced HIT {n}^3, Mt 0.6, M 1, Re_lambda {RE_LAMBDA:g} (Re "
+                       f"{info['reynolds']:.6g}), band forcing 0<|k|<=2 at injection rate "
+                       f"{rate:.6g} (the initial dissipation rate), CFL {cfl}",
+           "cells": n ** 3, "reynolds": info["reynolds"], "injection_rate": rate,
+           "initial": {k: st0[k] for k in ("kinetic", "dissipation", "mach_t", "re_lambda")}}
+    for sname, sch, long_mixed in (("hccs", nb.HCCS, True), ("crweno5", nb.CRWENO5, False)):
+        row, finals = {}, {}
+        for pname, prec in (("fp64", nb.FP64), ("mixed", nb.MIXED)):
+            d = nb.BoxDesc(n, n, n, mach=1.0, scheme=(sch,) * 3, precision=prec,
+                           forcing=nb.FORCING_BAND, forcing_amp=rate, forcing_k=2.0)
+            with nb.Solver(d, stream=stream) as s:
+                s.init_state(init)
+                s.step(args.warmup, cfl, stats=False)
+                s.sync()
+                k = max(3, min(args.steps, 10))
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                s.step(k, cfl, stats=False)
+                e1.record(stream)
+                s.sync()
+                ms = e0.elapsed_time(e1) / k
+                s.step(max(0, args.c3_steps - args.warmup - k), cfl, stats=False)
+                s.sync()
+                finals[pname] = s.get_state()
+                st = s.stats()
+                r = {"ms_per_step": ms, "cell_updates_per_s": n ** 3 / (ms * 1e-3),
+                     "kinetic": st["kinetic"], "dissipation": st["dissipation"],
+                     "mach_t": st["mach_t"],
+                     "finite": bool(all(np.isfinite(a).all() for a in finals[pname]))}
+                if prec == nb.MIXED and long_mixed:
+                    done, ok, kes = args.c3_steps, True, []
+                    while done < args.c3_long:
+                        try:
+                            s.step(min(100, args.c3_long - done), cfl, stats=False)
+                            s.sync()
+                        except nb.Nuc3dError as e:
+                            ok = False
+                            r["error"] = f"after {done} steps: {e}"
+                            break
+                        done = min(done + 100, args.c3_long)
+                        kes.append(s.stats()["kinetic"])
+                    r["long_steps"] = done
+                    r["long_finite"] = ok
+                    r["long_kinetic_every_100"] = kes
+            row[pname] = r
+        errs = [float(np.linalg.norm(a - b) / np.linalg.norm(b))
+                for a, b in zip(finals["mixed"], finals["fp64"])]
+        del finals
+        row["rel_l2_vs_fp64_per_field"] = errs
+        row["rel_l2_vs_fp64"] = max(errs)
+        row["compared_after_steps"] = args.c3_steps
+        row["mixed_speedup"] = row["fp64"]["ms_per_step"] / row["mixed"]["ms_per_step"]
+        out[sname] = row
+    return out
 
 
 # ------------------------------------------------------------- schemes -----
@@ -521,10 +742,11 @@ def served_requests(nreq, seed, rate):
     return out
 
 
-def run_stream(reqs, precision, max_resident, budget_bytes):
-    """Submits the requests at their arrival times to a fresh server and
-    collects every result (final state copied to the host) on a second
-    thread.  Latency = completion - submission on the server's clock."""
+def run_stream(reqs, precision, max_resident, budget_bytes, burst=False):
+    """Submits the requests at their arrival times (burst: all at once) to a
+    fresh server and collects every result (final state copied to the host)
+    on a second thread.  Latency = completion - submission on the server's
+    clock."""
     import threading
     import nuc3d_b200 as nb
     srv = nb.Server(precision=precision, budget_bytes=budget_bytes, max_resident=max_resident)
@@ -542,7 +764,7 @@ def run_stream(reqs, precision, max_resident, budget_bytes):
     th.start()
     t0 = time.perf_counter()
     for ta, d, steps, init in reqs:
-        delay = t0 + ta - time.perf_counter()
+        delay = 0.0 if burst else t0 + ta - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
         srv.submit(d, steps, CFL, init=init, want_state=True)
@@ -566,6 +788,11 @@ def run_stream(reqs, precision, max_resident, budget_bytes):
         "peak_resident": st["peak_resident"],
         "peak_resident_gb": st["peak_resident_bytes"] / 1e9,
         "chunks": st["chunks"],
+        "batch_steps": st["batch_steps"],
+        "steps_per_chunk": st["batch_steps"] / max(st["chunks"], 1),
+        "graph_captures": st["graph_captures"],
+        "busy_s": st["busy_s"],
+        "busy_frac": st["busy_s"] / span,
         "kernel_launches": st["launches"],
     }
 
@@ -587,9 +814,14 @@ def run_served(args):
                                  ("crweno5", nb.CRWENO5))},
         "mixed_continuous": run_stream(reqs, nb.MIXED, 256, budget),
         "fp64_serial": run_stream(reqs, nb.FP64, 1, budget),
+        # the same 32 solves submitted at once: the whole mix runs as one
+        # batch from the start, the ceiling of the continuous stream
+        "mixed_one_batch": run_stream(reqs, nb.MIXED, 256, budget, burst=True),
     }
     res["solves_per_s_ratio"] = (res["mixed_continuous"]["solves_per_s"]
                                  / res["fp64_serial"]["solves_per_s"])
+    res["continuous_vs_one_batch"] = (res["mixed_continuous"]["cell_updates_per_s"]
+                                      / res["mixed_one_batch"]["cell_updates_per_s"])
     return res
 
 
@@ -632,6 +864,15 @@ def main():
     ap.add_argument("--skip-schemes", action="store_true")
     ap.add_argument("--ensemble-boxes", type=int, default=64)
     ap.add_argument("--accuracy-steps", type=int, default=100)
+    ap.add_argument("--repeats", type=int, default=5,
+                    help="timed regions of --steps steps each; value from the median")
+    ap.add_argument("--skip-long", action="store_true")
+    ap.add_argument("--long-steps", type=int, default=2000)
+    ap.add_argument("--long-every", type=int, default=100)
+    ap.add_argument("--skip-config3", action="store_true")
+    ap.add_argument("--c3-n", type=int, default=384)
+    ap.add_argument("--c3-steps", type=int, default=100, help="steps compared FP64 vs mixed")
+    ap.add_argument("--c3-long", type=int, default=500, help="mixed steps checked for finiteness")
     ap.add_argument("--skip-serve", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-rate", type=float, default=20.0, help="mean arrivals per second")
@@ -642,6 +883,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.repeats < 1:
+        ap.error("--repeats must be >= 1")
     NX = args.n
     METRIC = METRIC.replace("256^3", f"{NX}^3")
     from nuc3d_b200.replicas import rank_info

@@ -271,7 +271,8 @@ NUC3D_API int nuc3d_batch_init_state(nuc3d_batch *b, int box_id, const nuc3d_ini
  * max_resident are resident; it allocates the box, uploads h_q0 or generates
  * the initial state, and advances all resident solves together in chunks of
  * steps (the batch's CUDA graph replayed; a chunk is no longer than the
- * shortest remaining solve and about chunk_ms long), so solves join and leave
+ * shortest remaining solve and about chunk_ms long, its step time predicted
+ * from the last chunk's device time per resident cell), so solves join and leave
  * the running batch between chunks (continuous batching).  A finished solve's
  * state is copied to h_q_out, its memory released and its result posted.
  * A solve gives the same final state alone and in any mix: no arithmetic
@@ -312,6 +313,8 @@ typedef struct nuc3d_serve_stats {
     int queued, resident, peak_resident, pad;
     long long resident_bytes, peak_resident_bytes, budget_bytes;
     long long batch_steps, chunks, cell_updates, launches;
+    long long graph_captures; /* CUDA-graph captures of the batch step (one per
+                                 change of the resident set that is stepped) */
     double busy_s;            /* wall time spent advancing resident solves */
     double now_s;             /* the server's clock */
 } nuc3d_serve_stats;

@@ -643,6 +643,7 @@ int Engine::step(int nsteps) {
             ECK(e);
             graph_ = g;
             ECK(cudaGraphInstantiate(&exec_, graph_, 0));
+            ++graph_captures;
             launches = before;
         }
         for (int s = 0; s < nsteps; ++s) ECK(cudaGraphLaunch(exec_, stream_));

@@ -63,6 +63,7 @@ public:
 
     // accounting
     long long launches = 0;
+    long long graph_captures = 0;  // step graphs captured (one per membership change)
     bool prof_on = false;
     double prof_ms[NUC3D_PROF_CLASSES] = {};
     long long prof_n[NUC3D_PROF_CLASSES] = {};

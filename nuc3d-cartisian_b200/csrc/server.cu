@@ -9,7 +9,9 @@
 //   2. advances every resident solve together by one chunk of steps (the
 //      batch's CUDA graph replayed), the chunk no longer than the shortest
 //      remaining solve and sized to about chunk_ms of device time, so that
-//      arrivals join within a chunk;
+//      arrivals join within a chunk.  The step time of a new composition is
+//      predicted from the last chunk's time per resident cell-step (the
+//      first chunk of all is one step, to measure);
 //   3. retires the solves whose step count is reached: final state to the
 //      client's host buffer, device memory released, result posted.
 // Solves therefore join and leave the running batch between chunks
@@ -240,7 +242,9 @@ private:
         if (!eng) return;
         std::vector<Resident> res;
         long long used = 0;
-        double ms_per_step = 0.0;  // of the current batch composition
+        // device milliseconds per resident cell and step, from the last chunk:
+        // predicts the step time of any composition (0: nothing measured yet)
+        double ms_per_cell_step = 0.0;
         for (;;) {
             std::vector<Queued> adm;
             bool stopping;
@@ -275,7 +279,6 @@ private:
                     continue;
                 }
                 res.push_back(r);
-                ms_per_step = 0.0;  // composition changed
             }
             if (!adm.empty()) {
                 std::lock_guard<std::mutex> lk(mu_);
@@ -286,11 +289,16 @@ private:
             }
             if (res.empty()) continue;
             long long chunk = cfg_.max_chunk_steps;
-            for (const Resident &r : res) chunk = std::min(chunk, r.remaining);
-            if (ms_per_step > 0.0)
-                chunk = std::max(1LL, std::min(chunk, (long long)(cfg_.chunk_ms / ms_per_step)));
+            double cells = 0.0;
+            for (const Resident &r : res) {
+                chunk = std::min(chunk, r.remaining);
+                cells += (double)r.q.req.desc.nx * r.q.req.desc.ny * r.q.req.desc.nz;
+            }
+            if (ms_per_cell_step > 0.0)
+                chunk = std::max(1LL, std::min(chunk, (long long)(cfg_.chunk_ms /
+                                                                  (ms_per_cell_step * cells))));
             else
-                chunk = 1;  // measure the new composition first
+                chunk = 1;  // nothing measured yet
             const double t_a = now();
             int rc = eng->step((int)chunk);
             if (!rc) {
@@ -308,7 +316,7 @@ private:
                 res.clear();
                 used = 0;
             } else {
-                ms_per_step = 1e3 * dt_chunk / (double)chunk;
+                ms_per_cell_step = 1e3 * dt_chunk / ((double)chunk * cells);
                 std::vector<Resident> keep;
                 for (Resident &r : res) {
                     r.remaining -= chunk;
@@ -320,7 +328,6 @@ private:
                     post(r, rrc, rrc ? nuc3d_last_error() : nullptr, eng);
                     eng->remove_box(r.box);
                     used -= r.q.bytes;
-                    ms_per_step = 0.0;
                 }
                 res.swap(keep);
             }
@@ -332,6 +339,7 @@ private:
                 info_.resident = (int)res.size();
                 info_.resident_bytes = used;
                 info_.launches = eng->launches;
+                info_.graph_captures = eng->graph_captures;
             }
         }
         // shutting down: cancel what is resident and queued

@@ -103,7 +103,7 @@ class _ServeStats(C.Structure):
                 ("peak_resident_bytes", C.c_longlong), ("budget_bytes", C.c_longlong),
                 ("batch_steps", C.c_longlong), ("chunks", C.c_longlong),
                 ("cell_updates", C.c_longlong), ("launches", C.c_longlong),
-                ("busy_s", C.c_double), ("now_s", C.c_double)]
+                ("graph_captures", C.c_longlong), ("busy_s", C.c_double), ("now_s", C.c_double)]
 
 
 _lib = None

@@ -11,6 +11,9 @@ tests/test_oracle.py pins bitwise to the reference's own translation units).
 * Decaying isotropic turbulence, 256^3, WENO5-Z: the seeded HIT field the
   benchmark advances (seed 0, k_peak 4, turbulent Mach 0.3, Re_lambda 100,
   M 1), one RHS evaluation and one TVD-RK3 step.
+* The forced shocklet configuration (turbulent Mach 0.6, band forcing, CFL
+  0.4) at 64^3 with the compact schemes in mixed precision: stays finite and
+  close to FP64.
 
 Tolerance: per-field relative L2 of 1e-12, as for the small boxes of
 tests/test_gpu_step.py.  The oracle runs its lines on all host cores
@@ -82,3 +85,41 @@ def test_hit_256_rhs_and_one_step_match_oracle(torch):
     assert err < TOL_FP64, f"256^3 HIT after one step: rel L2 {err:.3e}"
     np.testing.assert_allclose(dt, dt_ref, rtol=1e-13)
     np.testing.assert_allclose(res, res_ref, rtol=1e-9)
+
+
+@pytest.mark.parametrize("scheme,tol", [("crweno5", 1e-6), ("hccs", 1e-3)],
+                         ids=["crweno5", "hccs"])
+def test_forced_mach06_mixed_compact_schemes_stay_finite(torch, scheme, tol):
+    """The forced shocklet configuration at 64^3: seeded HIT at turbulent
+    Mach 0.6, band forcing on 0 < |k| <= 2 at the initial dissipation rate,
+    CFL 0.4, with CRWENO5 and with hccs (CRWENO5 with the hybrid linear /
+    weighted switch) in mixed precision (FP32 line solves).  The mixed run
+    stays finite for 500 steps, and after 100 steps it is within `tol`
+    (per-field relative L2) of the FP64 run and its kinetic energy within
+    1e-4.  hccs's switch is discontinuous: a row that FP32 rounding moves
+    across it changes that face by the local flux jump, hence its wider
+    bar."""
+    import nuc3d_b200 as nb
+    sch = nb.CRWENO5 if scheme == "crweno5" else nb.HCCS
+    init = {"kind": "hit", "seed": 0, "k_peak": 4.0, "mach_t": 0.6, "re_lambda": 100.0}
+    with nb.Solver(nb.BoxDesc(64, 64, 64, mach=1.0)) as s:
+        s.init_state(init)
+        rate = s.stats()["dissipation"]
+    finals, ke = {}, {}
+    for prec in (nb.FP64, nb.MIXED):
+        d = nb.BoxDesc(64, 64, 64, mach=1.0, scheme=(sch,) * 3, precision=prec,
+                       forcing=nb.FORCING_BAND, forcing_amp=rate, forcing_k=2.0)
+        with nb.Solver(d) as s:
+            s.init_state(init)
+            s.step(100, 0.4, stats=False)
+            finals[prec] = s.get_state()
+            ke[prec] = s.stats()["kinetic"]
+            if prec == nb.MIXED:
+                for _ in range(4):
+                    s.step(100, 0.4, stats=False)
+                    s.sync()  # raises on a non-finite state
+                q = s.get_state()
+                assert all(np.isfinite(a).all() for a in q)
+                assert 0.0 < s.stats()["kinetic"] < 1.0
+    assert max_rel_l2(finals[nb.MIXED], finals[nb.FP64]) < tol
+    assert abs(ke[nb.MIXED] - ke[nb.FP64]) <= 1e-4 * ke[nb.FP64]
