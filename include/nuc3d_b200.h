@@ -231,6 +231,18 @@ NUC3D_API int nuc3d_probe_peak(int precision, double *tflops);
 #define NUC3D_TUNING_SLOTS 12
 NUC3D_API int nuc3d_tuning(const nuc3d_ctx *ctx, int *run_len, double *ms);
 NUC3D_API int nuc3d_batch_tuning(const nuc3d_batch *b, int *run_len, double *ms);
+/* The other autotuned shape: the pencil depth of the 2.5-D stencil kernels
+ * (viscous flux, update), i.e. how many z-planes one 32 x 8 column tile
+ * marches (each tile re-reads a 6-plane halo, so deeper pencils read less but
+ * make fewer, longer blocks).  The first step, and every step after the
+ * batch's active cells have grown or shrunk past a factor 2 of those it was
+ * tuned at, times one viscous-flux + update pass at each of
+ * NUC3D_PENCIL_DEPTHS depths on the live boxes and keeps the fastest.
+ * *depth receives the chosen depth (0 = not tuned), ms (3 doubles, may be
+ * NULL) the measured milliseconds per pass for depths {32, 16, 64}. */
+#define NUC3D_PENCIL_DEPTHS 3
+NUC3D_API int nuc3d_tuning_pencil(const nuc3d_ctx *ctx, int *depth, double *ms);
+NUC3D_API int nuc3d_batch_tuning_pencil(const nuc3d_batch *b, int *depth, double *ms);
 
 /* ---- initial states generated on the device ------------------------------
  * NUC3D_INIT_TGV: block::initial_taylorgreen (block.cpp:359-395) on the cell

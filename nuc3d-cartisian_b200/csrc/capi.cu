@@ -92,9 +92,26 @@ int read_tuning(const Engine *eng, int *run_len, double *ms) {
     return NUC3D_OK;
 }
 
+int read_pencil(const Engine *eng, int *depth, double *ms) {
+    static_assert(NUC3D_PENCIL_DEPTHS == 3, "pencil tuning layout");
+    if (depth) *depth = eng->pencil_variant < 0 ? 0 : kPencilDepths[eng->pencil_variant];
+    for (int v = 0; v < 3; ++v)
+        if (ms) ms[v] = eng->pencil_tune_ms[v];
+    return NUC3D_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int nuc3d_tuning_pencil(const nuc3d_ctx *c, int *depth, double *ms) {
+    if (!c) return fail(NUC3D_ERR_INVALID, "null context");
+    return read_pencil(c->eng, depth, ms);
+}
+int nuc3d_batch_tuning_pencil(const nuc3d_batch *b, int *depth, double *ms) {
+    if (!b) return fail(NUC3D_ERR_INVALID, "null batch");
+    return read_pencil(b->eng, depth, ms);
+}
 
 int nuc3d_tuning(const nuc3d_ctx *c, int *run_len, double *ms) {
     if (!c) return fail(NUC3D_ERR_INVALID, "null context");

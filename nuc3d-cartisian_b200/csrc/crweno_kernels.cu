@@ -368,56 +368,38 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                 segment(std::integral_constant<int, 0>{});
             else
                 segment(std::integral_constant<int, 1>{});
-            // parallel cyclic reduction of the 2P segment-end unknowns
-            // (reduced row 2l: x_first of lane l, 2l+1: x_last) within the warp
-            const int base = 0;
-            for (int s = 1; s < 2 * P; s <<= 1) {
-                B fma_a, fma_c, fma_d, fpa, fpc, fpd;  // first's neighbours
-                B lma, lmc, lmd, lpa, lpc, lpd;        // last's neighbours
-                bool fm_ok, fp_ok, lm_ok, lp_ok;
-                if (s == 1) {
-                    const int sm = base + (hl - 1 + P) % P, sp = base + (hl + 1) % P;
-                    fma_a = shfl(la, sm);
-                    fma_c = shfl(lc, sm);
-                    fma_d = shfl(ld, sm);
-                    lpa = shfl(fa, sp);
-                    lpc = shfl(fc, sp);
-                    lpd = shfl(fd, sp);
-                    fpa = la;
-                    fpc = lc;
-                    fpd = ld;
-                    lma = fa;
-                    lmc = fc;
-                    lmd = fd;
-                    fm_ok = !bounded || hl >= 1;
-                    lp_ok = !bounded || hl + 1 < P;
-                    fp_ok = lm_ok = true;
-                } else {
-                    const int h = s >> 1;
-                    const int sm = base + (hl - h + P) % P, sp = base + (hl + h) % P;
-                    fma_a = shfl(fa, sm);
-                    fma_c = shfl(fc, sm);
-                    fma_d = shfl(fd, sm);
-                    fpa = shfl(fa, sp);
-                    fpc = shfl(fc, sp);
-                    fpd = shfl(fd, sp);
-                    lma = shfl(la, sm);
-                    lmc = shfl(lc, sm);
-                    lmd = shfl(ld, sm);
-                    lpa = shfl(la, sp);
-                    lpc = shfl(lc, sp);
-                    lpd = shfl(ld, sp);
-                    fm_ok = lm_ok = !bounded || hl >= h;
-                    fp_ok = lp_ok = !bounded || hl + h < P;
+            // The 2P segment-end unknowns couple as
+            //   fa x_last(l-1) + x_first(l) + fc x_last(l)  = fd   (lane l's first)
+            //   la x_first(l)  + x_last(l)  + lc x_first(l+1) = ld (lane l's last)
+            // (neighbour lanes wrap for periodic lines; for bounded lines lane
+            // 0's fa and lane P-1's lc are 0: identity end rows).  Substituting
+            // the first rows into the last rows leaves a tridiagonal system in
+            // the P unknowns x_last alone,
+            //   -la fa x_last(l-1) + (1 - la fc - lc fa') x_last(l) - lc fc' x_last(l+1)
+            //     = ld - la fd - lc fd'          (' : lane l+1),
+            // solved by parallel cyclic reduction with shuffles (log2 P levels
+            // of one row each, instead of log2 2P levels of two rows); then
+            // x_first(l) = fd - fa x_last(l-1) - fc x_last(l).
+            B xf, xl;
+            {
+                const int lp1 = (hl + 1) % P, lm1 = (hl - 1 + P) % P;
+                const B nfa = shfl(fa, lp1), nfc = shfl(fc, lp1), nfd = shfl(fd, lp1);
+                const B r = rcp_(B(1) - la * fc - lc * nfa);
+                B ra = -la * fa * r, rc = -lc * nfc * r, rd = (ld - la * fd - lc * nfd) * r;
+                for (int s = 1; s < P; s <<= 1) {
+                    const int sm = (hl - s + P) % P, sp = (hl + s) % P;
+                    B ma = shfl(ra, sm), mc = shfl(rc, sm), md = shfl(rd, sm);
+                    B pa = shfl(ra, sp), pc = shfl(rc, sp), pd = shfl(rd, sp);
+                    if (bounded && hl < s) ma = mc = md = B(0);
+                    if (bounded && hl + s >= P) pa = pc = pd = B(0);
+                    pcr_update(ra, rc, rd, ma, mc, md, pa, pc, pd);
                 }
-                if (!fm_ok) fma_a = fma_c = fma_d = B(0);
-                if (!fp_ok) fpa = fpc = fpd = B(0);
-                if (!lm_ok) lma = lmc = lmd = B(0);
-                if (!lp_ok) lpa = lpc = lpd = B(0);
-                pcr_update(fa, fc, fd, fma_a, fma_c, fma_d, fpa, fpc, fpd);
-                pcr_update(la, lc, ld, lma, lmc, lmd, lpa, lpc, lpd);
+                // after the last level each row couples only to itself
+                // (periodic) or to nothing (bounded)
+                xl = rd * rcp_(B(1) + ra + rc);
+                const B xlm = shfl(xl, lm1);
+                xf = fd - fa * xlm - fc * xl;
             }
-            const B xf = fd * rcp_(B(1) + fa + fc), xl = ld * rcp_(B(1) + la + lc);
             __syncwarp();  // every lane has read its staged fluxes
             if (act) {
                 const int off = bounded ? H : 0;

@@ -328,12 +328,13 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));
     const bool mixed = precision_ == NUC3D_MIXED;
     std::vector<BoxDev> table(boxes_.size());
-    std::vector<WorkItem> prim, prim_step, st25, inv[kSchemes][3], cr[2][3];
+    std::vector<WorkItem> prim, prim_step, st25[3], inv[kSchemes][3], cr[2][3];
     const int crtl = crweno_tile_lines();
     for (int c = 0; c < 2; ++c)
         for (int d = 0; d < 3; ++d) cr_nmax_[c][d] = cr_ms_[c][d] = 0;
     any_visc_ = false;
     nactive_ = 0;
+    active_cells_ = 0;
     for (size_t i = 0; i < boxes_.size(); ++i) {
         EngineBox &b = boxes_[i];
         table[i] = b.dev;
@@ -341,6 +342,7 @@ int Engine::rebuild() {
         if (!b.live || !b.dev.active) continue;
         ++nactive_;
         const BoxParams &p = b.dev.p;
+        active_cells_ += p.N;
         const int id = (int)i;
         any_visc_ = any_visc_ || p.navier_stokes;
         boxes_[i].prim_off = (int)prim.size();
@@ -349,9 +351,10 @@ int Engine::rebuild() {
         boxes_[i].prim_n = (int)prim.size() - boxes_[i].prim_off;
         if (p.scheme[0] == SCHEME_CR || p.scheme[0] == SCHEME_HC)
             prim_step.insert(prim_step.end(), prim.end() - boxes_[i].prim_n, prim.end());
-        for (int z = 0; z < ceil_div(p.n[2], kT25Z); ++z)
-            for (int y = 0; y < ceil_div(p.n[1], kT25Y); ++y)
-                for (int x = 0; x < ceil_div(p.n[0], kT25X); ++x) st25.push_back({id, x, y, z});
+        for (int v = 0; v < 3; ++v)
+            for (int z = 0; z < ceil_div(p.n[2], kPencilDepths[v]); ++z)
+                for (int y = 0; y < ceil_div(p.n[1], kT25Y); ++y)
+                    for (int x = 0; x < ceil_div(p.n[0], kT25X); ++x) st25[v].push_back({id, x, y, z});
         for (int d = 0; d < 3; ++d) {
             int s = p.scheme[d];
             if (s == SCHEME_CR || s == SCHEME_HC) {
@@ -397,7 +400,7 @@ int Engine::rebuild() {
     };
     append(prim, r_prim_);
     append(prim_step, r_prim_step_);
-    append(st25, r_25d_);
+    for (int v = 0; v < 3; ++v) append(st25[v], r_25d_[v]);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) append(inv[s][d], r_inv_[s][d]);
     for (int c = 0; c < 2; ++c)
@@ -424,7 +427,7 @@ int Engine::rebuild() {
     ECK(prepare_inviscid_kernels(mixed));
     ECK(prepare_crweno_kernels(mixed));
     ECK(prepare_stencil_kernels(mixed));
-    int per_stage = (r_prim_step_.n > 0) + (any_visc_ && r_25d_.n > 0) + (r_25d_.n > 0);
+    int per_stage = (r_prim_step_.n > 0) + (any_visc_ && r_25d_[0].n > 0) + (r_25d_[0].n > 0);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d].n > 0;
     for (int c = 0; c < 2; ++c)
@@ -511,7 +514,8 @@ int Engine::enqueue_step_t(cudaStream_t st) {
         }
         if (any_visc_) {
             ProfScope ps(this, NUC3D_PROF_VISC);
-            ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_.off, r_25d_.n, st)));
+            ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_[pv()].off, r_25d_[pv()].n,
+                                     kPencilDepths[pv()], st)));
         }
         for (int d = 1; d < 3; ++d)
             if (int rc = sweeps(d)) return rc;
@@ -519,7 +523,8 @@ int Engine::enqueue_step_t(cudaStream_t st) {
         {
             ProfScope ps(this, NUC3D_PROF_UPDATE);
             StageArgs sa{stage, in, out, nullptr};
-            ECK((launch_update<B>(d_boxes_, it + r_25d_.off, r_25d_.n, sa, any_visc_, st)));
+            ECK((launch_update<B>(d_boxes_, it + r_25d_[pv()].off, r_25d_[pv()].n,
+                                  kPencilDepths[pv()], sa, any_visc_, st)));
         }
     }
     {
@@ -549,60 +554,113 @@ int Engine::enqueue_step(cudaStream_t s) {
     return precision_ == NUC3D_MIXED ? enqueue_step_t<float>(s) : enqueue_step_t<double>(s);
 }
 
-// Picks the run length of the directional sweep per scheme and direction by
-// timing every variant on this batch's own work lists (the first step after a
-// rebuild that brings a new (scheme, direction) pair).  The sweeps only write
-// the RHS accumulator, which every stage recomputes, so timing them on the
+// Picks the run length of the directional sweep per scheme and direction,
+// and the pencil depth of the 2.5-D stencil kernels, by timing every variant
+// on this batch's own work lists: the sweeps on the first step after a
+// rebuild that brings a new (scheme, direction) pair, the depth on the first
+// step and whenever the active cells have moved past 2x (or 1/2x) of those
+// it was tuned at.  The sweeps only write the RHS accumulator and the
+// viscous-flux kernel the viscous fluxes, which every stage recomputes; the
+// update is timed as a first stage, which writes only the u1 slot that the
+// next step's first stage overwrites (and no residual), so timing on the
 // live state changes nothing.
 int Engine::autotune() {
-    bool need = false;
+    bool need_sweep = false;
     for (int s = 0; s < kSchemes; ++s)
-        for (int d = 0; d < 3; ++d) need = need || (r_inv_[s][d].n > 0 && inv_variant[s][d] < 0);
-    if (!need) return NUC3D_OK;
-    // NUC3D_SWEEP_RUN=1|2|4 pins the run length (reproducibility studies)
-    if (const char *pin = std::getenv("NUC3D_SWEEP_RUN")) {
-        int v = std::atoi(pin) == 1 ? 0 : (std::atoi(pin) == 2 ? 1 : 2);
-        for (int s = 0; s < kSchemes; ++s)
-            for (int d = 0; d < 3; ++d)
-                if (r_inv_[s][d].n > 0 && inv_variant[s][d] < 0) inv_variant[s][d] = v;
-        invalidate_graph();
-        return NUC3D_OK;
+        for (int d = 0; d < 3; ++d)
+            need_sweep = need_sweep || (r_inv_[s][d].n > 0 && inv_variant[s][d] < 0);
+    const bool need_pencil =
+        r_25d_[0].n > 0 && (pencil_variant < 0 || 2 * active_cells_ < pencil_tuned_cells ||
+                            active_cells_ > 2 * pencil_tuned_cells);
+    if (!need_sweep && !need_pencil) return NUC3D_OK;
+    // NUC3D_SWEEP_RUN=1|2|4 pins the run length and NUC3D_PENCIL_DEPTH=16|32|64
+    // the pencil depth (reproducibility studies)
+    if (need_sweep) {
+        if (const char *pin = std::getenv("NUC3D_SWEEP_RUN")) {
+            int v = std::atoi(pin) == 1 ? 0 : (std::atoi(pin) == 2 ? 1 : 2);
+            for (int s = 0; s < kSchemes; ++s)
+                for (int d = 0; d < 3; ++d)
+                    if (r_inv_[s][d].n > 0 && inv_variant[s][d] < 0) inv_variant[s][d] = v;
+            need_sweep = false;
+        }
     }
+    bool tune_pencil = need_pencil;
+    if (need_pencil) {
+        if (const char *pin = std::getenv("NUC3D_PENCIL_DEPTH")) {
+            const int want = std::atoi(pin);
+            pencil_variant = 0;
+            for (int v = 0; v < 3; ++v)
+                if (kPencilDepths[v] == want) pencil_variant = v;
+            pencil_tuned_cells = active_cells_;
+            tune_pencil = false;
+        }
+    }
+    invalidate_graph();
+    if (!need_sweep && !tune_pencil) return NUC3D_OK;
     ECK(launch_prim(d_boxes_, d_items_ + r_prim_.off, r_prim_.n, 0, 0, stream_));
     cudaEvent_t e0, e1;
     ECK(cudaEventCreate(&e0));
     ECK(cudaEventCreate(&e1));
     const bool mixed = precision_ == NUC3D_MIXED;
     int rc = NUC3D_OK;
-    for (int s = 0; s < kSchemes && rc == NUC3D_OK; ++s)
+    // ms of one warm-up-then-3-repeats timing of go(), or a negative value
+    // (with the error recorded) when a launch fails
+    auto time3 = [&](auto &&go) -> double {
+        cudaError_t err = go();  // warm-up
+        err = err == cudaSuccess ? cudaEventRecord(e0, stream_) : err;
+        for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) err = go();
+        err = err == cudaSuccess ? cudaEventRecord(e1, stream_) : err;
+        err = err == cudaSuccess ? cudaEventSynchronize(e1) : err;
+        float ms = 0.f;
+        err = err == cudaSuccess ? cudaEventElapsedTime(&ms, e0, e1) : err;
+        if (err != cudaSuccess) {
+            set_last_error(NUC3D_ERR_CUDA, cudaGetErrorString(err));
+            rc = NUC3D_ERR_CUDA;
+            return -1.0;
+        }
+        return ms / 3.0;
+    };
+    for (int s = 0; s < kSchemes && rc == NUC3D_OK && need_sweep; ++s)
         for (int d = 0; d < 3 && rc == NUC3D_OK; ++d) {
             const Range &rg = r_inv_[s][d];
             if (rg.n <= 0 || inv_variant[s][d] >= 0) continue;
             int best = 0;
-            for (int v = 0; v < kInvVariants; ++v) {
-                auto go = [&]() {
+            for (int v = 0; v < kInvVariants && rc == NUC3D_OK; ++v) {
+                const double ms = time3([&]() {
                     return mixed ? launch_inviscid<float>(s, d, v, d_boxes_, d_items_ + rg.off, rg.n,
                                                           0, d > 0, 0, stream_)
                                  : launch_inviscid<double>(s, d, v, d_boxes_, d_items_ + rg.off,
                                                            rg.n, 0, d > 0, 0, stream_);
-                };
-                cudaError_t err = go();  // warm-up
-                err = err == cudaSuccess ? cudaEventRecord(e0, stream_) : err;
-                for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) err = go();
-                err = err == cudaSuccess ? cudaEventRecord(e1, stream_) : err;
-                err = err == cudaSuccess ? cudaEventSynchronize(e1) : err;
-                float ms = 0.f;
-                err = err == cudaSuccess ? cudaEventElapsedTime(&ms, e0, e1) : err;
-                if (err != cudaSuccess) {
-                    set_last_error(NUC3D_ERR_CUDA, cudaGetErrorString(err));
-                    rc = NUC3D_ERR_CUDA;
-                    break;
-                }
-                inv_tune_ms[s][d][v] = ms / 3.0;
-                if (inv_tune_ms[s][d][v] < inv_tune_ms[s][d][best]) best = v;
+                });
+                inv_tune_ms[s][d][v] = ms;
+                if (ms < inv_tune_ms[s][d][best]) best = v;
             }
             inv_variant[s][d] = best;
         }
+    if (tune_pencil && rc == NUC3D_OK) {
+        int best = 0;
+        for (int v = 0; v < 3 && rc == NUC3D_OK; ++v) {
+            const Range &rg = r_25d_[v];
+            const StageArgs sa{0, 0, 1, nullptr};
+            const double ms = time3([&]() {
+                cudaError_t err = cudaSuccess;
+                if (any_visc_)
+                    err = mixed ? launch_visc_flux<float>(d_boxes_, d_items_ + rg.off, rg.n,
+                                                          kPencilDepths[v], stream_)
+                                : launch_visc_flux<double>(d_boxes_, d_items_ + rg.off, rg.n,
+                                                           kPencilDepths[v], stream_);
+                if (err != cudaSuccess) return err;
+                return mixed ? launch_update<float>(d_boxes_, d_items_ + rg.off, rg.n,
+                                                    kPencilDepths[v], sa, any_visc_, stream_)
+                             : launch_update<double>(d_boxes_, d_items_ + rg.off, rg.n,
+                                                     kPencilDepths[v], sa, any_visc_, stream_);
+            });
+            pencil_tune_ms[v] = ms;
+            if (ms < pencil_tune_ms[best]) best = v;
+        }
+        pencil_variant = best;
+        pencil_tuned_cells = active_cells_;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     invalidate_graph();
@@ -687,7 +745,9 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
     ECK(launch_clear_eig(d_boxes_, nb, stream_));
     ECK(launch_prim(d_boxes_, it + r_prim_.off, r_prim_.n, 0, 1, stream_));
     ECK(launch_dt(d_boxes_, nb, stream_));
-    if (any_visc_) ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_.off, r_25d_.n, stream_)));
+    if (any_visc_)
+        ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_[pv()].off, r_25d_[pv()].n,
+                                 kPencilDepths[pv()], stream_)));
     for (int d = 0; d < 3; ++d) {
         for (int s = 0; s < kSchemes; ++s)
             ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
@@ -699,7 +759,8 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
     }
     ECK(enqueue_forcing<B>(stream_));
     StageArgs sa{-1, 0, 0, d_rhs_ptrs_};
-    ECK((launch_update<B>(d_boxes_, it + r_25d_.off, r_25d_.n, sa, any_visc_, stream_)));
+    ECK((launch_update<B>(d_boxes_, it + r_25d_[pv()].off, r_25d_[pv()].n, kPencilDepths[pv()],
+                          sa, any_visc_, stream_)));
     ECK(cudaStreamSynchronize(stream_));  // ptrs is a host stack array
     return NUC3D_OK;
 }

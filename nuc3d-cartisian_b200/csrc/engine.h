@@ -72,6 +72,13 @@ public:
     // measured milliseconds per launch of each variant
     int inv_variant[kSchemes][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
     double inv_tune_ms[kSchemes][3][kInvVariants] = {};
+    // autotuned pencil depth of the 2.5-D stencil kernels: index into
+    // kPencilDepths (-1: not tuned yet), the measured milliseconds of one
+    // viscous-flux + update pass per depth, and the active cells it was tuned
+    // at (a batch that grows or shrinks past 2x is tuned again)
+    int pencil_variant = -1;
+    double pencil_tune_ms[3] = {};
+    long long pencil_tuned_cells = 0;
 
     static long long box_bytes(const nuc3d_box_desc &d);
     static int validate(const nuc3d_box_desc &d, std::string *why);
@@ -105,7 +112,11 @@ private:
         size_t off = 0;
         int n = 0;
     };
-    Range r_prim_, r_25d_, r_inv_[kSchemes][3];  // [scheme JS/Z/-/W7][dir]
+    Range r_prim_, r_inv_[kSchemes][3];  // [scheme JS/Z/-/W7][dir]
+    // 2.5-D stencil tiles for each pencil depth of kPencilDepths
+    Range r_25d_[3];
+    long long active_cells_ = 0;
+    int pv() const { return pencil_variant < 0 ? 0 : pencil_variant; }
     // k_prim items of the boxes whose x direction runs the line kernel; the
     // x sweep (k_inviscid) recovers the primitives of the other boxes itself
     Range r_prim_step_;

@@ -97,7 +97,10 @@ struct InvTileDims {
     int TL, TC;  // lines per tile, cells per tile along the sweep
 };
 InvTileDims inviscid_tile(int dir, bool mixed);
-constexpr int kT25X = 32, kT25Y = 8, kT25Z = 32;  // 2.5-D tile of the stencil kernels
+constexpr int kT25X = 32, kT25Y = 8;  // 2.5-D tile of the stencil kernels (x, y)
+// pencil depths (planes per work item) the autotuner chooses from; the first
+// is the default
+constexpr int kPencilDepths[3] = {32, 16, 64};
 constexpr int kPrimChunk = 4096;                  // cells per k_prim work item
 
 // Opt the inviscid kernels of one precision into their dynamic shared
@@ -124,12 +127,13 @@ cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxe
                             int prim_mode, cudaStream_t st);
 // raises the dynamic shared-memory limit of the viscous-flux kernel
 cudaError_t prepare_stencil_kernels(bool mixed);
+// depth: planes per work item along z (the items' z chunks are of that size)
 template <typename B>
-cudaError_t launch_visc_flux(const BoxDev *boxes, const WorkItem *items, int nitems,
+cudaError_t launch_visc_flux(const BoxDev *boxes, const WorkItem *items, int nitems, int depth,
                              cudaStream_t st);
 template <typename B>
-cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems, StageArgs sa,
-                          bool any_viscous, cudaStream_t st);
+cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems, int depth,
+                          StageArgs sa, bool any_viscous, cudaStream_t st);
 
 // CRWENO5 / hccs sweeps (crweno_kernels.cu), batched: one work item per tile of
 // crweno_tile_lines() lines of one box.  nmax is the longest line among the

@@ -1,7 +1,8 @@
 // 2.5-D blocked stencil kernels of the viscous part and the RK update.
 //
-// A block owns a 32 x 8 column tile of the box and marches a chunk of KZ
-// planes along z.  For each plane it stages the tile plus the x/y halo in
+// A block owns a 32 x 8 column tile of the box and marches a chunk of
+// `depth` planes along z (the pencil depth, a launch argument the engine's
+// autotuner picks).  For each plane it stages the tile plus the x/y halo in
 // shared memory (the x- and y-direction CD6 stencils read it there) while
 // every thread keeps a 7-deep register queue of its own column for the
 // z-direction stencil, so each value is fetched from L2/HBM about once per
@@ -13,7 +14,7 @@ namespace nuc3d {
 
 namespace {
 
-constexpr int TX = kT25X, TY = kT25Y, KZ = kT25Z;
+constexpr int TX = kT25X, TY = kT25Y;
 
 // a TMA tensor map as the kernels see it: 128 opaque, 64-byte aligned bytes
 // (the host encodes CUtensorMap values into the box's allocation)
@@ -86,9 +87,9 @@ __device__ __forceinline__ double cd6d(double m3, double m2, double m1, double p
 // solveGrads + solveViscousFlux (NaiverStokes3d.cpp:87-303): CD6 gradients
 // of u, v, w, T (FP64 differences), stresses and heat flux in the bulk type,
 // written as tau_xx, tau_xy, tau_xz, tau_yy, tau_yz, tau_zz, E_x, E_y, E_z.
-// Work item: (box, x tile, y tile, z chunk).
+// Work item: (box, x tile, y tile, z chunk of `depth` planes).
 template <typename B>
-__global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items) {
+__global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, int depth) {
     // dynamic shared memory (visc_smem_bytes): the two plane tiles with their
     // x/y halo (row pitch TX + 8: column 0 is cell i0 - 4, so that a TMA box
     // starts on a 32-byte boundary), each column's plane k+3 (z-queue
@@ -114,7 +115,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
     B *const vbase = fieldV<B>(bd, 0);
     const int nx = bp.n[0], ny = bp.n[1], nz = bp.n[2];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int i0 = it.a * TX, j0 = it.b * TY, k0 = it.c * KZ;
+    const int i0 = it.a * TX, j0 = it.b * TY, k0 = it.c * depth;
     const int i = i0 + tx, j = j0 + ty;
     const bool active = i < nx && j < ny;
     const long long sz = bp.stride[2];
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
         __syncthreads();
         return true;
     };
-    const int kend = min(k0 + KZ, nz);
+    const int kend = min(k0 + depth, nz);
     issue(k0, 0);
     cp_async_commit();
     double qz[4][7];
@@ -276,12 +277,13 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
 // TVD-RK3 stage (TVD-RK3.cpp:76-196, dQ/dt = -RHS) in FP64; on the last stage
 // also the residual sum of PDEData3d::setRES (PDEData3d.cpp:178-213).  Every
 // new state value passes a finite check.  stage = -1 writes the total RHS.
-// Work item: (box, x tile, y tile, z chunk).  ANYVIS: some box of the batch
+// Work item: (box, x tile, y tile, z chunk of `depth` planes).  ANYVIS: some box of the batch
 // is viscous (sizes the shared tiles); per box the viscous part runs only for
 // Navier-Stokes boxes.
 template <typename B, bool ANYVIS>
 __global__ void __launch_bounds__(TX *TY, 2)
-    k_update25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, StageArgs sa) {
+    k_update25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, int depth,
+               StageArgs sa) {
     // x stencils: tau_xx, tau_xy, tau_xz, E_x; y: tau_xy, tau_yy, tau_yz, E_y;
     // z: tau_xz, tau_yz, tau_zz, E_z
     // x and y halo tiles of the fluxes each stencil direction needs.  (The
@@ -312,14 +314,14 @@ __global__ void __launch_bounds__(TX *TY, 2)
     const StepScalars *sc = bd.sc;
     const int nx = bp.n[0], ny = bp.n[1], nz = bp.n[2];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int i0 = it.a * TX, j0 = it.b * TY, k0 = it.c * KZ;
+    const int i0 = it.a * TX, j0 = it.b * TY, k0 = it.c * depth;
     const int i = i0 + tx, j = j0 + ty;
     const bool active = i < nx && j < ny;
     const long long sz = bp.stride[2];
     const long long col = active ? (long long)i + (long long)nx * j : 0;
     const double dt = sc->dt;
     const B ixb = B(bp.inv_d[0]), iyb = B(bp.inv_d[1]), izb = B(bp.inv_d[2]);
-    const int kend = min(k0 + KZ, nz);
+    const int kend = min(k0 + depth, nz);
     if constexpr (wrap_table) {
         if (tid < TX + 6) sWx[tid] = pmod(i0 - 3 + tid, nx);
         if (tid < TY + 6) sWy[tid] = nx * pmod(j0 - 3 + tid, ny);
@@ -463,29 +465,31 @@ cudaError_t prepare_stencil_kernels(bool mixed) {
 }
 
 template <typename B>
-cudaError_t launch_visc_flux(const BoxDev *boxes, const WorkItem *items, int nitems,
+cudaError_t launch_visc_flux(const BoxDev *boxes, const WorkItem *items, int nitems, int kz,
                              cudaStream_t st) {
     if (nitems <= 0) return cudaSuccess;
-    k_visc_flux25<B><<<nitems, dim3(TX, TY), visc_smem_bytes(), st>>>(boxes, items);
+    k_visc_flux25<B><<<nitems, dim3(TX, TY), visc_smem_bytes(), st>>>(boxes, items, kz);
     return cudaGetLastError();
 }
 
 template <typename B>
-cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems, StageArgs sa,
-                          bool any_viscous, cudaStream_t st) {
+cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems, int kz,
+                          StageArgs sa, bool any_viscous, cudaStream_t st) {
     if (nitems <= 0) return cudaSuccess;
     if (any_viscous)
-        k_update25<B, true><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items, sa);
+        k_update25<B, true><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items, kz, sa);
     else
-        k_update25<B, false><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items, sa);
+        k_update25<B, false><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items, kz, sa);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_visc_flux<double>(const BoxDev *, const WorkItem *, int, cudaStream_t);
-template cudaError_t launch_visc_flux<float>(const BoxDev *, const WorkItem *, int, cudaStream_t);
-template cudaError_t launch_update<double>(const BoxDev *, const WorkItem *, int, StageArgs, bool,
-                                           cudaStream_t);
-template cudaError_t launch_update<float>(const BoxDev *, const WorkItem *, int, StageArgs, bool,
-                                          cudaStream_t);
+template cudaError_t launch_visc_flux<double>(const BoxDev *, const WorkItem *, int, int,
+                                              cudaStream_t);
+template cudaError_t launch_visc_flux<float>(const BoxDev *, const WorkItem *, int, int,
+                                             cudaStream_t);
+template cudaError_t launch_update<double>(const BoxDev *, const WorkItem *, int, int, StageArgs,
+                                           bool, cudaStream_t);
+template cudaError_t launch_update<float>(const BoxDev *, const WorkItem *, int, int, StageArgs,
+                                          bool, cudaStream_t);
 
 }  // namespace nuc3d

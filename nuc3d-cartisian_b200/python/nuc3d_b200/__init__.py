@@ -25,6 +25,7 @@ WENO5JS, WENO5Z, CRWENO5, WENO7JS, HCCS = 0, 1, 2, 3, 4
 SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5, "weno7js": WENO7JS,
            "hccs": HCCS}
 TUNING_SLOTS = 12  # NUC3D_TUNING_SLOTS: (scheme id, direction) pairs
+PENCIL_DEPTHS = (32, 16, 64)  # the 2.5-D kernels' pencil depths, in tuning order
 RIEMANN_LF, RIEMANN_AUSM, RIEMANN_AUSMP = 0, 1, 2
 RIEMANNS = {"LF": RIEMANN_LF, "AUSM": RIEMANN_AUSM, "AUSMp": RIEMANN_AUSMP}
 EULER3D, NAVIERSTOKES3D = 0, 1
@@ -159,6 +160,8 @@ def lib() -> C.CDLL:
         L.nuc3d_batch_launch_count.argtypes = [C.c_void_p]
         L.nuc3d_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.nuc3d_batch_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nuc3d_tuning_pencil.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nuc3d_batch_tuning_pencil.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.nuc3d_stats.argtypes = [C.c_void_p, C.c_void_p]
         L.nuc3d_batch_stats.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.nuc3d_spectra.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
@@ -402,7 +405,7 @@ class Solver:
         return int(lib().nuc3d_launch_count(self._h))
 
     def tuning(self):
-        return _tuning(lib().nuc3d_tuning, self._h)
+        return _tuning(lib().nuc3d_tuning, self._h, lib().nuc3d_tuning_pencil)
 
 
 class Batch:
@@ -514,7 +517,7 @@ class Batch:
         return int(lib().nuc3d_batch_launch_count(self._h))
 
     def tuning(self):
-        return _tuning(lib().nuc3d_batch_tuning, self._h)
+        return _tuning(lib().nuc3d_batch_tuning, self._h, lib().nuc3d_batch_tuning_pencil)
 
 
 class Server:
@@ -612,8 +615,9 @@ def _spectra(fn, *args):
     return out
 
 
-def _tuning(fn, h):
-    """{(scheme, dir): (chosen run length, {run length: ms per launch})}"""
+def _tuning(fn, h, fn_pencil=None):
+    """{"<scheme>_<dir>": (chosen run length, {run length: ms per launch}),
+    "pencil_depth": (chosen depth, {depth: ms per viscous-flux + update pass})}"""
     import numpy as np
     rl = np.zeros(TUNING_SLOTS, dtype=np.int32)
     ms = np.zeros(3 * TUNING_SLOTS)
@@ -624,6 +628,13 @@ def _tuning(fn, h):
             if rl[s * 3 + d]:
                 out[f"{sname}_{dname}"] = (int(rl[s * 3 + d]), {
                     L: round(float(ms[(s * 3 + d) * 3 + v]), 4) for v, L in enumerate((1, 2, 4))})
+    if fn_pencil is not None:
+        depth = C.c_int(0)
+        pms = np.zeros(3)
+        check(fn_pencil(h, C.byref(depth), pms.ctypes.data))
+        if depth.value:
+            out["pencil_depth"] = (depth.value, {D: round(float(pms[v]), 4)
+                                                 for v, D in enumerate(PENCIL_DEPTHS)})
     return out
 
 

@@ -1,6 +1,7 @@
-"""The autotuned sweep variants (runs of 1, 2 or 4 faces per thread) are the
-same arithmetic; this pins that they give identical states, so a box's result
-does not depend on which variant the autotuner picked for its batch."""
+"""The autotuned variants are the same arithmetic: the sweeps' runs of 1, 2
+or 4 faces per thread, and the 2.5-D stencil kernels' pencil depths.  These
+tests pin that they give identical states, so a box's result does not depend
+on which variant the autotuner picked for its batch."""
 
 import os
 import subprocess
@@ -46,3 +47,48 @@ def test_sweep_variants_agree(tmp_path, precision):
         diff = np.abs(res[run] - res[1]).max()
         print(f"run {run} vs 1: max abs diff {diff:.3e}")
         assert np.array_equal(res[run], res[1])
+
+
+PENCIL_SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, "oracle"); sys.path.insert(0, "nuc3d-cartisian_b200/python"); sys.path.insert(0, "tests")
+from oracle_ctypes import Box, Oracle, WENO5Z
+from helpers import desc_from_box
+import nuc3d_b200 as nb
+prec = int(sys.argv[2])
+# nz = 72: partial last pencils at every depth; two boxes in one batch
+boxes = [Box(40, 24, 72, scheme=(WENO5Z,) * 3, mach=0.3, reynolds=700.0),
+         Box(32, 40, 20, scheme=(WENO5Z,) * 3, mach=0.5, reynolds=300.0)]
+out = []
+with nb.Batch(prec) as b:
+    ids = []
+    for box in boxes:
+        rng = np.random.default_rng(7)
+        q = [np.ascontiguousarray(a * (1 + 0.02 * rng.standard_normal(a.shape)))
+             for a in Oracle().tgv(box)]
+        i = b.add(desc_from_box(box, prec))
+        b.set_state(i, q)
+        ids.append(i)
+    b.step(3)
+    depth = b.tuning()["pencil_depth"][0]
+    for i in ids:
+        out.append(np.stack(b.get_state(i)).ravel())
+np.save(sys.argv[1], np.concatenate(out))
+print(depth)
+"""
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_pencil_depths_agree(tmp_path, precision):
+    """The 2.5-D stencil kernels' pencil depths (16, 32, 64 planes per tile,
+    chosen by the autotuner) compute every cell alike: identical states."""
+    res = {}
+    for depth in (16, 32, 64):
+        f = tmp_path / f"d{depth}.npy"
+        env = dict(os.environ, NUC3D_PENCIL_DEPTH=str(depth))
+        r = subprocess.run([sys.executable, "-c", PENCIL_SCRIPT, str(f), str(precision)], cwd=ROOT,
+                           env=env, check=True, capture_output=True, text=True)
+        assert int(r.stdout.split()[-1]) == depth
+        res[depth] = np.load(f)
+    for depth in (16, 64):
+        assert np.array_equal(res[depth], res[32])
