@@ -216,59 +216,38 @@ __device__ __forceinline__ double weno_js_combine_dq(double is0, double is1, dou
     return fma_(fma_(w2, g2, fma_(w1, g1, mul_(w0, g0))),
                 __drcp_rn(fma_(6.0, w1, fma_(3.0, w2, w0))), f2);
 }
-// FP32 (mixed path): the same product forms as FP64, with one fast
-// reciprocal per face instead of one per indicator (the reciprocals run on the
-// SM's small special-function unit, which the four-reciprocal form kept
-// about a third busy).  Range: the indicators s_k are first multiplied by the
-// power of two that brings their median into [1, 2) (exact: every weight
-// ratio is unchanged), and the scaled squares q_k (and tau^2) are clamped to
-// [1e-18, 1e18], so that a weight, a product of three such factors, stays
-// between 1e-36 and 1e37 and the denominator can neither overflow nor flush
-// to zero.  The clamps only act where a weight is at least 1e18 times
-// smaller than the largest one, so the face is correct to FP32 rounding for
-// any spread of the indicators (a CPU emulation against the FP64 formulas
-// over spreads up to 1e48, flat sub-stencils and tau = 0 agrees to 2.5e-7 of
-// the stencil's scale).  WENO5-Z with tau = 0 keeps its linear weights.
-
-// 2^-e for 2^e <= m < 2^(e+1), m a positive normal float (exponent bits only)
-__device__ __forceinline__ float pow2_inv_scale(float m) {
-    return __int_as_float(0x7f000000 - (__float_as_int(m) & 0x7f800000));
-}
-__device__ __forceinline__ float clamp_w_(float x) { return fminf(fmaxf(x, 1.0e-18f), 1.0e18f); }
-// the scale that brings the median of three positive normal floats into [1, 2)
-__device__ __forceinline__ float median_scale(float a, float b, float c) {
-    return pow2_inv_scale(fmaxf(fminf(a, b), fminf(fmaxf(a, b), c)));
-}
-__device__ __forceinline__ float scaled_sq_(float s, float sc) {
-    const float t = mul_(s, sc);
-    return clamp_w_(mul_(t, t));
-}
 __device__ __forceinline__ float weno_js_combine_dq(float is0, float is1, float is2, float g0,
                                                     float g1, float g2, float f2) {
     const float ss = 4.0f * 1.0e-6f;  // 4 eps
-    const float s0 = add_(ss, is0), s1 = add_(ss, is1), s2 = add_(ss, is2);
-    const float sc = median_scale(s0, s1, s2);
-    const float q0 = scaled_sq_(s0, sc), q1 = scaled_sq_(s1, sc), q2 = scaled_sq_(s2, sc);
-    // alpha_k / c_k * q0 q1 q2 = prod_{j != k} q_j
-    const float w0 = mul_(q1, q2), w1 = mul_(q0, q2), w2 = mul_(q0, q1);
+    float r0 = frcp_fast(add_(ss, is0)), r1 = frcp_fast(add_(ss, is1)), r2 = frcp_fast(add_(ss, is2));
+    const float a0 = mul_(r0, r0), a1 = mul_(r1, r1), a2 = mul_(r2, r2);
+    return fma_(fma_(a2, g2, fma_(a1, g1, mul_(a0, g0))),
+                frcp_fast(fma_(6.0f, a1, fma_(3.0f, a2, a0))), f2);
+}
+__device__ __forceinline__ double weno_z_combine_dq(double is0, double is1, double is2,
+                                                    double g0, double g1, double g2,
+                                                    double f2) {
+    const double ss2 = 16.0 * 1.0e-80;  // (4 eps)^2, eps = 1e-40
+    double tau = fabs(sub_(is2, is0));
+    double t2 = mul_(tau, tau);
+    double s0 = fma_(is0, is0, ss2), s1 = fma_(is1, is1, ss2), s2 = fma_(is2, is2, ss2);
+    // alpha_k / c_k * s0^2 s1^2 s2^2 = (s_k^2 + tau^2) prod_{j!=k} s_j^2
+    const double w0 = mul_(add_(s0, t2), mul_(s1, s2));
+    const double w1 = mul_(add_(s1, t2), mul_(s0, s2));
+    const double w2 = mul_(add_(s2, t2), mul_(s0, s1));
     return fma_(fma_(w2, g2, fma_(w1, g1, mul_(w0, g0))),
-                frcp_fast(fma_(6.0f, w1, fma_(3.0f, w2, w0))), f2);
+                __drcp_rn(fma_(6.0, w1, fma_(3.0, w2, w0))), f2);
 }
 __device__ __forceinline__ float weno_z_combine_dq(float is0, float is1, float is2, float g0,
                                                    float g1, float g2, float f2) {
-    // 1e-40 is below FP32's normal range; 1e-30 stands in (it only matters
-    // where a sub-stencil is exactly constant)
-    const float ss = 4.0f * 1.0e-30f;  // 4 eps
-    const float s0 = add_(is0, ss), s1 = add_(is1, ss), s2 = add_(is2, ss);
-    const float sc = median_scale(s0, s1, s2);
-    const float q0 = scaled_sq_(s0, sc), q1 = scaled_sq_(s1, sc), q2 = scaled_sq_(s2, sc);
-    const float t = mul_(fabsf(sub_(is2, is0)), sc), t2 = fminf(mul_(t, t), 1.0e18f);
-    // alpha_k / c_k * q0 q1 q2 = (q_k + tau^2) prod_{j != k} q_j
-    const float w0 = mul_(add_(q0, t2), mul_(q1, q2));
-    const float w1 = mul_(add_(q1, t2), mul_(q0, q2));
-    const float w2 = mul_(add_(q2, t2), mul_(q0, q1));
-    return fma_(fma_(w2, g2, fma_(w1, g1, mul_(w0, g0))),
-                frcp_fast(fma_(6.0f, w1, fma_(3.0f, w2, w0))), f2);
+    const float ss = 4.0f * 1.0e-30f, cap = 1.0e15f;  // 4 eps
+    float tau = fabsf(sub_(is2, is0));
+    float t0 = fminf(mul_(tau, frcp_fast(add_(is0, ss))), cap);
+    float t1 = fminf(mul_(tau, frcp_fast(add_(is1, ss))), cap);
+    float t2 = fminf(mul_(tau, frcp_fast(add_(is2, ss))), cap);
+    const float a0 = fma_(t0, t0, 1.0f), a1 = fma_(t1, t1, 1.0f), a2 = fma_(t2, t2, 1.0f);
+    return fma_(fma_(a2, g2, fma_(a1, g1, mul_(a0, g0))),
+                frcp_fast(fma_(6.0f, a1, fma_(3.0f, a2, a0))), f2);
 }
 
 // One WENO5 face (either scheme) from the sliding window's differences:
