@@ -219,18 +219,26 @@ NUC3D_API long long nuc3d_batch_launch_count(const nuc3d_batch *b);
  * stencil kernels.  Runs a ~10 ms probe kernel on the legacy stream. */
 NUC3D_API int nuc3d_probe_peak(int precision, double *tflops);
 
-/* Autotuner result.  The directional WENO sweep has variants that give each
- * thread a run of 1, 2 or 4 consecutive faces; the first step after the set of
+/* Autotuner result.  The directional WENO sweep has variants in two tile
+ * shapes: 32 cells along the sweep with runs of 1, 2 or 4 consecutive faces
+ * per thread, and 64 cells with runs of 2 or 4 (fewer staged halo cells per
+ * cell, twice the shared memory per block).  The first step after the set of
  * (scheme, direction) pairs changes times every variant on the live boxes and
  * keeps the fastest.  run_len[s*3+d] (s: the scheme id, NUC3D_WENO5JS ..
  * NUC3D_WENO7JS; d: x, y, z) receives the chosen run length (0 = not tuned;
  * always 0 for CRWENO5, whose lines have no run variants),
- * ms[(s*3+d)*3+v] the measured milliseconds per launch of variant v (run
- * length 1, 2, 4).  run_len holds NUC3D_TUNING_SLOTS ints, ms
- * 3*NUC3D_TUNING_SLOTS doubles; either pointer may be NULL. */
+ * ms[(s*3+d)*3+v] the measured milliseconds per launch of the 32-cell
+ * variants (run length 1, 2, 4).  run_len holds NUC3D_TUNING_SLOTS ints, ms
+ * 3*NUC3D_TUNING_SLOTS doubles; either pointer may be NULL.
+ * nuc3d_tuning_tiles: tile_cells[s*3+d] the chosen tile length (32 or 64; 0 =
+ * not tuned), ms64[(s*3+d)*2+v] the milliseconds of the 64-cell variants
+ * (run length 2, 4); NUC3D_TUNING_SLOTS ints and 2*NUC3D_TUNING_SLOTS
+ * doubles, either may be NULL. */
 #define NUC3D_TUNING_SLOTS 12
 NUC3D_API int nuc3d_tuning(const nuc3d_ctx *ctx, int *run_len, double *ms);
 NUC3D_API int nuc3d_batch_tuning(const nuc3d_batch *b, int *run_len, double *ms);
+NUC3D_API int nuc3d_tuning_tiles(const nuc3d_ctx *ctx, int *tile_cells, double *ms64);
+NUC3D_API int nuc3d_batch_tuning_tiles(const nuc3d_batch *b, int *tile_cells, double *ms64);
 /* The other autotuned shape: the pencil depth of the 2.5-D stencil kernels
  * (viscous flux, update), i.e. how many z-planes one 32 x 8 column tile
  * marches (each tile re-reads a 6-plane halo, so deeper pencils read less but

@@ -80,14 +80,27 @@ int read_profile(Engine *eng, double *ms, long long *launches, int reset) {
 
 static_assert(kSchemes * 3 == NUC3D_TUNING_SLOTS, "tuning table layout");
 
+// run lengths and times of the 32-cell-tile variants 0..2 (runs of 1, 2, 4)
 int read_tuning(const Engine *eng, int *run_len, double *ms) {
-    static const int lens[kInvVariants] = {1, 2, 4};
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) {
             int v = eng->inv_variant[s][d];
-            if (run_len) run_len[s * 3 + d] = v < 0 ? 0 : lens[v];
-            for (int k = 0; k < kInvVariants; ++k)
-                if (ms) ms[(s * 3 + d) * kInvVariants + k] = eng->inv_tune_ms[s][d][k];
+            if (run_len) run_len[s * 3 + d] = v < 0 ? 0 : kInvRunLen[v];
+            for (int k = 0; k < 3; ++k)
+                if (ms) ms[(s * 3 + d) * 3 + k] = eng->inv_tune_ms[s][d][k];
+        }
+    return NUC3D_OK;
+}
+
+// tile lengths and times of the 64-cell-tile variants 3..4 (runs of 2, 4)
+int read_tiles(const Engine *eng, int *tile_cells, double *ms64) {
+    static_assert(kInvVariants == 5, "sweep tuning layout");
+    for (int s = 0; s < kSchemes; ++s)
+        for (int d = 0; d < 3; ++d) {
+            int v = eng->inv_variant[s][d];
+            if (tile_cells) tile_cells[s * 3 + d] = v < 0 ? 0 : kInvTileCells[v];
+            for (int k = 0; k < 2; ++k)
+                if (ms64) ms64[(s * 3 + d) * 2 + k] = eng->inv_tune_ms[s][d][3 + k];
         }
     return NUC3D_OK;
 }
@@ -111,6 +124,15 @@ int nuc3d_tuning_pencil(const nuc3d_ctx *c, int *depth, double *ms) {
 int nuc3d_batch_tuning_pencil(const nuc3d_batch *b, int *depth, double *ms) {
     if (!b) return fail(NUC3D_ERR_INVALID, "null batch");
     return read_pencil(b->eng, depth, ms);
+}
+
+int nuc3d_tuning_tiles(const nuc3d_ctx *c, int *tile_cells, double *ms64) {
+    if (!c) return fail(NUC3D_ERR_INVALID, "null context");
+    return read_tiles(c->eng, tile_cells, ms64);
+}
+int nuc3d_batch_tuning_tiles(const nuc3d_batch *b, int *tile_cells, double *ms64) {
+    if (!b) return fail(NUC3D_ERR_INVALID, "null batch");
+    return read_tiles(b->eng, tile_cells, ms64);
 }
 
 int nuc3d_tuning(const nuc3d_ctx *c, int *run_len, double *ms) {

@@ -328,7 +328,7 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));
     const bool mixed = precision_ == NUC3D_MIXED;
     std::vector<BoxDev> table(boxes_.size());
-    std::vector<WorkItem> prim, prim_step, st25[3], inv[kSchemes][3], cr[2][3];
+    std::vector<WorkItem> prim, prim_step, st25[3], inv[kSchemes][3][kInvTileClasses], cr[2][3];
     const int crtl = crweno_tile_lines();
     for (int c = 0; c < 2; ++c)
         for (int d = 0; d < 3; ++d) cr_nmax_[c][d] = cr_ms_[c][d] = 0;
@@ -375,20 +375,22 @@ int Engine::rebuild() {
                 }
                 continue;
             }
-            InvTileDims t = inviscid_tile(d, mixed);
-            auto &L = inv[s][d];
-            if (d == 0) {
-                for (int k = 0; k < p.n[2]; ++k)
-                    for (int b2 = 0; b2 < ceil_div(p.n[1], t.TL); ++b2)
-                        for (int a = 0; a < ceil_div(p.n[0], t.TC); ++a) L.push_back({id, a, b2, k});
-            } else if (d == 1) {
-                for (int k = 0; k < p.n[2]; ++k)
-                    for (int b2 = 0; b2 < ceil_div(p.n[1], t.TC); ++b2)
-                        for (int a = 0; a < ceil_div(p.n[0], t.TL); ++a) L.push_back({id, a, b2, k});
-            } else {
-                for (int c = 0; c < ceil_div(p.n[2], t.TC); ++c)
-                    for (int j = 0; j < p.n[1]; ++j)
-                        for (int a = 0; a < ceil_div(p.n[0], t.TL); ++a) L.push_back({id, a, j, c});
+            for (int tc = 0; tc < kInvTileClasses; ++tc) {
+                InvTileDims t = inviscid_tile(d, mixed, tc == 0 ? 32 : 64);
+                auto &L = inv[s][d][tc];
+                if (d == 0) {
+                    for (int k = 0; k < p.n[2]; ++k)
+                        for (int b2 = 0; b2 < ceil_div(p.n[1], t.TL); ++b2)
+                            for (int a = 0; a < ceil_div(p.n[0], t.TC); ++a) L.push_back({id, a, b2, k});
+                } else if (d == 1) {
+                    for (int k = 0; k < p.n[2]; ++k)
+                        for (int b2 = 0; b2 < ceil_div(p.n[1], t.TC); ++b2)
+                            for (int a = 0; a < ceil_div(p.n[0], t.TL); ++a) L.push_back({id, a, b2, k});
+                } else {
+                    for (int c = 0; c < ceil_div(p.n[2], t.TC); ++c)
+                        for (int j = 0; j < p.n[1]; ++j)
+                            for (int a = 0; a < ceil_div(p.n[0], t.TL); ++a) L.push_back({id, a, j, c});
+                }
             }
         }
     }
@@ -402,7 +404,8 @@ int Engine::rebuild() {
     append(prim_step, r_prim_step_);
     for (int v = 0; v < 3; ++v) append(st25[v], r_25d_[v]);
     for (int s = 0; s < kSchemes; ++s)
-        for (int d = 0; d < 3; ++d) append(inv[s][d], r_inv_[s][d]);
+        for (int d = 0; d < 3; ++d)
+            for (int tc = 0; tc < kInvTileClasses; ++tc) append(inv[s][d][tc], r_inv_[s][d][tc]);
     for (int c = 0; c < 2; ++c)
         for (int d = 0; d < 3; ++d) append(cr[c][d], r_cr_[c][d]);
     if ((int)boxes_.size() > d_boxes_cap_) {
@@ -429,7 +432,7 @@ int Engine::rebuild() {
     ECK(prepare_stencil_kernels(mixed));
     int per_stage = (r_prim_step_.n > 0) + (any_visc_ && r_25d_[0].n > 0) + (r_25d_[0].n > 0);
     for (int s = 0; s < kSchemes; ++s)
-        for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d].n > 0;
+        for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d][0].n > 0;
     for (int c = 0; c < 2; ++c)
         for (int d = 0; d < 3; ++d) per_stage += r_cr_[c][d].n > 0;
     launches_per_step_ = 3 * per_stage + 3;  // + clear_eig, dt, residual
@@ -498,8 +501,8 @@ int Engine::enqueue_step_t(cudaStream_t st) {
         auto sweeps = [&](int d) -> int {
             ProfScope ps(this, NUC3D_PROF_INV_X + d);
             for (int s = 0; s < kSchemes; ++s)
-                ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
-                                        r_inv_[s][d].n, in, d > 0,
+                ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + inv_range(s, d).off,
+                                        inv_range(s, d).n, in, d > 0,
                                         d == 0 ? (stage == 0 ? 2 : 1) : 0, st)));
             for (int c = 0; c < 2; ++c)
                 ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_,
@@ -568,19 +571,25 @@ int Engine::autotune() {
     bool need_sweep = false;
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d)
-            need_sweep = need_sweep || (r_inv_[s][d].n > 0 && inv_variant[s][d] < 0);
+            need_sweep = need_sweep || (r_inv_[s][d][0].n > 0 && inv_variant[s][d] < 0);
     const bool need_pencil =
         r_25d_[0].n > 0 && (pencil_variant < 0 || 2 * active_cells_ < pencil_tuned_cells ||
                             active_cells_ > 2 * pencil_tuned_cells);
     if (!need_sweep && !need_pencil) return NUC3D_OK;
-    // NUC3D_SWEEP_RUN=1|2|4 pins the run length and NUC3D_PENCIL_DEPTH=16|32|64
-    // the pencil depth (reproducibility studies)
+    // NUC3D_SWEEP_RUN=1|2|4 pins the run length (32-cell tiles; with
+    // NUC3D_SWEEP_TILE=64, runs of 2 or 4 on 64-cell tiles) and
+    // NUC3D_PENCIL_DEPTH=16|32|64 the pencil depth (reproducibility studies)
     if (need_sweep) {
         if (const char *pin = std::getenv("NUC3D_SWEEP_RUN")) {
-            int v = std::atoi(pin) == 1 ? 0 : (std::atoi(pin) == 2 ? 1 : 2);
+            const int run = std::atoi(pin);
+            const char *tile = std::getenv("NUC3D_SWEEP_TILE");
+            const int tc = tile && std::atoi(tile) == 64 && run != 1 ? 64 : 32;
+            int v = 2;
+            for (int k = 0; k < kInvVariants; ++k)
+                if (kInvRunLen[k] == run && kInvTileCells[k] == tc) v = k;
             for (int s = 0; s < kSchemes; ++s)
                 for (int d = 0; d < 3; ++d)
-                    if (r_inv_[s][d].n > 0 && inv_variant[s][d] < 0) inv_variant[s][d] = v;
+                    if (r_inv_[s][d][0].n > 0 && inv_variant[s][d] < 0) inv_variant[s][d] = v;
             need_sweep = false;
         }
     }
@@ -622,10 +631,10 @@ int Engine::autotune() {
     };
     for (int s = 0; s < kSchemes && rc == NUC3D_OK && need_sweep; ++s)
         for (int d = 0; d < 3 && rc == NUC3D_OK; ++d) {
-            const Range &rg = r_inv_[s][d];
-            if (rg.n <= 0 || inv_variant[s][d] >= 0) continue;
+            if (r_inv_[s][d][0].n <= 0 || inv_variant[s][d] >= 0) continue;
             int best = 0;
             for (int v = 0; v < kInvVariants && rc == NUC3D_OK; ++v) {
+                const Range &rg = r_inv_[s][d][inv_tile_class(v)];
                 const double ms = time3([&]() {
                     return mixed ? launch_inviscid<float>(s, d, v, d_boxes_, d_items_ + rg.off, rg.n,
                                                           0, d > 0, 0, stream_)
@@ -750,8 +759,8 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
                                  kPencilDepths[pv()], stream_)));
     for (int d = 0; d < 3; ++d) {
         for (int s = 0; s < kSchemes; ++s)
-            ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + r_inv_[s][d].off,
-                                    r_inv_[s][d].n, 0, d > 0, 0, stream_)));
+            ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + inv_range(s, d).off,
+                                    inv_range(s, d).n, 0, d > 0, 0, stream_)));
         for (int c = 0; c < 2; ++c)
             ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_, it + r_cr_[c][d].off,
                                   r_cr_[c][d].n, 0, d > 0, cr_nmax_[c][d], cr_ms_[c][d],

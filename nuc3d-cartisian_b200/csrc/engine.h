@@ -68,7 +68,8 @@ public:
     double prof_ms[NUC3D_PROF_CLASSES] = {};
     long long prof_n[NUC3D_PROF_CLASSES] = {};
     int profile_flush();
-    // autotuned run length per [scheme JS/Z][dir] (-1: not tuned yet) and the
+    // autotuned sweep variant (tile length and run length, kInvTileCells /
+    // kInvRunLen) per [scheme JS/Z/-/W7][dir] (-1: not tuned yet) and the
     // measured milliseconds per launch of each variant
     int inv_variant[kSchemes][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
     double inv_tune_ms[kSchemes][3][kInvVariants] = {};
@@ -112,7 +113,12 @@ private:
         size_t off = 0;
         int n = 0;
     };
-    Range r_prim_, r_inv_[kSchemes][3];  // [scheme JS/Z/-/W7][dir]
+    Range r_prim_;
+    Range r_inv_[kSchemes][3][kInvTileClasses];  // [scheme JS/Z/-/W7][dir][32/64-cell tiles]
+    // the work list of the variant the autotuner chose (32-cell tiles before)
+    const Range &inv_range(int s, int d) const {
+        return r_inv_[s][d][inv_variant[s][d] < 0 ? 0 : inv_tile_class(inv_variant[s][d])];
+    }
     // 2.5-D stencil tiles for each pencil depth of kPencilDepths
     Range r_25d_[3];
     long long active_cells_ = 0;

@@ -167,28 +167,41 @@ __global__ void k_residual(const BoxDev *boxes, int nboxes) {
 // -------------------------------------------------------------- k_inviscid --
 // Tile of the directional sweep: TL lines x TC cells along the sweep; every
 // thread owns one line and a run of R consecutive faces of it.  H is the
-// stencil half-width (3 for WENO5, 4 for WENO7).
-//   DIR 0 (x): 16 lines (rows j) per tile; the 8 runs of a line sit in 8
-//              consecutive lanes.
+// stencil half-width (3 for WENO5, 4 for WENO7).  TCX is the tile length
+// along the sweep, 32 or 64 cells (an autotuned shape: a 64-cell tile stages
+// 64 + 2H cells instead of 32 + 2H, 8 % fewer split fluxes per cell for
+// WENO5, at twice the shared memory per block).
+//   DIR 0 (x): 16 lines (rows j) per tile; the runs of a line sit in
+//              consecutive lanes of one warp (TCX / R <= 32).
 //   DIR 1/2:   TL = one 128-byte row of B (16 FP64 / 32 FP32 columns i) per
 //              tile; consecutive lanes are consecutive lines (coalesced).
-template <int DIR, typename B, int RUN, int H = 3>
+template <int DIR, typename B, int RUN, int H = 3, int TCX = 32>
 struct InvGeom {
+    static_assert(TCX == 32 || TCX == 64, "tile length");
+    static_assert(DIR != 0 || TCX / RUN <= 32, "the x sweep's runs of a line share a warp");
     static constexpr int R = RUN;               // faces per thread (1, 2 or 4)
-    static constexpr int NR = 32 / RUN;         // runs per line
-    static constexpr int TC = R * NR;           // cells per tile along the sweep (32)
+    static constexpr int NR = TCX / RUN;        // runs per line
+    static constexpr int TC = R * NR;           // cells per tile along the sweep (32 or 64)
     static constexpr int TL = DIR == 0 ? 16 : 128 / (int)sizeof(B);
     static constexpr int NF = TC + 2 * H;       // staged cells (H-cell halo each side)
     static constexpr int S = (NF + R - 1) / R;  // DIR 0 interleave stride
     static constexpr int NT = TL * NR;          // threads
     static constexpr int SF = DIR == 0 ? TL * R * S : NF * TL;  // staged values per flux
-    // WENO5: the staged tile (~52 KB) admits 4 blocks per SM; blocks of up to
-    // 256 threads are held to the registers that keep all 4 resident, larger
-    // ones to 64 registers per thread.  The FP32 4-face x tile (28 KB) is held
-    // to 6 blocks (80 registers; measured faster than 4 or 8).  (WENO7's sweep has its own kernel
-    // without a register cap.)
+    static constexpr size_t SMEM = sizeof(B) * (size_t)(10 * SF + 2 * NT);  // dynamic
+    // WENO5, 32-cell tiles: the staged tile (~52 KB) admits 4 blocks per SM;
+    // blocks of up to 256 threads are held to the registers that keep all 4
+    // resident, larger ones to 64 registers per thread.  The FP32 4-face x
+    // tile (28 KB) is held to 6 blocks (80 registers; measured faster than 4
+    // or 8).  64-cell tiles: as many blocks as their shared memory admits, at
+    // most 4 and at most 1024 threads per SM in all (at least 64 registers
+    // per thread).  (WENO7's sweep has its own kernel without a register
+    // cap.)
+    static constexpr int FIT = (int)((size_t)220 * 1024 / (SMEM + 1024));
+    static constexpr int MINB64 = FIT < 1 ? 1 : (FIT > 4 ? 4 : FIT);
+    static constexpr int CAP64 = 1024 / NT < 1 ? 1 : 1024 / NT;
     static constexpr int MINB =
-        NT <= 256 ? ((DIR == 0 && sizeof(B) == 4 && NT == 128) ? 6 : 4) : 1024 / NT;
+        TCX == 64 ? (MINB64 < CAP64 ? MINB64 : CAP64)
+                  : (NT <= 256 ? ((DIR == 0 && sizeof(B) == 4 && NT == 128) ? 6 : 4) : 1024 / NT);
     // thread -> (line, run)
     __device__ static void thread(int t, int &l, int &r) {
         if (DIR == 0) {
@@ -234,12 +247,12 @@ struct InvGeom {
 // line's value at the tile's first interior cell is subtracted before
 // rounding to FP32.  WENO5 commutes with adding a constant and the constant
 // cancels in the face difference, so this only removes rounding error.
-template <int SCHEME, int DIR, typename B, int RUN>
+template <int SCHEME, int DIR, typename B, int RUN, int TCX>
 __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
                                               const WorkItem *__restrict__ items, int in_slot,
                                               int accumulate, int prim_mode) {
     constexpr int H = scheme_halo(SCHEME);
-    using G = InvGeom<DIR, B, RUN, H>;
+    using G = InvGeom<DIR, B, RUN, H, TCX>;
     constexpr int TL = G::TL, TC = G::TC, NF = G::NF, R = G::R, NR = G::NR, NT = G::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     B *sF = reinterpret_cast<B *>(smem_raw);  // [10][SF] split fluxes (+ e, then - e)
@@ -616,60 +629,61 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
 // The WENO5 sweeps carry a register cap (InvGeom::MINB); the WENO7 sweep is
 // compiled without one (its own kernel, so that the register allocation is
 // left to the compiler's default).
-template <int SCHEME, int DIR, typename B, int RUN>
-__global__ void __launch_bounds__(InvGeom<DIR, B, RUN>::NT, InvGeom<DIR, B, RUN>::MINB)
+template <int SCHEME, int DIR, typename B, int RUN, int TCX>
+__global__ void __launch_bounds__(InvGeom<DIR, B, RUN, 3, TCX>::NT, InvGeom<DIR, B, RUN, 3, TCX>::MINB)
     k_inviscid(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, int in_slot,
                int accumulate, int prim_mode) {
-    inviscid_body<SCHEME, DIR, B, RUN>(boxes, items, in_slot, accumulate, prim_mode);
+    inviscid_body<SCHEME, DIR, B, RUN, TCX>(boxes, items, in_slot, accumulate, prim_mode);
 }
-template <int DIR, typename B, int RUN>
-__global__ void __launch_bounds__(InvGeom<DIR, B, RUN, 4>::NT)
+template <int DIR, typename B, int RUN, int TCX>
+__global__ void __launch_bounds__(InvGeom<DIR, B, RUN, 4, TCX>::NT)
     k_inviscid_w7(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items,
                   int in_slot, int accumulate, int prim_mode) {
-    inviscid_body<SCHEME_W7, DIR, B, RUN>(boxes, items, in_slot, accumulate, prim_mode);
+    inviscid_body<SCHEME_W7, DIR, B, RUN, TCX>(boxes, items, in_slot, accumulate, prim_mode);
 }
 
 using InvKernel = void (*)(const BoxDev *, const WorkItem *, int, int, int);
-template <int SCHEME, int DIR, typename B, int RUN>
+template <int SCHEME, int DIR, typename B, int RUN, int TCX>
 static InvKernel inv_kernel() {
     if constexpr (SCHEME == SCHEME_W7)
-        return k_inviscid_w7<DIR, B, RUN>;
+        return k_inviscid_w7<DIR, B, RUN, TCX>;
     else
-        return k_inviscid<SCHEME, DIR, B, RUN>;
+        return k_inviscid<SCHEME, DIR, B, RUN, TCX>;
 }
 
 // --------------------------------------------------------------- launches --
-template <int SCHEME, int DIR, typename B, int RUN>
+template <int SCHEME, int DIR, typename B, int RUN, int TCX>
 static size_t inv_smem_t() {
-    using G = InvGeom<DIR, B, RUN, scheme_halo(SCHEME)>;
-    return sizeof(B) * (size_t)(10 * G::SF + 2 * G::NT);
+    return InvGeom<DIR, B, RUN, scheme_halo(SCHEME), TCX>::SMEM;
 }
 
-InvTileDims inviscid_tile(int dir, bool mixed) {
-    // the tile shape is the same for every run length
-    if (dir == 0) return mixed ? InvTileDims{InvGeom<0, float, 1>::TL, InvGeom<0, float, 1>::TC}
-                               : InvTileDims{InvGeom<0, double, 1>::TL, InvGeom<0, double, 1>::TC};
-    return mixed ? InvTileDims{InvGeom<1, float, 1>::TL, InvGeom<1, float, 1>::TC}
-                 : InvTileDims{InvGeom<1, double, 1>::TL, InvGeom<1, double, 1>::TC};
+InvTileDims inviscid_tile(int dir, bool mixed, int tile_cells) {
+    // the lines per tile are the same for every run length and tile length
+    const int tl = dir == 0 ? InvGeom<0, double, 1>::TL
+                            : (mixed ? InvGeom<1, float, 1>::TL : InvGeom<1, double, 1>::TL);
+    return InvTileDims{tl, tile_cells};
 }
 
-template <int SCHEME, int DIR, typename B, int RUN>
+template <int SCHEME, int DIR, typename B, int RUN, int TCX>
 static cudaError_t launch_t(const BoxDev *boxes, const WorkItem *items, int nitems, int in_slot,
                             int accumulate, int prim_mode, cudaStream_t st) {
-    using G = InvGeom<DIR, B, RUN, scheme_halo(SCHEME)>;
+    using G = InvGeom<DIR, B, RUN, scheme_halo(SCHEME), TCX>;
     if (nitems <= 0) return cudaSuccess;
-    inv_kernel<SCHEME, DIR, B, RUN>()<<<nitems, G::NT, inv_smem_t<SCHEME, DIR, B, RUN>(), st>>>(
-        boxes, items, in_slot, accumulate, prim_mode);
+    inv_kernel<SCHEME, DIR, B, RUN, TCX>()<<<nitems, G::NT, inv_smem_t<SCHEME, DIR, B, RUN, TCX>(),
+                                             st>>>(boxes, items, in_slot, accumulate, prim_mode);
     return cudaGetLastError();
 }
 
+// variant v: kInvTileCells[v] cells per tile, kInvRunLen[v] faces per thread
 template <int SCHEME, int DIR, typename B>
 static cudaError_t launch_v(int variant, const BoxDev *boxes, const WorkItem *items, int nitems,
                             int in_slot, int accumulate, int prim_mode, cudaStream_t st) {
     switch (variant) {
-        case 0: return launch_t<SCHEME, DIR, B, 1>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
-        case 1: return launch_t<SCHEME, DIR, B, 2>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
-        default: return launch_t<SCHEME, DIR, B, 4>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        case 0: return launch_t<SCHEME, DIR, B, 1, 32>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        case 1: return launch_t<SCHEME, DIR, B, 2, 32>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        case 3: return launch_t<SCHEME, DIR, B, 2, 64>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        case 4: return launch_t<SCHEME, DIR, B, 4, 64>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        default: return launch_t<SCHEME, DIR, B, 4, 32>(boxes, items, nitems, in_slot, accumulate, prim_mode, st);
     }
 }
 
@@ -696,16 +710,17 @@ cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxe
     return cudaErrorInvalidValue;
 }
 
-template <int SCHEME, int DIR, typename B, int RUN>
+template <int SCHEME, int DIR, typename B, int RUN, int TCX>
 static cudaError_t prepare_t() {
-    return cudaFuncSetAttribute(inv_kernel<SCHEME, DIR, B, RUN>(),
+    return cudaFuncSetAttribute(inv_kernel<SCHEME, DIR, B, RUN, TCX>(),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)inv_smem_t<SCHEME, DIR, B, RUN>());
+                                (int)inv_smem_t<SCHEME, DIR, B, RUN, TCX>());
 }
 template <int SCHEME, int DIR, typename B>
 static cudaError_t prepare_runs() {
-    cudaError_t e[3] = {prepare_t<SCHEME, DIR, B, 1>(), prepare_t<SCHEME, DIR, B, 2>(),
-                        prepare_t<SCHEME, DIR, B, 4>()};
+    cudaError_t e[kInvVariants] = {prepare_t<SCHEME, DIR, B, 1, 32>(), prepare_t<SCHEME, DIR, B, 2, 32>(),
+                                   prepare_t<SCHEME, DIR, B, 4, 32>(), prepare_t<SCHEME, DIR, B, 2, 64>(),
+                                   prepare_t<SCHEME, DIR, B, 4, 64>()};
     for (cudaError_t x : e)
         if (x != cudaSuccess) return x;
     return cudaSuccess;

@@ -96,7 +96,7 @@ struct StageArgs {
 struct InvTileDims {
     int TL, TC;  // lines per tile, cells per tile along the sweep
 };
-InvTileDims inviscid_tile(int dir, bool mixed);
+InvTileDims inviscid_tile(int dir, bool mixed, int tile_cells);
 constexpr int kT25X = 32, kT25Y = 8;  // 2.5-D tile of the stencil kernels (x, y)
 // pencil depths (planes per work item) the autotuner chooses from; the first
 // is the default
@@ -111,9 +111,15 @@ cudaError_t launch_prim(const BoxDev *boxes, const WorkItem *items, int nitems, 
 cudaError_t launch_dt(const BoxDev *boxes, int nboxes, cudaStream_t st);
 cudaError_t launch_residual(const BoxDev *boxes, int nboxes, cudaStream_t st);
 cudaError_t launch_clear_eig(const BoxDev *boxes, int nboxes, cudaStream_t st);
-// variant: run length of the sweep kernel, 0 -> 1 face per thread,
-// 1 -> 2, 2 -> 4 (picked per scheme and direction by the engine's autotuner)
-constexpr int kInvVariants = 3;
+// variant v of the sweep kernel: tiles of kInvTileCells[v] cells along the
+// sweep, runs of kInvRunLen[v] faces per thread (picked per scheme and
+// direction by the engine's autotuner); variants 0-2 use 32-cell tiles, 3-4
+// 64-cell tiles (their work items differ: kInvTileClass)
+constexpr int kInvVariants = 5;
+constexpr int kInvTileCells[kInvVariants] = {32, 32, 32, 64, 64};
+constexpr int kInvRunLen[kInvVariants] = {1, 2, 4, 2, 4};
+constexpr int kInvTileClasses = 2;  // 32- and 64-cell tiles
+constexpr int inv_tile_class(int variant) { return variant >= 3 ? 1 : 0; }
 // scheme slots of the per-scheme sweep tables (indexed by scheme id; the
 // CRWENO5 slot stays empty, its lines run in launch_crweno)
 constexpr int kSchemes = 4;

@@ -161,6 +161,8 @@ def lib() -> C.CDLL:
         L.nuc3d_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.nuc3d_batch_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.nuc3d_tuning_pencil.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nuc3d_tuning_tiles.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nuc3d_batch_tuning_tiles.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.nuc3d_batch_tuning_pencil.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.nuc3d_stats.argtypes = [C.c_void_p, C.c_void_p]
         L.nuc3d_batch_stats.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
@@ -405,7 +407,8 @@ class Solver:
         return int(lib().nuc3d_launch_count(self._h))
 
     def tuning(self):
-        return _tuning(lib().nuc3d_tuning, self._h, lib().nuc3d_tuning_pencil)
+        return _tuning(lib().nuc3d_tuning, self._h, lib().nuc3d_tuning_pencil,
+                       lib().nuc3d_tuning_tiles)
 
 
 class Batch:
@@ -517,7 +520,8 @@ class Batch:
         return int(lib().nuc3d_batch_launch_count(self._h))
 
     def tuning(self):
-        return _tuning(lib().nuc3d_batch_tuning, self._h, lib().nuc3d_batch_tuning_pencil)
+        return _tuning(lib().nuc3d_batch_tuning, self._h, lib().nuc3d_batch_tuning_pencil,
+                       lib().nuc3d_batch_tuning_tiles)
 
 
 class Server:
@@ -615,19 +619,29 @@ def _spectra(fn, *args):
     return out
 
 
-def _tuning(fn, h, fn_pencil=None):
-    """{"<scheme>_<dir>": (chosen run length, {run length: ms per launch}),
-    "pencil_depth": (chosen depth, {depth: ms per viscous-flux + update pass})}"""
+def _tuning(fn, h, fn_pencil=None, fn_tiles=None):
+    """{"<scheme>_<dir>": (chosen "<tile cells>x<run length>", {variant: ms per
+    launch}), "pencil_depth": (chosen depth, {depth: ms per viscous-flux +
+    update pass})}; the sweep variants are "32x1", "32x2", "32x4", "64x2",
+    "64x4" (cells per tile along the sweep x faces per thread)."""
     import numpy as np
     rl = np.zeros(TUNING_SLOTS, dtype=np.int32)
     ms = np.zeros(3 * TUNING_SLOTS)
     check(fn(h, rl.ctypes.data, ms.ctypes.data))
+    tc = np.full(TUNING_SLOTS, 32, dtype=np.int32)
+    ms64 = np.zeros(2 * TUNING_SLOTS)
+    if fn_tiles is not None:
+        check(fn_tiles(h, tc.ctypes.data, ms64.ctypes.data))
     out = {}
     for s, sname in enumerate(("weno5js", "weno5z", "crweno5", "weno7js")):
         for d, dname in enumerate("xyz"):
-            if rl[s * 3 + d]:
-                out[f"{sname}_{dname}"] = (int(rl[s * 3 + d]), {
-                    L: round(float(ms[(s * 3 + d) * 3 + v]), 4) for v, L in enumerate((1, 2, 4))})
+            k = s * 3 + d
+            if rl[k]:
+                times = {f"32x{L}": round(float(ms[k * 3 + v]), 4) for v, L in enumerate((1, 2, 4))}
+                if fn_tiles is not None:
+                    times.update({f"64x{L}": round(float(ms64[k * 2 + v]), 4)
+                                  for v, L in enumerate((2, 4))})
+                out[f"{sname}_{dname}"] = (f"{int(tc[k])}x{int(rl[k])}", times)
     if fn_pencil is not None:
         depth = C.c_int(0)
         pms = np.zeros(3)

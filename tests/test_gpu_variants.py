@@ -1,5 +1,6 @@
 """The autotuned variants are the same arithmetic: the sweeps' runs of 1, 2
-or 4 faces per thread, and the 2.5-D stencil kernels' pencil depths.  These
+or 4 faces per thread on tiles of 32 or 64 cells, and the 2.5-D stencil
+kernels' pencil depths.  These
 tests pin that they give identical states, so a box's result does not depend
 on which variant the autotuner picked for its batch."""
 
@@ -36,17 +37,20 @@ np.save(sys.argv[1], np.stack(out))
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_sweep_variants_agree(tmp_path, precision):
+    """Runs of 1, 2, 4 faces on 32-cell tiles and of 2, 4 faces on 64-cell
+    tiles (the 40 x 24 x 36 box leaves partial 64-cell tiles along x and z)."""
     res = {}
-    for run in (1, 2, 4):
-        f = tmp_path / f"r{run}.npy"
-        env = dict(os.environ, NUC3D_SWEEP_RUN=str(run))
+    variants = [(1, 32), (2, 32), (4, 32), (2, 64), (4, 64)]
+    for run, tile in variants:
+        f = tmp_path / f"r{run}_{tile}.npy"
+        env = dict(os.environ, NUC3D_SWEEP_RUN=str(run), NUC3D_SWEEP_TILE=str(tile))
         subprocess.run([sys.executable, "-c", SCRIPT, str(f), str(precision)], cwd=ROOT, env=env,
                        check=True)
-        res[run] = np.load(f)
-    for run in (2, 4):
-        diff = np.abs(res[run] - res[1]).max()
-        print(f"run {run} vs 1: max abs diff {diff:.3e}")
-        assert np.array_equal(res[run], res[1])
+        res[(run, tile)] = np.load(f)
+    for v in variants[1:]:
+        diff = np.abs(res[v] - res[(1, 32)]).max()
+        print(f"variant {v} vs (1, 32): max abs diff {diff:.3e}")
+        assert np.array_equal(res[v], res[(1, 32)])
 
 
 PENCIL_SCRIPT = r"""
