@@ -232,8 +232,11 @@ NUC3D_API int nuc3d_probe_peak(int precision, double *tflops);
  * 3*NUC3D_TUNING_SLOTS doubles; either pointer may be NULL.
  * nuc3d_tuning_tiles: tile_cells[s*3+d] the chosen tile length (32 or 64; 0 =
  * not tuned), ms64[(s*3+d)*2+v] the milliseconds of the 64-cell variants
- * (run length 2, 4); NUC3D_TUNING_SLOTS ints and 2*NUC3D_TUNING_SLOTS
- * doubles, either may be NULL. */
+ * (run length 2, 4; 0 where not timed: mixed precision runs 32-cell tiles
+ * only, because its FP32 staging is offset by each line's value at the
+ * tile's first cell and another tile length would round differently);
+ * NUC3D_TUNING_SLOTS ints and 2*NUC3D_TUNING_SLOTS doubles, either may be
+ * NULL. */
 #define NUC3D_TUNING_SLOTS 12
 NUC3D_API int nuc3d_tuning(const nuc3d_ctx *ctx, int *run_len, double *ms);
 NUC3D_API int nuc3d_batch_tuning(const nuc3d_batch *b, int *run_len, double *ms);

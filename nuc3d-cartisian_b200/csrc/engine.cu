@@ -583,7 +583,9 @@ int Engine::autotune() {
         if (const char *pin = std::getenv("NUC3D_SWEEP_RUN")) {
             const int run = std::atoi(pin);
             const char *tile = std::getenv("NUC3D_SWEEP_TILE");
-            const int tc = tile && std::atoi(tile) == 64 && run != 1 ? 64 : 32;
+            const int tc = tile && std::atoi(tile) == 64 && run != 1 && !mixed_tiles_only32()
+                               ? 64
+                               : 32;
             int v = 2;
             for (int k = 0; k < kInvVariants; ++k)
                 if (kInvRunLen[k] == run && kInvTileCells[k] == tc) v = k;
@@ -634,6 +636,10 @@ int Engine::autotune() {
             if (r_inv_[s][d][0].n <= 0 || inv_variant[s][d] >= 0) continue;
             int best = 0;
             for (int v = 0; v < kInvVariants && rc == NUC3D_OK; ++v) {
+                if (inv_tile_class(v) == 1 && mixed_tiles_only32()) {
+                    inv_tune_ms[s][d][v] = 0.0;
+                    continue;
+                }
                 const Range &rg = r_inv_[s][d][inv_tile_class(v)];
                 const double ms = time3([&]() {
                     return mixed ? launch_inviscid<float>(s, d, v, d_boxes_, d_items_ + rg.off, rg.n,

@@ -123,6 +123,11 @@ private:
     Range r_25d_[3];
     long long active_cells_ = 0;
     int pv() const { return pencil_variant < 0 ? 0 : pencil_variant; }
+    // Mixed precision stages each line's split fluxes as FP32 offsets from
+    // their value at the tile's first cell, so the rounding depends on where
+    // tiles start: only the 32-cell tiles run there, which keeps every
+    // variant (and a box alone or in any batch) bitwise the same.
+    bool mixed_tiles_only32() const { return precision_ == NUC3D_MIXED; }
     // k_prim items of the boxes whose x direction runs the line kernel; the
     // x sweep (k_inviscid) recovers the primitives of the other boxes itself
     Range r_prim_step_;

@@ -37,10 +37,13 @@ np.save(sys.argv[1], np.stack(out))
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_sweep_variants_agree(tmp_path, precision):
-    """Runs of 1, 2, 4 faces on 32-cell tiles and of 2, 4 faces on 64-cell
-    tiles (the 40 x 24 x 36 box leaves partial 64-cell tiles along x and z)."""
+    """Runs of 1, 2, 4 faces on 32-cell tiles and, in FP64, of 2, 4 faces on
+    64-cell tiles (the 40 x 24 x 36 box leaves partial 64-cell tiles along x
+    and z).  Mixed precision runs 32-cell tiles only: its FP32 staging is
+    offset by each line's value at the tile's first cell, so another tile
+    length would round differently."""
     res = {}
-    variants = [(1, 32), (2, 32), (4, 32), (2, 64), (4, 64)]
+    variants = [(1, 32), (2, 32), (4, 32)] + ([(2, 64), (4, 64)] if precision == 0 else [])
     for run, tile in variants:
         f = tmp_path / f"r{run}_{tile}.npy"
         env = dict(os.environ, NUC3D_SWEEP_RUN=str(run), NUC3D_SWEEP_TILE=str(tile))
