@@ -90,7 +90,7 @@ __device__ __forceinline__ void cr_row(B f0, B f1, B f2, B f3, B f4, B &lo, B &b
              fma_(fma_(B(10), p0, fma_(B(25), p1, mul_(B(3), p2))), f2, mul_(mul_(B(2), p0), f1)));
 }
 
-__device__ __forceinline__ double rcp_(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ double rcp_(double x) { return drcp_nr(x); }
 __device__ __forceinline__ float rcp_(float x) { return frcp_fast(x); }
 
 template <typename B>

@@ -16,8 +16,8 @@ namespace nuc3d {
 
 // ----------------------------------------------------------------- k_prim --
 // physicsModel::con2prim (physicsModel.cpp:324-356) of one cell, FP64, with
-// one correctly rounded reciprocal of rho in place of the reference's five
-// divisions (each result within an ulp or two of the reference's).  k_prim
+// one reciprocal of rho (drcp_nr, within an ulp) in place of the reference's
+// five divisions (each result within an ulp or two of the reference's).  k_prim
 // and the x sweep (which recovers the primitives of its tile while staging)
 // share it, so both give bitwise the same W.
 struct PrimConst {
@@ -31,7 +31,7 @@ struct PrimCell {
     double u, v, w, p, c, T;
 };
 __device__ __forceinline__ void prim_cell(const PrimConst &k, const double Q[5], PrimCell &o) {
-    const double ri = __drcp_rn(Q[0]);
+    const double ri = drcp_nr(Q[0]);
     o.u = mul_(Q[1], ri);
     o.v = mul_(Q[2], ri);
     o.w = mul_(Q[3], ri);
