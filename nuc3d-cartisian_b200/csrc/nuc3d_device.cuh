@@ -134,7 +134,8 @@ __device__ __forceinline__ B sd2_(B f0, B f1, B f2) {
 // error, so the result is within an ulp of 1/x (not always the correctly
 // rounded value; an ulp is far below the 1e-12 parity bar).  Measured at
 // 256^3: WENO5-Z / WENO5-JS FP64 sweeps 4-6 % faster than with the correctly
-// rounded reciprocal.
+// rounded reciprocal.  (The WENO7 faces keep __drcp_rn: with this one their
+// uncapped y/z kernels took 158 instead of 128 registers and ran 7 % slower.)
 __device__ __forceinline__ double drcp_nr(double x) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
@@ -243,13 +244,15 @@ __device__ __forceinline__ double weno_z_combine_dq(double is0, double is1, doub
                                                     double g0, double g1, double g2,
                                                     double f2) {
     const double ss2 = 16.0 * 1.0e-80;  // (4 eps)^2, eps = 1e-40
-    double tau = fabs(sub_(is2, is0));
-    double t2 = mul_(tau, tau);
+    const double tau = sub_(is2, is0);
+    const double t2 = mul_(tau, tau);
     double s0 = fma_(is0, is0, ss2), s1 = fma_(is1, is1, ss2), s2 = fma_(is2, is2, ss2);
     // alpha_k / c_k * s0^2 s1^2 s2^2 = (s_k^2 + tau^2) prod_{j!=k} s_j^2
-    const double w0 = mul_(add_(s0, t2), mul_(s1, s2));
-    const double w1 = mul_(add_(s1, t2), mul_(s0, s2));
-    const double w2 = mul_(add_(s2, t2), mul_(s0, s1));
+    //                                = P + tau^2 prod_{j!=k} s_j^2,  P = s0^2 s1^2 s2^2
+    // (three products, one more for P, three FMAs)
+    const double p12 = mul_(s1, s2), p02 = mul_(s0, s2), p01 = mul_(s0, s1);
+    const double P = mul_(s0, p12);
+    const double w0 = fma_(t2, p12, P), w1 = fma_(t2, p02, P), w2 = fma_(t2, p01, P);
     return fma_(fma_(w2, g2, fma_(w1, g1, mul_(w0, g0))),
                 drcp_nr(fma_(6.0, w1, fma_(3.0, w2, w0))), f2);
 }
@@ -494,7 +497,7 @@ __device__ __forceinline__ double weno7_combine(const double is[4], const double
     double w2 = mul_(mul_(K7::C2, add_(s2, t2)), mul_(s3, p01));
     double w3 = mul_(mul_(K7::C3, add_(s3, t2)), mul_(s2, p01));
     double num = fma_(w3, q[3], fma_(w2, q[2], fma_(w1, q[1], mul_(w0, q[0]))));
-    return mul_(num, drcp_nr(add_(add_(add_(w0, w1), w2), w3)));
+    return mul_(num, __drcp_rn(add_(add_(add_(w0, w1), w2), w3)));
 }
 __device__ __forceinline__ double weno7_face(double f0, double f1, double f2, double f3, double f4,
                                              double f5, double f6) {
@@ -518,11 +521,11 @@ __device__ __forceinline__ double weno7_face_hc(double f0, double f1, double f2,
     double a[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const double r = mul_(tau, drcp_nr(add_(ss, is[k])));
+        const double r = mul_(tau, __drcp_rn(add_(ss, is[k])));
         a[k] = mul_(c[k], fma_(r, r, 1.0));
     }
     const double num = fma_(a[3], q[3], fma_(a[2], q[2], fma_(a[1], q[1], mul_(a[0], q[0]))));
-    return mul_(num, drcp_nr(add_(add_(add_(a[0], a[1]), a[2]), a[3])));
+    return mul_(num, __drcp_rn(add_(add_(add_(a[0], a[1]), a[2]), a[3])));
 }
 
 // FP32 (mixed path): the same indicators and candidates rewritten exactly in
@@ -619,10 +622,12 @@ __device__ __forceinline__ void hc_row(double f0, double f1, double f2, double f
     s0 = mul_(s0, s0);
     s1 = mul_(s1, s1);
     s2 = mul_(s2, s2);
-    const double P = mul_(mul_(s0, s1), s2);
-    const double A0 = mul_(mul_(K::CR0, add_(s0, t2)), mul_(s1, s2));
-    const double A1 = mul_(mul_(K::CR1, add_(s1, t2)), mul_(s0, s2));
-    const double A2 = mul_(mul_(K::CR2, add_(s2, t2)), mul_(s0, s1));
+    // A_k = c_k (s_k + tau^2) prod_{j!=k} s_j = c_k (P + tau^2 prod_{j!=k} s_j)
+    const double p12 = mul_(s1, s2), p02 = mul_(s0, s2), p01 = mul_(s0, s1);
+    const double P = mul_(s0, p12);
+    const double A0 = mul_(K::CR0, fma_(t2, p12, P));
+    const double A1 = mul_(K::CR1, fma_(t2, p02, P));
+    const double A2 = mul_(K::CR2, fma_(t2, p01, P));
     const double SA = add_(add_(A0, A1), A2);
     // theta = 1/(1 + x^2) > 1/2 with x = sum(alpha) - 1 = (SA - P)/P, i.e.
     // |SA - P| < P: decided without a division
