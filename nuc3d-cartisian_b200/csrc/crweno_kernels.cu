@@ -28,6 +28,7 @@
 #include <type_traits>
 
 #include "nuc3d_device.cuh"
+#include "prim_device.cuh"
 #include "rhs_kernels.h"
 
 namespace nuc3d {
@@ -141,10 +142,14 @@ int crweno_tile_lines() { return kCrTL; }
 
 // Work item (box, a, b, -): DIR 0: lines j = a*TL.., k = b; DIR 1: lines
 // i = a*TL.., k = b; DIR 2: lines i = a*TL.., j = b.
+// prim_mode (x lines only, whose blocks own whole lines): 0 reads the
+// primitives W; 1 first recovers the primitives of the block's lines from
+// the state (prim_cell, k_prim's work, bitwise the same) and writes W; 2
+// also folds their eigenvalues into the box's running maxima.
 template <typename B, int DIR, int SCH>
 __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
     k_crweno_lines(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items,
-                   int in_slot, int accumulate, int nmax, int ms) {
+                   int in_slot, int accumulate, int nmax, int ms, int prim_mode) {
     // SCH: SCHEME_CR (crweno5) or SCHEME_HC (hccs).  H: staged halo, explicit
     // faces per end and the first unknown face (3 for crweno5, 4 for hccs).
     constexpr int H = scheme_halo(SCH);
@@ -174,9 +179,8 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
     };
     // the box's point-wise split (LF / AUSM / AUSMp) of equation e at cell g
     const int riemann = bp.riemann;
-    auto split = [&](int e, long long g, double &fp, double &fm) {
-        const double qe = qbase[e * np + g];
-        const double un = wbase[DIR * np + g], p = wbase[3 * np + g], c = wbase[4 * np + g];
+    // (the cell's q_e, u_n, p, c already loaded)
+    auto split_v = [&](int e, double qe, double un, double p, double c, double &fp, double &fm) {
         if (riemann == RIEMANN_LF) {  // block-uniform; physicsModel.cpp:546-565
             const double hun = mul_(0.5, un), hlam = mul_(0.5, add_(fabs(un), c));
             double hf;
@@ -194,6 +198,10 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
             split_eq<DIR>(riemann, sc, e, qe, fp, fm);
         }
     };
+    auto split = [&](int e, long long g, double &fp, double &fm) {
+        split_v(e, qbase[e * np + g], wbase[DIR * np + g], wbase[3 * np + g], wbase[4 * np + g],
+                fp, fm);
+    };
     const bool mixed = sizeof(B) == sizeof(float);
     // hccs lines are always bounded (the reference's form); crweno5 has the
     // periodic form when the quirk bit is cleared
@@ -210,6 +218,29 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
     B *const wD = wC + ms * 32;
     const B inv_d = B(bp.inv_d[DIR]);
 
+    if (DIR == 0 && prim_mode != 0) {  // block-uniform
+        // con2prim of the block's whole lines: the staging below reads their
+        // W (written by this block, visible after the barrier)
+        const PrimConst pk(bp);
+        double lx = 0.0, ly = 0.0, lz = 0.0;
+        for (int t = threadIdx.x; t < kCrTL * n; t += kCrThreads) {
+            const int l = t / n, i = t - l * n;
+            if (l0 + l >= nl) break;  // lines are in order: the rest are outside too
+            const long long g = gidx(l, i);
+            double Q[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) Q[q] = qbase[q * np + g];
+            PrimCell o;
+            prim_cell(pk, Q, o);
+            prim_store(bd, g, o);
+            lx = fmax(add_(fabs(o.u), o.c), lx);
+            ly = fmax(add_(fabs(o.v), o.c), ly);
+            lz = fmax(add_(fabs(o.w), o.c), lz);
+        }
+        if (prim_mode == 2) eig_block_max(bd, lx, ly, lz);
+        __syncthreads();
+    }
+
     for (int e = 0; e < 5; ++e) {
         if (mixed) {  // per-line reference: the split flux at cell 0
             if (threadIdx.x < kCrTL) {
@@ -220,29 +251,54 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
             }
             __syncthreads();
         }
-        // stage F+ / F- of cells -H .. n+H-1
+        // stage F+ / F- of cells -H .. n+H-1, two cells per thread and pass
+        // with all eight loads issued before either split
         const int nst = n + 2 * H;
-        for (int t = threadIdx.x; t < kCrTL * nst; t += kCrThreads) {
-            int l, pc;
-            if (DIR == 0) {
-                l = t / nst;
-                pc = t - l * nst;
-            } else {
-                l = t % kCrTL;
-                pc = t / kCrTL;
-            }
-            double fp = 0.0, fm = 0.0;
-            if (l0 + l < nl) {
-                int pos = pc - H;
-                pos = pos < 0 ? pos + n : (pos >= n ? pos - n : pos);
-                split(e, gidx(l, pos), fp, fm);
-                if (mixed) {
-                    fp = sub_(fp, sRef[0][l]);
-                    fm = sub_(fm, sRef[1][l]);
+        constexpr int SU = 2;
+        for (int t0 = threadIdx.x; t0 < kCrTL * nst; t0 += SU * kCrThreads) {
+            int ls_[SU], pcs[SU];
+            bool ok[SU];
+            double qe[SU], un[SU], pp[SU], cc[SU];
+#pragma unroll
+            for (int u = 0; u < SU; ++u) {
+                const int t = t0 + u * kCrThreads;
+                int l, pc;
+                if (DIR == 0) {
+                    l = t / nst;
+                    pc = t - l * nst;
+                } else {
+                    l = t % kCrTL;
+                    pc = t / kCrTL;
+                }
+                ls_[u] = l;
+                pcs[u] = pc;
+                ok[u] = t < kCrTL * nst && l0 + l < nl;
+                qe[u] = un[u] = pp[u] = cc[u] = 0.0;
+                if (ok[u]) {
+                    int pos = pc - H;
+                    pos = pos < 0 ? pos + n : (pos >= n ? pos - n : pos);
+                    const long long g = gidx(l, pos);
+                    qe[u] = qbase[e * np + g];
+                    un[u] = wbase[DIR * np + g];
+                    pp[u] = wbase[3 * np + g];
+                    cc[u] = wbase[4 * np + g];
                 }
             }
-            sF[l * ls + pc] = B(fp);
-            sF[(kCrTL + l) * ls + pc] = B(fm);
+#pragma unroll
+            for (int u = 0; u < SU; ++u) {
+                if (t0 + u * kCrThreads >= kCrTL * nst) break;
+                const int l = ls_[u], pc = pcs[u];
+                double fp = 0.0, fm = 0.0;
+                if (ok[u]) {
+                    split_v(e, qe[u], un[u], pp[u], cc[u], fp, fm);
+                    if (mixed) {
+                        fp = sub_(fp, sRef[0][l]);
+                        fm = sub_(fm, sRef[1][l]);
+                    }
+                }
+                sF[l * ls + pc] = B(fp);
+                sF[(kCrTL + l) * ls + pc] = B(fm);
+            }
         }
         __syncthreads();
 
@@ -468,34 +524,37 @@ cudaError_t prepare_crweno_kernels(bool mixed) {
 
 template <typename B, int SCH>
 static void launch_t(int dir, const BoxDev *boxes, const WorkItem *items, int nitems, int in_slot,
-                     int accumulate, int nmax, int ms, size_t smem, cudaStream_t st) {
+                     int accumulate, int nmax, int ms, int prim_mode, size_t smem,
+                     cudaStream_t st) {
     if (dir == 0)
         k_crweno_lines<B, 0, SCH><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot,
-                                                                    accumulate, nmax, ms);
+                                                                    accumulate, nmax, ms, prim_mode);
     else if (dir == 1)
         k_crweno_lines<B, 1, SCH><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot,
-                                                                    accumulate, nmax, ms);
+                                                                    accumulate, nmax, ms, 0);
     else
         k_crweno_lines<B, 2, SCH><<<nitems, kCrThreads, smem, st>>>(boxes, items, in_slot,
-                                                                    accumulate, nmax, ms);
+                                                                    accumulate, nmax, ms, 0);
 }
 
 template <typename B>
 cudaError_t launch_crweno(int sch, int dir, const BoxDev *boxes, const WorkItem *items,
                           int nitems, int in_slot, int accumulate, int nmax, int ms,
-                          cudaStream_t st) {
+                          int prim_mode, cudaStream_t st) {
     if (nitems <= 0) return cudaSuccess;
     const size_t smem = crweno_smem_bytes(sch, nmax, ms, sizeof(B) == sizeof(float));
     if (sch == SCHEME_HC)
-        launch_t<B, SCHEME_HC>(dir, boxes, items, nitems, in_slot, accumulate, nmax, ms, smem, st);
+        launch_t<B, SCHEME_HC>(dir, boxes, items, nitems, in_slot, accumulate, nmax, ms, prim_mode,
+                               smem, st);
     else
-        launch_t<B, SCHEME_CR>(dir, boxes, items, nitems, in_slot, accumulate, nmax, ms, smem, st);
+        launch_t<B, SCHEME_CR>(dir, boxes, items, nitems, in_slot, accumulate, nmax, ms, prim_mode,
+                               smem, st);
     return cudaGetLastError();
 }
 
 template cudaError_t launch_crweno<double>(int, int, const BoxDev *, const WorkItem *, int, int,
-                                           int, int, int, cudaStream_t);
+                                           int, int, int, int, cudaStream_t);
 template cudaError_t launch_crweno<float>(int, int, const BoxDev *, const WorkItem *, int, int,
-                                          int, int, int, cudaStream_t);
+                                          int, int, int, int, cudaStream_t);
 
 }  // namespace nuc3d

@@ -328,7 +328,7 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));
     const bool mixed = precision_ == NUC3D_MIXED;
     std::vector<BoxDev> table(boxes_.size());
-    std::vector<WorkItem> prim, prim_step, st25[3], inv[kSchemes][3][kInvTileClasses], cr[2][3];
+    std::vector<WorkItem> prim, st25[3], inv[kSchemes][3][kInvTileClasses], cr[2][3];
     const int crtl = crweno_tile_lines();
     for (int c = 0; c < 2; ++c)
         for (int d = 0; d < 3; ++d) cr_nmax_[c][d] = cr_ms_[c][d] = 0;
@@ -349,8 +349,6 @@ int Engine::rebuild() {
         for (long long c = 0; c * kPrimChunk < p.N; ++c)
             prim.push_back({id, (int)c, (int)std::min<long long>(kPrimChunk, p.N - c * kPrimChunk), 0});
         boxes_[i].prim_n = (int)prim.size() - boxes_[i].prim_off;
-        if (p.scheme[0] == SCHEME_CR || p.scheme[0] == SCHEME_HC)
-            prim_step.insert(prim_step.end(), prim.end() - boxes_[i].prim_n, prim.end());
         for (int v = 0; v < 3; ++v)
             for (int z = 0; z < ceil_div(p.n[2], kPencilDepths[v]); ++z)
                 for (int y = 0; y < ceil_div(p.n[1], kT25Y); ++y)
@@ -401,7 +399,6 @@ int Engine::rebuild() {
         all.insert(all.end(), v.begin(), v.end());
     };
     append(prim, r_prim_);
-    append(prim_step, r_prim_step_);
     for (int v = 0; v < 3; ++v) append(st25[v], r_25d_[v]);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d)
@@ -430,7 +427,7 @@ int Engine::rebuild() {
     ECK(prepare_inviscid_kernels(mixed));
     ECK(prepare_crweno_kernels(mixed));
     ECK(prepare_stencil_kernels(mixed));
-    int per_stage = (r_prim_step_.n > 0) + (any_visc_ && r_25d_[0].n > 0) + (r_25d_[0].n > 0);
+    int per_stage = (any_visc_ && r_25d_[0].n > 0) + (r_25d_[0].n > 0);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d][0].n > 0;
     for (int c = 0; c < 2; ++c)
@@ -491,23 +488,19 @@ int Engine::enqueue_step_t(cudaStream_t st) {
     }
     for (int stage = 0; stage < 3; ++stage) {
         const int in = stage, out = (stage + 1) % 3;
-        // primitives of the boxes whose x lines run the line kernel; the x
-        // sweep recovers those of the other boxes (and their eigenvalues on
-        // the first stage) while staging
-        if (r_prim_step_.n > 0) {
-            ProfScope ps(this, NUC3D_PROF_PRIM);
-            ECK(launch_prim(d_boxes_, it + r_prim_step_.off, r_prim_step_.n, in, stage == 0, st));
-        }
+        // the x sweeps (WENO tiles and CRWENO5 / hccs lines alike) recover
+        // the primitives of their cells, and on the first stage fold the
+        // eigenvalue maxima, before their splits
         auto sweeps = [&](int d) -> int {
             ProfScope ps(this, NUC3D_PROF_INV_X + d);
+            const int prim_mode = d == 0 ? (stage == 0 ? 2 : 1) : 0;
             for (int s = 0; s < kSchemes; ++s)
                 ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + inv_range(s, d).off,
-                                        inv_range(s, d).n, in, d > 0,
-                                        d == 0 ? (stage == 0 ? 2 : 1) : 0, st)));
+                                        inv_range(s, d).n, in, d > 0, prim_mode, st)));
             for (int c = 0; c < 2; ++c)
                 ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_,
                                       it + r_cr_[c][d].off, r_cr_[c][d].n, in, d > 0,
-                                      cr_nmax_[c][d], cr_ms_[c][d], st)));
+                                      cr_nmax_[c][d], cr_ms_[c][d], prim_mode, st)));
             return NUC3D_OK;
         };
         if (int rc = sweeps(0)) return rc;
@@ -769,7 +762,7 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
                                     inv_range(s, d).n, 0, d > 0, 0, stream_)));
         for (int c = 0; c < 2; ++c)
             ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_, it + r_cr_[c][d].off,
-                                  r_cr_[c][d].n, 0, d > 0, cr_nmax_[c][d], cr_ms_[c][d],
+                                  r_cr_[c][d].n, 0, d > 0, cr_nmax_[c][d], cr_ms_[c][d], 0,
                                   stream_)));
     }
     ECK(enqueue_forcing<B>(stream_));

@@ -128,9 +128,6 @@ private:
     // tiles start: only the 32-cell tiles run there, which keeps every
     // variant (and a box alone or in any batch) bitwise the same.
     bool mixed_tiles_only32() const { return precision_ == NUC3D_MIXED; }
-    // k_prim items of the boxes whose x direction runs the line kernel; the
-    // x sweep (k_inviscid) recovers the primitives of the other boxes itself
-    Range r_prim_step_;
     // line-solve tiles per [scheme: 0 crweno5, 1 hccs][dir], with the longest
     // line and the rows per lane that size each launch's shared memory
     Range r_cr_[2][3];

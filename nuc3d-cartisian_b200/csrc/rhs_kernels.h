@@ -152,9 +152,10 @@ int crweno_lanes(int sch, int n, bool bounded);
 int crweno_segment_rows(int sch, int n, bool bounded);
 size_t crweno_smem_bytes(int sch, int nmax, int ms, bool mixed);
 constexpr int kCrMaxCells = 512;  // longest CRWENO5 / hccs line (shared-memory bound)
+// prim_mode (dir 0 only; the blocks own whole x lines): as launch_inviscid's
 template <typename B>
 cudaError_t launch_crweno(int sch, int dir, const BoxDev *boxes, const WorkItem *items,
                           int nitems, int in_slot, int accumulate, int nmax, int ms,
-                          cudaStream_t st);
+                          int prim_mode, cudaStream_t st);
 
 }  // namespace nuc3d
