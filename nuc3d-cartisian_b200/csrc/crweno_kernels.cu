@@ -251,54 +251,29 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
             }
             __syncthreads();
         }
-        // stage F+ / F- of cells -H .. n+H-1, two cells per thread and pass
-        // with all eight loads issued before either split
+        // stage F+ / F- of cells -H .. n+H-1
         const int nst = n + 2 * H;
-        constexpr int SU = 2;
-        for (int t0 = threadIdx.x; t0 < kCrTL * nst; t0 += SU * kCrThreads) {
-            int ls_[SU], pcs[SU];
-            bool ok[SU];
-            double qe[SU], un[SU], pp[SU], cc[SU];
-#pragma unroll
-            for (int u = 0; u < SU; ++u) {
-                const int t = t0 + u * kCrThreads;
-                int l, pc;
-                if (DIR == 0) {
-                    l = t / nst;
-                    pc = t - l * nst;
-                } else {
-                    l = t % kCrTL;
-                    pc = t / kCrTL;
-                }
-                ls_[u] = l;
-                pcs[u] = pc;
-                ok[u] = t < kCrTL * nst && l0 + l < nl;
-                qe[u] = un[u] = pp[u] = cc[u] = 0.0;
-                if (ok[u]) {
-                    int pos = pc - H;
-                    pos = pos < 0 ? pos + n : (pos >= n ? pos - n : pos);
-                    const long long g = gidx(l, pos);
-                    qe[u] = qbase[e * np + g];
-                    un[u] = wbase[DIR * np + g];
-                    pp[u] = wbase[3 * np + g];
-                    cc[u] = wbase[4 * np + g];
+        for (int t = threadIdx.x; t < kCrTL * nst; t += kCrThreads) {
+            int l, pc;
+            if (DIR == 0) {
+                l = t / nst;
+                pc = t - l * nst;
+            } else {
+                l = t % kCrTL;
+                pc = t / kCrTL;
+            }
+            double fp = 0.0, fm = 0.0;
+            if (l0 + l < nl) {
+                int pos = pc - H;
+                pos = pos < 0 ? pos + n : (pos >= n ? pos - n : pos);
+                split(e, gidx(l, pos), fp, fm);
+                if (mixed) {
+                    fp = sub_(fp, sRef[0][l]);
+                    fm = sub_(fm, sRef[1][l]);
                 }
             }
-#pragma unroll
-            for (int u = 0; u < SU; ++u) {
-                if (t0 + u * kCrThreads >= kCrTL * nst) break;
-                const int l = ls_[u], pc = pcs[u];
-                double fp = 0.0, fm = 0.0;
-                if (ok[u]) {
-                    split_v(e, qe[u], un[u], pp[u], cc[u], fp, fm);
-                    if (mixed) {
-                        fp = sub_(fp, sRef[0][l]);
-                        fm = sub_(fm, sRef[1][l]);
-                    }
-                }
-                sF[l * ls + pc] = B(fp);
-                sF[(kCrTL + l) * ls + pc] = B(fm);
-            }
+            sF[l * ls + pc] = B(fp);
+            sF[(kCrTL + l) * ls + pc] = B(fm);
         }
         __syncthreads();
 
