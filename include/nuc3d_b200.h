@@ -140,6 +140,14 @@ NUC3D_API long long nuc3d_ctx_bytes(const nuc3d_box_desc *desc);
  * five fields in its restart files. */
 NUC3D_API int nuc3d_set_state_host(nuc3d_ctx *ctx, const double *const h_q[5]);
 NUC3D_API int nuc3d_get_state_host(nuc3d_ctx *ctx, double *const h_q[5]);
+/* The host copies enqueued on the context's stream without synchronising,
+ * so that a caller advancing several contexts on their own streams overlaps
+ * one context's copies with another's steps (the copy engines work in both
+ * directions while the SMs compute).  The host arrays should be page-locked
+ * (cudaHostAlloc / cudaHostRegister; pageable memory makes the copy
+ * synchronous) and must stay valid and untouched until nuc3d_sync returns. */
+NUC3D_API int nuc3d_set_state_host_async(nuc3d_ctx *ctx, const double *const h_q[5]);
+NUC3D_API int nuc3d_get_state_host_async(nuc3d_ctx *ctx, double *const h_q[5]);
 NUC3D_API int nuc3d_set_state_device(nuc3d_ctx *ctx, const double *const d_q[5]);
 NUC3D_API int nuc3d_get_state_device(nuc3d_ctx *ctx, double *const d_q[5]);
 

@@ -213,6 +213,14 @@ int nuc3d_get_state_host(nuc3d_ctx *c, double *const h_q[5]) {
     if (!c) return fail(NUC3D_ERR_INVALID, "null context");
     return c->eng->get_state(c->id, h_q, cudaMemcpyDeviceToHost, true);
 }
+int nuc3d_set_state_host_async(nuc3d_ctx *c, const double *const h_q[5]) {
+    if (!c) return fail(NUC3D_ERR_INVALID, "null context");
+    return c->eng->set_state(c->id, h_q, cudaMemcpyHostToDevice, false);
+}
+int nuc3d_get_state_host_async(nuc3d_ctx *c, double *const h_q[5]) {
+    if (!c) return fail(NUC3D_ERR_INVALID, "null context");
+    return c->eng->get_state(c->id, h_q, cudaMemcpyDeviceToHost, false);
+}
 int nuc3d_set_state_device(nuc3d_ctx *c, const double *const d_q[5]) {
     if (!c) return fail(NUC3D_ERR_INVALID, "null context");
     return c->eng->set_state(c->id, d_q, cudaMemcpyDeviceToDevice, false);

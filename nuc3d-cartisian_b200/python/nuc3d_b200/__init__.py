@@ -126,6 +126,8 @@ def lib() -> C.CDLL:
         L.nuc3d_ctx_destroy.argtypes = [C.c_void_p]
         L.nuc3d_set_state_host.argtypes = [C.c_void_p, _P5]
         L.nuc3d_get_state_host.argtypes = [C.c_void_p, _P5]
+        L.nuc3d_set_state_host_async.argtypes = [C.c_void_p, _P5]
+        L.nuc3d_get_state_host_async.argtypes = [C.c_void_p, _P5]
         L.nuc3d_set_state_device.argtypes = [C.c_void_p, _P5]
         L.nuc3d_get_state_device.argtypes = [C.c_void_p, _P5]
         L.nuc3d_step.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
@@ -341,6 +343,17 @@ class Solver:
             check(lib().nuc3d_set_state_device(self._h, _ptrs5(q)))
         else:
             check(lib().nuc3d_set_state_host(self._h, _ptrs5(q)))
+
+    def set_state_async(self, q):
+        """Enqueue the upload of 5 page-locked host float64 arrays on the
+        solver's stream (nuc3d_set_state_host_async); they must stay valid
+        until sync()."""
+        check(lib().nuc3d_set_state_host_async(self._h, _ptrs5(q)))
+
+    def get_state_async(self, out):
+        """Enqueue the download into 5 page-locked host float64 arrays
+        (nuc3d_get_state_host_async); they hold the state after sync()."""
+        check(lib().nuc3d_get_state_host_async(self._h, _ptrs5(out)))
 
     def get_state(self, out=None):
         import numpy as np
