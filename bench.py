@@ -349,7 +349,7 @@ def run_b200(args, rank, world, local_rank):
     # state from pinned memory, advances it one step with dt/residual read
     # back, and downloads the result, which is the next step's input
     e2e_serial_steps = max(1, min(args.steps, 5))
-    ser_q = [p.copy() for p in host_q]
+    ser_q = [torch.from_numpy(p.copy()).pin_memory().numpy() for p in host_q]  # pinned
     s64.set_state(ser_q)
     barrier()
     t0 = time.perf_counter()
