@@ -347,23 +347,12 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                     };
                     B a0, b0, c0, d0;
                     gen(r0, a0, b0, c0, d0);
-                    // forward: row j -> A x_first + x_j + C x_{j+1} = D.  The
-                    // rows are generated one ahead of the elimination: row
-                    // j+1's weights do not depend on the elimination's serial
-                    // chain (reciprocal after reciprocal), so the scheduler
-                    // can issue them while the chain of row j waits.
+                    // forward: row j -> A x_first + x_j + C x_{j+1} = D
                     B Ap = B(0), Cp = B(0), Dp = B(0);
-                    B na = B(0), nb = B(1), nc = B(0), nd = B(0);
-                    if (L > 1) {
-                        advance();
-                        gen(r0 + 1, na, nb, nc, nd);
-                    }
                     for (int j = 1; j < L; ++j) {
-                        const B a = na, b = nb, c = nc, d = nd;
-                        if (j + 1 < L) {
-                            advance();
-                            gen(r0 + j + 1, na, nb, nc, nd);
-                        }
+                        advance();
+                        B a, b, c, d;
+                        gen(r0 + j, a, b, c, d);
                         B bpv = b, An = a, Dn = d;
                         if (j > 1) {
                             bpv = b - a * Cp;
