@@ -77,11 +77,11 @@ FLOPS_INV_LAUNCH = FLOPS_INV_Z + FLOPS_PRIM / 3
 STATE_BYTES_PER_CELL_UPDATE = 320  # compulsory FP64 state traffic of 3 RK stages
 # DRAM bytes (read + write) per launch of the FP64 WENO5-Z sweep at 256^3,
 # mean of x, y, z: the ncu capture at 128^3 in
-# profiles/k_inviscid_weno5z_fp64_128.md (215.9, 269.8, 276.8 MB; the x sweep
+# profiles/k_inviscid_weno5z_fp64_128.md (211.3, 268.3, 281.4 MB; the x sweep
 # reads the state only and writes the primitives as well as its RHS) scaled
 # by the cell count (x8); the traffic of a sweep is proportional to the cells
 # it covers (whole lines, no halo growth with size along the other axes).
-INV_TRAFFIC_BYTES = 8 * (215.891712e6 + 269.76768e6 + 276.840192e6) / 3
+INV_TRAFFIC_BYTES = 8 * (211.33696e6 + 268.335872e6 + 281.398784e6) / 3
 INV_TRAFFIC_NOTE = "ncu dram__bytes_read+write of the 128^3 capture x8 (cells), mean of x/y/z"
 
 
