@@ -116,23 +116,6 @@ int ceil_div(int a, int b) { return (a + b - 1) / b; }
         }                                                                 \
     } while (0)
 
-// A box whose y or z lines run the reference's bounded CRWENO5 / hccs system
-// sweeps them with the Thomas kernel and holds its scratch
-// (NUC3D_LINE_THOMAS=0 keeps the partitioned line solve for A/B studies).
-static bool uses_line_thomas(const nuc3d_box_desc &d) {
-    static const bool off = [] {
-        const char *v = std::getenv("NUC3D_LINE_THOMAS");
-        return v && std::atoi(v) == 0;
-    }();
-    if (off) return false;
-    for (int k = 1; k < 3; ++k) {
-        const int s = d.scheme[k];
-        if (s == NUC3D_HCCS || (s == NUC3D_CRWENO5 && (d.quirks & NUC3D_QUIRK_CRWENO_BOUNDED)))
-            return true;
-    }
-    return false;
-}
-
 int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
     auto bad = [&](int code, const char *m) {
         if (why) *why = m;
@@ -184,8 +167,6 @@ long long Engine::box_bytes(const nuc3d_box_desc &d) {
     long long bs = (long long)bulk_size(d.precision);
     long long b = 21 * np * 8 + 14 * np * bs + (long long)kSmallBytes;
     if (d.forcing != NUC3D_FORCING_NONE) b += (long long)forcing_scratch_bytes(bp, d.forcing_k);
-    if (uses_line_thomas(d))
-        b += (long long)crweno_thomas_scratch_bytes(bp, d.precision == NUC3D_MIXED);
     return b;
 }
 
@@ -197,7 +178,6 @@ Engine::~Engine() {
     for (auto &b : boxes_) {
         if (b.mem) cudaFreeAsync(b.mem, stream_);
         if (b.force_mem) cudaFreeAsync(b.force_mem, stream_);
-        if (b.line_mem) cudaFreeAsync(b.line_mem, stream_);
     }
     if (d_boxes_) cudaFreeAsync(d_boxes_, stream_);
     if (d_items_) cudaFreeAsync(d_items_, stream_);
@@ -230,12 +210,8 @@ int Engine::add_box(const nuc3d_box_desc &d, int *id) {
     cudaError_t e = cudaMallocAsync(&b.mem, bytes, stream_);
     if (e == cudaSuccess && d.forcing != NUC3D_FORCING_NONE)
         e = cudaMallocAsync(&b.force_mem, forcing_scratch_bytes(b.dev.p, d.forcing_k), stream_);
-    if (e == cudaSuccess && uses_line_thomas(d))
-        e = cudaMallocAsync(&b.line_mem,
-                            crweno_thomas_scratch_bytes(b.dev.p, precision_ == NUC3D_MIXED), stream_);
     if (e != cudaSuccess) {
         if (b.mem) cudaFreeAsync(b.mem, stream_);
-        if (b.force_mem) cudaFreeAsync(b.force_mem, stream_);
         cudaGetLastError();
         return set_last_error(NUC3D_ERR_NOMEM,
                               (std::string("device allocation failed: ") + cudaGetErrorString(e)).c_str());
@@ -259,7 +235,6 @@ int Engine::add_box(const nuc3d_box_desc &d, int *id) {
         ECK(forcing_prepare(b.dev.p, d.forcing_k, forcing_layout(b.dev.p, d.forcing_k, b.force_mem),
                             stream_));
     b.dev.tmw = nullptr;
-    b.dev.line_scratch = b.line_mem;
     if (b.dev.p.navier_stokes) {
         CUtensorMap maps[8];
         if (encode_visc_maps(b.dev, maps)) {
@@ -292,7 +267,6 @@ int Engine::remove_box(int id) {
     EngineBox &b = boxes_[id];
     ECK(cudaFreeAsync(b.mem, stream_));
     if (b.force_mem) ECK(cudaFreeAsync(b.force_mem, stream_));
-    if (b.line_mem) ECK(cudaFreeAsync(b.line_mem, stream_));
     b = EngineBox();
     dirty_ = true;
     return NUC3D_OK;
@@ -354,8 +328,7 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));
     const bool mixed = precision_ == NUC3D_MIXED;
     std::vector<BoxDev> table(boxes_.size());
-    std::vector<WorkItem> prim, st25[3], inv[kSchemes][3][kInvTileClasses], cr[2][3], crt[2][3];
-    const int thl = crweno_thomas_lines();
+    std::vector<WorkItem> prim, st25[3], inv[kSchemes][3][kInvTileClasses], cr[2][3];
     const int crtl = crweno_tile_lines();
     for (int c = 0; c < 2; ++c)
         for (int d = 0; d < 3; ++d) cr_nmax_[c][d] = cr_ms_[c][d] = 0;
@@ -385,13 +358,6 @@ int Engine::rebuild() {
             if (s == SCHEME_CR || s == SCHEME_HC) {
                 const int c = s == SCHEME_HC ? 1 : 0;
                 const bool bounded = s == SCHEME_HC || (p.quirks & QK_CRWENO_BOUNDED) != 0;
-                if (d > 0 && bounded && b.line_mem) {  // y/z Thomas sweep
-                    auto &T = crt[c][d];
-                    const int nf = d == 1 ? p.n[2] : p.n[1];
-                    for (int f = 0; f < nf; ++f)
-                        for (int g = 0; g < ceil_div(p.n[0], thl); ++g) T.push_back({id, g, f, 0});
-                    continue;
-                }
                 cr_nmax_[c][d] = std::max(cr_nmax_[c][d], p.n[d]);
                 cr_ms_[c][d] = std::max(cr_ms_[c][d], crweno_segment_rows(s, p.n[d], bounded));
                 auto &L = cr[c][d];
@@ -438,10 +404,7 @@ int Engine::rebuild() {
         for (int d = 0; d < 3; ++d)
             for (int tc = 0; tc < kInvTileClasses; ++tc) append(inv[s][d][tc], r_inv_[s][d][tc]);
     for (int c = 0; c < 2; ++c)
-        for (int d = 0; d < 3; ++d) {
-            append(cr[c][d], r_cr_[c][d]);
-            append(crt[c][d], r_crt_[c][d]);
-        }
+        for (int d = 0; d < 3; ++d) append(cr[c][d], r_cr_[c][d]);
     if ((int)boxes_.size() > d_boxes_cap_) {
         if (d_boxes_) ECK(cudaFreeAsync(d_boxes_, stream_));
         if (d_rhs_ptrs_) ECK(cudaFreeAsync(d_rhs_ptrs_, stream_));
@@ -468,7 +431,7 @@ int Engine::rebuild() {
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d][0].n > 0;
     for (int c = 0; c < 2; ++c)
-        for (int d = 0; d < 3; ++d) per_stage += (r_cr_[c][d].n > 0) + (r_crt_[c][d].n > 0);
+        for (int d = 0; d < 3; ++d) per_stage += r_cr_[c][d].n > 0;
     launches_per_step_ = 3 * per_stage + 3;  // + clear_eig, dt, residual
     for (const EngineBox &b : boxes_)
         if (b.live && b.dev.active && b.force_mem) launches_per_step_ += 3 * 8;  // forcing passes
@@ -534,13 +497,10 @@ int Engine::enqueue_step_t(cudaStream_t st) {
             for (int s = 0; s < kSchemes; ++s)
                 ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + inv_range(s, d).off,
                                         inv_range(s, d).n, in, d > 0, prim_mode, st)));
-            for (int c = 0; c < 2; ++c) {
+            for (int c = 0; c < 2; ++c)
                 ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_,
                                       it + r_cr_[c][d].off, r_cr_[c][d].n, in, d > 0,
                                       cr_nmax_[c][d], cr_ms_[c][d], prim_mode, st)));
-                ECK((launch_cr_thomas<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_,
-                                         it + r_crt_[c][d].off, r_crt_[c][d].n, in, d > 0, st)));
-            }
             return NUC3D_OK;
         };
         if (int rc = sweeps(0)) return rc;
@@ -800,13 +760,10 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
         for (int s = 0; s < kSchemes; ++s)
             ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + inv_range(s, d).off,
                                     inv_range(s, d).n, 0, d > 0, 0, stream_)));
-        for (int c = 0; c < 2; ++c) {
+        for (int c = 0; c < 2; ++c)
             ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_, it + r_cr_[c][d].off,
                                   r_cr_[c][d].n, 0, d > 0, cr_nmax_[c][d], cr_ms_[c][d], 0,
                                   stream_)));
-            ECK((launch_cr_thomas<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_,
-                                     it + r_crt_[c][d].off, r_crt_[c][d].n, 0, d > 0, stream_)));
-        }
     }
     ECK(enqueue_forcing<B>(stream_));
     StageArgs sa{-1, 0, 0, d_rhs_ptrs_};

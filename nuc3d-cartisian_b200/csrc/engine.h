@@ -20,7 +20,6 @@ struct EngineBox {
     int prim_off = 0, prim_n = 0;  // the box's k_prim work items (set by rebuild)
     void *mem = nullptr;   // one stream-ordered allocation holding all fields
     void *force_mem = nullptr;  // spectral forcing scratch (forced boxes only)
-    void *line_mem = nullptr;   // y/z Thomas line-sweep scratch (bounded CRWENO5 / hccs)
     double cfl = 0.5;
     long long steps = 0;   // host mirror of the device step counter
     bool live = false;     // slot in use
@@ -132,8 +131,6 @@ private:
     // line-solve tiles per [scheme: 0 crweno5, 1 hccs][dir], with the longest
     // line and the rows per lane that size each launch's shared memory
     Range r_cr_[2][3];
-    // Thomas line-sweep tiles of bounded CRWENO5 / hccs y and z lines [scheme][dir]
-    Range r_crt_[2][3];
     int cr_nmax_[2][3] = {}, cr_ms_[2][3] = {};
     int launches_per_step_ = 0;
     cudaGraph_t graph_ = nullptr;

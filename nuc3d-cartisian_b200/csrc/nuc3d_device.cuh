@@ -699,57 +699,6 @@ __device__ __forceinline__ void hc_row(float f0, float f1, float f2, float f3, f
                               mul_(mul_(sixth, w0), f1))));
 }
 
-// CRWENO5 weights up to a common positive factor (crweno5.cpp:136-150:
-// alpha_k = c_k / (eps + beta_k)^2, eps = 1e-6, c = 0.2, 0.5, 0.3 = 0.1 (2, 5,
-// 3)).  A compact row is linear in the weights and may be scaled freely, so
-// the normalisation by their sum is left out and the linear weights go into
-// the row's constants (cr_row): cr_p returns p_k with alpha_k proportional to
-// c_k p_k.  FP64 multiplies through by the product of the squares (no
-// division at all): p_k = prod_{j != k} (eps + beta_j)^2; FP32 uses fast
-// reciprocals: p_k = 1 / (eps + beta_k)^2.  The indicators arrive times 4
-// (is_k = 4 beta_k) and eps with them, an exact scaling.
-__device__ __forceinline__ void cr_p(double is0, double is1, double is2, double &p0, double &p1,
-                                     double &p2) {
-    const double ss = 4.0 * 1.0e-6;
-    double s0 = add_(ss, is0), s1 = add_(ss, is1), s2 = add_(ss, is2);
-    s0 = mul_(s0, s0);
-    s1 = mul_(s1, s1);
-    s2 = mul_(s2, s2);
-    p0 = mul_(s1, s2);
-    p1 = mul_(s0, s2);
-    p2 = mul_(s0, s1);
-}
-__device__ __forceinline__ void cr_p(float is0, float is1, float is2, float &p0, float &p1,
-                                     float &p2) {
-    const float ss = 4.0f * 1.0e-6f;
-    const float r0 = frcp_fast(add_(ss, is0)), r1 = frcp_fast(add_(ss, is1)),
-                r2 = frcp_fast(add_(ss, is2));
-    p0 = mul_(r0, r0);
-    p1 = mul_(r1, r1);
-    p2 = mul_(r2, r2);
-}
-
-// One compact-WENO row from the upwind-oriented stencil f0..f4 of its cell:
-// the upwind-side coupling lo, the diagonal b, the downwind-side coupling hi
-// and the right-hand side d (crweno5.cpp:151-161), all times 60 / (0.1 sum p)
-// (a row may be scaled freely): with w = 0.1 (2 p0, 5 p1, 3 p2),
-//   lo = 2/3 w0 + 1/3 w1            -> 8 p0 + 10 p1
-//   b  = 1/3 w0 + 2/3 (w1 + w2)     -> 4 p0 + 20 p1 + 12 p2
-//   hi = 1/3 w2                     -> 6 p2
-//   d  = w0/6 f1 + (5 (w0 + w1) + w2)/6 f2 + (w1 + 5 w2)/6 f3
-//                                   -> 2 p0 f1 + (10 p0 + 25 p1 + 3 p2) f2 + (5 p1 + 15 p2) f3
-template <typename B>
-__device__ __forceinline__ void cr_row(B f0, B f1, B f2, B f3, B f4, B &lo, B &b, B &hi, B &d) {
-    B is0, is1, is2, p0, p1, p2;
-    weno5_beta4(f0, f1, f2, f3, f4, is0, is1, is2);
-    cr_p(is0, is1, is2, p0, p1, p2);
-    lo = fma_(B(8), p0, mul_(B(10), p1));
-    b = fma_(B(4), p0, fma_(B(20), p1, mul_(B(12), p2)));
-    hi = mul_(B(6), p2);
-    d = fma_(fma_(B(15), p2, mul_(B(5), p1)), f3,
-             fma_(fma_(B(10), p0, fma_(B(25), p1, mul_(B(3), p2))), f2, mul_(mul_(B(2), p0), f1)));
-}
-
 // CD6 first derivative (centraldifference6th.cpp:44-46), times 1/dx.
 template <typename B>
 __device__ __forceinline__ B cd6(B m3, B m2, B m1, B p1, B p2, B p3, B inv_dx) {

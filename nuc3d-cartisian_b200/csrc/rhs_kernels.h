@@ -55,9 +55,6 @@ struct BoxDev {
     // (kViscTmaBox*); null when the box's rows are not TMA-aligned (odd nx)
     // or the box is inviscid
     const void *tmw;
-    // Thomas coefficients of the y/z line sweep (k_cr_thomas): bounded
-    // CRWENO5 / hccs boxes only, else null
-    void *line_scratch;
 };
 
 constexpr unsigned kFlagNonFinite = 1u, kFlagWaitTimeout = 2u;
@@ -160,15 +157,5 @@ template <typename B>
 cudaError_t launch_crweno(int sch, int dir, const BoxDev *boxes, const WorkItem *items,
                           int nitems, int in_slot, int accumulate, int nmax, int ms,
                           int prim_mode, cudaStream_t st);
-
-// CRWENO5 / hccs y and z sweeps of bounded (reference) lines, one thread per
-// (line, sign) Thomas solve (crweno_thomas.cu).  Work item (box, a, b, -):
-// lines i = a*crweno_thomas_lines() .. at k = b (dir 1) or j = b (dir 2).
-// The box's line_scratch holds crweno_thomas_scratch_bytes.
-int crweno_thomas_lines();
-size_t crweno_thomas_scratch_bytes(const BoxParams &p, bool mixed);
-template <typename B>
-cudaError_t launch_cr_thomas(int sch, int dir, const BoxDev *boxes, const WorkItem *items,
-                             int nitems, int in_slot, int accumulate, cudaStream_t st);
 
 }  // namespace nuc3d

@@ -99,44 +99,3 @@ def test_pencil_depths_agree(tmp_path, precision):
         res[depth] = np.load(f)
     for depth in (16, 64):
         assert np.array_equal(res[depth], res[32])
-
-
-LINE_SCRIPT = r"""
-import sys, numpy as np
-sys.path.insert(0, "oracle"); sys.path.insert(0, "nuc3d-cartisian_b200/python"); sys.path.insert(0, "tests")
-from oracle_ctypes import Box, Oracle, CRWENO5, HCCS
-from helpers import desc_from_box
-import nuc3d_b200 as nb
-prec = int(sys.argv[2])
-out = []
-for sch in (CRWENO5, HCCS):
-    # lines of 16 to 40 cells along y and z; nx = 72 leaves a partial
-    # 64-line group of the Thomas sweep
-    box = Box(72, 40, 16, scheme=(sch,) * 3, mach=0.3, reynolds=700.0)
-    rng = np.random.default_rng(3)
-    q = [np.ascontiguousarray(a * (1 + 0.02 * rng.standard_normal(a.shape))) for a in Oracle().tgv(box)]
-    with nb.Solver(desc_from_box(box, prec)) as s:
-        s.set_state(q)
-        s.step(3, 0.5)
-        out.append(np.stack(s.get_state()))
-np.save(sys.argv[1], np.stack(out))
-"""
-
-
-@pytest.mark.parametrize("precision", [0, 1])
-def test_line_sweeps_agree(tmp_path, precision):
-    """The y/z CRWENO5 and hccs lines solved by the one-thread-per-system
-    Thomas sweep (default) and by the partitioned warp solve
-    (NUC3D_LINE_THOMAS=0) agree to rounding: 1e-12 per-field relative L2 in
-    FP64, 1e-6 in mixed precision (hccs's discontinuous switch allowed 1e-4)."""
-    res = {}
-    for flag in ("1", "0"):
-        f = tmp_path / f"t{flag}.npy"
-        env = dict(os.environ, NUC3D_LINE_THOMAS=flag)
-        subprocess.run([sys.executable, "-c", LINE_SCRIPT, str(f), str(precision)], cwd=ROOT,
-                       env=env, check=True)
-        res[flag] = np.load(f)
-    for k, tol in enumerate((1e-12, 1e-12) if precision == 0 else (1e-6, 1e-4)):
-        a, b = res["1"][k], res["0"][k]
-        err = max(float(np.linalg.norm(x - y) / np.linalg.norm(y)) for x, y in zip(a, b))
-        assert err < tol, (k, err)
