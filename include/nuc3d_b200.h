@@ -222,9 +222,12 @@ NUC3D_API int nuc3d_batch_profile_read(nuc3d_batch *b, double *ms, long long *la
                                        int reset);
 NUC3D_API long long nuc3d_batch_launch_count(const nuc3d_batch *b);
 
-/* Measured FMA-pipe throughput of the current device in TFLOP/s (FP64 for
- * NUC3D_FP64, FP32 for NUC3D_MIXED): the roofline denominator of these
- * stencil kernels.  Runs a ~10 ms probe kernel on the legacy stream. */
+/* Diagnostic, not part of the solver: the measured FMA-pipe throughput of
+ * the current device in TFLOP/s (FP64 for NUC3D_FP64, FP32 for
+ * NUC3D_MIXED), the roofline denominator of these stencil kernels (which run
+ * on the FMA pipes, not on tensor cores, so neither a copy-bandwidth nor a
+ * tensor-GEMM peak bounds them).  Runs a ~10 ms probe kernel on the
+ * legacy stream; no solver entry point calls it. */
 NUC3D_API int nuc3d_probe_peak(int precision, double *tflops);
 
 /* Autotuner result.  The directional WENO sweep has variants in two tile
