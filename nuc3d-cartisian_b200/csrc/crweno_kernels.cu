@@ -223,8 +223,16 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
         // W (written by this block, visible after the barrier)
         const PrimConst pk(bp);
         double lx = 0.0, ly = 0.0, lz = 0.0;
+        // (line, cell) of t = tid, tid + kCrThreads, ... advanced without a division
+        int l = threadIdx.x / n, i = threadIdx.x - l * n;
         for (int t = threadIdx.x; t < kCrTL * n; t += kCrThreads) {
-            const int l = t / n, i = t - l * n;
+            if (t != (int)threadIdx.x) {
+                i += kCrThreads;
+                while (i >= n) {
+                    i -= n;
+                    ++l;
+                }
+            }
             if (l0 + l >= nl) break;  // lines are in order: the rest are outside too
             const long long g = gidx(l, i);
             double Q[5];
@@ -253,11 +261,21 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
         }
         // stage F+ / F- of cells -H .. n+H-1
         const int nst = n + 2 * H;
+        // x lines: (line, cell) of t advanced without a division
+        int sl = DIR == 0 ? (int)threadIdx.x / nst : 0;
+        int spc = DIR == 0 ? (int)threadIdx.x - sl * nst : 0;
         for (int t = threadIdx.x; t < kCrTL * nst; t += kCrThreads) {
             int l, pc;
             if (DIR == 0) {
-                l = t / nst;
-                pc = t - l * nst;
+                if (t != (int)threadIdx.x) {
+                    spc += kCrThreads;
+                    while (spc >= nst) {
+                        spc -= nst;
+                        ++sl;
+                    }
+                }
+                l = sl;
+                pc = spc;
             } else {
                 l = t % kCrTL;
                 pc = t / kCrTL;
@@ -308,9 +326,24 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                     return weno5js_face(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
                                         F(c0 + 4 * dir));
                 };
-                if (bounded && hl < 2 * H) {
-                    xm = hl < H ? hl : n - 2 * H + 1 + hl;
-                    xv = js(xm);
+                // lanes 0..2H-1: the explicit faces; lanes 2H and 2H+1: the
+                // identity rows' values (faces H and n-H), passed to the lanes
+                // that own those rows, so the warp evaluates explicit faces once
+                B did0 = B(0), did1 = B(0);
+                if (bounded) {
+                    B v = B(0);
+                    if (hl < 2 * H + 2) {
+                        const int m = hl < H ? hl
+                                             : (hl < 2 * H ? n - 2 * H + 1 + hl
+                                                           : (hl == 2 * H ? H : n - H));
+                        v = js(m);
+                        if (hl < 2 * H) {
+                            xm = m;
+                            xv = v;
+                        }
+                    }
+                    did0 = shfl(v, 2 * H);
+                    did1 = shfl(v, 2 * H + 1);
                 }
                 if (act) {
                     // window w[k] = F(i - 2 + k) of the current row's cell i (face i + 1)
@@ -318,12 +351,14 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                     B w[6];
     #pragma unroll
                     for (int k = 0; k < 6; ++k) w[k] = F(i - 2 + k);
-                    auto gen = [&](int r, B &a, B &b, B &c, B &d) {
-                        if (bounded && (r == 0 || r == N - 1)) {
+                    // row r of the system; `ends`: r may be a bounded system's
+                    // first or last row (identity rows)
+                    auto gen = [&](int r, bool ends, B &a, B &b, B &c, B &d) {
+                        if (ends && bounded && (r == 0 || r == N - 1)) {
                             a = B(0);
                             b = B(1);
                             c = B(0);
-                            d = js(r + H);
+                            d = r == 0 ? did0 : did1;
                         } else {
                             // '+': cells i-2..i+2 = w[0..4]; '-': cells i+3..i-1 = w[5..1]
                             // with the off-diagonals swapped (crweno5.cpp:335-338)
@@ -346,19 +381,16 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                         w[5] = F(i + 3);
                     };
                     B a0, b0, c0, d0;
-                    gen(r0, a0, b0, c0, d0);
-                    // forward: row j -> A x_first + x_j + C x_{j+1} = D
-                    B Ap = B(0), Cp = B(0), Dp = B(0);
-                    for (int j = 1; j < L; ++j) {
-                        advance();
-                        B a, b, c, d;
-                        gen(r0 + j, a, b, c, d);
-                        B bpv = b, An = a, Dn = d;
-                        if (j > 1) {
-                            bpv = b - a * Cp;
-                            An = -a * Ap;
-                            Dn = d - a * Dp;
-                        }
+                    gen(r0, true, a0, b0, c0, d0);
+                    // forward: row j -> A x_first + x_j + C x_{j+1} = D.  Starting
+                    // from (A, C, D) = (-1, 0, 0) makes row 1's update exact
+                    // (b - a 0 = b, -a (-1) = a, d - a 0 = d), so every row takes
+                    // the same code; only the last row can be an identity row.
+                    B Ap = B(-1), Cp = B(0), Dp = B(0);
+                    auto eliminate = [&](int j, B a, B b, B c, B d) {
+                        const B bpv = b - a * Cp;
+                        const B An = -a * Ap;
+                        const B Dn = d - a * Dp;
                         const B r = rcp_(bpv);
                         Ap = An * r;
                         Cp = c * r;
@@ -366,6 +398,18 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                         wA[j * 32 + lane] = Ap;
                         wC[j * 32 + lane] = Cp;
                         wD[j * 32 + lane] = Dp;
+                    };
+                    for (int j = 1; j < L - 1; ++j) {
+                        advance();
+                        B a, b, c, d;
+                        gen(r0 + j, false, a, b, c, d);
+                        eliminate(j, a, b, c, d);
+                    }
+                    {
+                        advance();
+                        B a, b, c, d;
+                        gen(r0 + L - 1, true, a, b, c, d);
+                        eliminate(L - 1, a, b, c, d);
                     }
                     la = Ap;
                     lc = Cp;
@@ -413,12 +457,16 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
             // x_first(l) = fd - fa x_last(l-1) - fc x_last(l).
             B xf, xl;
             {
-                const int lp1 = (hl + 1) % P, lm1 = (hl - 1 + P) % P;
+                // P is a power of two: lane indices wrap with a mask
+                const int pm = P - 1;
+                const int lp1 = (hl + 1) & pm, lm1 = (hl - 1) & pm;
                 const B nfa = shfl(fa, lp1), nfc = shfl(fc, lp1), nfd = shfl(fd, lp1);
                 const B r = rcp_(B(1) - la * fc - lc * nfa);
                 B ra = -la * fa * r, rc = -lc * nfc * r, rd = (ld - la * fd - lc * nfd) * r;
-                for (int s = 1; s < P; s <<= 1) {
-                    const int sm = (hl - s + P) % P, sp = (hl + s) % P;
+#pragma unroll
+                for (int s = 1; s < kCrLanes; s <<= 1) {
+                    if (s >= P) break;  // warp-uniform
+                    const int sm = (hl - s) & pm, sp = (hl + s) & pm;
                     B ma = shfl(ra, sm), mc = shfl(rc, sm), md = shfl(rd, sm);
                     B pa = shfl(ra, sp), pc = shfl(rc, sp), pd = shfl(rd, sp);
                     if (bounded && hl < s) ma = mc = md = B(0);
@@ -447,6 +495,9 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
         // dF/dx of the tile's cells from F^ = F^+ + F^- (euler3d.cpp:23-56, 143-253)
         // four cells per thread and pass, their RHS loads issued together
         constexpr int U = 4;
+        // x lines: (line, cell) of t = tid + m kCrThreads, advanced without a division
+        int dl = DIR == 0 ? (int)threadIdx.x / n : 0;
+        int di = DIR == 0 ? (int)threadIdx.x - dl * n : 0;
         for (int t0 = threadIdx.x; t0 < kCrTL * n; t0 += U * kCrThreads) {
             long long gi[U];
             B dfe[U], racc[U];
@@ -455,8 +506,13 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                 const int t = t0 + u * kCrThreads;
                 int l, i;
                 if (DIR == 0) {
-                    l = t / n;
-                    i = t - l * n;
+                    l = dl;
+                    i = di;
+                    di += kCrThreads;
+                    while (di >= n) {
+                        di -= n;
+                        ++dl;
+                    }
                 } else {
                     l = t % kCrTL;
                     i = t / kCrTL;
