@@ -264,6 +264,9 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
         // x lines: (line, cell) of t advanced without a division
         int sl = DIR == 0 ? (int)threadIdx.x / nst : 0;
         int spc = DIR == 0 ? (int)threadIdx.x - sl * nst : 0;
+        // two cells per pass keep more loads in flight (measured faster for
+        // crweno5; hccs's heavier rows leave no room for it)
+#pragma unroll(SCH == SCHEME_CR ? 2 : 1)
         for (int t = threadIdx.x; t < kCrTL * nst; t += kCrThreads) {
             int l, pc;
             if (DIR == 0) {
