@@ -148,6 +148,18 @@ NUC3D_API int nuc3d_get_state_host(nuc3d_ctx *ctx, double *const h_q[5]);
  * synchronous) and must stay valid and untouched until nuc3d_sync returns. */
 NUC3D_API int nuc3d_set_state_host_async(nuc3d_ctx *ctx, const double *const h_q[5]);
 NUC3D_API int nuc3d_get_state_host_async(nuc3d_ctx *ctx, double *const h_q[5]);
+/* Copy lane (on != 0; off when a context is created): the context's host
+ * transfers (the four host copies above) are issued one at a time per
+ * direction together with those of every other context on the device whose
+ * lane is on, in submission order.  Two large transfers in flight in the
+ * same direction share the host link and both finish late; chained, each
+ * one has the whole link, while uploads, downloads and the contexts' steps
+ * still overlap.  A transfer waits for the previously submitted one and so
+ * for whatever that one waits for on its own stream: turn the lane on for
+ * contexts that take turns (a pipeline of steps through host memory), not
+ * for independent ones.  No counterpart in the reference (one solver per
+ * process, singleBlock.cpp:50-71). */
+NUC3D_API int nuc3d_ctx_copy_lane(nuc3d_ctx *ctx, int on);
 NUC3D_API int nuc3d_set_state_device(nuc3d_ctx *ctx, const double *const d_q[5]);
 NUC3D_API int nuc3d_get_state_device(nuc3d_ctx *ctx, double *const d_q[5]);
 

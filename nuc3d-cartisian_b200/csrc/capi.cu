@@ -221,6 +221,11 @@ int nuc3d_get_state_host_async(nuc3d_ctx *c, double *const h_q[5]) {
     if (!c) return fail(NUC3D_ERR_INVALID, "null context");
     return c->eng->get_state(c->id, h_q, cudaMemcpyDeviceToHost, false);
 }
+int nuc3d_ctx_copy_lane(nuc3d_ctx *c, int on) {
+    if (!c) return fail(NUC3D_ERR_INVALID, "null context");
+    c->eng->copy_lane = on != 0;
+    return NUC3D_OK;
+}
 int nuc3d_set_state_device(nuc3d_ctx *c, const double *const d_q[5]) {
     if (!c) return fail(NUC3D_ERR_INVALID, "null context");
     return c->eng->set_state(c->id, d_q, cudaMemcpyDeviceToDevice, false);

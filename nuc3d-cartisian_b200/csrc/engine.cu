@@ -8,6 +8,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "forcing_kernels.h"
 #include "init_kernels.h"
@@ -170,9 +172,49 @@ long long Engine::box_bytes(const nuc3d_box_desc &d) {
     return b;
 }
 
-Engine::Engine(int precision, cudaStream_t stream) : precision_(precision), stream_(stream) {}
+namespace {
+// Copy lanes.  Host<->device state transfers of the engines on a device that
+// have their copy lane on run one at a time per direction, in submission
+// order (a transfer waits for the previously submitted one, whatever that
+// one waits for on its own stream): two large transfers in
+// flight in the same direction share the host link and both finish late, and
+// so do the steps that wait on them (at 256^3, two 671 MB uploads issued
+// together took 27 ms each against 12 ms one after the other).  Chained, each
+// transfer has the whole link; uploads and downloads still overlap each other
+// and the steps of other engines.  A lane holds the event of the last
+// transfer and the engine that owns it.
+struct CopyLane {
+    const void *owner = nullptr;
+    cudaEvent_t ev = nullptr;
+};
+std::mutex g_lane_mu;
+std::map<int, CopyLane> g_lanes[2];  // [upload, download][device]
+
+// the flags pointers of up to kMax boxes, passed by value to k_export_flags
+struct FlagPtrs {
+    static constexpr int kMax = 32;
+    const unsigned *p[kMax];
+    int n;
+};
+// flags of up to kMax boxes -> mapped host memory (zero-copy stores)
+__global__ void k_export_flags(FlagPtrs f, unsigned *out) {
+    const int i = threadIdx.x;
+    if (i < f.n) out[i] = *f.p[i];
+}
+}  // namespace
+
+Engine::Engine(int precision, cudaStream_t stream) : precision_(precision), stream_(stream) {
+    cudaGetDevice(&device_);
+}
 
 Engine::~Engine() {
+    {
+        std::lock_guard<std::mutex> lk(g_lane_mu);
+        for (auto &lanes : g_lanes) {
+            auto it = lanes.find(device_);
+            if (it != lanes.end() && it->second.owner == this) it->second = CopyLane{};
+        }
+    }
     cudaStreamSynchronize(stream_);
     invalidate_graph();
     for (auto &b : boxes_) {
@@ -185,6 +227,9 @@ Engine::~Engine() {
     if (d_stats_) cudaFreeAsync(d_stats_, stream_);
     cudaStreamSynchronize(stream_);
     for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
+    for (cudaEvent_t e : copy_ev_)
+        if (e) cudaEventDestroy(e);
+    if (h_flags_) cudaFreeHost(h_flags_);
     if (cap_stream_) cudaStreamDestroy(cap_stream_);
 }
 
@@ -295,15 +340,42 @@ int Engine::set_cfl(int id, double cfl) {
     return NUC3D_OK;
 }
 
+int Engine::chained_host_copy(int dir, int id, double *const host[5]) {
+    EngineBox &b = boxes_[id];
+    const size_t bytes = sizeof(double) * (size_t)b.dev.p.N;
+    if (!copy_ev_[dir]) ECK(cudaEventCreateWithFlags(&copy_ev_[dir], cudaEventDisableTiming));
+    std::lock_guard<std::mutex> lk(g_lane_mu);
+    CopyLane &lane = g_lanes[dir][device_];
+    // (this engine's own earlier transfers are ordered by its stream)
+    if (lane.ev && lane.owner != this) ECK(cudaStreamWaitEvent(stream_, lane.ev, 0));
+    for (int e = 0; e < 5; ++e) {
+        if (dir == 0)
+            ECK(cudaMemcpyAsync(fieldU(b.dev, 0, e), host[e], bytes, cudaMemcpyHostToDevice,
+                                stream_));
+        else
+            ECK(cudaMemcpyAsync(host[e], fieldU(b.dev, 0, e), bytes, cudaMemcpyDeviceToHost,
+                                stream_));
+    }
+    ECK(cudaEventRecord(copy_ev_[dir], stream_));
+    lane.owner = this;
+    lane.ev = copy_ev_[dir];
+    return NUC3D_OK;
+}
+
 int Engine::set_state(int id, const double *const q[5], cudaMemcpyKind kind, bool sync) {
     if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
         return set_last_error(NUC3D_ERR_INVALID, "no such box");
     if (!q) return set_last_error(NUC3D_ERR_INVALID, "null argument");
+    for (int e = 0; e < 5; ++e)
+        if (!q[e]) return set_last_error(NUC3D_ERR_INVALID, "null field pointer");
     EngineBox &b = boxes_[id];
     size_t bytes = sizeof(double) * (size_t)b.dev.p.N;
-    for (int e = 0; e < 5; ++e) {
-        if (!q[e]) return set_last_error(NUC3D_ERR_INVALID, "null field pointer");
-        ECK(cudaMemcpyAsync(fieldU(b.dev, 0, e), q[e], bytes, kind, stream_));
+    if (kind == cudaMemcpyHostToDevice && copy_lane) {
+        int rc = chained_host_copy(0, id, const_cast<double *const *>(q));
+        if (rc) return rc;
+    } else {
+        for (int e = 0; e < 5; ++e)
+            ECK(cudaMemcpyAsync(fieldU(b.dev, 0, e), q[e], bytes, kind, stream_));
     }
     if (sync) ECK(cudaStreamSynchronize(stream_));
     return NUC3D_OK;
@@ -313,11 +385,16 @@ int Engine::get_state(int id, double *const q[5], cudaMemcpyKind kind, bool sync
     if (id < 0 || id >= (int)boxes_.size() || !boxes_[id].live)
         return set_last_error(NUC3D_ERR_INVALID, "no such box");
     if (!q) return set_last_error(NUC3D_ERR_INVALID, "null argument");
+    for (int e = 0; e < 5; ++e)
+        if (!q[e]) return set_last_error(NUC3D_ERR_INVALID, "null field pointer");
     EngineBox &b = boxes_[id];
     size_t bytes = sizeof(double) * (size_t)b.dev.p.N;
-    for (int e = 0; e < 5; ++e) {
-        if (!q[e]) return set_last_error(NUC3D_ERR_INVALID, "null field pointer");
-        ECK(cudaMemcpyAsync(q[e], fieldU(b.dev, 0, e), bytes, kind, stream_));
+    if (kind == cudaMemcpyDeviceToHost && copy_lane) {
+        int rc = chained_host_copy(1, id, q);
+        if (rc) return rc;
+    } else {
+        for (int e = 0; e < 5; ++e)
+            ECK(cudaMemcpyAsync(q[e], fieldU(b.dev, 0, e), bytes, kind, stream_));
     }
     if (sync) ECK(cudaStreamSynchronize(stream_));
     return NUC3D_OK;
@@ -922,11 +999,34 @@ int Engine::spectra(int id, double *out, int *kmax_out) {
 }
 
 int Engine::sync_and_check(int id) {
+    // The boxes' status flags reach the host through page-locked memory mapped
+    // into the device, written by a one-warp kernel on this engine's stream:
+    // no copy engine is involved, so the check cannot queue behind another
+    // context's large state transfer (a synchronous cudaMemcpy of the flags
+    // waited for such a transfer and released contexts in bursts).
+    std::vector<int> ids;
+    for (size_t i = 0; i < boxes_.size(); ++i)
+        if (boxes_[i].live && (id < 0 || (int)i == id) && boxes_[i].dev.flags) ids.push_back((int)i);
+    if ((int)ids.size() > h_flags_cap_) {
+        if (h_flags_) cudaFreeHost(h_flags_);
+        h_flags_ = nullptr;
+        h_flags_cap_ = 0;
+        const int cap = std::max(64, (int)ids.size());
+        ECK(cudaHostAlloc(reinterpret_cast<void **>(&h_flags_), sizeof(unsigned) * cap,
+                          cudaHostAllocMapped));
+        h_flags_cap_ = cap;
+        ECK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&h_flags_dev_), h_flags_, 0));
+    }
+    for (size_t c = 0; c < ids.size(); c += FlagPtrs::kMax) {
+        FlagPtrs fp{};
+        fp.n = (int)std::min(ids.size() - c, (size_t)FlagPtrs::kMax);
+        for (int k = 0; k < fp.n; ++k) fp.p[k] = boxes_[ids[c + k]].dev.flags;
+        k_export_flags<<<1, FlagPtrs::kMax, 0, stream_>>>(fp, h_flags_dev_ + c);
+        ECK(cudaGetLastError());
+    }
     ECK(cudaStreamSynchronize(stream_));
-    for (size_t i = 0; i < boxes_.size(); ++i) {
-        if (!boxes_[i].live || (id >= 0 && (int)i != id)) continue;
-        unsigned f = 0;
-        ECK(cudaMemcpy(&f, boxes_[i].dev.flags, sizeof f, cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < ids.size(); ++k) {
+        const unsigned f = reinterpret_cast<volatile unsigned *>(h_flags_)[k];
         if (f & kFlagWaitTimeout)
             return set_last_error(NUC3D_ERR_CUDA, "a bounded device wait timed out (viscous-flux TMA load)");
         if (f & kFlagNonFinite) return set_last_error(NUC3D_ERR_NONFINITE, "state became non-finite (NaN/Inf)");

@@ -35,6 +35,8 @@ public:
     int remove_box(int id);
     int set_active(int id, bool on);
     int set_cfl(int id, double cfl);
+    // host transfers in the device's copy lanes (see chained_host_copy)
+    bool copy_lane = false;
     int set_state(int id, const double *const q[5], cudaMemcpyKind kind, bool sync);
     int get_state(int id, double *const q[5], cudaMemcpyKind kind, bool sync);
     // nsteps TVD-RK3 steps of every active box (graph replay unless profiling)
@@ -85,6 +87,10 @@ public:
     static int validate(const nuc3d_box_desc &d, std::string *why);
 
 private:
+    // issues this engine's copies of a host<->device state transfer (dir 0:
+    // upload, 1: download) after the last such transfer any engine on the
+    // device issued in that direction (copy lanes, engine.cu)
+    int chained_host_copy(int dir, int id, double *const host[5]);
     int rebuild();
     // launches of one step into stream s (eager on stream_, or on the private
     // capture stream while recording the graph)
@@ -136,6 +142,11 @@ private:
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
     cudaStream_t cap_stream_ = nullptr;  // graphs cannot be captured on the legacy stream
+    unsigned *h_flags_ = nullptr;      // mapped page-locked mirror of the boxes' flags
+    unsigned *h_flags_dev_ = nullptr;  // its device address
+    int h_flags_cap_ = 0;
+    int device_ = 0;                      // the device current at construction
+    cudaEvent_t copy_ev_[2] = {nullptr, nullptr};  // this engine's last upload / download
     double **d_rhs_ptrs_ = nullptr;  // 5 per box, for stage -1
     double *d_stats_ = nullptr;       // statistics scratch
     // profiling events

@@ -136,6 +136,7 @@ def lib() -> C.CDLL:
         L.nuc3d_ctx_time.restype = C.c_double
         L.nuc3d_ctx_time.argtypes = [C.c_void_p]
         L.nuc3d_profile_enable.argtypes = [C.c_void_p, C.c_int]
+        L.nuc3d_ctx_copy_lane.argtypes = [C.c_void_p, C.c_int]
         L.nuc3d_profile_read.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.nuc3d_launch_count.restype = C.c_longlong
         L.nuc3d_launch_count.argtypes = [C.c_void_p]
@@ -306,6 +307,84 @@ def _init_info(fn, *args):
             "reynolds": float(info[2])}
 
 
+class StepPipeline:
+    """Advances host-resident states of one box description through `depth`
+    solver contexts on their own streams, taking turns: submit() uploads a
+    page-locked input state, advances it `nsteps` TVD-RK3 steps and downloads
+    the result into a page-locked output, all enqueued without waiting.  The
+    contexts' transfers go through the device's copy lanes, so one context's
+    upload, another's steps and a third's download run at the same time and
+    each transfer has the whole host link.
+
+    A submitted pair of arrays must stay untouched until the same slot is
+    submitted again (submit() first waits for that slot's previous result)
+    or until drain() returns; submit() returns the slot.
+    """
+
+    def __init__(self, desc: "BoxDesc", depth: int = 3, cfl: float = 0.5, device=None):
+        import torch
+        if depth < 1:
+            raise ValueError("depth must be >= 1")
+        self.desc, self.cfl = desc, cfl
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else device
+        self._streams = [torch.cuda.Stream(dev) for _ in range(depth)]
+        self._solvers = []
+        try:
+            for st in self._streams:
+                s = Solver(desc, stream=st)
+                s.copy_lane(True)
+                self._solvers.append(s)
+        except Exception:
+            self.close()
+            raise
+        self._busy = [False] * depth
+        self._next = 0
+
+    @property
+    def depth(self) -> int:
+        return len(self._solvers)
+
+    def warm_up(self, q, nsteps: int = 1):
+        """Capture every context's step graph and tune its kernels on state q
+        (host arrays), so that submit() only replays."""
+        for s in self._solvers:
+            s.set_state(q)
+            s.step(nsteps, self.cfl, stats=False)
+            s.sync()
+
+    def submit(self, q_in, q_out, nsteps: int = 1) -> int:
+        k = self._next
+        self._next = (k + 1) % len(self._solvers)
+        s = self._solvers[k]
+        if self._busy[k]:
+            s.sync()  # the slot's previous result has landed in its output
+        s.set_state_async(q_in)
+        s.step(nsteps, self.cfl, stats=False)
+        s.get_state_async(q_out)
+        self._busy[k] = True
+        return k
+
+    def wait(self, slot: int):
+        """Blocks until the given slot's last submission has completed."""
+        self._solvers[slot].sync()
+        self._busy[slot] = False
+
+    def drain(self):
+        for k in range(len(self._solvers)):
+            self.wait(k)
+
+    def close(self):
+        for s in self._solvers:
+            s.close()
+        self._solvers = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class Solver:
     """One periodic box resident on the current CUDA device (nuc3d_ctx)."""
 
@@ -354,6 +433,12 @@ class Solver:
         """Enqueue the download into 5 page-locked host float64 arrays
         (nuc3d_get_state_host_async); they hold the state after sync()."""
         check(lib().nuc3d_get_state_host_async(self._h, _ptrs5(out)))
+
+    def copy_lane(self, on: bool = True):
+        """Issue this solver's host transfers in the device's copy lanes
+        (nuc3d_ctx_copy_lane): one transfer per direction at a time, in
+        submission order, across the solvers whose lane is on."""
+        check(lib().nuc3d_ctx_copy_lane(self._h, int(on)))
 
     def get_state(self, out=None):
         import numpy as np

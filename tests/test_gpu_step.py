@@ -413,3 +413,37 @@ def test_async_host_copies_match_sync(torch):
     for out in outs:
         for a, b in zip(out, ref):
             assert np.array_equal(a.numpy(), b)
+
+
+def test_step_pipeline_results_equal_single_steps(torch):
+    """nb.StepPipeline (contexts taking turns, transfers in the device's copy
+    lanes): every submission's output is one step of its own input, bit for
+    bit, with more submissions than slots so that slots are reused, and a
+    solver whose lane is off interleaved with the pipeline's transfers."""
+    import nuc3d_b200 as nb
+    box = Box(24, 20, 16, scheme=(WENO5Z,) * 3, mach=0.3, reynolds=500.0)
+    rng = np.random.default_rng(37)
+    base = Oracle().tgv(box)
+    inputs = [[np.ascontiguousarray(a * (1 + 0.02 * rng.standard_normal(a.shape))) for a in base]
+              for _ in range(5)]
+    refs = [gpu_steps(box, q, 1)[0] for q in inputs]
+    pin_in = [[torch.from_numpy(a).pin_memory().numpy() for a in q] for q in inputs]
+    outs = [[torch.empty(box.shape, dtype=torch.float64).pin_memory().numpy() for _ in range(5)]
+            for _ in inputs]
+    desc = desc_from_box(box)
+    other = nb.Solver(desc, stream=torch.cuda.Stream())
+    with nb.StepPipeline(desc, depth=2, cfl=0.5) as pipe:
+        pipe.warm_up(pin_in[0])
+        slots = []
+        for i, (qi, qo) in enumerate(zip(pin_in, outs)):
+            slots.append(pipe.submit(qi, qo))
+            if i == 1:  # an unchained context's transfers in between
+                other.set_state_async(pin_in[0])
+                other.step(1, 0.5, stats=False)
+        pipe.drain()
+        assert slots == [0, 1, 0, 1, 0]
+    other.sync()
+    other.close()
+    for out, ref in zip(outs, refs):
+        for a, b in zip(out, ref):
+            assert np.array_equal(a, b)
