@@ -370,7 +370,9 @@ def run_b200(args, rank, world, local_rank):
     pipe.warm_up(host_q, args.warmup)  # graph capture, autotuning
     outs = [[torch.empty(desc.shape, dtype=torch.float64).pin_memory().numpy()
              for _ in range(5)] for _ in range(n_pipe)]
-    e2e_steps = n_pipe * max(2, min(args.steps, 20) // n_pipe)
+    # (30 steps by default: the pipeline's fill and drain, about one step's
+    # upload + compute + download, spread over enough steps)
+    e2e_steps = n_pipe * max(2, min(max(args.steps, 30), 60) // n_pipe)
     barrier()
     t0 = time.perf_counter()
     for i in range(e2e_steps):

@@ -317,8 +317,11 @@ class StepPipeline:
     each transfer has the whole host link.
 
     A submitted pair of arrays must stay untouched until the same slot is
-    submitted again (submit() first waits for that slot's previous result)
-    or until drain() returns; submit() returns the slot.
+    submitted again (its previous result has landed when submit() returns)
+    or until drain() returns; submit() returns the slot.  A slot's next
+    upload and step are enqueued before the wait for its previous result, so
+    the wait never holds back work the device could start; drain() also
+    checks every context's status (non-finite state, device waits).
     """
 
     def __init__(self, desc: "BoxDesc", depth: int = 3, cfl: float = 0.5, device=None):
@@ -337,7 +340,7 @@ class StepPipeline:
         except Exception:
             self.close()
             raise
-        self._busy = [False] * depth
+        self._done = [None] * depth  # event after each slot's last download
         self._next = 0
 
     @property
@@ -353,21 +356,25 @@ class StepPipeline:
             s.sync()
 
     def submit(self, q_in, q_out, nsteps: int = 1) -> int:
+        import torch
         k = self._next
         self._next = (k + 1) % len(self._solvers)
         s = self._solvers[k]
-        if self._busy[k]:
-            s.sync()  # the slot's previous result has landed in its output
         s.set_state_async(q_in)
         s.step(nsteps, self.cfl, stats=False)
+        if self._done[k] is not None:
+            self._done[k].synchronize()  # the slot's previous result has landed
         s.get_state_async(q_out)
-        self._busy[k] = True
+        ev = torch.cuda.Event()
+        ev.record(self._streams[k])
+        self._done[k] = ev
         return k
 
     def wait(self, slot: int):
-        """Blocks until the given slot's last submission has completed."""
+        """Blocks until the given slot's last submission has completed and
+        checks its context's status."""
         self._solvers[slot].sync()
-        self._busy[slot] = False
+        self._done[slot] = None
 
     def drain(self):
         for k in range(len(self._solvers)):
