@@ -76,6 +76,12 @@ __device__ __forceinline__ int pmod(int c, int n) {
     int r = c % n;
     return r < 0 ? r + n : r;
 }
+// c mod n for c in [-n, 2n) (a halo index of at most one period outside the
+// box): a compare and an add instead of a division
+__device__ __forceinline__ int wrap1(int c, int n) {
+    c += c < 0 ? n : 0;
+    return c >= n ? c - n : c;
+}
 
 __device__ __forceinline__ double cd6d(double m3, double m2, double m1, double p1, double p2,
                                        double p3, double inv) {
@@ -331,8 +337,8 @@ __global__ void __launch_bounds__(TX *TY, 2)
     auto wxy = [&](int xx, int yy) -> long long {
         if constexpr (wrap_table)
             return sWx[xx] + sWy[yy];
-        else
-            return pmod(i0 - 3 + xx, nx) + (long long)nx * pmod(j0 - 3 + yy, ny);
+        else  // (halo indices lie within 3 cells of the box, extents >= 8)
+            return wrap1(i0 - 3 + xx, nx) + (long long)nx * wrap1(j0 - 3 + yy, ny);
     };
     auto issue = [&](int k, int buf) {
         const long long plane = sz * k;
