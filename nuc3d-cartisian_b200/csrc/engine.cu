@@ -190,6 +190,13 @@ struct CopyLane {
 std::mutex g_lane_mu;
 std::map<int, CopyLane> g_lanes[2];  // [upload, download][device]
 
+// NUC3D_STEP_FORK=0 keeps a captured step on one stream (the viscous fluxes
+// then run between the x and y sweeps); the default forks them
+bool step_fork_enabled() {
+    const char *env = std::getenv("NUC3D_STEP_FORK");
+    return !(env && env[0] == '0');
+}
+
 // the flags pointers of up to kMax boxes, passed by value to k_export_flags
 struct FlagPtrs {
     static constexpr int kMax = 32;
@@ -231,6 +238,9 @@ Engine::~Engine() {
         if (e) cudaEventDestroy(e);
     if (h_flags_) cudaFreeHost(h_flags_);
     if (cap_stream_) cudaStreamDestroy(cap_stream_);
+    if (fork_stream_) cudaStreamDestroy(fork_stream_);
+    for (cudaEvent_t e : fork_ev_)
+        if (e) cudaEventDestroy(e);
 }
 
 void Engine::invalidate_graph() {
@@ -585,14 +595,28 @@ int Engine::enqueue_step_t(cudaStream_t st) {
             ProfScope ps(this, NUC3D_PROF_DT);
             ECK(launch_dt(d_boxes_, nb, st));
         }
+        // The viscous fluxes need only this stage's primitives (the x sweep)
+        // and only the update reads them: in a captured step they run on a
+        // forked stream, beside the y and z sweeps (an HBM- and
+        // latency-bound kernel next to FP64-bound ones), and join before the
+        // update.  Eager (profiled) steps keep one stream.
+        const bool fork = any_visc_ && fork_stream_ && st == cap_stream_;
         if (any_visc_) {
             ProfScope ps(this, NUC3D_PROF_VISC);
+            cudaStream_t vs = st;
+            if (fork) {
+                ECK(cudaEventRecord(fork_ev_[0], st));
+                ECK(cudaStreamWaitEvent(fork_stream_, fork_ev_[0], 0));
+                vs = fork_stream_;
+            }
             ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_[pv()].off, r_25d_[pv()].n,
-                                     kPencilDepths[pv()], st)));
+                                     kPencilDepths[pv()], vs)));
+            if (fork) ECK(cudaEventRecord(fork_ev_[1], fork_stream_));
         }
         for (int d = 1; d < 3; ++d)
             if (int rc = sweeps(d)) return rc;
         ECK(enqueue_forcing<B>(st));
+        if (fork) ECK(cudaStreamWaitEvent(st, fork_ev_[1], 0));
         {
             ProfScope ps(this, NUC3D_PROF_UPDATE);
             StageArgs sa{stage, in, out, nullptr};
@@ -775,6 +799,11 @@ int Engine::step(int nsteps) {
         if (!exec_) {
             long long before = launches;
             if (!cap_stream_) ECK(cudaStreamCreateWithFlags(&cap_stream_, cudaStreamNonBlocking));
+            if (!fork_stream_ && step_fork_enabled()) {
+                ECK(cudaStreamCreateWithFlags(&fork_stream_, cudaStreamNonBlocking));
+                for (cudaEvent_t &ev : fork_ev_)
+                    ECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            }
             ECK(cudaStreamBeginCapture(cap_stream_, cudaStreamCaptureModeThreadLocal));
             int rc = enqueue_step(cap_stream_);
             cudaGraph_t g = nullptr;

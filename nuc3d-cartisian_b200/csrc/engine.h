@@ -142,6 +142,8 @@ private:
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
     cudaStream_t cap_stream_ = nullptr;  // graphs cannot be captured on the legacy stream
+    cudaStream_t fork_stream_ = nullptr;  // the captured step's viscous-flux branch
+    cudaEvent_t fork_ev_[2] = {nullptr, nullptr};  // fork after the x sweep, join before the update
     unsigned *h_flags_ = nullptr;      // mapped page-locked mirror of the boxes' flags
     unsigned *h_flags_dev_ = nullptr;  // its device address
     int h_flags_cap_ = 0;
