@@ -127,3 +127,28 @@ def test_batch_rejects_mismatched_precision(torch):
         bid = C.c_int(-1)
         rc = nb.lib().nuc3d_batch_add(B._h, C.byref(dd), C.byref(bid))
         assert rc == nb.ERR_INVALID
+
+
+def test_status_of_many_boxes_is_checked(torch):
+    """nuc3d_batch_sync reads every box's status flags (through mapped host
+    memory, up to 32 boxes per export launch): a zero density in box 37 of 40
+    (the second export chunk) is reported as a non-finite state, and the same
+    batch without it syncs cleanly."""
+    import nuc3d_b200 as nb
+    box = Box(8, 8, 8, scheme=(WENO5Z,) * 3, mach=0.2, reynolds=400.0)
+    q = Oracle().tgv(box)
+    for bad in (None, 37):
+        with nb.Batch(0) as B:
+            ids = [B.add(desc_from_box(box)) for _ in range(40)]
+            for i in ids:
+                qi = [np.array(a, copy=True) for a in q]
+                if i == ids[-3] and bad is not None:
+                    qi[0][2, 3, 4] = 0.0  # zero density -> non-finite con2prim
+                B.set_state(i, qi)
+            B.step(1)
+            if bad is None:
+                B.sync()
+            else:
+                with pytest.raises(nb.Nuc3dError) as ei:
+                    B.sync()
+                assert ei.value.code == nb.ERR_NONFINITE
