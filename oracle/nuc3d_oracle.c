@@ -199,8 +199,88 @@ static double weno7_face_eps(const double f[7], double ss, int literal_square) {
     return omega0 * q40 + omega1 * q41 + omega2 * q42 + omega3 * q43;
 }
 
+/* schemes.hpp:30 coeff_upwindcompact_c */
+static const double C_UPC[3] = {2.0 / 7.0, 4.0 / 7.0, 1.0 / 7.0};
+
+/* The WENO7-Z face of hccs77 and hccs78 (hccs77.cpp:79-135, hccs78.cpp:81-139
+ * and their halo forms): eps = 1e-20 (their member ss, :14), squares through
+ * libm's pow with their runtime member p = 2, as weno7js.  Also returns the
+ * unnormalised weights' sum, from which both form their blend
+ * theta = 1/(1 + (sum alpha - 1)^p). */
+static double weno7z_face_sum(const double f[7], double *alpha_sum) {
+    const double ss = 1.0e-20;
+    double is0 = f[0] * (547.0 * f[0] - 3882.0 * f[1] + 4642.0 * f[2] - 1854.0 * f[3]) +
+                 f[1] * (7043.0 * f[1] - 17246.0 * f[2] + 7042.0 * f[3]) +
+                 f[2] * (11003.0 * f[2] - 9402.0 * f[3]) + 2107.0 * f[3] * f[3];
+    double is1 = f[1] * (267.0 * f[1] - 1642.0 * f[2] + 1602.0 * f[3] - 494.0 * f[4]) +
+                 f[2] * (2843.0 * f[2] - 5966.0 * f[3] + 1922.0 * f[4]) +
+                 f[3] * (3443.0 * f[3] - 2522.0 * f[4]) + 547.0 * f[4] * f[4];
+    double is2 = f[2] * (547.0 * f[2] - 2522.0 * f[3] + 1922.0 * f[4] - 494.0 * f[5]) +
+                 f[3] * (3443.0 * f[3] - 5966.0 * f[4] + 1602.0 * f[5]) +
+                 f[4] * (2843.0 * f[4] - 1642.0 * f[5]) + 267.0 * f[5] * f[5];
+    double is3 = f[3] * (2107.0 * f[3] - 9402.0 * f[4] + 7042.0 * f[5] - 1854.0 * f[6]) +
+                 f[4] * (11003.0 * f[4] - 17246.0 * f[5] + 4642.0 * f[6]) +
+                 f[5] * (7043.0 * f[5] - 3882.0 * f[6]) + 547.0 * f[6] * f[6];
+    double q40 = A7[0][0] * f[0] + A7[0][1] * f[1] + A7[0][2] * f[2] + A7[0][3] * f[3];
+    double q41 = A7[1][0] * f[1] + A7[1][1] * f[2] + A7[1][2] * f[3] + A7[1][3] * f[4];
+    double q42 = A7[2][0] * f[2] + A7[2][1] * f[3] + A7[2][2] * f[4] + A7[2][3] * f[5];
+    double q43 = A7[3][0] * f[3] + A7[3][1] * f[4] + A7[3][2] * f[5] + A7[3][3] * f[6];
+    double tau7 = fabs(is0 - is3);
+    double alpha0 = C_W7[0] * (1.0 + PW(tau7 / (ss + is0)));
+    double alpha1 = C_W7[1] * (1.0 + PW(tau7 / (ss + is1)));
+    double alpha2 = C_W7[2] * (1.0 + PW(tau7 / (ss + is2)));
+    double alpha3 = C_W7[3] * (1.0 + PW(tau7 / (ss + is3)));
+    double alphaSum = alpha0 + alpha1 + alpha2 + alpha3;
+    double omega0 = alpha0 / alphaSum;
+    double omega1 = alpha1 / alphaSum;
+    double omega2 = alpha2 / alphaSum;
+    double omega3 = alpha3 / alphaSum;
+    *alpha_sum = alphaSum;
+    return omega0 * q40 + omega1 * q41 + omega2 * q42 + omega3 * q43;
+}
+
+/* hccs78's inner face (hccs78.cpp:81-139 for '+', :171-229 for '-'): the
+ * WENO7-Z face blended with the 8-cell central value q8 (symmetric about the
+ * face, the same expression for both signs) by theta = 1/(1 + (sum alpha -
+ * 1)^2): (1 - theta) W7 + theta q8.  g: the upwind-oriented 7-cell WENO7
+ * stencil; c[0..7]: cells m-4..m+3 around face m. */
+static double hccs78_face(const double g[7], const double c[8]) {
+    const double q8 = (-3.0 * (c[7] + c[0]) + 29.0 * (c[6] + c[1]) - 139.0 * (c[5] + c[2]) +
+                       533.0 * (c[4] + c[3])) / 840.0;
+    double alphaSum;
+    const double w7 = weno7z_face_sum(g, &alphaSum);
+    const double theta = 1.0 / (1.0 + PW(alphaSum - 1.0));
+    return (1.0 - theta) * w7 + theta * q8;
+}
+
+/* One row of hccs77 (hccs77.cpp:79-162 for '+', :246-305 for '-').  g[0..6]:
+ * the upwind-oriented 7-cell stencil of the row's cell i ('+': cells
+ * i-3..i+3; '-': cells i+4..i-2).  WENO7-Z weights and candidates, the
+ * 7th-order upwind compact value q7, theta = 1/(1 + (sum alpha - 1)^2);
+ * theta > 1/2 gives the linear upwind compact row (2/7, 4/7, 1/7 | q7),
+ * otherwise (2/7 theta, 1 - 3/7 theta, 1/7 theta | (1 - theta) W7 + theta q7).
+ * Returns the upwind-side coupling lo, the diagonal b, the downwind-side
+ * coupling hi and d. */
+static void hccs77_row(const double g[7], double *lo, double *b, double *hi, double *d) {
+    const double q7 = (-g[1] + 19.0 * g[2] + 239.0 * g[3] + 159.0 * g[4] + 4.0 * g[5]) / 420.0;
+    double alphaSum;
+    const double w7 = weno7z_face_sum(g, &alphaSum);
+    const double theta = 1.0 / (1.0 + PW(alphaSum - 1.0));
+    if (theta > 0.5) {
+        *lo = 2.0 / 7.0;
+        *b = 4.0 / 7.0;
+        *hi = 1.0 / 7.0;
+        *d = q7;
+    } else {
+        *lo = C_UPC[0] * theta;
+        *b = 1.0 + (C_UPC[1] - 1.0) * theta;
+        *hi = C_UPC[2] * theta;
+        *d = w7 * (1.0 - theta) + q7 * theta;
+    }
+}
+
 /* buffer (halo) width of a scheme (fieldOperator.cpp:128-175) */
-static int halo_of(int scheme) { return (scheme == OR_WENO7 || scheme == OR_HCCS) ? 4 : 3; }
+static int halo_of(int scheme) { return scheme >= OR_WENO7 ? 4 : 3; }
 
 /* One compact-WENO row (crweno5.cpp:131-162 for '+', :311-341 for '-').
  * f[0..4] is the upwind-oriented 5-cell stencil of the row's cell i
@@ -246,8 +326,6 @@ static void thomas_ref(int M, double *a, double *b, double *c, double *d, double
     for (int i = M - 2; i >= 0; i--) x[i] = d[i] - c[i] * x[i + 1];
 }
 
-/* schemes.hpp:30 coeff_upwindcompact_c */
-static const double C_UPC[3] = {2.0 / 7.0, 4.0 / 7.0, 1.0 / 7.0};
 
 /* One hybrid compact row of hccs (hccs.cpp:138-185 for '+', :375-420 for
  * '-').  f[0..4] is the upwind-oriented 5-cell stencil of the row's cell i
@@ -344,6 +422,63 @@ static void reconstruct_line_ref(int scheme, int upwind, unsigned quirks, int n,
                     for (int k = 0; k < 5; ++k) f[k] = line[i + 3 - k];
                     hccs_row(f, &lo, &bb, &hi, &dd);
                     c[r] = lo;
+                    a[r] = hi;
+                }
+                b[r] = bb;
+                d[r] = dd;
+            }
+        }
+        thomas_ref(M, a, b, c, d, x);
+        for (int r = 0; r < M; ++r) out[ibeg + 1 + r] = x[r];
+        return;
+    }
+    if (scheme == OR_HCCS78) {
+        /* hccs78 (hccs78.cpp): explicit.  Faces 0..3 and n-3..n WENO7-Z from
+         * the halos (:242-732); faces 4..n-4 (inner, :44-229) blended with
+         * q8. */
+        double g[7], c[8], sum;
+        for (int m = 0; m <= n; ++m) {
+            for (int k = 0; k < 7; ++k) g[k] = upwind > 0 ? line[m - 4 + k] : line[m + 3 - k];
+            if (m >= 4 && m <= n - 4) {
+                for (int k = 0; k < 8; ++k) c[k] = line[m - 4 + k];
+                out[m] = hccs78_face(g, c);
+            } else {
+                out[m] = weno7z_face_sum(g, &sum);
+            }
+        }
+        return;
+    }
+    if (scheme == OR_HCCS77) {
+        /* hccs77 (hccs77.cpp): faces 0..3 and n-3..n WENO7-Z from the halos
+         * (:330-818); the rows of cells i = 3..n-5 (faces 4..n-4, :44-305)
+         * solved by its Thomas sweep (:165-175), the first and last rows
+         * identity rows holding WENO7-Z values. */
+        double g[7], sum;
+        for (int m = 0; m <= n; ++m) {
+            if (m >= 4 && m <= n - 4) continue;
+            for (int k = 0; k < 7; ++k) g[k] = upwind > 0 ? line[m - 4 + k] : line[m + 3 - k];
+            out[m] = weno7z_face_sum(g, &sum);
+        }
+        int ibeg = 3, iend = n - 4, M = iend - ibeg;
+        if (M < 2) return;
+        double *a = work, *b = work + M, *c = work + 2 * M, *d = work + 3 * M, *x = work + 4 * M;
+        for (int r = 0; r < M; ++r) {
+            int i = ibeg + r;
+            /* the row's stencil: '+' cells i-3..i+3, '-' cells i+4..i-2 */
+            for (int k = 0; k < 7; ++k) g[k] = upwind > 0 ? line[i - 3 + k] : line[i + 4 - k];
+            if (r == 0 || r == M - 1) {
+                a[r] = 0.0;
+                b[r] = 1.0;
+                c[r] = 0.0;
+                d[r] = weno7z_face_sum(g, &sum);
+            } else {
+                double lo, bb, hi, dd;
+                hccs77_row(g, &lo, &bb, &hi, &dd);
+                if (upwind > 0) {
+                    a[r] = lo;
+                    c[r] = hi;
+                } else {
+                    c[r] = lo;  /* hccs77.cpp:282-291: '-' couples face i+2 upwind */
                     a[r] = hi;
                 }
                 b[r] = bb;

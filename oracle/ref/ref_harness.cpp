@@ -47,6 +47,8 @@
 #include "fft.h"
 #include "fieldOperator.h"
 #include "hccs.hpp"
+#include "hccs77.hpp"
+#include "hccs78.hpp"
 #include "physicsModel.h"
 #include "weno5js.h"
 #include "weno5z.hpp"
@@ -125,9 +127,10 @@ struct RefSolver {
 
 extern "C" {
 
-// scheme: 0 = weno5js, 1 = weno5z, 2 = crweno5, 3 = weno7js, 4 = hccs.
+// scheme: 0 = weno5js, 1 = weno5z, 2 = crweno5, 3 = weno7js, 4 = hccs,
+// 5 = hccs77, 6 = hccs78.
 // in: (nx,ny,nz); halos: (tile,ny,nz) with tile the scheme's bufferSize (3,
-// or 4 for weno7js and hccs);
+// or 4 for weno7js and the hccs family);
 // out: (nx+1,ny,nz).  Reconstruction runs along the fastest axis.
 int ref_reconstruct(int scheme, int upwind, int nx, int ny, int nz, const double *in,
                     const double *halo_l, const double *halo_r, double *out) {
@@ -159,6 +162,16 @@ int ref_reconstruct(int scheme, int upwind, int nx, int ny, int nz, const double
         s.interpolationBoundaryR(fin, fr, upwind, fout, tile);
     } else if (scheme == 4) {
         nuc3d::hccs s;
+        s.interpolationInner(fin, upwind, fout, tile);
+        s.interpolationBoundaryL(fin, fl, upwind, fout, tile);
+        s.interpolationBoundaryR(fin, fr, upwind, fout, tile);
+    } else if (scheme == 5) {
+        nuc3d::hccs77 s;
+        s.interpolationInner(fin, upwind, fout, tile);
+        s.interpolationBoundaryL(fin, fl, upwind, fout, tile);
+        s.interpolationBoundaryR(fin, fr, upwind, fout, tile);
+    } else if (scheme == 6) {
+        nuc3d::hccs78 s;
         s.interpolationInner(fin, upwind, fout, tile);
         s.interpolationBoundaryL(fin, fl, upwind, fout, tile);
         s.interpolationBoundaryR(fin, fr, upwind, fout, tile);

@@ -19,10 +19,11 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT / "oracle"))
 
-from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, WENO5JS, WENO5Z, WENO7, Box,  # noqa: E402
-                           Oracle, Reference)
+from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, HCCS77, HCCS78, WENO5JS, WENO5Z,  # noqa: E402
+                           WENO7, Box, Oracle, Reference)
 
-SCHEME_TAG = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr", WENO7: "w7", HCCS: "hc"}
+SCHEME_TAG = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr", WENO7: "w7", HCCS: "hc", HCCS77: "h77",
+              HCCS78: "h78"}
 
 
 def perturbed_tgv(box: Box, seed: int):
@@ -35,6 +36,10 @@ def perturbed_tgv(box: Box, seed: int):
 
 def main():
     R = Reference()
+    if sys.argv[1:] == ["hccs_siblings"]:  # only the hccs77 / hccs78 fixtures
+        hccs_sibling_fixtures(R)
+        print("fixtures written to", HERE)
+        return
     rng = np.random.default_rng(2024)
     out = {}
     # --- per-operator: reconstruction, CD6, RK stages -------------------
@@ -98,6 +103,7 @@ def main():
     spectra_fixture(R)
     forcing_fixture(R)
     hccs_fixtures(R)
+    hccs_sibling_fixtures(R)
     print("fixtures written to", HERE)
 
 
@@ -133,6 +139,40 @@ def hccs_fixtures(R):
                             rhs=np.stack(rhs), dt_local=np.array(dtl), q3=np.stack(qn), dt=dt,
                             res=res, shape=np.array(box.shape), mach=box.mach,
                             reynolds=box.reynolds, prandtl=box.prandtl)
+
+
+def hccs_sibling_fixtures(R):
+    """The reference's hccs77 (WENO7-Z blended into the 7th-order upwind
+    compact rows, a tridiagonal line system) and hccs78 (WENO7-Z blended with
+    the 8th-order central value, explicit): both directions on smooth and
+    rough lines, 4-wide halos; one RHS plus three steps, N-S and Euler."""
+    rng = np.random.default_rng(45)
+    shape = (5, 4, 20)
+    x = np.linspace(0.0, 2.0 * np.pi, shape[2], endpoint=False)
+    for sch in (HCCS77, HCCS78):
+        out = {}
+        for up in (1, -1):
+            for kind in ("smooth", "rough"):
+                if kind == "smooth":
+                    f = np.sin(x)[None, None, :] + 0.05 * rng.standard_normal(shape)
+                else:
+                    f = rng.standard_normal(shape) * np.exp(rng.standard_normal(shape))
+                hl = rng.standard_normal(shape[:2] + (4,))
+                hr = rng.standard_normal(shape[:2] + (4,))
+                tag = f"{kind}_{'p' if up > 0 else 'm'}"
+                out[f"rec_{tag}_in"], out[f"rec_{tag}_hl"], out[f"rec_{tag}_hr"] = f, hl, hr
+                out[f"rec_{tag}_out"] = R.reconstruct_field(sch, up, f, hl, hr)
+        np.savez_compressed(HERE / f"operators_{SCHEME_TAG[sch]}.npz", **out)
+        for ns in (True, False):
+            box = Box(16, 12, 10, scheme=(sch,) * 3, navier_stokes=ns, mach=0.3, reynolds=800.0,
+                      prandtl=0.71)
+            q = perturbed_tgv(box, 11 + sch)
+            rhs, dtl = R.rhs(box, q)
+            qn, dt, res = R.run_steps(box, 0.5, 3, q)
+            np.savez_compressed(HERE / f"step_{SCHEME_TAG[sch]}_{'ns' if ns else 'eu'}.npz",
+                                q0=np.stack(q), rhs=np.stack(rhs), dt_local=np.array(dtl),
+                                q3=np.stack(qn), dt=dt, res=res, shape=np.array(box.shape),
+                                mach=box.mach, reynolds=box.reynolds, prandtl=box.prandtl)
 
 
 def forcing_fixture(R):

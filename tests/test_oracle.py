@@ -10,8 +10,8 @@ import numpy as np
 import pytest
 
 from helpers import box_from_golden, golden
-from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, LF, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_WENOZ_BETA2, WENO5JS,
-                           WENO5Z, WENO7, Box, Oracle, Reference)
+from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, HCCS77, HCCS78, LF, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED,
+                           Q_WENOZ_BETA2, WENO5JS, WENO5Z, WENO7, Box, Oracle, Reference)
 
 TAGS = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr"}
 
@@ -277,6 +277,36 @@ def test_hccs_reconstruct_matches_reference_golden(O, kind, up):
 def test_hccs_rhs_and_steps_match_reference_golden(O, ns):
     z = golden(f"step_hc_{'ns' if ns else 'eu'}.npz")
     box = box_from_golden(z, HCCS, ns)
+    rhs, dtl = O.rhs(box, list(z["q0"]))
+    assert np.array_equal(np.stack(rhs), z["rhs"]) and dtl == float(z["dt_local"])
+    q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
+    assert np.array_equal(np.stack(q3), z["q3"])
+    assert np.array_equal(dt, z["dt"]) and np.array_equal(res, z["res"])
+
+
+SIBLING_TAGS = {HCCS77: "h77", HCCS78: "h78"}
+
+
+@pytest.mark.parametrize("scheme", [HCCS77, HCCS78])
+@pytest.mark.parametrize("kind", ["smooth", "rough"])
+@pytest.mark.parametrize("up", [1, -1])
+def test_hccs_siblings_reconstruct_match_reference_golden(O, scheme, kind, up):
+    """hccs77 (WENO7-Z blended into the 7th-order upwind compact rows, WENO7-Z
+    end faces and identity rows, the reference's Thomas sweep) and hccs78
+    (WENO7-Z blended with the 8th-order central value on faces 4..n-4,
+    WENO7-Z at the ends), eps 1e-20 and squares through pow."""
+    z = golden(f"operators_{SIBLING_TAGS[scheme]}.npz")
+    tag = f"{kind}_{'p' if up > 0 else 'm'}"
+    out = O.reconstruct_field(scheme, up, QUIRKS_REFERENCE, z[f"rec_{tag}_in"], z[f"rec_{tag}_hl"],
+                              z[f"rec_{tag}_hr"])
+    assert np.array_equal(out, z[f"rec_{tag}_out"])
+
+
+@pytest.mark.parametrize("scheme", [HCCS77, HCCS78])
+@pytest.mark.parametrize("ns", [True, False])
+def test_hccs_siblings_rhs_and_steps_match_reference_golden(O, scheme, ns):
+    z = golden(f"step_{SIBLING_TAGS[scheme]}_{'ns' if ns else 'eu'}.npz")
+    box = box_from_golden(z, scheme, ns)
     rhs, dtl = O.rhs(box, list(z["q0"]))
     assert np.array_equal(np.stack(rhs), z["rhs"]) and dtl == float(z["dt_local"])
     q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
