@@ -380,13 +380,14 @@ long long nuc3d_batch_launch_count(const nuc3d_batch *b) { return b ? b->eng->la
 int nuc3d_reconstruct(int scheme, int upwind, unsigned quirks, int nx, int ny, int nz,
                       const double *in, const double *hl, const double *hr, double *out,
                       void *stream) {
-    if (scheme < NUC3D_WENO5JS || scheme > NUC3D_HCCS)
+    if (scheme < NUC3D_WENO5JS || scheme > NUC3D_HCCS78)
         return fail(NUC3D_ERR_UNSUPPORTED, "weno error: no such scheme");
     if (upwind != 1 && upwind != -1) return fail(NUC3D_ERR_INVALID, "weno error: no such direction");
     if (nx < 8 || ny < 1 || nz < 1) return fail(NUC3D_ERR_INVALID, "need nx >= 8, ny, nz >= 1");
-    if ((scheme == NUC3D_CRWENO5 || scheme == NUC3D_HCCS) && nx > 4096)
-        return fail(NUC3D_ERR_INVALID, "crweno5 / hccs need nx <= 4096");
-    if (scheme == NUC3D_HCCS && nx < 9) return fail(NUC3D_ERR_INVALID, "hccs needs nx >= 9");
+    if ((scheme == NUC3D_CRWENO5 || scheme == NUC3D_HCCS || scheme == NUC3D_HCCS77) && nx > 4096)
+        return fail(NUC3D_ERR_INVALID, "crweno5 / hccs / hccs77 need nx <= 4096");
+    if ((scheme == NUC3D_HCCS || scheme == NUC3D_HCCS77) && nx < 9)
+        return fail(NUC3D_ERR_INVALID, "hccs / hccs77 need nx >= 9");
     if (!in || !hl || !hr || !out) return fail(NUC3D_ERR_INVALID, "null buffer");
     CK(op_reconstruct(scheme, upwind, quirks, nx, (long long)ny * nz, in, hl, hr, out,
                       static_cast<cudaStream_t>(stream)));

@@ -1,7 +1,10 @@
-// CRWENO5 and hccs directional sweeps, batched over boxes: one block per tile
-// of kCrTL lines of one box, one warp per (line, sign) tridiagonal system.  hccs (hccs.cpp) has the same bounded structure with 4-cell ends:
+// CRWENO5, hccs and hccs77 directional sweeps, batched over boxes: one block
+// per tile of kCrTL lines of one box, one warp per (line, sign) tridiagonal
+// system.  hccs (hccs.cpp) has the same bounded structure with 4-cell ends:
 // faces 0..3 and n-3..n explicit WENO7 (eps 1e-40), identity rows at faces 4
-// and n-4, hybrid compact rows in between (hc_row).
+// and n-4, hybrid compact rows in between (hc_row).  hccs77 (hccs77.cpp)
+// has that structure too, with WENO7-Z (eps 1e-20) at the ends and rows that
+// blend WENO7-Z into the 7th-order upwind compact row (h77_row).
 //
 // Reference system (crweno5.cpp:45-402, quirk bit QK_CRWENO_BOUNDED set): on
 // a line of n cells, faces 0..2 and n-2..n take explicit WENO5-JS values
@@ -150,7 +153,8 @@ template <typename B, int DIR, int SCH>
 __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
     k_crweno_lines(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items,
                    int in_slot, int accumulate, int nmax, int ms, int prim_mode) {
-    // SCH: SCHEME_CR (crweno5) or SCHEME_HC (hccs).  H: staged halo, explicit
+    // SCH: SCHEME_CR (crweno5), SCHEME_HC (hccs) or SCHEME_H77 (hccs77).  H:
+    // staged halo, explicit
     // faces per end and the first unknown face (3 for crweno5, 4 for hccs).
     constexpr int H = scheme_halo(SCH);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -205,7 +209,7 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
     const bool mixed = sizeof(B) == sizeof(float);
     // hccs lines are always bounded (the reference's form); crweno5 has the
     // periodic form when the quirk bit is cleared
-    const bool bounded = SCH == SCHEME_HC || (bp.quirks & QK_CRWENO_BOUNDED) != 0;
+    const bool bounded = SCH != SCHEME_CR || (bp.quirks & QK_CRWENO_BOUNDED) != 0;
     const int N = bounded ? n - (2 * H - 1) : n;  // unknowns of the system
     int P = 1;  // lanes per system
     while (P < kCrLanes && 2 * P <= N / 2) P *= 2;
@@ -317,13 +321,17 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                 // the sign (warp-uniform) only selects which cells feed a
                 // stencil ('+' reads upwind from the left, '-' from the right)
                 constexpr int dir = S == 0 ? 1 : -1;
-                // explicit face m: WENO5-JS (crweno5.cpp:425-837) or hccs's WENO7
-                // (hccs.cpp:538-980)
+                // explicit face m: WENO5-JS (crweno5.cpp:425-837), hccs's WENO7
+                // (hccs.cpp:538-980) or hccs77's WENO7-Z (hccs77.cpp:330-818)
                 auto js = [&](int m) -> B {
-                    if (SCH == SCHEME_HC) {
+                    if (SCH == SCHEME_HC || SCH == SCHEME_H77) {
                         const int c0 = S == 0 ? m - 4 : m + 3;
-                        return weno7_face_hc(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
-                                             F(c0 + 4 * dir), F(c0 + 5 * dir), F(c0 + 6 * dir));
+                        if (SCH == SCHEME_HC)
+                            return weno7_face_hc(F(c0), F(c0 + dir), F(c0 + 2 * dir),
+                                                 F(c0 + 3 * dir), F(c0 + 4 * dir), F(c0 + 5 * dir),
+                                                 F(c0 + 6 * dir));
+                        return weno7_face(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
+                                          F(c0 + 4 * dir), F(c0 + 5 * dir), F(c0 + 6 * dir));
                     }
                     const int c0 = S == 0 ? m - 3 : m + 2;
                     return weno5js_face(F(c0), F(c0 + dir), F(c0 + 2 * dir), F(c0 + 3 * dir),
@@ -349,11 +357,14 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                     did1 = shfl(v, 2 * H + 1);
                 }
                 if (act) {
-                    // window w[k] = F(i - 2 + k) of the current row's cell i (face i + 1)
+                    // window w[k] = F(i - WO + k) of the current row's cell i (face
+                    // i + 1): cells i-2..i+3 for the 5-cell rows, i-3..i+4 for
+                    // hccs77's 7-cell rows
+                    constexpr int WN = SCH == SCHEME_H77 ? 8 : 6, WO = SCH == SCHEME_H77 ? 3 : 2;
                     int i = bounded ? r0 + H - 1 : r0 - 1;
-                    B w[6];
+                    B w[WN];
     #pragma unroll
-                    for (int k = 0; k < 6; ++k) w[k] = F(i - 2 + k);
+                    for (int k = 0; k < WN; ++k) w[k] = F(i - WO + k);
                     // row r of the system; `ends`: r may be a bounded system's
                     // first or last row (identity rows)
                     auto gen = [&](int r, bool ends, B &a, B &b, B &c, B &d) {
@@ -367,7 +378,12 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                             // with the off-diagonals swapped (crweno5.cpp:335-338)
                             constexpr bool m = S != 0;
                             B lo, hi;
-                            if (SCH == SCHEME_HC)
+                            if (SCH == SCHEME_H77)
+                                // '+': cells i-3..i+3 = w[0..6]; '-': cells i+4..i-2 = w[7..1]
+                                // (hccs77.cpp:282-291 swaps the couplings alike)
+                                h77_row(w[m ? 7 : 0], w[m ? 6 : 1], w[m ? 5 : 2], w[m ? 4 : 3],
+                                        w[m ? 3 : 4], w[m ? 2 : 5], w[m ? 1 : 6], lo, b, hi, d);
+                            else if (SCH == SCHEME_HC)
                                 hc_row(m ? w[5] : w[0], m ? w[4] : w[1], m ? w[3] : w[2],
                                        m ? w[2] : w[3], m ? w[1] : w[4], lo, b, hi, d);
                             else
@@ -379,9 +395,9 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                     };
                     auto advance = [&]() {
     #pragma unroll
-                        for (int k = 0; k < 5; ++k) w[k] = w[k + 1];
+                        for (int k = 0; k < WN - 1; ++k) w[k] = w[k + 1];
                         ++i;
-                        w[5] = F(i + 3);
+                        w[WN - 1] = F(i + WN - 1 - WO);
                     };
                     B a0, b0, c0, d0;
                     gen(r0, true, a0, b0, c0, d0);
@@ -553,6 +569,8 @@ static cudaError_t prepare_t() {
 cudaError_t prepare_crweno_kernels(bool mixed) {
     cudaError_t e = mixed ? prepare_t<float, SCHEME_CR>() : prepare_t<double, SCHEME_CR>();
     if (e == cudaSuccess) e = mixed ? prepare_t<float, SCHEME_HC>() : prepare_t<double, SCHEME_HC>();
+    if (e == cudaSuccess)
+        e = mixed ? prepare_t<float, SCHEME_H77>() : prepare_t<double, SCHEME_H77>();
     return e;
 }
 
@@ -580,6 +598,9 @@ cudaError_t launch_crweno(int sch, int dir, const BoxDev *boxes, const WorkItem 
     if (sch == SCHEME_HC)
         launch_t<B, SCHEME_HC>(dir, boxes, items, nitems, in_slot, accumulate, nmax, ms, prim_mode,
                                smem, st);
+    else if (sch == SCHEME_H77)
+        launch_t<B, SCHEME_H77>(dir, boxes, items, nitems, in_slot, accumulate, nmax, ms,
+                                prim_mode, smem, st);
     else
         launch_t<B, SCHEME_CR>(dir, boxes, items, nitems, in_slot, accumulate, nmax, ms, prim_mode,
                                smem, st);

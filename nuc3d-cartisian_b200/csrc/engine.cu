@@ -126,15 +126,15 @@ int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
     const int n[3] = {d.nx, d.ny, d.nz};
     for (int i = 0; i < 3; ++i) {
         if (n[i] < 8) return bad(NUC3D_ERR_INVALID, "every box extent must be >= 8 cells");
-        if (d.scheme[i] < NUC3D_WENO5JS || d.scheme[i] > NUC3D_HCCS)
+        if (d.scheme[i] < NUC3D_WENO5JS || d.scheme[i] > NUC3D_HCCS78)
             return bad(NUC3D_ERR_UNSUPPORTED, "unknown reconstruction scheme");
     }
     for (int i = 0; i < 3; ++i)
-        if ((d.scheme[i] == NUC3D_CRWENO5 || d.scheme[i] == NUC3D_HCCS) && n[i] > kCrMaxCells)
-            return bad(NUC3D_ERR_UNSUPPORTED, "CRWENO5 / hccs lines are limited to 512 cells");
+        if (line_slot(d.scheme[i]) >= 0 && n[i] > kCrMaxCells)
+            return bad(NUC3D_ERR_UNSUPPORTED, "CRWENO5 / hccs / hccs77 lines are limited to 512 cells");
     for (int i = 0; i < 3; ++i)
-        if (d.scheme[i] == NUC3D_HCCS && n[i] < 9)
-            return bad(NUC3D_ERR_INVALID, "hccs lines need at least 9 cells");
+        if ((d.scheme[i] == NUC3D_HCCS || d.scheme[i] == NUC3D_HCCS77) && n[i] < 9)
+            return bad(NUC3D_ERR_INVALID, "hccs / hccs77 lines need at least 9 cells");
     if ((long long)d.nx * d.ny * d.nz > (1LL << 31)) return bad(NUC3D_ERR_INVALID, "box larger than 2^31 cells");
     if (!(d.lx > 0 && d.ly > 0 && d.lz > 0)) return bad(NUC3D_ERR_INVALID, "box lengths must be > 0");
     if (d.pde_model != NUC3D_EULER3D && d.pde_model != NUC3D_NAVIERSTOKES3D)
@@ -415,9 +415,9 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));
     const bool mixed = precision_ == NUC3D_MIXED;
     std::vector<BoxDev> table(boxes_.size());
-    std::vector<WorkItem> prim, st25[3], inv[kSchemes][3][kInvTileClasses], cr[2][3];
+    std::vector<WorkItem> prim, st25[3], inv[kSchemes][3][kInvTileClasses], cr[kLineSchemes][3];
     const int crtl = crweno_tile_lines();
-    for (int c = 0; c < 2; ++c)
+    for (int c = 0; c < kLineSchemes; ++c)
         for (int d = 0; d < 3; ++d) cr_nmax_[c][d] = cr_ms_[c][d] = 0;
     any_visc_ = false;
     nactive_ = 0;
@@ -442,9 +442,9 @@ int Engine::rebuild() {
                     for (int x = 0; x < ceil_div(p.n[0], kT25X); ++x) st25[v].push_back({id, x, y, z});
         for (int d = 0; d < 3; ++d) {
             int s = p.scheme[d];
-            if (s == SCHEME_CR || s == SCHEME_HC) {
-                const int c = s == SCHEME_HC ? 1 : 0;
-                const bool bounded = s == SCHEME_HC || (p.quirks & QK_CRWENO_BOUNDED) != 0;
+            if (line_slot(s) >= 0) {
+                const int c = line_slot(s);
+                const bool bounded = s != SCHEME_CR || (p.quirks & QK_CRWENO_BOUNDED) != 0;
                 cr_nmax_[c][d] = std::max(cr_nmax_[c][d], p.n[d]);
                 cr_ms_[c][d] = std::max(cr_ms_[c][d], crweno_segment_rows(s, p.n[d], bounded));
                 auto &L = cr[c][d];
@@ -490,7 +490,7 @@ int Engine::rebuild() {
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d)
             for (int tc = 0; tc < kInvTileClasses; ++tc) append(inv[s][d][tc], r_inv_[s][d][tc]);
-    for (int c = 0; c < 2; ++c)
+    for (int c = 0; c < kLineSchemes; ++c)
         for (int d = 0; d < 3; ++d) append(cr[c][d], r_cr_[c][d]);
     if ((int)boxes_.size() > d_boxes_cap_) {
         if (d_boxes_) ECK(cudaFreeAsync(d_boxes_, stream_));
@@ -517,7 +517,7 @@ int Engine::rebuild() {
     int per_stage = (any_visc_ && r_25d_[0].n > 0) + (r_25d_[0].n > 0);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d][0].n > 0;
-    for (int c = 0; c < 2; ++c)
+    for (int c = 0; c < kLineSchemes; ++c)
         for (int d = 0; d < 3; ++d) per_stage += r_cr_[c][d].n > 0;
     launches_per_step_ = 3 * per_stage + 3;  // + clear_eig, dt, residual
     for (const EngineBox &b : boxes_)
@@ -584,8 +584,8 @@ int Engine::enqueue_step_t(cudaStream_t st) {
             for (int s = 0; s < kSchemes; ++s)
                 ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + inv_range(s, d).off,
                                         inv_range(s, d).n, in, d > 0, prim_mode, st)));
-            for (int c = 0; c < 2; ++c)
-                ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_,
+            for (int c = 0; c < kLineSchemes; ++c)
+                ECK((launch_crweno<B>(kLineScheme[c], d, d_boxes_,
                                       it + r_cr_[c][d].off, r_cr_[c][d].n, in, d > 0,
                                       cr_nmax_[c][d], cr_ms_[c][d], prim_mode, st)));
             return NUC3D_OK;
@@ -866,8 +866,8 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
         for (int s = 0; s < kSchemes; ++s)
             ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + inv_range(s, d).off,
                                     inv_range(s, d).n, 0, d > 0, 0, stream_)));
-        for (int c = 0; c < 2; ++c)
-            ECK((launch_crweno<B>(c ? SCHEME_HC : SCHEME_CR, d, d_boxes_, it + r_cr_[c][d].off,
+        for (int c = 0; c < kLineSchemes; ++c)
+            ECK((launch_crweno<B>(kLineScheme[c], d, d_boxes_, it + r_cr_[c][d].off,
                                   r_cr_[c][d].n, 0, d > 0, cr_nmax_[c][d], cr_ms_[c][d], 0,
                                   stream_)));
     }

@@ -73,7 +73,8 @@ public:
     // autotuned sweep variant (tile length and run length, kInvTileCells /
     // kInvRunLen) per [scheme JS/Z/-/W7][dir] (-1: not tuned yet) and the
     // measured milliseconds per launch of each variant
-    int inv_variant[kSchemes][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
+    int inv_variant[kSchemes][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1},
+                                    {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
     double inv_tune_ms[kSchemes][3][kInvVariants] = {};
     // autotuned pencil depth of the 2.5-D stencil kernels: index into
     // kPencilDepths (-1: not tuned yet), the measured milliseconds of one
@@ -120,7 +121,7 @@ private:
         int n = 0;
     };
     Range r_prim_;
-    Range r_inv_[kSchemes][3][kInvTileClasses];  // [scheme JS/Z/-/W7][dir][32/64-cell tiles]
+    Range r_inv_[kSchemes][3][kInvTileClasses];  // [scheme id][dir][32/64-cell tiles]
     // the work list of the variant the autotuner chose (32-cell tiles before)
     const Range &inv_range(int s, int d) const {
         return r_inv_[s][d][inv_variant[s][d] < 0 ? 0 : inv_tile_class(inv_variant[s][d])];
@@ -134,10 +135,11 @@ private:
     // tiles start: only the 32-cell tiles run there, which keeps every
     // variant (and a box alone or in any batch) bitwise the same.
     bool mixed_tiles_only32() const { return precision_ == NUC3D_MIXED; }
-    // line-solve tiles per [scheme: 0 crweno5, 1 hccs][dir], with the longest
-    // line and the rows per lane that size each launch's shared memory
-    Range r_cr_[2][3];
-    int cr_nmax_[2][3] = {}, cr_ms_[2][3] = {};
+    // line-solve tiles per [line scheme: 0 crweno5, 1 hccs, 2 hccs77][dir],
+    // with the longest line and the rows per lane that size each launch's
+    // shared memory
+    Range r_cr_[kLineSchemes][3];
+    int cr_nmax_[kLineSchemes][3] = {}, cr_ms_[kLineSchemes][3] = {};
     int launches_per_step_ = 0;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;

@@ -18,14 +18,20 @@ enum : unsigned {
     QK_CRWENO_BOUNDED = 0x10u,
 };
 
-enum : int { SCHEME_JS = 0, SCHEME_Z = 1, SCHEME_CR = 2, SCHEME_W7 = 3, SCHEME_HC = 4 };
+enum : int {
+    SCHEME_JS = 0,
+    SCHEME_Z = 1,
+    SCHEME_CR = 2,
+    SCHEME_W7 = 3,
+    SCHEME_HC = 4,
+    SCHEME_H77 = 5,
+    SCHEME_H78 = 6
+};
 
 // reconstruction stencil half-width (the reference's bufferSize,
-// fieldOperator.cpp:128-175): 4 cells for weno7js and hccs, 3 for the WENO5
-// family
-__host__ __device__ constexpr int scheme_halo(int scheme) {
-    return (scheme == SCHEME_W7 || scheme == SCHEME_HC) ? 4 : 3;
-}
+// fieldOperator.cpp:128-175): 4 cells for weno7js and the hccs family, 3 for
+// the WENO5 family
+__host__ __device__ constexpr int scheme_halo(int scheme) { return scheme >= SCHEME_W7 ? 4 : 3; }
 enum : int { VISC_SUTHERLAND = 0, VISC_CONSTANT = 1, VISC_POWERLAW = 2 };
 enum : int { RIEMANN_LF = 0, RIEMANN_AUSM = 1, RIEMANN_AUSMP = 2 };
 
@@ -111,6 +117,7 @@ __device__ __forceinline__ double add_(double a, double b) { return __dadd_rn(a,
 __device__ __forceinline__ float add_(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double sub_(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float sub_(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double div_(double a, double b) { return __ddiv_rn(a, b); }
 
 // second difference f0 - 2 f1 + f2
 template <typename B>
@@ -589,6 +596,109 @@ __device__ __forceinline__ float weno7_face_eps(float f0, float f1, float f2, fl
     float num = fma_(al[3], r[3], fma_(al[2], r[2], fma_(al[1], r[1], mul_(al[0], r[0]))));
     float den = add_(add_(add_(al[0], al[1]), al[2]), al[3]);
     return fma_(mul_(num, frcp_fast(den)), 1.0f / 12.0f, f3);
+}
+
+// ---- hccs77 / hccs78 (hccs77.cpp, hccs78.cpp) ----
+// Their WENO7-Z face (eps = 1e-20, squares through pow with their member
+// p = 2) and the unnormalised weights' sum S = sum alpha, from which both
+// blend with theta = 1/(1 + (S - 1)^2).  FP64 forms S and theta with the
+// reference's own operations (a division per weight, x*x for pow(x, 2), the
+// sums left to right; the indicators come from weno7_parts in the
+// reference's order), so theta, and hccs77's switch on theta > 1/2, come out
+// as the reference's.
+__device__ __forceinline__ double weno7z_face_sum(double f0, double f1, double f2, double f3,
+                                                  double f4, double f5, double f6, double &theta) {
+    double is[4], q[4];
+    weno7_parts(f0, f1, f2, f3, f4, f5, f6, is, q);
+    const double ss = 1.0e-20;
+    const double tau = fabs(sub_(is[0], is[3]));
+    const double c[4] = {K7::C0, K7::C1, K7::C2, K7::C3};
+    double a[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double r = div_(tau, add_(ss, is[k]));
+        a[k] = mul_(c[k], add_(1.0, mul_(r, r)));
+    }
+    const double sa = add_(add_(add_(a[0], a[1]), a[2]), a[3]);
+    const double x = sub_(sa, 1.0);
+    theta = div_(1.0, add_(1.0, mul_(x, x)));
+    const double num = fma_(a[3], q[3], fma_(a[2], q[2], fma_(a[1], q[1], mul_(a[0], q[0]))));
+    return div_(num, sa);
+}
+// FP32 (mixed path): the difference-form WENO7-Z of weno7_face_eps and its
+// weights' sum
+__device__ __forceinline__ float weno7z_face_sum(float f0, float f1, float f2, float f3, float f4,
+                                                 float f5, float f6, float &theta) {
+    float d1 = sub_(f1, f0), d2 = sub_(f2, f1), d3 = sub_(f3, f2);
+    float d4 = sub_(f4, f3), d5 = sub_(f5, f4), d6 = sub_(f6, f5);
+    float s2 = sub_(d2, d1), s3 = sub_(d3, d2), s4 = sub_(d4, d3), s5 = sub_(d5, d4),
+          s6 = sub_(d6, d5);
+    float is[4], r[4];
+    is[0] = w7_beta(d2, s2, s3, -160.0f, 880.0f, 547.0f, -1854.0f, 2107.0f);
+    is[1] = w7_beta(d3, s3, s4, 80.0f, 160.0f, 267.0f, -494.0f, 547.0f);
+    is[2] = w7_beta(d4, s4, s5, -160.0f, -80.0f, 547.0f, -494.0f, 267.0f);
+    is[3] = w7_beta(d5, s5, s6, -880.0f, 160.0f, 2107.0f, -1854.0f, 547.0f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) is[k] = fmaxf(is[k], 0.0f);
+    r[0] = fma_(3.0f, d1, fma_(-10.0f, d2, mul_(13.0f, d3)));
+    r[1] = fma_(-1.0f, d2, fma_(4.0f, d3, mul_(3.0f, d4)));
+    r[2] = fma_(-1.0f, d5, fma_(6.0f, d4, d3));
+    r[3] = fma_(9.0f, d4, fma_(-4.0f, d5, d6));
+    const float ss = 1.0e-20f, cap = 1.0e15f;
+    const float c[4] = {float(K7::C0), float(K7::C1), float(K7::C2), float(K7::C3)};
+    float tau = fabsf(sub_(is[0], is[3]));
+    float al[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float t = fminf(mul_(tau, frcp_fast(add_(ss, is[k]))), cap);
+        al[k] = mul_(c[k], fma_(t, t, 1.0f));
+    }
+    float num = fma_(al[3], r[3], fma_(al[2], r[2], fma_(al[1], r[1], mul_(al[0], r[0]))));
+    float den = add_(add_(add_(al[0], al[1]), al[2]), al[3]);
+    const float x = sub_(den, 1.0f);
+    theta = frcp_fast(fma_(x, x, 1.0f));  // 0 once x^2 overflows
+    return fma_(mul_(num, frcp_fast(den)), 1.0f / 12.0f, f3);
+}
+
+// hccs78's face on faces 4..n-4 (hccs78.cpp:81-139, '-' :171-229): the
+// WENO7-Z face of the upwind-oriented stencil f0..f6 blended with the
+// 8th-order central value of the cells c0..c7 around the face (m-4..m+3;
+// the same expression for both signs): (1 - theta) W7 + theta q8.
+template <typename B>
+__device__ __forceinline__ B hccs78_face(B f0, B f1, B f2, B f3, B f4, B f5, B f6, B c0, B c1, B c2,
+                                         B c3, B c4, B c5, B c6, B c7) {
+    B theta;
+    const B w7 = weno7z_face_sum(f0, f1, f2, f3, f4, f5, f6, theta);
+    const B q8 = mul_(add_(add_(add_(mul_(B(-3), add_(c7, c0)), mul_(B(29), add_(c6, c1))),
+                                mul_(B(-139), add_(c5, c2))),
+                           mul_(B(533), add_(c4, c3))),
+                      B(1.0 / 840.0));
+    return add_(mul_(sub_(B(1), theta), w7), mul_(theta, q8));
+}
+
+// One row of hccs77 (hccs77.cpp:79-162 for '+', :246-305 for '-'), from the
+// upwind-oriented 7-cell stencil g0..g6 of the row's cell i ('+': cells
+// i-3..i+3): theta > 1/2 gives the linear upwind compact row (2/7, 4/7, 1/7
+// | q7), otherwise (2/7 theta, 1 - 3/7 theta, 1/7 theta | (1 - theta) W7 +
+// theta q7); lo couples the upwind-side face, hi the downwind side.
+template <typename B>
+__device__ __forceinline__ void h77_row(B g0, B g1, B g2, B g3, B g4, B g5, B g6, B &lo, B &b,
+                                        B &hi, B &d) {
+    B theta;
+    const B w7 = weno7z_face_sum(g0, g1, g2, g3, g4, g5, g6, theta);
+    const B q7 = mul_(fma_(B(4), g5, fma_(B(159), g4, fma_(B(239), g3, fma_(B(19), g2, -g1)))),
+                      B(1.0 / 420.0));
+    if (theta > B(0.5)) {
+        lo = B(2.0 / 7.0);
+        b = B(4.0 / 7.0);
+        hi = B(1.0 / 7.0);
+        d = q7;
+    } else {
+        lo = mul_(B(2.0 / 7.0), theta);
+        b = add_(B(1), mul_(B(4.0 / 7.0 - 1.0), theta));
+        hi = mul_(B(1.0 / 7.0), theta);
+        d = add_(mul_(w7, sub_(B(1), theta)), mul_(q7, theta));
+    }
 }
 
 // One hybrid row of hccs (hccs.cpp:138-185; '-' mirrored, :375-420), scaled

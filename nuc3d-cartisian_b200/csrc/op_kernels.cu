@@ -46,9 +46,11 @@ __global__ void k_op_weno(int upwind, unsigned quirks, int nx, long long lines, 
                                 : weno5js_face(f[0], f[1], f[2], f[3], f[4]);
 }
 
-// One thread per face of weno7js (weno7js.cpp:17-824): face m reads cells
-// m-4..m+2 ('+') or m+3..m-3 ('-'); the boundary faces use the same
-// expression on halo cells.
+// One thread per face of weno7js (weno7js.cpp:17-824) or hccs78
+// (hccs78.cpp:44-732): face m reads cells m-4..m+2 ('+') or m+3..m-3 ('-');
+// the boundary faces use the same expression on halo cells.  hccs78 blends
+// faces 4..nx-4 with the central value of cells m-4..m+3.
+template <bool H78>
 __global__ void k_op_weno7(int upwind, int nx, long long lines, const double *in,
                            const double *hl, const double *hr, double *out) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -61,6 +63,14 @@ __global__ void k_op_weno7(int upwind, int nx, long long lines, const double *in
     for (int k = 0; k < 7; ++k)
         f[k] = upwind > 0 ? line_at<4>(in, hl, hr, nx, line, m - 4 + k)
                           : line_at<4>(in, hl, hr, nx, line, m + 3 - k);
+    if (H78 && m >= 4 && m <= nx - 4) {
+        double c[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) c[k] = line_at<4>(in, hl, hr, nx, line, m - 4 + k);
+        out[t] = hccs78_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6], c[0], c[1], c[2], c[3],
+                             c[4], c[5], c[6], c[7]);
+        return;
+    }
     out[t] = weno7_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6]);
 }
 
@@ -127,19 +137,26 @@ __global__ void k_op_crweno(int upwind, int nx, long long lines, const double *i
 }
 
 // One thread per line: hccs (hccs.cpp): faces 0..3 and nx-3..nx explicit
-// WENO7 with hccs's eps (:538-980), the system of faces 4..nx-4 (identity
-// rows at its ends, hybrid rows between, :54-245 / :272-471) by a Thomas
-// sweep.  scratch holds 2*nx values per line, interleaved as in
-// k_op_crweno.
+// hccs (hccs.cpp) and hccs77 (hccs77.cpp): WENO7 with hccs's eps
+// (:538-980) or hccs77's WENO7-Z (:330-818) at the ends, the system of faces
+// 4..nx-4 (identity rows at its ends, hybrid rows between; hccs.cpp:54-245
+// / :272-471, hccs77.cpp:44-305) by a Thomas sweep.  scratch holds 2*nx
+// values per line, interleaved as in k_op_crweno.
+template <int SCH>
 __global__ void k_op_hccs(int upwind, int nx, long long lines, const double *in,
                           const double *hl, const double *hr, double *out, double *scratch) {
     long long line = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (line >= lines) return;
     auto F = [&](int c) { return line_at<4>(in, hl, hr, nx, line, c); };
+    auto w7face = [&](double f0, double f1, double f2, double f3, double f4, double f5,
+                      double f6) {
+        return SCH == SCHEME_H77 ? weno7_face(f0, f1, f2, f3, f4, f5, f6)
+                                 : weno7_face_hc(f0, f1, f2, f3, f4, f5, f6);
+    };
     auto w7 = [&](int m) {
         if (upwind > 0)
-            return weno7_face_hc(F(m - 4), F(m - 3), F(m - 2), F(m - 1), F(m), F(m + 1), F(m + 2));
-        return weno7_face_hc(F(m + 3), F(m + 2), F(m + 1), F(m), F(m - 1), F(m - 2), F(m - 3));
+            return w7face(F(m - 4), F(m - 3), F(m - 2), F(m - 1), F(m), F(m + 1), F(m + 2));
+        return w7face(F(m + 3), F(m + 2), F(m + 1), F(m), F(m - 1), F(m - 2), F(m - 3));
     };
     double *o = out + (long long)(nx + 1) * line;
     for (int m = 0; m <= 3; ++m) o[m] = w7(m);
@@ -157,10 +174,18 @@ __global__ void k_op_hccs(int upwind, int nx, long long lines, const double *in,
         } else {
             const int i = r + 3;
             double lo, hi;
-            if (upwind > 0)
+            if (SCH == SCHEME_H77) {
+                if (upwind > 0)
+                    h77_row(F(i - 3), F(i - 2), F(i - 1), F(i), F(i + 1), F(i + 2), F(i + 3), lo, b,
+                            hi, d);
+                else
+                    h77_row(F(i + 4), F(i + 3), F(i + 2), F(i + 1), F(i), F(i - 1), F(i - 2), lo, b,
+                            hi, d);
+            } else if (upwind > 0) {
                 hc_row(F(i - 2), F(i - 1), F(i), F(i + 1), F(i + 2), lo, b, hi, d);
-            else
+            } else {
                 hc_row(F(i + 3), F(i + 2), F(i + 1), F(i), F(i - 1), lo, b, hi, d);
+            }
             if (upwind > 0) { a = lo; c = hi; } else { c = lo; a = hi; }
         }
         double den = b - cp * a;
@@ -209,14 +234,16 @@ __global__ void k_op_rk3(int stage, long long n, double dt, RK5 rk) {
 cudaError_t op_reconstruct(int scheme, int upwind, unsigned quirks, int nx, long long lines,
                            const double *in, const double *hl, const double *hr, double *out,
                            cudaStream_t st) {
-    if (scheme == SCHEME_CR || scheme == SCHEME_HC) {
+    if (scheme == SCHEME_CR || scheme == SCHEME_HC || scheme == SCHEME_H77) {
         double *scratch = nullptr;
         size_t bytes = sizeof(double) * 2 * (size_t)nx * (size_t)lines;
         cudaError_t e = cudaMallocAsync(&scratch, bytes, st);
         if (e != cudaSuccess) return e;
         unsigned grid = (unsigned)((lines + 127) / 128);
         if (scheme == SCHEME_HC)
-            k_op_hccs<<<grid, 128, 0, st>>>(upwind, nx, lines, in, hl, hr, out, scratch);
+            k_op_hccs<SCHEME_HC><<<grid, 128, 0, st>>>(upwind, nx, lines, in, hl, hr, out, scratch);
+        else if (scheme == SCHEME_H77)
+            k_op_hccs<SCHEME_H77><<<grid, 128, 0, st>>>(upwind, nx, lines, in, hl, hr, out, scratch);
         else
             k_op_crweno<<<grid, 128, 0, st>>>(upwind, nx, lines, in, hl, hr, out, scratch);
         e = cudaGetLastError();
@@ -226,7 +253,9 @@ cudaError_t op_reconstruct(int scheme, int upwind, unsigned quirks, int nx, long
     long long total = (long long)(nx + 1) * lines;
     unsigned grid = (unsigned)((total + 255) / 256);
     if (scheme == SCHEME_W7)
-        k_op_weno7<<<grid, 256, 0, st>>>(upwind, nx, lines, in, hl, hr, out);
+        k_op_weno7<false><<<grid, 256, 0, st>>>(upwind, nx, lines, in, hl, hr, out);
+    else if (scheme == SCHEME_H78)
+        k_op_weno7<true><<<grid, 256, 0, st>>>(upwind, nx, lines, in, hl, hr, out);
     else if (scheme == SCHEME_Z)
         k_op_weno<SCHEME_Z><<<grid, 256, 0, st>>>(upwind, quirks, nx, lines, in, hl, hr, out);
     else

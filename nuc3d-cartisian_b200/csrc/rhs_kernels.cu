@@ -348,29 +348,52 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
             racc[k] = (accumulate && line_ok && gc < n) ? rbase[gidx(l, gc) + e * np] : B(0);
         }
         B Fh[R + 1];
-        if constexpr (SCHEME == SCHEME_W7) {
+        if constexpr (SCHEME == SCHEME_W7 || SCHEME == SCHEME_H78) {
             // face m: '+' reads positions m..m+6 (cells m-4..m+2), '-' reads
-            // m+7..m+1 (cells m+3..m-3)
-            B f[7];
+            // m+7..m+1 (cells m+3..m-3).  hccs78 blends faces 4..n-4 with the
+            // central value of cells m-4..m+3 (positions m..m+7): its '+'
+            // window carries position m+7 in f[7], its '-' window position m.
+            constexpr bool h78 = SCHEME == SCHEME_H78;
+            auto blended = [&](int k) {
+                const int gm = c0 + m0 + k;
+                return h78 && gm >= 4 && gm <= n - 4;
+            };
+            B f[8];
 #pragma unroll
             for (int j = 0; j < 7; ++j) f[j] = sF[G::sf(e, l, m0 + j)];
+            if (h78) f[7] = sF[G::sf(e, l, m0 + 7)];
 #pragma unroll
             for (int k = 0; k <= R; ++k) {
                 if (k == R && !last) break;
-                Fh[k] = weno7_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6]);
+                if (blended(k))
+                    Fh[k] = hccs78_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[0], f[1], f[2],
+                                        f[3], f[4], f[5], f[6], f[7]);
+                else
+                    Fh[k] = weno7_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6]);
                 if (k < R) {
 #pragma unroll
                     for (int j = 0; j < 6; ++j) f[j] = f[j + 1];
-                    f[6] = sF[G::sf(e, l, m0 + k + 7)];
+                    if (h78) {
+                        f[6] = f[7];
+                        f[7] = sF[G::sf(e, l, m0 + k + 8)];
+                    } else {
+                        f[6] = sF[G::sf(e, l, m0 + k + 7)];
+                    }
                 }
             }
 #pragma unroll
             for (int j = 0; j < 7; ++j) f[j] = sF[G::sf(5 + e, l, m0 + 7 - j)];
+            if (h78) f[7] = sF[G::sf(5 + e, l, m0)];
 #pragma unroll
             for (int k = 0; k <= R; ++k) {
                 if (k == R && !last) break;
-                Fh[k] = add_(Fh[k], weno7_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6]));
+                if (blended(k))
+                    Fh[k] = add_(Fh[k], hccs78_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7],
+                                                    f[6], f[5], f[4], f[3], f[2], f[1], f[0]));
+                else
+                    Fh[k] = add_(Fh[k], weno7_face(f[0], f[1], f[2], f[3], f[4], f[5], f[6]));
                 if (k < R) {
+                    if (h78) f[7] = f[6];  // position m+1 of the next face
 #pragma unroll
                     for (int j = 6; j > 0; --j) f[j] = f[j - 1];
                     f[0] = (m0 + k + 8 < NF) ? sF[G::sf(5 + e, l, m0 + k + 8)] : B(0);
@@ -564,18 +587,19 @@ __global__ void __launch_bounds__(InvGeom<DIR, B, RUN, 3, TCX>::NT, InvGeom<DIR,
                int accumulate, int prim_mode) {
     inviscid_body<SCHEME, DIR, B, RUN, TCX>(boxes, items, in_slot, accumulate, prim_mode);
 }
-template <int DIR, typename B, int RUN, int TCX>
+// WENO7 and hccs78 (4-cell halos)
+template <int SCHEME, int DIR, typename B, int RUN, int TCX>
 __global__ void __launch_bounds__(InvGeom<DIR, B, RUN, 4, TCX>::NT)
     k_inviscid_w7(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items,
                   int in_slot, int accumulate, int prim_mode) {
-    inviscid_body<SCHEME_W7, DIR, B, RUN, TCX>(boxes, items, in_slot, accumulate, prim_mode);
+    inviscid_body<SCHEME, DIR, B, RUN, TCX>(boxes, items, in_slot, accumulate, prim_mode);
 }
 
 using InvKernel = void (*)(const BoxDev *, const WorkItem *, int, int, int);
 template <int SCHEME, int DIR, typename B, int RUN, int TCX>
 static InvKernel inv_kernel() {
-    if constexpr (SCHEME == SCHEME_W7)
-        return k_inviscid_w7<DIR, B, RUN, TCX>;
+    if constexpr (SCHEME == SCHEME_W7 || SCHEME == SCHEME_H78)
+        return k_inviscid_w7<SCHEME, DIR, B, RUN, TCX>;
     else
         return k_inviscid<SCHEME, DIR, B, RUN, TCX>;
 }
@@ -636,6 +660,11 @@ cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxe
         if (dir == 1) return launch_v<SCHEME_W7, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
         return launch_v<SCHEME_W7, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
     }
+    if (scheme == SCHEME_H78) {
+        if (dir == 0) return launch_v<SCHEME_H78, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        if (dir == 1) return launch_v<SCHEME_H78, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        return launch_v<SCHEME_H78, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+    }
     return cudaErrorInvalidValue;
 }
 
@@ -656,11 +685,12 @@ static cudaError_t prepare_runs() {
 }
 template <typename B>
 static cudaError_t prepare_all() {
-    cudaError_t e[9] = {prepare_runs<SCHEME_JS, 0, B>(), prepare_runs<SCHEME_JS, 1, B>(),
-                        prepare_runs<SCHEME_JS, 2, B>(), prepare_runs<SCHEME_Z, 0, B>(),
-                        prepare_runs<SCHEME_Z, 1, B>(), prepare_runs<SCHEME_Z, 2, B>(),
-                        prepare_runs<SCHEME_W7, 0, B>(), prepare_runs<SCHEME_W7, 1, B>(),
-                        prepare_runs<SCHEME_W7, 2, B>()};
+    cudaError_t e[12] = {prepare_runs<SCHEME_JS, 0, B>(), prepare_runs<SCHEME_JS, 1, B>(),
+                         prepare_runs<SCHEME_JS, 2, B>(), prepare_runs<SCHEME_Z, 0, B>(),
+                         prepare_runs<SCHEME_Z, 1, B>(), prepare_runs<SCHEME_Z, 2, B>(),
+                         prepare_runs<SCHEME_W7, 0, B>(), prepare_runs<SCHEME_W7, 1, B>(),
+                         prepare_runs<SCHEME_W7, 2, B>(), prepare_runs<SCHEME_H78, 0, B>(),
+                         prepare_runs<SCHEME_H78, 1, B>(), prepare_runs<SCHEME_H78, 2, B>()};
     for (cudaError_t x : e)
         if (x != cudaSuccess) return x;
     return cudaSuccess;

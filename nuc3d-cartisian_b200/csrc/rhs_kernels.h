@@ -121,8 +121,15 @@ constexpr int kInvRunLen[kInvVariants] = {1, 2, 4, 2, 4};
 constexpr int kInvTileClasses = 2;  // 32- and 64-cell tiles
 constexpr int inv_tile_class(int variant) { return variant >= 3 ? 1 : 0; }
 // scheme slots of the per-scheme sweep tables (indexed by scheme id; the
-// CRWENO5 slot stays empty, its lines run in launch_crweno)
-constexpr int kSchemes = 4;
+// line-solve schemes' slots (CRWENO5, hccs, hccs77) stay empty, their lines
+// run in launch_crweno)
+constexpr int kSchemes = 7;
+// the line-solve schemes, in the order of the engine's line tables
+constexpr int kLineSchemes = 3;
+constexpr int kLineScheme[kLineSchemes] = {SCHEME_CR, SCHEME_HC, SCHEME_H77};
+constexpr int line_slot(int scheme) {
+    return scheme == SCHEME_CR ? 0 : (scheme == SCHEME_HC ? 1 : (scheme == SCHEME_H77 ? 2 : -1));
+}
 // prim_mode (x sweep only): 0 reads the primitives W; 1 recovers them from
 // the state while staging and writes W for the tile's own cells (k_prim's
 // work, bitwise the same); 2 also folds their eigenvalues into the boxes'
@@ -145,7 +152,8 @@ cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems
 // crweno_tile_lines() lines of one box.  nmax is the longest line among the
 // launch's boxes and ms = crweno_segment_rows of it (rows per lane of the
 // partitioned line solve); they size the dynamic shared memory.
-// sch: SCHEME_CR (crweno5) or SCHEME_HC (hccs, always the bounded system).
+// sch: SCHEME_CR (crweno5), SCHEME_HC (hccs) or SCHEME_H77 (hccs77); the
+// hccs family always solves the bounded system.
 cudaError_t prepare_crweno_kernels(bool mixed);
 int crweno_tile_lines();
 int crweno_lanes(int sch, int n, bool bounded);

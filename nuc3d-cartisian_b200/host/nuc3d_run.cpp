@@ -73,10 +73,13 @@ int scheme_id(const std::string &s) {
     if (s == "crweno5") return NUC3D_CRWENO5;
     if (s == "weno7js") return NUC3D_WENO7JS;
     if (s == "hccs") return NUC3D_HCCS;
-    for (const char *other : {"hccs77", "hccs78", "weno3js", "upwind1st"})
+    if (s == "hccs77") return NUC3D_HCCS77;
+    if (s == "hccs78") return NUC3D_HCCS78;
+    for (const char *other : {"weno3js", "upwind1st"})
         if (s == other)
             die("reconstruction scheme '" + s +
-                "' is not on the B200 path (weno5js, weno5z, crweno5, weno7js, hccs)");
+                "' is not on the B200 path (weno5js, weno5z, crweno5, weno7js, hccs, hccs77, "
+                "hccs78)");
     return NUC3D_WENO5JS;
 }
 

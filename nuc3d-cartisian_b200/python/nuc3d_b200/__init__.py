@@ -21,10 +21,10 @@ OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2
 ERR_TIMEOUT, ERR_CANCELLED = -6, -7
 INIT_STATE, INIT_TGV, INIT_HIT = 0, 1, 2
 FORCING_NONE, FORCING_CONST, FORCING_BAND = 0, 1, 2
-WENO5JS, WENO5Z, CRWENO5, WENO7JS, HCCS = 0, 1, 2, 3, 4
+WENO5JS, WENO5Z, CRWENO5, WENO7JS, HCCS, HCCS77, HCCS78 = 0, 1, 2, 3, 4, 5, 6
 SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5, "weno7js": WENO7JS,
-           "hccs": HCCS}
-TUNING_SLOTS = 12  # NUC3D_TUNING_SLOTS: (scheme id, direction) pairs
+           "hccs": HCCS, "hccs77": HCCS77, "hccs78": HCCS78}
+TUNING_SLOTS = 21  # NUC3D_TUNING_SLOTS: (scheme id, direction) pairs
 PENCIL_DEPTHS = (32, 16, 64)  # the 2.5-D kernels' pencil depths, in tuning order
 RIEMANN_LF, RIEMANN_AUSM, RIEMANN_AUSMP = 0, 1, 2
 RIEMANNS = {"LF": RIEMANN_LF, "AUSM": RIEMANN_AUSM, "AUSMp": RIEMANN_AUSMP}
@@ -738,7 +738,7 @@ def _tuning(fn, h, fn_pencil=None, fn_tiles=None):
     if fn_tiles is not None:
         check(fn_tiles(h, tc.ctypes.data, ms64.ctypes.data))
     out = {}
-    for s, sname in enumerate(("weno5js", "weno5z", "crweno5", "weno7js")):
+    for sname, s in SCHEMES.items():
         for d, dname in enumerate("xyz"):
             k = s * 3 + d
             if rl[k]:

@@ -16,7 +16,7 @@ from . import (CONSTANT, EULER3D, FORCING_BAND, FORCING_CONST, FORCING_NONE, NAV
 
 _FORCINGS = {"None": FORCING_NONE, "Const": FORCING_CONST, "Band": FORCING_BAND}
 
-_NOT_ON_PATH = ("hccs77", "hccs78", "weno3js", "upwind1st")
+_NOT_ON_PATH = ("weno3js", "upwind1st")
 
 
 def _scheme(name: str) -> int:
