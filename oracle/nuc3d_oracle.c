@@ -103,6 +103,23 @@ static const double CD6[3] = {3.0 / 4.0, -3.0 / 20.0, 1.0 / 60.0};
 
 /* ---------------------------------------------------------------- WENO5 --- */
 
+/* WENO3-JS on an upwind-oriented stencil g[0..2] (weno3js.cpp:79-93 for '+',
+ * :134-148 for '-', and the halo forms): eps = 1e-6, linear weights 1/3,
+ * 2/3; the indicators square with a literal std::pow(x, 2) (x*x), the
+ * weights raise to the member p = 2 through libm's pow. */
+static double weno3js_face(const double g[3]) {
+    const double ss = 1.0e-6;
+    double is0 = SQ(g[0] - g[1]);
+    double is1 = SQ(g[1] - g[2]);
+    double q20 = -0.5 * g[0] + 1.5 * g[1];
+    double q21 = 0.5 * g[1] + 0.5 * g[2];
+    double aa0 = 1.0 / 3.0 / PW(ss + is0);
+    double aa1 = 2.0 / 3.0 / PW(ss + is1);
+    double w0 = aa0 / (aa0 + aa1);
+    double w1 = aa1 / (aa0 + aa1);
+    return w0 * q20 + w1 * q21;
+}
+
 /* WENO5-JS on an upwind-oriented stencil f[0..4] (f[0] farthest upwind).
  * weno5js.cpp:75-108 (inner +), :156-189 (inner -), :275-308 (halo forms);
  * all four are this expression on differently gathered stencils.  eps=1e-6. */
@@ -280,7 +297,11 @@ static void hccs77_row(const double g[7], double *lo, double *b, double *hi, dou
 }
 
 /* buffer (halo) width of a scheme (fieldOperator.cpp:128-175) */
-static int halo_of(int scheme) { return scheme >= OR_WENO7 ? 4 : 3; }
+static int halo_of(int scheme) {
+    if (scheme == OR_WENO3JS) return 2;
+    if (scheme == OR_UPWIND1) return 1;
+    return scheme >= OR_WENO7 ? 4 : 3;
+}
 
 /* One compact-WENO row (crweno5.cpp:131-162 for '+', :311-341 for '-').
  * f[0..4] is the upwind-oriented 5-cell stencil of the row's cell i
@@ -430,6 +451,21 @@ static void reconstruct_line_ref(int scheme, int upwind, unsigned quirks, int n,
         }
         thomas_ref(M, a, b, c, d, x);
         for (int r = 0; r < M; ++r) out[ibeg + 1 + r] = x[r];
+        return;
+    }
+    if (scheme == OR_UPWIND1) {
+        /* upwind1st.cpp:40-368: face m takes the upwind cell, m-1 ('+') or m
+         * ('-') */
+        for (int m = 0; m <= n; ++m) out[m] = upwind > 0 ? line[m - 1] : line[m];
+        return;
+    }
+    if (scheme == OR_WENO3JS) {
+        /* weno3js.cpp: face m from cells m-2, m-1, m ('+') or m+1, m, m-1 ('-') */
+        double g[3];
+        for (int m = 0; m <= n; ++m) {
+            for (int k = 0; k < 3; ++k) g[k] = upwind > 0 ? line[m - 2 + k] : line[m + 1 - k];
+            out[m] = weno3js_face(g);
+        }
         return;
     }
     if (scheme == OR_HCCS78) {

@@ -24,7 +24,7 @@ extern "C" {
 
 /* scheme ids (fieldOperator.cpp:152-166 strings weno5js / weno5z / crweno5) */
 enum { OR_WENO5JS = 0, OR_WENO5Z = 1, OR_CRWENO5 = 2, OR_WENO7 = 3, OR_HCCS = 4, OR_HCCS77 = 5,
-       OR_HCCS78 = 6 };
+       OR_HCCS78 = 6, OR_WENO3JS = 7, OR_UPWIND1 = 8 };
 /* viscosity models (physicsModel.cpp:44-49; power law is an extra model) */
 enum { OR_SUTHERLAND = 0, OR_CONSTANT = 1, OR_POWERLAW = 2 };
 

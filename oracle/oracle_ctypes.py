@@ -26,9 +26,10 @@ HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libnuc3d_oracle.so"
 REF_SO = HERE / "_ref" / "libnuc3d_ref.so"
 
-WENO5JS, WENO5Z, CRWENO5, WENO7, HCCS, HCCS77, HCCS78 = 0, 1, 2, 3, 4, 5, 6
+WENO5JS, WENO5Z, CRWENO5, WENO7, HCCS, HCCS77, HCCS78, WENO3JS, UPWIND1 = range(9)
 SCHEME_NAMES = {WENO5JS: "weno5js", WENO5Z: "weno5z", CRWENO5: "crweno5", WENO7: "weno7js",
-                HCCS: "hccs", HCCS77: "hccs77", HCCS78: "hccs78"}
+                HCCS: "hccs", HCCS77: "hccs77", HCCS78: "hccs78", WENO3JS: "weno3js",
+                UPWIND1: "upwind1st"}
 SUTHERLAND, CONSTANT, POWERLAW = 0, 1, 2
 LF, AUSM, AUSMP = 0, 1, 2
 RIEMANN_NAMES = {LF: "LF", AUSM: "AUSM", AUSMP: "AUSMp"}

@@ -49,6 +49,8 @@
 #include "hccs.hpp"
 #include "hccs77.hpp"
 #include "hccs78.hpp"
+#include "upwind1st.hpp"
+#include "weno3js.hpp"
 #include "physicsModel.h"
 #include "weno5js.h"
 #include "weno5z.hpp"
@@ -128,13 +130,14 @@ struct RefSolver {
 extern "C" {
 
 // scheme: 0 = weno5js, 1 = weno5z, 2 = crweno5, 3 = weno7js, 4 = hccs,
-// 5 = hccs77, 6 = hccs78.
-// in: (nx,ny,nz); halos: (tile,ny,nz) with tile the scheme's bufferSize (3,
-// or 4 for weno7js and the hccs family);
+// 5 = hccs77, 6 = hccs78, 7 = weno3js, 8 = upwind1st.
+// in: (nx,ny,nz); halos: (tile,ny,nz) with tile the scheme's bufferSize (3;
+// 4 for weno7js and the hccs family, 2 for weno3js, 1 for upwind1st);
 // out: (nx+1,ny,nz).  Reconstruction runs along the fastest axis.
 int ref_reconstruct(int scheme, int upwind, int nx, int ny, int nz, const double *in,
                     const double *halo_l, const double *halo_r, double *out) {
-    const int tile = scheme >= 3 ? 4 : 3;  // bufferSize (fieldOperator.cpp:131-175)
+    // bufferSize (fieldOperator.cpp:131-175)
+    const int tile = scheme == 7 ? 2 : (scheme == 8 ? 1 : (scheme >= 3 ? 4 : 3));
     Field fin(nx, ny, nz), fl(tile, ny, nz), fr(tile, ny, nz), fout(nx + 1, ny, nz);
     to_field(in, fin);
     to_field(halo_l, fl);
@@ -172,6 +175,16 @@ int ref_reconstruct(int scheme, int upwind, int nx, int ny, int nz, const double
         s.interpolationBoundaryR(fin, fr, upwind, fout, tile);
     } else if (scheme == 6) {
         nuc3d::hccs78 s;
+        s.interpolationInner(fin, upwind, fout, tile);
+        s.interpolationBoundaryL(fin, fl, upwind, fout, tile);
+        s.interpolationBoundaryR(fin, fr, upwind, fout, tile);
+    } else if (scheme == 7) {
+        nuc3d::weno3js s;
+        s.interpolationInner(fin, upwind, fout, tile);
+        s.interpolationBoundaryL(fin, fl, upwind, fout, tile);
+        s.interpolationBoundaryR(fin, fr, upwind, fout, tile);
+    } else if (scheme == 8) {
+        nuc3d::upwind1st s;
         s.interpolationInner(fin, upwind, fout, tile);
         s.interpolationBoundaryL(fin, fl, upwind, fout, tile);
         s.interpolationBoundaryR(fin, fr, upwind, fout, tile);

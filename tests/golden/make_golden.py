@@ -19,11 +19,11 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT / "oracle"))
 
-from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, HCCS77, HCCS78, WENO5JS, WENO5Z,  # noqa: E402
-                           WENO7, Box, Oracle, Reference)
+from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, HCCS77, HCCS78, UPWIND1, WENO3JS,  # noqa: E402
+                           WENO5JS, WENO5Z, WENO7, Box, Oracle, Reference)
 
 SCHEME_TAG = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr", WENO7: "w7", HCCS: "hc", HCCS77: "h77",
-              HCCS78: "h78"}
+              HCCS78: "h78", WENO3JS: "w3", UPWIND1: "u1"}
 
 
 def perturbed_tgv(box: Box, seed: int):
@@ -38,6 +38,10 @@ def main():
     R = Reference()
     if sys.argv[1:] == ["hccs_siblings"]:  # only the hccs77 / hccs78 fixtures
         hccs_sibling_fixtures(R)
+        print("fixtures written to", HERE)
+        return
+    if sys.argv[1:] == ["low_order"]:  # only the weno3js / upwind1st fixtures
+        low_order_fixtures(R)
         print("fixtures written to", HERE)
         return
     rng = np.random.default_rng(2024)
@@ -104,6 +108,7 @@ def main():
     forcing_fixture(R)
     hccs_fixtures(R)
     hccs_sibling_fixtures(R)
+    low_order_fixtures(R)
     print("fixtures written to", HERE)
 
 
@@ -173,6 +178,41 @@ def hccs_sibling_fixtures(R):
                                 q0=np.stack(q), rhs=np.stack(rhs), dt_local=np.array(dtl),
                                 q3=np.stack(qn), dt=dt, res=res, shape=np.array(box.shape),
                                 mach=box.mach, reynolds=box.reynolds, prandtl=box.prandtl)
+
+
+def low_order_fixtures(R):
+    """The reference's weno3js (2-cell halos) and upwind1st (1-cell halos):
+    both directions on smooth and rough lines; one RHS plus three steps of the
+    Euler equations only.  With Navier-Stokes the reference hands its CD6
+    viscous stencils these schemes' halo width (2 or 1 cells against the 3
+    they read), so its viscous terms read outside their data; no fixture is
+    taken from that combination."""
+    rng = np.random.default_rng(46)
+    shape = (5, 4, 20)
+    x = np.linspace(0.0, 2.0 * np.pi, shape[2], endpoint=False)
+    for sch, halo in ((WENO3JS, 2), (UPWIND1, 1)):
+        out = {}
+        for up in (1, -1):
+            for kind in ("smooth", "rough"):
+                if kind == "smooth":
+                    f = np.sin(x)[None, None, :] + 0.05 * rng.standard_normal(shape)
+                else:
+                    f = rng.standard_normal(shape) * np.exp(rng.standard_normal(shape))
+                hl = rng.standard_normal(shape[:2] + (halo,))
+                hr = rng.standard_normal(shape[:2] + (halo,))
+                tag = f"{kind}_{'p' if up > 0 else 'm'}"
+                out[f"rec_{tag}_in"], out[f"rec_{tag}_hl"], out[f"rec_{tag}_hr"] = f, hl, hr
+                out[f"rec_{tag}_out"] = R.reconstruct_field(sch, up, f, hl, hr)
+        np.savez_compressed(HERE / f"operators_{SCHEME_TAG[sch]}.npz", **out)
+        box = Box(16, 12, 10, scheme=(sch,) * 3, navier_stokes=False, mach=0.3, reynolds=800.0,
+                  prandtl=0.71)
+        q = perturbed_tgv(box, 11 + sch)
+        rhs, dtl = R.rhs(box, q)
+        qn, dt, res = R.run_steps(box, 0.5, 3, q)
+        np.savez_compressed(HERE / f"step_{SCHEME_TAG[sch]}_eu.npz", q0=np.stack(q),
+                            rhs=np.stack(rhs), dt_local=np.array(dtl), q3=np.stack(qn), dt=dt,
+                            res=res, shape=np.array(box.shape), mach=box.mach,
+                            reynolds=box.reynolds, prandtl=box.prandtl)
 
 
 def forcing_fixture(R):

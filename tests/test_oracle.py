@@ -11,7 +11,8 @@ import pytest
 
 from helpers import box_from_golden, golden
 from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, HCCS77, HCCS78, LF, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED,
-                           Q_WENOZ_BETA2, WENO5JS, WENO5Z, WENO7, Box, Oracle, Reference)
+                           Q_WENOZ_BETA2, UPWIND1, WENO3JS, WENO5JS, WENO5Z, WENO7, Box, Oracle,
+                           Reference)
 
 TAGS = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr"}
 
@@ -307,6 +308,36 @@ def test_hccs_siblings_reconstruct_match_reference_golden(O, scheme, kind, up):
 def test_hccs_siblings_rhs_and_steps_match_reference_golden(O, scheme, ns):
     z = golden(f"step_{SIBLING_TAGS[scheme]}_{'ns' if ns else 'eu'}.npz")
     box = box_from_golden(z, scheme, ns)
+    rhs, dtl = O.rhs(box, list(z["q0"]))
+    assert np.array_equal(np.stack(rhs), z["rhs"]) and dtl == float(z["dt_local"])
+    q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
+    assert np.array_equal(np.stack(q3), z["q3"])
+    assert np.array_equal(dt, z["dt"]) and np.array_equal(res, z["res"])
+
+
+LOW_ORDER_TAGS = {WENO3JS: "w3", UPWIND1: "u1"}
+
+
+@pytest.mark.parametrize("scheme", [WENO3JS, UPWIND1])
+@pytest.mark.parametrize("kind", ["smooth", "rough"])
+@pytest.mark.parametrize("up", [1, -1])
+def test_low_order_reconstruct_match_reference_golden(O, scheme, kind, up):
+    """weno3js (eps 1e-6, indicators squared as x*x, weights through pow) and
+    upwind1st (the upwind cell), with their 2- and 1-cell halos."""
+    z = golden(f"operators_{LOW_ORDER_TAGS[scheme]}.npz")
+    tag = f"{kind}_{'p' if up > 0 else 'm'}"
+    out = O.reconstruct_field(scheme, up, QUIRKS_REFERENCE, z[f"rec_{tag}_in"], z[f"rec_{tag}_hl"],
+                              z[f"rec_{tag}_hr"])
+    assert np.array_equal(out, z[f"rec_{tag}_out"])
+
+
+@pytest.mark.parametrize("scheme", [WENO3JS, UPWIND1])
+def test_low_order_euler_rhs_and_steps_match_reference_golden(O, scheme):
+    """Euler only: with Navier-Stokes the reference gives its CD6 viscous
+    stencils these schemes' 2- or 1-cell halo width, too narrow for the 3
+    cells they read, so its viscous terms read outside their data."""
+    z = golden(f"step_{LOW_ORDER_TAGS[scheme]}_eu.npz")
+    box = box_from_golden(z, scheme, False)
     rhs, dtl = O.rhs(box, list(z["q0"]))
     assert np.array_equal(np.stack(rhs), z["rhs"]) and dtl == float(z["dt_local"])
     q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
