@@ -35,9 +35,9 @@ extern "C" {
 #define NUC3D_ERR_CANCELLED (-7)   /* solve dropped by nuc3d_serve_destroy */
 
 /* Reconstruction schemes: the Method.in strings weno5js, weno5z, crweno5,
- * weno7js, hccs, hccs77, hccs78 (fieldOperator.cpp:128-175).  weno7js and
- * the hccs family read 4 halo cells per side (their bufferSize), the others
- * 3.  hccs is the hybrid compact scheme of hccs.cpp (WENO7 end faces,
+ * weno7js, hccs, hccs77, hccs78, weno3js, upwind1st (fieldOperator.cpp:
+ * 128-189).  weno7js and the hccs family read 4 halo cells per side (their
+ * bufferSize), weno3js 2, upwind1st 1, the others 3.  hccs is the hybrid compact scheme of hccs.cpp (WENO7 end faces,
  * linear upwind compact rows blended with CRWENO5-weighted rows); hccs77
  * (hccs77.cpp) blends WENO7-Z into the 7th-order upwind compact rows; their
  * lines are bounded tridiagonal systems like crweno5's reference form.
@@ -50,6 +50,8 @@ extern "C" {
 #define NUC3D_HCCS 4
 #define NUC3D_HCCS77 5
 #define NUC3D_HCCS78 6
+#define NUC3D_WENO3JS 7
+#define NUC3D_UPWIND1ST 8
 
 /* PDEModel (block.cpp:146-157) */
 #define NUC3D_EULER3D 0
@@ -253,7 +255,7 @@ NUC3D_API int nuc3d_probe_peak(int precision, double *tflops);
  * cell, twice the shared memory per block).  The first step after the set of
  * (scheme, direction) pairs changes times every variant on the live boxes and
  * keeps the fastest.  run_len[s*3+d] (s: the scheme id, NUC3D_WENO5JS ..
- * NUC3D_HCCS78; d: x, y, z) receives the chosen run length (0 = not tuned;
+ * NUC3D_UPWIND1ST; d: x, y, z) receives the chosen run length (0 = not tuned;
  * always 0 for the line-solve schemes CRWENO5, hccs and hccs77, whose lines
  * have no run variants),
  * ms[(s*3+d)*3+v] the measured milliseconds per launch of the 32-cell
@@ -266,7 +268,7 @@ NUC3D_API int nuc3d_probe_peak(int precision, double *tflops);
  * tile's first cell and another tile length would round differently);
  * NUC3D_TUNING_SLOTS ints and 2*NUC3D_TUNING_SLOTS doubles, either may be
  * NULL. */
-#define NUC3D_TUNING_SLOTS 21
+#define NUC3D_TUNING_SLOTS 27
 NUC3D_API int nuc3d_tuning(const nuc3d_ctx *ctx, int *run_len, double *ms);
 NUC3D_API int nuc3d_batch_tuning(const nuc3d_batch *b, int *run_len, double *ms);
 NUC3D_API int nuc3d_tuning_tiles(const nuc3d_ctx *ctx, int *tile_cells, double *ms64);

@@ -380,7 +380,7 @@ long long nuc3d_batch_launch_count(const nuc3d_batch *b) { return b ? b->eng->la
 int nuc3d_reconstruct(int scheme, int upwind, unsigned quirks, int nx, int ny, int nz,
                       const double *in, const double *hl, const double *hr, double *out,
                       void *stream) {
-    if (scheme < NUC3D_WENO5JS || scheme > NUC3D_HCCS78)
+    if (scheme < NUC3D_WENO5JS || scheme > NUC3D_UPWIND1ST)
         return fail(NUC3D_ERR_UNSUPPORTED, "weno error: no such scheme");
     if (upwind != 1 && upwind != -1) return fail(NUC3D_ERR_INVALID, "weno error: no such direction");
     if (nx < 8 || ny < 1 || nz < 1) return fail(NUC3D_ERR_INVALID, "need nx >= 8, ny, nz >= 1");

@@ -126,7 +126,7 @@ int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
     const int n[3] = {d.nx, d.ny, d.nz};
     for (int i = 0; i < 3; ++i) {
         if (n[i] < 8) return bad(NUC3D_ERR_INVALID, "every box extent must be >= 8 cells");
-        if (d.scheme[i] < NUC3D_WENO5JS || d.scheme[i] > NUC3D_HCCS78)
+        if (d.scheme[i] < NUC3D_WENO5JS || d.scheme[i] > NUC3D_UPWIND1ST)
             return bad(NUC3D_ERR_UNSUPPORTED, "unknown reconstruction scheme");
     }
     for (int i = 0; i < 3; ++i)

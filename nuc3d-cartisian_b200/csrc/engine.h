@@ -73,7 +73,8 @@ public:
     // autotuned sweep variant (tile length and run length, kInvTileCells /
     // kInvRunLen) per [scheme JS/Z/-/W7][dir] (-1: not tuned yet) and the
     // measured milliseconds per launch of each variant
-    int inv_variant[kSchemes][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1},
+    int inv_variant[kSchemes][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1},
+                                    {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1},
                                     {-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
     double inv_tune_ms[kSchemes][3][kInvVariants] = {};
     // autotuned pencil depth of the 2.5-D stencil kernels: index into

@@ -25,13 +25,17 @@ enum : int {
     SCHEME_W7 = 3,
     SCHEME_HC = 4,
     SCHEME_H77 = 5,
-    SCHEME_H78 = 6
+    SCHEME_H78 = 6,
+    SCHEME_W3 = 7,
+    SCHEME_U1 = 8
 };
 
 // reconstruction stencil half-width (the reference's bufferSize,
 // fieldOperator.cpp:128-175): 4 cells for weno7js and the hccs family, 3 for
-// the WENO5 family
-__host__ __device__ constexpr int scheme_halo(int scheme) { return scheme >= SCHEME_W7 ? 4 : 3; }
+// the WENO5 family, 2 for weno3js, 1 for upwind1st
+__host__ __device__ constexpr int scheme_halo(int scheme) {
+    return scheme == SCHEME_W3 ? 2 : (scheme == SCHEME_U1 ? 1 : (scheme >= SCHEME_W7 ? 4 : 3));
+}
 enum : int { VISC_SUTHERLAND = 0, VISC_CONSTANT = 1, VISC_POWERLAW = 2 };
 enum : int { RIEMANN_LF = 0, RIEMANN_AUSM = 1, RIEMANN_AUSMP = 2 };
 
@@ -596,6 +600,29 @@ __device__ __forceinline__ float weno7_face_eps(float f0, float f1, float f2, fl
     float num = fma_(al[3], r[3], fma_(al[2], r[2], fma_(al[1], r[1], mul_(al[0], r[0]))));
     float den = add_(add_(add_(al[0], al[1]), al[2]), al[3]);
     return fma_(mul_(num, frcp_fast(den)), 1.0f / 12.0f, f3);
+}
+
+// weno3js (weno3js.cpp:79-93 for '+', :134-148 for '-', and its halo
+// forms) on an upwind-oriented stencil g0..g2: indicators (g0 - g1)^2 and
+// (g1 - g2)^2, candidates -g0/2 + 3 g1/2 and (g1 + g2)/2, linear weights
+// 1/3 and 2/3, eps = 1e-6, alpha_k = d_k/(eps + beta_k)^2.  The weights are
+// multiplied through by s0^2 s1^2 (s_k = eps + beta_k >= 1e-6, so no product
+// leaves the range of either precision), which leaves one reciprocal:
+// face = (s1^2 q20 + 2 s0^2 q21) / (s1^2 + 2 s0^2).
+template <typename B>
+__device__ __forceinline__ B weno3js_face(B g0, B g1, B g2) {
+    const B ss = B(1.0e-6);
+    const B e0 = sub_(g0, g1), e1 = sub_(g1, g2);
+    B s0 = fma_(e0, e0, ss), s1 = fma_(e1, e1, ss);
+    s0 = mul_(s0, s0);
+    s1 = mul_(s1, s1);
+    const B w1 = mul_(B(2), s0);  // (2/3) s0^2 over (1/3) s1^2, times 3
+    const B q20 = fma_(B(-0.5), g0, mul_(B(1.5), g1)), q21 = mul_(B(0.5), add_(g1, g2));
+    const B den = add_(s1, w1);
+    if constexpr (sizeof(B) == 8)
+        return mul_(fma_(w1, q21, mul_(s1, q20)), drcp_nr(den));
+    else
+        return mul_(fma_(w1, q21, mul_(s1, q20)), frcp_fast(den));
 }
 
 // ---- hccs77 / hccs78 (hccs77.cpp, hccs78.cpp) ----

@@ -46,6 +46,32 @@ __global__ void k_op_weno(int upwind, unsigned quirks, int nx, long long lines, 
                                 : weno5js_face(f[0], f[1], f[2], f[3], f[4]);
 }
 
+// One thread per face of weno3js (weno3js.cpp:44-483: cells m-2..m for '+',
+// m+1..m-1 for '-', 2-cell halos) or upwind1st (upwind1st.cpp:40-368: the
+// upwind cell, 1-cell halos).
+template <int SCH>
+__global__ void k_op_low(int upwind, int nx, long long lines, const double *in, const double *hl,
+                         const double *hr, double *out) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long total = (long long)(nx + 1) * lines;
+    if (t >= total) return;
+    long long line = t / (nx + 1);
+    int m = (int)(t - line * (nx + 1));
+    constexpr int H = scheme_halo(SCH);
+    if (SCH == SCHEME_U1) {
+        out[t] = line_at<H>(in, hl, hr, nx, line, upwind > 0 ? m - 1 : m);
+        return;
+    }
+    if (upwind > 0)
+        out[t] = weno3js_face(line_at<H>(in, hl, hr, nx, line, m - 2),
+                              line_at<H>(in, hl, hr, nx, line, m - 1),
+                              line_at<H>(in, hl, hr, nx, line, m));
+    else
+        out[t] = weno3js_face(line_at<H>(in, hl, hr, nx, line, m + 1),
+                              line_at<H>(in, hl, hr, nx, line, m),
+                              line_at<H>(in, hl, hr, nx, line, m - 1));
+}
+
 // One thread per face of weno7js (weno7js.cpp:17-824) or hccs78
 // (hccs78.cpp:44-732): face m reads cells m-4..m+2 ('+') or m+3..m-3 ('-');
 // the boundary faces use the same expression on halo cells.  hccs78 blends
@@ -256,6 +282,10 @@ cudaError_t op_reconstruct(int scheme, int upwind, unsigned quirks, int nx, long
         k_op_weno7<false><<<grid, 256, 0, st>>>(upwind, nx, lines, in, hl, hr, out);
     else if (scheme == SCHEME_H78)
         k_op_weno7<true><<<grid, 256, 0, st>>>(upwind, nx, lines, in, hl, hr, out);
+    else if (scheme == SCHEME_W3)
+        k_op_low<SCHEME_W3><<<grid, 256, 0, st>>>(upwind, nx, lines, in, hl, hr, out);
+    else if (scheme == SCHEME_U1)
+        k_op_low<SCHEME_U1><<<grid, 256, 0, st>>>(upwind, nx, lines, in, hl, hr, out);
     else if (scheme == SCHEME_Z)
         k_op_weno<SCHEME_Z><<<grid, 256, 0, st>>>(upwind, quirks, nx, lines, in, hl, hr, out);
     else

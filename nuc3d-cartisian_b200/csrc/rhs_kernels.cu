@@ -399,6 +399,23 @@ __device__ __forceinline__ void inviscid_body(const BoxDev *__restrict__ boxes,
                     f[0] = (m0 + k + 8 < NF) ? sF[G::sf(5 + e, l, m0 + k + 8)] : B(0);
                 }
             }
+        } else if constexpr (SCHEME == SCHEME_W3 || SCHEME == SCHEME_U1) {
+            // weno3js: face m from positions m..m+2 ('+', cells m-2..m) and
+            // m+3..m+1 ('-'); upwind1st: position m ('+', cell m-1) and m+1
+            // ('-', cell m)
+#pragma unroll
+            for (int k = 0; k <= R; ++k) {
+                if (k == R && !last) break;
+                const int m = m0 + k;
+                if (SCHEME == SCHEME_U1)
+                    Fh[k] = add_(sF[G::sf(e, l, m)], sF[G::sf(5 + e, l, m + 1)]);
+                else
+                    Fh[k] = add_(weno3js_face(sF[G::sf(e, l, m)], sF[G::sf(e, l, m + 1)],
+                                              sF[G::sf(e, l, m + 2)]),
+                                 weno3js_face(sF[G::sf(5 + e, l, m + 3)],
+                                              sF[G::sf(5 + e, l, m + 2)],
+                                              sF[G::sf(5 + e, l, m + 1)]));
+            }
         } else {
             // FP64 runs of 4 faces step both windows together; the others step
             // them one after the other (measured faster for FP32, and the joint
@@ -665,6 +682,16 @@ cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxe
         if (dir == 1) return launch_v<SCHEME_H78, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
         return launch_v<SCHEME_H78, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
     }
+    if (scheme == SCHEME_W3) {
+        if (dir == 0) return launch_v<SCHEME_W3, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        if (dir == 1) return launch_v<SCHEME_W3, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        return launch_v<SCHEME_W3, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+    }
+    if (scheme == SCHEME_U1) {
+        if (dir == 0) return launch_v<SCHEME_U1, 0, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        if (dir == 1) return launch_v<SCHEME_U1, 1, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+        return launch_v<SCHEME_U1, 2, B>(variant, boxes, items, nitems, in_slot, accumulate, prim_mode, st);
+    }
     return cudaErrorInvalidValue;
 }
 
@@ -685,12 +712,15 @@ static cudaError_t prepare_runs() {
 }
 template <typename B>
 static cudaError_t prepare_all() {
-    cudaError_t e[12] = {prepare_runs<SCHEME_JS, 0, B>(), prepare_runs<SCHEME_JS, 1, B>(),
+    cudaError_t e[18] = {prepare_runs<SCHEME_JS, 0, B>(), prepare_runs<SCHEME_JS, 1, B>(),
                          prepare_runs<SCHEME_JS, 2, B>(), prepare_runs<SCHEME_Z, 0, B>(),
                          prepare_runs<SCHEME_Z, 1, B>(), prepare_runs<SCHEME_Z, 2, B>(),
                          prepare_runs<SCHEME_W7, 0, B>(), prepare_runs<SCHEME_W7, 1, B>(),
                          prepare_runs<SCHEME_W7, 2, B>(), prepare_runs<SCHEME_H78, 0, B>(),
-                         prepare_runs<SCHEME_H78, 1, B>(), prepare_runs<SCHEME_H78, 2, B>()};
+                         prepare_runs<SCHEME_H78, 1, B>(), prepare_runs<SCHEME_H78, 2, B>(),
+                         prepare_runs<SCHEME_W3, 0, B>(), prepare_runs<SCHEME_W3, 1, B>(),
+                         prepare_runs<SCHEME_W3, 2, B>(), prepare_runs<SCHEME_U1, 0, B>(),
+                         prepare_runs<SCHEME_U1, 1, B>(), prepare_runs<SCHEME_U1, 2, B>()};
     for (cudaError_t x : e)
         if (x != cudaSuccess) return x;
     return cudaSuccess;

@@ -123,7 +123,7 @@ constexpr int inv_tile_class(int variant) { return variant >= 3 ? 1 : 0; }
 // scheme slots of the per-scheme sweep tables (indexed by scheme id; the
 // line-solve schemes' slots (CRWENO5, hccs, hccs77) stay empty, their lines
 // run in launch_crweno)
-constexpr int kSchemes = 7;
+constexpr int kSchemes = 9;
 // the line-solve schemes, in the order of the engine's line tables
 constexpr int kLineSchemes = 3;
 constexpr int kLineScheme[kLineSchemes] = {SCHEME_CR, SCHEME_HC, SCHEME_H77};

@@ -64,9 +64,9 @@ std::vector<std::string> words(const std::string &path, bool required) {
     return w;
 }
 
-// fieldOperator3d::setMethodIvs* (fieldOperator.cpp:128-180): a string the
-// reference does not know falls back to weno5js; the reference's other
-// schemes are not on this path and stop the run.
+// fieldOperator3d::setMethodIvs* (fieldOperator.cpp:128-189): every scheme
+// string the reference registers is on this path; a string it does not know
+// falls back to weno5js, as the reference's does.
 int scheme_id(const std::string &s) {
     if (s == "weno5js") return NUC3D_WENO5JS;
     if (s == "weno5z") return NUC3D_WENO5Z;
@@ -75,11 +75,8 @@ int scheme_id(const std::string &s) {
     if (s == "hccs") return NUC3D_HCCS;
     if (s == "hccs77") return NUC3D_HCCS77;
     if (s == "hccs78") return NUC3D_HCCS78;
-    for (const char *other : {"weno3js", "upwind1st"})
-        if (s == other)
-            die("reconstruction scheme '" + s +
-                "' is not on the B200 path (weno5js, weno5z, crweno5, weno7js, hccs, hccs77, "
-                "hccs78)");
+    if (s == "weno3js") return NUC3D_WENO3JS;
+    if (s == "upwind1st") return NUC3D_UPWIND1ST;
     return NUC3D_WENO5JS;
 }
 

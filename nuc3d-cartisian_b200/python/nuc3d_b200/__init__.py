@@ -21,10 +21,11 @@ OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2
 ERR_TIMEOUT, ERR_CANCELLED = -6, -7
 INIT_STATE, INIT_TGV, INIT_HIT = 0, 1, 2
 FORCING_NONE, FORCING_CONST, FORCING_BAND = 0, 1, 2
-WENO5JS, WENO5Z, CRWENO5, WENO7JS, HCCS, HCCS77, HCCS78 = 0, 1, 2, 3, 4, 5, 6
+WENO5JS, WENO5Z, CRWENO5, WENO7JS, HCCS, HCCS77, HCCS78, WENO3JS, UPWIND1ST = range(9)
 SCHEMES = {"weno5js": WENO5JS, "weno5z": WENO5Z, "crweno5": CRWENO5, "weno7js": WENO7JS,
-           "hccs": HCCS, "hccs77": HCCS77, "hccs78": HCCS78}
-TUNING_SLOTS = 21  # NUC3D_TUNING_SLOTS: (scheme id, direction) pairs
+           "hccs": HCCS, "hccs77": HCCS77, "hccs78": HCCS78, "weno3js": WENO3JS,
+           "upwind1st": UPWIND1ST}
+TUNING_SLOTS = 27  # NUC3D_TUNING_SLOTS: (scheme id, direction) pairs
 PENCIL_DEPTHS = (32, 16, 64)  # the 2.5-D kernels' pencil depths, in tuning order
 RIEMANN_LF, RIEMANN_AUSM, RIEMANN_AUSMP = 0, 1, 2
 RIEMANNS = {"LF": RIEMANN_LF, "AUSM": RIEMANN_AUSM, "AUSMp": RIEMANN_AUSMP}

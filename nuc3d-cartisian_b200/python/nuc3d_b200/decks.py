@@ -16,15 +16,10 @@ from . import (CONSTANT, EULER3D, FORCING_BAND, FORCING_CONST, FORCING_NONE, NAV
 
 _FORCINGS = {"None": FORCING_NONE, "Const": FORCING_CONST, "Band": FORCING_BAND}
 
-_NOT_ON_PATH = ("weno3js", "upwind1st")
-
-
 def _scheme(name: str) -> int:
-    """fieldOperator3d::setMethodIvs* (fieldOperator.cpp:128-180): unknown
-    strings fall back to weno5js; the reference's other schemes are refused."""
-    if name in _NOT_ON_PATH:
-        raise ValueError(f"reconstruction scheme {name!r} is not on the B200 path "
-                         f"({', '.join(SCHEMES)})")
+    """fieldOperator3d::setMethodIvs* (fieldOperator.cpp:128-189): every
+    scheme string the reference registers is on this path; unknown strings
+    fall back to weno5js, as the reference's do."""
     return SCHEMES.get(name, SCHEMES["weno5js"])
 
 

@@ -48,8 +48,8 @@ def test_ctx_bytes_accounting():
 
 
 @pytest.mark.parametrize("args,code", [
-    ((9, 1, 0, 16, 2, 2), nb.ERR_UNSUPPORTED),   # no such scheme
-    ((7, 1, 0, 16, 2, 2), nb.ERR_UNSUPPORTED),   # one past hccs78
+    ((12, 1, 0, 16, 2, 2), nb.ERR_UNSUPPORTED),  # no such scheme
+    ((9, 1, 0, 16, 2, 2), nb.ERR_UNSUPPORTED),   # one past upwind1st
     ((4, 1, 0, 8, 2, 2), nb.ERR_INVALID),        # hccs line too short
     ((5, 1, 0, 8, 2, 2), nb.ERR_INVALID),        # hccs77 line too short
     ((5, 1, 0, 5000, 2, 2), nb.ERR_INVALID),     # hccs77 line too long
@@ -67,7 +67,7 @@ def test_reconstruct_validation_without_device(args, code):
 def test_ctx_create_rejects_bad_descriptions_without_device():
     L = nb.lib()
     h = C.c_void_p()
-    for bad in (nb.BoxDesc(4, 16, 16), nb.BoxDesc(16, 16, 16, scheme=(0, 7, 0)),
+    for bad in (nb.BoxDesc(4, 16, 16), nb.BoxDesc(16, 16, 16, scheme=(0, 9, 0)),
                 nb.BoxDesc(16, 16, 16, mach=-1.0), nb.BoxDesc(16, 16, 16, precision=3),
                 nb.BoxDesc(16, 16, 16, riemann=3)):
         d = bad.c_struct()

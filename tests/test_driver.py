@@ -82,9 +82,9 @@ def test_driver_rejects_what_the_path_does_not_cover(driver, tmp_path):
     r = run(driver, tmp_path, "--check-decks")
     assert r.returncode != 0 and "word Bogus does not exist" in r.stderr
     nb.write_decks(tmp_path, nb.BoxDesc(16, 16, 16))
-    text = (inp / "Method.in").read_text().replace("scheme_z_ivs weno5js", "scheme_z_ivs weno3js")
+    text = (inp / "Method.in").read_text().replace("scheme_z_vis cd6", "scheme_z_vis cd8")
     (inp / "Method.in").write_text(text)
     r = run(driver, tmp_path, "--check-decks")
-    assert r.returncode != 0 and "weno3js" in r.stderr
+    assert r.returncode != 0 and "cd8" in r.stderr
     r = run(driver, "--help")
     assert r.returncode == 0 and "usage" in r.stdout

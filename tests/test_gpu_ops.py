@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 from helpers import golden, rel_l2
-from oracle_ctypes import HCCS, HCCS77, HCCS78, QUIRKS_REFERENCE, Q_WENOZ_BETA2, WENO7, Oracle
+from oracle_ctypes import (HCCS, HCCS77, HCCS78, QUIRKS_REFERENCE, Q_WENOZ_BETA2, UPWIND1, WENO3JS,
+                           WENO7, Oracle)
 
 pytestmark = pytest.mark.gpu
 
@@ -119,6 +120,24 @@ def test_hccs_siblings_reconstruct_golden(torch_cuda, scheme, tag, kind, up):
     """hccs77 (WENO7-Z blended into 7th-order upwind compact rows, a line
     solve) and hccs78 (WENO7-Z blended with the 8th-order central value) with
     4-cell halos against the reference's own outputs at 1e-12."""
+    import nuc3d_b200 as nb
+    torch = torch_cuda
+    z = golden(f"operators_{tag}.npz")
+    key = f"{kind}_{'p' if up > 0 else 'm'}"
+    fin = to_dev(torch, z[f"rec_{key}_in"])
+    out = torch.zeros(fin.shape[:2] + (fin.shape[2] + 1,), dtype=torch.float64, device="cuda")
+    nb.reconstruct(scheme, up, QUIRKS_REFERENCE, fin, to_dev(torch, z[f"rec_{key}_hl"]),
+                   to_dev(torch, z[f"rec_{key}_hr"]), out)
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), z[f"rec_{key}_out"]) < 1e-12
+
+
+@pytest.mark.parametrize("scheme,tag", [(WENO3JS, "w3"), (UPWIND1, "u1")])
+@pytest.mark.parametrize("kind", ["smooth", "rough"])
+@pytest.mark.parametrize("up", [1, -1])
+def test_low_order_reconstruct_golden(torch_cuda, scheme, tag, kind, up):
+    """weno3js (2-cell halos) and upwind1st (1-cell halos) against the
+    reference's own outputs at 1e-12."""
     import nuc3d_b200 as nb
     torch = torch_cuda
     z = golden(f"operators_{tag}.npz")

@@ -40,7 +40,8 @@ import pytest
 from helpers import (box_from_golden, desc_from_box, golden, max_rel_l2, rel_l2,
                      rhs_rounding_sensitivity, rounding_sensitivity)
 from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, HCCS77, HCCS78, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, Q_OFFDIAG_DIV,
-                           Q_WENOZ_BETA2, Q_ZETA_EIGEN, WENO5JS, WENO5Z, WENO7, Box, Oracle)
+                           Q_WENOZ_BETA2, Q_ZETA_EIGEN, UPWIND1, WENO3JS, WENO5JS, WENO5Z, WENO7, Box,
+                           Oracle)
 
 pytestmark = pytest.mark.gpu
 
@@ -154,6 +155,38 @@ def test_hccs_mixed_precision_close_to_fp64(torch):
           f"kinetic energy rel diff {abs(ke[1] - ke[0]) / ke[0]:.2e}")
     assert err < 1e-3
     assert abs(ke[1] - ke[0]) <= 5e-3 * ke[0]
+
+
+@pytest.mark.parametrize("scheme,tag", [(WENO3JS, "w3"), (UPWIND1, "u1")])
+def test_low_order_euler_rhs_and_three_steps_match_reference(torch, scheme, tag):
+    """weno3js / upwind1st, Euler: the first RHS, dt and three steps against
+    the reference's own outputs at 1e-12."""
+    z = golden(f"step_{tag}_eu.npz")
+    box = box_from_golden(z, scheme, False)
+    rhs, dtl = gpu_rhs(torch, box, z["q0"])
+    assert max_rel_l2(rhs, z["rhs"]) < TOL_FP64
+    assert abs(dtl - float(z["dt_local"])) <= 1e-14 * float(z["dt_local"])
+    q3, dt, res = gpu_steps(box, z["q0"], 3)
+    assert max_rel_l2(q3, z["q3"]) < TOL_FP64
+    np.testing.assert_allclose(dt, z["dt"], rtol=1e-13)
+
+
+@pytest.mark.parametrize("scheme", [WENO3JS, UPWIND1])
+def test_low_order_navier_stokes_match_oracle(torch, scheme):
+    """weno3js / upwind1st with Navier-Stokes against the oracle (the
+    reference's own runs of this combination give its CD6 viscous stencils
+    the scheme's 2- or 1-cell halo width and read outside their data; the
+    oracle's viscous terms are pinned through the other schemes)."""
+    box = Box(20, 14, 12, scheme=(scheme,) * 3, mach=0.3, reynolds=600.0)
+    rng = np.random.default_rng(60 + scheme)
+    O = Oracle()
+    q = [np.ascontiguousarray(a * (1 + 0.02 * rng.standard_normal(a.shape))) for a in O.tgv(box)]
+    ref, _ = O.rhs(box, q)
+    got, _ = gpu_rhs(torch, box, q)
+    assert max_rel_l2(got, ref) < TOL_FP64
+    q3o, _, _ = O.run_steps(box, 0.5, 3, q)
+    q3g, _, _ = gpu_steps(box, q, 3)
+    assert max_rel_l2(q3g, q3o) < TOL_FP64
 
 
 @pytest.mark.parametrize("scheme,bar", [(HCCS77, 1e-3), (HCCS78, 1e-5)])
