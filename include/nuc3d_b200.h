@@ -109,7 +109,20 @@ typedef struct nuc3d_box_desc {
      * NUC3D_QUIRK_ZETA_EIGEN belongs to RiemannLF only: the AUSM loops keep
      * each direction's own maximum eigenvalue. */
     int riemann;
+    /* Method.in scheme_{x,y,z}_vis (fieldOperator.cpp:301-375): NUC3D_CD6
+     * (centraldifference6th, the default), NUC3D_CD2 (centraldifference2nd)
+     * or NUC3D_CD8 (centraldifference8th) per direction, for the velocity and
+     * temperature gradients, the divergence of the viscous fluxes and the
+     * statistics' gradients.  The halos are periodic whatever the inviscid
+     * scheme (the reference hands these stencils the inviscid scheme's
+     * bufferSize as their halo width, which cd8 outreaches with a 3-cell
+     * scheme and cd6 with weno3js / upwind1st: there it reads outside its
+     * data). */
+    int vis_scheme[3];
 } nuc3d_box_desc;
+#define NUC3D_CD6 0
+#define NUC3D_CD2 1
+#define NUC3D_CD8 2
 #define NUC3D_RIEMANN_LF 0
 #define NUC3D_RIEMANN_AUSM 1
 #define NUC3D_RIEMANN_AUSMP 2
@@ -480,6 +493,17 @@ NUC3D_API int nuc3d_reconstruct_crweno5_noalloc(int upwind, int nx, int ny, int 
  * (centraldifference6th.cpp:16-186); out is (nx,ny,nz). */
 NUC3D_API int nuc3d_cd6(int nx, int ny, int nz, double dx, const double *d_in, const double *d_halo_l,
               const double *d_halo_r, double *d_out, void *stream);
+
+/* The `differential` plug-in of any registered scheme (fieldOperator.h:58-81):
+ * scheme NUC3D_CD6, NUC3D_CD2 or NUC3D_CD8 (centraldifference6th.cpp:16-186,
+ * centraldifference2nd.cpp:16-146, centraldifference8th.cpp:22-205) with the
+ * reference's tilesize `tile` (the inviscid scheme's bufferSize, 1..4): the
+ * halos are (tile,ny,nz) and cd8's cells within `tile` of a line end take its
+ * boundary form.  NUC3D_ERR_INVALID where the stencil would reach past the
+ * halo (cd6 with tile < 3, cd8 with tile < 4), nx < 2 tile or nx > 4096. */
+NUC3D_API int nuc3d_differential(int scheme, int tile, int nx, int ny, int nz, double dx,
+                                 const double *d_in, const double *d_halo_l,
+                                 const double *d_halo_r, double *d_out, void *stream);
 
 /* tvdrk3rd::integrationAll (TVD-RK3.cpp:16-157): d_ui updated in place from
  * d_rhs (the RHS R, dQ/dt = -R), d_un (u_n), stage 0..2. */

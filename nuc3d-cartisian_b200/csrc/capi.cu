@@ -402,6 +402,20 @@ int nuc3d_cd6(int nx, int ny, int nz, double dx, const double *in, const double 
     return NUC3D_OK;
 }
 
+int nuc3d_differential(int scheme, int tile, int nx, int ny, int nz, double dx, const double *in,
+                       const double *hl, const double *hr, double *out, void *stream) {
+    if (scheme < NUC3D_CD6 || scheme > NUC3D_CD8) return fail(NUC3D_ERR_UNSUPPORTED, "unknown differential scheme");
+    const int reach = scheme == NUC3D_CD2 ? 1 : (scheme == NUC3D_CD8 ? 4 : 3);
+    if (tile < reach || tile > 4)
+        return fail(NUC3D_ERR_INVALID, "tilesize must cover the stencil's reach and be <= 4");
+    if (nx < 2 * tile || nx > 4096 || ny < 1 || nz < 1 || !(dx > 0.0))
+        return fail(NUC3D_ERR_INVALID, "bad size or dx");
+    if (!in || !hl || !hr || !out) return fail(NUC3D_ERR_INVALID, "null buffer");
+    CK(op_differential(scheme, tile, nx, (long long)ny * nz, dx, in, hl, hr, out,
+                       static_cast<cudaStream_t>(stream)));
+    return NUC3D_OK;
+}
+
 int nuc3d_tvdrk3_stage(int stage, long long n, double dt, const double *const d_rhs[5],
                        const double *const d_un[5], double *const d_ui[5], void *stream) {
     if (stage < 0 || stage > 2) return fail(NUC3D_ERR_INVALID, "stage must be 0, 1 or 2");

@@ -101,7 +101,29 @@ BoxParams make_params(const nuc3d_box_desc &d) {
     bp.quirks = d.quirks;
     for (int i = 0; i < 3; ++i) bp.scheme[i] = d.scheme[i];
     bp.riemann = d.riemann;
+    // differential schemes as coefficients of f(i+m) - f(i-m), m = 1..4
+    // (schemes.hpp:36-42)
+    for (int i = 0; i < 3; ++i) {
+        bp.vis[i] = d.vis_scheme[i];
+        double *c = bp.vcoef[i];
+        c[0] = c[1] = c[2] = c[3] = 0.0;
+        if (d.vis_scheme[i] == NUC3D_CD2) {
+            c[0] = K::C21;
+        } else if (d.vis_scheme[i] == NUC3D_CD8) {
+            c[0] = K::C81, c[1] = K::C82, c[2] = K::C83, c[3] = K::C84;
+        } else {
+            c[0] = K::CD1, c[1] = K::CD2, c[2] = K::CD3;
+        }
+    }
     return bp;
+}
+
+// stencil class of the 2.5-D kernels (kVisReach): 1 for a Navier-Stokes box
+// with cd2 or cd8 in some direction
+int vis_class(const BoxParams &p) {
+    return p.navier_stokes && (p.vis[0] != VIS_CD6 || p.vis[1] != VIS_CD6 || p.vis[2] != VIS_CD6)
+               ? 1
+               : 0;
 }
 
 int ceil_div(int a, int b) { return (a + b - 1) / b; }
@@ -147,6 +169,9 @@ int Engine::validate(const nuc3d_box_desc &d, std::string *why) {
         return bad(NUC3D_ERR_INVALID, "gamma must be > 1 and Mach, Re, Pr > 0");
     if (d.riemann < NUC3D_RIEMANN_LF || d.riemann > NUC3D_RIEMANN_AUSMP)
         return bad(NUC3D_ERR_UNSUPPORTED, "unknown Riemann solver (flux splitting)");
+    for (int i = 0; i < 3; ++i)
+        if (d.vis_scheme[i] < NUC3D_CD6 || d.vis_scheme[i] > NUC3D_CD8)
+            return bad(NUC3D_ERR_UNSUPPORTED, "unknown differential scheme");
     if (d.forcing != NUC3D_FORCING_NONE && d.forcing != NUC3D_FORCING_CONST &&
         d.forcing != NUC3D_FORCING_BAND)
         return bad(NUC3D_ERR_UNSUPPORTED, "unknown forcing model");
@@ -415,7 +440,8 @@ int Engine::rebuild() {
     ECK(cudaStreamSynchronize(stream_));
     const bool mixed = precision_ == NUC3D_MIXED;
     std::vector<BoxDev> table(boxes_.size());
-    std::vector<WorkItem> prim, st25[3], inv[kSchemes][3][kInvTileClasses], cr[kLineSchemes][3];
+    std::vector<WorkItem> prim, st25[kVisClasses][3], inv[kSchemes][3][kInvTileClasses],
+        cr[kLineSchemes][3];
     const int crtl = crweno_tile_lines();
     for (int c = 0; c < kLineSchemes; ++c)
         for (int d = 0; d < 3; ++d) cr_nmax_[c][d] = cr_ms_[c][d] = 0;
@@ -436,10 +462,12 @@ int Engine::rebuild() {
         for (long long c = 0; c * kPrimChunk < p.N; ++c)
             prim.push_back({id, (int)c, (int)std::min<long long>(kPrimChunk, p.N - c * kPrimChunk), 0});
         boxes_[i].prim_n = (int)prim.size() - boxes_[i].prim_off;
+        const int vc = vis_class(p);
         for (int v = 0; v < 3; ++v)
             for (int z = 0; z < ceil_div(p.n[2], kPencilDepths[v]); ++z)
                 for (int y = 0; y < ceil_div(p.n[1], kT25Y); ++y)
-                    for (int x = 0; x < ceil_div(p.n[0], kT25X); ++x) st25[v].push_back({id, x, y, z});
+                    for (int x = 0; x < ceil_div(p.n[0], kT25X); ++x)
+                        st25[vc][v].push_back({id, x, y, z});
         for (int d = 0; d < 3; ++d) {
             int s = p.scheme[d];
             if (line_slot(s) >= 0) {
@@ -486,7 +514,8 @@ int Engine::rebuild() {
         all.insert(all.end(), v.begin(), v.end());
     };
     append(prim, r_prim_);
-    for (int v = 0; v < 3; ++v) append(st25[v], r_25d_[v]);
+    for (int c = 0; c < kVisClasses; ++c)
+        for (int v = 0; v < 3; ++v) append(st25[c][v], r_25d_[c][v]);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d)
             for (int tc = 0; tc < kInvTileClasses; ++tc) append(inv[s][d][tc], r_inv_[s][d][tc]);
@@ -514,7 +543,9 @@ int Engine::rebuild() {
     ECK(prepare_inviscid_kernels(mixed));
     ECK(prepare_crweno_kernels(mixed));
     ECK(prepare_stencil_kernels(mixed));
-    int per_stage = (any_visc_ && r_25d_[0].n > 0) + (r_25d_[0].n > 0);
+    int per_stage = 0;
+    for (int c = 0; c < kVisClasses; ++c)
+        per_stage += (any_visc_ && r_25d_[c][0].n > 0) + (r_25d_[c][0].n > 0);
     for (int s = 0; s < kSchemes; ++s)
         for (int d = 0; d < 3; ++d) per_stage += r_inv_[s][d][0].n > 0;
     for (int c = 0; c < kLineSchemes; ++c)
@@ -609,8 +640,7 @@ int Engine::enqueue_step_t(cudaStream_t st) {
                 ECK(cudaStreamWaitEvent(fork_stream_, fork_ev_[0], 0));
                 vs = fork_stream_;
             }
-            ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_[pv()].off, r_25d_[pv()].n,
-                                     kPencilDepths[pv()], vs)));
+            ECK(launch_visc_classes<B>(pv(), vs));
             if (fork) ECK(cudaEventRecord(fork_ev_[1], fork_stream_));
         }
         for (int d = 1; d < 3; ++d)
@@ -620,8 +650,7 @@ int Engine::enqueue_step_t(cudaStream_t st) {
         {
             ProfScope ps(this, NUC3D_PROF_UPDATE);
             StageArgs sa{stage, in, out, nullptr};
-            ECK((launch_update<B>(d_boxes_, it + r_25d_[pv()].off, r_25d_[pv()].n,
-                                  kPencilDepths[pv()], sa, any_visc_, st)));
+            ECK(launch_update_classes<B>(pv(), sa, st));
         }
     }
     {
@@ -629,6 +658,28 @@ int Engine::enqueue_step_t(cudaStream_t st) {
         ECK(launch_residual(d_boxes_, nb, st));
     }
     return NUC3D_OK;
+}
+
+template <typename B>
+cudaError_t Engine::launch_visc_classes(int v, cudaStream_t st) {
+    for (int c = 0; c < kVisClasses; ++c) {
+        const Range &rg = r_25d_[c][v];
+        cudaError_t e = launch_visc_flux<B>(d_boxes_, d_items_ + rg.off, rg.n, kPencilDepths[v],
+                                            kVisReach[c], st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template <typename B>
+cudaError_t Engine::launch_update_classes(int v, StageArgs sa, cudaStream_t st) {
+    for (int c = 0; c < kVisClasses; ++c) {
+        const Range &rg = r_25d_[c][v];
+        cudaError_t e = launch_update<B>(d_boxes_, d_items_ + rg.off, rg.n, kPencilDepths[v], sa,
+                                         any_visc_, kVisReach[c], st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // Spectral forcing of the forced boxes (physicsModel::solveSource after
@@ -667,7 +718,8 @@ int Engine::autotune() {
         for (int d = 0; d < 3; ++d)
             need_sweep = need_sweep || (r_inv_[s][d][0].n > 0 && inv_variant[s][d] < 0);
     const bool need_pencil =
-        r_25d_[0].n > 0 && (pencil_variant < 0 || 2 * active_cells_ < pencil_tuned_cells ||
+        (r_25d_[0][0].n > 0 || r_25d_[1][0].n > 0) &&
+        (pencil_variant < 0 || 2 * active_cells_ < pencil_tuned_cells ||
                             active_cells_ > 2 * pencil_tuned_cells);
     if (!need_sweep && !need_pencil) return NUC3D_OK;
     // NUC3D_SWEEP_RUN=1|2|4 pins the run length (32-cell tiles; with
@@ -749,20 +801,15 @@ int Engine::autotune() {
     if (tune_pencil && rc == NUC3D_OK) {
         int best = 0;
         for (int v = 0; v < 3 && rc == NUC3D_OK; ++v) {
-            const Range &rg = r_25d_[v];
             const StageArgs sa{0, 0, 1, nullptr};
             const double ms = time3([&]() {
                 cudaError_t err = cudaSuccess;
                 if (any_visc_)
-                    err = mixed ? launch_visc_flux<float>(d_boxes_, d_items_ + rg.off, rg.n,
-                                                          kPencilDepths[v], stream_)
-                                : launch_visc_flux<double>(d_boxes_, d_items_ + rg.off, rg.n,
-                                                           kPencilDepths[v], stream_);
+                    err = mixed ? launch_visc_classes<float>(v, stream_)
+                                : launch_visc_classes<double>(v, stream_);
                 if (err != cudaSuccess) return err;
-                return mixed ? launch_update<float>(d_boxes_, d_items_ + rg.off, rg.n,
-                                                    kPencilDepths[v], sa, any_visc_, stream_)
-                             : launch_update<double>(d_boxes_, d_items_ + rg.off, rg.n,
-                                                     kPencilDepths[v], sa, any_visc_, stream_);
+                return mixed ? launch_update_classes<float>(v, sa, stream_)
+                             : launch_update_classes<double>(v, sa, stream_);
             });
             pencil_tune_ms[v] = ms;
             if (ms < pencil_tune_ms[best]) best = v;
@@ -859,9 +906,7 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
     ECK(launch_clear_eig(d_boxes_, nb, stream_));
     ECK(launch_prim(d_boxes_, it + r_prim_.off, r_prim_.n, 0, 1, stream_));
     ECK(launch_dt(d_boxes_, nb, stream_));
-    if (any_visc_)
-        ECK((launch_visc_flux<B>(d_boxes_, it + r_25d_[pv()].off, r_25d_[pv()].n,
-                                 kPencilDepths[pv()], stream_)));
+    if (any_visc_) ECK(launch_visc_classes<B>(pv(), stream_));
     for (int d = 0; d < 3; ++d) {
         for (int s = 0; s < kSchemes; ++s)
             ECK((launch_inviscid<B>(s, d, inv_variant[s][d], d_boxes_, it + inv_range(s, d).off,
@@ -873,8 +918,7 @@ int Engine::enqueue_rhs_t(int id, double *const d_rhs[5]) {
     }
     ECK(enqueue_forcing<B>(stream_));
     StageArgs sa{-1, 0, 0, d_rhs_ptrs_};
-    ECK((launch_update<B>(d_boxes_, it + r_25d_[pv()].off, r_25d_[pv()].n, kPencilDepths[pv()],
-                          sa, any_visc_, stream_)));
+    ECK(launch_update_classes<B>(pv(), sa, stream_));
     ECK(cudaStreamSynchronize(stream_));  // ptrs is a host stack array
     return NUC3D_OK;
 }

@@ -103,6 +103,11 @@ private:
     int enqueue_rhs_t(int id, double *const d_rhs[5]);
     template <typename B>
     cudaError_t enqueue_forcing(cudaStream_t st);
+    // the 2.5-D kernels of both stencil classes at pencil-depth variant v
+    template <typename B>
+    cudaError_t launch_visc_classes(int v, cudaStream_t st);
+    template <typename B>
+    cudaError_t launch_update_classes(int v, StageArgs sa, cudaStream_t st);
     void invalidate_graph();
     int autotune();
 
@@ -127,8 +132,9 @@ private:
     const Range &inv_range(int s, int d) const {
         return r_inv_[s][d][inv_variant[s][d] < 0 ? 0 : inv_tile_class(inv_variant[s][d])];
     }
-    // 2.5-D stencil tiles for each pencil depth of kPencilDepths
-    Range r_25d_[3];
+    // 2.5-D stencil tiles per [stencil class (kVisReach)][pencil depth of
+    // kPencilDepths]
+    Range r_25d_[kVisClasses][3];
     long long active_cells_ = 0;
     int pv() const { return pencil_variant < 0 ? 0 : pencil_variant; }
     // Mixed precision stages each line's split fluxes as FP32 offsets from

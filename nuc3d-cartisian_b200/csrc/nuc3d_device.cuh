@@ -37,6 +37,9 @@ __host__ __device__ constexpr int scheme_halo(int scheme) {
     return scheme == SCHEME_W3 ? 2 : (scheme == SCHEME_U1 ? 1 : (scheme >= SCHEME_W7 ? 4 : 3));
 }
 enum : int { VISC_SUTHERLAND = 0, VISC_CONSTANT = 1, VISC_POWERLAW = 2 };
+// differential schemes of the viscous terms (Method.in scheme_*_vis,
+// fieldOperator.cpp:301-375): centraldifference6th / 2nd / 8th
+enum : int { VIS_CD6 = 0, VIS_CD2 = 1, VIS_CD8 = 2 };
 enum : int { RIEMANN_LF = 0, RIEMANN_AUSM = 1, RIEMANN_AUSMP = 2 };
 
 // Everything a kernel needs to know about one periodic box.
@@ -52,6 +55,10 @@ struct BoxParams {
     unsigned quirks;
     int scheme[3];
     int riemann;  // RIEMANN_LF / _AUSM / _AUSMP
+    int vis[3];   // VIS_CD6 / _CD2 / _CD8 per direction
+    // each direction's differential scheme as the coefficients of
+    // f(i+m) - f(i-m), m = 1..4 (zero beyond the scheme's reach)
+    double vcoef[3][4];
 };
 
 // Field pointers of one box.  q: conserved state (double); w: primitives in
@@ -76,6 +83,10 @@ struct K {
     static constexpr double G0 = 13.0 / 12.0, G1 = 1.0 / 4.0;
     static constexpr double SG0 = 1.0408329997330663;  // sqrt(13/12)
     static constexpr double CD1 = 3.0 / 4.0, CD2 = -3.0 / 20.0, CD3 = 1.0 / 60.0;
+    // schemes.hpp:36, :42
+    static constexpr double C81 = 4.0 / 5.0, C82 = -1.0 / 5.0, C83 = 4.0 / 105.0,
+                            C84 = -1.0 / 280.0;
+    static constexpr double C21 = 0.5;
 };
 
 __device__ __forceinline__ int wrap(int c, int n) {
@@ -842,15 +853,21 @@ __device__ __forceinline__ B cd6(B m3, B m2, B m1, B p1, B p2, B p3, B inv_dx) {
     return (B(K::CD3) * (p3 - m3) + B(K::CD2) * (p2 - m2) + B(K::CD1) * (p1 - m1)) * inv_dx;
 }
 
-// CD6 derivative of a whole-box field f at cell (i, j, k) along axis d with
-// the periodic wrap (centraldifference6th.cpp:44-46 on one rank), FP64; the
-// diagnostics' gradients (statistics, spectra).
-__device__ __forceinline__ double cd6_at(const double *f, const BoxParams &p, int i, int j, int k,
-                                         int d) {
+// Derivative of a whole-box field f at cell (i, j, k) along axis d with the
+// periodic wrap by the direction's differential scheme (centraldifference6th
+// .cpp:44-46, centraldifference2nd.cpp:44, centraldifference8th.cpp:120-123
+// on one rank), FP64; the diagnostics' gradients (statistics, spectra).
+__device__ __forceinline__ double diff_at(const double *f, const BoxParams &p, int i, int j, int k,
+                                          int d) {
     const int n = p.n[d];
     const int c = d == 0 ? i : (d == 1 ? j : k);
     const long long base = (long long)i + p.stride[1] * j + p.stride[2] * k - p.stride[d] * c;
     auto at = [&](int o) { return f[base + p.stride[d] * wrap(c + o, n)]; };
+    if (p.vis[d] == VIS_CD2) return K::C21 * (at(1) - at(-1)) / p.d[d];
+    if (p.vis[d] == VIS_CD8)
+        return (K::C84 * (at(4) - at(-4)) + K::C83 * (at(3) - at(-3)) +
+                K::C82 * (at(2) - at(-2)) + K::C81 * (at(1) - at(-1))) /
+               p.d[d];
     return (K::CD3 * (at(3) - at(-3)) + K::CD2 * (at(2) - at(-2)) + K::CD1 * (at(1) - at(-1))) /
            p.d[d];
 }

@@ -239,6 +239,51 @@ __global__ void k_op_cd6(int nx, long long lines, double inv_dx, const double *i
     out[t] = cd6<double>(F(i - 3), F(i - 2), F(i - 1), F(i + 1), F(i + 2), F(i + 3), inv_dx);
 }
 
+// centraldifference2nd.cpp:16-146 / centraldifference8th.cpp:22-205 (and
+// centraldifference6th with any tilesize): one thread per cell, halos of the
+// tilesize's width.  cd8's cells at least `tile` from both line ends take its
+// inner form (the two one-sided sums, :50-60), the others its symmetric
+// differences (:120-123, :188-191); cd2 and cd6 have one form.
+template <int SCH>
+__global__ void k_op_diff(int nx, int tile, long long lines, double dx, const double *in,
+                          const double *hl, const double *hr, double *out) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)nx * lines) return;
+    long long line = t / nx;
+    int i = (int)(t - line * nx);
+    auto F = [&](int c) {
+        if (c < 0) return hl[tile * line + (c + tile)];
+        if (c >= nx) return hr[tile * line + (c - nx)];
+        return in[(long long)nx * line + c];
+    };
+    double r;
+    if constexpr (SCH == VIS_CD2) {
+        r = div_(mul_(K::C21, sub_(F(i + 1), F(i - 1))), dx);
+    } else if constexpr (SCH == VIS_CD8) {
+        if (i >= tile && i < nx - tile) {
+            const double an = add_(add_(add_(mul_(K::C84, F(i - 4)), mul_(K::C83, F(i - 3))),
+                                        mul_(K::C82, F(i - 2))),
+                                   mul_(K::C81, F(i - 1)));
+            const double ap = add_(add_(add_(mul_(K::C81, F(i + 1)), mul_(K::C82, F(i + 2))),
+                                        mul_(K::C83, F(i + 3))),
+                                   mul_(K::C84, F(i + 4)));
+            r = div_(sub_(ap, an), dx);
+        } else {
+            r = div_(add_(add_(add_(mul_(K::C84, sub_(F(i + 4), F(i - 4))),
+                                    mul_(K::C83, sub_(F(i + 3), F(i - 3)))),
+                               mul_(K::C82, sub_(F(i + 2), F(i - 2)))),
+                          mul_(K::C81, sub_(F(i + 1), F(i - 1)))),
+                     dx);
+        }
+    } else {
+        r = div_(add_(add_(mul_(K::CD3, sub_(F(i + 3), F(i - 3))),
+                           mul_(K::CD2, sub_(F(i + 2), F(i - 2)))),
+                      mul_(K::CD1, sub_(F(i + 1), F(i - 1)))),
+                 dx);
+    }
+    out[t] = r;
+}
+
 // TVD-RK3.cpp:76-196
 __global__ void k_op_rk3(int stage, long long n, double dt, RK5 rk) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -305,6 +350,20 @@ cudaError_t op_cd6(int nx, long long lines, double dx, const double *in, const d
                    const double *hr, double *out, cudaStream_t st) {
     long long total = (long long)nx * lines;
     k_op_cd6<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(nx, lines, 1.0 / dx, in, hl, hr, out);
+    return cudaGetLastError();
+}
+
+cudaError_t op_differential(int scheme, int tile, int nx, long long lines, double dx,
+                            const double *in, const double *hl, const double *hr, double *out,
+                            cudaStream_t st) {
+    long long total = (long long)nx * lines;
+    const unsigned grid = (unsigned)((total + 255) / 256);
+    if (scheme == VIS_CD2)
+        k_op_diff<VIS_CD2><<<grid, 256, 0, st>>>(nx, tile, lines, dx, in, hl, hr, out);
+    else if (scheme == VIS_CD8)
+        k_op_diff<VIS_CD8><<<grid, 256, 0, st>>>(nx, tile, lines, dx, in, hl, hr, out);
+    else
+        k_op_diff<VIS_CD6><<<grid, 256, 0, st>>>(nx, tile, lines, dx, in, hl, hr, out);
     return cudaGetLastError();
 }
 

@@ -22,6 +22,10 @@ cudaError_t op_crweno_into(int upwind, int nx, long long lines, const double *in
 int set_last_error(int code, const char *msg);
 cudaError_t op_cd6(int nx, long long lines, double dx, const double *in, const double *hl,
                    const double *hr, double *out, cudaStream_t st);
+// scheme: VIS_CD6 / VIS_CD2 / VIS_CD8; halos (tile, lines)
+cudaError_t op_differential(int scheme, int tile, int nx, long long lines, double dx,
+                            const double *in, const double *hl, const double *hr, double *out,
+                            cudaStream_t st);
 cudaError_t op_rk3(int stage, long long n, double dt, RK5 rk, cudaStream_t st);
 
 }  // namespace nuc3d

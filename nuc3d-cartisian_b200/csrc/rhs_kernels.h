@@ -138,15 +138,21 @@ template <typename B>
 cudaError_t launch_inviscid(int scheme, int dir, int variant, const BoxDev *boxes,
                             const WorkItem *items, int nitems, int in_slot, int accumulate,
                             int prim_mode, cudaStream_t st);
-// raises the dynamic shared-memory limit of the viscous-flux kernel
+// raises the dynamic shared-memory limits of the 2.5-D stencil kernels
 cudaError_t prepare_stencil_kernels(bool mixed);
-// depth: planes per work item along z (the items' z chunks are of that size)
+// Stencil classes of the 2.5-D kernels: boxes whose three directions use cd6
+// (class 0, reach 3) and all others (class 1, reach 4: each direction's
+// scheme as coefficients, BoxParams::vcoef).
+constexpr int kVisClasses = 2;
+constexpr int kVisReach[kVisClasses] = {3, 4};
+// depth: planes per work item along z (the items' z chunks are of that size);
+// reach: the stencil class's reach (3 or 4)
 template <typename B>
 cudaError_t launch_visc_flux(const BoxDev *boxes, const WorkItem *items, int nitems, int depth,
-                             cudaStream_t st);
+                             int reach, cudaStream_t st);
 template <typename B>
 cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems, int depth,
-                          StageArgs sa, bool any_viscous, cudaStream_t st);
+                          StageArgs sa, bool any_viscous, int reach, cudaStream_t st);
 
 // CRWENO5 / hccs sweeps (crweno_kernels.cu), batched: one work item per tile of
 // crweno_tile_lines() lines of one box.  nmax is the longest line among the

@@ -4,7 +4,7 @@
 //
 //   k_spec_fields  u, v, w, the helicity field w.u, the enstrophy field
 //                  |w|^2/2 (solveQ's fields, postproc.cpp:812-853, vorticity
-//                  from CD6 gradients), density and pressure, as complex
+//                  from the differential scheme's gradients), density and pressure, as complex
 //                  fields with zero imaginary part;
 //   cuFFT          one batched forward 3-D Z2Z transform of the seven fields
 //                  (FFTW_FORWARD sign; the 1/N of fft.cpp:277-278 is applied
@@ -42,9 +42,9 @@ __global__ void __launch_bounds__(kThreads) k_spec_fields(BoxDev b, double2 *F) 
         const int j = (int)((c / p.n[0]) % p.n[1]);
         const int k = (int)(c / ((long long)p.n[0] * p.n[1]));
         const double u0 = u[c], u1 = v[c], u2 = w[c];
-        const double uy = cd6_at(u, p, i, j, k, 1), uz = cd6_at(u, p, i, j, k, 2);
-        const double vx = cd6_at(v, p, i, j, k, 0), vz = cd6_at(v, p, i, j, k, 2);
-        const double wx = cd6_at(w, p, i, j, k, 0), wy = cd6_at(w, p, i, j, k, 1);
+        const double uy = diff_at(u, p, i, j, k, 1), uz = diff_at(u, p, i, j, k, 2);
+        const double vx = diff_at(v, p, i, j, k, 0), vz = diff_at(v, p, i, j, k, 2);
+        const double wx = diff_at(w, p, i, j, k, 0), wy = diff_at(w, p, i, j, k, 1);
         const double w0 = wy - vz, w1 = uz - wx, w2 = vx - uy;
         F[c] = make_double2(u0, 0.0);
         F[N + c] = make_double2(u1, 0.0);

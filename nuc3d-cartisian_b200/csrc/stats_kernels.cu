@@ -3,8 +3,9 @@
 // vorticity, enstrophy, Q, helicity and kinetic energy of enstrophy.dat and
 // the sums behind turb_para.dat — plus the viscous dissipation
 // <mu (|omega|^2 + 4/3 (div u)^2)>, which the reference does not compute.
-// Gradients are CD6 of the primitives with the periodic wrap (the operator's
-// differential scheme on one rank, postproc.cpp:2111-2124).
+// Gradients are the primitives' derivatives by each direction's differential
+// scheme (cd6, cd2 or cd8) with the periodic wrap (the operator's
+// differential scheme on one rank, postproc.cpp:2111-2124, :2285-2297).
 //
 // One launch of a fixed grid accumulates per-block partial sums in a fixed
 // order; a one-block launch adds the partials in a fixed order, so the
@@ -49,12 +50,12 @@ __global__ void __launch_bounds__(kThreads) k_stats(BoxDev b, double *partials) 
         const int j = (int)((c / p.n[0]) % p.n[1]);
         const int k = (int)(c / ((long long)p.n[0] * p.n[1]));
         const double u0 = u[c], u1 = v[c], u2 = w[c];
-        const double ux = cd6_at(u, p, i, j, k, 0), uy = cd6_at(u, p, i, j, k, 1),
-                     uz = cd6_at(u, p, i, j, k, 2);
-        const double vx = cd6_at(v, p, i, j, k, 0), vy = cd6_at(v, p, i, j, k, 1),
-                     vz = cd6_at(v, p, i, j, k, 2);
-        const double wx = cd6_at(w, p, i, j, k, 0), wy = cd6_at(w, p, i, j, k, 1),
-                     wz = cd6_at(w, p, i, j, k, 2);
+        const double ux = diff_at(u, p, i, j, k, 0), uy = diff_at(u, p, i, j, k, 1),
+                     uz = diff_at(u, p, i, j, k, 2);
+        const double vx = diff_at(v, p, i, j, k, 0), vy = diff_at(v, p, i, j, k, 1),
+                     vz = diff_at(v, p, i, j, k, 2);
+        const double wx = diff_at(w, p, i, j, k, 0), wy = diff_at(w, p, i, j, k, 1),
+                     wz = diff_at(w, p, i, j, k, 2);
         // postproc.cpp:812-853
         const double w0 = wy - vz, w1 = uz - wx, w2 = vx - uy;
         const double q0 = ux * vy + ux * wz + vy * wz - uy * vx - uz * wx - vz * wy;

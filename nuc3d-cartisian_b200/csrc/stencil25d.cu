@@ -3,10 +3,15 @@
 // A block owns a 32 x 8 column tile of the box and marches a chunk of
 // `depth` planes along z (the pencil depth, a launch argument the engine's
 // autotuner picks).  For each plane it stages the tile plus the x/y halo in
-// shared memory (the x- and y-direction CD6 stencils read it there) while
-// every thread keeps a 7-deep register queue of its own column for the
+// shared memory (the x- and y-direction stencils read it there) while every
+// thread keeps a (2R+1)-deep register queue of its own column for the
 // z-direction stencil, so each value is fetched from L2/HBM about once per
 // plane instead of once per stencil tap.
+//
+// R is the stencil reach.  R = 3: boxes whose three directions use cd6 (the
+// CD6 stencil written out).  R = 4: every other box; each direction's
+// differential scheme (cd2, cd6 or cd8) is its coefficients of
+// f(i+m) - f(i-m), m = 1..4 (BoxParams::vcoef, zero beyond its reach).
 #include "nuc3d_device.cuh"
 #include "rhs_kernels.h"
 
@@ -88,30 +93,44 @@ __device__ __forceinline__ double cd6d(double m3, double m2, double m1, double p
     return (K::CD3 * (p3 - m3) + K::CD2 * (p2 - m2) + K::CD1 * (p1 - m1)) * inv;
 }
 
+// a direction's differential scheme from the cells at offsets -4..4:
+// c[m-1] is its coefficient of f(i+m) - f(i-m)
+template <typename T, typename C>
+__device__ __forceinline__ T cd_any(T m4, T m3, T m2, T m1, T p1, T p2, T p3, T p4, const C *c,
+                                   T inv) {
+    return (T(c[3]) * (p4 - m4) + T(c[2]) * (p3 - m3) + T(c[1]) * (p2 - m2) +
+            T(c[0]) * (p1 - m1)) *
+           inv;
+}
+
 }  // namespace
 
-// solveGrads + solveViscousFlux (NaiverStokes3d.cpp:87-303): CD6 gradients
-// of u, v, w, T (FP64 differences), stresses and heat flux in the bulk type,
-// written as tau_xx, tau_xy, tau_xz, tau_yy, tau_yz, tau_zz, E_x, E_y, E_z.
+// solveGrads + solveViscousFlux (NaiverStokes3d.cpp:87-303): gradients of
+// u, v, w, T by the differential schemes (FP64 differences), stresses and
+// heat flux in the bulk type, written as tau_xx, tau_xy, tau_xz, tau_yy,
+// tau_yz, tau_zz, E_x, E_y, E_z.
 // Work item: (box, x tile, y tile, z chunk of `depth` planes).
-template <typename B>
+template <typename B, int R>
 __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, int depth) {
     // dynamic shared memory (visc_smem_bytes): the two plane tiles with their
     // x/y halo (row pitch TX + 8: column 0 is cell i0 - 4, so that a TMA box
-    // starts on a 32-byte boundary), each column's plane k+3 (z-queue
+    // starts on a 32-byte boundary), each column's plane k+R (z-queue
     // refill), the tile offsets, two mbarriers
+    static_assert(R == 3 || R == 4, "stencil reach");
     static_assert(kViscTmaHaloX == TX + 8 && kViscTmaHaloY == TY + 6, "TMA halo box");
     static_assert(kViscTmaTileX == TX && kViscTmaTileY == TY, "TMA tile box");
+    constexpr int QD = 2 * R + 1;                   // z-queue depth
+    constexpr int RY = TY + 2 * R, RX = TX + 2 * R;  // halo tile rows, halo columns
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // TMA destinations must start on 128-byte boundaries: the layout starts
     // at the first such boundary of the window (128 bytes are reserved)
     unsigned char *const sbase = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
     constexpr int PX = TX + 8;
-    auto sP = reinterpret_cast<double (*)[4][TY + 6][PX]>(sbase);
-    auto sZ = reinterpret_cast<double (*)[4][TX * TY]>(sbase + sizeof(double) * 2 * 4 * (TY + 6) * PX);
-    int *sOff = reinterpret_cast<int *>(sbase + sizeof(double) * 2 * 4 * ((TY + 6) * PX + TX * TY));
+    auto sP = reinterpret_cast<double (*)[4][RY][PX]>(sbase);
+    auto sZ = reinterpret_cast<double (*)[4][TX * TY]>(sbase + sizeof(double) * 2 * 4 * RY * PX);
+    int *sOff = reinterpret_cast<int *>(sbase + sizeof(double) * 2 * 4 * (RY * PX + TX * TY));
     auto mbar = reinterpret_cast<unsigned long long *>(
-        sbase + sizeof(double) * 2 * 4 * ((TY + 6) * PX + TX * TY) + 16 * ((TY + 6) * (TX + 6) * 4 / 16 + 1));
+        sbase + sizeof(double) * 2 * 4 * (RY * PX + TX * TY) + 16 * (RY * RX * 4 / 16 + 1));
     const WorkItem it = items[blockIdx.x];
     const BoxDev &bd = boxes[it.box];
     if (!bd.active || !bd.p.navier_stokes) return;
@@ -127,13 +146,14 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
     const long long sz = bp.stride[2];
     const long long col = active ? (long long)i + (long long)nx * j : 0;
     const int src[4] = {0, 1, 2, 5};  // u, v, w, T
-    // A tile whose halo plane lies inside the box (no periodic wrap) loads
-    // each plane with TMA: one thread issues 8 tile copies (halo plane and
-    // plane k+3 of u, v, w, T) completing on the buffer's mbarrier.  Other
-    // tiles copy element by element with cp.async through the wrapped offset
-    // table.
+    // A CD6 tile (R = 3) whose halo plane lies inside the box (no periodic
+    // wrap) loads each plane with TMA: one thread issues 8 tile copies (halo
+    // plane and plane k+3 of u, v, w, T) completing on the buffer's mbarrier.
+    // Other tiles copy element by element with cp.async through the wrapped
+    // offset table.
     const CUtensorMapLike *tm = static_cast<const CUtensorMapLike *>(bd.tmw);
-    const bool tma = tm != nullptr && i0 >= 4 && i0 + TX + 4 <= nx && j0 >= 3 && j0 + TY + 3 <= ny;
+    const bool tma = R == 3 && tm != nullptr && i0 >= 4 && i0 + TX + 4 <= nx && j0 >= 3 &&
+                     j0 + TY + 3 <= ny;
     if (tma) {
         if (tid == 0) {
             mbar_init(&mbar[0], 1);
@@ -141,17 +161,17 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
             asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         }
     } else {
-        for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
-            int yy = t / (TX + 6), xx = t - yy * (TX + 6);
-            sOff[t] = pmod(i0 - 3 + xx, nx) + nx * pmod(j0 - 3 + yy, ny);
+        for (int t = tid; t < RY * RX; t += TX * TY) {
+            int yy = t / RX, xx = t - yy * RX;
+            sOff[t] = pmod(i0 - R + xx, nx) + nx * pmod(j0 - R + yy, ny);
         }
     }
     __syncthreads();
     constexpr unsigned kTmaBytes = 4 * sizeof(double) * ((TY + 6) * PX + TX * TY);
-    // plane k's halo tile, and each column's plane k+3 for the z-queue: both
+    // plane k's halo tile, and each column's plane k+R for the z-queue: both
     // arrive while plane k-1 is computed
     auto issue = [&](int k, int buf) {
-        const int kz = k + 3 < nz ? k + 3 : k + 3 - nz;  // nz >= 8
+        const int kz = k + R < nz ? k + R : k + R - nz;  // nz >= 8
         if (tma) {
             if (tid == 0) {
                 // the buffer's previous contents were read before the block's
@@ -167,12 +187,12 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
             return;
         }
         const long long plane = sz * k;
-        for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
-            int yy = t / (TX + 6), xx = t - yy * (TX + 6);
+        for (int t = tid; t < RY * RX; t += TX * TY) {
+            int yy = t / RX, xx = t - yy * RX;
             long long g = plane + sOff[t];
 #pragma unroll
             for (int f = 0; f < 4; ++f)
-                cp_async_elem(&sP[buf][f][yy][xx + 1], wbase + src[f] * np + g);
+                cp_async_elem(&sP[buf][f][yy][xx + 4 - R], wbase + src[f] * np + g);
         }
         if (active) {
             const long long g6 = col + sz * kz;
@@ -195,10 +215,10 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
     const int kend = min(k0 + depth, nz);
     issue(k0, 0);
     cp_async_commit();
-    double qz[4][7];
+    double qz[4][QD];
 #pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        long long g = col + sz * pmod(k0 - 3 + s, nz);
+    for (int s = 0; s < 2 * R; ++s) {
+        long long g = col + sz * pmod(k0 - R + s, nz);
 #pragma unroll
         for (int f = 0; f < 4; ++f) qz[f][s] = active ? wbase[src[f] * np + g] : 0.0;
     }
@@ -206,12 +226,12 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
     const B c23 = B(2.0 / 3.0);
     const bool od = (bp.quirks & QK_OFFDIAG_DIV) != 0;
     const ViscConst<B> vc(bp);
-    // The z queue is a ring of 7 register slots: plane k+s-3 sits in slot
-    // (k-k0+s) % 7.  The plane loop is unrolled by 7 so that every slot index
-    // is a constant and the ring turns without register moves.
-    for (int kb = k0; kb < kend; kb += 7) {
+    // The z queue is a ring of QD register slots: plane k+s-R sits in slot
+    // (k-k0+s) % QD.  The plane loop is unrolled by QD so that every slot
+    // index is a constant and the ring turns without register moves.
+    for (int kb = k0; kb < kend; kb += QD) {
 #pragma unroll
-        for (int u = 0; u < 7; ++u) {
+        for (int u = 0; u < QD; ++u) {
             const int k = kb + u;
             if (k >= kend) break;  // block-uniform
             const int buf = (k - k0) & 1;
@@ -229,22 +249,33 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
                 }
                 return;
             }
-            // slot of plane k+s-3 (kb - k0 is a multiple of 7)
-#define QZ(f, s) qz[f][(u + (s)) % 7]
+            // slot of plane k+s-R (kb - k0 is a multiple of QD)
+#define QZ(f, s) qz[f][(u + (s)) % QD]
 #pragma unroll
-            for (int f = 0; f < 4; ++f) QZ(f, 6) = active ? sZ[buf][f][tid] : 0.0;
+            for (int f = 0; f < 4; ++f) QZ(f, 2 * R) = active ? sZ[buf][f][tid] : 0.0;
             if (active) {
                 B gr[4][3];
 #pragma unroll
                 for (int f = 0; f < 4; ++f) {
-                    const int r = ty + 3, c = tx + 4;
+                    const int r = ty + R, c = tx + 4;
                     const double(*P)[PX] = sP[buf][f];
-                    gr[f][0] = B(cd6d(P[r][c - 3], P[r][c - 2], P[r][c - 1], P[r][c + 1],
-                                      P[r][c + 2], P[r][c + 3], ix));
-                    gr[f][1] = B(cd6d(P[r - 3][c], P[r - 2][c], P[r - 1][c], P[r + 1][c],
-                                      P[r + 2][c], P[r + 3][c], iy));
-                    gr[f][2] = B(cd6d(QZ(f, 0), QZ(f, 1), QZ(f, 2), QZ(f, 4), QZ(f, 5), QZ(f, 6),
-                                      iz));
+                    if constexpr (R == 3) {
+                        gr[f][0] = B(cd6d(P[r][c - 3], P[r][c - 2], P[r][c - 1], P[r][c + 1],
+                                          P[r][c + 2], P[r][c + 3], ix));
+                        gr[f][1] = B(cd6d(P[r - 3][c], P[r - 2][c], P[r - 1][c], P[r + 1][c],
+                                          P[r + 2][c], P[r + 3][c], iy));
+                        gr[f][2] = B(cd6d(QZ(f, 0), QZ(f, 1), QZ(f, 2), QZ(f, 4), QZ(f, 5),
+                                          QZ(f, 6), iz));
+                    } else {
+                        gr[f][0] = B(cd_any(P[r][c - 4], P[r][c - 3], P[r][c - 2], P[r][c - 1],
+                                            P[r][c + 1], P[r][c + 2], P[r][c + 3], P[r][c + 4],
+                                            bp.vcoef[0], ix));
+                        gr[f][1] = B(cd_any(P[r - 4][c], P[r - 3][c], P[r - 2][c], P[r - 1][c],
+                                            P[r + 1][c], P[r + 2][c], P[r + 3][c], P[r + 4][c],
+                                            bp.vcoef[1], iy));
+                        gr[f][2] = B(cd_any(QZ(f, 0), QZ(f, 1), QZ(f, 2), QZ(f, 3), QZ(f, 5),
+                                            QZ(f, 6), QZ(f, 7), QZ(f, 8), bp.vcoef[2], iz));
+                    }
                 }
                 B ux = gr[0][0], uy = gr[0][1], uz = gr[0][2];
                 B vx = gr[1][0], vy = gr[1][1], vz = gr[1][2];
@@ -252,7 +283,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
                 B tx_ = gr[3][0], ty_ = gr[3][1], tz_ = gr[3][2];
                 B grad = ux + vy + wz;
                 B miu0, coeff0;
-                vc.eval(B(QZ(3, 3)), miu0, coeff0);
+                vc.eval(B(QZ(3, R)), miu0, coeff0);
                 B dv = od ? c23 * grad : B(0);
                 B t_xx = miu0 * (B(2) * ux - c23 * grad);
                 B t_xy = miu0 * (uy + vx - dv);
@@ -260,7 +291,7 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
                 B t_yy = miu0 * (B(2) * vy - c23 * grad);
                 B t_yz = miu0 * (vz + wy - dv);
                 B t_zz = miu0 * (B(2) * wz - c23 * grad);
-                B uu = B(QZ(0, 3)), v = B(QZ(1, 3)), ww = B(QZ(2, 3));
+                B uu = B(QZ(0, R)), v = B(QZ(1, R)), ww = B(QZ(2, R));
 #undef QZ
                 long long g = col + sz * k;
                 vbase[0 * np + g] = t_xx;
@@ -278,7 +309,8 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
     }
 }
 
-// setDerivativesVis (NaiverStokes3d.cpp:305-369): CD6 of the viscous fluxes,
+// setDerivativesVis (NaiverStokes3d.cpp:305-369): the differential schemes
+// of the viscous fluxes,
 // RHS = inviscid - viscous in the reference's order (:385-499), then the
 // TVD-RK3 stage (TVD-RK3.cpp:76-196, dQ/dt = -RHS) in FP64; on the last stage
 // also the residual sum of PDEData3d::setRES (PDEData3d.cpp:178-213).  Every
@@ -286,24 +318,42 @@ __global__ void __launch_bounds__(TX *TY, 2) k_visc_flux25(const BoxDev *__restr
 // Work item: (box, x tile, y tile, z chunk of `depth` planes).  ANYVIS: some box of the batch
 // is viscous (sizes the shared tiles); per box the viscous part runs only for
 // Navier-Stokes boxes.
-template <typename B, bool ANYVIS>
+template <typename B, bool ANYVIS, int R>
 __global__ void __launch_bounds__(TX *TY, 2)
     k_update25(const BoxDev *__restrict__ boxes, const WorkItem *__restrict__ items, int depth,
                StageArgs sa) {
+    static_assert(R == 3 || R == 4, "stencil reach");
+    constexpr int QD = 2 * R + 1;  // z-queue depth
     // x stencils: tau_xx, tau_xy, tau_xz, E_x; y: tau_xy, tau_yy, tau_yz, E_y;
     // z: tau_xz, tau_yz, tau_zz, E_z
     // x and y halo tiles of the fluxes each stencil direction needs.  (The
     // z-queue refill stays a direct load here: routing it through shared
     // memory as k_visc_flux25 does pushed this kernel into register spills.)
-    __shared__ B sX[2][4][TY][TX + 6];
-    __shared__ B sY[2][4][TY + 6][TX];
+    // R = 3 keeps them in static shared memory; the R = 4 tiles (52 KB in
+    // FP64) lie in the dynamic window (update_smem_bytes).
+    using XTile = B[2][4][TY][TX + 2 * R];
+    using YTile = B[2][4][TY + 2 * R][TX];
+    XTile *sXp;
+    YTile *sYp;
+    if constexpr (R == 3) {
+        __shared__ XTile sX3;
+        __shared__ YTile sY3;
+        sXp = &sX3;
+        sYp = &sY3;
+    } else {
+        extern __shared__ __align__(16) unsigned char smem_dyn[];
+        sXp = reinterpret_cast<XTile *>(smem_dyn);
+        sYp = reinterpret_cast<YTile *>(smem_dyn + sizeof(XTile));
+    }
+    XTile &sX = *sXp;
+    YTile &sY = *sYp;
     __shared__ double red[TX * TY / 32];
-    // periodic wraps of the tile's columns and rows with their 3-cell halos
+    // periodic wraps of the tile's columns and rows with their R-cell halos
     // (x: i index; y: row offset j nx), resolved once per block.  FP32 only:
     // in the FP64 instance (at its register limit) the table lookups cost
     // register spills that outweigh the remainders they save.
     constexpr bool wrap_table = sizeof(B) == 4;
-    __shared__ int sWx[TX + 6], sWy[TY + 6];
+    __shared__ int sWx[TX + 2 * R], sWy[TY + 2 * R];
     const int cx[4] = {0, 1, 2, 6}, cy[4] = {1, 3, 4, 7}, cz[4] = {2, 4, 5, 8};
     const WorkItem it = items[blockIdx.x];
     const BoxDev &bd = boxes[it.box];
@@ -329,39 +379,44 @@ __global__ void __launch_bounds__(TX *TY, 2)
     const B ixb = B(bp.inv_d[0]), iyb = B(bp.inv_d[1]), izb = B(bp.inv_d[2]);
     const int kend = min(k0 + depth, nz);
     if constexpr (wrap_table) {
-        if (tid < TX + 6) sWx[tid] = pmod(i0 - 3 + tid, nx);
-        if (tid < TY + 6) sWy[tid] = nx * pmod(j0 - 3 + tid, ny);
+        if (tid < TX + 2 * R) sWx[tid] = pmod(i0 - R + tid, nx);
+        if (tid < TY + 2 * R) sWy[tid] = nx * pmod(j0 - R + tid, ny);
         __syncthreads();
     }
-    // in-plane offset of tile position (xx, yy) relative to (i0 - 3, j0 - 3)
+    // in-plane offset of tile position (xx, yy) relative to (i0 - R, j0 - R).
+    // Active threads read cells i0 - R .. nx + R - 1 (and rows alike); a tile
+    // reaching further past the box (a box narrower than its tile) loads
+    // cell nx + R - 1 in those unread slots, so that every index stays within
+    // one period of the box, where the compare-and-add wrap holds (n >= 8 > R).
     auto wxy = [&](int xx, int yy) -> long long {
         if constexpr (wrap_table)
             return sWx[xx] + sWy[yy];
-        else  // (halo indices lie within 3 cells of the box, extents >= 8)
-            return wrap1(i0 - 3 + xx, nx) + (long long)nx * wrap1(j0 - 3 + yy, ny);
+        else
+            return wrap1(min(i0 - R + xx, nx + R - 1), nx) +
+                   (long long)nx * wrap1(min(j0 - R + yy, ny + R - 1), ny);
     };
     auto issue = [&](int k, int buf) {
         const long long plane = sz * k;
-        for (int t = tid; t < TY * (TX + 6); t += TX * TY) {
-            int yy = t / (TX + 6), xx = t - yy * (TX + 6);
-            long long g = plane + wxy(xx, yy + 3);
+        for (int t = tid; t < TY * (TX + 2 * R); t += TX * TY) {
+            int yy = t / (TX + 2 * R), xx = t - yy * (TX + 2 * R);
+            long long g = plane + wxy(xx, yy + R);
 #pragma unroll
             for (int f = 0; f < 4; ++f) cp_async_elem(&sX[buf][f][yy][xx], vbase + cx[f] * np + g);
         }
-        for (int t = tid; t < (TY + 6) * TX; t += TX * TY) {
+        for (int t = tid; t < (TY + 2 * R) * TX; t += TX * TY) {
             int yy = t / TX, xx = t - yy * TX;
-            long long g = plane + wxy(xx + 3, yy);
+            long long g = plane + wxy(xx + R, yy);
 #pragma unroll
             for (int f = 0; f < 4; ++f) cp_async_elem(&sY[buf][f][yy][xx], vbase + cy[f] * np + g);
         }
     };
-    B qz[4][7];
+    B qz[4][QD];
     if (VIS) {
         issue(k0, 0);
         cp_async_commit();
 #pragma unroll
-        for (int s = 0; s < 6; ++s) {
-            long long g = col + sz * pmod(k0 - 3 + s, nz);
+        for (int s = 0; s < 2 * R; ++s) {
+            long long g = col + sz * pmod(k0 - R + s, nz);
 #pragma unroll
             for (int f = 0; f < 4; ++f) qz[f][s] = active ? vbase[cz[f] * np + g] : B(0);
         }
@@ -374,17 +429,17 @@ __global__ void __launch_bounds__(TX *TY, 2)
         if (VIS) {
             if (k + 1 < kend) issue(k + 1, buf ^ 1);
             cp_async_commit();
-            long long g6 = col + sz * (k + 3 < nz ? k + 3 : k + 3 - nz);  // nz >= 8
+            long long g6 = col + sz * (k + R < nz ? k + R : k + R - nz);  // nz >= 8
 #pragma unroll
-            for (int f = 0; f < 4; ++f) qz[f][6] = active ? vbase[cz[f] * np + g6] : B(0);
+            for (int f = 0; f < 4; ++f) qz[f][2 * R] = active ? vbase[cz[f] * np + g6] : B(0);
         }
         // pointwise operands, loaded before the wait so their latency overlaps
-        B R[5];
+        B Rv[5];
         double ui[5], u_n[5];
         if (active) {
 #pragma unroll
             for (int e = 0; e < 5; ++e) {
-                R[e] = rbase[e * np + g];
+                Rv[e] = rbase[e * np + g];
                 if (stage >= 0) ui[e] = uinb[e * np + g];
                 if (stage >= 1) u_n[e] = unb[e * np + g];
             }
@@ -397,27 +452,42 @@ __global__ void __launch_bounds__(TX *TY, 2)
             if (VIS) {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) {
-                    const int c = tx + 3, rr = ty + 3;
+                    const int c = tx + R, rr = ty + R;
                     const B *X = sX[buf][f][ty];
-                    B dfx = cd6<B>(X[c - 3], X[c - 2], X[c - 1], X[c + 1], X[c + 2], X[c + 3], ixb);
-                    B dfy = cd6<B>(sY[buf][f][rr - 3][tx], sY[buf][f][rr - 2][tx],
-                                   sY[buf][f][rr - 1][tx], sY[buf][f][rr + 1][tx],
-                                   sY[buf][f][rr + 2][tx], sY[buf][f][rr + 3][tx], iyb);
-                    B dfz = cd6<B>(qz[f][0], qz[f][1], qz[f][2], qz[f][4], qz[f][5], qz[f][6], izb);
-                    B t = R[1 + f];
+                    B dfx, dfy, dfz;
+                    if constexpr (R == 3) {
+                        dfx = cd6<B>(X[c - 3], X[c - 2], X[c - 1], X[c + 1], X[c + 2], X[c + 3],
+                                     ixb);
+                        dfy = cd6<B>(sY[buf][f][rr - 3][tx], sY[buf][f][rr - 2][tx],
+                                     sY[buf][f][rr - 1][tx], sY[buf][f][rr + 1][tx],
+                                     sY[buf][f][rr + 2][tx], sY[buf][f][rr + 3][tx], iyb);
+                        dfz = cd6<B>(qz[f][0], qz[f][1], qz[f][2], qz[f][4], qz[f][5], qz[f][6],
+                                     izb);
+                    } else {
+                        dfx = cd_any(X[c - 4], X[c - 3], X[c - 2], X[c - 1], X[c + 1], X[c + 2],
+                                     X[c + 3], X[c + 4], bp.vcoef[0], ixb);
+                        dfy = cd_any(sY[buf][f][rr - 4][tx], sY[buf][f][rr - 3][tx],
+                                     sY[buf][f][rr - 2][tx], sY[buf][f][rr - 1][tx],
+                                     sY[buf][f][rr + 1][tx], sY[buf][f][rr + 2][tx],
+                                     sY[buf][f][rr + 3][tx], sY[buf][f][rr + 4][tx], bp.vcoef[1],
+                                     iyb);
+                        dfz = cd_any(qz[f][0], qz[f][1], qz[f][2], qz[f][3], qz[f][5], qz[f][6],
+                                     qz[f][7], qz[f][8], bp.vcoef[2], izb);
+                    }
+                    B t = Rv[1 + f];
                     t -= dfx;
                     t -= dfy;
                     t -= dfz;
-                    R[1 + f] = t;
+                    Rv[1 + f] = t;
                 }
             }
             if (stage < 0) {
 #pragma unroll
-                for (int e = 0; e < 5; ++e) sa.rhs_out[5 * it.box + e][g] = double(R[e]);
+                for (int e = 0; e < 5; ++e) sa.rhs_out[5 * it.box + e][g] = double(Rv[e]);
             } else {
 #pragma unroll
                 for (int e = 0; e < 5; ++e) {
-                    double rhs = -double(R[e]);
+                    double rhs = -double(Rv[e]);
                     double out;
                     if (stage == 0) {
                         out = 1.0 * ui[e] + 1.0 * rhs * dt;
@@ -436,7 +506,7 @@ __global__ void __launch_bounds__(TX *TY, 2)
         if (VIS) {
             __syncthreads();
 #pragma unroll
-            for (int s = 0; s < 6; ++s)
+            for (int s = 0; s < 2 * R; ++s)
 #pragma unroll
                 for (int f = 0; f < 4; ++f) qz[f][s] = qz[f][s + 1];
         }
@@ -453,49 +523,69 @@ __global__ void __launch_bounds__(TX *TY, 2)
 }
 
 namespace {
-constexpr size_t visc_smem_bytes() {
+constexpr size_t visc_smem_bytes(int R) {
     // planes (row pitch TX + 8) and z refills, the offset table rounded up to
     // 16 bytes, two mbarriers, and the 128 bytes of alignment slack
-    return sizeof(double) * 2 * 4 * ((TY + 6) * (TX + 8) + TX * TY) +
-           16 * ((TY + 6) * (TX + 6) * 4 / 16 + 1) + 2 * sizeof(unsigned long long) + 128;
+    return sizeof(double) * 2 * 4 * ((TY + 2 * R) * (TX + 8) + TX * TY) +
+           16 * ((TY + 2 * R) * (TX + 2 * R) * 4 / 16 + 1) + 2 * sizeof(unsigned long long) + 128;
+}
+// the R = 4 update kernel's x and y flux tiles (dynamic shared memory)
+template <typename B>
+constexpr size_t update_smem_bytes() {
+    return sizeof(B) * 2 * 4 * (TY * (TX + 8) + (TY + 8) * TX);
+}
+template <typename B>
+cudaError_t prepare_stencil_t() {
+    cudaError_t e = cudaFuncSetAttribute(k_visc_flux25<B, 3>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)visc_smem_bytes(3));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_visc_flux25<B, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)visc_smem_bytes(4));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_update25<B, true, 4>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)update_smem_bytes<B>());
+    return e;
 }
 }  // namespace
 
 cudaError_t prepare_stencil_kernels(bool mixed) {
-    return mixed ? cudaFuncSetAttribute(k_visc_flux25<float>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)visc_smem_bytes())
-                 : cudaFuncSetAttribute(k_visc_flux25<double>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)visc_smem_bytes());
+    return mixed ? prepare_stencil_t<float>() : prepare_stencil_t<double>();
 }
 
 template <typename B>
 cudaError_t launch_visc_flux(const BoxDev *boxes, const WorkItem *items, int nitems, int kz,
-                             cudaStream_t st) {
+                             int reach, cudaStream_t st) {
     if (nitems <= 0) return cudaSuccess;
-    k_visc_flux25<B><<<nitems, dim3(TX, TY), visc_smem_bytes(), st>>>(boxes, items, kz);
+    if (reach == 3)
+        k_visc_flux25<B, 3><<<nitems, dim3(TX, TY), visc_smem_bytes(3), st>>>(boxes, items, kz);
+    else
+        k_visc_flux25<B, 4><<<nitems, dim3(TX, TY), visc_smem_bytes(4), st>>>(boxes, items, kz);
     return cudaGetLastError();
 }
 
 template <typename B>
 cudaError_t launch_update(const BoxDev *boxes, const WorkItem *items, int nitems, int kz,
-                          StageArgs sa, bool any_viscous, cudaStream_t st) {
+                          StageArgs sa, bool any_viscous, int reach, cudaStream_t st) {
     if (nitems <= 0) return cudaSuccess;
-    if (any_viscous)
-        k_update25<B, true><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items, kz, sa);
+    if (!any_viscous)
+        k_update25<B, false, 3><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items, kz, sa);
+    else if (reach == 3)
+        k_update25<B, true, 3><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items, kz, sa);
     else
-        k_update25<B, false><<<nitems, dim3(TX, TY), 0, st>>>(boxes, items, kz, sa);
+        k_update25<B, true, 4><<<nitems, dim3(TX, TY), update_smem_bytes<B>(), st>>>(boxes, items,
+                                                                                  kz, sa);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_visc_flux<double>(const BoxDev *, const WorkItem *, int, int,
+template cudaError_t launch_visc_flux<double>(const BoxDev *, const WorkItem *, int, int, int,
                                               cudaStream_t);
-template cudaError_t launch_visc_flux<float>(const BoxDev *, const WorkItem *, int, int,
+template cudaError_t launch_visc_flux<float>(const BoxDev *, const WorkItem *, int, int, int,
                                              cudaStream_t);
 template cudaError_t launch_update<double>(const BoxDev *, const WorkItem *, int, int, StageArgs,
-                                           bool, cudaStream_t);
+                                           bool, int, cudaStream_t);
 template cudaError_t launch_update<float>(const BoxDev *, const WorkItem *, int, int, StageArgs,
-                                          bool, cudaStream_t);
+                                          bool, int, cudaStream_t);
 
 }  // namespace nuc3d

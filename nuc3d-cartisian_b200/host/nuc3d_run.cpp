@@ -114,8 +114,13 @@ Case read_case(const std::string &dir) {
     c.desc.scheme[0] = scheme_id(method["scheme_x_ivs"]);
     c.desc.scheme[1] = scheme_id(method["scheme_y_ivs"]);
     c.desc.scheme[2] = scheme_id(method["scheme_z_ivs"]);
-    for (const char *k : {"scheme_x_vis", "scheme_y_vis", "scheme_z_vis"})
-        if (method[k] != "cd6") die(std::string(k) + " " + method[k] + ": only cd6 is on the B200 path");
+    // fieldOperator3d::setDiffMethod* (fieldOperator.cpp:301-375): cd8, cd6
+    // or cd2; any other string is cd6
+    const char *vis_keys[3] = {"scheme_x_vis", "scheme_y_vis", "scheme_z_vis"};
+    for (int d = 0; d < 3; ++d) {
+        const std::string &v = method[vis_keys[d]];
+        c.desc.vis_scheme[d] = v == "cd8" ? NUC3D_CD8 : (v == "cd2" ? NUC3D_CD2 : NUC3D_CD6);
+    }
     if (method["scheme_time"] != "RK3") die("scheme_time " + method["scheme_time"] + ": only RK3");
     // PhysModel.in: six positional "key value" lines, then key/value pairs
     // (physicsModel.cpp:66-156); unknown keys stop the reference
@@ -318,7 +323,8 @@ int main(int argc, char **argv) {
                   << " t_ref " << c.desc.t_ref << " t_inf " << c.desc.t_inf << " forcing "
                   << c.desc.forcing << " forcing_amp " << c.desc.forcing_amp << " forcing_hel "
                   << c.desc.forcing_hel << " forcing_k " << c.desc.forcing_k << " riemann "
-                  << c.desc.riemann << " cfl "
+                  << c.desc.riemann << " vis " << c.desc.vis_scheme[0] << " "
+                  << c.desc.vis_scheme[1] << " " << c.desc.vis_scheme[2] << " cfl "
                   << c.io["cfl"] << " endStep " << c.io["endStep"] << " tl " << c.io["tl"]
                   << std::endl;
         return 0;

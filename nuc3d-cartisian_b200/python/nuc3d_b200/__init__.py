@@ -29,6 +29,8 @@ TUNING_SLOTS = 27  # NUC3D_TUNING_SLOTS: (scheme id, direction) pairs
 PENCIL_DEPTHS = (32, 16, 64)  # the 2.5-D kernels' pencil depths, in tuning order
 RIEMANN_LF, RIEMANN_AUSM, RIEMANN_AUSMP = 0, 1, 2
 RIEMANNS = {"LF": RIEMANN_LF, "AUSM": RIEMANN_AUSM, "AUSMp": RIEMANN_AUSMP}
+CD6, CD2, CD8 = 0, 1, 2  # differential schemes (Method.in scheme_*_vis)
+VIS_SCHEMES = {"cd6": CD6, "cd2": CD2, "cd8": CD8}
 EULER3D, NAVIERSTOKES3D = 0, 1
 SUTHERLAND, CONSTANT, POWERLAW = 0, 1, 2
 FP64, MIXED = 0, 1
@@ -68,6 +70,7 @@ class _Desc(C.Structure):
         ("forcing", C.c_int),
         ("forcing_amp", C.c_double), ("forcing_hel", C.c_double), ("forcing_k", C.c_double),
         ("riemann", C.c_int),
+        ("vis_scheme", C.c_int * 3),
     ]
 
 
@@ -186,6 +189,9 @@ def lib() -> C.CDLL:
                                         C.c_void_p]
         L.nuc3d_cd6.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_void_p, C.c_void_p]
+        L.nuc3d_differential.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p]
         L.nuc3d_tvdrk3_stage.argtypes = [C.c_int, C.c_longlong, C.c_double, _P5, _P5, _P5,
                                          C.c_void_p]
         _lib = L
@@ -225,6 +231,7 @@ class BoxDesc:
     forcing_hel: float = 0.01       # Forcing_amplitude_hel
     forcing_k: float = 1.0          # Forcing_wave_k
     riemann: int = RIEMANN_LF       # PhysModel.in RiemannSolver: LF, AUSM, AUSMp
+    vis_scheme: tuple = (CD6, CD6, CD6)  # Method.in scheme_{x,y,z}_vis: cd6, cd2, cd8
 
     @property
     def cells(self) -> int:
@@ -249,6 +256,8 @@ class BoxDesc:
         d.forcing = int(self.forcing)
         d.forcing_amp, d.forcing_hel, d.forcing_k = self.forcing_amp, self.forcing_hel, self.forcing_k
         d.riemann = int(self.riemann)
+        for i in range(3):
+            d.vis_scheme[i] = int(self.vis_scheme[i])
         return d
 
     def device_bytes(self) -> int:
@@ -778,6 +787,15 @@ def cd6(dx, d_in, d_hl, d_hr, d_out, stream=None):
     nz, ny, nx = d_in.shape
     check(lib().nuc3d_cd6(nx, ny, nz, dx, d_in.data_ptr(), d_hl.data_ptr(), d_hr.data_ptr(),
                           d_out.data_ptr(), _stream_handle(stream)))
+
+
+def differential(scheme, tile, dx, d_in, d_hl, d_hr, d_out, stream=None):
+    """nuc3d_differential: scheme CD6 / CD2 / CD8 with the reference's
+    tilesize; halos (nz, ny, tile)."""
+    nz, ny, nx = d_in.shape
+    check(lib().nuc3d_differential(scheme, tile, nx, ny, nz, dx, d_in.data_ptr(),
+                                   d_hl.data_ptr(), d_hr.data_ptr(), d_out.data_ptr(),
+                                   _stream_handle(stream)))
 
 
 def tvdrk3_stage(stage, dt, d_rhs, d_un, d_ui, stream=None):

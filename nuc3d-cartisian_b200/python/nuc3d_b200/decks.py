@@ -12,7 +12,7 @@ from __future__ import annotations
 from pathlib import Path
 
 from . import (CONSTANT, EULER3D, FORCING_BAND, FORCING_CONST, FORCING_NONE, NAVIERSTOKES3D, RIEMANNS,
-               SCHEMES, SUTHERLAND, BoxDesc)
+               SCHEMES, SUTHERLAND, VIS_SCHEMES, BoxDesc)
 
 _FORCINGS = {"None": FORCING_NONE, "Const": FORCING_CONST, "Band": FORCING_BAND}
 
@@ -21,6 +21,12 @@ def _scheme(name: str) -> int:
     scheme string the reference registers is on this path; unknown strings
     fall back to weno5js, as the reference's do."""
     return SCHEMES.get(name, SCHEMES["weno5js"])
+
+
+def _vis_scheme(name: str) -> int:
+    """fieldOperator3d::setDiffMethod* (fieldOperator.cpp:301-375): cd8, cd6
+    or cd2; unknown strings fall back to cd6, as the reference's do."""
+    return VIS_SCHEMES.get(name, VIS_SCHEMES["cd6"])
 
 
 _METHOD_DEFAULTS = {"scheme_time": "RK3", "scheme_x_ivs": "weno5js", "scheme_y_ivs": "weno5js",
@@ -93,17 +99,19 @@ def read_decks(dirpath):
                    t_ref=phys["T_ref"], t_inf=phys["T_inf"],
                    forcing=_FORCINGS[pos[5]],
                    forcing_amp=phys["Forcing_amplitude"], forcing_hel=phys["Forcing_amplitude_hel"],
-                   forcing_k=phys["Forcing_wave_k"], riemann=RIEMANNS[pos[2]])
+                   forcing_k=phys["Forcing_wave_k"], riemann=RIEMANNS[pos[2]],
+                   vis_scheme=tuple(_vis_scheme(method[f"scheme_{a}_vis"]) for a in "xyz"))
     return desc, io, phys
 
 
 def write_decks(dirpath, desc, io=None):
     inv = {v: k for k, v in SCHEMES.items()}
+    vinv = {v: k for k, v in VIS_SCHEMES.items()}
     inp = Path(dirpath) / "inp"
     inp.mkdir(parents=True, exist_ok=True)
     (inp / "Method.in").write_text(
         "scheme_time RK3\n" + "".join(f"scheme_{a}_ivs {inv[s]}\n" for a, s in zip("xyz", desc.scheme))
-        + "scheme_x_vis cd6\nscheme_y_vis cd6\nscheme_z_vis cd6\n")
+        + "".join(f"scheme_{a}_vis {vinv[v]}\n" for a, v in zip("xyz", desc.vis_scheme)))
     model = "NavierStokes3d" if desc.pde_model == NAVIERSTOKES3D else "Euler3d"
     visc = "Constant" if desc.visc_model == CONSTANT else "Sutherland"
     forcing = {v: k for k, v in _FORCINGS.items()}[desc.forcing]

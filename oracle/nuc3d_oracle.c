@@ -100,6 +100,7 @@ static const double C_CR5[3] = {0.2, 0.5, 0.3};
 static const double G0 = 13.0 / 12.0;
 static const double G1 = 1.0 / 4.0;
 static const double CD6[3] = {3.0 / 4.0, -3.0 / 20.0, 1.0 / 60.0};
+static const double CD8[4] = {4.0 / 5.0, -1.0 / 5.0, 4.0 / 105.0, -1.0 / 280.0}; /* schemes.hpp:36 */
 
 /* ---------------------------------------------------------------- WENO5 --- */
 
@@ -673,6 +674,60 @@ static double cd6_at(const double *line, int i, double dx) {
            dx;
 }
 
+/* centraldifference2nd.cpp:44 (inner), :82 / :136 (halo): one form everywhere. */
+static double cd2_at(const double *line, int i, double dx) {
+    return 0.5 * (line[i + 1] - line[i - 1]) / dx;
+}
+
+/* centraldifference8th.cpp:50-60 (inner cells): the two one-sided sums, then
+ * their difference. */
+static double cd8_inner_at(const double *line, int i, double dx) {
+    const double an = CD8[3] * line[i - 4] + CD8[2] * line[i - 3] + CD8[1] * line[i - 2] +
+                      CD8[0] * line[i - 1];
+    const double ap = CD8[0] * line[i + 1] + CD8[1] * line[i + 2] + CD8[2] * line[i + 3] +
+                      CD8[3] * line[i + 4];
+    return (ap - an) / dx;
+}
+
+/* centraldifference8th.cpp:120-123 / :188-191 (cells within the tile width
+ * of a line end): symmetric differences. */
+static double cd8_edge_at(const double *line, int i, double dx) {
+    return (CD8[3] * (line[i + 4] - line[i - 4]) + CD8[2] * (line[i + 3] - line[i - 3]) +
+            CD8[1] * (line[i + 2] - line[i - 2]) + CD8[0] * (line[i + 1] - line[i - 1])) /
+           dx;
+}
+
+/* derivative at cell i of an n-cell line whose halos are filled as far as the
+ * scheme reaches; `tile` is the reference's tilesize (the inviscid scheme's
+ * bufferSize, fieldOperator.cpp:520-610): cd8 cells within it of a line end
+ * take the boundary form. */
+static double cd_at(int scheme, int tile, const double *line, int n, int i, double dx) {
+    if (scheme == OR_CD2) return cd2_at(line, i, dx);
+    if (scheme == OR_CD8)
+        return (i < tile || i >= n - tile) ? cd8_edge_at(line, i, dx) : cd8_inner_at(line, i, dx);
+    return cd6_at(line, i, dx);
+}
+
+int or_cd_field(int scheme, int tile, int nx, int ny, int nz, double dx, const double *in,
+                const double *halo_l, const double *halo_r, double *out) {
+    const int reach = scheme == OR_CD2 ? 1 : (scheme == OR_CD8 ? 4 : 3);
+    if (tile < 1 || tile > 4 || tile < reach || nx < 2 * tile) return -1;
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(nx + 2 * tile));
+    double *line = buf + tile;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j) {
+            for (int c = 0; c < tile; ++c) {
+                line[c - tile] = halo_l[c + tile * (j + ny * k)];
+                line[nx + c] = halo_r[c + tile * (j + ny * k)];
+            }
+            for (int i = 0; i < nx; ++i) line[i] = in[i + nx * (j + ny * k)];
+            for (int i = 0; i < nx; ++i)
+                out[i + nx * (j + ny * k)] = cd_at(scheme, tile, line, nx, i, dx);
+        }
+    free(buf);
+    return 0;
+}
+
 int or_cd6_field(int nx, int ny, int nz, double dx, const double *in, const double *halo_l,
                  const double *halo_r, double *out) {
     double *buf = (double *)malloc(sizeof(double) * (size_t)(nx + 6));
@@ -1002,7 +1057,7 @@ static void inviscid_direction(const or_box *b, int d, double *const fl[5], doub
 
 typedef struct {
     const or_box *b;
-    int d, n, na;
+    int d, n, na, scheme, tile;
     long s;
     double delta;
     const double *src;
@@ -1019,18 +1074,25 @@ static void cd6_range(void *vc, int part, long lo, long hi) {
         const int c = (int)(L / x->na), a = (int)(L - (long)c * x->na);
         long base = line_base(x->b, x->d, a, c);
         gather_periodic(x->src, base, x->s, n, line);
-        for (int i = 0; i < n; ++i) x->dst[base + (long)i * x->s] = cd6_at(line, i, x->delta);
+        for (int i = 0; i < n; ++i)
+            x->dst[base + (long)i * x->s] = cd_at(x->scheme, x->tile, line, n, i, x->delta);
     }
     free(buf);
 }
 
-/* CD6 along direction d of a periodic field (the halo exchange with one
- * rank is the periodic wrap). */
-static void cd6_direction(const or_box *b, int d, const double *src, double *dst) {
+/* The direction's differential scheme along direction d of a periodic field
+ * (the halo exchange with one rank is the periodic wrap), with the tilesize
+ * the reference passes it: the inviscid scheme's bufferSize.  With cd8 and a
+ * bufferSize below 4 the reference's stencils read outside their halo buffers
+ * and across line starts (centraldifference8th.cpp:46-57, :101-113); here
+ * they read the periodic neighbours. */
+static void cd_direction(const or_box *b, int d, const double *src, double *dst) {
     cd6_ctx x;
     int nc;
     x.b = b;
     x.d = d;
+    x.scheme = b->vis[d];
+    x.tile = halo_of(b->scheme[d]);
     x.n = dir_len(b, d);
     x.s = dir_stride(b, d);
     x.delta = d == 0 ? b->dx : (d == 1 ? b->dy : b->dz);
@@ -1148,12 +1210,13 @@ double or_rhs(const or_box *b, const double *const q[5], double *const rhs[5]) {
     double *dvis[15] = {0};
     double *blk_v = NULL;
     if (b->navier_stokes) {
-        /* solveGrads (NaiverStokes3d.cpp:87-175): CD6 of u, v, w, T along x, y, z */
+        /* solveGrads (NaiverStokes3d.cpp:87-175): derivatives of u, v, w, T
+         * along x, y, z with each direction's differential scheme */
         double *g[12];
         double *blk_g = alloc_fields(12, N, g);
         const double *src[4] = {prim[1], prim[2], prim[3], prim[5]};
         for (int vix = 0; vix < 4; ++vix)
-            for (int d = 0; d < 3; ++d) cd6_direction(b, d, src[vix], g[vix * 3 + d]);
+            for (int d = 0; d < 3; ++d) cd_direction(b, d, src[vix], g[vix * 3 + d]);
         /* solveViscousFlux (NaiverStokes3d.cpp:177-303) */
         double *fv[15];
         double *blk_fv = alloc_fields(15, N, fv);
@@ -1163,7 +1226,7 @@ double or_rhs(const or_box *b, const double *const q[5], double *const rhs[5]) {
         /* setDerivativesVis (NaiverStokes3d.cpp:305-369) */
         blk_v = alloc_fields(15, N, dvis);
         for (int d = 0; d < 3; ++d)
-            for (int e = 0; e < 5; ++e) cd6_direction(b, d, fv[d * 5 + e], dvis[d * 5 + e]);
+            for (int e = 0; e < 5; ++e) cd_direction(b, d, fv[d * 5 + e], dvis[d * 5 + e]);
         free(blk_fv);
     }
     /* solveRHS: NaiverStokes3d.cpp:385-499 / euler3d.cpp:389-457 */
@@ -1272,9 +1335,9 @@ void or_init_tgv(const or_box *b, double x0, double y0, double z0, double *const
 }
 
 /* ---------------------------------------------------------- statistics --- */
-/* postproc::solveQ (postproc.cpp:736-930).  Gradients are CD6 of the
- * primitives (solveGrad -> the operator's differential scheme, periodic
- * halos); the per-cell expressions and the (k, j, i) summation order follow
+/* postproc::solveQ (postproc.cpp:736-930).  Gradients are the primitives'
+ * derivatives by each direction's differential scheme (solveGrad -> the
+ * operator's differential scheme, periodic halos; postproc.cpp:2285-2297); the per-cell expressions and the (k, j, i) summation order follow
  * postproc.cpp:805-853, the field averages MPICommunicator.cpp:161-185. */
 void or_stats(const or_box *b, const double *const q[5], double out[OR_NSTATS]) {
     const long N = (long)b->nx * b->ny * b->nz;
@@ -1285,7 +1348,7 @@ void or_stats(const or_box *b, const double *const q[5], double out[OR_NSTATS]) 
     or_con2prim(b, q, prim);
     const double *src[3] = {prim[1], prim[2], prim[3]};
     for (int v = 0; v < 3; ++v)
-        for (int d = 0; d < 3; ++d) cd6_direction(b, d, src[v], g[v * 3 + d]);
+        for (int d = 0; d < 3; ++d) cd_direction(b, d, src[v], g[v * 3 + d]);
     const double non_dim_T_ref = b->t_ref / b->t_inf;
     double u_rms_aver = 0.0, miu_aver = 0.0, rho_bar = 0.0, div_aver = 0.0, alpha_aver = 0.0;
     double Skew2 = 0.0, Skew3 = 0.0, diss = 0.0;

@@ -27,6 +27,9 @@ enum { OR_WENO5JS = 0, OR_WENO5Z = 1, OR_CRWENO5 = 2, OR_WENO7 = 3, OR_HCCS = 4,
        OR_HCCS78 = 6, OR_WENO3JS = 7, OR_UPWIND1 = 8 };
 /* viscosity models (physicsModel.cpp:44-49; power law is an extra model) */
 enum { OR_SUTHERLAND = 0, OR_CONSTANT = 1, OR_POWERLAW = 2 };
+/* differential schemes: Method.in scheme_*_vis "cd6", "cd2", "cd8"
+ * (fieldOperator.cpp:301-375; any other string is cd6) */
+enum { OR_CD6 = 0, OR_CD2 = 1, OR_CD8 = 2 };
 
 /* Reference behaviours that look like defects; each is reproduced when its
  * bit is set (the default, OR_QUIRKS_REFERENCE) and replaced by the textbook
@@ -49,6 +52,7 @@ typedef struct {
     double gamma, mach, reynolds, prandtl, t_ref, t_inf, powerlaw_exp;
     unsigned quirks;
     int riemann;        /* OR_LF, OR_AUSM, OR_AUSMP: PhysModel.in RiemannSolver */
+    int vis[3];         /* OR_CD6, OR_CD2, OR_CD8 per direction: scheme_*_vis */
 } or_box;
 
 /* flux splittings (physicsModel.cpp:16-20 map "LF", "AUSM", "AUSMp") */
@@ -82,6 +86,13 @@ int or_reconstruct_field(int scheme, int upwind, unsigned quirks, int nx, int ny
 /* centraldifference6th, same field/halo convention; out is (nx,ny,nz). */
 int or_cd6_field(int nx, int ny, int nz, double dx, const double *in, const double *halo_l,
                  const double *halo_r, double *out);
+
+/* differentialInner + differentialBoundaryL/R of the scheme (OR_CD6, OR_CD2,
+ * OR_CD8) with the reference's tilesize `tile` (1..4): halos are (tile,ny,nz)
+ * and cells within `tile` of a line end take the boundary form.  -1 for cd8
+ * with tile < 4 (the reference's stencil reads outside its data there). */
+int or_cd_field(int scheme, int tile, int nx, int ny, int nz, double dx, const double *in,
+                const double *halo_l, const double *halo_r, double *out);
 
 /* tvdrk3rd::integrationAll on n cells, ui updated in place. */
 void or_rk3_stage(int stage, long n, double dt, const double *const rhs[5],

@@ -31,6 +31,12 @@ SCHEME_NAMES = {WENO5JS: "weno5js", WENO5Z: "weno5z", CRWENO5: "crweno5", WENO7:
                 HCCS: "hccs", HCCS77: "hccs77", HCCS78: "hccs78", WENO3JS: "weno3js",
                 UPWIND1: "upwind1st"}
 SUTHERLAND, CONSTANT, POWERLAW = 0, 1, 2
+CD6, CD2, CD8 = 0, 1, 2
+VIS_NAMES = {CD6: "cd6", CD2: "cd2", CD8: "cd8"}
+# the reference's bufferSize of each inviscid scheme (fieldOperator.cpp:128-290):
+# the tilesize its differential schemes get
+SCHEME_HALO = {WENO5JS: 3, WENO5Z: 3, CRWENO5: 3, WENO7: 4, HCCS: 4, HCCS77: 4, HCCS78: 4,
+               WENO3JS: 2, UPWIND1: 1}
 LF, AUSM, AUSMP = 0, 1, 2
 RIEMANN_NAMES = {LF: "LF", AUSM: "AUSM", AUSMP: "AUSMp"}
 VISC_NAMES = {SUTHERLAND: "Sutherland", CONSTANT: "Constant"}
@@ -57,6 +63,7 @@ class _Box(C.Structure):
         ("powerlaw_exp", C.c_double),
         ("quirks", C.c_uint),
         ("riemann", C.c_int),
+        ("vis", C.c_int * 3),
     ]
 
 
@@ -83,6 +90,8 @@ class Box:
     powerlaw_exp: float = 0.76
     quirks: int = QUIRKS_REFERENCE
     riemann: int = LF
+    # Method.in scheme_{x,y,z}_vis (fieldOperator.cpp:301-375)
+    vis: tuple = (CD6, CD6, CD6)
     # PhysModel.in Forcing (physicsModel.cpp:50-56): 0 None, 1 Const.  Only
     # the compiled reference runs it (the C restatement has no forcing; its
     # numpy restatement is forcing_oracle.py).
@@ -120,6 +129,8 @@ class Box:
         b.powerlaw_exp = self.powerlaw_exp
         b.quirks = int(self.quirks)
         b.riemann = int(self.riemann)
+        for d in range(3):
+            b.vis[d] = int(self.vis[d])
         return b
 
 
@@ -161,6 +172,16 @@ class Oracle:
         rc = self.lib.or_cd6_field(nx, ny, nz, C.c_double(dx), _ptr(fin), _ptr(hl), _ptr(hr),
                                    _ptr(out))
         assert rc == 0
+        return out
+
+    def cd_field(self, scheme, tile, fin, dx, hl, hr):
+        """or_cd_field: scheme CD6/CD2/CD8 with the reference's tilesize;
+        halos (nz, ny, tile)."""
+        nz, ny, nx = fin.shape
+        out = np.zeros_like(fin)
+        rc = self.lib.or_cd_field(scheme, tile, nx, ny, nz, C.c_double(dx), _ptr(fin), _ptr(hl),
+                                  _ptr(hr), _ptr(out))
+        assert rc == 0, rc
         return out
 
     def con2prim(self, box: Box, q):
@@ -231,7 +252,8 @@ def write_decks(dirpath: Path, box: Box, cfl: float = 0.5):
     (inp / "Method.in").write_text(
         "scheme_time RK3\n"
         f"scheme_x_ivs {names[0]}\nscheme_y_ivs {names[1]}\nscheme_z_ivs {names[2]}\n"
-        "scheme_x_vis cd6\nscheme_y_vis cd6\nscheme_z_vis cd6\n")
+        f"scheme_x_vis {VIS_NAMES[box.vis[0]]}\nscheme_y_vis {VIS_NAMES[box.vis[1]]}\n"
+        f"scheme_z_vis {VIS_NAMES[box.vis[2]]}\n")
     model = "NavierStokes3d" if box.navier_stokes else "Euler3d"
     (inp / "PhysModel.in").write_text(
         f"Neqs 5\nEosName IdealGas\nRiemannSolver {RIEMANN_NAMES[box.riemann]}\n"
@@ -271,6 +293,14 @@ class Reference:
         nz, ny, nx = fin.shape
         out = np.zeros_like(fin)
         self.lib.ref_cd6(nx, ny, nz, C.c_double(dx), _ptr(fin), _ptr(hl), _ptr(hr), _ptr(out))
+        return out
+
+    def cd_field(self, scheme, tile, fin, dx, hl, hr):
+        nz, ny, nx = fin.shape
+        out = np.zeros_like(fin)
+        rc = self.lib.ref_cd(scheme, tile, nx, ny, nz, C.c_double(dx), _ptr(fin), _ptr(hl),
+                             _ptr(hr), _ptr(out))
+        assert rc == 0, rc
         return out
 
     def rk3_stage(self, stage, dt, rhs, un, ui):

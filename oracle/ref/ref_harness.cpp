@@ -10,6 +10,9 @@
 //                     weno5z.cpp:18-637, crweno5.cpp:25-837); output = n+1 faces
 //   ref_cd6           centraldifference6th::differentialInner/BoundaryL/R
 //                     (centraldifference6th.cpp:16-186)
+//   ref_cd            centraldifference6th / 2nd / 8th (scheme 0 / 1 / 2) with a
+//                     given tilesize (centraldifference2nd.cpp:16-146,
+//                     centraldifference8th.cpp:22-205)
 //   ref_rk3_stage     tvdrk3rd::integrationAll (TVD-RK3.cpp:16-157)
 //   ref_split         physicsModel::solve (con2prim) + solveRiemann (RiemannLF)
 //                     (physicsModel.cpp:158-165, 276-357, 436-680)
@@ -41,7 +44,9 @@
 #include "PDEData3d.hpp"
 #include "TVD-RK3.h"
 #include "bufferData.hpp"
+#include "centraldifference2nd.hpp"
 #include "centraldifference6th.h"
+#include "centraldifference8th.hpp"
 #include "crweno5.hpp"
 #include "euler3d.h"
 #include "fft.h"
@@ -127,6 +132,16 @@ struct RefSolver {
 
 }  // namespace
 
+// one differential scheme's inner and boundary passes over a field
+template <typename S>
+void run_differential(const Field &fin, double dx, const Field &fl, const Field &fr, Field &fout,
+                      int tile) {
+    S s;
+    s.differentialInner(fin, dx, fout, tile);
+    s.differentialBoundaryL(fin, dx, fl, fout, tile);
+    s.differentialBoundaryR(fin, dx, fr, fout, tile);
+}
+
 extern "C" {
 
 // scheme: 0 = weno5js, 1 = weno5z, 2 = crweno5, 3 = weno7js, 4 = hccs,
@@ -206,6 +221,28 @@ int ref_cd6(int nx, int ny, int nz, double dx, const double *in, const double *h
     s.differentialInner(fin, dx, fout, tile);
     s.differentialBoundaryL(fin, dx, fl, fout, tile);
     s.differentialBoundaryR(fin, dx, fr, fout, tile);
+    from_field(fout, out);
+    return 0;
+}
+
+// halos are (tile, ny, nz); -1 where the scheme's stencil would read outside
+// them (cd6 with tile < 3, cd8 with tile < 4)
+int ref_cd(int scheme, int tile, int nx, int ny, int nz, double dx, const double *in,
+           const double *halo_l, const double *halo_r, double *out) {
+    const int reach = scheme == 1 ? 1 : (scheme == 2 ? 4 : 3);
+    if (tile < reach || tile > 4 || nx < 2 * tile) return -1;
+    Field fin(nx, ny, nz), fl(tile, ny, nz), fr(tile, ny, nz), fout(nx, ny, nz);
+    to_field(in, fin);
+    to_field(halo_l, fl);
+    to_field(halo_r, fr);
+    if (scheme == 0)
+        run_differential<nuc3d::centraldifference6th>(fin, dx, fl, fr, fout, tile);
+    else if (scheme == 1)
+        run_differential<nuc3d::centraldifference2nd>(fin, dx, fl, fr, fout, tile);
+    else if (scheme == 2)
+        run_differential<nuc3d::centraldifference8th>(fin, dx, fl, fr, fout, tile);
+    else
+        return -1;
     from_field(fout, out);
     return 0;
 }

@@ -19,8 +19,8 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT / "oracle"))
 
-from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, HCCS77, HCCS78, UPWIND1, WENO3JS,  # noqa: E402
-                           WENO5JS, WENO5Z, WENO7, Box, Oracle, Reference)
+from oracle_ctypes import (AUSM, AUSMP, CD2, CD6, CD8, CRWENO5, HCCS, HCCS77, HCCS78,  # noqa: E402
+                           UPWIND1, WENO3JS, WENO5JS, WENO5Z, WENO7, Box, Oracle, Reference)
 
 SCHEME_TAG = {WENO5JS: "js", WENO5Z: "z", CRWENO5: "cr", WENO7: "w7", HCCS: "hc", HCCS77: "h77",
               HCCS78: "h78", WENO3JS: "w3", UPWIND1: "u1"}
@@ -42,6 +42,10 @@ def main():
         return
     if sys.argv[1:] == ["low_order"]:  # only the weno3js / upwind1st fixtures
         low_order_fixtures(R)
+        print("fixtures written to", HERE)
+        return
+    if sys.argv[1:] == ["viscous_schemes"]:  # only the cd2 / cd8 fixtures
+        viscous_scheme_fixtures(R)
         print("fixtures written to", HERE)
         return
     rng = np.random.default_rng(2024)
@@ -215,6 +219,51 @@ def low_order_fixtures(R):
                             reynolds=box.reynolds, prandtl=box.prandtl)
 
 
+# (tag, inviscid scheme, differential scheme per direction) of the viscous-
+# scheme step fixtures
+VIS_STEP_CASES = (("js_cd2", WENO5JS, (CD2, CD2, CD2)), ("w7_cd8", WENO7, (CD8, CD8, CD8)),
+                  ("w3_cd2", WENO3JS, (CD2, CD2, CD2)), ("u1_cd2", UPWIND1, (CD2, CD2, CD2)),
+                  ("hc_mix", HCCS, (CD8, CD2, CD6)))
+
+
+def viscous_scheme_fixtures(R):
+    """The reference's other differential schemes, centraldifference2nd and
+    centraldifference8th (Method.in scheme_*_vis cd2 / cd8): the operators at
+    every tilesize they accept (cd8 reads 4 cells, so only tilesize 4), and
+    one Navier-Stokes RHS plus three steps with inviscid schemes whose
+    bufferSize covers the differential stencil (cd8 with a 4-cell scheme; cd2
+    with any, weno3js and upwind1st included), plus solveQ's statistics, whose
+    gradients take the same schemes."""
+    rng = np.random.default_rng(58)
+    shape = (5, 4, 16)
+    out = {"dx": np.array(0.37)}
+    for name, sch, tiles in (("cd2", CD2, (1, 2, 3, 4)), ("cd6", CD6, (4,)), ("cd8", CD8, (4,))):
+        for t in tiles:
+            f = rng.standard_normal(shape)
+            hl = rng.standard_normal(shape[:2] + (t,))
+            hr = rng.standard_normal(shape[:2] + (t,))
+            k = f"{name}_t{t}"
+            out[f"{k}_in"], out[f"{k}_hl"], out[f"{k}_hr"] = f, hl, hr
+            out[f"{k}_out"] = R.cd_field(sch, t, f, 0.37, hl, hr)
+    np.savez_compressed(HERE / "operators_vis.npz", **out)
+    for tag, sch, vis in VIS_STEP_CASES:
+        box = Box(16, 12, 10, scheme=(sch,) * 3, vis=vis, mach=0.3, reynolds=800.0,
+                  prandtl=0.71)
+        q = perturbed_tgv(box, 17 + sch)
+        rhs, dtl = R.rhs(box, q)
+        qn, dt, res = R.run_steps(box, 0.5, 3, q)
+        np.savez_compressed(HERE / f"step_vis_{tag}.npz", q0=np.stack(q), rhs=np.stack(rhs),
+                            dt_local=np.array(dtl), q3=np.stack(qn), dt=dt, res=res,
+                            shape=np.array(box.shape), mach=box.mach, reynolds=box.reynolds,
+                            prandtl=box.prandtl, scheme=np.array(box.scheme),
+                            vis=np.array(vis))
+    box = Box(24, 20, 16, scheme=(WENO7,) * 3, vis=(CD8, CD2, CD6), mach=0.3, reynolds=400.0)
+    q = perturbed_tgv(box, 5)
+    np.savez_compressed(HERE / "stats_vis.npz", q=np.stack(q), stats=R.stats(box, q),
+                        shape=np.array(box.shape), mach=box.mach, reynolds=box.reynolds,
+                        prandtl=box.prandtl, scheme=np.array(box.scheme), vis=np.array(box.vis))
+
+
 def forcing_fixture(R):
     """physicsModel::AddForcing_Const (physicsModel.cpp:1368-1641) run by the
     reference itself (FFTs through the DFT stand-in for FFTW): one RHS with
@@ -320,6 +369,7 @@ def stats_fixture(R):
     np.savez_compressed(HERE / "stats.npz", q=np.stack(q), stats=out,
                         shape=np.array(box.shape), mach=box.mach, reynolds=box.reynolds,
                         prandtl=box.prandtl)
+    viscous_scheme_fixtures(R)
 
 
 if __name__ == "__main__":

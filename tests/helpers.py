@@ -39,7 +39,7 @@ def desc_from_box(box, precision=0):
                       visc_model=box.visc_model, gamma=box.gamma, mach=box.mach,
                       reynolds=box.reynolds, prandtl=box.prandtl, t_ref=box.t_ref,
                       t_inf=box.t_inf, powerlaw_exp=box.powerlaw_exp, precision=precision,
-                      quirks=box.quirks, riemann=box.riemann)
+                      quirks=box.quirks, riemann=box.riemann, vis_scheme=tuple(box.vis))
 
 
 def _ulp_perturbed(q, seed):

@@ -51,3 +51,13 @@ def test_riemann_solver_round_trip(tmp_path, riemann):
     text = (tmp_path / "inp" / "PhysModel.in").read_text()
     assert f"RiemannSolver {['LF', 'AUSM', 'AUSMp'][riemann]}\n" in text
     assert nb.read_decks(tmp_path)[0].riemann == riemann
+
+
+def test_differential_scheme_strings_follow_the_reference(tmp_path):
+    """fieldOperator.cpp:301-375: scheme_*_vis cd8, cd6 or cd2 per direction;
+    an unknown string falls back to cd6."""
+    nb.write_decks(tmp_path, nb.BoxDesc(16, 16, 16, vis_scheme=(nb.CD8, nb.CD2, nb.CD6)))
+    assert nb.read_decks(tmp_path)[0].vis_scheme == (nb.CD8, nb.CD2, nb.CD6)
+    p = tmp_path / "inp" / "Method.in"
+    p.write_text(p.read_text().replace("scheme_x_vis cd8", "scheme_x_vis cd4"))
+    assert nb.read_decks(tmp_path)[0].vis_scheme == (nb.CD6, nb.CD2, nb.CD6)

@@ -39,6 +39,7 @@ def parsed(text):
     dict(nx=24, ny=16, nz=12, scheme=(4, 2, 4)),
     dict(nx=32, ny=32, nz=32, forcing=1, forcing_amp=0.02, forcing_hel=0.1, forcing_k=2.0),
     dict(nx=32, ny=32, nz=32, forcing=2, forcing_amp=0.3, forcing_k=2.0),
+    dict(nx=20, ny=16, nz=16, scheme=(3, 7, 8), vis_scheme=(2, 1, 0)),
 ])
 def test_driver_reads_decks_like_the_python_reader(driver, tmp_path, kw):
     import nuc3d_b200 as nb
@@ -59,6 +60,7 @@ def test_driver_reads_decks_like_the_python_reader(driver, tmp_path, kw):
     assert float(got["endStep"]) == io["endStep"]
     assert int(got["forcing"]) == ref.forcing
     assert int(got["riemann"]) == ref.riemann
+    assert [int(x) for x in r.stdout.split(" vis ")[1].split()[:3]] == list(ref.vis_scheme)
     for k in ("forcing_amp", "forcing_hel", "forcing_k"):
         assert float(got[k]) == getattr(ref, k)
 
@@ -82,9 +84,9 @@ def test_driver_rejects_what_the_path_does_not_cover(driver, tmp_path):
     r = run(driver, tmp_path, "--check-decks")
     assert r.returncode != 0 and "word Bogus does not exist" in r.stderr
     nb.write_decks(tmp_path, nb.BoxDesc(16, 16, 16))
-    text = (inp / "Method.in").read_text().replace("scheme_z_vis cd6", "scheme_z_vis cd8")
+    text = (inp / "Method.in").read_text().replace("scheme_time RK3", "scheme_time RK4")
     (inp / "Method.in").write_text(text)
     r = run(driver, tmp_path, "--check-decks")
-    assert r.returncode != 0 and "cd8" in r.stderr
+    assert r.returncode != 0 and "RK4" in r.stderr
     r = run(driver, "--help")
     assert r.returncode == 0 and "usage" in r.stdout

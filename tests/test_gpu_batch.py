@@ -7,8 +7,8 @@ import numpy as np
 import pytest
 
 from helpers import desc_from_box, max_rel_l2
-from oracle_ctypes import (CRWENO5, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, WENO5JS, WENO5Z, Box,
-                           Oracle)
+from oracle_ctypes import (CD2, CD6, CD8, CRWENO5, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED, WENO5JS,
+                           WENO5Z, Box, Oracle)
 
 pytestmark = pytest.mark.gpu
 
@@ -29,10 +29,12 @@ def mix_of_boxes():
         Box(32, 18, 9, scheme=(WENO5Z, WENO5JS, CRWENO5), mach=0.25, reynolds=900.0,
             quirks=QUIRKS_REFERENCE & ~Q_CRWENO_BOUNDED),
         Box(12, 20, 16, scheme=(WENO5JS,) * 3, mach=0.15, reynolds=300.0, visc_model=1),
+        # cd8 / cd2 / cd6 viscous stencils: the 2.5-D kernels' reach-4 class
+        Box(16, 16, 12, scheme=(WENO5Z,) * 3, vis=(CD8, CD2, CD6), mach=0.2, reynolds=500.0),
     ]
     O = Oracle()
     states = [[a * (1 + 0.02 * rng.standard_normal(a.shape)) for a in O.tgv(b)] for b in boxes]
-    cfls = [0.5, 0.4, 0.45, 0.3, 0.5]
+    cfls = [0.5, 0.4, 0.45, 0.3, 0.5, 0.45]
     return boxes, states, cfls
 
 

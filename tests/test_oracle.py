@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 from helpers import box_from_golden, golden
-from oracle_ctypes import (AUSM, AUSMP, CRWENO5, HCCS, HCCS77, HCCS78, LF, QUIRKS_REFERENCE, Q_CRWENO_BOUNDED,
+from oracle_ctypes import (AUSM, AUSMP, CD2, CD6, CD8, CRWENO5, HCCS, HCCS77, HCCS78, LF,
+                           QUIRKS_REFERENCE, Q_CRWENO_BOUNDED,
                            Q_WENOZ_BETA2, UPWIND1, WENO3JS, WENO5JS, WENO5Z, WENO7, Box, Oracle,
                            Reference)
 
@@ -343,3 +344,44 @@ def test_low_order_euler_rhs_and_steps_match_reference_golden(O, scheme):
     q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
     assert np.array_equal(np.stack(q3), z["q3"])
     assert np.array_equal(dt, z["dt"]) and np.array_equal(res, z["res"])
+
+
+def _vis_box(z):
+    nz, ny, nx = (int(v) for v in z["shape"])
+    return Box(nx, ny, nz, scheme=tuple(int(s) for s in z["scheme"]),
+               vis=tuple(int(v) for v in z["vis"]), mach=float(z["mach"]),
+               reynolds=float(z["reynolds"]), prandtl=float(z["prandtl"]))
+
+
+@pytest.mark.parametrize("key", ["cd2_t1", "cd2_t2", "cd2_t3", "cd2_t4", "cd6_t4", "cd8_t4"])
+def test_differential_schemes_match_reference_golden(O, key):
+    """centraldifference2nd / 6th / 8th at the tilesizes they accept: cells
+    within the tilesize of a line end read the halo; cd8's inner cells use its
+    two one-sided sums, its boundary cells symmetric differences."""
+    z = golden("operators_vis.npz")
+    scheme = {"cd2": CD2, "cd6": CD6, "cd8": CD8}[key[:3]]
+    out = O.cd_field(scheme, int(key[-1]), z[f"{key}_in"], float(z["dx"]), z[f"{key}_hl"],
+                     z[f"{key}_hr"])
+    assert np.array_equal(out, z[f"{key}_out"])
+
+
+@pytest.mark.parametrize("tag", ["js_cd2", "w7_cd8", "w3_cd2", "u1_cd2", "hc_mix"])
+def test_viscous_schemes_rhs_and_steps_match_reference_golden(O, tag):
+    """Navier-Stokes with Method.in scheme_*_vis cd2 / cd8 (one direction mix
+    cd8 / cd2 / cd6): RHS, dt and three steps bitwise."""
+    z = golden(f"step_vis_{tag}.npz")
+    box = _vis_box(z)
+    rhs, dtl = O.rhs(box, list(z["q0"]))
+    assert np.array_equal(np.stack(rhs), z["rhs"]) and dtl == float(z["dt_local"])
+    q3, dt, res = O.run_steps(box, 0.5, 3, list(z["q0"]))
+    assert np.array_equal(np.stack(q3), z["q3"])
+    assert np.array_equal(dt, z["dt"]) and np.array_equal(res, z["res"])
+
+
+def test_stats_with_viscous_schemes_match_reference_golden(O):
+    """solveQ's gradients take the operator's differential schemes (cd8, cd2,
+    cd6 along x, y, z here)."""
+    z = golden("stats_vis.npz")
+    box = _vis_box(z)
+    got = O.stats(box, list(z["q"]))
+    np.testing.assert_allclose(got[:25], z["stats"], rtol=1e-11, atol=0)
