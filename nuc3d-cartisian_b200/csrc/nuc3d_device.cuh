@@ -134,6 +134,24 @@ __device__ __forceinline__ double sub_(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ float sub_(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ double div_(double a, double b) { return __ddiv_rn(a, b); }
 
+// ---- packed FP32 pairs (sm_100 f32x2 arithmetic) ----
+// Component-wise each is the correctly rounded scalar operation of the same
+// name (fma_, mul_, add_, sub_), so a pair of reconstructions computed
+// together gives bitwise the values of the two computed apart, in half the
+// FP32 instructions.  a - b is formed as fma(b, -1, a): one rounding, as the
+// subtraction.
+__device__ __forceinline__ float2 splat2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 fma2_(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2_(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2_(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2_(float2 a, float2 b) {
+    return __ffma2_rn(b, splat2(-1.0f), a);
+}
+__device__ __forceinline__ float2 dd2_of(float2 D) {
+    const float2 t = mul2_(splat2(float(2.0 * K::SG0)), D);
+    return mul2_(t, t);
+}
+
 // second difference f0 - 2 f1 + f2
 template <typename B>
 __device__ __forceinline__ B d2_(B f0, B f1, B f2) {
@@ -312,6 +330,53 @@ __device__ __forceinline__ B weno5_face_dq(B f2, B a21, B a32, B a43, B D0, B D2
     const B g2 = fma_(B(2), a32, mul_(B(-0.5), a43));
     if (SCHEME == SCHEME_Z) return weno_z_combine_dq(is0, is1, is2, g0, g1, g2, f2);
     return weno_js_combine_dq(is0, is1, is2, g0, g1, g2, f2);
+}
+
+// Two FP32 faces at once (component x: one stencil, y: another), packed:
+// component-wise the operations of weno5_face_dq<SCHEME, float> with
+// weno_z_combine_dq / weno_js_combine_dq, in the same order, so each
+// component is bitwise that face.  The reciprocals, |.| and min stay scalar.
+template <int SCHEME>
+__device__ __forceinline__ float2 weno5_face_dq2(float2 f2, float2 a21, float2 a32, float2 a43,
+                                                 float2 D0, float2 D2, float2 dd0, float2 dd1,
+                                                 float2 dd2) {
+    const float2 e0 = fma2_(splat2(2.0f), a21, D0);
+    const float2 e1 = add2_(a21, a32);
+    const float2 e2 = fma2_(splat2(-2.0f), a32, D2);
+    const float2 is0 = fma2_(e0, e0, dd0), is1 = fma2_(e1, e1, dd1), is2 = fma2_(e2, e2, dd2);
+    const float2 g0 = fma2_(splat2(float(1.0 / 3.0)), D0, mul2_(splat2(0.5f), a21));
+    const float2 g1 = fma2_(splat2(2.0f), a32, a21);
+    const float2 g2 = fma2_(splat2(2.0f), a32, mul2_(splat2(-0.5f), a43));
+    float2 a0, a1, a2;
+    if (SCHEME == SCHEME_Z) {
+        const float ss = 4.0f * 1.0e-30f, cap = 1.0e15f;
+        const float2 d = sub2_(is2, is0);
+        const float2 tau = make_float2(fabsf(d.x), fabsf(d.y));
+        const float2 q0 = add2_(is0, splat2(ss)), q1 = add2_(is1, splat2(ss)),
+                     q2 = add2_(is2, splat2(ss));
+        float2 t0 = mul2_(tau, make_float2(frcp_fast(q0.x), frcp_fast(q0.y)));
+        float2 t1 = mul2_(tau, make_float2(frcp_fast(q1.x), frcp_fast(q1.y)));
+        float2 t2 = mul2_(tau, make_float2(frcp_fast(q2.x), frcp_fast(q2.y)));
+        t0 = make_float2(fminf(t0.x, cap), fminf(t0.y, cap));
+        t1 = make_float2(fminf(t1.x, cap), fminf(t1.y, cap));
+        t2 = make_float2(fminf(t2.x, cap), fminf(t2.y, cap));
+        a0 = fma2_(t0, t0, splat2(1.0f));
+        a1 = fma2_(t1, t1, splat2(1.0f));
+        a2 = fma2_(t2, t2, splat2(1.0f));
+    } else {
+        const float ss = 4.0f * 1.0e-6f;
+        const float2 q0 = add2_(splat2(ss), is0), q1 = add2_(splat2(ss), is1),
+                     q2 = add2_(splat2(ss), is2);
+        const float2 r0 = make_float2(frcp_fast(q0.x), frcp_fast(q0.y));
+        const float2 r1 = make_float2(frcp_fast(q1.x), frcp_fast(q1.y));
+        const float2 r2 = make_float2(frcp_fast(q2.x), frcp_fast(q2.y));
+        a0 = mul2_(r0, r0);
+        a1 = mul2_(r1, r1);
+        a2 = mul2_(r2, r2);
+    }
+    const float2 num = fma2_(a2, g2, fma2_(a1, g1, mul2_(a0, g0)));
+    const float2 den = fma2_(splat2(6.0f), a1, fma2_(splat2(3.0f), a2, a0));
+    return fma2_(num, make_float2(frcp_fast(den.x), frcp_fast(den.y)), f2);
 }
 
 // 4 (13/12) D^2 as (2 sqrt(13/12) D)^2 (the sweeps' indicators are formed
