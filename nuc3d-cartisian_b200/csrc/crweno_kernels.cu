@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
     const int ls = nmax + 2 * H;                       // staged cells per line
     B *sF = reinterpret_cast<B *>(smem_raw);           // [sign][line][ls]
     B *sRow = sF + 2 * kCrTL * ls;                     // [warp][3][ms][32]
-    __shared__ double sRef[2][kCrTL];
+    __shared__ double sRef[2][5][kCrTL];
 
     const WorkItem it = items[blockIdx.x];
     const BoxDev &bd = boxes[it.box];
@@ -253,16 +253,23 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
         __syncthreads();
     }
 
-    for (int e = 0; e < 5; ++e) {
-        if (mixed) {  // per-line reference: the split flux at cell 0
-            if (threadIdx.x < kCrTL) {
+    if (mixed) {  // per-line references of the five equations: the split fluxes at cell 0
+        if (threadIdx.x < kCrTL) {
+            const bool in = l0 + (int)threadIdx.x < nl;
+            const long long g = in ? gidx(threadIdx.x, 0) : 0;
+            const double un = in ? wbase[DIR * np + g] : 0.0, p = in ? wbase[3 * np + g] : 0.0,
+                         c = in ? wbase[4 * np + g] : 0.0;
+#pragma unroll
+            for (int e = 0; e < 5; ++e) {
                 double fp = 0.0, fm = 0.0;
-                if (l0 + (int)threadIdx.x < nl) split(e, gidx(threadIdx.x, 0), fp, fm);
-                sRef[0][threadIdx.x] = fp;
-                sRef[1][threadIdx.x] = fm;
+                if (in) split_v(e, qbase[e * np + g], un, p, c, fp, fm);
+                sRef[0][e][threadIdx.x] = fp;
+                sRef[1][e][threadIdx.x] = fm;
             }
-            __syncthreads();
         }
+        __syncthreads();
+    }
+    for (int e = 0; e < 5; ++e) {
         // stage F+ / F- of cells -H .. n+H-1
         const int nst = n + 2 * H;
         // x lines: (line, cell) of t advanced without a division
@@ -293,8 +300,8 @@ __global__ void __launch_bounds__(kCrThreads, sizeof(B) == 8 ? 3 : 4)
                 pos = pos < 0 ? pos + n : (pos >= n ? pos - n : pos);
                 split(e, gidx(l, pos), fp, fm);
                 if (mixed) {
-                    fp = sub_(fp, sRef[0][l]);
-                    fm = sub_(fm, sRef[1][l]);
+                    fp = sub_(fp, sRef[0][e][l]);
+                    fm = sub_(fm, sRef[1][e][l]);
                 }
             }
             sF[l * ls + pc] = B(fp);
