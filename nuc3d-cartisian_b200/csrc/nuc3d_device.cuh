@@ -678,6 +678,52 @@ __device__ __forceinline__ float weno7_face_eps(float f0, float f1, float f2, fl
     return fma_(mul_(num, frcp_fast(den)), 1.0f / 12.0f, f3);
 }
 
+// Two FP32 WENO7 faces at once (component x: one stencil, y: another) on
+// the packed f32x2 arithmetic: component-wise the operations of
+// weno7_face_eps<float> in the same order, so each component is bitwise that
+// face.  The reciprocals, max, |.| and min stay scalar.
+__device__ __forceinline__ float2 w7_beta2(float2 u, float2 a, float2 b, float p, float r,
+                                           float s, float t, float v) {
+    const float2 tu = fma2_(splat2(r), b, fma2_(splat2(p), a, mul2_(splat2(240.0f), u)));
+    const float2 ta = fma2_(splat2(t), b, mul2_(splat2(s), a));
+    return fma2_(u, tu, fma2_(a, ta, mul2_(mul2_(splat2(v), b), b)));
+}
+__device__ __forceinline__ float2 weno7_face2(float2 f0, float2 f1, float2 f2, float2 f3,
+                                              float2 f4, float2 f5, float2 f6) {
+    const float ss = 1.0e-20f;
+    const float2 d1 = sub2_(f1, f0), d2 = sub2_(f2, f1), d3 = sub2_(f3, f2);
+    const float2 d4 = sub2_(f4, f3), d5 = sub2_(f5, f4), d6 = sub2_(f6, f5);
+    const float2 s2 = sub2_(d2, d1), s3 = sub2_(d3, d2), s4 = sub2_(d4, d3), s5 = sub2_(d5, d4),
+                 s6 = sub2_(d6, d5);
+    float2 is[4], r[4];
+    is[0] = w7_beta2(d2, s2, s3, -160.0f, 880.0f, 547.0f, -1854.0f, 2107.0f);
+    is[1] = w7_beta2(d3, s3, s4, 80.0f, 160.0f, 267.0f, -494.0f, 547.0f);
+    is[2] = w7_beta2(d4, s4, s5, -160.0f, -80.0f, 547.0f, -494.0f, 267.0f);
+    is[3] = w7_beta2(d5, s5, s6, -880.0f, 160.0f, 2107.0f, -1854.0f, 547.0f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) is[k] = make_float2(fmaxf(is[k].x, 0.0f), fmaxf(is[k].y, 0.0f));
+    r[0] = fma2_(splat2(3.0f), d1, fma2_(splat2(-10.0f), d2, mul2_(splat2(13.0f), d3)));
+    r[1] = fma2_(splat2(-1.0f), d2, fma2_(splat2(4.0f), d3, mul2_(splat2(3.0f), d4)));
+    r[2] = fma2_(splat2(-1.0f), d5, fma2_(splat2(6.0f), d4, d3));
+    r[3] = fma2_(splat2(9.0f), d4, fma2_(splat2(-4.0f), d5, d6));
+    const float cap = 1.0e15f;
+    const float c[4] = {float(K7::C0), float(K7::C1), float(K7::C2), float(K7::C3)};
+    const float2 dt = sub2_(is[0], is[3]);
+    const float2 tau = make_float2(fabsf(dt.x), fabsf(dt.y));
+    float2 al[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 q = add2_(splat2(ss), is[k]);
+        const float2 t0 = mul2_(tau, make_float2(frcp_fast(q.x), frcp_fast(q.y)));
+        const float2 t = make_float2(fminf(t0.x, cap), fminf(t0.y, cap));
+        al[k] = mul2_(splat2(c[k]), fma2_(t, t, splat2(1.0f)));
+    }
+    const float2 num = fma2_(al[3], r[3], fma2_(al[2], r[2], fma2_(al[1], r[1], mul2_(al[0], r[0]))));
+    const float2 den = add2_(add2_(add2_(al[0], al[1]), al[2]), al[3]);
+    return fma2_(mul2_(num, make_float2(frcp_fast(den.x), frcp_fast(den.y))),
+                 splat2(1.0f / 12.0f), f3);
+}
+
 // weno3js (weno3js.cpp:79-93 for '+', :134-148 for '-', and its halo
 // forms) on an upwind-oriented stencil g0..g2: indicators (g0 - g1)^2 and
 // (g1 - g2)^2, candidates -g0/2 + 3 g1/2 and (g1 + g2)/2, linear weights
