@@ -463,6 +463,14 @@ def run_b200(args, rank, world, local_rank):
             "autotuned_sweep_variant": tuning32,
         }
 
+    # The per-GPU characterisations (scheme timings, the 2000-step statistics
+    # leg, the 384^3 configuration, the served stream) are the same on every
+    # rank: a run on N > 1 GPUs measures the replicas' headline, mixed and
+    # ensemble rates only, so that it holds the N GPUs for about as long as
+    # the timed work needs.
+    per_gpu_only = ["schemes", "long_horizon", "config3", "served"] if world > 1 else []
+    if world > 1:
+        args.skip_schemes = args.skip_long = args.skip_config3 = True
     schemes = None if args.skip_schemes else run_schemes(args, desc, q, stream, timed_steps,
                                                          max_over_ranks)
     long_horizon = None if (args.skip_long or args.skip_mixed) else run_long_horizon(
@@ -522,6 +530,8 @@ def run_b200(args, rank, world, local_rank):
         "served": served,
         "cpu_baseline": cpu,
     }
+    if per_gpu_only:
+        line["legs_run_at_one_gpu_only"] = per_gpu_only
     reps.close()
     return line
 
