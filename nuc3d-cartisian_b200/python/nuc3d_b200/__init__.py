@@ -774,17 +774,44 @@ def probe_peak(precision=FP64) -> float:
     return t.value
 
 
+# halo width of each reconstruction scheme (the reference's bufferSize,
+# fieldOperator.cpp:128-175)
+SCHEME_HALO = {WENO5JS: 3, WENO5Z: 3, CRWENO5: 3, WENO7JS: 4, HCCS: 4, HCCS77: 4, HCCS78: 4,
+               WENO3JS: 2, UPWIND1ST: 1}
+
+
+def _operand(t, shape, name):
+    """The operator entry points take raw device pointers: check that each
+    tensor is a contiguous FP64 CUDA tensor of exactly the size the kernel
+    reads or writes, so that a wrong halo width cannot turn into a read
+    outside the buffer."""
+    if (not hasattr(t, "data_ptr") or not t.is_cuda or str(t.dtype) != "torch.float64"
+            or not t.is_contiguous() or tuple(t.shape) != tuple(shape)):
+        raise ValueError(f"{name}: need a contiguous float64 CUDA tensor of shape {tuple(shape)}, "
+                         f"got {getattr(t, 'dtype', type(t))} {tuple(getattr(t, 'shape', ()))}")
+
+
 def reconstruct(scheme, upwind, quirks, d_in, d_hl, d_hr, d_out, stream=None):
-    """nuc3d_reconstruct on torch CUDA tensors shaped (nz,ny,nx), (nz,ny,3)x2,
-    (nz,ny,nx+1)."""
+    """nuc3d_reconstruct on torch CUDA tensors shaped (nz,ny,nx), (nz,ny,H)x2
+    (H: the scheme's halo width, SCHEME_HALO), (nz,ny,nx+1)."""
     nz, ny, nx = d_in.shape
+    h = SCHEME_HALO.get(scheme, 3)
+    _operand(d_in, (nz, ny, nx), "in")
+    _operand(d_hl, (nz, ny, h), "halo_l")
+    _operand(d_hr, (nz, ny, h), "halo_r")
+    _operand(d_out, (nz, ny, nx + 1), "out")
     check(lib().nuc3d_reconstruct(scheme, upwind, quirks, nx, ny, nz, d_in.data_ptr(),
                                   d_hl.data_ptr(), d_hr.data_ptr(), d_out.data_ptr(),
                                   _stream_handle(stream)))
 
 
 def cd6(dx, d_in, d_hl, d_hr, d_out, stream=None):
+    """nuc3d_cd6: (nz,ny,nx) with halos (nz,ny,3)."""
     nz, ny, nx = d_in.shape
+    _operand(d_in, (nz, ny, nx), "in")
+    _operand(d_hl, (nz, ny, 3), "halo_l")
+    _operand(d_hr, (nz, ny, 3), "halo_r")
+    _operand(d_out, (nz, ny, nx), "out")
     check(lib().nuc3d_cd6(nx, ny, nz, dx, d_in.data_ptr(), d_hl.data_ptr(), d_hr.data_ptr(),
                           d_out.data_ptr(), _stream_handle(stream)))
 
@@ -793,6 +820,10 @@ def differential(scheme, tile, dx, d_in, d_hl, d_hr, d_out, stream=None):
     """nuc3d_differential: scheme CD6 / CD2 / CD8 with the reference's
     tilesize; halos (nz, ny, tile)."""
     nz, ny, nx = d_in.shape
+    _operand(d_in, (nz, ny, nx), "in")
+    _operand(d_hl, (nz, ny, tile), "halo_l")
+    _operand(d_hr, (nz, ny, tile), "halo_r")
+    _operand(d_out, (nz, ny, nx), "out")
     check(lib().nuc3d_differential(scheme, tile, nx, ny, nz, dx, d_in.data_ptr(),
                                    d_hl.data_ptr(), d_hr.data_ptr(), d_out.data_ptr(),
                                    _stream_handle(stream)))

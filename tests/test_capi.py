@@ -64,12 +64,39 @@ def test_reconstruct_validation_without_device(args, code):
     assert nb.lib().nuc3d_last_error()
 
 
+@pytest.mark.parametrize("args,code", [
+    ((3, 4, 16, 2, 2, 0.1), nb.ERR_UNSUPPORTED),  # no such differential scheme
+    ((2, 3, 16, 2, 2, 0.1), nb.ERR_INVALID),      # cd8 reads 4 cells: tilesize 3 too small
+    ((0, 2, 16, 2, 2, 0.1), nb.ERR_INVALID),      # cd6 reads 3 cells
+    ((1, 5, 16, 2, 2, 0.1), nb.ERR_INVALID),      # tilesize above 4
+    ((1, 2, 3, 2, 2, 0.1), nb.ERR_INVALID),       # line shorter than two tiles
+    ((1, 1, 16, 2, 2, 0.0), nb.ERR_INVALID),      # dx must be > 0
+])
+def test_differential_validation_without_device(args, code):
+    rc = nb.lib().nuc3d_differential(*args, None, None, None, None, None)
+    assert rc == code
+    assert nb.lib().nuc3d_last_error()
+
+
+def test_operator_wrappers_check_their_operands():
+    """The Python operator wrappers refuse tensors the kernels would read
+    outside of (wrong halo width, host memory) before calling the library."""
+    torch = pytest.importorskip("torch")
+    a = torch.zeros((2, 2, 16), dtype=torch.float64)
+    h = torch.zeros((2, 2, 4), dtype=torch.float64)
+    with pytest.raises(ValueError):
+        nb.differential(nb.CD8, 4, 0.1, a, h, h, a.clone())  # host tensors
+    with pytest.raises(ValueError):
+        nb.reconstruct(nb.WENO5JS, 1, nb.QUIRKS_REFERENCE, a, h, h,
+                       torch.zeros((2, 2, 17), dtype=torch.float64))
+
+
 def test_ctx_create_rejects_bad_descriptions_without_device():
     L = nb.lib()
     h = C.c_void_p()
     for bad in (nb.BoxDesc(4, 16, 16), nb.BoxDesc(16, 16, 16, scheme=(0, 9, 0)),
                 nb.BoxDesc(16, 16, 16, mach=-1.0), nb.BoxDesc(16, 16, 16, precision=3),
-                nb.BoxDesc(16, 16, 16, riemann=3)):
+                nb.BoxDesc(16, 16, 16, riemann=3), nb.BoxDesc(16, 16, 16, vis_scheme=(0, 3, 0))):
         d = bad.c_struct()
         assert L.nuc3d_ctx_create(C.byref(d), None, C.byref(h)) in (nb.ERR_INVALID,
                                                                     nb.ERR_UNSUPPORTED)
