@@ -265,16 +265,35 @@ class BoxDesc:
         return int(lib().nuc3d_ctx_bytes(C.byref(d)))
 
 
-def _ptrs5(arrs) -> "_P5":
+def _ptrs5(arrs, n=None, device=None) -> "_P5":
+    """Pointers of five contiguous FP64 fields (torch tensors or numpy
+    arrays).  The library reads or writes n values through each, so n (when
+    given) and the placement (device=True: CUDA tensors, False: host memory)
+    are checked here: a short or misplaced buffer is an error, not a copy past
+    its end."""
+    if len(arrs) != 5:
+        raise ValueError(f"need 5 fields, got {len(arrs)}")
     out = _P5()
     for i, a in enumerate(arrs):
         if hasattr(a, "data_ptr"):  # torch tensor
-            assert a.is_contiguous() and str(a.dtype) == "torch.float64"
+            if not a.is_contiguous() or str(a.dtype) != "torch.float64":
+                raise ValueError(f"field {i}: need a contiguous float64 tensor")
+            size, on_dev = a.numel(), bool(a.is_cuda)
             out[i] = a.data_ptr()
         else:  # numpy array (host)
-            assert a.dtype.name == "float64" and a.flags.c_contiguous
+            if a.dtype.name != "float64" or not a.flags.c_contiguous:
+                raise ValueError(f"field {i}: need a C-contiguous float64 array")
+            size, on_dev = a.size, False
             out[i] = a.ctypes.data
+        if n is not None and size != n:
+            raise ValueError(f"field {i}: {size} values, the box has {n} cells")
+        if device is not None and on_dev != device:
+            raise ValueError(f"field {i}: expected {'CUDA' if device else 'host'} memory")
     return out
+
+
+def _on_device(q) -> bool:
+    return bool(hasattr(q[0], "is_cuda") and q[0].is_cuda)
 
 
 def _stream_handle(stream) -> int:
@@ -435,21 +454,23 @@ class Solver:
 
     def set_state(self, q):
         """q: 5 host numpy float64 arrays or 5 CUDA float64 tensors."""
-        if hasattr(q[0], "is_cuda") and q[0].is_cuda:
-            check(lib().nuc3d_set_state_device(self._h, _ptrs5(q)))
+        dev = _on_device(q)
+        p = _ptrs5(q, self.desc.cells, dev)
+        if dev:
+            check(lib().nuc3d_set_state_device(self._h, p))
         else:
-            check(lib().nuc3d_set_state_host(self._h, _ptrs5(q)))
+            check(lib().nuc3d_set_state_host(self._h, p))
 
     def set_state_async(self, q):
         """Enqueue the upload of 5 page-locked host float64 arrays on the
         solver's stream (nuc3d_set_state_host_async); they must stay valid
         until sync()."""
-        check(lib().nuc3d_set_state_host_async(self._h, _ptrs5(q)))
+        check(lib().nuc3d_set_state_host_async(self._h, _ptrs5(q, self.desc.cells, False)))
 
     def get_state_async(self, out):
         """Enqueue the download into 5 page-locked host float64 arrays
         (nuc3d_get_state_host_async); they hold the state after sync()."""
-        check(lib().nuc3d_get_state_host_async(self._h, _ptrs5(out)))
+        check(lib().nuc3d_get_state_host_async(self._h, _ptrs5(out, self.desc.cells, False)))
 
     def copy_lane(self, on: bool = True):
         """Issue this solver's host transfers in the device's copy lanes
@@ -461,10 +482,12 @@ class Solver:
         import numpy as np
         if out is None:
             out = [np.zeros(self.desc.shape) for _ in range(5)]
-        if hasattr(out[0], "is_cuda") and out[0].is_cuda:
-            check(lib().nuc3d_get_state_device(self._h, _ptrs5(out)))
+        dev = _on_device(out)
+        p = _ptrs5(out, self.desc.cells, dev)
+        if dev:
+            check(lib().nuc3d_get_state_device(self._h, p))
         else:
-            check(lib().nuc3d_get_state_host(self._h, _ptrs5(out)))
+            check(lib().nuc3d_get_state_host(self._h, p))
         return out
 
     def init_state(self, init):
@@ -501,7 +524,7 @@ class Solver:
     def rhs(self, out):
         """out: 5 CUDA float64 tensors.  Returns dt_local."""
         dtl = C.c_double(0.0)
-        check(lib().nuc3d_rhs(self._h, _ptrs5(out), C.byref(dtl)))
+        check(lib().nuc3d_rhs(self._h, _ptrs5(out, self.desc.cells, True), C.byref(dtl)))
         return dtl.value
 
     def time(self) -> float:
@@ -572,19 +595,23 @@ class Batch:
         check(lib().nuc3d_batch_set_cfl(self._h, bid, cfl))
 
     def set_state(self, bid: int, q):
-        if hasattr(q[0], "is_cuda") and q[0].is_cuda:
-            check(lib().nuc3d_batch_set_state_device(self._h, bid, _ptrs5(q)))
+        dev = _on_device(q)
+        p = _ptrs5(q, self.descs[bid].cells, dev)
+        if dev:
+            check(lib().nuc3d_batch_set_state_device(self._h, bid, p))
         else:
-            check(lib().nuc3d_batch_set_state_host(self._h, bid, _ptrs5(q)))
+            check(lib().nuc3d_batch_set_state_host(self._h, bid, p))
 
     def get_state(self, bid: int, out=None):
         import numpy as np
         if out is None:
             out = [np.zeros(self.descs[bid].shape) for _ in range(5)]
-        if hasattr(out[0], "is_cuda") and out[0].is_cuda:
-            check(lib().nuc3d_batch_get_state_device(self._h, bid, _ptrs5(out)))
+        dev = _on_device(out)
+        p = _ptrs5(out, self.descs[bid].cells, dev)
+        if dev:
+            check(lib().nuc3d_batch_get_state_device(self._h, bid, p))
         else:
-            check(lib().nuc3d_batch_get_state_host(self._h, bid, _ptrs5(out)))
+            check(lib().nuc3d_batch_get_state_host(self._h, bid, p))
         return out
 
     def init_state(self, bid: int, init):
@@ -692,14 +719,14 @@ class Server:
         if q0 is not None:
             q0 = [np.ascontiguousarray(a, dtype=np.float64) for a in q0]
             r.init.kind = INIT_STATE
-            r.h_q0 = _ptrs5(q0)
+            r.h_q0 = _ptrs5(q0, desc.cells, False)
             keep.append(q0)
         else:
             r.init = _init_struct(init)
         out = None
         if want_state:
             out = [np.empty(desc.shape) for _ in range(5)]
-            r.h_q_out = _ptrs5(out)
+            r.h_q_out = _ptrs5(out, desc.cells, False)
         t = C.c_longlong(-1)
         check(lib().nuc3d_serve_submit(self._h, C.byref(r), C.byref(t)))
         self._pending[t.value] = (keep, out)
@@ -831,8 +858,8 @@ def differential(scheme, tile, dx, d_in, d_hl, d_hr, d_out, stream=None):
 
 def tvdrk3_stage(stage, dt, d_rhs, d_un, d_ui, stream=None):
     n = d_rhs[0].numel()
-    check(lib().nuc3d_tvdrk3_stage(stage, n, dt, _ptrs5(d_rhs), _ptrs5(d_un), _ptrs5(d_ui),
-                                   _stream_handle(stream)))
+    check(lib().nuc3d_tvdrk3_stage(stage, n, dt, _ptrs5(d_rhs, n, True), _ptrs5(d_un, n, True),
+                                   _ptrs5(d_ui, n, True), _stream_handle(stream)))
 
 
 from .decks import read_decks, write_decks  # noqa: E402

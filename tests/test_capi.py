@@ -150,3 +150,21 @@ def test_serve_and_init_validation_without_device():
     assert L.nuc3d_serve_wait(None, 0, 0.0, None) == nb.ERR_INVALID
     assert L.nuc3d_init_state(None, None, None) == nb.ERR_INVALID
     assert L.nuc3d_serve_destroy(None) == nb.OK
+
+
+def test_field_pointers_are_size_checked():
+    """Five fields of exactly the box's cell count, in the memory the call
+    expects; anything else is refused before the library copies."""
+    import numpy as np
+    good = [np.zeros((4, 4, 8)) for _ in range(5)]
+    nb._ptrs5(good, 128, False)
+    with pytest.raises(ValueError):
+        nb._ptrs5(good, 129, False)          # wrong size
+    with pytest.raises(ValueError):
+        nb._ptrs5(good[:4], 128, False)      # four fields
+    with pytest.raises(ValueError):
+        nb._ptrs5(good, 128, True)           # host memory where device memory is expected
+    with pytest.raises(ValueError):
+        nb._ptrs5([a.astype(np.float32) for a in good], 128, False)
+    with pytest.raises(ValueError):
+        nb._ptrs5([np.zeros((8, 4, 4)).T for _ in range(5)], 128, False)  # not C-contiguous
