@@ -111,3 +111,25 @@ def test_case_runner_module(capsys):
     main(["--n", "16", "--scheme", "crweno5", "--precision", "mixed", "--steps", "2"])
     out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     assert out["steps"] == 2 and out["dt_last"] > 0 and out["kinetic"] > 0
+
+
+def test_driver_runs_the_differential_schemes_of_its_decks(driver, tmp_path):
+    """Method.in scheme_{x,y,z}_vis cd2 / cd6 / cd8 read by the driver and run
+    through the C ABI: 5 Taylor-Green steps against the oracle with the same
+    schemes (cd8 beside a 3-cell scheme: periodic halos, as on this path)."""
+    import nuc3d_b200 as nb
+    from oracle_ctypes import CD2, CD6, CD8, WENO5JS, WENO5Z, Box, Oracle
+    d = nb.BoxDesc(24, 20, 16, mach=0.2, reynolds=800.0, prandtl=0.71,
+                   scheme=(nb.WENO5JS, nb.WENO5Z, nb.WENO5JS),
+                   vis_scheme=(nb.CD2, nb.CD6, nb.CD8))
+    nb.write_decks(tmp_path, d, io={"Benchmark": 2, "cfl": 0.5, "tl": 100.0, "postStep": 0,
+                                    "endStep": 5, "saveStep": 5})
+    assert "scheme_z_vis cd8" in (tmp_path / "inp" / "Method.in").read_text()
+    r = subprocess.run([str(driver), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    _, q = read_restart(tmp_path / "flowData" / "NUC3d_step_5_ID_0.bin", d.shape)
+    box = Box(24, 20, 16, mach=0.2, reynolds=800.0, prandtl=0.71,
+              scheme=(WENO5JS, WENO5Z, WENO5JS), vis=(CD2, CD6, CD8))
+    O = Oracle()
+    q5, _, _ = O.run_steps(box, 0.5, 5, O.tgv(box))
+    assert max_rel_l2(q, q5) < 1e-12
