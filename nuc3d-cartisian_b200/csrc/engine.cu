@@ -707,7 +707,8 @@ int Engine::enqueue_step(cudaStream_t s) {
 // on this batch's own work lists: the sweeps on the first step after a
 // rebuild that brings a new (scheme, direction) pair, the depth on the first
 // step and whenever the active cells have moved past 2x (or 1/2x) of those
-// it was tuned at.  The sweeps only write the RHS accumulator and the
+// it was tuned at.  The sweeps only write the RHS accumulator (and the x
+// sweep the primitives, with the values they already hold) and the
 // viscous-flux kernel the viscous fluxes, which every stage recomputes; the
 // update is timed as a first stage, which writes only the u1 slot that the
 // next step's first stage overwrites (and no residual), so timing on the
@@ -787,11 +788,15 @@ int Engine::autotune() {
                     continue;
                 }
                 const Range &rg = r_inv_[s][d][inv_tile_class(v)];
+                // the x sweep is timed as the step runs it, recovering the
+                // primitives of its tiles (prim_mode 1): it rewrites W with
+                // bitwise the values k_prim has just written
+                const int pm = d == 0 ? 1 : 0;
                 const double ms = time3([&]() {
                     return mixed ? launch_inviscid<float>(s, d, v, d_boxes_, d_items_ + rg.off, rg.n,
-                                                          0, d > 0, 0, stream_)
+                                                          0, d > 0, pm, stream_)
                                  : launch_inviscid<double>(s, d, v, d_boxes_, d_items_ + rg.off,
-                                                           rg.n, 0, d > 0, 0, stream_);
+                                                           rg.n, 0, d > 0, pm, stream_);
                 });
                 inv_tune_ms[s][d][v] = ms;
                 if (ms < inv_tune_ms[s][d][best]) best = v;
