@@ -81,7 +81,7 @@ STATE_BYTES_PER_CELL_UPDATE = 320  # compulsory FP64 state traffic of 3 RK stage
 # reads the state only and writes the primitives as well as its RHS) scaled
 # by the cell count (x8); the traffic of a sweep is proportional to the cells
 # it covers (whole lines, no halo growth with size along the other axes).
-INV_TRAFFIC_BYTES = 8 * (211.33696e6 + 268.335872e6 + 281.398784e6) / 3
+INV_TRAFFIC_BYTES = 8 * (212.03072e6 + 269.391872e6 + 281.837568e6) / 3
 INV_TRAFFIC_NOTE = "ncu dram__bytes_read+write of the 128^3 capture x8 (cells), mean of x/y/z"
 
 
