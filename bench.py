@@ -77,7 +77,7 @@ FLOPS_INV_LAUNCH = FLOPS_INV_Z + FLOPS_PRIM / 3
 STATE_BYTES_PER_CELL_UPDATE = 320  # compulsory FP64 state traffic of 3 RK stages
 # DRAM bytes (read + write) per launch of the FP64 WENO5-Z sweep at 256^3,
 # mean of x, y, z: the ncu capture at 128^3 in
-# profiles/k_inviscid_weno5z_fp64_128.md (211.3, 268.3, 281.4 MB; the x sweep
+# profiles/k_inviscid_weno5z_fp64_128.md (212.0, 269.4, 281.8 MB; the x sweep
 # reads the state only and writes the primitives as well as its RHS) scaled
 # by the cell count (x8); the traffic of a sweep is proportional to the cells
 # it covers (whole lines, no halo growth with size along the other axes).
